@@ -1,0 +1,234 @@
+"""ctypes front end of the oracle (liboracle_piny.so).
+
+TEST INFRASTRUCTURE ONLY: the checker for the device path.  Imported by
+tests/, the smoke check and the benchmark's CPU-baseline leg, never by the
+product package.
+
+A "system" is a dict of numpy arrays/scalars with the field names of
+``orc_system`` (piny_oracle.h), 0-based, PINY internal units.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle_piny.so")
+
+_i = C.c_int
+_d = C.c_double
+_pi = C.POINTER(C.c_int)
+_pd = C.POINTER(C.c_double)
+
+
+class OrcSystem(C.Structure):
+    _fields_ = [
+        ("natm", _i), ("ntyp", _i), ("atm_typ", _pi), ("charge", _pd),
+        ("nsplin", _i), ("ninter_unique", _i), ("inter_map", _pi), ("cutoff", _pd),
+        ("rmin_spl", _pd), ("dr_spl", _pd), ("dri_spl", _pd),
+        ("cv0", _pd), ("cdv0", _pd), ("cv0_c", _pd), ("cdv0_c", _pd),
+        ("skin", _d), ("clong", _d), ("iswit_vdw", _i),
+        ("excl_off", _pi), ("excl_j", _pi),
+        ("alp_ewd", _d), ("self_erf", _d), ("nktot", _i),
+        ("kastr", _pi), ("kbstr", _pi), ("kcstr", _pi), ("bweight", _pd),
+        ("ngrid_a", _i), ("ngrid_b", _i), ("ngrid_c", _i), ("n_interp", _i),
+        ("necor", _i), ("ecor_j1", _pi), ("ecor_j2", _pi), ("ecor_nsplin", _i),
+        ("ecor_rmin", _d), ("ecor_dr", _d), ("ecor_dri", _d), ("ecor_cv0", _pd), ("ecor_cdv0", _pd),
+        ("nbond", _i), ("bond_j1", _pi), ("bond_j2", _pi), ("bond_typ", _pi), ("nbond_typ", _i),
+        ("bond_eq", _pd), ("bond_c", _pd), ("bond_dc", _pd),
+        ("nbend", _i), ("bend_j1", _pi), ("bend_j2", _pi), ("bend_j3", _pi), ("bend_typ", _pi),
+        ("nbend_typ", _i), ("bend_c", _pd), ("bend_s", _pd), ("bend_dc", _pd), ("bend_ds", _pd),
+        ("nghost", _i), ("ghost_ncomp", _i), ("ghost_atom", _pi), ("ghost_comp", _pi), ("ghost_coef", _pd),
+    ]
+
+
+class OrcEnergies(C.Structure):
+    _fields_ = [(n, _d) for n in ("vreal", "vvdw", "vcoul", "vrecip", "vself", "vbgr", "vecor",
+                                  "vlong", "vbond", "vbend", "vintert", "vintrat")] + [("pvten", _d * 9)]
+
+
+def build():
+    """Compile the oracle restatement (plain gcc)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+class Oracle:
+    def __init__(self):
+        if not os.path.exists(LIB):
+            build()
+        self.lib = C.CDLL(LIB)
+        L = self.lib
+        L.orc_spline_table.argtypes = [_i, _d, _d, _i, _d, _d, _d, _d, _i, _pd, _pd, _pd, _pd]
+        L.orc_ewald_ecut.restype = _d
+        L.orc_ewald_ecut.argtypes = [_i, _d]
+        L.orc_kmaxv.argtypes = [_d, _pd, _pi]
+        L.orc_kvec_count.restype = _i
+        L.orc_kvec_count.argtypes = [_d, _pi, _pd]
+        L.orc_kvec_fill.restype = _i
+        L.orc_kvec_fill.argtypes = [_d, _pi, _pd, _pi, _pi, _pi]
+        L.orc_pme_grid.argtypes = [_d, _d, _pd, _pi, _i, _pi]
+        L.orc_pme_bweight.argtypes = [_i, _pi, _pi, _pi, _pi, _i, _pd]
+        L.orc_ecor_table.argtypes = [_i, _d, _d, _d, _pd, _pd, _pd, _pd, _pd]
+        L.orc_gauss_legendre.argtypes = [_i, _pd, _pd]
+        L.orc_bond_power.argtypes = [_d, _d, _d, _pd, _pd]
+        L.orc_bend_harm.argtypes = [_d, _d, _pd, _pd, _pd, _pd]
+        L.orc_clong.restype = _d
+        L.orc_clong.argtypes = [_i, _i, _pi, _pd, _pd, _d, _i]
+        L.orc_verlist.restype = C.c_long
+        L.orc_verlist.argtypes = [C.POINTER(OrcSystem), _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd,
+                                  C.c_long, _pi, _pi]
+        L.orc_energy_force.argtypes = [C.POINTER(OrcSystem), _i, _pd, _pd, _pd, C.c_long, _pi, _pi, _i,
+                                       _pd, C.POINTER(OrcEnergies)]
+
+    # -- helpers -----------------------------------------------------------
+    @staticmethod
+    def _d(a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        return a, a.ctypes.data_as(_pd)
+
+    @staticmethod
+    def _i(a):
+        a = np.ascontiguousarray(a, dtype=np.int32)
+        return a, a.ctypes.data_as(_pi)
+
+    def make_struct(self, sysd):
+        keep = []
+        s = OrcSystem()
+        for name, ctype in OrcSystem._fields_:
+            v = sysd.get(name)
+            if ctype is _pd:
+                if v is None:
+                    v = np.zeros(1)
+                a, p = self._d(v)
+                keep.append(a)
+                setattr(s, name, p)
+            elif ctype is _pi:
+                if v is None:
+                    v = np.zeros(1, np.int32)
+                a, p = self._i(v)
+                keep.append(a)
+                setattr(s, name, p)
+            else:
+                setattr(s, name, 0 if v is None else v)
+        s._keep = keep
+        return s
+
+    # -- setup -------------------------------------------------------------
+    def spline_table(self, nsplin, rmin, rmax, itype, sig, eps, alp, rheal, ishift):
+        v = np.zeros(nsplin)
+        dv = np.zeros(nsplin)
+        dr = C.c_double()
+        dri = C.c_double()
+        self.lib.orc_spline_table(nsplin, rmin, rmax, itype, sig, eps, alp, rheal, ishift,
+                                  v.ctypes.data_as(_pd), dv.ctypes.data_as(_pd), C.byref(dr), C.byref(dri))
+        return v, dv, dr.value, dri.value
+
+    def kvectors(self, kmax, hmat):
+        hmat = np.ascontiguousarray(hmat, np.float64)
+        hi = np.linalg.inv(hmat.reshape(3, 3, order="F")).reshape(-1, order="F")
+        hi = np.ascontiguousarray(hi)
+        deth = float(np.linalg.det(hmat.reshape(3, 3, order="F")))
+        ecut = self.lib.orc_ewald_ecut(kmax, deth)
+        kmaxv = np.zeros(3, np.int32)
+        self.lib.orc_kmaxv(ecut, hi.ctypes.data_as(_pd), kmaxv.ctypes.data_as(_pi))
+        n = self.lib.orc_kvec_count(ecut, kmaxv.ctypes.data_as(_pi), hi.ctypes.data_as(_pd))
+        ka = np.zeros(n, np.int32)
+        kb = np.zeros(n, np.int32)
+        kc = np.zeros(n, np.int32)
+        self.lib.orc_kvec_fill(ecut, kmaxv.ctypes.data_as(_pi), hi.ctypes.data_as(_pd),
+                               ka.ctypes.data_as(_pi), kb.ctypes.data_as(_pi), kc.ctypes.data_as(_pi))
+        return ecut, kmaxv, ka, kb, kc
+
+    def pme_grid(self, ecut, hmat, kmaxv, kmax_pme):
+        hmat = np.ascontiguousarray(hmat, np.float64)
+        hi = np.ascontiguousarray(np.linalg.inv(hmat.reshape(3, 3, order="F")).reshape(-1, order="F"))
+        deth = float(np.linalg.det(hmat.reshape(3, 3, order="F")))
+        kmaxv = np.ascontiguousarray(kmaxv, np.int32)
+        ng = np.zeros(3, np.int32)
+        self.lib.orc_pme_grid(ecut, deth, hi.ctypes.data_as(_pd), kmaxv.ctypes.data_as(_pi), kmax_pme,
+                              ng.ctypes.data_as(_pi))
+        return ng
+
+    def bweight(self, ka, kb, kc, ngrid, n_interp):
+        ka, pa = self._i(ka)
+        kb, pb = self._i(kb)
+        kc, pc = self._i(kc)
+        ng, pg = self._i(ngrid)
+        bw = np.zeros(len(ka))
+        self.lib.orc_pme_bweight(len(ka), pa, pb, pc, pg, n_interp, bw.ctypes.data_as(_pd))
+        return bw
+
+    def ecor_table(self, nsplin, rmax, alp, ecut):
+        cv0 = np.zeros(nsplin)
+        cdv0 = np.zeros(nsplin)
+        dr = C.c_double()
+        dri = C.c_double()
+        se = C.c_double()
+        self.lib.orc_ecor_table(nsplin, rmax, alp, ecut, cv0.ctypes.data_as(_pd), cdv0.ctypes.data_as(_pd),
+                                C.byref(dr), C.byref(dri), C.byref(se))
+        return cv0, cdv0, dr.value, dri.value, se.value
+
+    def bond_power(self, c2, c3, c4):
+        c = np.zeros(7)
+        dc = np.zeros(7)
+        self.lib.orc_bond_power(c2, c3, c4, c.ctypes.data_as(_pd), dc.ctypes.data_as(_pd))
+        return c, dc
+
+    def bend_harm(self, fk, theta0):
+        out = [np.zeros(7) for _ in range(4)]
+        self.lib.orc_bend_harm(fk, theta0, *[o.ctypes.data_as(_pd) for o in out])
+        return out
+
+    def clong(self, atm_typ, ntyp, c6, cutoff, rheal, iswit):
+        at, pa = self._i(atm_typ)
+        c6, p6 = self._d(c6)
+        cu, pc = self._d(cutoff)
+        return self.lib.orc_clong(len(at), ntyp, pa, p6, pc, rheal, iswit)
+
+    # -- evaluation --------------------------------------------------------
+    def verlist(self, sysd, pos1, xmod, hmat, cutskin2):
+        s = self.make_struct(sysd)
+        pos1 = np.ascontiguousarray(pos1, np.float64).reshape(-1, 3)
+        x, y, z = [np.ascontiguousarray(pos1[:, d]) for d in range(3)]
+        if xmod is not None:
+            xm = np.ascontiguousarray(xmod, np.float64).reshape(-1, 3)
+            xs = [np.ascontiguousarray(xm[:, d]) for d in range(3)]
+            xp = [a.ctypes.data_as(_pd) for a in xs]
+        else:
+            xp = [None, None, None]
+        hmat, ph = self._d(hmat)
+        cs, pcs = self._d(cutskin2)
+        n = sysd["natm"]
+        cap = 0
+        cnt = self.lib.orc_verlist(C.byref(s), x.ctypes.data_as(_pd), y.ctypes.data_as(_pd),
+                                   z.ctypes.data_as(_pd), *xp, ph, None, pcs, cap, None, None)
+        pi = np.zeros(max(cnt, 1), np.int32)
+        pj = np.zeros(max(cnt, 1), np.int32)
+        self.lib.orc_verlist(C.byref(s), x.ctypes.data_as(_pd), y.ctypes.data_as(_pd),
+                             z.ctypes.data_as(_pd), *xp, ph, None, pcs, cnt,
+                             pi.ctypes.data_as(_pi), pj.ctypes.data_as(_pi))
+        del n
+        return pi[:cnt], pj[:cnt]
+
+    def energy_force(self, sysd, pos, xmod, hmat, pi, pj, distribute_ghosts=False):
+        s = self.make_struct(sysd)
+        pos = np.ascontiguousarray(pos, np.float64)
+        P = pos.shape[0]
+        force = np.zeros_like(pos)
+        xm = None
+        if xmod is not None:
+            xm = np.ascontiguousarray(xmod, np.float64)
+        hmat, ph = self._d(hmat)
+        pi, ppi = self._i(pi)
+        pj, ppj = self._i(pj)
+        e = OrcEnergies()
+        self.lib.orc_energy_force(C.byref(s), P, pos.ctypes.data_as(_pd),
+                                  xm.ctypes.data_as(_pd) if xm is not None else None, ph, len(pi),
+                                  ppi, ppj, 1 if distribute_ghosts else 0, force.ctypes.data_as(_pd),
+                                  C.byref(e))
+        out = {n: getattr(e, n) for n, _ in OrcEnergies._fields_ if n != "pvten"}
+        out["pvten"] = np.array(e.pvten[:])
+        return force, out

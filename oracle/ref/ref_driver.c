@@ -1,0 +1,390 @@
+/*
+ * Test infrastructure only: a driver around PINY's own, unmodified CPU force
+ * path.  It parses a PINY input directory exactly as PINY's main() does
+ * (src/main/main.c:78-85) and then runs the four force sub-steps that
+ * energy_control_pimd() runs before it transforms forces to modes
+ * (src/energy/control/energy_control_pimd.c:91-111):
+ *   energy_control_initial, energy_control_inter_real,
+ *   energy_control_inter_recip, energy_control_intra.
+ * The flags are set as PINYEmpirical does (python/piny/piny.pyx:185-188):
+ * full inter and intra, no RESPA.
+ *
+ * Modes
+ *   piny_ref dump  <dir> <input> <out.bin>           one evaluation, dump all
+ *   piny_ref recip <dir> <input>                      print bead-1 PME energy
+ *   piny_ref time  <dir> <input> <reps> <nbeads>      time <reps> evaluations
+ *                                                     of the first <nbeads>
+ *
+ * The dump is a flat record file: for each record a 32-byte name, a one-byte
+ * kind ('d' double, 'i' int32), 7 pad bytes, an int64 count, then the data.
+ */
+#include "standard_include.h"
+#include "../typ_defs/typedefs_class.h"
+#include "../typ_defs/typedefs_bnd.h"
+#include "../typ_defs/typedefs_gen.h"
+#include "../typ_defs/typedefs_cp.h"
+#include "../typ_defs/typedefs_par.h"
+#include "../typ_defs/typedefs_stat.h"
+#include "../proto_defs/proto_parse_entry.h"
+#include "../proto_defs/proto_energy_ctrl_entry.h"
+#include "../proto_defs/proto_energy_ctrl_local.h"
+#include "../proto_defs/proto_intra_con_entry.h"
+#include "../proto_defs/proto_recip3d_entry.h"
+#include <unistd.h>
+#include <stdint.h>
+#include <sys/time.h>
+
+void Init_PINY(int argc, char *argv[], CLASS *class, GENERAL_DATA *general_data);
+
+static FILE *g_out;
+
+static void put(const char *name, char kind, const void *data, int64_t n)
+{
+    char hdr[40];
+    memset(hdr, 0, sizeof(hdr));
+    strncpy(hdr, name, 31);
+    hdr[32] = kind;
+    fwrite(hdr, 1, 40, g_out);
+    fwrite(&n, sizeof(int64_t), 1, g_out);
+    if (n > 0) fwrite(data, kind == 'd' ? 8 : 4, (size_t)n, g_out);
+}
+static void putd(const char *name, const double *one_based, int64_t n) { put(name, 'd', one_based + 1, n); }
+static void puti(const char *name, const int *one_based, int64_t n) { put(name, 'i', one_based + 1, n); }
+static void put1d(const char *name, double v) { put(name, 'd', &v, 1); }
+static void put1i(const char *name, int v) { put(name, 'i', &v, 1); }
+
+static double now_s(void)
+{
+    struct timeval tv;
+    gettimeofday(&tv, NULL);
+    return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
+static CLASS class_;
+static BONDED bonded_;
+static GENERAL_DATA gd_;
+static CP cp_;
+static ANALYSIS analysis_;
+
+static void setup(const char *dir, const char *input)
+{
+    if (chdir(dir) != 0) { fprintf(stderr, "piny_ref: cannot chdir to %s\n", dir); exit(2); }
+    /* PINY writes its setup log to stdout; keep it out of ours. */
+    fflush(stdout);
+    int saved = dup(1);
+    FILE *log = fopen("piny_setup.log", "w");
+    if (log) dup2(fileno(log), 1);
+    Init_PINY(0, NULL, &class_, &gd_);
+    parse(&class_, &bonded_, &gd_, &cp_, &analysis_, (char *)input);
+    fflush(stdout);
+    if (log) { dup2(saved, 1); fclose(log); }
+    close(saved);
+    class_.energy_ctrl.iget_full_inter = 1;
+    class_.energy_ctrl.iget_res_inter = 0;
+    class_.energy_ctrl.iget_full_intra = 1;
+    class_.energy_ctrl.iget_res_intra = 0;
+}
+
+static void evaluate(void)
+{
+    int ip;
+    for (ip = 1; ip <= class_.clatoms_info.pi_beads_proc; ip++)
+        get_ghost_pos(&class_.clatoms_info, &class_.clatoms_pos[ip], &class_.ghost_atoms);
+    energy_control_initial(&class_, &bonded_, &gd_);
+    energy_control_inter_real(&class_, &bonded_, &gd_);
+    energy_control_inter_recip(&class_, &bonded_, &gd_);
+    energy_control_intra(&class_, &bonded_, &gd_);
+}
+
+static void dump_all(const char *path)
+{
+    int i, ip;
+    CLATOMS_INFO *ci = &class_.clatoms_info;
+    int n = ci->natm_tot, P = ci->pi_beads;
+    g_out = fopen(path, "wb");
+    if (!g_out) { fprintf(stderr, "piny_ref: cannot open %s\n", path); exit(2); }
+
+    put1i("natm_tot", n);
+    put1i("pi_beads", P);
+    put1i("nchrg", ci->nchrg);
+    putd("q", ci->q, n);
+    putd("mass", ci->mass, n);
+    if (P > 1 && ci->xmod) {
+        putd("xmod", ci->xmod, n); putd("ymod", ci->ymod, n); putd("zmod", ci->zmod, n);
+    }
+    CELL *cell = &gd_.cell;
+    putd("hmat", cell->hmat, 9);
+    putd("hmati", cell->hmati, 9);
+    put1d("vol", cell->vol);
+    put1i("iperd", cell->iperd);
+    put1i("cubic_box_flag", cell->cubic_box_flag);
+    put1i("intra_perds", cell->intra_perds);
+
+    /* positions actually used and raw per-bead forces (M sites still loaded) */
+    double *buf = (double *)malloc(sizeof(double) * (size_t)n * P * 3 + 8);
+    for (ip = 1; ip <= P; ip++)
+        for (i = 1; i <= n; i++) {
+            size_t o = ((size_t)(ip - 1) * n + (i - 1)) * 3;
+            buf[o] = class_.clatoms_pos[ip].x[i];
+            buf[o + 1] = class_.clatoms_pos[ip].y[i];
+            buf[o + 2] = class_.clatoms_pos[ip].z[i];
+        }
+    put("pos", 'd', buf, (int64_t)n * P * 3);
+    for (ip = 1; ip <= P; ip++)
+        for (i = 1; i <= n; i++) {
+            size_t o = ((size_t)(ip - 1) * n + (i - 1)) * 3;
+            buf[o] = class_.clatoms_pos[ip].fx[i];
+            buf[o + 1] = class_.clatoms_pos[ip].fy[i];
+            buf[o + 2] = class_.clatoms_pos[ip].fz[i];
+        }
+    put("force_raw", 'd', buf, (int64_t)n * P * 3);
+    if (P > 1) {
+        for (ip = 1; ip <= P; ip++)
+            for (i = 1; i <= n; i++) {
+                size_t o = ((size_t)(ip - 1) * n + (i - 1)) * 3;
+                buf[o] = class_.clatoms_pos[ip].fxt[i];
+                buf[o + 1] = class_.clatoms_pos[ip].fyt[i];
+                buf[o + 2] = class_.clatoms_pos[ip].fzt[i];
+            }
+        put("forcet_raw", 'd', buf, (int64_t)n * P * 3);
+    }
+    /* forces after the M-site redistribution energy_control_final applies */
+    for (ip = 1; ip <= P; ip++)
+        distrib_ghost_force(ci, &class_.clatoms_pos[ip], &class_.ghost_atoms, 0);
+    for (ip = 1; ip <= P; ip++)
+        for (i = 1; i <= n; i++) {
+            size_t o = ((size_t)(ip - 1) * n + (i - 1)) * 3;
+            buf[o] = class_.clatoms_pos[ip].fx[i];
+            buf[o + 1] = class_.clatoms_pos[ip].fy[i];
+            buf[o + 2] = class_.clatoms_pos[ip].fz[i];
+        }
+    put("force", 'd', buf, (int64_t)n * P * 3);
+    free(buf);
+
+    STAT_AVG *sa = &gd_.stat_avg;
+    put1d("vintert", sa->vintert);
+    put1d("vintrat", sa->vintrat);
+    put1d("vvdw", sa->vvdw);
+    put1d("vcoul", sa->vcoul);
+    put1d("vrecip", sa->vrecip);
+    put1d("vlong", sa->vlong);
+    put1d("vbondt", sa->vbondt);
+    put1d("vbendt", sa->vbendt);
+    putd("pvten", gd_.ptens.pvten, 9);
+    putd("pvten_tot", gd_.ptens.pvten_tot, 9);
+
+    /* interaction tables */
+    ATOMMAPS *am = &class_.atommaps;
+    INTERACT *it = &class_.interact;
+    put1i("natm_typ", am->natm_typ);
+    puti("iatm_atm_typ", am->iatm_atm_typ, n);
+    int nter = am->natm_typ * (am->natm_typ + 1) / 2;
+    int nuniq = 0;
+    for (i = 1; i <= nter; i++) if (it->inter_map_index[i] > nuniq) nuniq = it->inter_map_index[i];
+    put1i("nsplin", it->nsplin);
+    put1i("ninter_unique", nuniq);
+    puti("inter_map_index", it->inter_map_index, nter);
+    putd("cutoff", it->cutoff, nter);
+    putd("cutoff_res", it->cutoff_res, nter);
+    putd("cutti", it->cutti, nter);
+    putd("cutskin", it->cutskin, nter);
+    putd("rmin_spl", it->rmin_spl, nuniq);
+    putd("dr_spl", it->dr_spl, nuniq);
+    putd("dri_spl", it->dri_spl, nuniq);
+    putd("cv0", it->cv0, (int64_t)it->nsplin * nuniq);
+    putd("cdv0", it->cdv0, (int64_t)it->nsplin * nuniq);
+    if (ci->nchrg > 0) {
+        putd("cv0_c", it->cv0_c, (int64_t)it->nsplin * nuniq);
+        putd("cdv0_c", it->cdv0_c, (int64_t)it->nsplin * nuniq);
+    }
+    put1d("clong", it->clong);
+    put1d("skin", it->skin);
+    put1d("spread", it->spread);
+    put1d("spread_now", it->spread_now);
+    put1d("rheal_res", it->rheal_res);
+    put1i("ishave_opt", it->ishave_opt);
+    put1i("iswit_vdw", it->iswit_vdw);
+    put1i("nlen", class_.for_scr.nlen);
+
+    /* Verlet list as (i, j) pairs, i > j, in PINY's storage order */
+    NBR_LIST *nl = &class_.nbr_list;
+    put1i("iver", nl->iver);
+    if (nl->iver == 1) {
+        int64_t np = 0;
+        for (i = 1; i <= n; i++) np += nl->verlist.nter[i];
+        int *pairs = (int *)malloc(sizeof(int) * (size_t)(2 * np + 2));
+        int64_t k = 0;
+        for (i = 1; i <= n; i++) {
+            int off = nl->verlist.jver_off[i];
+            for (int j = 1; j <= nl->verlist.nter[i]; j++) {
+                pairs[2 * k] = i;
+                pairs[2 * k + 1] = nl->verlist.jter[off + j];
+                k++;
+            }
+        }
+        put("verlist_pairs", 'i', pairs, 2 * np);
+        free(pairs);
+    }
+
+    /* exclusions */
+    EXCL *ex = &bonded_.excl;
+    put1i("excl_nlst", ex->nlst);
+    puti("excl_num", ex->num, n);
+    puti("excl_j_off", ex->j_off, n);
+    puti("excl_j", ex->j, ex->nlst);
+
+    /* Ewald / PME */
+    EWALD *ew = &gd_.ewald;
+    PART_MESH *pm = &class_.part_mesh;
+    put1d("alp_ewd", ew->alp_ewd);
+    put1d("self_erf", ew->self_erf);
+    put1i("nktot", ew->nktot);
+    puti("kastr", ew->kastr, ew->nktot);
+    puti("kbstr", ew->kbstr, ew->nktot);
+    puti("kcstr", ew->kcstr, ew->nktot);
+    put1i("pme_on", pm->pme_on);
+    if (pm->pme_on) {
+        put1i("n_interp", pm->n_interp);
+        put1i("ngrid_a", pm->ngrid_a);
+        put1i("ngrid_b", pm->ngrid_b);
+        put1i("ngrid_c", pm->ngrid_c);
+        putd("bweight_tot", pm->bweight_tot, ew->nktot);
+    }
+
+    /* Ewald exclusion correction */
+    ECOR *ec = &bonded_.ecor;
+    put1i("ecor_num", ec->num);
+    if (ec->num > 0) {
+        puti("ecor_j1", ec->j1, ec->num);
+        puti("ecor_j2", ec->j2, ec->num);
+        put1i("ecor_nsplin", ec->nsplin);
+        put1d("ecor_rmin_spl", ec->rmin_spl);
+        put1d("ecor_rmax_spl", ec->rmax_spl);
+        put1d("ecor_dr_spl", ec->dr_spl);
+        put1d("ecor_dri_spl", ec->dri_spl);
+        put1d("ecor_alp_ewd", ec->alp_ewd);
+        put1d("ecor_ecut", ec->ecut);
+        putd("ecor_cv0", ec->cv0, ec->nsplin);
+        putd("ecor_cdv0", ec->cdv0, ec->nsplin);
+    }
+
+    /* bonds and bends (power series) */
+    BOND *bd = &bonded_.bond;
+    put1i("bond_npow", bd->npow);
+    put1i("bond_ntyp_pow", bd->ntyp_pow);
+    if (bd->npow > 0) {
+        puti("bond_j1", bd->j1_pow, bd->npow);
+        puti("bond_j2", bd->j2_pow, bd->npow);
+        puti("bond_jtyp", bd->jtyp_pow, bd->npow);
+        putd("bond_eq", bd->eq_pow, bd->ntyp_pow);
+        putd("bond_c0", bd->c_0, bd->ntyp_pow); putd("bond_c1", bd->c_1, bd->ntyp_pow);
+        putd("bond_c2", bd->c_2, bd->ntyp_pow); putd("bond_c3", bd->c_3, bd->ntyp_pow);
+        putd("bond_c4", bd->c_4, bd->ntyp_pow); putd("bond_c5", bd->c_5, bd->ntyp_pow);
+        putd("bond_c6", bd->c_6, bd->ntyp_pow);
+        putd("bond_dc0", bd->dc_0, bd->ntyp_pow); putd("bond_dc1", bd->dc_1, bd->ntyp_pow);
+        putd("bond_dc2", bd->dc_2, bd->ntyp_pow); putd("bond_dc3", bd->dc_3, bd->ntyp_pow);
+        putd("bond_dc4", bd->dc_4, bd->ntyp_pow); putd("bond_dc5", bd->dc_5, bd->ntyp_pow);
+        putd("bond_dc6", bd->dc_6, bd->ntyp_pow);
+    }
+    BEND *be = &bonded_.bend;
+    put1i("bend_npow", be->npow);
+    put1i("bend_ntyp_pow", be->ntyp_pow);
+    if (be->npow > 0) {
+        puti("bend_j1", be->j1_pow, be->npow);
+        puti("bend_j2", be->j2_pow, be->npow);
+        puti("bend_j3", be->j3_pow, be->npow);
+        puti("bend_jtyp", be->jtyp_pow, be->npow);
+        putd("bend_eq", be->eq_pow, be->ntyp_pow);
+        putd("bend_c0", be->c_0, be->ntyp_pow); putd("bend_c1", be->c_1, be->ntyp_pow);
+        putd("bend_c2", be->c_2, be->ntyp_pow); putd("bend_c3", be->c_3, be->ntyp_pow);
+        putd("bend_c4", be->c_4, be->ntyp_pow); putd("bend_c5", be->c_5, be->ntyp_pow);
+        putd("bend_c6", be->c_6, be->ntyp_pow);
+        putd("bend_s0", be->s_0, be->ntyp_pow); putd("bend_s1", be->s_1, be->ntyp_pow);
+        putd("bend_s2", be->s_2, be->ntyp_pow); putd("bend_s3", be->s_3, be->ntyp_pow);
+        putd("bend_s4", be->s_4, be->ntyp_pow); putd("bend_s5", be->s_5, be->ntyp_pow);
+        putd("bend_s6", be->s_6, be->ntyp_pow);
+    }
+
+    /* ghost (M site) definitions */
+    GHOST_ATOMS *gh = &class_.ghost_atoms;
+    put1i("nghost", gh->nghost_tot);
+    if (gh->nghost_tot > 0) {
+        puti("ighost_map", gh->ighost_map, gh->nghost_tot);
+        puti("ghost_ncomp", gh->natm_comp, gh->nghost_tot);
+        int nc = gh->natm_comp_max;
+        put1i("ghost_ncomp_max", nc);
+        for (int c = 1; c <= nc; c++) {
+            char nm[32];
+            snprintf(nm, sizeof nm, "ghost_iatm_%d", c);
+            puti(nm, gh->iatm_comp[c], gh->nghost_tot);
+            snprintf(nm, sizeof nm, "ghost_coef_%d", c);
+            putd(nm, gh->coef[c], gh->nghost_tot);
+        }
+    }
+    fclose(g_out);
+}
+
+int main(int argc, char **argv)
+{
+    if (argc < 4) {
+        fprintf(stderr, "usage: piny_ref dump|recip|time <dir> <input> [...]\n");
+        return 2;
+    }
+    const char *mode = argv[1];
+    char *outpath = NULL;
+    if (strcmp(mode, "dump") == 0) {
+        if (argc < 5) return 2;
+        outpath = realpath(argv[4], NULL);
+        if (!outpath) {
+            /* file does not exist yet: resolve its directory */
+            char *tmp = strdup(argv[4]);
+            char *slash = strrchr(tmp, '/');
+            char *d = slash ? (*slash = 0, realpath(tmp[0] ? tmp : "/", NULL)) : realpath(".", NULL);
+            const char *base = slash ? slash + 1 : argv[4];
+            outpath = malloc(strlen(d) + strlen(base) + 2);
+            sprintf(outpath, "%s/%s", d, base);
+        }
+    }
+    setup(argv[2], argv[3]);
+
+    if (strcmp(mode, "dump") == 0) {
+        evaluate();
+        dump_all(outpath);
+        return 0;
+    }
+    if (strcmp(mode, "recip") == 0) {
+        double vrecip = 0.0;
+        int ip;
+        for (ip = 1; ip <= class_.clatoms_info.pi_beads_proc; ip++)
+            get_ghost_pos(&class_.clatoms_info, &class_.clatoms_pos[ip], &class_.ghost_atoms);
+        class_.energy_ctrl.iget_pv_real_inter = 1;
+        class_.energy_ctrl.iget_pe_real_inter = 1;
+        ewald3d_recip_pme(&class_.clatoms_info, &class_.clatoms_pos[1], &gd_.cell, &gd_.ptens,
+                          gd_.ewald.alp_ewd, gd_.ewald.nktot, gd_.ewald.kastr, gd_.ewald.kbstr,
+                          gd_.ewald.kcstr, &class_.ewd_scr, &vrecip, class_.for_scr.wght_ter_res, 0,
+                          &class_.part_mesh, 0, &class_.class_comm_forc_pkg,
+                          class_.energy_ctrl.iget_pv_real_inter, &gd_.pme_fft_pkg, &class_.for_scr,
+                          gd_.ewald.clus_corr_r, gd_.ewald.dclus_corr_r);
+        printf("recip %.13g grid %d %d %d order %d alp %.10g\n", vrecip, class_.part_mesh.ngrid_a,
+               class_.part_mesh.ngrid_b, class_.part_mesh.ngrid_c, class_.part_mesh.n_interp,
+               gd_.ewald.alp_ewd / BOHR);
+        return 0;
+    }
+    if (strcmp(mode, "time") == 0) {
+        int reps = argc > 4 ? atoi(argv[4]) : 1;
+        int nb = argc > 5 ? atoi(argv[5]) : class_.clatoms_info.pi_beads;
+        if (nb < 1 || nb > class_.clatoms_info.pi_beads) nb = class_.clatoms_info.pi_beads;
+        class_.clatoms_info.pi_beads_proc = nb;
+        evaluate(); /* warm-up */
+        for (int r = 0; r < reps; r++) {
+            double t0 = now_s();
+            evaluate();
+            double t1 = now_s();
+            printf("time %d beads %.6f s\n", nb, t1 - t0);
+            fflush(stdout);
+        }
+        return 0;
+    }
+    fprintf(stderr, "piny_ref: unknown mode %s\n", mode);
+    return 2;
+}

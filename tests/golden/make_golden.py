@@ -1,0 +1,215 @@
+"""Generate the golden fixtures in tests/golden/ from PINY itself.
+
+Runs PINY's own CPU force path (oracle/_ref/piny_ref, built by
+``make -C oracle ref`` from the PINY sources) on seeded synthetic water boxes
+and stores, per configuration, a compressed .npz with
+
+* the inputs exactly as PINY used them (bead positions in Bohr after PINY's
+  mode round trip, the mode-1 positions for the PIMD image shift, the cell),
+* PINY's setup products (spline tables, k list, B-spline weights, exclusion
+  and Ewald-correction lists, bond/bend coefficients, ghost definitions),
+* PINY's outputs (per-bead forces before and after the M-site
+  redistribution, energy components, pressure tensor, the Verlet pair set).
+
+Run in a container that has the PINY tree:  python tests/golden/make_golden.py
+The GPU tests only read the .npz files.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import shutil
+import struct
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, ROOT)
+
+from piny_b200 import water  # noqa: E402
+
+PINY_REF = os.path.join(ROOT, "oracle", "_ref", "piny_ref")
+
+
+def read_dump(path):
+    out = {}
+    with open(path, "rb") as f:
+        while True:
+            h = f.read(40)
+            if len(h) < 40:
+                break
+            name = h[:32].split(b"\0")[0].decode()
+            kind = chr(h[32])
+            n = struct.unpack("<q", f.read(8))[0]
+            dt = np.float64 if kind == "d" else np.int32
+            out[name] = np.frombuffer(f.read(n * np.dtype(dt).itemsize), dtype=dt).copy()
+    return out
+
+
+def run_piny(spec, pos_angstrom, workdir):
+    d = os.path.join(workdir, "inp")
+    shutil.rmtree(d, ignore_errors=True)
+    water.write_piny_input(d, spec, pos_angstrom)
+    out = os.path.join(workdir, "dump.bin")
+    subprocess.run([PINY_REF, "dump", d, "water.input", out], check=True, capture_output=True)
+    return read_dump(out)
+
+
+def pair_hash(pi, pj):
+    """Order-independent digest of an (i > j) pair set."""
+    key = np.sort(pi.astype(np.int64) * (1 << 32) + pj.astype(np.int64))
+    return hashlib.sha256(key.tobytes()).hexdigest()
+
+
+def dump_to_fixture(D, keep_pairs):
+    """PINY dump (1-based) -> fixture dict (0-based, orc_system field names)."""
+    n = int(D["natm_tot"][0])
+    P = int(D["pi_beads"][0])
+    f = {}
+    f["natm"] = n
+    f["nbeads"] = P
+    f["pos"] = D["pos"].reshape(P, n, 3)
+    if P > 1:
+        f["xmod"] = np.stack([D["xmod"], D["ymod"], D["zmod"]], axis=1)
+    f["hmat"] = D["hmat"]
+    f["ntyp"] = int(D["natm_typ"][0])
+    f["atm_typ"] = D["iatm_atm_typ"] - 1
+    f["charge"] = D["q"]
+    f["nsplin"] = int(D["nsplin"][0])
+    f["ninter_unique"] = int(D["ninter_unique"][0])
+    f["inter_map"] = D["inter_map_index"] - 1
+    f["cutoff"] = D["cutoff"]
+    f["cutskin2"] = D["cutskin"]
+    f["rmin_spl"] = D["rmin_spl"]
+    f["dr_spl"] = D["dr_spl"]
+    f["dri_spl"] = D["dri_spl"]
+    for k in ("cv0", "cdv0", "cv0_c", "cdv0_c"):
+        f[k] = D[k]
+    f["skin"] = float(D["skin"][0])
+    f["spread"] = float(D["spread"][0])
+    f["clong"] = float(D["clong"][0])
+    f["iswit_vdw"] = int(D["iswit_vdw"][0])
+    # exclusions as CSR (PINY: excl_num / excl_j_off / excl_j, 1-based)
+    num = D["excl_num"]
+    off = D["excl_j_off"]
+    ej = D["excl_j"] - 1
+    excl_off = np.zeros(n + 1, np.int32)
+    excl_off[1:] = np.cumsum(num)
+    excl_j = np.concatenate([ej[off[i]:off[i] + num[i]] for i in range(n)]) if num.sum() else np.zeros(0, np.int32)
+    f["excl_off"] = excl_off
+    f["excl_j"] = excl_j.astype(np.int32)
+    f["alp_ewd"] = float(D["alp_ewd"][0])
+    f["self_erf"] = float(D["self_erf"][0])
+    f["nktot"] = int(D["nktot"][0])
+    f["kastr"], f["kbstr"], f["kcstr"] = D["kastr"], D["kbstr"], D["kcstr"]
+    f["bweight"] = D["bweight_tot"]
+    f["ngrid_a"], f["ngrid_b"], f["ngrid_c"] = int(D["ngrid_a"][0]), int(D["ngrid_b"][0]), int(D["ngrid_c"][0])
+    f["n_interp"] = int(D["n_interp"][0])
+    f["necor"] = int(D["ecor_num"][0])
+    f["ecor_j1"] = D["ecor_j1"] - 1
+    f["ecor_j2"] = D["ecor_j2"] - 1
+    f["ecor_nsplin"] = int(D["ecor_nsplin"][0])
+    f["ecor_rmin"] = float(D["ecor_rmin_spl"][0])
+    f["ecor_rmax"] = float(D["ecor_rmax_spl"][0])
+    f["ecor_dr"] = float(D["ecor_dr_spl"][0])
+    f["ecor_dri"] = float(D["ecor_dri_spl"][0])
+    f["ecor_ecut"] = float(D["ecor_ecut"][0])
+    f["ecor_cv0"] = D["ecor_cv0"]
+    f["ecor_cdv0"] = D["ecor_cdv0"]
+    f["nbond"] = int(D["bond_npow"][0])
+    f["bond_j1"] = D["bond_j1"] - 1
+    f["bond_j2"] = D["bond_j2"] - 1
+    f["bond_typ"] = D["bond_jtyp"] - 1
+    f["nbond_typ"] = int(D["bond_ntyp_pow"][0])
+    f["bond_eq"] = D["bond_eq"]
+    f["bond_c"] = np.stack([D["bond_c%d" % i] for i in range(7)], axis=1).reshape(-1)
+    f["bond_dc"] = np.stack([D["bond_dc%d" % i] for i in range(7)], axis=1).reshape(-1)
+    f["nbend"] = int(D["bend_npow"][0])
+    f["bend_j1"] = D["bend_j1"] - 1
+    f["bend_j2"] = D["bend_j2"] - 1
+    f["bend_j3"] = D["bend_j3"] - 1
+    f["bend_typ"] = D["bend_jtyp"] - 1
+    f["nbend_typ"] = int(D["bend_ntyp_pow"][0])
+    f["bend_eq"] = D["bend_eq"]
+    f["bend_c"] = np.stack([D["bend_c%d" % i] for i in range(7)], axis=1).reshape(-1)
+    f["bend_s"] = np.stack([D["bend_s%d" % i] for i in range(7)], axis=1).reshape(-1)
+    # derivative coefficients as bend_coef forms them (intra_coefs.c:355-371)
+    c = f["bend_c"].reshape(-1, 7)
+    sn = f["bend_s"].reshape(-1, 7)
+    dc = c * np.arange(7.0)
+    dc[:, 1] = c[:, 1]
+    ds = sn * np.array([0.0, 1.0, 1.0, 2.0, 3.0, 4.0, 5.0])
+    f["bend_dc"] = dc.reshape(-1)
+    f["bend_ds"] = ds.reshape(-1)
+    ng = int(D["nghost"][0])
+    f["nghost"] = ng
+    if ng:
+        nc = int(D["ghost_ncomp_max"][0])
+        f["ghost_ncomp"] = nc
+        f["ghost_atom"] = D["ighost_map"] - 1
+        comp = np.full((ng, nc), -1, np.int32)
+        coef = np.zeros((ng, nc))
+        for c in range(nc):
+            comp[:, c] = D["ghost_iatm_%d" % (c + 1)] - 1
+            coef[:, c] = D["ghost_coef_%d" % (c + 1)]
+        f["ghost_comp"] = comp.reshape(-1)
+        f["ghost_coef"] = coef.reshape(-1)
+    else:
+        f["ghost_ncomp"] = 0
+    pairs = D["verlist_pairs"].reshape(-1, 2) - 1
+    f["npairs"] = pairs.shape[0]
+    f["pairs_sha256"] = pair_hash(pairs[:, 0], pairs[:, 1])
+    if keep_pairs:
+        f["pairs"] = pairs.astype(np.int32)
+    # outputs
+    f["ref_force_raw"] = D["force_raw"].reshape(P, n, 3)
+    f["ref_force"] = D["force"].reshape(P, n, 3)
+    for k in ("vintert", "vintrat", "vvdw", "vcoul", "vrecip", "vlong", "vbondt", "vbendt"):
+        f["ref_" + k] = float(D[k][0])
+    f["ref_pvten_tot"] = D["pvten_tot"]
+    return f
+
+
+# (name, spec, keep the full pair list in the fixture)
+def golden_specs():
+    S = water
+    return [
+        ("spcfw_64_p1", S.BoxSpec(S.SPC_FW, 64, 12.416, 1, 300.0, 101, cutoff=6.0, grid=16, order=6, kmax=6), True),
+        ("spcfw_64_p4", S.BoxSpec(S.SPC_FW, 64, 12.416, 4, 300.0, 102, cutoff=6.0, grid=16, order=6, kmax=6), True),
+        ("tip4pf_64_p4", S.BoxSpec(S.TIP4P_F, 64, 12.416, 4, 298.0, 103, cutoff=6.0, grid=16, order=8, kmax=6),
+         True),
+        ("spcfw_256_p1", S.named_spec("spcfw_256_p1"), False),
+        ("tip4pf_128_p2", S.BoxSpec(S.TIP4P_F, 128, 15.66, 2, 298.0, 104, cutoff=7.5, grid=24, order=8, kmax=9),
+         False),
+    ]
+
+
+def main():
+    if not os.path.exists(PINY_REF):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    tmp = tempfile.mkdtemp(prefix="piny_golden_")
+    for name, spec, keep in golden_specs():
+        pos = water.build_positions(spec)
+        D = run_piny(spec, pos, tmp)
+        fx = dump_to_fixture(D, keep)
+        fx["spec_nmol"] = spec.nmol
+        fx["spec_L"] = spec.L
+        fx["spec_model"] = "tip4pf" if spec.model is water.TIP4P_F else "spcfw"
+        fx["spec_cutoff"] = spec.cutoff
+        fx["spec_kmax"] = spec.kmax_ewald
+        fx["spec_kmax_pme"] = spec.kmax_pme
+        fx["spec_order"] = spec.order
+        fx["spec_nsplin"] = spec.nsplin
+        fx["spec_temperature"] = spec.temperature
+        out = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(out, **{k: np.asarray(v) for k, v in fx.items()})
+        print(name, os.path.getsize(out), "bytes", fx["npairs"], "pairs")
+    shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()
