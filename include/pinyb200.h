@@ -1,0 +1,216 @@
+/*
+ * pinyb200 -- B200-native force path for PINY_MD flexible point-charge water.
+ *
+ * C ABI: plain pointers and sizes, no CUDA or torch types.  Indices are
+ * 0-based, arrays are in PINY internal units (Bohr, Hartree).  Every entry
+ * point returns a pinyb200_status; none of them exits the process.
+ *
+ * The path replaces the three force sub-steps PINY's integrators reach
+ * through energy_control()/energy_control_pimd():
+ *   energy_control_inter_real   (src/energy/control/energy_control_inter_real.c:33)
+ *   energy_control_inter_recip  (src/energy/control/energy_control_inter_recip.c:32)
+ *   energy_control_intra        (src/energy/control/energy_control_intra.c:33)
+ * as called from energy_control_pimd.c:91-111 and energy_control.c:49-74,
+ * for all path-integral beads at once.
+ */
+#ifndef PINYB200_H
+#define PINYB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pinyb200_status {
+    PINYB200_OK = 0,
+    PINYB200_ERR_ARG = 1,            /* bad argument or inconsistent sizes      */
+    PINYB200_ERR_CUDA = 2,           /* a CUDA runtime call failed              */
+    PINYB200_ERR_NO_DEVICE = 3,      /* no usable GPU                           */
+    PINYB200_ERR_LIST_OVERFLOW = 4,  /* Verlet list larger than its capacity    */
+    PINYB200_ERR_CUTOFF = 5,         /* cutoff exceeds half the box (warning)   */
+    PINYB200_ERR_TIMEOUT = 6,        /* a bounded device wait gave up           */
+    PINYB200_ERR_NAN = 7,            /* non-finite positions or forces          */
+    PINYB200_ERR_UNSUPPORTED = 8,    /* option not built for this path          */
+    PINYB200_ERR_STATE = 9           /* call order violated (e.g. no list yet)  */
+} pinyb200_status;
+
+enum {
+    PINYB200_FP64 = 0,  /* every kernel in FP64                                */
+    PINYB200_MIXED = 1  /* FP32 pair/PME arithmetic, FP64 force accumulation,  */
+                        /* FP64 energies/virial and intramolecular terms      */
+};
+
+/* Flags for pinyb200_energy_force*(). */
+enum {
+    PINYB200_DISTRIB_GHOSTS = 1, /* apply distrib_ghost_force (ghost_control.c:71) */
+    PINYB200_NO_ENERGY = 2       /* skip energy/virial reductions                   */
+};
+
+/*
+ * Set-up data of one box: the products of PINY's input stage (parse()),
+ * field by field.  PINY owns these arrays; pinyb200_create copies them.
+ *   INTERACT       cv0/cdv0/cv0_c/cdv0_c, rmin_spl, dr_spl, dri_spl,
+ *                  inter_map_index, cutoff   (include/typ_defs/typedefs_class.h:610)
+ *   EXCL           num/j_off/j -> excl_off/excl_j (typedefs_bnd.h:449)
+ *   EWALD          alp_ewd, self_erf, kastr/kbstr/kcstr (typedefs_gen.h:232)
+ *   PART_MESH      bweight_tot, ngrid_*, n_interp (typedefs_class.h:790)
+ *   ECOR, BOND, BEND, GHOST_ATOMS (typedefs_bnd.h:420, :21, :182;
+ *                  typedefs_class.h:225)
+ */
+typedef struct pinyb200_system {
+    int natm;
+    int ntyp;
+    const int *atm_typ;
+    const double *charge;
+
+    int nsplin;
+    int ninter_unique;
+    const int *inter_map;
+    const double *cutoff;
+    const double *rmin_spl;
+    const double *dr_spl;
+    const double *dri_spl;
+    const double *cv0;
+    const double *cdv0;
+    const double *cv0_c;
+    const double *cdv0_c;
+    double skin;
+    double clong;
+    int iswit_vdw;
+
+    const int *excl_off;
+    const int *excl_j;
+
+    double alp_ewd;
+    double self_erf;
+    int nktot;
+    const int *kastr;
+    const int *kbstr;
+    const int *kcstr;
+    const double *bweight;
+    int ngrid_a, ngrid_b, ngrid_c;
+    int n_interp;
+
+    int necor;
+    const int *ecor_j1;
+    const int *ecor_j2;
+    int ecor_nsplin;
+    double ecor_rmin;
+    double ecor_dr;
+    double ecor_dri;
+    const double *ecor_cv0;
+    const double *ecor_cdv0;
+
+    int nbond;
+    const int *bond_j1;
+    const int *bond_j2;
+    const int *bond_typ;
+    int nbond_typ;
+    const double *bond_eq;
+    const double *bond_c;
+    const double *bond_dc;
+
+    int nbend;
+    const int *bend_j1;
+    const int *bend_j2;
+    const int *bend_j3;
+    const int *bend_typ;
+    int nbend_typ;
+    const double *bend_c;
+    const double *bend_s;
+    const double *bend_dc;
+    const double *bend_ds;
+
+    int nghost;
+    int ghost_ncomp;
+    const int *ghost_atom;
+    const int *ghost_comp;
+    const double *ghost_coef;
+} pinyb200_system;
+
+/* Energy components with PINY's bead averaging
+ * (energy_control_inter_real.c:141-183, energy_control_inter_recip.c:341-349,
+ *  energy_control_intra.c:284-309).  pvten is the bead-summed PINY pvten_tot. */
+typedef struct pinyb200_energies {
+    double vreal, vvdw, vcoul, vrecip, vself, vbgr, vecor, vlong;
+    double vbond, vbend, vintert, vintrat;
+    double pvten[9];
+} pinyb200_energies;
+
+typedef struct pinyb200_ctx pinyb200_ctx;
+
+/* Library version and the device it will use. */
+int pinyb200_version(void);
+int pinyb200_device_info(char *name, int len, int *sm_count);
+
+/* Create a context for one box with nbeads path-integral beads (the
+ * per-replica state PINY keeps in CLASS/BONDED/GENERAL_DATA).  One context
+ * per CLASS; contexts are independent and may be driven from separate host
+ * threads (python/piny/piny.pyx:426-436 runs replicas concurrently). */
+int pinyb200_create(const pinyb200_system *sys, int nbeads, int precision,
+                    pinyb200_ctx **out);
+int pinyb200_destroy(pinyb200_ctx *ctx);
+
+/*
+ * Build the Verlet list from bead-1 positions: every non-excluded pair
+ * i > j whose minimum-image separation has r^2 < cutskin2[pair type]
+ * (verlist_control.c:30-128 -> verlist_create.c:25-221).  For PIMD the image
+ * shift comes from xmod, the mode-1 positions (period_pimd, period.c:121);
+ * pass xmod = NULL for classical runs.
+ *   pos1, xmod : natm x 3 (AoS) host arrays;  hmat : 9, column-major;
+ *   cutskin2   : ntyp(ntyp+1)/2 squared list radii (get_cut_skin,
+ *                nbr_list_control.c:249-281).
+ * Returns the number of pairs in *npairs.
+ */
+int pinyb200_build_list(pinyb200_ctx *ctx, const double *pos1,
+                        const double *xmod, const double *hmat,
+                        const double *cutskin2, long *npairs);
+
+/* Copy the current list out as (i, j) pairs, i > j, in the device's order. */
+int pinyb200_get_list(pinyb200_ctx *ctx, int *pi, int *pj, long cap,
+                      long *npairs);
+
+/*
+ * One force/energy evaluation of all beads with host buffers.
+ *   pos   : nbeads x natm x 3 host array (bead-major AoS), ghosts are
+ *           recomputed from their components (get_ghost_pos);
+ *   xmod  : natm x 3 mode-1 positions for the PIMD image, or NULL;
+ *   force : nbeads x natm x 3 output, overwritten (not accumulated).
+ */
+int pinyb200_energy_force(pinyb200_ctx *ctx, const double *pos,
+                          const double *xmod, const double *hmat, int flags,
+                          double *force, pinyb200_energies *e);
+
+/* Same, with device-resident pos / xmod / force (cudaMalloc'd by the
+ * caller, same layouts) on the CUDA stream passed as an opaque handle
+ * (NULL = the context's own stream).  Returns after the stream is idle. */
+int pinyb200_energy_force_device(pinyb200_ctx *ctx, const double *d_pos,
+                                 const double *d_xmod, const double *hmat,
+                                 int flags, double *d_force,
+                                 pinyb200_energies *e, void *stream);
+
+/*
+ * PINY-layout drop-in for energy_control_inter_real + _inter_recip + _intra
+ * over all beads.  x[ip], y[ip], z[ip] and fx[ip], fy[ip], fz[ip] are
+ * PINY's 1-based per-bead arrays (clatoms_pos[ip+1].x etc., element 1 is the
+ * first atom); xmod/ymod/zmod are clatoms_info.xmod etc. (1-based) or NULL;
+ * hmat is cell.hmat (1-based).  Forces and pvten_tot (1-based, 9) are ADDED
+ * to, as PINY's routines do; energies are returned in *e.
+ */
+int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
+                        double *const *y, double *const *z, const double *xmod,
+                        const double *ymod, const double *zmod,
+                        const double *hmat, double *const *fx,
+                        double *const *fy, double *const *fz,
+                        double *pvten_tot, pinyb200_energies *e);
+
+/* Milliseconds of the last evaluation's device work, per phase
+ * (0 total, 1 pair, 2 PME, 3 intra) and the pair count it used. */
+int pinyb200_last_timing(pinyb200_ctx *ctx, float *ms, int n);
+
+/* Last error text for this context (or the library if ctx is NULL). */
+const char *pinyb200_last_error(pinyb200_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

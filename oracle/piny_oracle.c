@@ -73,23 +73,23 @@ static void period_pimd_one(double *dx, double *dy, double *dz, double dxs,
     }
 }
 
-/* 3x3 inverse and determinant of a column-major cell (gethinv). */
-static double cell_inverse(const double *h, double *hi)
+/* Inverse and determinant of the column-major cell, with the operation
+ * order of gethinv's periodic branch (src/mathlib/mathlib.c:353-380). */
+static double cell_inverse(const double *hm, double *hi)
 {
-    double a = h[0], b = h[3], c = h[6], d = h[1], e = h[4], f = h[7], g = h[2], k = h[5], l = h[8];
-    double det = a * (e * l - f * k) - b * (d * l - f * g) + c * (d * k - e * g);
-    double inv[9];
-    inv[0] = (e * l - f * k) / det;
-    inv[3] = -(b * l - c * k) / det;
-    inv[6] = (b * f - c * e) / det;
-    inv[1] = -(d * l - f * g) / det;
-    inv[4] = (a * l - c * g) / det;
-    inv[7] = -(a * f - c * d) / det;
-    inv[2] = (d * k - e * g) / det;
-    inv[5] = -(a * k - b * g) / det;
-    inv[8] = (a * e - b * d) / det;
-    memcpy(hi, inv, sizeof inv);
-    return det;
+    const double *h = hm - 1; /* 1-based view */
+    double vol = (h[1] * (h[5] * h[9] - h[8] * h[6]) + h[4] * (h[8] * h[3] - h[2] * h[9]) +
+                  h[7] * (h[2] * h[6] - h[5] * h[3]));
+    hi[0] = (h[5] * h[9] - h[8] * h[6]) / vol;
+    hi[4] = (h[1] * h[9] - h[7] * h[3]) / vol;
+    hi[8] = (h[1] * h[5] - h[4] * h[2]) / vol;
+    hi[3] = (h[7] * h[6] - h[4] * h[9]) / vol;
+    hi[1] = (h[3] * h[8] - h[2] * h[9]) / vol;
+    hi[6] = (h[4] * h[8] - h[7] * h[5]) / vol;
+    hi[2] = (h[2] * h[6] - h[3] * h[5]) / vol;
+    hi[7] = (h[7] * h[2] - h[8] * h[1]) / vol;
+    hi[5] = (h[3] * h[4] - h[6] * h[1]) / vol;
+    return vol;
 }
 
 /* ------------------------------------------------------------------------ */

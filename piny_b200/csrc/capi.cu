@@ -1,0 +1,601 @@
+// C ABI of the pinyb200 library: context set-up, list build and the force
+// evaluation that replaces PINY's energy_control_inter_real /
+// energy_control_inter_recip / energy_control_intra for all beads.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+using namespace pinyb200;
+
+namespace {
+
+thread_local std::string g_lib_err;
+
+int fail(pinyb200_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->err = msg;
+    else g_lib_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(c, PINYB200_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+cudaError_t upload(T **dst, const T *src, size_t n)
+{
+    *dst = nullptr;
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc((void **)dst, n * sizeof(T));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+// Cell inverse with the operation order of gethinv (src/mathlib/mathlib.c:353).
+Cell make_cell(const double *hm)
+{
+    Cell c;
+    const double *h = hm - 1;
+    double vol = (h[1] * (h[5] * h[9] - h[8] * h[6]) + h[4] * (h[8] * h[3] - h[2] * h[9]) +
+                  h[7] * (h[2] * h[6] - h[5] * h[3]));
+    c.hi[0] = (h[5] * h[9] - h[8] * h[6]) / vol;
+    c.hi[4] = (h[1] * h[9] - h[7] * h[3]) / vol;
+    c.hi[8] = (h[1] * h[5] - h[4] * h[2]) / vol;
+    c.hi[3] = (h[7] * h[6] - h[4] * h[9]) / vol;
+    c.hi[1] = (h[3] * h[8] - h[2] * h[9]) / vol;
+    c.hi[6] = (h[4] * h[8] - h[7] * h[5]) / vol;
+    c.hi[2] = (h[2] * h[6] - h[3] * h[5]) / vol;
+    c.hi[7] = (h[7] * h[2] - h[8] * h[1]) / vol;
+    c.hi[5] = (h[3] * h[4] - h[6] * h[1]) / vol;
+    for (int i = 0; i < 9; i++) c.h[i] = hm[i];
+    c.vol = vol;
+    // cubic_box_flag: PINY sets it for an orthorhombic cell with equal edges
+    c.cubic = (hm[1] == 0.0 && hm[2] == 0.0 && hm[3] == 0.0 && hm[5] == 0.0 && hm[6] == 0.0 && hm[7] == 0.0 &&
+               hm[0] == hm[4] && hm[0] == hm[8]);
+    return c;
+}
+
+// Interval coefficients of npol_vspl_fetch (force_npol.c:339-375) for knot
+// k (1-based) of a table: c0 + del (c1 + del (c2 + del c3)).
+void cubic_coefs(const double *t, int nsplin, std::vector<double> &out)
+{
+    // host code is built with -ffp-contract=off: these are PINY's roundings
+    const double oneth = (1.0 / 3.0), onesi = (1.0 / 6.0);
+    out.assign((size_t)4 * nsplin, 0.0);
+    for (int k = 3; k <= nsplin - 1; k++) {
+        const double c0 = t[k - 1], fp1 = t[k], fm1 = t[k - 2], fm2 = t[k - 3];
+        out[4 * (size_t)(k - 1) + 0] = c0;
+        out[4 * (size_t)(k - 1) + 1] = oneth * fp1 + 0.5 * c0 - fm1 + onesi * fm2;
+        out[4 * (size_t)(k - 1) + 2] = 0.5 * fp1 - c0 + 0.5 * fm1;
+        out[4 * (size_t)(k - 1) + 3] = onesi * fp1 - 0.5 * c0 + 0.5 * fm1 - onesi * fm2;
+    }
+}
+
+void free_sys(DeviceSystem &s)
+{
+    void *ptrs[] = {s.atm_typ, s.charge, s.inter_map, s.cutoff, s.rmin, s.dr, s.dri, s.has_vdw, s.tab64, s.tab32,
+                    s.excl_off, s.excl_j, s.ichrg, s.kvec, s.bweight, s.kmask, s.ecor_j1, s.ecor_j2, s.ecor_tab,
+                    s.bond_j, s.bond_eq, s.bond_c, s.bond_dc, s.bend_j, s.bend_c, s.bend_s, s.bend_dc, s.bend_ds,
+                    s.ghost_atom, s.ghost_comp, s.ghost_coef};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    s = DeviceSystem();
+}
+
+int check_system(pinyb200_ctx *c, const pinyb200_system *s, int nbeads)
+{
+    if (!s || s->natm <= 0 || s->ntyp <= 0 || !s->atm_typ || !s->charge)
+        return fail(c, PINYB200_ERR_ARG, "system: natm/ntyp/atm_typ/charge required");
+    if (nbeads != 1 && nbeads != 2 && nbeads != 4 && nbeads != 8 && nbeads != 16 && nbeads != 32 && nbeads != 64)
+        return fail(c, PINYB200_ERR_UNSUPPORTED, "nbeads must be one of 1,2,4,8,16,32,64");
+    if (s->nsplin < 8 || s->ninter_unique <= 0) return fail(c, PINYB200_ERR_ARG, "system: spline tables missing");
+    for (int i = 0; i < s->natm; i++)
+        if (s->atm_typ[i] < 0 || s->atm_typ[i] >= s->ntyp) return fail(c, PINYB200_ERR_ARG, "atm_typ out of range");
+    const int npt = s->ntyp * (s->ntyp + 1) / 2;
+    for (int p = 0; p < npt; p++)
+        if (s->inter_map[p] < 0 || s->inter_map[p] >= s->ninter_unique)
+            return fail(c, PINYB200_ERR_ARG, "inter_map out of range");
+    for (int i = 0; i < s->excl_off[s->natm]; i++)
+        if (s->excl_j[i] < 0 || s->excl_j[i] >= s->natm) return fail(c, PINYB200_ERR_ARG, "excl_j out of range");
+    if (s->nktot > 0) {
+        int N[3] = {s->ngrid_a, s->ngrid_b, s->ngrid_c};
+        for (int d = 0; d < 3; d++)
+            if (N[d] < s->n_interp || N[d] > 256) return fail(c, PINYB200_ERR_ARG, "PME grid size out of range");
+        for (int i = 0; i < s->nktot; i++) {
+            int k[3] = {s->kastr[i], s->kbstr[i], s->kcstr[i]};
+            for (int d = 0; d < 3; d++)
+                if (2 * abs(k[d]) >= N[d]) return fail(c, PINYB200_ERR_ARG, "k vector beyond the PME grid");
+        }
+    }
+    for (int i = 0; i < s->nbond; i++)
+        if (s->bond_j1[i] < 0 || s->bond_j1[i] >= s->natm || s->bond_j2[i] < 0 || s->bond_j2[i] >= s->natm ||
+            s->bond_typ[i] < 0 || s->bond_typ[i] >= s->nbond_typ)
+            return fail(c, PINYB200_ERR_ARG, "bond index out of range");
+    for (int i = 0; i < s->nbend; i++)
+        if (s->bend_j1[i] < 0 || s->bend_j1[i] >= s->natm || s->bend_j2[i] < 0 || s->bend_j2[i] >= s->natm ||
+            s->bend_j3[i] < 0 || s->bend_j3[i] >= s->natm || s->bend_typ[i] < 0 || s->bend_typ[i] >= s->nbend_typ)
+            return fail(c, PINYB200_ERR_ARG, "bend index out of range");
+    for (int i = 0; i < s->necor; i++)
+        if (s->ecor_j1[i] < 0 || s->ecor_j1[i] >= s->natm || s->ecor_j2[i] < 0 || s->ecor_j2[i] >= s->natm)
+            return fail(c, PINYB200_ERR_ARG, "ecor index out of range");
+    for (int g = 0; g < s->nghost; g++) {
+        if (s->ghost_atom[g] < 0 || s->ghost_atom[g] >= s->natm) return fail(c, PINYB200_ERR_ARG, "ghost atom");
+        for (int k = 0; k < s->ghost_ncomp; k++) {
+            int a = s->ghost_comp[g * s->ghost_ncomp + k];
+            if (a >= s->natm) return fail(c, PINYB200_ERR_ARG, "ghost component out of range");
+        }
+    }
+    return PINYB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pinyb200_version(void) { return 1; }
+
+const char *pinyb200_last_error(pinyb200_ctx *ctx) { return ctx ? ctx->err.c_str() : g_lib_err.c_str(); }
+
+int pinyb200_device_info(char *name, int len, int *sm_count)
+{
+    pinyb200_ctx *c = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(c, PINYB200_ERR_NO_DEVICE, "no CUDA device");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    cudaDeviceProp p;
+    CK(cudaGetDeviceProperties(&p, dev));
+    if (name && len > 0) {
+        strncpy(name, p.name, len - 1);
+        name[len - 1] = 0;
+    }
+    if (sm_count) *sm_count = p.multiProcessorCount;
+    return PINYB200_OK;
+}
+
+int pinyb200_destroy(pinyb200_ctx *c)
+{
+    if (!c) return PINYB200_OK;
+    cudaSetDevice(c->device);
+    free_sys(c->sys);
+    void *ptrs[] = {c->d_row, c->d_col, c->d_rowA, c->d_colA, c->d_count, c->d_tot, c->d_posT, c->d_forceT,
+                    c->d_xmod, c->d_pos_aos, c->d_force_aos, c->d_acc, c->d_grid, c->d_filter, c->d_twiddle64,
+                    c->d_twiddle32, c->d_err};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    for (int i = 0; i < 8; i++)
+        if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return PINYB200_OK;
+}
+
+int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb200_ctx **out)
+{
+    pinyb200_ctx *c = nullptr;
+    if (!out) return fail(c, PINYB200_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(c, PINYB200_ERR_NO_DEVICE, "no CUDA device");
+    int rc = check_system(nullptr, s, nbeads);
+    if (rc) return rc;
+    if (precision != PINYB200_FP64 && precision != PINYB200_MIXED)
+        return fail(c, PINYB200_ERR_ARG, "precision must be PINYB200_FP64 or PINYB200_MIXED");
+    c = new pinyb200_ctx();
+    for (int i = 0; i < 8; i++) c->ev[i] = nullptr;
+    CK(cudaGetDevice(&c->device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, c->device));
+    c->sm_count = prop.multiProcessorCount;
+    c->precision = precision;
+    c->P = nbeads;
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 8; i++) CK(cudaEventCreate(&c->ev[i]));
+
+    DeviceSystem &d = c->sys;
+    const int natm = s->natm;
+    d.natm = natm;
+    d.ntyp = s->ntyp;
+    d.npair_typ = s->ntyp * (s->ntyp + 1) / 2;
+    d.nsplin = s->nsplin;
+    d.nuniq = s->ninter_unique;
+    CK(upload(&d.atm_typ, s->atm_typ, natm));
+    CK(upload(&d.charge, s->charge, natm));
+    c->h_charge.assign(s->charge, s->charge + natm);
+    CK(upload(&d.inter_map, s->inter_map, d.npair_typ));
+    CK(upload(&d.cutoff, s->cutoff, d.npair_typ));
+    CK(upload(&d.rmin, s->rmin_spl, d.nuniq));
+    CK(upload(&d.dr, s->dr_spl, d.nuniq));
+    CK(upload(&d.dri, s->dri_spl, d.nuniq));
+    // tables -> interval coefficients, [kind][u][k]
+    {
+        const size_t per = (size_t)s->nsplin;
+        std::vector<double> all((size_t)4 * 4 * d.nuniq * per, 0.0), tmp;
+        std::vector<int> has_vdw(d.nuniq, 0);
+        const double *tabs[4] = {s->cv0, s->cdv0, s->cv0_c, s->cdv0_c};
+        for (int kind = 0; kind < 4; kind++)
+            for (int u = 0; u < d.nuniq; u++) {
+                const double *t = tabs[kind] + (size_t)u * per;
+                if (kind <= 1)
+                    for (size_t k = 0; k < per; k++)
+                        if (t[k] != 0.0) has_vdw[u] = 1;
+                cubic_coefs(t, s->nsplin, tmp);
+                std::copy(tmp.begin(), tmp.end(), all.begin() + ((size_t)kind * d.nuniq + u) * per * 4);
+            }
+        CK(upload(&d.has_vdw, has_vdw.data(), d.nuniq));
+        CK(upload((double **)&d.tab64, all.data(), all.size()));
+        std::vector<float> f32(all.size());
+        for (size_t i = 0; i < all.size(); i++) f32[i] = (float)all[i];
+        CK(upload((float **)&d.tab32, f32.data(), f32.size()));
+    }
+    c->clong = s->clong;
+    c->iswit_vdw = s->iswit_vdw;
+    CK(upload(&d.excl_off, s->excl_off, natm + 1));
+    CK(upload(&d.excl_j, s->excl_j, (size_t)s->excl_off[natm]));
+    {
+        std::vector<int> ich;
+        for (int i = 0; i < natm; i++)
+            if (s->charge[i] != 0.0) ich.push_back(i);
+        d.nchrg = (int)ich.size();
+        CK(upload(&d.ichrg, ich.data(), ich.size()));
+    }
+    c->alp_ewd = s->alp_ewd;
+    c->self_erf = s->self_erf;
+    d.nktot = s->nktot;
+    d.ngrid[0] = s->ngrid_a;
+    d.ngrid[1] = s->ngrid_b;
+    d.ngrid[2] = s->ngrid_c;
+    d.n_interp = s->n_interp;
+    if (s->nktot > 0) {
+        std::vector<int> kv((size_t)3 * s->nktot);
+        for (int i = 0; i < s->nktot; i++) {
+            kv[3 * i] = s->kastr[i];
+            kv[3 * i + 1] = s->kbstr[i];
+            kv[3 * i + 2] = s->kcstr[i];
+        }
+        CK(upload(&d.kvec, kv.data(), kv.size()));
+        CK(upload(&d.bweight, s->bweight, s->nktot));
+        const int Na = s->ngrid_a, Nb = s->ngrid_b, Nc = s->ngrid_c;
+        const size_t G = (size_t)Na * Nb * Nc;
+        std::vector<int> mask(G, -1);
+        for (int i = 0; i < s->nktot; i++) {
+            int a = ((s->kastr[i] % Na) + Na) % Na, b = ((s->kbstr[i] % Nb) + Nb) % Nb,
+                cc = ((s->kcstr[i] % Nc) + Nc) % Nc;
+            mask[((size_t)cc * Nb + b) * Na + a] = i;
+            int am = (Na - a) % Na, bm = (Nb - b) % Nb, cm = (Nc - cc) % Nc;
+            mask[((size_t)cm * Nb + bm) * Na + am] = i;
+        }
+        CK(upload(&d.kmask, mask.data(), G));
+        CK(cudaMalloc(&c->d_filter, G * (sizeof(double) + sizeof(float))));
+        const size_t csz = precision == PINYB200_FP64 ? sizeof(double2) : sizeof(float2);
+        CK(cudaMalloc(&c->d_grid, csz * G * nbeads));
+        // twiddles exp(2 pi i m / N) per axis, 256 entries each
+        std::vector<double> tw(2 * 256 * 3, 0.0);
+        std::vector<float> tw32(tw.size());
+        const int N3[3] = {Na, Nb, Nc};
+        for (int ax = 0; ax < 3; ax++)
+            for (int m = 0; m < N3[ax]; m++) {
+                tw[2 * (256 * ax + m)] = cos(2.0 * M_PI * m / N3[ax]);
+                tw[2 * (256 * ax + m) + 1] = sin(2.0 * M_PI * m / N3[ax]);
+            }
+        for (size_t i = 0; i < tw.size(); i++) tw32[i] = (float)tw[i];
+        CK(upload(&c->d_twiddle64, tw.data(), tw.size()));
+        CK(upload(&c->d_twiddle32, tw32.data(), tw32.size()));
+    }
+    d.necor = s->necor;
+    if (s->necor > 0) {
+        CK(upload(&d.ecor_j1, s->ecor_j1, s->necor));
+        CK(upload(&d.ecor_j2, s->ecor_j2, s->necor));
+        d.ecor_nsplin = s->ecor_nsplin;
+        d.ecor_rmin = s->ecor_rmin;
+        d.ecor_dr = s->ecor_dr;
+        d.ecor_dri = s->ecor_dri;
+        std::vector<double> a, b;
+        cubic_coefs(s->ecor_cv0, s->ecor_nsplin, a);
+        cubic_coefs(s->ecor_cdv0, s->ecor_nsplin, b);
+        a.insert(a.end(), b.begin(), b.end());
+        CK(upload((double **)&d.ecor_tab, a.data(), a.size()));
+    }
+    d.nbond = s->nbond;
+    if (s->nbond > 0) {
+        std::vector<int> bj((size_t)3 * s->nbond);
+        for (int i = 0; i < s->nbond; i++) {
+            bj[3 * i] = s->bond_j1[i];
+            bj[3 * i + 1] = s->bond_j2[i];
+            bj[3 * i + 2] = s->bond_typ[i];
+        }
+        CK(upload(&d.bond_j, bj.data(), bj.size()));
+        CK(upload(&d.bond_eq, s->bond_eq, s->nbond_typ));
+        CK(upload(&d.bond_c, s->bond_c, (size_t)7 * s->nbond_typ));
+        CK(upload(&d.bond_dc, s->bond_dc, (size_t)7 * s->nbond_typ));
+    }
+    d.nbend = s->nbend;
+    if (s->nbend > 0) {
+        std::vector<int> bj((size_t)4 * s->nbend);
+        for (int i = 0; i < s->nbend; i++) {
+            bj[4 * i] = s->bend_j1[i];
+            bj[4 * i + 1] = s->bend_j2[i];
+            bj[4 * i + 2] = s->bend_j3[i];
+            bj[4 * i + 3] = s->bend_typ[i];
+        }
+        CK(upload(&d.bend_j, bj.data(), bj.size()));
+        CK(upload(&d.bend_c, s->bend_c, (size_t)7 * s->nbend_typ));
+        CK(upload(&d.bend_s, s->bend_s, (size_t)7 * s->nbend_typ));
+        CK(upload(&d.bend_dc, s->bend_dc, (size_t)7 * s->nbend_typ));
+        CK(upload(&d.bend_ds, s->bend_ds, (size_t)7 * s->nbend_typ));
+    }
+    d.nghost = s->nghost;
+    d.ghost_ncomp = s->ghost_ncomp;
+    if (s->nghost > 0) {
+        CK(upload(&d.ghost_atom, s->ghost_atom, s->nghost));
+        CK(upload(&d.ghost_comp, s->ghost_comp, (size_t)s->nghost * s->ghost_ncomp));
+        CK(upload(&d.ghost_coef, s->ghost_coef, (size_t)s->nghost * s->ghost_ncomp));
+    }
+    const size_t nb = (size_t)natm * 3 * nbeads;
+    CK(cudaMalloc(&c->d_posT, nb * sizeof(double)));
+    CK(cudaMalloc(&c->d_forceT, nb * sizeof(double)));
+    CK(cudaMalloc(&c->d_pos_aos, nb * sizeof(double)));
+    CK(cudaMalloc(&c->d_force_aos, nb * sizeof(double)));
+    CK(cudaMalloc(&c->d_xmod, (size_t)natm * 3 * sizeof(double)));
+    CK(cudaMalloc(&c->d_acc, (size_t)nbeads * S_NSLOT * sizeof(double)));
+    CK(cudaMalloc(&c->d_row, (size_t)(natm + 1) * sizeof(int)));
+    CK(cudaMalloc(&c->d_rowA, (size_t)(natm + 1) * sizeof(int)));
+    CK(cudaMalloc(&c->d_count, (size_t)2 * natm * sizeof(int)));
+    CK(cudaMalloc(&c->d_tot, 2 * sizeof(long long)));
+    CK(cudaMalloc(&c->d_err, sizeof(int)));
+    CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    *out = c;
+    return PINYB200_OK;
+}
+
+int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod, const double *hmat,
+                        const double *cutskin2, long *npairs)
+{
+    if (!c || !pos1 || !hmat || !cutskin2) return fail(c, PINYB200_ERR_ARG, "build_list: NULL argument");
+    CK(cudaSetDevice(c->device));
+    const int natm = c->sys.natm;
+    Cell cell = make_cell(hmat);
+    double *d_p1 = c->d_pos_aos;  // bead-1 positions in the staging buffer
+    CK(cudaMemcpyAsync(d_p1, pos1, (size_t)natm * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const double *d_xm = nullptr;
+    if (xmod) {
+        CK(cudaMemcpyAsync(c->d_xmod, xmod, (size_t)natm * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        d_xm = c->d_xmod;
+    }
+    double *d_cs = nullptr;
+    CK(cudaMalloc(&d_cs, c->sys.npair_typ * sizeof(double)));
+    CK(cudaMemcpyAsync(d_cs, cutskin2, c->sys.npair_typ * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(launch_build_list(c, cell, d_p1, d_xm, d_cs, 0));
+    long long tot[2];
+    CK(cudaMemcpyAsync(tot, c->d_tot, sizeof(tot), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (tot[0] > 0x7fffffffLL) {
+        cudaFree(d_cs);
+        return fail(c, PINYB200_ERR_LIST_OVERFLOW, "Verlet list exceeds 2^31 pairs");
+    }
+    if (tot[0] > c->list_cap) {
+        // grow like ver_list_mem_check (verlist_control.c:87-110), with slack
+        if (c->d_col) cudaFree(c->d_col);
+        if (c->d_colA) cudaFree(c->d_colA);
+        c->d_col = c->d_colA = nullptr;
+        long long cap = tot[0] + tot[0] / 8 + 1024;
+        CK(cudaMalloc(&c->d_col, cap * sizeof(int)));
+        CK(cudaMalloc(&c->d_colA, cap * sizeof(int)));
+        c->list_cap = cap;
+    }
+    CK(launch_build_list(c, cell, d_p1, d_xm, d_cs, 1));
+    CK(cudaStreamSynchronize(c->stream));
+    cudaFree(d_cs);
+    c->npairs = tot[0];
+    c->nactive = tot[1];
+    c->have_list = true;
+    if (npairs) *npairs = (long)tot[0];
+    return PINYB200_OK;
+}
+
+int pinyb200_get_list(pinyb200_ctx *c, int *pi, int *pj, long cap, long *npairs)
+{
+    if (!c) return fail(c, PINYB200_ERR_ARG, "NULL context");
+    if (!c->have_list) return fail(c, PINYB200_ERR_STATE, "no list built yet");
+    if (npairs) *npairs = (long)c->npairs;
+    if (!pi || !pj) return PINYB200_OK;
+    if (cap < c->npairs) return fail(c, PINYB200_ERR_ARG, "get_list: capacity too small");
+    CK(cudaSetDevice(c->device));
+    std::vector<int> row(c->sys.natm + 1);
+    CK(cudaMemcpy(row.data(), c->d_row, row.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(pj, c->d_col, c->npairs * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < c->sys.natm; i++)
+        for (int k = row[i]; k < row[i + 1]; k++) pi[k] = i;
+    return PINYB200_OK;
+}
+
+// Device evaluation on inputs already in d_posT (and d_xmod for PIMD).
+static int evaluate(pinyb200_ctx *c, const Cell &cell, int flags, pinyb200_energies *e)
+{
+    const bool energy = !(flags & PINYB200_NO_ENERGY);
+    const size_t nb = (size_t)c->sys.natm * 3 * c->P;
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    CK(launch_ghost_pos(c));
+    CK(cudaMemsetAsync(c->d_forceT, 0, nb * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->d_acc, 0, (size_t)c->P * S_NSLOT * sizeof(double), c->stream));
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(launch_pair(c, cell, energy));
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    CK(launch_pme(c, cell, energy));
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    CK(launch_intra(c, cell, energy));
+    if (flags & PINYB200_DISTRIB_GHOSTS) CK(launch_ghost_distrib(c));
+    CK(cudaEventRecord(c->ev[4], c->stream));
+    std::vector<double> acc;
+    if (energy) {
+        acc.resize((size_t)c->P * S_NSLOT);
+        CK(cudaMemcpyAsync(acc.data(), c->d_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]));
+    CK(cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]));
+    CK(cudaEventElapsedTime(&c->last_ms[2], c->ev[2], c->ev[3]));
+    CK(cudaEventElapsedTime(&c->last_ms[3], c->ev[3], c->ev[4]));
+    if (e) {
+        memset(e, 0, sizeof(*e));
+        if (energy) {
+            // bead averages and constant terms as PINY books them
+            const double P = (double)c->P;
+            double s[S_NSLOT] = {0};
+            for (int b = 0; b < c->P; b++)
+                for (int k = 0; k < S_NSLOT; k++) s[k] += acc[(size_t)b * S_NSLOT + k];
+            double q2 = 0, q1 = 0;
+            for (double q : c->h_charge) { q2 += q * q; q1 += q; }
+            const bool ewald = c->sys.nktot > 0 && c->sys.nchrg > 0;
+            e->vself = ewald ? -q2 * c->alp_ewd * c->self_erf / sqrt(M_PI) : 0.0;
+            e->vbgr = ewald ? -0.5 * q1 * q1 * M_PI / (c->alp_ewd * c->alp_ewd * cell.vol) : 0.0;
+            e->vlong = c->clong / cell.vol;
+            const double vvdw = s[S_VVDW] / P, vcoul = s[S_VCOUL] / P;
+            e->vreal = vvdw + vcoul;
+            e->vrecip = s[S_VRECIP] / P;
+            e->vecor = s[S_VECOR] / P;
+            e->vbond = s[S_VBOND] / P;
+            e->vbend = s[S_VBEND] / P;
+            e->vvdw = vvdw + e->vlong;
+            e->vcoul = vcoul + e->vrecip + e->vself + e->vbgr + e->vecor;
+            e->vintert = e->vreal + e->vlong + e->vrecip + e->vself + e->vbgr + e->vecor;
+            e->vintrat = e->vbond + e->vbend;
+            const double amult = c->iswit_vdw ? 1.0 : 2.0;
+            const double diag = (c->clong / cell.vol) * amult * P + e->vbgr * P;
+            e->pvten[0] = s[S_PXX] + diag;
+            e->pvten[4] = s[S_PYY] + diag;
+            e->pvten[8] = s[S_PZZ] + diag;
+            e->pvten[1] = e->pvten[3] = s[S_PXY];
+            e->pvten[2] = e->pvten[6] = s[S_PXZ];
+            e->pvten[5] = e->pvten[7] = s[S_PYZ];
+        }
+    }
+    return PINYB200_OK;
+}
+
+// mode-1 positions for a PIMD call without xmod: the bead centroid
+__global__ void centroid_kernel(const double *__restrict__ posT, double *__restrict__ xm, int natm, int P)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)natm * 3) return;
+    double s = 0.0;
+    for (int b = 0; b < P; b++) s += posT[t * P + b];
+    xm[t] = s / (double)P;
+}
+
+int pinyb200_energy_force_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const double *hmat,
+                                 int flags, double *d_force, pinyb200_energies *e, void *stream)
+{
+    if (!c || !d_pos || !hmat || !d_force) return fail(c, PINYB200_ERR_ARG, "energy_force_device: NULL argument");
+    if (!c->have_list) return fail(c, PINYB200_ERR_STATE, "energy_force: build the Verlet list first");
+    CK(cudaSetDevice(c->device));
+    cudaStream_t user = (cudaStream_t)stream;
+    if (user) {
+        // order the context stream after the caller's stream
+        CK(cudaEventRecord(c->ev[5], user));
+        CK(cudaStreamWaitEvent(c->stream, c->ev[5], 0));
+    }
+    Cell cell = make_cell(hmat);
+    CK(launch_transpose_in(c, d_pos));
+    if (c->P > 1) {
+        if (d_xmod) {
+            CK(cudaMemcpyAsync(c->d_xmod, d_xmod, (size_t)c->sys.natm * 3 * sizeof(double), cudaMemcpyDeviceToDevice,
+                               c->stream));
+        } else {
+            const long long n = (long long)c->sys.natm * 3;
+            centroid_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->d_posT, c->d_xmod, c->sys.natm, c->P);
+            CK(cudaGetLastError());
+        }
+    }
+    int rc = evaluate(c, cell, flags, e);
+    if (rc) return rc;
+    CK(launch_transpose_out(c, d_force));
+    CK(cudaStreamSynchronize(c->stream));
+    return PINYB200_OK;
+}
+
+int pinyb200_energy_force(pinyb200_ctx *c, const double *pos, const double *xmod, const double *hmat, int flags,
+                          double *force, pinyb200_energies *e)
+{
+    if (!c || !pos || !hmat || !force) return fail(c, PINYB200_ERR_ARG, "energy_force: NULL argument");
+    if (!c->have_list) return fail(c, PINYB200_ERR_STATE, "energy_force: build the Verlet list first");
+    CK(cudaSetDevice(c->device));
+    const size_t nb = (size_t)c->sys.natm * 3 * c->P;
+    CK(cudaMemcpyAsync(c->d_pos_aos, pos, nb * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    Cell cell = make_cell(hmat);
+    CK(launch_transpose_in(c, c->d_pos_aos));
+    if (c->P > 1) {
+        if (xmod) {
+            CK(cudaMemcpyAsync(c->d_xmod, xmod, (size_t)c->sys.natm * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                               c->stream));
+        } else {
+            const long long n = (long long)c->sys.natm * 3;
+            centroid_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->d_posT, c->d_xmod, c->sys.natm, c->P);
+            CK(cudaGetLastError());
+        }
+    }
+    int rc = evaluate(c, cell, flags, e);
+    if (rc) return rc;
+    CK(launch_transpose_out(c, c->d_force_aos));
+    CK(cudaMemcpyAsync(force, c->d_force_aos, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return PINYB200_OK;
+}
+
+int pinyb200_piny_force(pinyb200_ctx *c, double *const *x, double *const *y, double *const *z, const double *xmod,
+                        const double *ymod, const double *zmod, const double *hmat, double *const *fx,
+                        double *const *fy, double *const *fz, double *pvten_tot, pinyb200_energies *e)
+{
+    if (!c || !x || !y || !z || !hmat || !fx || !fy || !fz) return fail(c, PINYB200_ERR_ARG, "piny_force: NULL");
+    const int natm = c->sys.natm, P = c->P;
+    std::vector<double> pos((size_t)P * natm * 3), frc(pos.size()), xm;
+    for (int b = 0; b < P; b++)
+        for (int i = 0; i < natm; i++) {
+            pos[((size_t)b * natm + i) * 3 + 0] = x[b][i + 1];
+            pos[((size_t)b * natm + i) * 3 + 1] = y[b][i + 1];
+            pos[((size_t)b * natm + i) * 3 + 2] = z[b][i + 1];
+        }
+    if (P > 1 && xmod && ymod && zmod) {
+        xm.resize((size_t)natm * 3);
+        for (int i = 0; i < natm; i++) {
+            xm[3 * i] = xmod[i + 1];
+            xm[3 * i + 1] = ymod[i + 1];
+            xm[3 * i + 2] = zmod[i + 1];
+        }
+    }
+    double h[9];
+    for (int k = 0; k < 9; k++) h[k] = hmat[k + 1];
+    pinyb200_energies en;
+    int rc = pinyb200_energy_force(c, pos.data(), xm.empty() ? nullptr : xm.data(), h, 0, frc.data(), &en);
+    if (rc) return rc;
+    for (int b = 0; b < P; b++)
+        for (int i = 0; i < natm; i++) {
+            fx[b][i + 1] += frc[((size_t)b * natm + i) * 3 + 0];
+            fy[b][i + 1] += frc[((size_t)b * natm + i) * 3 + 1];
+            fz[b][i + 1] += frc[((size_t)b * natm + i) * 3 + 2];
+        }
+    if (pvten_tot)
+        for (int k = 0; k < 9; k++) pvten_tot[k + 1] += en.pvten[k];
+    if (e) *e = en;
+    return PINYB200_OK;
+}
+
+int pinyb200_last_timing(pinyb200_ctx *c, float *ms, int n)
+{
+    if (!c || !ms) return fail(c, PINYB200_ERR_ARG, "last_timing: NULL");
+    for (int i = 0; i < n && i < 4; i++) ms[i] = c->last_ms[i];
+    return PINYB200_OK;
+}
+
+}  // extern "C"

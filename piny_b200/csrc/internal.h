@@ -1,0 +1,126 @@
+// Internal state and launchers of the pinyb200 library (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/pinyb200.h"
+
+namespace pinyb200 {
+
+// Per-bead accumulator slots (FP64).
+enum Slot {
+    S_VVDW = 0,   // real-space vdW energy
+    S_VCOUL,      // real-space Ewald energy
+    S_VRECIP,     // PME reciprocal energy
+    S_VECOR,      // Ewald exclusion correction
+    S_VBOND,
+    S_VBEND,
+    S_PXX, S_PYY, S_PZZ, S_PXY, S_PXZ, S_PYZ,  // bead pressure tensor
+    S_NSLOT = 16
+};
+
+// Cell passed by value to kernels: h column-major, hi = h^-1 (gethinv).
+struct Cell {
+    double h[9];
+    double hi[9];
+    double vol;
+    int cubic;
+};
+
+// Table kinds in the coefficient arrays.
+enum TabKind { T_CV0 = 0, T_CDV0 = 1, T_CV0C = 2, T_CDV0C = 3 };
+
+struct DeviceSystem {
+    int natm, ntyp, npair_typ, nsplin, nuniq;
+    int *atm_typ = nullptr;
+    double *charge = nullptr;
+    int *inter_map = nullptr;       // [npair_typ]
+    double *cutoff = nullptr;       // [npair_typ]
+    double *rmin = nullptr, *dr = nullptr, *dri = nullptr;  // [nuniq]
+    int *has_vdw = nullptr;         // [nuniq]
+    double4 *tab64 = nullptr;       // [4][nuniq][nsplin] cubic coefficients
+    float4 *tab32 = nullptr;
+    int *excl_off = nullptr, *excl_j = nullptr;
+    int nchrg;
+    int *ichrg = nullptr;           // charged atoms
+    // PME
+    int ngrid[3];
+    int n_interp;
+    int nktot;
+    int *kvec = nullptr;            // [nktot][3]
+    double *bweight = nullptr;
+    int *kmask = nullptr;           // [G] -> index into kvec or -1
+    // ecor / bonds / bends / ghosts
+    int necor, ecor_nsplin;
+    int *ecor_j1 = nullptr, *ecor_j2 = nullptr;
+    double ecor_rmin, ecor_dr, ecor_dri;
+    double4 *ecor_tab = nullptr;    // [2][ecor_nsplin]  cv0, cdv0 coefficients
+    int nbond;
+    int *bond_j = nullptr;          // [nbond][3] j1, j2, typ
+    double *bond_eq = nullptr, *bond_c = nullptr, *bond_dc = nullptr;
+    int nbend;
+    int *bend_j = nullptr;          // [nbend][4] j1, j2, j3, typ
+    double *bend_c = nullptr, *bend_s = nullptr, *bend_dc = nullptr, *bend_ds = nullptr;
+    int nghost, ghost_ncomp;
+    int *ghost_atom = nullptr, *ghost_comp = nullptr;
+    double *ghost_coef = nullptr;
+};
+
+}  // namespace pinyb200
+
+struct pinyb200_ctx {
+    int device = 0;
+    int precision = PINYB200_FP64;
+    int P = 1;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    pinyb200::DeviceSystem sys;
+    // host copies needed for energy bookkeeping
+    std::vector<double> h_charge;
+    double alp_ewd = 0, self_erf = 1, clong = 0;
+    int iswit_vdw = 1;
+    // Verlet list: full (parity) and active (force) CSR by i, j < i
+    long list_cap = 0;
+    long npairs = 0, nactive = 0;
+    int *d_row = nullptr, *d_col = nullptr;        // full
+    int *d_rowA = nullptr, *d_colA = nullptr;      // active
+    int *d_count = nullptr;                        // [2*natm] scratch
+    long long *d_tot = nullptr;                    // device totals
+    bool have_list = false;
+    // work buffers
+    double *d_posT = nullptr;     // [natm][3][P]
+    double *d_forceT = nullptr;   // [natm][3][P]
+    double *d_xmod = nullptr;     // [natm][3]
+    double *d_pos_aos = nullptr;  // [P][natm][3] staging for host calls
+    double *d_force_aos = nullptr;
+    double *d_acc = nullptr;      // [P][S_NSLOT]
+    void *d_grid = nullptr;       // [P][G] complex (float2 or double2)
+    void *d_filter = nullptr;     // [G] real: preg * bweight, 0 outside the sphere
+    double *d_twiddle64 = nullptr;  // per axis twiddles
+    float *d_twiddle32 = nullptr;
+    int *d_err = nullptr;
+    double filter_h[9] = {0};     // cell the filter was built for
+    bool filter_ok = false;
+    cudaEvent_t ev[8];
+    float last_ms[4] = {0, 0, 0, 0};
+    std::string err;
+};
+
+namespace pinyb200 {
+
+// launchers (defined in the .cu files)
+cudaError_t launch_build_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1,
+                              const double *d_xm, const double *d_cutskin2, int pass);
+cudaError_t launch_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
+cudaError_t launch_pme(pinyb200_ctx *c, const Cell &cell, bool energy);
+cudaError_t launch_intra(pinyb200_ctx *c, const Cell &cell, bool energy);
+cudaError_t launch_ghost_pos(pinyb200_ctx *c);
+cudaError_t launch_ghost_distrib(pinyb200_ctx *c);
+cudaError_t launch_transpose_in(pinyb200_ctx *c, const double *d_pos_aos);
+cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_force_aos);
+
+}  // namespace pinyb200

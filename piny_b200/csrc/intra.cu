@@ -1,0 +1,295 @@
+// Intramolecular terms, Ewald exclusion correction, ghost sites and the
+// layout transposes, all in FP64 for every bead.
+//
+//   bonds   bond_both (src/energy/intra/bond_both.c:29-420): power series
+//           V = sum c_n (r - r0)^n by Horner, F = -dV/dr d/r
+//   bends   bend (src/energy/intra/bend.c:28-440): cos/sin series with the
+//           sin clamp at 1e-8 and PINY's chain-rule forces
+//   ecor    ecor (src/energy/intra/ecorr.c:28-274): q_i q_j S(cv0),
+//           spline of -erf(alpha r)/r plus the finite-k correction
+//   ghosts  get_ghost_pos / distrib_ghost_force
+//           (src/energy/intra_con/ghost_control.c:28-129)
+#include "common.cuh"
+
+namespace pinyb200 {
+
+__device__ __forceinline__ void acc_bead(double *acc, int P, int b, int slot, double v)
+{
+    const int lane = threadIdx.x & 31;
+    if (P < 32) {
+        v = warp_sum_strided(v, P);
+        if (lane < P) atomicAdd(&acc[(size_t)b * S_NSLOT + slot], v);
+    } else {
+        atomicAdd(&acc[(size_t)b * S_NSLOT + slot], v);
+    }
+}
+
+__global__ void transpose_in_kernel(const double *__restrict__ aos, double *__restrict__ posT, int natm, int P)
+{
+    // aos[b][i][d] -> posT[i][d][b]
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)natm * 3 * P;
+    if (t >= n) return;
+    const int b = (int)(t % P);
+    const long long id = t / P;  // i*3 + d
+    posT[t] = aos[(size_t)b * natm * 3 + id];
+}
+
+__global__ void transpose_out_kernel(const double *__restrict__ fT, double *__restrict__ aos, int natm, int P)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)natm * 3 * P;
+    if (t >= n) return;
+    const long long id = t % ((long long)natm * 3);
+    const int b = (int)(t / ((long long)natm * 3));
+    aos[t] = fT[id * P + b];
+}
+
+__global__ void ghost_pos_kernel(double *__restrict__ posT, int P, int nghost, int ncomp,
+                                 const int *__restrict__ gatom, const int *__restrict__ gcomp,
+                                 const double *__restrict__ gcoef)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nghost * P) return;
+    const int b = (int)(t % P);
+    const int g = (int)(t / P);
+    const int gl = gatom[g];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        double v = 0.0;
+        for (int c = 0; c < ncomp; c++) {
+            const int at = gcomp[g * ncomp + c];
+            if (at < 0) continue;
+            v = __dadd_rn(v, __dmul_rn(gcoef[g * ncomp + c], posT[(3 * (size_t)at + d) * P + b]));
+        }
+        posT[(3 * (size_t)gl + d) * P + b] = v;
+    }
+}
+
+__global__ void ghost_distrib_kernel(double *__restrict__ fT, int P, int nghost, int ncomp,
+                                     const int *__restrict__ gatom, const int *__restrict__ gcomp,
+                                     const double *__restrict__ gcoef)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nghost * P) return;
+    const int b = (int)(t % P);
+    const int g = (int)(t / P);
+    const int gl = gatom[g];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double fg = fT[(3 * (size_t)gl + d) * P + b];
+        for (int c = 0; c < ncomp; c++) {
+            const int at = gcomp[g * ncomp + c];
+            if (at < 0) continue;
+            fT[(3 * (size_t)at + d) * P + b] += gcoef[g * ncomp + c] * fg;
+        }
+        fT[(3 * (size_t)gl + d) * P + b] = 0.0;
+    }
+}
+
+struct IntraArgs {
+    int natm, P;
+    const double *posT;
+    double *forceT;
+    double *acc;
+    const double *charge;
+    int energy;
+};
+
+__device__ __forceinline__ void add_f(double *fT, int P, int at, int b, double fx, double fy, double fz)
+{
+    atomicAdd(&fT[(3 * (size_t)at + 0) * P + b], fx);
+    atomicAdd(&fT[(3 * (size_t)at + 1) * P + b], fy);
+    atomicAdd(&fT[(3 * (size_t)at + 2) * P + b], fz);
+}
+
+__device__ __forceinline__ void load_x(const double *posT, int P, int at, int b, double &x, double &y, double &z)
+{
+    x = posT[(3 * (size_t)at + 0) * P + b];
+    y = posT[(3 * (size_t)at + 1) * P + b];
+    z = posT[(3 * (size_t)at + 2) * P + b];
+}
+
+__global__ void __launch_bounds__(256) bond_kernel(IntraArgs a, int nbond, const int *__restrict__ bj,
+                                                   const double *__restrict__ eq, const double *__restrict__ cc,
+                                                   const double *__restrict__ dc)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = t < (long long)nbond * a.P;
+    const int b = (int)(t % a.P);
+    double v = 0, p[6] = {0, 0, 0, 0, 0, 0};
+    if (valid) {
+        const int ib = (int)(t / a.P);
+        const int j1 = bj[3 * ib], j2 = bj[3 * ib + 1], ty = bj[3 * ib + 2];
+        double x1, y1, z1, x2, y2, z2;
+        load_x(a.posT, a.P, j1, b, x1, y1, z1);
+        load_x(a.posT, a.P, j2, b, x2, y2, z2);
+        const double dx = x1 - x2, dy = y1 - y2, dz = z1 - z2;
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double rr0 = r - eq[ty];
+        const double *c = cc + 7 * ty, *d = dc + 7 * ty;
+        v = (((((c[6] * rr0 + c[5]) * rr0 + c[4]) * rr0 + c[3]) * rr0 + c[2]) * rr0 + c[1]) * rr0 + c[0];
+        const double dv = ((((d[6] * rr0 + d[5]) * rr0 + d[4]) * rr0 + d[3]) * rr0 + d[2]) * rr0 + d[1];
+        const double pre = -dv / r;
+        const double fx = dx * pre, fy = dy * pre, fz = dz * pre;
+        add_f(a.forceT, a.P, j1, b, fx, fy, fz);
+        add_f(a.forceT, a.P, j2, b, -fx, -fy, -fz);
+        p[0] = dx * fx; p[1] = dy * fy; p[2] = dz * fz; p[3] = dx * fy; p[4] = dx * fz; p[5] = dy * fz;
+    }
+    if (a.energy) {
+        acc_bead(a.acc, a.P, b, S_VBOND, v);
+        for (int c = 0; c < 6; c++) acc_bead(a.acc, a.P, b, S_PXX + c, p[c]);
+    }
+}
+
+__global__ void __launch_bounds__(256) bend_kernel(IntraArgs a, int nbend, const int *__restrict__ bj,
+                                                   const double *__restrict__ bc, const double *__restrict__ bs,
+                                                   const double *__restrict__ bdc, const double *__restrict__ bds)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = t < (long long)nbend * a.P;
+    const int b = (int)(t % a.P);
+    double v = 0, p[6] = {0, 0, 0, 0, 0, 0};
+    if (valid) {
+        const int ib = (int)(t / a.P);
+        const int a1 = bj[4 * ib], a2 = bj[4 * ib + 1], a3 = bj[4 * ib + 2], ty = bj[4 * ib + 3];
+        double x1, y1, z1, x2, y2, z2, x3, y3, z3;
+        load_x(a.posT, a.P, a1, b, x1, y1, z1);
+        load_x(a.posT, a.P, a2, b, x2, y2, z2);
+        load_x(a.posT, a.P, a3, b, x3, y3, z3);
+        const double dx12 = x1 - x2, dy12 = y1 - y2, dz12 = z1 - z2;
+        const double dx23 = x3 - x2, dy23 = y3 - y2, dz23 = z3 - z2;
+        const double r122i = 1.0 / (dx12 * dx12 + dy12 * dy12 + dz12 * dz12);
+        const double r12i = sqrt(r122i);
+        const double r322i = 1.0 / (dx23 * dx23 + dy23 * dy23 + dz23 * dz23);
+        const double r32i = sqrt(r322i);
+        const double rpmag = r12i * r32i;
+        double cost = (dx12 * dx23 + dy12 * dy23 + dz12 * dz23) * rpmag;
+        cost = cost < 1.0 ? cost : 1.0;
+        cost = cost > -1.0 ? cost : -1.0;
+        double sint = sqrt(1.0 - cost * cost);
+        sint = sint > 1.0e-8 ? sint : 1.0e-8;
+        const double cos122 = cost * r122i, cos322 = cost * r322i;
+        const double *c = bc + 7 * ty, *s = bs + 7 * ty, *dc = bdc + 7 * ty, *ds = bds + 7 * ty;
+        const double vc = ((((((c[6] * cost + c[5]) * cost + c[4]) * cost + c[3]) * cost + c[2]) * cost + c[1]) * cost +
+                           c[0]);
+        const double sisum = (((((s[6] * sint + s[5]) * sint + s[4]) * sint + s[3]) * sint + s[2]) * sint);
+        v = vc + (sisum * cost + s[1] * sint);
+        const double dvc = (((((dc[6] * cost + dc[5]) * cost + dc[4]) * cost + dc[3]) * cost + dc[2]) * cost + dc[1]);
+        double dvs = ((((ds[6] * sint + ds[5]) * sint + ds[4]) * sint + ds[3]) * sint + ds[2]);
+        dvs = dvs * cost + ds[1];
+        const double pre = -(dvc + sisum - dvs * cost / sint);
+        const double fx1 = (dx23 * rpmag - dx12 * cos122) * pre, fy1 = (dy23 * rpmag - dy12 * cos122) * pre,
+                     fz1 = (dz23 * rpmag - dz12 * cos122) * pre;
+        const double fx3 = (dx12 * rpmag - dx23 * cos322) * pre, fy3 = (dy12 * rpmag - dy23 * cos322) * pre,
+                     fz3 = (dz12 * rpmag - dz23 * cos322) * pre;
+        add_f(a.forceT, a.P, a1, b, fx1, fy1, fz1);
+        add_f(a.forceT, a.P, a2, b, -(fx1 + fx3), -(fy1 + fy3), -(fz1 + fz3));
+        add_f(a.forceT, a.P, a3, b, fx3, fy3, fz3);
+        p[0] = dx12 * fx1 + dx23 * fx3;
+        p[1] = dy12 * fy1 + dy23 * fy3;
+        p[2] = dz12 * fz1 + dz23 * fz3;
+        p[3] = dx12 * fy1 + dx23 * fy3;
+        p[4] = dx12 * fz1 + dx23 * fz3;
+        p[5] = dy12 * fz1 + dy23 * fz3;
+    }
+    if (a.energy) {
+        acc_bead(a.acc, a.P, b, S_VBEND, v);
+        for (int c = 0; c < 6; c++) acc_bead(a.acc, a.P, b, S_PXX + c, p[c]);
+    }
+}
+
+__global__ void __launch_bounds__(256) ecor_kernel(IntraArgs a, int necor, const int *__restrict__ j1s,
+                                                   const int *__restrict__ j2s, int nsplin, double rmin, double dr,
+                                                   double dri, const double4 *__restrict__ tab)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = t < (long long)necor * a.P;
+    const int b = (int)(t % a.P);
+    double v = 0, p[6] = {0, 0, 0, 0, 0, 0};
+    if (valid) {
+        const int ie = (int)(t / a.P);
+        const int j1 = j1s[ie], j2 = j2s[ie];
+        double x1, y1, z1, x2, y2, z2;
+        load_x(a.posT, a.P, j1, b, x1, y1, z1);
+        load_x(a.posT, a.P, j2, b, x2, y2, z2);
+        const double dx = x1 - x2, dy = y1 - y2, dz = z1 - z2;
+        const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+        int k = __double2int_rz(__dadd_rn(__dmul_rn(__dsub_rn(r, rmin), dri), 0.5)) + 3;
+        k = k < nsplin - 2 ? k : nsplin - 2;
+        k = k > 3 ? k : 3;
+        const double rsp = __dadd_rn(__dmul_rn((double)(k - 3), dr), rmin);
+        const double del = __dmul_rn(__dsub_rn(r, rsp), dri);
+        const double q12 = a.charge[j1] * a.charge[j2];
+        v = spline_eval<double4, double>(tab[k - 1], del) * q12;
+        const double dvt = spline_eval<double4, double>(tab[nsplin + k - 1], del) * q12;
+        const double fx = dx * dvt, fy = dy * dvt, fz = dz * dvt;
+        add_f(a.forceT, a.P, j1, b, fx, fy, fz);
+        add_f(a.forceT, a.P, j2, b, -fx, -fy, -fz);
+        p[0] = dx * fx; p[1] = dy * fy; p[2] = dz * fz; p[3] = dx * fy; p[4] = dx * fz; p[5] = dy * fz;
+    }
+    if (a.energy) {
+        acc_bead(a.acc, a.P, b, S_VECOR, v);
+        for (int c = 0; c < 6; c++) acc_bead(a.acc, a.P, b, S_PXX + c, p[c]);
+    }
+}
+
+static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+cudaError_t launch_transpose_in(pinyb200_ctx *c, const double *d_aos)
+{
+    const long long n = (long long)c->sys.natm * 3 * c->P;
+    transpose_in_kernel<<<nblk(n, 256), 256, 0, c->stream>>>(d_aos, c->d_posT, c->sys.natm, c->P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_aos)
+{
+    const long long n = (long long)c->sys.natm * 3 * c->P;
+    transpose_out_kernel<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_forceT, d_aos, c->sys.natm, c->P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost_pos(pinyb200_ctx *c)
+{
+    const DeviceSystem &s = c->sys;
+    if (s.nghost == 0) return cudaSuccess;
+    ghost_pos_kernel<<<nblk((long long)s.nghost * c->P, 256), 256, 0, c->stream>>>(
+        c->d_posT, c->P, s.nghost, s.ghost_ncomp, s.ghost_atom, s.ghost_comp, s.ghost_coef);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost_distrib(pinyb200_ctx *c)
+{
+    const DeviceSystem &s = c->sys;
+    if (s.nghost == 0) return cudaSuccess;
+    ghost_distrib_kernel<<<nblk((long long)s.nghost * c->P, 256), 256, 0, c->stream>>>(
+        c->d_forceT, c->P, s.nghost, s.ghost_ncomp, s.ghost_atom, s.ghost_comp, s.ghost_coef);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_intra(pinyb200_ctx *c, const Cell &cell, bool energy)
+{
+    (void)cell;
+    const DeviceSystem &s = c->sys;
+    IntraArgs a;
+    a.natm = s.natm;
+    a.P = c->P;
+    a.posT = c->d_posT;
+    a.forceT = c->d_forceT;
+    a.acc = c->d_acc;
+    a.charge = s.charge;
+    a.energy = energy ? 1 : 0;
+    if (s.nbond)
+        bond_kernel<<<nblk((long long)s.nbond * c->P, 256), 256, 0, c->stream>>>(a, s.nbond, s.bond_j, s.bond_eq,
+                                                                                  s.bond_c, s.bond_dc);
+    if (s.nbend)
+        bend_kernel<<<nblk((long long)s.nbend * c->P, 256), 256, 0, c->stream>>>(a, s.nbend, s.bend_j, s.bend_c,
+                                                                                  s.bend_s, s.bend_dc, s.bend_ds);
+    if (s.necor)
+        ecor_kernel<<<nblk((long long)s.necor * c->P, 256), 256, 0, c->stream>>>(
+            a, s.necor, s.ecor_j1, s.ecor_j2, s.ecor_nsplin, s.ecor_rmin, s.ecor_dr, s.ecor_dri, s.ecor_tab);
+    return cudaGetLastError();
+}
+
+}  // namespace pinyb200

@@ -1,0 +1,210 @@
+"""ctypes binding of the pinyb200 C ABI (include/pinyb200.h).
+
+The device library is the only compute path: if libpinyb200.so is missing
+and cannot be built, or no GPU is present, every call raises.  There is no
+CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_i = C.c_int
+_d = C.c_double
+_pi = C.POINTER(C.c_int)
+_pd = C.POINTER(C.c_double)
+
+PINYB200_FP64 = 0
+PINYB200_MIXED = 1
+DISTRIB_GHOSTS = 1
+NO_ENERGY = 2
+
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NO_DEVICE", 4: "ERR_LIST_OVERFLOW", 5: "ERR_CUTOFF",
+          6: "ERR_TIMEOUT", 7: "ERR_NAN", 8: "ERR_UNSUPPORTED", 9: "ERR_STATE"}
+
+
+class PinySystem(C.Structure):
+    """pinyb200_system (include/pinyb200.h)."""
+    _fields_ = [
+        ("natm", _i), ("ntyp", _i), ("atm_typ", _pi), ("charge", _pd),
+        ("nsplin", _i), ("ninter_unique", _i), ("inter_map", _pi), ("cutoff", _pd),
+        ("rmin_spl", _pd), ("dr_spl", _pd), ("dri_spl", _pd),
+        ("cv0", _pd), ("cdv0", _pd), ("cv0_c", _pd), ("cdv0_c", _pd),
+        ("skin", _d), ("clong", _d), ("iswit_vdw", _i),
+        ("excl_off", _pi), ("excl_j", _pi),
+        ("alp_ewd", _d), ("self_erf", _d), ("nktot", _i),
+        ("kastr", _pi), ("kbstr", _pi), ("kcstr", _pi), ("bweight", _pd),
+        ("ngrid_a", _i), ("ngrid_b", _i), ("ngrid_c", _i), ("n_interp", _i),
+        ("necor", _i), ("ecor_j1", _pi), ("ecor_j2", _pi), ("ecor_nsplin", _i),
+        ("ecor_rmin", _d), ("ecor_dr", _d), ("ecor_dri", _d), ("ecor_cv0", _pd), ("ecor_cdv0", _pd),
+        ("nbond", _i), ("bond_j1", _pi), ("bond_j2", _pi), ("bond_typ", _pi), ("nbond_typ", _i),
+        ("bond_eq", _pd), ("bond_c", _pd), ("bond_dc", _pd),
+        ("nbend", _i), ("bend_j1", _pi), ("bend_j2", _pi), ("bend_j3", _pi), ("bend_typ", _pi),
+        ("nbend_typ", _i), ("bend_c", _pd), ("bend_s", _pd), ("bend_dc", _pd), ("bend_ds", _pd),
+        ("nghost", _i), ("ghost_ncomp", _i), ("ghost_atom", _pi), ("ghost_comp", _pi), ("ghost_coef", _pd),
+    ]
+
+
+ENERGY_NAMES = ("vreal", "vvdw", "vcoul", "vrecip", "vself", "vbgr", "vecor", "vlong",
+                "vbond", "vbend", "vintert", "vintrat")
+
+
+class PinyEnergies(C.Structure):
+    _fields_ = [(n, _d) for n in ENERGY_NAMES] + [("pvten", _d * 9)]
+
+
+# every symbol include/pinyb200.h declares
+EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb200_destroy",
+           "pinyb200_build_list", "pinyb200_get_list", "pinyb200_energy_force",
+           "pinyb200_energy_force_device", "pinyb200_piny_force", "pinyb200_last_timing",
+           "pinyb200_last_error")
+
+_LIB = None
+
+
+class PinyError(RuntimeError):
+    pass
+
+
+def load(build_if_missing: bool = True):
+    """Load (building if needed) the in-tree libpinyb200.so."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = _build.LIB
+    if not os.path.exists(path) or (build_if_missing and _build.needs_build()):
+        if not build_if_missing:
+            raise PinyError("libpinyb200.so is not built (python -m piny_b200.build)")
+        _build.build()
+    L = C.CDLL(path)
+    L.pinyb200_version.restype = _i
+    L.pinyb200_device_info.argtypes = [C.c_char_p, _i, _pi]
+    L.pinyb200_create.argtypes = [C.POINTER(PinySystem), _i, _i, C.POINTER(C.c_void_p)]
+    L.pinyb200_destroy.argtypes = [C.c_void_p]
+    L.pinyb200_build_list.argtypes = [C.c_void_p, _pd, _pd, _pd, _pd, C.POINTER(C.c_long)]
+    L.pinyb200_get_list.argtypes = [C.c_void_p, _pi, _pi, C.c_long, C.POINTER(C.c_long)]
+    L.pinyb200_energy_force.argtypes = [C.c_void_p, _pd, _pd, _pd, _i, _pd, C.POINTER(PinyEnergies)]
+    L.pinyb200_energy_force_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, _i, C.c_void_p,
+                                               C.POINTER(PinyEnergies), C.c_void_p]
+    L.pinyb200_piny_force.argtypes = [C.c_void_p] + [C.c_void_p] * 3 + [_pd] * 3 + [_pd] + [C.c_void_p] * 3 + \
+        [_pd, C.POINTER(PinyEnergies)]
+    L.pinyb200_last_timing.argtypes = [C.c_void_p, C.POINTER(C.c_float), _i]
+    L.pinyb200_last_error.restype = C.c_char_p
+    L.pinyb200_last_error.argtypes = [C.c_void_p]
+    _LIB = L
+    return L
+
+
+def _dp(a):
+    return a.ctypes.data_as(_pd)
+
+
+def make_struct(sysd: dict):
+    """pinyb200_system from a set-up dict (piny_b200.system.build_system)."""
+    keep = []
+    s = PinySystem()
+    for name, ctype in PinySystem._fields_:
+        v = sysd.get(name)
+        if ctype is _pd:
+            a = np.ascontiguousarray(np.zeros(1) if v is None else v, dtype=np.float64)
+            keep.append(a)
+            setattr(s, name, a.ctypes.data_as(_pd))
+        elif ctype is _pi:
+            a = np.ascontiguousarray(np.zeros(1, np.int32) if v is None else v, dtype=np.int32)
+            keep.append(a)
+            setattr(s, name, a.ctypes.data_as(_pi))
+        else:
+            setattr(s, name, 0 if v is None else v)
+    s._keep = keep
+    return s
+
+
+def energies_dict(e: PinyEnergies):
+    out = {n: getattr(e, n) for n in ENERGY_NAMES}
+    out["pvten"] = np.array(e.pvten[:])
+    return out
+
+
+class DeviceBox:
+    """One box of nbeads beads resident on the GPU (a pinyb200 context)."""
+
+    def __init__(self, sysd: dict, nbeads: int, precision: str = "fp64"):
+        self.L = load()
+        self.natm = int(sysd["natm"])
+        self.P = int(nbeads)
+        self.ntyp = int(sysd["ntyp"])
+        self.precision = precision
+        prec = PINYB200_FP64 if precision == "fp64" else PINYB200_MIXED
+        st = make_struct(sysd)
+        h = C.c_void_p()
+        rc = self.L.pinyb200_create(C.byref(st), self.P, prec, C.byref(h))
+        if rc != 0:
+            raise PinyError("pinyb200_create: %s %s" % (STATUS.get(rc, rc), self.L.pinyb200_last_error(None).decode()))
+        self.h = h
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise PinyError("%s: %s %s" % (what, STATUS.get(rc, rc), self.L.pinyb200_last_error(self.h).decode()))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pinyb200_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def build_list(self, pos1, xmod, hmat, cutskin2):
+        pos1 = np.ascontiguousarray(pos1, np.float64).reshape(self.natm, 3)
+        xm = None if xmod is None else np.ascontiguousarray(xmod, np.float64).reshape(self.natm, 3)
+        hmat = np.ascontiguousarray(hmat, np.float64)
+        cs = np.ascontiguousarray(cutskin2, np.float64)
+        n = C.c_long()
+        self._check(self.L.pinyb200_build_list(self.h, _dp(pos1), None if xm is None else _dp(xm), _dp(hmat),
+                                               _dp(cs), C.byref(n)), "build_list")
+        return n.value
+
+    def get_list(self):
+        n = C.c_long()
+        self._check(self.L.pinyb200_get_list(self.h, None, None, 0, C.byref(n)), "get_list")
+        pi = np.zeros(max(n.value, 1), np.int32)
+        pj = np.zeros(max(n.value, 1), np.int32)
+        self._check(self.L.pinyb200_get_list(self.h, pi.ctypes.data_as(_pi), pj.ctypes.data_as(_pi), n.value,
+                                             C.byref(n)), "get_list")
+        return pi[:n.value], pj[:n.value]
+
+    def energy_force(self, pos, xmod, hmat, distribute_ghosts=False, energy=True):
+        pos = np.ascontiguousarray(pos, np.float64).reshape(self.P, self.natm, 3)
+        xm = None if xmod is None else np.ascontiguousarray(xmod, np.float64).reshape(self.natm, 3)
+        hmat = np.ascontiguousarray(hmat, np.float64)
+        force = np.empty_like(pos)
+        e = PinyEnergies()
+        flags = (DISTRIB_GHOSTS if distribute_ghosts else 0) | (0 if energy else NO_ENERGY)
+        self._check(self.L.pinyb200_energy_force(self.h, _dp(pos), None if xm is None else _dp(xm), _dp(hmat),
+                                                 flags, _dp(force), C.byref(e)), "energy_force")
+        return force, energies_dict(e)
+
+    def energy_force_device(self, d_pos: int, d_xmod, hmat, d_force: int, stream=None, distribute_ghosts=False,
+                            energy=True):
+        """Device-pointer variant; pointers are integers (e.g. tensor.data_ptr())."""
+        hmat = np.ascontiguousarray(hmat, np.float64)
+        e = PinyEnergies()
+        flags = (DISTRIB_GHOSTS if distribute_ghosts else 0) | (0 if energy else NO_ENERGY)
+        self._check(self.L.pinyb200_energy_force_device(self.h, C.c_void_p(d_pos),
+                                                        None if d_xmod is None else C.c_void_p(d_xmod), _dp(hmat),
+                                                        flags, C.c_void_p(d_force), C.byref(e),
+                                                        None if stream is None else C.c_void_p(stream)),
+                    "energy_force_device")
+        return energies_dict(e)
+
+    def last_timing(self):
+        ms = (C.c_float * 4)()
+        self._check(self.L.pinyb200_last_timing(self.h, ms, 4), "last_timing")
+        return list(ms)

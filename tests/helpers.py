@@ -1,0 +1,32 @@
+"""Shared test helpers: golden fixtures and box specs."""
+import hashlib
+import os
+
+import numpy as np
+
+from piny_b200 import water
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+GOLDEN_NAMES = ["spcfw_64_p1", "spcfw_64_p4", "tip4pf_64_p4", "spcfw_256_p1", "tip4pf_128_p2"]
+
+
+def load_fixture(name):
+    F = dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+    return {k: (v.item() if v.ndim == 0 else v) for k, v in F.items()}
+
+
+def spec_from_fixture(F):
+    model = water.TIP4P_F if str(F["spec_model"]) == "tip4pf" else water.SPC_FW
+    return water.BoxSpec(model, int(F["spec_nmol"]), float(F["spec_L"]), int(F["nbeads"]),
+                         float(F["spec_temperature"]), 0, cutoff=float(F["spec_cutoff"]),
+                         grid=int(F["ngrid_a"]), order=int(F["spec_order"]), kmax=int(F["spec_kmax"]),
+                         nsplin=int(F["spec_nsplin"]), kmax_pme_in=int(F["spec_kmax_pme"]))
+
+
+def pair_hash(pi, pj):
+    key = np.sort(np.asarray(pi, np.int64) * (1 << 32) + np.asarray(pj, np.int64))
+    return hashlib.sha256(key.tobytes()).hexdigest()
+
+
+def rel_rms(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))

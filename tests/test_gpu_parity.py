@@ -1,0 +1,84 @@
+"""Device path against PINY's outputs (golden fixtures) and the oracle.
+
+Tolerances (force relative RMS  ||F - F_ref|| / ||F_ref||):
+  FP64 mode   1e-12
+  MIXED mode  1e-5
+Pair sets must match PINY's bit for bit in every mode.
+"""
+import numpy as np
+import pytest
+
+from helpers import GOLDEN_NAMES, load_fixture, pair_hash, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-12, "mixed": 1e-5}
+ETOL = {"fp64": 1e-11, "mixed": 1e-6}
+
+
+def _box(F, prec):
+    from piny_b200.lib import DeviceBox
+    return DeviceBox(F, int(F["nbeads"]), prec)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
+def test_device_matches_piny(name, prec):
+    F = load_fixture(name)
+    box = _box(F, prec)
+    xmod = F.get("xmod")
+    n = box.build_list(F["pos"][0], xmod, F["hmat"], F["cutskin2"])
+    pi, pj = box.get_list()
+    assert n == F["npairs"]
+    assert pair_hash(pi, pj) == F["pairs_sha256"]
+    force, e = box.energy_force(F["pos"], xmod, F["hmat"])
+    assert rel_rms(force, F["ref_force_raw"]) < TOL[prec]
+    force2, _ = box.energy_force(F["pos"], xmod, F["hmat"], distribute_ghosts=True)
+    assert rel_rms(force2, F["ref_force"]) < TOL[prec]
+    for k, kr in [("vintert", "vintert"), ("vintrat", "vintrat"), ("vvdw", "vvdw"), ("vcoul", "vcoul"),
+                  ("vlong", "vlong"), ("vbond", "vbondt"), ("vbend", "vbendt")]:
+        ref = F["ref_" + kr]
+        assert abs(e[k] - ref) <= ETOL[prec] * max(1.0, abs(ref)), (k, e[k], ref)
+    vrec = e["vrecip"] + e["vself"] + e["vbgr"] + e["vecor"]
+    assert abs(vrec - F["ref_vrecip"]) <= ETOL[prec] * max(1.0, abs(F["ref_vrecip"]))
+    pv = F["ref_pvten_tot"]
+    assert np.abs(e["pvten"] - pv).max() <= ETOL[prec] * 10 * np.abs(pv).max()
+    box.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_device_matches_oracle_32_beads(prec, oracle):
+    """q-SPC/Fw 256 molecules, P = 32 (mixed-precision config), host set-up
+    from piny_b200.system, oracle on the same inputs."""
+    from piny_b200 import system, water
+    spec = water.named_spec("spcfw_256_p32")
+    pos = water.build_positions(spec) / water.BOHR
+    S = system.build_system(spec, pos)
+    xmod = pos.mean(axis=0)
+    pi, pj = oracle.verlist(S, pos[0], xmod, S["hmat"], S["cutskin2"])
+    fref, eref = oracle.energy_force(S, pos, xmod, S["hmat"], pi, pj)
+    from piny_b200.lib import DeviceBox
+    box = DeviceBox(S, spec.nbeads, prec)
+    n = box.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+    gi, gj = box.get_list()
+    assert n == len(pi) and pair_hash(gi, gj) == pair_hash(pi, pj)
+    f, e = box.energy_force(pos, xmod, S["hmat"])
+    assert rel_rms(f, fref) < TOL[prec]
+    assert abs(e["vintert"] - eref["vintert"]) <= ETOL[prec] * abs(eref["vintert"])
+    assert abs(e["vintrat"] - eref["vintrat"]) <= ETOL[prec] * abs(eref["vintrat"])
+    box.close()
+
+
+def test_list_errors_and_state():
+    F = load_fixture("spcfw_64_p1")
+    from piny_b200.lib import DeviceBox, PinyError
+    box = DeviceBox(F, 1, "fp64")
+    with pytest.raises(PinyError, match="ERR_STATE"):
+        box.energy_force(F["pos"], None, F["hmat"])
+    box.close()
+    bad = dict(F)
+    bad["atm_typ"] = np.array(F["atm_typ"]) + 5
+    with pytest.raises(PinyError, match="ERR_ARG"):
+        DeviceBox(bad, 1, "fp64")
+    with pytest.raises(PinyError, match="ERR_UNSUPPORTED"):
+        DeviceBox(F, 3, "fp64")
