@@ -169,6 +169,11 @@ int pinyb200_build_list(pinyb200_ctx *ctx, const double *pos1,
 int pinyb200_get_list(pinyb200_ctx *ctx, int *pi, int *pj, long cap,
                       long *npairs);
 
+/* Sizes of the current list: all pairs, the force-bearing ("active") pairs
+ * the pair kernel walks (a charge product or a vdW table), and capacity. */
+int pinyb200_list_info(pinyb200_ctx *ctx, long *npairs, long *nactive,
+                       long *capacity);
+
 /*
  * One force/energy evaluation of all beads with host buffers.
  *   pos   : nbeads x natm x 3 host array (bead-major AoS), ghosts are
@@ -181,8 +186,9 @@ int pinyb200_energy_force(pinyb200_ctx *ctx, const double *pos,
                           double *force, pinyb200_energies *e);
 
 /* Same, with device-resident pos / xmod / force (cudaMalloc'd by the
- * caller, same layouts) on the CUDA stream passed as an opaque handle
- * (NULL = the context's own stream).  Returns after the stream is idle. */
+ * caller, same layouts).  The work is launched on the CUDA stream passed as
+ * an opaque handle (NULL = the context's own stream); the call returns after
+ * that stream is idle. */
 int pinyb200_energy_force_device(pinyb200_ctx *ctx, const double *d_pos,
                                  const double *d_xmod, const double *hmat,
                                  int flags, double *d_force,
@@ -203,8 +209,9 @@ int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
                         double *const *fy, double *const *fz,
                         double *pvten_tot, pinyb200_energies *e);
 
-/* Milliseconds of the last evaluation's device work, per phase
- * (0 total, 1 pair, 2 PME, 3 intra) and the pair count it used. */
+/* Milliseconds of the last evaluation, from CUDA events on its stream:
+ * 0 device work, 1 pair forces, 2 PME, 3 intramolecular, 4 the whole
+ * host-buffer call of pinyb200_energy_force (copies included). */
 int pinyb200_last_timing(pinyb200_ctx *ctx, float *ms, int n);
 
 /* Last error text for this context (or the library if ctx is NULL). */

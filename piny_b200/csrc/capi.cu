@@ -500,12 +500,14 @@ int pinyb200_energy_force_device(pinyb200_ctx *c, const double *d_pos, const dou
     if (!c || !d_pos || !hmat || !d_force) return fail(c, PINYB200_ERR_ARG, "energy_force_device: NULL argument");
     if (!c->have_list) return fail(c, PINYB200_ERR_STATE, "energy_force: build the Verlet list first");
     CK(cudaSetDevice(c->device));
-    cudaStream_t user = (cudaStream_t)stream;
-    if (user) {
-        // order the context stream after the caller's stream
-        CK(cudaEventRecord(c->ev[5], user));
-        CK(cudaStreamWaitEvent(c->stream, c->ev[5], 0));
-    }
+    // launch on the caller's stream when one is given
+    cudaStream_t own = c->stream;
+    if (stream) c->stream = (cudaStream_t)stream;
+    struct Restore {
+        pinyb200_ctx *c;
+        cudaStream_t s;
+        ~Restore() { c->stream = s; }
+    } restore{c, own};
     Cell cell = make_cell(hmat);
     CK(launch_transpose_in(c, d_pos));
     if (c->P > 1) {
@@ -532,6 +534,7 @@ int pinyb200_energy_force(pinyb200_ctx *c, const double *pos, const double *xmod
     if (!c->have_list) return fail(c, PINYB200_ERR_STATE, "energy_force: build the Verlet list first");
     CK(cudaSetDevice(c->device));
     const size_t nb = (size_t)c->sys.natm * 3 * c->P;
+    CK(cudaEventRecord(c->ev[6], c->stream));
     CK(cudaMemcpyAsync(c->d_pos_aos, pos, nb * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     Cell cell = make_cell(hmat);
     CK(launch_transpose_in(c, c->d_pos_aos));
@@ -549,7 +552,9 @@ int pinyb200_energy_force(pinyb200_ctx *c, const double *pos, const double *xmod
     if (rc) return rc;
     CK(launch_transpose_out(c, c->d_force_aos));
     CK(cudaMemcpyAsync(force, c->d_force_aos, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaEventRecord(c->ev[7], c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    CK(cudaEventElapsedTime(&c->last_ms[4], c->ev[6], c->ev[7]));
     return PINYB200_OK;
 }
 
@@ -591,10 +596,19 @@ int pinyb200_piny_force(pinyb200_ctx *c, double *const *x, double *const *y, dou
     return PINYB200_OK;
 }
 
+int pinyb200_list_info(pinyb200_ctx *c, long *npairs, long *nactive, long *capacity)
+{
+    if (!c) return fail(c, PINYB200_ERR_ARG, "list_info: NULL context");
+    if (npairs) *npairs = (long)c->npairs;
+    if (nactive) *nactive = (long)c->nactive;
+    if (capacity) *capacity = (long)c->list_cap;
+    return c->have_list ? PINYB200_OK : fail(c, PINYB200_ERR_STATE, "no list built yet");
+}
+
 int pinyb200_last_timing(pinyb200_ctx *c, float *ms, int n)
 {
     if (!c || !ms) return fail(c, PINYB200_ERR_ARG, "last_timing: NULL");
-    for (int i = 0; i < n && i < 4; i++) ms[i] = c->last_ms[i];
+    for (int i = 0; i < n && i < 5; i++) ms[i] = c->last_ms[i];
     return PINYB200_OK;
 }
 

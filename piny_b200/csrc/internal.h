@@ -106,7 +106,7 @@ struct pinyb200_ctx {
     double filter_h[9] = {0};     // cell the filter was built for
     bool filter_ok = false;
     cudaEvent_t ev[8];
-    float last_ms[4] = {0, 0, 0, 0};
+    float last_ms[5] = {0, 0, 0, 0, 0};
     std::string err;
 };
 

@@ -61,6 +61,10 @@ __device__ __forceinline__ void scaled(double s, int N, int &i0, double &frac)
     double xs = __dmul_rn(s, (double)N);
     i0 = (int)xs;
     frac = __dsub_rn(xs, (double)i0);
+    // s == 1 exactly (a coordinate on a cell face) and non-finite positions
+    // would index outside the grid; keep every access in bounds.
+    if (i0 == N) i0 = 0;
+    if (!(i0 >= 0 && i0 < N)) { i0 = 0; frac = 0.0; }
 }
 
 template <typename R, int NI>
@@ -371,11 +375,14 @@ __global__ void __launch_bounds__(256) conv_kernel(void *data, const R *__restri
     }
 }
 
+// Lines per block: a power of two <= 16 that divides the line count of the
+// tile decomposition and keeps the staged tile within 48 KB.
 template <typename R>
-static int pick_tl(int Na)
+static int pick_tl(long long divisor, int N)
 {
+    typedef typename Cplx<R>::T C2;
     int tl = 16;
-    while (tl > 1 && (Na % tl)) tl >>= 1;
+    while (tl > 1 && ((divisor % tl) || (size_t)tl * N * sizeof(C2) > 48 * 1024)) tl >>= 1;
     return tl;
 }
 
@@ -407,12 +414,14 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     const R *twbase = (const R *)(sizeof(R) == 8 ? (const void *)c->d_twiddle64 : (const void *)c->d_twiddle32);
     const int maxN = 256;
     for (int ax = 0; ax < 3; ax++) tw[ax] = twbase + 2 * maxN * ax;
-    const int TL = pick_tl<R>(a.Na);
     const int dims[3] = {a.Na, a.Nb, a.Nc};
+    const int TLs[3] = {pick_tl<R>((long long)a.Nb * a.Nc * a.P, a.Na), pick_tl<R>(a.Na, a.Nb),
+                        pick_tl<R>(a.Na, a.Nc)};
     for (int pass = 0; pass < 2; pass++) {
         const int sign = pass == 0 ? +1 : -1;
         for (int ax = 0; ax < 3; ax++) {
             const int N = dims[ax];
+            const int TL = TLs[ax];
             long long nlines = (long long)G * a.P / N;
             int tiles = (int)(nlines / TL);
             size_t sh = sizeof(C2) * TL * N;

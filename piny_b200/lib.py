@@ -59,7 +59,7 @@ class PinyEnergies(C.Structure):
 
 # every symbol include/pinyb200.h declares
 EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb200_destroy",
-           "pinyb200_build_list", "pinyb200_get_list", "pinyb200_energy_force",
+           "pinyb200_build_list", "pinyb200_get_list", "pinyb200_list_info", "pinyb200_energy_force",
            "pinyb200_energy_force_device", "pinyb200_piny_force", "pinyb200_last_timing",
            "pinyb200_last_error")
 
@@ -87,6 +87,7 @@ def load(build_if_missing: bool = True):
     L.pinyb200_destroy.argtypes = [C.c_void_p]
     L.pinyb200_build_list.argtypes = [C.c_void_p, _pd, _pd, _pd, _pd, C.POINTER(C.c_long)]
     L.pinyb200_get_list.argtypes = [C.c_void_p, _pi, _pi, C.c_long, C.POINTER(C.c_long)]
+    L.pinyb200_list_info.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long), C.POINTER(C.c_long)]
     L.pinyb200_energy_force.argtypes = [C.c_void_p, _pd, _pd, _pd, _i, _pd, C.POINTER(PinyEnergies)]
     L.pinyb200_energy_force_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, _i, C.c_void_p,
                                                C.POINTER(PinyEnergies), C.c_void_p]
@@ -180,6 +181,11 @@ class DeviceBox:
                                              C.byref(n)), "get_list")
         return pi[:n.value], pj[:n.value]
 
+    def list_info(self):
+        n, a, c = C.c_long(), C.c_long(), C.c_long()
+        self._check(self.L.pinyb200_list_info(self.h, C.byref(n), C.byref(a), C.byref(c)), "list_info")
+        return {"npairs": n.value, "nactive": a.value, "capacity": c.value}
+
     def energy_force(self, pos, xmod, hmat, distribute_ghosts=False, energy=True):
         pos = np.ascontiguousarray(pos, np.float64).reshape(self.P, self.natm, 3)
         xm = None if xmod is None else np.ascontiguousarray(xmod, np.float64).reshape(self.natm, 3)
@@ -205,6 +211,6 @@ class DeviceBox:
         return energies_dict(e)
 
     def last_timing(self):
-        ms = (C.c_float * 4)()
-        self._check(self.L.pinyb200_last_timing(self.h, ms, 4), "last_timing")
+        ms = (C.c_float * 5)()
+        self._check(self.L.pinyb200_last_timing(self.h, ms, 5), "last_timing")
         return list(ms)
