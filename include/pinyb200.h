@@ -42,7 +42,8 @@ enum {
 /* Flags for pinyb200_energy_force*(). */
 enum {
     PINYB200_DISTRIB_GHOSTS = 1, /* apply distrib_ghost_force (ghost_control.c:71) */
-    PINYB200_NO_ENERGY = 2       /* skip energy/virial reductions                   */
+    PINYB200_NO_ENERGY = 2,      /* skip energy/virial reductions                   */
+    PINYB200_SITE_PAIRS = 4      /* walk the site list instead of molecule pairs    */
 };
 
 /*

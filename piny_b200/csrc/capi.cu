@@ -170,8 +170,8 @@ int pinyb200_destroy(pinyb200_ctx *c)
     cudaSetDevice(c->device);
     free_sys(c->sys);
     void *ptrs[] = {c->d_row, c->d_col, c->d_rowA, c->d_colA, c->d_count, c->d_tot, c->d_posT, c->d_forceT,
-                    c->d_xmod, c->d_pos_aos, c->d_force_aos, c->d_acc, c->d_grid, c->d_filter, c->d_twiddle64,
-                    c->d_twiddle32, c->d_err};
+                    c->d_xmod, c->d_pos_aos, c->d_force_aos, c->d_acc, c->d_grid, c->d_spec, c->d_filter, c->d_twiddle64,
+                    c->d_twiddle32, c->d_err, c->d_mstart, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_chunk};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i < 8; i++)
@@ -278,8 +278,16 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
         }
         CK(upload(&d.kmask, mask.data(), G));
         CK(cudaMalloc(&c->d_filter, G * (sizeof(double) + sizeof(float))));
-        const size_t csz = precision == PINYB200_FP64 ? sizeof(double2) : sizeof(float2);
-        CK(cudaMalloc(&c->d_grid, csz * G * nbeads));
+        const bool f64 = precision == PINYB200_FP64;
+        if (pme_plane_smem(Na, Nb, f64) > 220 * 1024 || pme_slab_smem(Na, Nc, f64) > 220 * 1024) {
+            int rc2 = fail(nullptr, PINYB200_ERR_UNSUPPORTED, "PME grid plane too large for shared memory");
+            pinyb200_destroy(c);
+            return rc2;
+        }
+        const size_t rsz = f64 ? sizeof(double) : sizeof(float);
+        const size_t csz = f64 ? sizeof(double2) : sizeof(float2);
+        CK(cudaMalloc(&c->d_grid, rsz * G * nbeads));
+        CK(cudaMalloc(&c->d_spec, csz * (size_t)Nc * Nb * (Na / 2 + 1) * nbeads));
         // twiddles exp(2 pi i m / N) per axis, 256 entries each
         std::vector<double> tw(2 * 256 * 3, 0.0);
         std::vector<float> tw32(tw.size());
@@ -352,7 +360,48 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
     CK(cudaMalloc(&c->d_row, (size_t)(natm + 1) * sizeof(int)));
     CK(cudaMalloc(&c->d_rowA, (size_t)(natm + 1) * sizeof(int)));
     CK(cudaMalloc(&c->d_count, (size_t)2 * natm * sizeof(int)));
-    CK(cudaMalloc(&c->d_tot, 2 * sizeof(long long)));
+    CK(cudaMalloc(&c->d_tot, 4 * sizeof(long long)));
+    // molecules: connected components of the exclusion graph, each a run of
+    // at most 4 consecutive sites (water); otherwise the site kernel is used
+    {
+        std::vector<int> root(natm);
+        for (int i = 0; i < natm; i++) root[i] = i;
+        auto find = [&](int x) {
+            while (root[x] != x) x = root[x] = root[root[x]];
+            return x;
+        };
+        for (int i = 0; i < natm; i++)
+            for (int e = s->excl_off[i]; e < s->excl_off[i + 1]; e++) {
+                int a = find(i), b = find(s->excl_j[e]);
+                if (a != b) root[a < b ? b : a] = a < b ? a : b;
+            }
+        std::vector<int> mstart;
+        bool ok = true;
+        int maxn = 0;
+        for (int i = 0; i < natm; i++) {
+            if (i == 0 || find(i) != find(i - 1)) {
+                if (find(i) != i) ok = false;  // not a new contiguous component
+                mstart.push_back(i);
+            }
+        }
+        mstart.push_back(natm);
+        for (size_t m = 0; m + 1 < mstart.size(); m++) maxn = std::max(maxn, mstart[m + 1] - mstart[m]);
+        // the molecule kernel also needs identical molecules (sizes, types, charges)
+        for (size_t m = 1; ok && m + 1 < mstart.size(); m++) {
+            const int n0 = mstart[1] - mstart[0], nm = mstart[m + 1] - mstart[m];
+            if (nm != n0) ok = false;
+            for (int k = 0; ok && k < nm; k++)
+                if (s->atm_typ[mstart[m] + k] != s->atm_typ[k] || s->charge[mstart[m] + k] != s->charge[k]) ok = false;
+        }
+        if (ok && maxn <= 4 && s->ntyp <= 8) {
+            c->use_mol = true;
+            c->nmol = (int)mstart.size() - 1;
+            c->mol_ns = maxn <= 3 ? 3 : 4;
+            CK(upload(&c->d_mstart, mstart.data(), mstart.size()));
+            CK(cudaMalloc(&c->d_mcount, (size_t)c->nmol * sizeof(int)));
+            CK(cudaMalloc(&c->d_mrow, (size_t)(c->nmol + 1) * sizeof(int)));
+        }
+    }
     CK(cudaMalloc(&c->d_err, sizeof(int)));
     CK(cudaMemset(c->d_err, 0, sizeof(int)));
     *out = c;
@@ -396,9 +445,50 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
     }
     CK(launch_build_list(c, cell, d_p1, d_xm, d_cs, 1));
     CK(cudaStreamSynchronize(c->stream));
-    cudaFree(d_cs);
     c->npairs = tot[0];
     c->nactive = tot[1];
+    c->mol_ok = false;
+    if (c->use_mol) {
+        CK(cudaMemsetAsync(c->d_tot + 2, 0, 2 * sizeof(long long), c->stream));
+        CK(launch_mol_list(c, cell, d_p1, d_xm, d_cs, 0));
+        long long mt[2];
+        CK(cudaMemcpyAsync(mt, c->d_tot + 2, sizeof(mt), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (mt[0] > c->mlist_cap) {
+            if (c->d_mj) cudaFree(c->d_mj);
+            if (c->d_mmask) cudaFree(c->d_mmask);
+            c->d_mj = nullptr;
+            c->d_mmask = nullptr;
+            long long cap = mt[0] + mt[0] / 8 + 1024;
+            CK(cudaMalloc(&c->d_mj, cap * sizeof(int)));
+            CK(cudaMalloc(&c->d_mmask, cap * sizeof(unsigned)));
+            c->mlist_cap = cap;
+        }
+        CK(launch_mol_list(c, cell, d_p1, d_xm, d_cs, 1));
+        CK(cudaMemcpyAsync(mt, c->d_tot + 2, sizeof(mt), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->nmp = mt[0];
+        // the molecule masks must hold exactly the active site pairs
+        if (mt[1] == c->nactive) {
+            std::vector<int> mrow(c->nmol + 1);
+            CK(cudaMemcpy(mrow.data(), c->d_mrow, mrow.size() * sizeof(int), cudaMemcpyDeviceToHost));
+            const int jpi = c->P >= 32 ? 1 : 32 / c->P;
+            const int ch = 8 * jpi;
+            std::vector<int> chunks;
+            for (int m = 0; m < c->nmol; m++)
+                for (int k = mrow[m]; k < mrow[m + 1]; k += ch) {
+                    chunks.push_back(m);
+                    chunks.push_back(k);
+                    chunks.push_back(std::min(k + ch, mrow[m + 1]));
+                }
+            if (c->d_chunk) cudaFree(c->d_chunk);
+            c->d_chunk = nullptr;
+            c->nchunk = (int)(chunks.size() / 3);
+            CK(upload(&c->d_chunk, chunks.data(), chunks.size()));
+            c->mol_ok = true;
+        }
+    }
+    cudaFree(d_cs);
     c->have_list = true;
     if (npairs) *npairs = (long)tot[0];
     return PINYB200_OK;
@@ -430,7 +520,10 @@ static int evaluate(pinyb200_ctx *c, const Cell &cell, int flags, pinyb200_energ
     CK(cudaMemsetAsync(c->d_forceT, 0, nb * sizeof(double), c->stream));
     CK(cudaMemsetAsync(c->d_acc, 0, (size_t)c->P * S_NSLOT * sizeof(double), c->stream));
     CK(cudaEventRecord(c->ev[1], c->stream));
-    CK(launch_pair(c, cell, energy));
+    const bool ortho = cell.h[1] == 0.0 && cell.h[2] == 0.0 && cell.h[3] == 0.0 && cell.h[5] == 0.0 &&
+                       cell.h[6] == 0.0 && cell.h[7] == 0.0;
+    if (c->use_mol && c->mol_ok && ortho && !(flags & PINYB200_SITE_PAIRS)) CK(launch_mol_pair(c, cell, energy));
+    else CK(launch_pair(c, cell, energy));
     CK(cudaEventRecord(c->ev[2], c->stream));
     CK(launch_pme(c, cell, energy));
     CK(cudaEventRecord(c->ev[3], c->stream));

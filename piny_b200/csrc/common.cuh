@@ -95,6 +95,41 @@ __device__ __forceinline__ double4 ldg4(const double4 *p)
     return make_double4(a.x, a.y, b.x, b.y);
 }
 
+template <typename R> struct Idx;
+
+// Spline knot and offset.  FP64 keeps PINY's rounding exactly (no FMA), FP32
+// uses plain arithmetic.
+template <> struct Idx<double> {
+    static __device__ __forceinline__ int knot(double r, double rmin, double dr, double dri, int nsm2, double &del)
+    {
+        int k = __double2int_rz(__dadd_rn(__dmul_rn(__dsub_rn(r, rmin), dri), 0.5)) + 3;
+        k = k < nsm2 ? k : nsm2;
+        k = k > 3 ? k : 3;
+        double rsp = __dadd_rn(__dmul_rn((double)(k - 3), dr), rmin);
+        del = __dmul_rn(__dsub_rn(r, rsp), dri);
+        return k;
+    }
+    static __device__ __forceinline__ double dist(double dx, double dy, double dz)
+    {
+        return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+    }
+};
+template <> struct Idx<float> {
+    static __device__ __forceinline__ int knot(float r, float rmin, float dr, float dri, int nsm2, float &del)
+    {
+        int k = (int)((r - rmin) * dri + 0.5f) + 3;
+        k = k < nsm2 ? k : nsm2;
+        k = k > 3 ? k : 3;
+        float rsp = (float)(k - 3) * dr + rmin;
+        del = (r - rsp) * dri;
+        return k;
+    }
+    static __device__ __forceinline__ float dist(float dx, float dy, float dz)
+    {
+        return sqrtf(dx * dx + dy * dy + dz * dz);
+    }
+};
+
 // Warp sum of a double over the lanes that share (lane mod stride).
 __device__ __forceinline__ double warp_sum_strided(double v, int stride)
 {

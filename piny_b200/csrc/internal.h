@@ -89,8 +89,20 @@ struct pinyb200_ctx {
     int *d_row = nullptr, *d_col = nullptr;        // full
     int *d_rowA = nullptr, *d_colA = nullptr;      // active
     int *d_count = nullptr;                        // [2*natm] scratch
-    long long *d_tot = nullptr;                    // device totals
+    long long *d_tot = nullptr;                    // device totals [4]
     bool have_list = false;
+    // molecule-pair list (sites grouped into molecules of <= 4 consecutive sites)
+    bool use_mol = false;      // the system splits into such molecules
+    bool mol_ok = false;       // the current molecule list matches the site list
+    int nmol = 0, mol_ns = 0;
+    int *d_mstart = nullptr;   // [nmol+1]
+    int *d_mcount = nullptr;   // [nmol]
+    int *d_mrow = nullptr;     // [nmol+1]
+    int *d_mj = nullptr;       // [nmp]
+    unsigned *d_mmask = nullptr;
+    long long mlist_cap = 0, nmp = 0;
+    int nchunk = 0;
+    int *d_chunk = nullptr;    // [nchunk][3]
     // work buffers
     double *d_posT = nullptr;     // [natm][3][P]
     double *d_forceT = nullptr;   // [natm][3][P]
@@ -98,7 +110,8 @@ struct pinyb200_ctx {
     double *d_pos_aos = nullptr;  // [P][natm][3] staging for host calls
     double *d_force_aos = nullptr;
     double *d_acc = nullptr;      // [P][S_NSLOT]
-    void *d_grid = nullptr;       // [P][G] complex (float2 or double2)
+    void *d_grid = nullptr;       // [P][Nc][Nb][Na] real charge / potential grid
+    void *d_spec = nullptr;       // [P][Nc][Nb][Na/2+1] complex half spectrum
     void *d_filter = nullptr;     // [G] real: preg * bweight, 0 outside the sphere
     double *d_twiddle64 = nullptr;  // per axis twiddles
     float *d_twiddle32 = nullptr;
@@ -116,11 +129,16 @@ namespace pinyb200 {
 cudaError_t launch_build_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1,
                               const double *d_xm, const double *d_cutskin2, int pass);
 cudaError_t launch_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
+cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
+                            const double *d_cutskin2, int pass);
+cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_pme(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_intra(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_ghost_pos(pinyb200_ctx *c);
 cudaError_t launch_ghost_distrib(pinyb200_ctx *c);
 cudaError_t launch_transpose_in(pinyb200_ctx *c, const double *d_pos_aos);
 cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_force_aos);
+size_t pme_plane_smem(int Na, int Nb, bool fp64);
+size_t pme_slab_smem(int Na, int Nc, bool fp64);
 
 }  // namespace pinyb200

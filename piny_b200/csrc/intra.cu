@@ -13,15 +13,20 @@
 
 namespace pinyb200 {
 
-__device__ __forceinline__ void acc_bead(double *acc, int P, int b, int slot, double v)
+// Block-level reduction of per-thread energy/virial sums by bead: shared
+// FP64 atomics (S_NSLOT slots per bead), then one global atomic per (bead,
+// slot) per block.  Every thread of the block must call it.
+template <int NV>
+__device__ __forceinline__ void block_acc(double *acc, int P, int b, const int *slot, const double *v, double *sh)
 {
-    const int lane = threadIdx.x & 31;
-    if (P < 32) {
-        v = warp_sum_strided(v, P);
-        if (lane < P) atomicAdd(&acc[(size_t)b * S_NSLOT + slot], v);
-    } else {
-        atomicAdd(&acc[(size_t)b * S_NSLOT + slot], v);
-    }
+    for (int i = threadIdx.x; i < P * NV; i += blockDim.x) sh[i] = 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < NV; c++)
+        if (v[c] != 0.0) atomicAdd(&sh[b * NV + c], v[c]);
+    __syncthreads();
+    for (int i = threadIdx.x; i < P * NV; i += blockDim.x)
+        if (sh[i] != 0.0) atomicAdd(&acc[(size_t)(i / NV) * S_NSLOT + slot[i % NV]], sh[i]);
 }
 
 __global__ void transpose_in_kernel(const double *__restrict__ aos, double *__restrict__ posT, int natm, int P)
@@ -114,11 +119,12 @@ __global__ void __launch_bounds__(256) bond_kernel(IntraArgs a, int nbond, const
                                                    const double *__restrict__ eq, const double *__restrict__ cc,
                                                    const double *__restrict__ dc)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = t < (long long)nbond * a.P;
-    const int b = (int)(t % a.P);
+    __shared__ double sh[64 * 7];
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;  // a multiple of P
+    const int b = (int)(t0 % a.P);
     double v = 0, p[6] = {0, 0, 0, 0, 0, 0};
-    if (valid) {
+    for (long long t = t0; t < (long long)nbond * a.P; t += stride) {
         const int ib = (int)(t / a.P);
         const int j1 = bj[3 * ib], j2 = bj[3 * ib + 1], ty = bj[3 * ib + 2];
         double x1, y1, z1, x2, y2, z2;
@@ -128,17 +134,18 @@ __global__ void __launch_bounds__(256) bond_kernel(IntraArgs a, int nbond, const
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
         const double rr0 = r - eq[ty];
         const double *c = cc + 7 * ty, *d = dc + 7 * ty;
-        v = (((((c[6] * rr0 + c[5]) * rr0 + c[4]) * rr0 + c[3]) * rr0 + c[2]) * rr0 + c[1]) * rr0 + c[0];
+        v += (((((c[6] * rr0 + c[5]) * rr0 + c[4]) * rr0 + c[3]) * rr0 + c[2]) * rr0 + c[1]) * rr0 + c[0];
         const double dv = ((((d[6] * rr0 + d[5]) * rr0 + d[4]) * rr0 + d[3]) * rr0 + d[2]) * rr0 + d[1];
         const double pre = -dv / r;
         const double fx = dx * pre, fy = dy * pre, fz = dz * pre;
         add_f(a.forceT, a.P, j1, b, fx, fy, fz);
         add_f(a.forceT, a.P, j2, b, -fx, -fy, -fz);
-        p[0] = dx * fx; p[1] = dy * fy; p[2] = dz * fz; p[3] = dx * fy; p[4] = dx * fz; p[5] = dy * fz;
+        p[0] += dx * fx; p[1] += dy * fy; p[2] += dz * fz; p[3] += dx * fy; p[4] += dx * fz; p[5] += dy * fz;
     }
     if (a.energy) {
-        acc_bead(a.acc, a.P, b, S_VBOND, v);
-        for (int c = 0; c < 6; c++) acc_bead(a.acc, a.P, b, S_PXX + c, p[c]);
+        const int slot[7] = {S_VBOND, S_PXX, S_PYY, S_PZZ, S_PXY, S_PXZ, S_PYZ};
+        const double vals[7] = {v, p[0], p[1], p[2], p[3], p[4], p[5]};
+        block_acc<7>(a.acc, a.P, b, slot, vals, sh);
     }
 }
 
@@ -146,11 +153,12 @@ __global__ void __launch_bounds__(256) bend_kernel(IntraArgs a, int nbend, const
                                                    const double *__restrict__ bc, const double *__restrict__ bs,
                                                    const double *__restrict__ bdc, const double *__restrict__ bds)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = t < (long long)nbend * a.P;
-    const int b = (int)(t % a.P);
+    __shared__ double sh[64 * 7];
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;  // a multiple of P
+    const int b = (int)(t0 % a.P);
     double v = 0, p[6] = {0, 0, 0, 0, 0, 0};
-    if (valid) {
+    for (long long t = t0; t < (long long)nbend * a.P; t += stride) {
         const int ib = (int)(t / a.P);
         const int a1 = bj[4 * ib], a2 = bj[4 * ib + 1], a3 = bj[4 * ib + 2], ty = bj[4 * ib + 3];
         double x1, y1, z1, x2, y2, z2, x3, y3, z3;
@@ -174,7 +182,7 @@ __global__ void __launch_bounds__(256) bend_kernel(IntraArgs a, int nbend, const
         const double vc = ((((((c[6] * cost + c[5]) * cost + c[4]) * cost + c[3]) * cost + c[2]) * cost + c[1]) * cost +
                            c[0]);
         const double sisum = (((((s[6] * sint + s[5]) * sint + s[4]) * sint + s[3]) * sint + s[2]) * sint);
-        v = vc + (sisum * cost + s[1] * sint);
+        v += vc + (sisum * cost + s[1] * sint);
         const double dvc = (((((dc[6] * cost + dc[5]) * cost + dc[4]) * cost + dc[3]) * cost + dc[2]) * cost + dc[1]);
         double dvs = ((((ds[6] * sint + ds[5]) * sint + ds[4]) * sint + ds[3]) * sint + ds[2]);
         dvs = dvs * cost + ds[1];
@@ -186,16 +194,17 @@ __global__ void __launch_bounds__(256) bend_kernel(IntraArgs a, int nbend, const
         add_f(a.forceT, a.P, a1, b, fx1, fy1, fz1);
         add_f(a.forceT, a.P, a2, b, -(fx1 + fx3), -(fy1 + fy3), -(fz1 + fz3));
         add_f(a.forceT, a.P, a3, b, fx3, fy3, fz3);
-        p[0] = dx12 * fx1 + dx23 * fx3;
-        p[1] = dy12 * fy1 + dy23 * fy3;
-        p[2] = dz12 * fz1 + dz23 * fz3;
-        p[3] = dx12 * fy1 + dx23 * fy3;
-        p[4] = dx12 * fz1 + dx23 * fz3;
-        p[5] = dy12 * fz1 + dy23 * fz3;
+        p[0] += dx12 * fx1 + dx23 * fx3;
+        p[1] += dy12 * fy1 + dy23 * fy3;
+        p[2] += dz12 * fz1 + dz23 * fz3;
+        p[3] += dx12 * fy1 + dx23 * fy3;
+        p[4] += dx12 * fz1 + dx23 * fz3;
+        p[5] += dy12 * fz1 + dy23 * fz3;
     }
     if (a.energy) {
-        acc_bead(a.acc, a.P, b, S_VBEND, v);
-        for (int c = 0; c < 6; c++) acc_bead(a.acc, a.P, b, S_PXX + c, p[c]);
+        const int slot[7] = {S_VBEND, S_PXX, S_PYY, S_PZZ, S_PXY, S_PXZ, S_PYZ};
+        const double vals[7] = {v, p[0], p[1], p[2], p[3], p[4], p[5]};
+        block_acc<7>(a.acc, a.P, b, slot, vals, sh);
     }
 }
 
@@ -203,11 +212,12 @@ __global__ void __launch_bounds__(256) ecor_kernel(IntraArgs a, int necor, const
                                                    const int *__restrict__ j2s, int nsplin, double rmin, double dr,
                                                    double dri, const double4 *__restrict__ tab)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = t < (long long)necor * a.P;
-    const int b = (int)(t % a.P);
+    __shared__ double sh[64 * 7];
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;  // a multiple of P
+    const int b = (int)(t0 % a.P);
     double v = 0, p[6] = {0, 0, 0, 0, 0, 0};
-    if (valid) {
+    for (long long t = t0; t < (long long)necor * a.P; t += stride) {
         const int ie = (int)(t / a.P);
         const int j1 = j1s[ie], j2 = j2s[ie];
         double x1, y1, z1, x2, y2, z2;
@@ -221,20 +231,28 @@ __global__ void __launch_bounds__(256) ecor_kernel(IntraArgs a, int necor, const
         const double rsp = __dadd_rn(__dmul_rn((double)(k - 3), dr), rmin);
         const double del = __dmul_rn(__dsub_rn(r, rsp), dri);
         const double q12 = a.charge[j1] * a.charge[j2];
-        v = spline_eval<double4, double>(tab[k - 1], del) * q12;
+        v += spline_eval<double4, double>(tab[k - 1], del) * q12;
         const double dvt = spline_eval<double4, double>(tab[nsplin + k - 1], del) * q12;
         const double fx = dx * dvt, fy = dy * dvt, fz = dz * dvt;
         add_f(a.forceT, a.P, j1, b, fx, fy, fz);
         add_f(a.forceT, a.P, j2, b, -fx, -fy, -fz);
-        p[0] = dx * fx; p[1] = dy * fy; p[2] = dz * fz; p[3] = dx * fy; p[4] = dx * fz; p[5] = dy * fz;
+        p[0] += dx * fx; p[1] += dy * fy; p[2] += dz * fz; p[3] += dx * fy; p[4] += dx * fz; p[5] += dy * fz;
     }
     if (a.energy) {
-        acc_bead(a.acc, a.P, b, S_VECOR, v);
-        for (int c = 0; c < 6; c++) acc_bead(a.acc, a.P, b, S_PXX + c, p[c]);
+        const int slot[7] = {S_VECOR, S_PXX, S_PYY, S_PZZ, S_PXY, S_PXZ, S_PYZ};
+        const double vals[7] = {v, p[0], p[1], p[2], p[3], p[4], p[5]};
+        block_acc<7>(a.acc, a.P, b, slot, vals, sh);
     }
 }
 
 static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// grid-stride launch size for the intramolecular kernels
+static inline unsigned nblk_gs(pinyb200_ctx *c, long long n)
+{
+    long long b = (n + 255) / 256, cap = (long long)c->sm_count * 4;
+    return (unsigned)(b < cap ? (b > 0 ? b : 1) : cap);
+}
 
 cudaError_t launch_transpose_in(pinyb200_ctx *c, const double *d_aos)
 {
@@ -281,13 +299,13 @@ cudaError_t launch_intra(pinyb200_ctx *c, const Cell &cell, bool energy)
     a.charge = s.charge;
     a.energy = energy ? 1 : 0;
     if (s.nbond)
-        bond_kernel<<<nblk((long long)s.nbond * c->P, 256), 256, 0, c->stream>>>(a, s.nbond, s.bond_j, s.bond_eq,
+        bond_kernel<<<nblk_gs(c, (long long)s.nbond * c->P), 256, 0, c->stream>>>(a, s.nbond, s.bond_j, s.bond_eq,
                                                                                   s.bond_c, s.bond_dc);
     if (s.nbend)
-        bend_kernel<<<nblk((long long)s.nbend * c->P, 256), 256, 0, c->stream>>>(a, s.nbend, s.bend_j, s.bend_c,
+        bend_kernel<<<nblk_gs(c, (long long)s.nbend * c->P), 256, 0, c->stream>>>(a, s.nbend, s.bend_j, s.bend_c,
                                                                                   s.bend_s, s.bend_dc, s.bend_ds);
     if (s.necor)
-        ecor_kernel<<<nblk((long long)s.necor * c->P, 256), 256, 0, c->stream>>>(
+        ecor_kernel<<<nblk_gs(c, (long long)s.necor * c->P), 256, 0, c->stream>>>(
             a, s.necor, s.ecor_j1, s.ecor_j2, s.ecor_nsplin, s.ecor_rmin, s.ecor_dr, s.ecor_dri, s.ecor_tab);
     return cudaGetLastError();
 }

@@ -1,0 +1,491 @@
+// Molecule-pair form of the real-space kernel.
+//
+// The site Verlet list of PINY (verlist_create.c) is regrouped by molecule:
+// one entry per molecule pair (mi > mj) with a bit mask of the site pairs
+// (si, sj) that PINY's list holds and that carry a force (a charge product
+// or a vdW table).  The mask is computed with the same FP64 criterion as the
+// site list (r^2 < cutskin^2 on the bead-1 minimum image, exclusions), so
+// the molecule list and the site list contain exactly the same site pairs.
+//
+// Per site pair and bead the arithmetic is force_npol's (force_npol.c:
+// 28-329, see pair.cu).  What the grouping buys on B200:
+//   * one list index and one set of j positions per molecule pair;
+//   * j-site reactions summed in registers over the molecule pair, one FP64
+//     red.add per j site that received a force;
+//   * rows cut into chunks of a few molecule pairs, so warps get even work;
+//   * MIXED: the pair separation is d0 + e_i - e_j, with d0 the site-0
+//     separation formed in FP64 and e the FP32 site offsets inside each
+//     molecule; the per-site-pair image shift of period_pimd (period.c:121)
+//     is evaluated from the mode-1 separations the same way.
+//   * FP64: every site-pair separation and image shift in FP64 with PINY's
+//     operation order, as in the site kernel.
+#include "common.cuh"
+
+namespace pinyb200 {
+
+// ---------------------------------------------------------------------------
+// molecule-pair list build (count / fill), FP64 criterion of the site list
+template <int FILL, int NS>
+__global__ void __launch_bounds__(256) mol_list_kernel(int nmol, const int *__restrict__ mstart, int ntyp,
+                                                       const double *__restrict__ pos1, const double *__restrict__ xm,
+                                                       int use_xm, Cell cell, const double *__restrict__ cutskin2,
+                                                       const int *__restrict__ atm_typ,
+                                                       const double *__restrict__ charge,
+                                                       const int *__restrict__ inter_map,
+                                                       const int *__restrict__ has_vdw, int *__restrict__ count,
+                                                       const int *__restrict__ row, int *__restrict__ mj_out,
+                                                       unsigned *__restrict__ mask_out, long long cap,
+                                                       unsigned long long *__restrict__ nsite)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long sites = 0;
+    for (int mi = warp; mi < nmol; mi += nwarps) {
+        const int i0 = mstart[mi], ni = mstart[mi + 1] - i0;
+        int n = 0;
+        const long long w0 = FILL ? row[mi] : 0;
+        for (int m0 = 0; m0 < mi; m0 += 32) {
+            const int mj = m0 + lane;
+            unsigned mask = 0;
+            if (mj < mi) {
+                const int j0 = mstart[mj], nj = mstart[mj + 1] - j0;
+                for (int si = 0; si < ni; si++) {
+                    const int i = i0 + si;
+                    const double xi = pos1[3 * i], yi = pos1[3 * i + 1], zi = pos1[3 * i + 2];
+                    const int ti = atm_typ[i];
+                    const double qi = charge[i];
+                    for (int sj = 0; sj < nj; sj++) {
+                        const int j = j0 + sj;
+                        double dx = __dsub_rn(xi, pos1[3 * j]);
+                        double dy = __dsub_rn(yi, pos1[3 * j + 1]);
+                        double dz = __dsub_rn(zi, pos1[3 * j + 2]);
+                        if (use_xm)
+                            period_pimd_exact(dx, dy, dz, __dsub_rn(xm[3 * i], xm[3 * j]),
+                                              __dsub_rn(xm[3 * i + 1], xm[3 * j + 1]),
+                                              __dsub_rn(xm[3 * i + 2], xm[3 * j + 2]), cell);
+                        else
+                            period_exact(dx, dy, dz, cell);
+                        const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+                        const int pt = pair_type(ti, atm_typ[j], ntyp);
+                        if (r2 < cutskin2[pt] && (has_vdw[inter_map[pt]] || qi * charge[j] != 0.0))
+                            mask |= 1u << (si * NS + sj);
+                    }
+                }
+            }
+            const bool keep = mask != 0;
+            const unsigned bk = __ballot_sync(0xffffffffu, keep);
+            if (FILL && keep) {
+                const long long p = w0 + n + __popc(bk & ((1u << lane) - 1u));
+                if (p < cap) {
+                    mj_out[p] = mj;
+                    mask_out[p] = mask;
+                }
+            }
+            if (FILL) sites += __popc(mask);
+            n += __popc(bk);
+        }
+        if (!FILL && lane == 0) count[mi] = n;
+    }
+    if (FILL) {
+        for (int o = 16; o >= 1; o >>= 1) sites += __shfl_xor_sync(0xffffffffu, sites, o);
+        if (lane == 0) atomicAdd(nsite, sites);
+    }
+}
+
+__global__ void __launch_bounds__(1024) mol_scan_kernel(int n, const int *__restrict__ count, int *__restrict__ row,
+                                                         long long *__restrict__ tot)
+{
+    __shared__ long long part[1024];
+    const int t = threadIdx.x;
+    const int chunk = (n + blockDim.x - 1) / blockDim.x;
+    const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
+    long long s0 = 0;
+    for (int i = lo; i < hi; i++) s0 += count[i];
+    part[t] = s0;
+    __syncthreads();
+    for (int o = 1; o < blockDim.x; o <<= 1) {
+        long long a0 = t >= o ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += a0;
+        __syncthreads();
+    }
+    long long b0 = part[t] - s0;
+    for (int i = lo; i < hi; i++) {
+        row[i] = (int)b0;
+        b0 += count[i];
+    }
+    if (t == blockDim.x - 1) {
+        row[n] = (int)part[t];
+        *tot = part[t];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// force kernel
+
+struct MolArgs {
+    int nchunk;
+    const int *chunk;  // [nchunk][3]: mi, begin, end
+    const int *mj;
+    const unsigned *mask;
+    const int *mstart;
+    int ntyp, npt, nuniq, nsplin;
+    const double *posT, *xmod;  // xmod: [natm][3] (bead positions when P == 1)
+    int pimd;
+    const int *atm_typ;
+    const double *charge;
+    const int *inter_map;
+    const double *cutoff, *rmin, *dr, *dri;
+    const int *has_vdw;
+    const void *tab;
+    double *forceT;
+    double *acc;
+    int energy;
+};
+
+// Site-pair constants of the (uniform) molecule: pair type, table row and
+// charge product of site si of molecule i with site sj of molecule j.
+template <typename R>
+struct PairConst {
+    R rc[16], rmin[16], dr[16], dri[16], q2[16];
+    int off[16];  // table row offset u * nsplin
+    int vdw[16];
+};
+
+// Exact PINY image shift -NINT(h^-1 dmode) of one site pair along the
+// diagonal of an orthorhombic cell (period_pimd, period.c:163-176).
+__device__ __forceinline__ double shift_exact(double dm, double hi) { return -nint_rn(__dmul_rn(dm, hi)); }
+
+// Sites of a molecule sit within this distance (Bohr) of its site 0 in the
+// mode-1 coordinates; a site pair can take a different image than the
+// site-0 pair only when the site-0 separation is within twice this of half
+// a box, and only then is its own shift evaluated.
+#define PINYB200_MOL_EXTENT 5.0
+
+// Resident blocks of 128 threads per SM the register allocation aims at.
+#ifndef PINYB200_MOL_BLOCKS32
+#define PINYB200_MOL_BLOCKS32 4
+#endif
+#ifndef PINYB200_MOL_BLOCKS64
+#define PINYB200_MOL_BLOCKS64 3
+#endif
+
+template <typename R, int P, int NS, bool FAST, bool ENERGY>
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : PINYB200_MOL_BLOCKS64)
+    mol_pair_kernel(MolArgs a, Cell cell)
+{
+    typedef typename Vec4<R>::T V;
+    constexpr int G = P >= 32 ? 32 : P;  // lanes per molecule pair
+    constexpr int JPI = 32 / G;          // molecule pairs per warp step
+    __shared__ PairConst<R> pc;
+    if (threadIdx.x < NS * NS) {
+        // every molecule has the sites of molecule 0 (checked on the host)
+        const int si = threadIdx.x / NS, sj = threadIdx.x % NS;
+        const int nm0 = a.mstart[1];
+        const int ia = si < nm0 ? si : 0, ja = sj < nm0 ? sj : 0;
+        const int p = pair_type(a.atm_typ[ia], a.atm_typ[ja], a.ntyp);
+        const int u = a.inter_map[p];
+        pc.rc[threadIdx.x] = (R)a.cutoff[p];
+        pc.off[threadIdx.x] = u * a.nsplin;
+        pc.vdw[threadIdx.x] = a.has_vdw[u];
+        pc.rmin[threadIdx.x] = (R)a.rmin[u];
+        pc.dr[threadIdx.x] = (R)a.dr[u];
+        pc.dri[threadIdx.x] = (R)a.dri[u];
+        pc.q2[threadIdx.x] = (R)(a.charge[ia] * a.charge[ja]);
+    }
+    __syncthreads();
+    const V *__restrict__ tab = (const V *)a.tab;
+    const size_t tstride = (size_t)a.nuniq * a.nsplin;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int sub = lane / G;
+    const int b = (lane % G) + 32 * blockIdx.y;  // bead
+    const int nsm2 = a.nsplin - 2;
+    const double *__restrict__ posT = a.posT;
+    const double hd[3] = {cell.h[0], cell.h[4], cell.h[8]};
+    const double hid[3] = {cell.hi[0], cell.hi[4], cell.hi[8]};
+    double half_lim[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) half_lim[d] = 0.5 - 2.0 * PINYB200_MOL_EXTENT * hid[d];
+
+    double ev = 0.0, ec = 0.0, pv[6] = {0, 0, 0, 0, 0, 0};
+
+    for (int ch = warp; ch < a.nchunk; ch += nwarps) {
+        const int mi = a.chunk[3 * ch], beg = a.chunk[3 * ch + 1], end = a.chunk[3 * ch + 2];
+        const int i0 = a.mstart[mi], ni = a.mstart[mi + 1] - i0;
+        double xi[NS][3];  // FP64 mode: all sites; MIXED: site 0 only is kept in FP64
+        R ei[NS][3];
+        R fi[NS][3];
+        double xmi0[3];
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            const int i = i0 + (s < ni ? s : 0);
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                xi[s][d] = posT[(3 * (size_t)i + d) * P + b];
+                fi[s][d] = (R)0;
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; d++) xmi0[d] = a.xmod[3 * (size_t)i0 + d];
+#pragma unroll
+        for (int s = 0; s < NS; s++)
+#pragma unroll
+            for (int d = 0; d < 3; d++) ei[s][d] = (R)(xi[s][d] - xi[0][d]);
+        R evs = 0, ecs = 0, pvs[6] = {0, 0, 0, 0, 0, 0};
+        for (int k = beg + sub; k < end; k += JPI) {
+            const int mj = a.mj[k];
+            const unsigned mask = a.mask[k];
+            const int j0 = a.mstart[mj];
+            unsigned jm = 1u;
+#pragma unroll
+            for (int si = 0; si < NS; si++) jm |= (mask >> (si * NS)) & ((1u << NS) - 1u);
+            double xj[NS][3];
+#pragma unroll
+            for (int s = 0; s < NS; s++) {
+                const int j = j0 + (((jm >> s) & 1u) ? s : 0);
+#pragma unroll
+                for (int d = 0; d < 3; d++) xj[s][d] = posT[(3 * (size_t)j + d) * P + b];
+            }
+            // site-0 image (mode-1 separation, FP64) and whether the pair is
+            // close enough to half a box for site pairs to differ from it
+            double sh0[3];
+            bool near = false;
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const double dm = __dsub_rn(xmi0[d], a.xmod[3 * (size_t)j0 + d]);
+                const double t = __dmul_rn(dm, hid[d]);
+                sh0[d] = -nint_rn(t);
+                near |= fabs(t + sh0[d]) > half_lim[d];
+            }
+            R d0[3], ej[NS][3];
+            if (FAST) {
+#pragma unroll
+                for (int d = 0; d < 3; d++) d0[d] = (R)(__dsub_rn(xi[0][d], xj[0][d]) + sh0[d] * hd[d]);
+#pragma unroll
+                for (int s = 0; s < NS; s++)
+#pragma unroll
+                    for (int d = 0; d < 3; d++) ej[s][d] = (R)(xj[s][d] - xj[0][d]);
+            }
+            // One loop body for every site pair; per-site values are picked
+            // out of register arrays by predicated static-index loops, so the
+            // arrays stay in registers and the code stays small.
+#pragma unroll 1
+            for (int sj = 0; sj < NS; sj++) {
+                unsigned col = 0;
+#pragma unroll
+                for (int si = 0; si < NS; si++) col |= ((mask >> (si * NS + sj)) & 1u) << si;
+                if (!col) continue;
+                R ejx = 0, ejy = 0, ejz = 0;
+                double xjx = 0, xjy = 0, xjz = 0;
+#pragma unroll
+                for (int s2 = 0; s2 < NS; s2++)
+                    if (sj == s2) {
+                        if (FAST) { ejx = ej[s2][0]; ejy = ej[s2][1]; ejz = ej[s2][2]; }
+                        else { xjx = xj[s2][0]; xjy = xj[s2][1]; xjz = xj[s2][2]; }
+                    }
+                R fjx = 0, fjy = 0, fjz = 0;
+                while (col) {
+                    const int si = __ffs(col) - 1;
+                    col &= col - 1u;
+                    const int sp = si * NS + sj;
+                    double sh[3] = {sh0[0], sh0[1], sh0[2]};
+                    if (near) {
+#pragma unroll
+                        for (int d = 0; d < 3; d++)
+                            sh[d] = shift_exact(__dsub_rn(a.xmod[3 * (size_t)(i0 + si) + d],
+                                                          a.xmod[3 * (size_t)(j0 + sj) + d]), hid[d]);
+                    }
+                    R rx, ry, rz;
+                    if (FAST) {
+                        R eix = 0, eiy = 0, eiz = 0;
+#pragma unroll
+                        for (int s2 = 0; s2 < NS; s2++)
+                            if (si == s2) { eix = ei[s2][0]; eiy = ei[s2][1]; eiz = ei[s2][2]; }
+                        rx = d0[0] + (eix - ejx);
+                        ry = d0[1] + (eiy - ejy);
+                        rz = d0[2] + (eiz - ejz);
+                        if (near) {
+                            rx += (R)((sh[0] - sh0[0]) * hd[0]);
+                            ry += (R)((sh[1] - sh0[1]) * hd[1]);
+                            rz += (R)((sh[2] - sh0[2]) * hd[2]);
+                        }
+                    } else {
+                        double xix = 0, xiy = 0, xiz = 0;
+#pragma unroll
+                        for (int s2 = 0; s2 < NS; s2++)
+                            if (si == s2) { xix = xi[s2][0]; xiy = xi[s2][1]; xiz = xi[s2][2]; }
+                        rx = (R)__dadd_rn(__dsub_rn(xix, xjx), __dmul_rn(sh[0], hd[0]));
+                        ry = (R)__dadd_rn(__dsub_rn(xiy, xjy), __dmul_rn(sh[1], hd[1]));
+                        rz = (R)__dadd_rn(__dsub_rn(xiz, xjz), __dmul_rn(sh[2], hd[2]));
+                    }
+                    const R r = Idx<R>::dist(rx, ry, rz);
+                    if (!(r < pc.rc[sp])) continue;
+                    R del;
+                    const int kk = Idx<R>::knot(r, pc.rmin[sp], pc.dr[sp], pc.dri[sp], nsm2, del);
+                    const R q2 = pc.q2[sp];
+                    const size_t off = (size_t)pc.off[sp] + (kk - 1);
+                    const bool vdw = pc.vdw[sp] != 0;
+                    R dv = q2 * spline_eval<V, R>(ldg4(tab + T_CDV0C * tstride + off), del);
+                    if (vdw) dv += spline_eval<V, R>(ldg4(tab + T_CDV0 * tstride + off), del);
+                    const R fx = rx * dv, fy = ry * dv, fz = rz * dv;
+#pragma unroll
+                    for (int s2 = 0; s2 < NS; s2++)
+                        if (si == s2) { fi[s2][0] += fx; fi[s2][1] += fy; fi[s2][2] += fz; }
+                    fjx -= fx;
+                    fjy -= fy;
+                    fjz -= fz;
+                    if (ENERGY) {
+                        ecs += q2 * spline_eval<V, R>(ldg4(tab + T_CV0C * tstride + off), del);
+                        if (vdw) evs += spline_eval<V, R>(ldg4(tab + T_CV0 * tstride + off), del);
+                        pvs[0] += rx * fx;
+                        pvs[1] += ry * fy;
+                        pvs[2] += rz * fz;
+                        pvs[3] += rx * fy;
+                        pvs[4] += rx * fz;
+                        pvs[5] += ry * fz;
+                    }
+                }
+                if (fjx != (R)0 || fjy != (R)0 || fjz != (R)0) {
+                    const int j = j0 + sj;
+                    atomicAdd(&a.forceT[(3 * (size_t)j + 0) * P + b], (double)fjx);
+                    atomicAdd(&a.forceT[(3 * (size_t)j + 1) * P + b], (double)fjy);
+                    atomicAdd(&a.forceT[(3 * (size_t)j + 2) * P + b], (double)fjz);
+                }
+            }
+        }
+        // i-site forces: sum the lane groups that hold the same bead
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                double v = (double)fi[s][d];
+                if (G < 32) v = warp_sum_strided(v, G);
+                if ((G == 32 || sub == 0) && s < ni && v != 0.0)
+                    atomicAdd(&a.forceT[(3 * (size_t)(i0 + s) + d) * P + b], v);
+            }
+        }
+        ev += (double)evs;
+        ec += (double)ecs;
+#pragma unroll
+        for (int c = 0; c < 6; c++) pv[c] += (double)pvs[c];
+    }
+    if (ENERGY) {
+        double v[8] = {ev, ec, pv[0], pv[1], pv[2], pv[3], pv[4], pv[5]};
+        const int slot[8] = {S_VVDW, S_VCOUL, S_PXX, S_PYY, S_PZZ, S_PXY, S_PXZ, S_PYZ};
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            double t = v[c];
+            if (G < 32) t = warp_sum_strided(t, G);
+            if (G == 32 || sub == 0) atomicAdd(&a.acc[(size_t)b * S_NSLOT + slot[c]], t);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+
+cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
+                            const double *d_cutskin2, int pass)
+{
+    const DeviceSystem &s = c->sys;
+    const int threads = 256;
+    int blocks = (c->nmol * 32 + threads - 1) / threads;
+    const int maxb = c->sm_count * 8;
+    if (blocks > maxb) blocks = maxb;
+    if (blocks < 1) blocks = 1;
+#define MOL_LIST(NSV)                                                                                            \
+    if (pass == 0) {                                                                                             \
+        mol_list_kernel<0, NSV><<<blocks, threads, 0, c->stream>>>(                                              \
+            c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell, d_cutskin2, s.atm_typ, s.charge, \
+            s.inter_map, s.has_vdw, c->d_mcount, nullptr, nullptr, nullptr, 0, nullptr);                         \
+        mol_scan_kernel<<<1, 1024, 0, c->stream>>>(c->nmol, c->d_mcount, c->d_mrow, c->d_tot + 2);               \
+    } else {                                                                                                     \
+        mol_list_kernel<1, NSV><<<blocks, threads, 0, c->stream>>>(                                              \
+            c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell, d_cutskin2, s.atm_typ, s.charge, \
+            s.inter_map, s.has_vdw, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->mlist_cap,                  \
+            (unsigned long long *)(c->d_tot + 3));                                                               \
+    }
+    if (c->mol_ns == 3) { MOL_LIST(3) }
+    else if (c->mol_ns == 4) { MOL_LIST(4) }
+    else return cudaErrorInvalidValue;
+#undef MOL_LIST
+    return cudaGetLastError();
+}
+
+template <typename R, int P, int NS>
+static void launch_mol_t(pinyb200_ctx *c, const MolArgs &a, const Cell &cell, bool fast)
+{
+    const int threads = 128;
+    long long blocks = ((long long)a.nchunk * 32 + threads - 1) / threads;
+    const long long maxb = (long long)c->sm_count * 16;
+    if (blocks > maxb) blocks = maxb;
+    if (blocks < 1) blocks = 1;
+    dim3 grid((unsigned)blocks, P > 32 ? P / 32 : 1);
+    if constexpr (sizeof(R) == 4) {
+        if (fast) {
+            if (a.energy) mol_pair_kernel<R, P, NS, true, true><<<grid, threads, 0, c->stream>>>(a, cell);
+            else mol_pair_kernel<R, P, NS, true, false><<<grid, threads, 0, c->stream>>>(a, cell);
+            return;
+        }
+    }
+    if (a.energy) mol_pair_kernel<R, P, NS, false, true><<<grid, threads, 0, c->stream>>>(a, cell);
+    else mol_pair_kernel<R, P, NS, false, false><<<grid, threads, 0, c->stream>>>(a, cell);
+}
+
+template <typename R, int NS>
+static cudaError_t launch_mol_ns(pinyb200_ctx *c, const MolArgs &a, const Cell &cell, bool fast)
+{
+    switch (c->P) {
+    case 1: launch_mol_t<R, 1, NS>(c, a, cell, fast); break;
+    case 2: launch_mol_t<R, 2, NS>(c, a, cell, fast); break;
+    case 4: launch_mol_t<R, 4, NS>(c, a, cell, fast); break;
+    case 8: launch_mol_t<R, 8, NS>(c, a, cell, fast); break;
+    case 16: launch_mol_t<R, 16, NS>(c, a, cell, fast); break;
+    case 32: launch_mol_t<R, 32, NS>(c, a, cell, fast); break;
+    case 64: launch_mol_t<R, 64, NS>(c, a, cell, fast); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy)
+{
+    const DeviceSystem &s = c->sys;
+    MolArgs a;
+    a.nchunk = c->nchunk;
+    a.chunk = c->d_chunk;
+    a.mj = c->d_mj;
+    a.mask = c->d_mmask;
+    a.mstart = c->d_mstart;
+    a.ntyp = s.ntyp;
+    a.npt = s.npair_typ;
+    a.nuniq = s.nuniq;
+    a.nsplin = s.nsplin;
+    a.posT = c->d_posT;
+    a.pimd = c->P > 1;
+    a.xmod = c->P > 1 ? c->d_xmod : c->d_posT;  // P == 1: [natm][3][1] is [natm][3]
+    a.atm_typ = s.atm_typ;
+    a.charge = s.charge;
+    a.inter_map = s.inter_map;
+    a.cutoff = s.cutoff;
+    a.rmin = s.rmin;
+    a.dr = s.dr;
+    a.dri = s.dri;
+    a.has_vdw = s.has_vdw;
+    a.forceT = c->d_forceT;
+    a.acc = c->d_acc;
+    a.energy = energy ? 1 : 0;
+    if (c->precision == PINYB200_FP64) {
+        a.tab = s.tab64;
+        if (c->mol_ns == 3) return launch_mol_ns<double, 3>(c, a, cell, false);
+        return launch_mol_ns<double, 4>(c, a, cell, false);
+    }
+    a.tab = s.tab32;
+    if (c->mol_ns == 3) return launch_mol_ns<float, 3>(c, a, cell, true);
+    return launch_mol_ns<float, 4>(c, a, cell, true);
+}
+
+}  // namespace pinyb200

@@ -7,11 +7,23 @@
 // splines (:301-338, :512-532), grid points ia - (j-2) wrapped (:274-300),
 // the half-space spherical k list with preg = exp(-g^2/4a^2)/(g^2 V/4pi) and
 // the B-spline weights (:366-425), and the gather F = -q sum grad(M) phi
-// (:534-559).  PINY fills a complex grid and runs unnormalised complex FFTs
-// (para_fft_gen3d_bck_to_g / _fwd_to_r); the device does the same per bead.
-// Filtering with a symmetric kernel over the full grid equals PINY's
+// (:534-559).  PINY spreads into a complex grid with zero imaginary part and
+// runs unnormalised complex FFTs (para_fft_gen3d_bck_to_g / _fwd_to_r).
+// The device spreads into a real grid and keeps half of the spectrum
+// (a <= Na/2): the charge grid is real, so the other half is its complex
+// conjugate.  Filtering with the symmetric influence function equals PINY's
 // half-list convolution plus Hermitian fill (pme_sngl_pack_coef,
-// fft_package.c:458-503), and half the full-grid sum is PINY's energy.
+// fft_package.c:458-503); half of the full-grid sum is PINY's energy.
+//
+// Kernels per evaluation (all beads in each launch):
+//   spread      real grid, FP32 rows added with 16-byte vector atomics
+//   plane_fwd   per (bead, c) plane: FFT along a then b in shared memory,
+//               half spectrum out
+//   conv_c      per (bead, b): FFT along c, filter + energy + virial,
+//               inverse FFT along c
+//   plane_inv   per (bead, c): inverse FFT along b, Hermitian completion,
+//               inverse FFT along a, real potential out
+//   gather      forces from the potential grid
 #include "common.cuh"
 
 namespace pinyb200 {
@@ -22,7 +34,7 @@ struct PmeArgs {
     const double *charge;
     const double *posT;
     int Na, Nb, Nc, n;
-    void *grid;
+    void *grid;  // real [P][Nc][Nb][Na]
     double *forceT;
 };
 
@@ -67,49 +79,108 @@ __device__ __forceinline__ void scaled(double s, int N, int &i0, double &frac)
     if (!(i0 >= 0 && i0 < N)) { i0 = 0; frac = 0.0; }
 }
 
-template <typename R, int NI>
-__global__ void __launch_bounds__(256) spread_kernel(PmeArgs a, Cell cell)
+// Grid stencil of one charge: splines and the first (lowest) grid index per
+// axis.  PINY's points ia-(j-2), j = 1..n, are the n consecutive indices
+// ia-n+1 .. ia (wrapped), and point j carries weight m[j]; so grid index
+// lo + t (t = 0..n-1) carries m[n - t].
+template <typename R, int NI, bool DERIV>
+__device__ __forceinline__ void stencil(const PmeArgs &a, const Cell &cell, int at, int b, R *ma, R *mb, R *mc,
+                                        R *da, R *db, R *dc, int &la, int &lb, int &lc)
 {
-    typedef typename Cplx<R>::T C2;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)a.nchrg * a.P) return;
-    const int b = (int)(t % a.P);
-    const int ic = (int)(t / a.P);
-    const int at = a.ichrg[ic];
     const double x = a.posT[(3 * (size_t)at + 0) * a.P + b];
     const double y = a.posT[(3 * (size_t)at + 1) * a.P + b];
     const double z = a.posT[(3 * (size_t)at + 2) * a.P + b];
-    const double q = a.charge[at];
     const double sa = __dadd_rn(__dadd_rn(__dmul_rn(x, cell.hi[0]), __dmul_rn(y, cell.hi[3])), __dmul_rn(z, cell.hi[6]));
     const double sb = __dadd_rn(__dadd_rn(__dmul_rn(x, cell.hi[1]), __dmul_rn(y, cell.hi[4])), __dmul_rn(z, cell.hi[7]));
     const double sc = __dadd_rn(__dadd_rn(__dmul_rn(x, cell.hi[2]), __dmul_rn(y, cell.hi[5])), __dmul_rn(z, cell.hi[8]));
-    int ia, ib, icc;
+    int ia, ib, ic;
     double fa, fb, fc;
     scaled(sa, a.Na, ia, fa);
     scaled(sb, a.Nb, ib, fb);
-    scaled(sc, a.Nc, icc, fc);
-    R ma[NI + 1], mb[NI + 1], mc[NI + 1];
-    bspline<R, NI, false>((R)fa, ma, nullptr);
-    bspline<R, NI, false>((R)fb, mb, nullptr);
-    bspline<R, NI, false>((R)fc, mc, nullptr);
-    C2 *g = (C2 *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
-    int ga[NI + 1];
+    scaled(sc, a.Nc, ic, fc);
+    bspline<R, NI, DERIV>((R)fa, ma, da);
+    bspline<R, NI, DERIV>((R)fb, mb, db);
+    bspline<R, NI, DERIV>((R)fc, mc, dc);
+    la = ia - NI + 1;
+    if (la < 0) la += a.Na;
+    lb = ib - NI + 1;
+    if (lb < 0) lb += a.Nb;
+    lc = ic - NI + 1;
+    if (lc < 0) lc += a.Nc;
+}
+
+// Add w[t] (t = 0..NI-1) to row[(lo + t) mod N].  FP32 rows go out as
+// 16-byte vector atomics over the aligned chunks the run touches (zeros in
+// the unused lanes); FP64 rows as scalar atomics.
+template <int NI>
+__device__ __forceinline__ void row_add(float *row, int N, int lo, const float *w)
+{
+    if ((N & 3) == 0) {
+        int t = 0;
+        while (t < NI) {
+            int idx = lo + t;
+            if (idx >= N) idx -= N;
+            const int base = idx & ~3;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            // fill lanes of this chunk while the run stays inside it
+            while (t < NI) {
+                int id2 = lo + t;
+                if (id2 >= N) id2 -= N;
+                if ((id2 & ~3) != base) break;
+                const int l = id2 & 3;
+                if (l == 0) v.x = w[t];
+                else if (l == 1) v.y = w[t];
+                else if (l == 2) v.z = w[t];
+                else v.w = w[t];
+                t++;
+            }
+            atomicAdd((float4 *)(row + base), v);
+        }
+    } else {
 #pragma unroll
-    for (int j = 1; j <= NI; j++) {
-        int v = ia - (j - 2);
-        ga[j] = (v > 0 ? v : a.Na + v) - 1;
+        for (int t = 0; t < NI; t++) {
+            int idx = lo + t;
+            if (idx >= N) idx -= N;
+            atomicAdd(row + idx, w[t]);
+        }
     }
-    for (int jc = 1; jc <= NI; jc++) {
-        int vc = icc - (jc - 2);
-        const int gc = (vc > 0 ? vc : a.Nc + vc) - 1;
-        const R qc = (R)q * mc[jc];
-        for (int jb = 1; jb <= NI; jb++) {
-            int vb = ib - (jb - 2);
-            const int gb = (vb > 0 ? vb : a.Nb + vb) - 1;
-            const R qbc = mb[jb] * qc;
-            C2 *rowp = g + ((size_t)gc * a.Nb + gb) * a.Na;
+}
+
+template <int NI>
+__device__ __forceinline__ void row_add(double *row, int N, int lo, const double *w)
+{
 #pragma unroll
-            for (int ja = 1; ja <= NI; ja++) atomicAdd(&rowp[ga[ja]].x, ma[ja] * qbc);
+    for (int t = 0; t < NI; t++) {
+        int idx = lo + t;
+        if (idx >= N) idx -= N;
+        atomicAdd(row + idx, w[t]);
+    }
+}
+
+template <typename R, int NI>
+__global__ void __launch_bounds__(256) spread_kernel(PmeArgs a, Cell cell)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)a.nchrg * a.P) return;
+    const int b = (int)(t % a.P);
+    const int at = a.ichrg[t / a.P];
+    R ma[NI + 1], mb[NI + 1], mc[NI + 1];
+    int la, lb, lc;
+    stencil<R, NI, false>(a, cell, at, b, ma, mb, mc, nullptr, nullptr, nullptr, la, lb, lc);
+    const R q = (R)a.charge[at];
+    R *g = (R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
+    for (int tc = 0; tc < NI; tc++) {
+        int gc = lc + tc;
+        if (gc >= a.Nc) gc -= a.Nc;
+        const R qc = q * mc[NI - tc];
+        for (int tb = 0; tb < NI; tb++) {
+            int gb = lb + tb;
+            if (gb >= a.Nb) gb -= a.Nb;
+            const R qbc = mb[NI - tb] * qc;
+            R w[NI];
+#pragma unroll
+            for (int ta = 0; ta < NI; ta++) w[ta] = ma[NI - ta] * qbc;
+            row_add<NI>(g + ((size_t)gc * a.Nb + gb) * a.Na, a.Na, la, w);
         }
     }
 }
@@ -117,59 +188,41 @@ __global__ void __launch_bounds__(256) spread_kernel(PmeArgs a, Cell cell)
 template <typename R, int NI>
 __global__ void __launch_bounds__(256) gather_kernel(PmeArgs a, Cell cell)
 {
-    typedef typename Cplx<R>::T C2;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)a.nchrg * a.P) return;
     const int b = (int)(t % a.P);
-    const int ic = (int)(t / a.P);
-    const int at = a.ichrg[ic];
-    const double x = a.posT[(3 * (size_t)at + 0) * a.P + b];
-    const double y = a.posT[(3 * (size_t)at + 1) * a.P + b];
-    const double z = a.posT[(3 * (size_t)at + 2) * a.P + b];
-    const double q = a.charge[at];
-    const double sa = __dadd_rn(__dadd_rn(__dmul_rn(x, cell.hi[0]), __dmul_rn(y, cell.hi[3])), __dmul_rn(z, cell.hi[6]));
-    const double sb = __dadd_rn(__dadd_rn(__dmul_rn(x, cell.hi[1]), __dmul_rn(y, cell.hi[4])), __dmul_rn(z, cell.hi[7]));
-    const double sc = __dadd_rn(__dadd_rn(__dmul_rn(x, cell.hi[2]), __dmul_rn(y, cell.hi[5])), __dmul_rn(z, cell.hi[8]));
-    int ia, ib, icc;
-    double fa, fb, fc;
-    scaled(sa, a.Na, ia, fa);
-    scaled(sb, a.Nb, ib, fb);
-    scaled(sc, a.Nc, icc, fc);
+    const int at = a.ichrg[t / a.P];
     R ma[NI + 1], mb[NI + 1], mc[NI + 1], da[NI + 1], db[NI + 1], dc[NI + 1];
-    bspline<R, NI, true>((R)fa, ma, da);
-    bspline<R, NI, true>((R)fb, mb, db);
-    bspline<R, NI, true>((R)fc, mc, dc);
-    const C2 *g = (const C2 *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
-    int ga[NI + 1];
-#pragma unroll
-    for (int j = 1; j <= NI; j++) {
-        int v = ia - (j - 2);
-        ga[j] = (v > 0 ? v : a.Na + v) - 1;
-    }
+    int la, lb, lc;
+    stencil<R, NI, true>(a, cell, at, b, ma, mb, mc, da, db, dc, la, lb, lc);
+    const double q = a.charge[at];
+    const R *g = (const R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
     // separable sums: d/ds_a, d/ds_b, d/ds_c of sum M_a M_b M_c phi
     double ea = 0.0, eb = 0.0, ec = 0.0;
-    for (int jc = 1; jc <= NI; jc++) {
-        int vc = icc - (jc - 2);
-        const int gc = (vc > 0 ? vc : a.Nc + vc) - 1;
+    for (int tc = 0; tc < NI; tc++) {
+        int gc = lc + tc;
+        if (gc >= a.Nc) gc -= a.Nc;
         R sa_c = 0, sda_c = 0, sdb_c = 0;
-        for (int jb = 1; jb <= NI; jb++) {
-            int vb = ib - (jb - 2);
-            const int gb = (vb > 0 ? vb : a.Nb + vb) - 1;
-            const C2 *rowp = g + ((size_t)gc * a.Nb + gb) * a.Na;
+        for (int tb = 0; tb < NI; tb++) {
+            int gb = lb + tb;
+            if (gb >= a.Nb) gb -= a.Nb;
+            const R *rowp = g + ((size_t)gc * a.Nb + gb) * a.Na;
             R s0 = 0, s1 = 0;
 #pragma unroll
-            for (int ja = 1; ja <= NI; ja++) {
-                const R phi = rowp[ga[ja]].x;
-                s0 += ma[ja] * phi;
-                s1 += da[ja] * phi;
+            for (int ta = 0; ta < NI; ta++) {
+                int ga = la + ta;
+                if (ga >= a.Na) ga -= a.Na;
+                const R phi = __ldg(rowp + ga);
+                s0 += ma[NI - ta] * phi;
+                s1 += da[NI - ta] * phi;
             }
-            sa_c += mb[jb] * s0;      // for the c derivative
-            sda_c += mb[jb] * s1;     // for the a derivative
-            sdb_c += db[jb] * s0;     // for the b derivative
+            sa_c += mb[NI - tb] * s0;   // for the c derivative
+            sda_c += mb[NI - tb] * s1;  // for the a derivative
+            sdb_c += db[NI - tb] * s0;  // for the b derivative
         }
-        ea += (double)(mc[jc] * sda_c);
-        eb += (double)(mc[jc] * sdb_c);
-        ec += (double)(dc[jc] * sa_c);
+        ea += (double)(mc[NI - tc] * sda_c);
+        eb += (double)(mc[NI - tc] * sdb_c);
+        ec += (double)(dc[NI - tc] * sa_c);
     }
     ea *= (double)a.Na;
     eb *= (double)a.Nb;
@@ -184,99 +237,228 @@ __global__ void __launch_bounds__(256) gather_kernel(PmeArgs a, Cell cell)
 }
 
 // ---------------------------------------------------------------------------
-// Batched complex FFT along one axis of the [bead][c][b][a] grid.  A block
-// stages TL lines of length N in shared memory with coalesced loads (lines
-// are consecutive in a for the b and c axes), runs an in-place radix-2
-// decimation-in-time transform (or a direct DFT when N is not a power of
-// two), and writes the lines back.  Unnormalised, exp(sign 2 pi i nk/N).
+// In-place FFTs of `nl` lines of length N held in shared memory: element n of
+// line l at sm[l * ls + n * es].  Unnormalised, exp(sign 2 pi i n k / N);
+// tw[2m], tw[2m+1] = cos, sin(2 pi m / N).  Power-of-two lengths use an
+// iterative radix-2 decimation in time; other lengths a direct DFT done a
+// block of lines at a time.  Every thread of the block must call these.
 template <typename R>
-__global__ void __launch_bounds__(256) fft_axis_kernel(void *data, int axis, int Na, int Nb, int Nc, int P, int TL,
-                                                       const R *__restrict__ tw, int sign)
+__device__ void smem_fft(typename Cplx<R>::T *sm, int N, int nl, int ls, int es, const R *tw, int sign)
 {
     typedef typename Cplx<R>::T C2;
-    extern __shared__ unsigned char smem_raw[];
-    C2 *sm = (C2 *)smem_raw;
-    C2 *g = (C2 *)data;
-    const int N = axis == 0 ? Na : (axis == 1 ? Nb : Nc);
-    const size_t G = (size_t)Na * Nb * Nc;
-    size_t base;
-    long long estride, lstride;
-    const int tile = blockIdx.x;
-    if (axis == 0) {
-        base = (size_t)tile * TL * Na;
-        estride = 1;
-        lstride = Na;
-    } else {
-        const int nat = Na / TL;
-        const int at = tile % nat;
-        const int rest = tile / nat;
-        const int outer = axis == 1 ? Nc : Nb;
-        const int o = rest % outer;
-        const int bead = rest / outer;
-        if (axis == 1) base = (size_t)bead * G + (size_t)o * Na * Nb + (size_t)at * TL;
-        else base = (size_t)bead * G + (size_t)o * Na + (size_t)at * TL;
-        estride = axis == 1 ? Na : (long long)Na * Nb;
-        lstride = 1;
-    }
-    const bool pow2 = (N & (N - 1)) == 0;
-    int logn = 0;
-    while ((1 << logn) < N) logn++;
-    const int tot = TL * N;
-    // load (bit-reversed for the radix-2 path)
-    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
-        int l, nn;
-        if (axis == 0) { l = idx / N; nn = idx % N; }
-        else { nn = idx / TL; l = idx % TL; }
-        C2 v = g[base + (size_t)l * lstride + (size_t)nn * estride];
-        int dst = nn;
-        if (pow2) dst = __brev(nn) >> (32 - logn);
-        if (logn == 0) dst = 0;
-        sm[l * N + dst] = v;
-    }
-    __syncthreads();
-    if (pow2) {
-        for (int half = 1; half < N; half <<= 1) {
-            const int tstep = N / (2 * half);
-            for (int idx = threadIdx.x; idx < TL * (N / 2); idx += blockDim.x) {
-                const int l = idx / (N / 2);
-                const int bf = idx % (N / 2);
-                const int grp = bf / half, k = bf % half;
-                const int i0 = grp * 2 * half + k, i1 = i0 + half;
-                const R wr = tw[2 * (k * tstep)], wi = (R)sign * tw[2 * (k * tstep) + 1];
-                C2 u = sm[l * N + i0], v = sm[l * N + i1];
-                C2 vw;
-                vw.x = v.x * wr - v.y * wi;
-                vw.y = v.x * wi + v.y * wr;
-                sm[l * N + i0].x = u.x + vw.x;
-                sm[l * N + i0].y = u.y + vw.y;
-                sm[l * N + i1].x = u.x - vw.x;
-                sm[l * N + i1].y = u.y - vw.y;
+    const int nt = blockDim.x;
+    if ((N & (N - 1)) == 0) {
+        int logn = 0;
+        while ((1 << logn) < N) logn++;
+        if (logn > 0) {
+            for (int idx = threadIdx.x; idx < nl * N; idx += nt) {
+                const int l = idx / N, n = idx % N;
+                const int r = __brev(n) >> (32 - logn);
+                if (n < r) {
+                    C2 *p = sm + l * ls;
+                    C2 u = p[n * es];
+                    p[n * es] = p[r * es];
+                    p[r * es] = u;
+                }
             }
             __syncthreads();
         }
-        for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
-            int l, nn;
-            if (axis == 0) { l = idx / N; nn = idx % N; }
-            else { nn = idx / TL; l = idx % TL; }
-            g[base + (size_t)l * lstride + (size_t)nn * estride] = sm[l * N + nn];
+        for (int half = 1; half < N; half <<= 1) {
+            const int tstep = N / (2 * half);
+            for (int idx = threadIdx.x; idx < nl * (N / 2); idx += nt) {
+                const int l = idx / (N / 2);
+                const int bf = idx % (N / 2);
+                const int k = bf % half;
+                const int i0 = (bf / half) * 2 * half + k, i1 = i0 + half;
+                const R wr = tw[2 * (k * tstep)], wi = (R)sign * tw[2 * (k * tstep) + 1];
+                C2 *p = sm + l * ls;
+                const C2 u = p[i0 * es], v = p[i1 * es];
+                const R vr = v.x * wr - v.y * wi, vi = v.x * wi + v.y * wr;
+                p[i0 * es].x = u.x + vr;
+                p[i0 * es].y = u.y + vi;
+                p[i1 * es].x = u.x - vr;
+                p[i1 * es].y = u.y - vi;
+            }
+            __syncthreads();
         }
     } else {
-        for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
-            int l, kk;
-            if (axis == 0) { l = idx / N; kk = idx % N; }
-            else { kk = idx / TL; l = idx % TL; }
+        const int per = nt / N;  // lines per pass
+        for (int l0 = 0; l0 < nl; l0 += per) {
+            const int l = l0 + threadIdx.x / N, k = threadIdx.x % N;
             R sr = 0, si = 0;
-            for (int nn = 0; nn < N; nn++) {
-                const int e = (int)(((long long)nn * kk) % N);
-                const R wr = tw[2 * e], wi = (R)sign * tw[2 * e + 1];
-                const C2 v = sm[l * N + nn];
-                sr += v.x * wr - v.y * wi;
-                si += v.x * wi + v.y * wr;
+            const bool act = threadIdx.x < per * N && l < nl;
+            if (act) {
+                const C2 *p = sm + l * ls;
+                for (int n = 0; n < N; n++) {
+                    const int e = (int)(((long long)n * k) % N);
+                    const R wr = tw[2 * e], wi = (R)sign * tw[2 * e + 1];
+                    const C2 v = p[n * es];
+                    sr += v.x * wr - v.y * wi;
+                    si += v.x * wi + v.y * wr;
+                }
             }
-            C2 o;
-            o.x = sr;
-            o.y = si;
-            g[base + (size_t)l * lstride + (size_t)kk * estride] = o;
+            __syncthreads();
+            if (act) {
+                sm[l * ls + k * es].x = sr;
+                sm[l * ls + k * es].y = si;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void load_twiddles(R *dst, const R *src, int N)
+{
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) dst[i] = src[i];
+}
+
+// Forward transform of one (bead, c) plane along a then b; half spectrum
+// (a <= Na/2) out.  Shared: plane [Nb][Na+1] complex, twiddles.
+template <typename R>
+__global__ void __launch_bounds__(256) plane_fwd_kernel(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
+                                                        int Na, int Nb, int Nc, const R *__restrict__ twa,
+                                                        const R *__restrict__ twb)
+{
+    typedef typename Cplx<R>::T C2;
+    extern __shared__ unsigned char smem_raw[];
+    C2 *pl = (C2 *)smem_raw;
+    const int ls = Na + 1;
+    R *ta = (R *)(pl + (size_t)Nb * ls);
+    R *tb = ta + 2 * Na;
+    const int Nh = Na / 2 + 1;
+    const size_t plane = blockIdx.x;  // bead * Nc + c
+    load_twiddles(ta, twa, Na);
+    load_twiddles(tb, twb, Nb);
+    const R *src = q + plane * Na * Nb;
+    for (int idx = threadIdx.x; idx < Na * Nb; idx += blockDim.x) {
+        C2 v;
+        v.x = src[idx];
+        v.y = (R)0;
+        pl[(idx / Na) * ls + idx % Na] = v;
+    }
+    __syncthreads();
+    smem_fft<R>(pl, Na, Nb, ls, 1, ta, +1);   // along a, every row
+    smem_fft<R>(pl, Nb, Nh, 1, ls, tb, +1);   // along b, columns a <= Na/2
+    C2 *dst = spec + plane * (size_t)Nb * Nh;
+    for (int idx = threadIdx.x; idx < Nb * Nh; idx += blockDim.x) dst[idx] = pl[(idx / Nh) * ls + idx % Nh];
+}
+
+// Inverse of plane_fwd: half spectrum in, along b, Hermitian completion of
+// each row (U(Na-a) = conj U(a) once b and c are back in real space), along
+// a, real part out.
+template <typename R>
+__global__ void __launch_bounds__(256) plane_inv_kernel(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phi,
+                                                        int Na, int Nb, int Nc, const R *__restrict__ twa,
+                                                        const R *__restrict__ twb)
+{
+    typedef typename Cplx<R>::T C2;
+    extern __shared__ unsigned char smem_raw[];
+    C2 *pl = (C2 *)smem_raw;
+    const int ls = Na + 1;
+    R *ta = (R *)(pl + (size_t)Nb * ls);
+    R *tb = ta + 2 * Na;
+    const int Nh = Na / 2 + 1;
+    const size_t plane = blockIdx.x;
+    load_twiddles(ta, twa, Na);
+    load_twiddles(tb, twb, Nb);
+    const C2 *src = spec + plane * (size_t)Nb * Nh;
+    for (int idx = threadIdx.x; idx < Nb * Nh; idx += blockDim.x) pl[(idx / Nh) * ls + idx % Nh] = src[idx];
+    __syncthreads();
+    smem_fft<R>(pl, Nb, Nh, 1, ls, tb, -1);
+    for (int idx = threadIdx.x; idx < Nb * Na; idx += blockDim.x) {
+        const int b = idx / Na, a = idx % Na;
+        if (a >= Nh) {
+            C2 v = pl[b * ls + (Na - a)];
+            v.y = -v.y;
+            pl[b * ls + a] = v;
+        }
+    }
+    __syncthreads();
+    smem_fft<R>(pl, Na, Nb, ls, 1, ta, -1);
+    R *dst = phi + plane * Na * Nb;
+    for (int idx = threadIdx.x; idx < Na * Nb; idx += blockDim.x) dst[idx] = pl[(idx / Na) * ls + idx % Na].x;
+}
+
+// One (bead, b) slab of the half spectrum: FFT along c, energy and virial
+// of the k-sphere terms (ewald3d_pme.c:366-425), multiplication by the
+// influence function, inverse FFT along c.  Half-spectrum points with
+// 0 < a < Na/2 stand for two full-grid points; E = 1/2 sum_full w |S|^2.
+template <typename R>
+__global__ void __launch_bounds__(256) conv_c_kernel(typename Cplx<R>::T *__restrict__ spec, const R *__restrict__ filt,
+                                                     int Na, int Nb, int Nc, const R *__restrict__ twc, Cell cell,
+                                                     double alp, double *__restrict__ acc, int energy)
+{
+    typedef typename Cplx<R>::T C2;
+    extern __shared__ unsigned char smem_raw[];
+    C2 *sl = (C2 *)smem_raw;
+    const int Nh = Na / 2 + 1;
+    const int ls = Nh + 1;  // padded line stride: element c of column a at sl[c * ls + a]
+    R *tc = (R *)(sl + (size_t)Nc * ls);
+    __shared__ double red[7][8];
+    const int bead = blockIdx.x / Nb, b = blockIdx.x % Nb;
+    load_twiddles(tc, twc, Nc);
+    C2 *base = spec + ((size_t)bead * Nc * Nb + b) * Nh;
+    const size_t cstride = (size_t)Nb * Nh;
+    for (int idx = threadIdx.x; idx < Nc * Nh; idx += blockDim.x) {
+        const int c = idx / Nh, a = idx % Nh;
+        sl[c * ls + a] = base[c * cstride + a];
+    }
+    __syncthreads();
+    smem_fft<R>(sl, Nc, Nh, 1, ls, tc, +1);
+    double e = 0, pxx = 0, pyy = 0, pzz = 0, pxy = 0, pxz = 0, pyz = 0;
+    const double kb = b <= Nb / 2 ? b : b - Nb;
+    const double tpi = 2.0 * M_PI, falp2 = 4.0 * alp * alp;
+    for (int idx = threadIdx.x; idx < Nc * Nh; idx += blockDim.x) {
+        const int c = idx / Nh, a = idx % Nh;
+        const R w = filt[((size_t)c * Nb + b) * Na + a];
+        C2 s = sl[c * ls + a];
+        if (w != (R)0 && energy) {
+            const double ka = a, kc = c <= Nc / 2 ? c : c - Nc;
+            const double xk = tpi * (ka * cell.hi[0] + kb * cell.hi[1] + kc * cell.hi[2]);
+            const double yk = tpi * (ka * cell.hi[3] + kb * cell.hi[4] + kc * cell.hi[5]);
+            const double zk = tpi * (ka * cell.hi[6] + kb * cell.hi[7] + kc * cell.hi[8]);
+            const double g2 = xk * xk + yk * yk + zk * zk;
+            const double mult = (a == 0 || 2 * a == Na) ? 0.5 : 1.0;
+            const double sm = mult * ((double)s.x * (double)s.x + (double)s.y * (double)s.y) * (double)w;
+            const double prep = -2.0 * ((g2 / falp2) + 1.0) / g2 * sm;
+            e += sm;
+            pxx += prep * xk * xk;
+            pyy += prep * yk * yk;
+            pzz += prep * zk * zk;
+            pxy += prep * xk * yk;
+            pxz += prep * xk * zk;
+            pyz += prep * yk * zk;
+        }
+        s.x *= w;
+        s.y *= w;
+        sl[c * ls + a] = s;
+    }
+    __syncthreads();
+    smem_fft<R>(sl, Nc, Nh, 1, ls, tc, -1);
+    for (int idx = threadIdx.x; idx < Nc * Nh; idx += blockDim.x) {
+        const int c = idx / Nh, a = idx % Nh;
+        base[c * cstride + a] = sl[c * ls + a];
+    }
+    if (!energy) return;
+    double v[7] = {e, pxx, pyy, pzz, pxy, pxz, pyz};
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        double t = warp_sum(v[k]);
+        if (lane == 0) red[k][wid] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        double t = 0;
+        for (int w2 = 0; w2 < (int)(blockDim.x >> 5); w2++) t += red[threadIdx.x][w2];
+        const int slot[7] = {S_VRECIP, S_PXX, S_PYY, S_PZZ, S_PXY, S_PXZ, S_PYZ};
+        atomicAdd(&acc[(size_t)bead * S_NSLOT + slot[threadIdx.x]], t);
+        if (threadIdx.x == 0) {
+            // diagonal vnow term of the pressure tensor (ewald3d_pme.c:415-417)
+            atomicAdd(&acc[(size_t)bead * S_NSLOT + S_PXX], t);
+            atomicAdd(&acc[(size_t)bead * S_NSLOT + S_PYY], t);
+            atomicAdd(&acc[(size_t)bead * S_NSLOT + S_PZZ], t);
         }
     }
 }
@@ -309,86 +491,22 @@ __global__ void filter_kernel(int Na, int Nb, int Nc, const int *__restrict__ km
     f32[g] = (float)w;
 }
 
-// Energy, virial and convolution over one bead's transformed grid.  Energy
-// per half-list entry is |S|^2 preg bw (ewald3d_pme.c:396); the full grid
-// holds every entry twice, hence the 1/2.
-template <typename R>
-__global__ void __launch_bounds__(256) conv_kernel(void *data, const R *__restrict__ filt, int Na, int Nb, int Nc,
-                                                   Cell cell, double alp, double *__restrict__ acc, int energy)
+// Shared memory of the plane and slab kernels.
+size_t pme_plane_smem(int Na, int Nb, bool fp64)
 {
-    typedef typename Cplx<R>::T C2;
-    const size_t G = (size_t)Na * Nb * Nc;
-    const int bead = blockIdx.y;
-    const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    double e = 0, pxx = 0, pyy = 0, pzz = 0, pxy = 0, pxz = 0, pyz = 0;
-    if (g < G) {
-        C2 *p = (C2 *)data + (size_t)bead * G + g;
-        const R w = filt[g];
-        C2 s = *p;
-        if (w != (R)0 && energy) {
-            const int a = (int)(g % Na);
-            const int bb = (int)((g / Na) % Nb);
-            const int c = (int)(g / ((size_t)Na * Nb));
-            const double ka = a <= Na / 2 ? a : a - Na, kb = bb <= Nb / 2 ? bb : bb - Nb,
-                         kc = c <= Nc / 2 ? c : c - Nc;
-            const double tpi = 2.0 * M_PI;
-            const double xk = tpi * (ka * cell.hi[0] + kb * cell.hi[1] + kc * cell.hi[2]);
-            const double yk = tpi * (ka * cell.hi[3] + kb * cell.hi[4] + kc * cell.hi[5]);
-            const double zk = tpi * (ka * cell.hi[6] + kb * cell.hi[7] + kc * cell.hi[8]);
-            const double g2 = xk * xk + yk * yk + zk * zk;
-            const double falp2 = 4.0 * alp * alp;
-            const double sm = 0.5 * ((double)s.x * (double)s.x + (double)s.y * (double)s.y) * (double)w;
-            e = sm;
-            const double prep = -2.0 * ((g2 / falp2) + 1.0) / g2 * sm;
-            pxx = prep * xk * xk;
-            pyy = prep * yk * yk;
-            pzz = prep * zk * zk;
-            pxy = prep * xk * yk;
-            pxz = prep * xk * zk;
-            pyz = prep * yk * zk;
-        }
-        s.x *= w;
-        s.y *= w;
-        *p = s;
-    }
-    if (!energy) return;
-    double v[7] = {e, pxx, pyy, pzz, pxy, pxz, pyz};
-    __shared__ double red[7][8];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int c = 0; c < 7; c++) {
-        double t = warp_sum(v[c]);
-        if (lane == 0) red[c][wid] = t;
-    }
-    __syncthreads();
-    if (threadIdx.x < 7) {
-        double t = 0;
-        for (int w2 = 0; w2 < (int)(blockDim.x >> 5); w2++) t += red[threadIdx.x][w2];
-        const int slot[7] = {S_VRECIP, S_PXX, S_PYY, S_PZZ, S_PXY, S_PXZ, S_PYZ};
-        atomicAdd(&acc[(size_t)bead * S_NSLOT + slot[threadIdx.x]], t);
-        if (threadIdx.x == 0) {
-            // diagonal vnow term of the pressure tensor (ewald3d_pme.c:415-417)
-            atomicAdd(&acc[(size_t)bead * S_NSLOT + S_PXX], t);
-            atomicAdd(&acc[(size_t)bead * S_NSLOT + S_PYY], t);
-            atomicAdd(&acc[(size_t)bead * S_NSLOT + S_PZZ], t);
-        }
-    }
+    const size_t cs = fp64 ? 16 : 8, rs = fp64 ? 8 : 4;
+    return cs * (size_t)Nb * (Na + 1) + rs * 2 * (size_t)(Na + Nb);
 }
-
-// Lines per block: a power of two <= 16 that divides the line count of the
-// tile decomposition and keeps the staged tile within 48 KB.
-template <typename R>
-static int pick_tl(long long divisor, int N)
+size_t pme_slab_smem(int Na, int Nc, bool fp64)
 {
-    typedef typename Cplx<R>::T C2;
-    int tl = 16;
-    while (tl > 1 && ((divisor % tl) || (size_t)tl * N * sizeof(C2) > 48 * 1024)) tl >>= 1;
-    return tl;
+    const size_t cs = fp64 ? 16 : 8, rs = fp64 ? 8 : 4;
+    return cs * (size_t)Nc * (Na / 2 + 2) + rs * 2 * (size_t)Nc;
 }
 
 template <typename R, int NI>
 static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
 {
+    typedef typename Cplx<R>::T C2;
     const DeviceSystem &s = c->sys;
     PmeArgs a;
     a.natm = s.natm;
@@ -403,38 +521,33 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     a.n = s.n_interp;
     a.grid = c->d_grid;
     a.forceT = c->d_forceT;
-    typedef typename Cplx<R>::T C2;
     const size_t G = (size_t)a.Na * a.Nb * a.Nc;
-    cudaError_t err = cudaMemsetAsync(c->d_grid, 0, sizeof(C2) * G * c->P, c->stream);
+    const bool f64 = sizeof(R) == 8;
+    cudaError_t err = cudaMemsetAsync(c->d_grid, 0, sizeof(R) * G * c->P, c->stream);
     if (err != cudaSuccess) return err;
     const long long nt = (long long)a.nchrg * a.P;
     const int threads = 256;
     spread_kernel<R, NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell);
-    const R *tw[3];
-    const R *twbase = (const R *)(sizeof(R) == 8 ? (const void *)c->d_twiddle64 : (const void *)c->d_twiddle32);
-    const int maxN = 256;
-    for (int ax = 0; ax < 3; ax++) tw[ax] = twbase + 2 * maxN * ax;
-    const int dims[3] = {a.Na, a.Nb, a.Nc};
-    const int TLs[3] = {pick_tl<R>((long long)a.Nb * a.Nc * a.P, a.Na), pick_tl<R>(a.Na, a.Nb),
-                        pick_tl<R>(a.Na, a.Nc)};
-    for (int pass = 0; pass < 2; pass++) {
-        const int sign = pass == 0 ? +1 : -1;
-        for (int ax = 0; ax < 3; ax++) {
-            const int N = dims[ax];
-            const int TL = TLs[ax];
-            long long nlines = (long long)G * a.P / N;
-            int tiles = (int)(nlines / TL);
-            size_t sh = sizeof(C2) * TL * N;
-            fft_axis_kernel<R><<<tiles, 256, sh, c->stream>>>(c->d_grid, ax, a.Na, a.Nb, a.Nc, a.P, TL, tw[ax], sign);
-        }
-        if (pass == 0) {
-            dim3 grid((unsigned)((G + 255) / 256), (unsigned)a.P);
-            const R *filt = (const R *)c->d_filter;
-            if (sizeof(R) == 4) filt = (const R *)((const double *)c->d_filter + G);
-            conv_kernel<R><<<grid, 256, 0, c->stream>>>(c->d_grid, filt, a.Na, a.Nb, a.Nc, cell, c->alp_ewd, c->d_acc,
-                                                        energy ? 1 : 0);
-        }
+    const R *twbase = (const R *)(f64 ? (const void *)c->d_twiddle64 : (const void *)c->d_twiddle32);
+    const R *tw[3] = {twbase, twbase + 2 * 256, twbase + 4 * 256};
+    const size_t sp = pme_plane_smem(a.Na, a.Nb, f64), ss = pme_slab_smem(a.Na, a.Nc, f64);
+    // opt in to more than 48 KB of dynamic shared memory where a plane needs it
+    if (sp > 48 * 1024) {
+        err = cudaFuncSetAttribute(plane_fwd_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(plane_inv_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp);
+        if (err != cudaSuccess) return err;
     }
+    if (ss > 48 * 1024) {
+        err = cudaFuncSetAttribute(conv_c_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss);
+        if (err != cudaSuccess) return err;
+    }
+    C2 *spec = (C2 *)c->d_spec;
+    plane_fwd_kernel<R><<<a.P * a.Nc, 256, sp, c->stream>>>((const R *)c->d_grid, spec, a.Na, a.Nb, a.Nc, tw[0], tw[1]);
+    const R *filt = f64 ? (const R *)c->d_filter : (const R *)((const double *)c->d_filter + G);
+    conv_c_kernel<R><<<a.P * a.Nb, 256, ss, c->stream>>>(spec, filt, a.Na, a.Nb, a.Nc, tw[2], cell, c->alp_ewd,
+                                                          c->d_acc, energy ? 1 : 0);
+    plane_inv_kernel<R><<<a.P * a.Nc, 256, sp, c->stream>>>(spec, (R *)c->d_grid, a.Na, a.Nb, a.Nc, tw[0], tw[1]);
     gather_kernel<R, NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell);
     return cudaGetLastError();
 }

@@ -22,6 +22,7 @@ PINYB200_FP64 = 0
 PINYB200_MIXED = 1
 DISTRIB_GHOSTS = 1
 NO_ENERGY = 2
+SITE_PAIRS = 4
 
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NO_DEVICE", 4: "ERR_LIST_OVERFLOW", 5: "ERR_CUTOFF",
           6: "ERR_TIMEOUT", 7: "ERR_NAN", 8: "ERR_UNSUPPORTED", 9: "ERR_STATE"}
@@ -186,13 +187,14 @@ class DeviceBox:
         self._check(self.L.pinyb200_list_info(self.h, C.byref(n), C.byref(a), C.byref(c)), "list_info")
         return {"npairs": n.value, "nactive": a.value, "capacity": c.value}
 
-    def energy_force(self, pos, xmod, hmat, distribute_ghosts=False, energy=True):
+    def energy_force(self, pos, xmod, hmat, distribute_ghosts=False, energy=True, site_pairs=False):
         pos = np.ascontiguousarray(pos, np.float64).reshape(self.P, self.natm, 3)
         xm = None if xmod is None else np.ascontiguousarray(xmod, np.float64).reshape(self.natm, 3)
         hmat = np.ascontiguousarray(hmat, np.float64)
         force = np.empty_like(pos)
         e = PinyEnergies()
-        flags = (DISTRIB_GHOSTS if distribute_ghosts else 0) | (0 if energy else NO_ENERGY)
+        flags = (DISTRIB_GHOSTS if distribute_ghosts else 0) | (0 if energy else NO_ENERGY) | \
+            (SITE_PAIRS if site_pairs else 0)
         self._check(self.L.pinyb200_energy_force(self.h, _dp(pos), None if xm is None else _dp(xm), _dp(hmat),
                                                  flags, _dp(force), C.byref(e)), "energy_force")
         return force, energies_dict(e)

@@ -350,6 +350,8 @@ def named_spec(name: str) -> BoxSpec:
         return BoxSpec(TIP4P_F, 4096, 49.66, 32, 298.0, 12345, grid=64, order=8)
     if name == "tip4pf_1024_p16":
         return BoxSpec(TIP4P_F, 1024, 31.28, 16, 298.0, 12345, grid=32, order=8)
+    if name == "tip4pf_1024_p32":
+        return BoxSpec(TIP4P_F, 1024, 31.28, 32, 298.0, 12345, grid=32, order=8)
     if name == "tip4pf_256_p4":
         return BoxSpec(TIP4P_F, 256, 19.73, 4, 298.0, 777, grid=32, order=8)
     if name == "spcfw_216_p4":

@@ -35,6 +35,10 @@ def test_device_matches_piny(name, prec):
     assert rel_rms(force, F["ref_force_raw"]) < TOL[prec]
     force2, _ = box.energy_force(F["pos"], xmod, F["hmat"], distribute_ghosts=True)
     assert rel_rms(force2, F["ref_force"]) < TOL[prec]
+    # the site-list kernel (general fallback) agrees as well
+    force3, e3 = box.energy_force(F["pos"], xmod, F["hmat"], site_pairs=True)
+    assert rel_rms(force3, F["ref_force_raw"]) < TOL[prec]
+    assert abs(e3["vintert"] - e["vintert"]) <= ETOL[prec] * max(1.0, abs(e["vintert"]))
     for k, kr in [("vintert", "vintert"), ("vintrat", "vintrat"), ("vvdw", "vvdw"), ("vcoul", "vcoul"),
                   ("vlong", "vlong"), ("vbond", "vbondt"), ("vbend", "vbendt")]:
         ref = F["ref_" + kr]
