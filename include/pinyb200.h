@@ -176,6 +176,38 @@ int pinyb200_list_info(pinyb200_ctx *ctx, long *npairs, long *nactive,
                        long *capacity);
 
 /*
+ * Pair count without allocation.  This entry point has no counterpart in
+ * the reference: PINY sizes its list by counting inside verlist_create and
+ * growing with realloc, which a caller that must not allocate device memory
+ * cannot do.  Counts, for bead-1 positions already on the device, the pairs
+ * pinyb200_build_list would hold (*npairs) and the force-bearing subset
+ * (*nactive), with the same FP64 criterion, without touching the context's
+ * list.  Arguments as in pinyb200_build_list, except:
+ *   d_pos1, d_xmod : device arrays natm x 3 (d_xmod may be NULL);
+ *   stream         : opaque CUDA stream handle, NULL = the context's stream;
+ *                    the call returns after that stream is idle.
+ * It calls no cudaMalloc/cudaFree: its scratch is one fixed device array per
+ * GPU (about 1 MiB) inside the library, so
+ *   - it accepts natm <= PINYB200_COUNT_MAX_ATOMS and at most
+ *     PINYB200_COUNT_MAX_PAIR_TYPES pair types (ntyp(ntyp+1)/2), and returns
+ *     PINYB200_ERR_ARG beyond them;
+ *   - the first call on each GPU looks up the scratch address
+ *     (cudaGetSymbolAddress, which may load the library's device code):
+ *     make that first call before any stream capture begins;
+ *   - calls on the same GPU share the scratch: calls that overlap in time
+ *     (from several host threads, or on several streams) race and give
+ *     wrong counts; serialise them.
+ */
+enum {
+    PINYB200_COUNT_MAX_ATOMS = 65536,
+    PINYB200_COUNT_MAX_PAIR_TYPES = 64
+};
+int pinyb200_count_list_device(pinyb200_ctx *ctx, const double *d_pos1,
+                               const double *d_xmod, const double *hmat,
+                               const double *cutskin2, long *npairs,
+                               long *nactive, void *stream);
+
+/*
  * One force/energy evaluation of all beads with host buffers.
  *   pos   : nbeads x natm x 3 host array (bead-major AoS), ghosts are
  *           recomputed from their components (get_ghost_pos);

@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -140,6 +141,27 @@ int check_system(pinyb200_ctx *c, const pinyb200_system *s, int nbeads)
 }
 
 }  // namespace
+
+// Scratch of pinyb200_count_list_device: one fixed array per GPU, so that
+// call allocates no device memory.  Byte layout:
+//   [0, 16)                 totals (full, active) as two unsigned 64-bit
+//                           integers; accumulated, so cleared by every call
+//   [256, 256 + 8*MAXPT)    copy of cutskin2 (PINYB200_COUNT_MAX_PAIR_TYPES)
+//   [4096, 4096 + 8*MAXAT)  per-atom counts [2][natm] (full, active); every
+//                           entry is written by the count pass, none is read
+//                           before it is written
+static constexpr size_t kCountTotOff = 0;
+static constexpr size_t kCountCutOff = 256;
+static constexpr size_t kCountRowOff = 4096;
+static constexpr size_t kCountScratchBytes = kCountRowOff + 2 * sizeof(int) * (size_t)PINYB200_COUNT_MAX_ATOMS;
+static_assert(kCountCutOff + 8 * PINYB200_COUNT_MAX_PAIR_TYPES <= kCountRowOff, "count scratch layout");
+static __device__ __align__(256) unsigned char g_count_scratch[kCountScratchBytes];
+
+// Device address of g_count_scratch per GPU, looked up on the first call
+// made with that GPU current.
+static constexpr int kCountMaxDevices = 64;
+static std::mutex g_count_mu;
+static unsigned char *g_count_addr[kCountMaxDevices];
 
 extern "C" {
 
@@ -686,6 +708,54 @@ int pinyb200_piny_force(pinyb200_ctx *c, double *const *x, double *const *y, dou
     if (pvten_tot)
         for (int k = 0; k < 9; k++) pvten_tot[k + 1] += en.pvten[k];
     if (e) *e = en;
+    return PINYB200_OK;
+}
+
+int pinyb200_count_list_device(pinyb200_ctx *c, const double *d_pos1, const double *d_xmod, const double *hmat,
+                               const double *cutskin2, long *npairs, long *nactive, void *stream)
+{
+    if (!c || !d_pos1 || !hmat || !cutskin2) return fail(c, PINYB200_ERR_ARG, "count_list_device: NULL argument");
+    if (c->sys.natm > PINYB200_COUNT_MAX_ATOMS)
+        return fail(c, PINYB200_ERR_ARG,
+                    "count_list_device: natm = " + std::to_string(c->sys.natm) +
+                        " exceeds the fixed scratch limit PINYB200_COUNT_MAX_ATOMS = " +
+                        std::to_string((int)PINYB200_COUNT_MAX_ATOMS) + "; use pinyb200_build_list");
+    if (c->sys.npair_typ > PINYB200_COUNT_MAX_PAIR_TYPES)
+        return fail(c, PINYB200_ERR_ARG,
+                    "count_list_device: " + std::to_string(c->sys.npair_typ) +
+                        " pair types exceed the fixed scratch limit PINYB200_COUNT_MAX_PAIR_TYPES = " +
+                        std::to_string((int)PINYB200_COUNT_MAX_PAIR_TYPES));
+    if (c->device < 0 || c->device >= kCountMaxDevices)
+        return fail(c, PINYB200_ERR_UNSUPPORTED, "count_list_device: device ordinal beyond 63");
+    CK(cudaSetDevice(c->device));
+    unsigned char *base = nullptr;
+    {
+        // set-up, once per GPU, with that GPU current
+        std::lock_guard<std::mutex> lock(g_count_mu);
+        if (!g_count_addr[c->device]) {
+            void *p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_count_scratch);
+            if (e != cudaSuccess || !p)
+                return fail(c, PINYB200_ERR_CUDA,
+                            std::string("count_list_device: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            g_count_addr[c->device] = (unsigned char *)p;
+        }
+        base = g_count_addr[c->device];
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    unsigned long long *d_tot = (unsigned long long *)(base + kCountTotOff);
+    double *d_cs = (double *)(base + kCountCutOff);
+    int *d_cnt = (int *)(base + kCountRowOff);
+    const Cell cell = make_cell(hmat);
+    CK(cudaMemcpyAsync(d_cs, cutskin2, (size_t)c->sys.npair_typ * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(d_tot, 0, 2 * sizeof(unsigned long long), st));
+    CK(launch_list_count(c, cell, d_pos1, d_xmod, d_cs, d_cnt, st));
+    CK(launch_count_total(c, d_cnt, d_tot, st));
+    unsigned long long tot[2] = {0, 0};
+    CK(cudaMemcpyAsync(tot, d_tot, sizeof(tot), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (npairs) *npairs = (long)tot[0];
+    if (nactive) *nactive = (long)tot[1];
     return PINYB200_OK;
 }
 

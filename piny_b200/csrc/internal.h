@@ -138,6 +138,9 @@ cudaError_t launch_ghost_pos(pinyb200_ctx *c);
 cudaError_t launch_ghost_distrib(pinyb200_ctx *c);
 cudaError_t launch_transpose_in(pinyb200_ctx *c, const double *d_pos_aos);
 cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_force_aos);
+cudaError_t launch_list_count(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
+                              const double *d_cutskin2, int *d_count, cudaStream_t st);
+cudaError_t launch_count_total(pinyb200_ctx *c, const int *d_count, unsigned long long *d_tot, cudaStream_t st);
 size_t pme_plane_smem(int Na, int Nb, bool fp64);
 size_t pme_slab_smem(int Na, int Nc, bool fp64);
 

@@ -145,3 +145,65 @@ cudaError_t launch_build_list(pinyb200_ctx *c, const Cell &cell, const double *d
 }
 
 }  // namespace pinyb200
+
+namespace pinyb200 {
+
+// Count pass alone, into a caller-supplied count array [2][natm] (full,
+// active), on the given stream.  Every row's counts are written.
+cudaError_t launch_list_count(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
+                              const double *d_cutskin2, int *d_count, cudaStream_t st)
+{
+    const DeviceSystem &s = c->sys;
+    const int threads = 256;
+    int blocks = (s.natm * 32 + threads - 1) / threads;
+    const int maxb = c->sm_count * 8;
+    if (blocks > maxb) blocks = maxb;
+    list_kernel<0><<<blocks, threads, 0, st>>>(s.natm, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell, d_cutskin2,
+                                               s.atm_typ, s.charge, s.inter_map, s.has_vdw, s.excl_off, s.excl_j,
+                                               d_count, nullptr, nullptr, nullptr, nullptr, 0);
+    return cudaGetLastError();
+}
+
+// Sums of the two count arrays added into tot[0] (full) and tot[1] (active);
+// tot must hold zero before the launch.
+__global__ void __launch_bounds__(256) count_total_kernel(int n, const int *__restrict__ count,
+                                                          unsigned long long *__restrict__ tot)
+{
+    __shared__ unsigned long long part[2][8];
+    unsigned long long s0 = 0, s1 = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        s0 += (unsigned)count[i];
+        s1 += (unsigned)count[n + i];
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        part[0][w] = s0;
+        part[1][w] = s1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t0 = 0, t1 = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+            t0 += part[0][k];
+            t1 += part[1][k];
+        }
+        atomicAdd(&tot[0], t0);
+        atomicAdd(&tot[1], t1);
+    }
+}
+
+cudaError_t launch_count_total(pinyb200_ctx *c, const int *d_count, unsigned long long *d_tot, cudaStream_t st)
+{
+    const int n = c->sys.natm;
+    int blocks = (n + 255) / 256;
+    if (blocks > c->sm_count) blocks = c->sm_count;
+    if (blocks < 1) blocks = 1;
+    count_total_kernel<<<blocks, 256, 0, st>>>(n, d_count, d_tot);
+    return cudaGetLastError();
+}
+
+}  // namespace pinyb200

@@ -62,7 +62,10 @@ class PinyEnergies(C.Structure):
 EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb200_destroy",
            "pinyb200_build_list", "pinyb200_get_list", "pinyb200_list_info", "pinyb200_energy_force",
            "pinyb200_energy_force_device", "pinyb200_piny_force", "pinyb200_last_timing",
-           "pinyb200_last_error")
+           "pinyb200_last_error", "pinyb200_count_list_device")
+
+COUNT_MAX_ATOMS = 65536       # PINYB200_COUNT_MAX_ATOMS
+COUNT_MAX_PAIR_TYPES = 64     # PINYB200_COUNT_MAX_PAIR_TYPES
 
 _LIB = None
 
@@ -95,6 +98,8 @@ def load(build_if_missing: bool = True):
     L.pinyb200_piny_force.argtypes = [C.c_void_p] + [C.c_void_p] * 3 + [_pd] * 3 + [_pd] + [C.c_void_p] * 3 + \
         [_pd, C.POINTER(PinyEnergies)]
     L.pinyb200_last_timing.argtypes = [C.c_void_p, C.POINTER(C.c_float), _i]
+    L.pinyb200_count_list_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, _pd, C.POINTER(C.c_long),
+                                             C.POINTER(C.c_long), C.c_void_p]
     L.pinyb200_last_error.restype = C.c_char_p
     L.pinyb200_last_error.argtypes = [C.c_void_p]
     _LIB = L
@@ -172,6 +177,19 @@ class DeviceBox:
         self._check(self.L.pinyb200_build_list(self.h, _dp(pos1), None if xm is None else _dp(xm), _dp(hmat),
                                                _dp(cs), C.byref(n)), "build_list")
         return n.value
+
+    def count_list_device(self, d_pos1: int, d_xmod, hmat, cutskin2, stream=None):
+        """Pair counts (npairs, nactive) for device-resident bead-1 positions,
+        through the allocation-free pinyb200_count_list_device."""
+        hmat = np.ascontiguousarray(hmat, np.float64)
+        cs = np.ascontiguousarray(cutskin2, np.float64)
+        n, a = C.c_long(), C.c_long()
+        self._check(self.L.pinyb200_count_list_device(self.h, C.c_void_p(d_pos1),
+                                                      None if d_xmod is None else C.c_void_p(d_xmod), _dp(hmat),
+                                                      _dp(cs), C.byref(n), C.byref(a),
+                                                      None if stream is None else C.c_void_p(stream)),
+                    "count_list_device")
+        return n.value, a.value
 
     def get_list(self):
         n = C.c_long()

@@ -48,3 +48,9 @@ def test_header_struct_fields_in_order():
 def test_version_without_device():
     L = lib.load()
     assert L.pinyb200_version() == 1
+
+
+def test_count_scratch_limits_match_header():
+    text = open(HEADER).read()
+    assert int(re.search(r"PINYB200_COUNT_MAX_ATOMS\s*=\s*(\d+)", text).group(1)) == lib.COUNT_MAX_ATOMS
+    assert int(re.search(r"PINYB200_COUNT_MAX_PAIR_TYPES\s*=\s*(\d+)", text).group(1)) == lib.COUNT_MAX_PAIR_TYPES
