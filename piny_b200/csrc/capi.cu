@@ -193,7 +193,8 @@ int pinyb200_destroy(pinyb200_ctx *c)
     free_sys(c->sys);
     void *ptrs[] = {c->d_row, c->d_col, c->d_rowA, c->d_colA, c->d_count, c->d_tot, c->d_posT, c->d_forceT,
                     c->d_xmod, c->d_pos_aos, c->d_force_aos, c->d_acc, c->d_grid, c->d_spec, c->d_filter, c->d_twiddle64,
-                    c->d_twiddle32, c->d_err, c->d_mstart, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_chunk};
+                    c->d_twiddle32, c->d_err, c->d_mstart, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_chunk,
+                    c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i < 8; i++)
@@ -310,6 +311,17 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
         const size_t csz = f64 ? sizeof(double2) : sizeof(float2);
         CK(cudaMalloc(&c->d_grid, rsz * G * nbeads));
         CK(cudaMalloc(&c->d_spec, csz * (size_t)Nc * Nb * (Na / 2 + 1) * nbeads));
+        // charge bins per grid tile and bead; about twice the mean occupancy,
+        // the rest goes to the overflow list (which can hold every charge)
+        c->pme_nt[0] = (Na + PINYB200_PME_TILE - 1) / PINYB200_PME_TILE;
+        c->pme_nt[1] = (Nb + PINYB200_PME_TILE - 1) / PINYB200_PME_TILE;
+        c->pme_nt[2] = (Nc + PINYB200_PME_TILE - 1) / PINYB200_PME_TILE;
+        c->pme_ntile = c->pme_nt[0] * c->pme_nt[1] * c->pme_nt[2];
+        const int mean = (d.nchrg + c->pme_ntile - 1) / c->pme_ntile;
+        c->pme_cap = (2 * mean + 32 + 31) / 32 * 32;
+        CK(cudaMalloc(&c->d_pme_cnt, ((size_t)nbeads * c->pme_ntile + 1) * sizeof(int)));
+        CK(cudaMalloc(&c->d_pme_bin, (size_t)nbeads * c->pme_ntile * c->pme_cap * sizeof(int)));
+        CK(cudaMalloc(&c->d_pme_ovf, (size_t)std::max(1, d.nchrg) * nbeads * sizeof(int)));
         // twiddles exp(2 pi i m / N) per axis, 256 entries each
         std::vector<double> tw(2 * 256 * 3, 0.0);
         std::vector<float> tw32(tw.size());

@@ -113,6 +113,12 @@ struct pinyb200_ctx {
     void *d_grid = nullptr;       // [P][Nc][Nb][Na] real charge / potential grid
     void *d_spec = nullptr;       // [P][Nc][Nb][Na/2+1] complex half spectrum
     void *d_filter = nullptr;     // [G] real: preg * bweight, 0 outside the sphere
+    // charges binned by PME grid tile (PINYB200_PME_TILE points per edge)
+    int pme_nt[3] = {0, 0, 0};    // tiles per axis
+    int pme_ntile = 0, pme_cap = 0;
+    int *d_pme_cnt = nullptr;     // [P][ntile] entries per bin, then [1] overflow count
+    int *d_pme_bin = nullptr;     // [P][ntile][cap] charge numbers (index into ichrg)
+    int *d_pme_ovf = nullptr;     // [nchrg*P] overflowing (charge, bead) as k*P + b
     double *d_twiddle64 = nullptr;  // per axis twiddles
     float *d_twiddle32 = nullptr;
     int *d_err = nullptr;
@@ -124,6 +130,9 @@ struct pinyb200_ctx {
 };
 
 namespace pinyb200 {
+
+// Edge of the PME grid tiles (grid points) that charges are binned by.
+#define PINYB200_PME_TILE 16
 
 // launchers (defined in the .cu files)
 cudaError_t launch_build_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1,

@@ -16,14 +16,17 @@
 // fft_package.c:458-503); half of the full-grid sum is PINY's energy.
 //
 // Kernels per evaluation (all beads in each launch):
-//   spread      real grid, FP32 rows added with 16-byte vector atomics
+//   bin         (charge, bead) -> grid tile of its stencil origin
+//   spread      per (tile, bead): shared-memory copy of the tile, added to
+//               the real grid once (FP32: 16-byte vector atomics)
 //   plane_fwd   per (bead, c) plane: FFT along a then b in shared memory,
 //               half spectrum out
 //   conv_c      per (bead, b): FFT along c, filter + energy + virial,
 //               inverse FFT along c
 //   plane_inv   per (bead, c): inverse FFT along b, Hermitian completion,
 //               inverse FFT along a, real potential out
-//   gather      forces from the potential grid
+//   gather      per (tile, bead): forces from a shared copy of the tile's
+//               potential
 #include "common.cuh"
 
 namespace pinyb200 {
@@ -79,13 +82,13 @@ __device__ __forceinline__ void scaled(double s, int N, int &i0, double &frac)
     if (!(i0 >= 0 && i0 < N)) { i0 = 0; frac = 0.0; }
 }
 
-// Grid stencil of one charge: splines and the first (lowest) grid index per
-// axis.  PINY's points ia-(j-2), j = 1..n, are the n consecutive indices
+// First grid index per axis of one charge's stencil and the fractional
+// offsets.  PINY's points ia-(j-2), j = 1..n, are the n consecutive indices
 // ia-n+1 .. ia (wrapped), and point j carries weight m[j]; so grid index
-// lo + t (t = 0..n-1) carries m[n - t].
-template <typename R, int NI, bool DERIV>
-__device__ __forceinline__ void stencil(const PmeArgs &a, const Cell &cell, int at, int b, R *ma, R *mb, R *mc,
-                                        R *da, R *db, R *dc, int &la, int &lb, int &lc)
+// lo + t (t = 0..n-1) carries m[n - t].  The binning and both tile kernels
+// call this same FP64 code, so they agree on every charge's tile.
+__device__ __forceinline__ void stencil_origin(const PmeArgs &a, const Cell &cell, int at, int b, int ni, int &la,
+                                               int &lb, int &lc, double &fa, double &fb, double &fc)
 {
     const double x = a.posT[(3 * (size_t)at + 0) * a.P + b];
     const double y = a.posT[(3 * (size_t)at + 1) * a.P + b];
@@ -94,139 +97,230 @@ __device__ __forceinline__ void stencil(const PmeArgs &a, const Cell &cell, int 
     const double sb = __dadd_rn(__dadd_rn(__dmul_rn(x, cell.hi[1]), __dmul_rn(y, cell.hi[4])), __dmul_rn(z, cell.hi[7]));
     const double sc = __dadd_rn(__dadd_rn(__dmul_rn(x, cell.hi[2]), __dmul_rn(y, cell.hi[5])), __dmul_rn(z, cell.hi[8]));
     int ia, ib, ic;
-    double fa, fb, fc;
     scaled(sa, a.Na, ia, fa);
     scaled(sb, a.Nb, ib, fb);
     scaled(sc, a.Nc, ic, fc);
-    bspline<R, NI, DERIV>((R)fa, ma, da);
-    bspline<R, NI, DERIV>((R)fb, mb, db);
-    bspline<R, NI, DERIV>((R)fc, mc, dc);
-    la = ia - NI + 1;
+    la = ia - ni + 1;
     if (la < 0) la += a.Na;
-    lb = ib - NI + 1;
+    lb = ib - ni + 1;
     if (lb < 0) lb += a.Nb;
-    lc = ic - NI + 1;
+    lc = ic - ni + 1;
     if (lc < 0) lc += a.Nc;
 }
 
-// Add w[t] (t = 0..NI-1) to row[(lo + t) mod N].  FP32 rows go out as
-// 16-byte vector atomics over the aligned chunks the run touches (zeros in
-// the unused lanes); FP64 rows as scalar atomics.
-template <int NI>
-__device__ __forceinline__ void row_add(float *row, int N, int lo, const float *w)
+template <typename R, int NI, bool DERIV>
+__device__ __forceinline__ void stencil(const PmeArgs &a, const Cell &cell, int at, int b, R *ma, R *mb, R *mc,
+                                        R *da, R *db, R *dc, int &la, int &lb, int &lc)
 {
-    if ((N & 3) == 0) {
-        int t = 0;
-        while (t < NI) {
-            int idx = lo + t;
-            if (idx >= N) idx -= N;
-            const int base = idx & ~3;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            // fill lanes of this chunk while the run stays inside it
-            while (t < NI) {
-                int id2 = lo + t;
-                if (id2 >= N) id2 -= N;
-                if ((id2 & ~3) != base) break;
-                const int l = id2 & 3;
-                if (l == 0) v.x = w[t];
-                else if (l == 1) v.y = w[t];
-                else if (l == 2) v.z = w[t];
-                else v.w = w[t];
-                t++;
-            }
-            atomicAdd((float4 *)(row + base), v);
-        }
-    } else {
-#pragma unroll
-        for (int t = 0; t < NI; t++) {
-            int idx = lo + t;
-            if (idx >= N) idx -= N;
-            atomicAdd(row + idx, w[t]);
-        }
-    }
+    double fa, fb, fc;
+    stencil_origin(a, cell, at, b, NI, la, lb, lc, fa, fb, fc);
+    bspline<R, NI, DERIV>((R)fa, ma, da);
+    bspline<R, NI, DERIV>((R)fb, mb, db);
+    bspline<R, NI, DERIV>((R)fc, mc, dc);
 }
 
+// Charges binned by the grid tile that holds their stencil origin, per bead.
+struct TileArgs {
+    int nta, ntb, ntc, ntile, cap;
+    int *cnt;  // [P][ntile], then the overflow count
+    int *bin;  // [P][ntile][cap]
+    int *ovf;  // [nchrg * P]
+};
+
+// Tile geometry: T^3 grid points own the charges whose stencil starts in
+// them; the shared copy spans E = T + NI - 1 points per edge (the stencils
+// reach NI - 1 beyond), rows padded to PA.
 template <int NI>
-__device__ __forceinline__ void row_add(double *row, int N, int lo, const double *w)
+struct TileGeom {
+    static constexpr int T = PINYB200_PME_TILE;
+    static constexpr int E = T + NI - 1;
+    static constexpr int PA = (E + 3) & ~3;
+    static constexpr int NPT = E * E * PA;
+};
+
+__device__ __forceinline__ int wrapi(int i, int N) { return i >= N ? i - N : i; }
+
+template <int NI>
+__global__ void __launch_bounds__(256) pme_bin_kernel(PmeArgs a, Cell cell, TileArgs t)
 {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)a.nchrg * a.P) return;
+    const int b = (int)(idx % a.P);
+    const int k = (int)(idx / a.P);
+    int la, lb, lc;
+    double fa, fb, fc;
+    stencil_origin(a, cell, a.ichrg[k], b, NI, la, lb, lc, fa, fb, fc);
+    const int T = PINYB200_PME_TILE;
+    const int tile = ((lc / T) * t.ntb + lb / T) * t.nta + la / T;
+    const int slot = atomicAdd(&t.cnt[b * t.ntile + tile], 1);
+    if (slot < t.cap) t.bin[((size_t)b * t.ntile + tile) * t.cap + slot] = k;
+    else t.ovf[atomicAdd(&t.cnt[a.P * t.ntile], 1)] = (int)idx;
+}
+
+// The a-weights of lane l8 of an 8-lane group: grid points lo + l8 and
+// lo + l8 + 8 (orders above 8), picked with static indices.
+template <typename R, int NI>
+__device__ __forceinline__ void lane_weights(const R *m, int l8, R &w0, R &w1)
+{
+    w0 = (R)0;
+    w1 = (R)0;
 #pragma unroll
     for (int t = 0; t < NI; t++) {
-        int idx = lo + t;
-        if (idx >= N) idx -= N;
-        atomicAdd(row + idx, w[t]);
+        if (t == l8) w0 = m[NI - t];
+        if (t == l8 + 8) w1 = m[NI - t];
     }
 }
 
+// Spread one charge of bead b straight into the global grid (overflow
+// entries); the 8 lanes of the group share the a points.
 template <typename R, int NI>
-__global__ void __launch_bounds__(256) spread_kernel(PmeArgs a, Cell cell)
+__device__ __forceinline__ void spread_global(const PmeArgs &a, R *g, int la, int lb, int lc, R wa0, R wa1,
+                                              const R *mb, const R *mc, R q, int l8)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)a.nchrg * a.P) return;
-    const int b = (int)(t % a.P);
-    const int at = a.ichrg[t / a.P];
-    R ma[NI + 1], mb[NI + 1], mc[NI + 1];
-    int la, lb, lc;
-    stencil<R, NI, false>(a, cell, at, b, ma, mb, mc, nullptr, nullptr, nullptr, la, lb, lc);
-    const R q = (R)a.charge[at];
-    R *g = (R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
+    const int ga0 = wrapi(la + l8, a.Na), ga1 = wrapi(la + l8 + 8, a.Na);
+#pragma unroll
     for (int tc = 0; tc < NI; tc++) {
-        int gc = lc + tc;
-        if (gc >= a.Nc) gc -= a.Nc;
+        const int gc = wrapi(lc + tc, a.Nc);
         const R qc = q * mc[NI - tc];
-        for (int tb = 0; tb < NI; tb++) {
-            int gb = lb + tb;
-            if (gb >= a.Nb) gb -= a.Nb;
-            const R qbc = mb[NI - tb] * qc;
-            R w[NI];
 #pragma unroll
-            for (int ta = 0; ta < NI; ta++) w[ta] = ma[NI - ta] * qbc;
-            row_add<NI>(g + ((size_t)gc * a.Nb + gb) * a.Na, a.Na, la, w);
+        for (int tb = 0; tb < NI; tb++) {
+            const int gb = wrapi(lb + tb, a.Nb);
+            const R w = mb[NI - tb] * qc;
+            R *row = g + ((size_t)gc * a.Nb + gb) * a.Na;
+            if (l8 < NI) atomicAdd(row + ga0, wa0 * w);
+            if (NI > 8 && l8 + 8 < NI) atomicAdd(row + ga1, wa1 * w);
         }
     }
 }
 
+// Spread: one block per (tile, bead).  The charges of the bin go into a
+// shared copy of the tile with shared-memory atomics (8 lanes per charge,
+// one lane per a point), then the copy is added to the grid once, with
+// 16-byte vector atomics where the rows allow.  Overflow entries are shared
+// out over all blocks and go straight to the grid.
 template <typename R, int NI>
-__global__ void __launch_bounds__(256) gather_kernel(PmeArgs a, Cell cell)
+__global__ void __launch_bounds__(256) spread_tile_kernel(PmeArgs a, Cell cell, TileArgs t)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)a.nchrg * a.P) return;
-    const int b = (int)(t % a.P);
-    const int at = a.ichrg[t / a.P];
-    R ma[NI + 1], mb[NI + 1], mc[NI + 1], da[NI + 1], db[NI + 1], dc[NI + 1];
-    int la, lb, lc;
-    stencil<R, NI, true>(a, cell, at, b, ma, mb, mc, da, db, dc, la, lb, lc);
-    const double q = a.charge[at];
-    const R *g = (const R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
-    // separable sums: d/ds_a, d/ds_b, d/ds_c of sum M_a M_b M_c phi
-    double ea = 0.0, eb = 0.0, ec = 0.0;
-    for (int tc = 0; tc < NI; tc++) {
-        int gc = lc + tc;
-        if (gc >= a.Nc) gc -= a.Nc;
-        R sa_c = 0, sda_c = 0, sdb_c = 0;
-        for (int tb = 0; tb < NI; tb++) {
-            int gb = lb + tb;
-            if (gb >= a.Nb) gb -= a.Nb;
-            const R *rowp = g + ((size_t)gc * a.Nb + gb) * a.Na;
-            R s0 = 0, s1 = 0;
+    typedef TileGeom<NI> TG;
+    extern __shared__ unsigned char smem_raw[];
+    R *tl = (R *)smem_raw;
+    for (int i = threadIdx.x; i < TG::NPT; i += blockDim.x) tl[i] = (R)0;
+    __syncthreads();
+    const int tile = blockIdx.x, b = blockIdx.y;
+    const int ta0 = (tile % t.nta) * TG::T, tb0 = ((tile / t.nta) % t.ntb) * TG::T, tc0 = (tile / (t.nta * t.ntb)) * TG::T;
+    const int grp = threadIdx.x >> 3, l8 = threadIdx.x & 7, ngrp = blockDim.x >> 3;
+    const int n = min(t.cnt[b * t.ntile + tile], t.cap);
+    const int *list = t.bin + ((size_t)b * t.ntile + tile) * t.cap;
+    R *g = (R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
+    for (int e = grp; e < n; e += ngrp) {
+        const int at = a.ichrg[list[e]];
+        R ma[NI + 1], mb[NI + 1], mc[NI + 1];
+        int la, lb, lc;
+        stencil<R, NI, false>(a, cell, at, b, ma, mb, mc, nullptr, nullptr, nullptr, la, lb, lc);
+        const R q = (R)a.charge[at];
+        R wa0, wa1;
+        lane_weights<R, NI>(ma, l8, wa0, wa1);
+        const int oa = la - ta0, ob = lb - tb0, oc = lc - tc0;
+        if (oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T) {
 #pragma unroll
-            for (int ta = 0; ta < NI; ta++) {
-                int ga = la + ta;
-                if (ga >= a.Na) ga -= a.Na;
-                const R phi = __ldg(rowp + ga);
-                s0 += ma[NI - ta] * phi;
-                s1 += da[NI - ta] * phi;
+            for (int tc = 0; tc < NI; tc++) {
+                const R qc = q * mc[NI - tc];
+#pragma unroll
+                for (int tb = 0; tb < NI; tb++) {
+                    const R w = mb[NI - tb] * qc;
+                    R *row = tl + ((oc + tc) * TG::E + (ob + tb)) * TG::PA + oa;
+                    if (l8 < NI) atomicAdd(row + l8, wa0 * w);
+                    if (NI > 8 && l8 + 8 < NI) atomicAdd(row + l8 + 8, wa1 * w);
+                }
             }
-            sa_c += mb[NI - tb] * s0;   // for the c derivative
-            sda_c += mb[NI - tb] * s1;  // for the a derivative
-            sdb_c += db[NI - tb] * s0;  // for the b derivative
+        } else {
+            spread_global<R, NI>(a, g, la, lb, lc, wa0, wa1, mb, mc, q, l8);
         }
-        ea += (double)(mc[NI - tc] * sda_c);
-        eb += (double)(mc[NI - tc] * sdb_c);
-        ec += (double)(dc[NI - tc] * sa_c);
     }
+    const int nov = t.cnt[a.P * t.ntile];
+    const int gid = blockIdx.y * gridDim.x + blockIdx.x, nblk = gridDim.x * gridDim.y;
+    for (int e = gid * ngrp + grp; e < nov; e += nblk * ngrp) {
+        const int idx = t.ovf[e];
+        const int b2 = idx % a.P, at = a.ichrg[idx / a.P];
+        R ma[NI + 1], mb[NI + 1], mc[NI + 1];
+        int la, lb, lc;
+        stencil<R, NI, false>(a, cell, at, b2, ma, mb, mc, nullptr, nullptr, nullptr, la, lb, lc);
+        R wa0, wa1;
+        lane_weights<R, NI>(ma, l8, wa0, wa1);
+        R *g2 = (R *)a.grid + (size_t)b2 * a.Na * a.Nb * a.Nc;
+        spread_global<R, NI>(a, g2, la, lb, lc, wa0, wa1, mb, mc, (R)a.charge[at], l8);
+    }
+    __syncthreads();
+    // add the shared copy to the grid
+    constexpr int NQ = TG::PA / 4;
+    if (sizeof(R) == 4 && (a.Na & 3) == 0) {
+        for (int i = threadIdx.x; i < TG::E * TG::E * NQ; i += blockDim.x) {
+            const int row = i / NQ, q4 = i % NQ;
+            const int cz = row / TG::E, by = row % TG::E;
+            const float4 v = ((const float4 *)tl)[i];
+            if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
+            const int gc = (tc0 + cz) % a.Nc, gb = (tb0 + by) % a.Nb, ga = (ta0 + 4 * q4) % a.Na;
+            atomicAdd((float4 *)((float *)g + ((size_t)gc * a.Nb + gb) * a.Na + ga), v);
+        }
+    } else {
+        for (int i = threadIdx.x; i < TG::NPT; i += blockDim.x) {
+            const R v = tl[i];
+            if (v == (R)0) continue;
+            const int row = i / TG::PA, ax = i % TG::PA;
+            const int cz = row / TG::E, by = row % TG::E;
+            const int gc = (tc0 + cz) % a.Nc, gb = (tb0 + by) % a.Nb, ga = (ta0 + ax) % a.Na;
+            atomicAdd(g + ((size_t)gc * a.Nb + gb) * a.Na + ga, v);
+        }
+    }
+}
+
+// Gather sums of one charge for lane l8: d/ds_a, d/ds_b, d/ds_c of
+// sum M_a M_b M_c phi over the lane's a points; phi(tc, tb, ta) reads the
+// potential at stencil point (tc, tb, ta).
+template <typename R, int NI, typename PHI>
+__device__ __forceinline__ void gather_lane(PHI phi, R wa0, R wa1, R wd0, R wd1, const R *mb, const R *db,
+                                            const R *mc, const R *dc, int l8, double &ea, double &eb, double &ec)
+{
+    ea = eb = ec = 0.0;
+    if (l8 >= NI) return;
+#pragma unroll
+    for (int tc = 0; tc < NI; tc++) {
+        R um = 0, udm = 0, udb = 0;
+#pragma unroll
+        for (int tb = 0; tb < NI; tb++) {
+            const R p0 = phi(tc, tb, l8);
+            R s0 = wa0 * p0, s1 = wd0 * p0;
+            if (NI > 8 && l8 + 8 < NI) {
+                const R p1 = phi(tc, tb, l8 + 8);
+                s0 += wa1 * p1;
+                s1 += wd1 * p1;
+            }
+            um += mb[NI - tb] * s0;
+            udm += mb[NI - tb] * s1;
+            udb += db[NI - tb] * s0;
+        }
+        ea += (double)(mc[NI - tc] * udm);
+        eb += (double)(mc[NI - tc] * udb);
+        ec += (double)(dc[NI - tc] * um);
+    }
+}
+
+// Force of one charge from its three sums (summed over the 8-lane group;
+// lane 0 writes): F = -q h^-T (N_a e_a, N_b e_b, N_c e_c).
+__device__ __forceinline__ void gather_store(const PmeArgs &a, const Cell &cell, int at, int b, double ea, double eb,
+                                             double ec, int l8)
+{
+#pragma unroll
+    for (int o = 4; o >= 1; o >>= 1) {
+        ea += __shfl_xor_sync(0xffffffffu, ea, o);
+        eb += __shfl_xor_sync(0xffffffffu, eb, o);
+        ec += __shfl_xor_sync(0xffffffffu, ec, o);
+    }
+    if (l8 != 0) return;
     ea *= (double)a.Na;
     eb *= (double)a.Nb;
     ec *= (double)a.Nc;
+    const double q = a.charge[at];
     const double gx = ea * cell.hi[0] + eb * cell.hi[1] + ec * cell.hi[2];
     const double gy = ea * cell.hi[3] + eb * cell.hi[4] + ec * cell.hi[5];
     const double gz = ea * cell.hi[6] + eb * cell.hi[7] + ec * cell.hi[8];
@@ -234,6 +328,97 @@ __global__ void __launch_bounds__(256) gather_kernel(PmeArgs a, Cell cell)
     f[(3 * (size_t)at + 0) * a.P + b] -= gx * q;
     f[(3 * (size_t)at + 1) * a.P + b] -= gy * q;
     f[(3 * (size_t)at + 2) * a.P + b] -= gz * q;
+}
+
+// Gather: one block per (tile, bead); the tile's potential (with the
+// stencil reach) is copied to shared memory once and the bin's charges read
+// it there.  Overflow entries read the grid directly.  Every (charge, bead)
+// is handled by exactly one 8-lane group, so the force update needs no
+// atomics.
+template <typename R, int NI>
+__global__ void __launch_bounds__(256) gather_tile_kernel(PmeArgs a, Cell cell, TileArgs t)
+{
+    typedef TileGeom<NI> TG;
+    extern __shared__ unsigned char smem_raw[];
+    R *tl = (R *)smem_raw;
+    const int tile = blockIdx.x, b = blockIdx.y;
+    const int ta0 = (tile % t.nta) * TG::T, tb0 = ((tile / t.nta) % t.ntb) * TG::T, tc0 = (tile / (t.nta * t.ntb)) * TG::T;
+    const R *g = (const R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
+    const int n = min(t.cnt[b * t.ntile + tile], t.cap);
+    if (n > 0) {
+        for (int i = threadIdx.x; i < TG::NPT; i += blockDim.x) {
+            const int row = i / TG::PA, ax = i % TG::PA;
+            const int cz = row / TG::E, by = row % TG::E;
+            R v = (R)0;
+            if (ax < TG::E) {
+                const int gc = (tc0 + cz) % a.Nc, gb = (tb0 + by) % a.Nb, ga = (ta0 + ax) % a.Na;
+                v = g[((size_t)gc * a.Nb + gb) * a.Na + ga];
+            }
+            tl[i] = v;
+        }
+    }
+    __syncthreads();
+    const int grp = threadIdx.x >> 3, l8 = threadIdx.x & 7, ngrp = blockDim.x >> 3;
+    const int *list = t.bin + ((size_t)b * t.ntile + tile) * t.cap;
+    // every lane of a warp takes part in the group reductions: loop to the
+    // same trip count in all groups of the warp
+    const int nr = (n + ngrp - 1) / ngrp;
+    for (int r = 0; r < nr; r++) {
+        const int e = r * ngrp + grp;
+        const bool act = e < n;
+        const int at = act ? a.ichrg[list[e]] : 0;
+        double ea = 0, eb = 0, ec = 0;
+        if (act) {
+            R ma[NI + 1], mb[NI + 1], mc[NI + 1], da[NI + 1], db[NI + 1], dc[NI + 1];
+            int la, lb, lc;
+            stencil<R, NI, true>(a, cell, at, b, ma, mb, mc, da, db, dc, la, lb, lc);
+            R wa0, wa1, wd0, wd1;
+            lane_weights<R, NI>(ma, l8, wa0, wa1);
+            lane_weights<R, NI>(da, l8, wd0, wd1);
+            const int oa = la - ta0, ob = lb - tb0, oc = lc - tc0;
+            if (oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T) {
+                const R *base = tl + (oc * TG::E + ob) * TG::PA + oa;
+                gather_lane<R, NI>([&](int tc, int tb, int ta) { return base[(tc * TG::E + tb) * TG::PA + ta]; },
+                                   wa0, wa1, wd0, wd1, mb, db, mc, dc, l8, ea, eb, ec);
+            } else {
+                gather_lane<R, NI>(
+                    [&](int tc, int tb, int ta) {
+                        return g[((size_t)wrapi(lc + tc, a.Nc) * a.Nb + wrapi(lb + tb, a.Nb)) * a.Na +
+                                 wrapi(la + ta, a.Na)];
+                    },
+                    wa0, wa1, wd0, wd1, mb, db, mc, dc, l8, ea, eb, ec);
+            }
+        }
+        gather_store(a, cell, at, b, ea, eb, ec, act ? l8 : 1);
+    }
+    const int nov = t.cnt[a.P * t.ntile];
+    const int gid = blockIdx.y * gridDim.x + blockIdx.x, nblk = gridDim.x * gridDim.y;
+    const int nr2 = (nov + nblk * ngrp - 1) / (nblk * ngrp);
+    for (int r = 0; r < nr2; r++) {
+        const int e = (r * nblk + gid) * ngrp + grp;
+        const bool act = e < nov;
+        int at = 0, b2 = 0;
+        double ea = 0, eb = 0, ec = 0;
+        if (act) {
+            const int idx = t.ovf[e];
+            b2 = idx % a.P;
+            at = a.ichrg[idx / a.P];
+            R ma[NI + 1], mb[NI + 1], mc[NI + 1], da[NI + 1], db[NI + 1], dc[NI + 1];
+            int la, lb, lc;
+            stencil<R, NI, true>(a, cell, at, b2, ma, mb, mc, da, db, dc, la, lb, lc);
+            R wa0, wa1, wd0, wd1;
+            lane_weights<R, NI>(ma, l8, wa0, wa1);
+            lane_weights<R, NI>(da, l8, wd0, wd1);
+            const R *g2 = (const R *)a.grid + (size_t)b2 * a.Na * a.Nb * a.Nc;
+            gather_lane<R, NI>(
+                [&](int tc, int tb, int ta) {
+                    return g2[((size_t)wrapi(lc + tc, a.Nc) * a.Nb + wrapi(lb + tb, a.Nb)) * a.Na +
+                              wrapi(la + ta, a.Na)];
+                },
+                wa0, wa1, wd0, wd1, mb, db, mc, dc, l8, ea, eb, ec);
+        }
+        gather_store(a, cell, at, b2, ea, eb, ec, act ? l8 : 1);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -525,9 +710,29 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     const bool f64 = sizeof(R) == 8;
     cudaError_t err = cudaMemsetAsync(c->d_grid, 0, sizeof(R) * G * c->P, c->stream);
     if (err != cudaSuccess) return err;
+    TileArgs t;
+    t.nta = c->pme_nt[0];
+    t.ntb = c->pme_nt[1];
+    t.ntc = c->pme_nt[2];
+    t.ntile = c->pme_ntile;
+    t.cap = c->pme_cap;
+    t.cnt = c->d_pme_cnt;
+    t.bin = c->d_pme_bin;
+    t.ovf = c->d_pme_ovf;
+    err = cudaMemsetAsync(t.cnt, 0, ((size_t)a.P * t.ntile + 1) * sizeof(int), c->stream);
+    if (err != cudaSuccess) return err;
     const long long nt = (long long)a.nchrg * a.P;
     const int threads = 256;
-    spread_kernel<R, NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell);
+    pme_bin_kernel<NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell, t);
+    const size_t st = (size_t)TileGeom<NI>::NPT * sizeof(R);
+    if (st > 48 * 1024) {
+        err = cudaFuncSetAttribute(spread_tile_kernel<R, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(gather_tile_kernel<R, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st);
+        if (err != cudaSuccess) return err;
+    }
+    const dim3 tgrid((unsigned)t.ntile, (unsigned)a.P);
+    spread_tile_kernel<R, NI><<<tgrid, 256, st, c->stream>>>(a, cell, t);
     const R *twbase = (const R *)(f64 ? (const void *)c->d_twiddle64 : (const void *)c->d_twiddle32);
     const R *tw[3] = {twbase, twbase + 2 * 256, twbase + 4 * 256};
     const size_t sp = pme_plane_smem(a.Na, a.Nb, f64), ss = pme_slab_smem(a.Na, a.Nc, f64);
@@ -548,7 +753,7 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     conv_c_kernel<R><<<a.P * a.Nb, 256, ss, c->stream>>>(spec, filt, a.Na, a.Nb, a.Nc, tw[2], cell, c->alp_ewd,
                                                           c->d_acc, energy ? 1 : 0);
     plane_inv_kernel<R><<<a.P * a.Nc, 256, sp, c->stream>>>(spec, (R *)c->d_grid, a.Na, a.Nb, a.Nc, tw[0], tw[1]);
-    gather_kernel<R, NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell);
+    gather_tile_kernel<R, NI><<<tgrid, 256, st, c->stream>>>(a, cell, t);
     return cudaGetLastError();
 }
 
