@@ -424,49 +424,144 @@ __global__ void __launch_bounds__(256) gather_tile_kernel(PmeArgs a, Cell cell, 
 // ---------------------------------------------------------------------------
 // In-place FFTs of `nl` lines of length N held in shared memory: element n of
 // line l at sm[l * ls + n * es].  Unnormalised, exp(sign 2 pi i n k / N);
-// tw[2m], tw[2m+1] = cos, sin(2 pi m / N).  Power-of-two lengths use an
-// iterative radix-2 decimation in time; other lengths a direct DFT done a
-// block of lines at a time.  Every thread of the block must call these.
+// tw[2m], tw[2m+1] = cos, sin(2 pi m / N).  Power-of-two lengths up to 256
+// use Stockham autosort passes of radix 8 and 4 (16 = 4x4, 32 = 8x4,
+// 64 = 8x8, 128 = 8x4x4, 256 = 8x8x4): one butterfly per thread and pass,
+// read into registers, barrier, written back in place.  Other lengths use a
+// direct DFT done a block of lines at a time.  Every thread of the block
+// must call these.
+
+// R-point DFT in registers, exp(SIGN 2 pi i r k / R), R = 2, 4, 8.
+template <typename R, int RAD, int SIGN>
+__device__ __forceinline__ void dft_small(typename Cplx<R>::T *v)
+{
+    typedef typename Cplx<R>::T C2;
+    if (RAD == 2) {
+        const C2 a = v[0], b = v[1];
+        v[0].x = a.x + b.x;
+        v[0].y = a.y + b.y;
+        v[1].x = a.x - b.x;
+        v[1].y = a.y - b.y;
+    } else if (RAD == 4) {
+        const R s = (R)SIGN;
+        const C2 t0 = {v[0].x + v[2].x, v[0].y + v[2].y}, t1 = {v[0].x - v[2].x, v[0].y - v[2].y};
+        const C2 t2 = {v[1].x + v[3].x, v[1].y + v[3].y};
+        // (v1 - v3) * (SIGN i)
+        const C2 t3 = {-s * (v[1].y - v[3].y), s * (v[1].x - v[3].x)};
+        v[0].x = t0.x + t2.x;
+        v[0].y = t0.y + t2.y;
+        v[2].x = t0.x - t2.x;
+        v[2].y = t0.y - t2.y;
+        v[1].x = t1.x + t3.x;
+        v[1].y = t1.y + t3.y;
+        v[3].x = t1.x - t3.x;
+        v[3].y = t1.y - t3.y;
+    } else {
+        // radix 2 over two 4-point DFTs: X_k = E_k + w^k O_k, X_k+4 = E_k - w^k O_k
+        C2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+        dft_small<R, 4, SIGN>(e);
+        dft_small<R, 4, SIGN>(o);
+        const R s = (R)SIGN, h = (R)0.70710678118654752440;  // cos(pi/4)
+        C2 w[4];
+        w[0] = o[0];
+        w[1] = {h * (o[1].x - s * o[1].y), h * (o[1].y + s * o[1].x)};   // (1 + s i) / sqrt 2
+        w[2] = {-s * o[2].y, s * o[2].x};                                  // s i
+        w[3] = {h * (-o[3].x - s * o[3].y), h * (-o[3].y + s * o[3].x)};  // (-1 + s i) / sqrt 2
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            v[k].x = e[k].x + w[k].x;
+            v[k].y = e[k].y + w[k].y;
+            v[k + 4].x = e[k].x - w[k].x;
+            v[k + 4].y = e[k].y - w[k].y;
+        }
+    }
+}
+
+__host__ __device__ constexpr int stockham_radix(int rem) { return rem == 16 ? 4 : (rem % 8 == 0 ? 8 : rem); }
+__host__ __device__ constexpr int stockham_min_radix(int n, int ns)
+{
+    return ns >= n ? 8 : (stockham_radix(n / ns) < stockham_min_radix(n, ns * stockham_radix(n / ns))
+                              ? stockham_radix(n / ns)
+                              : stockham_min_radix(n, ns * stockham_radix(n / ns)));
+}
+
+// One Stockham pass (stride NS) over lines l0 .. l0+nlg-1, then the next.
+template <typename R, int N, int NS, int SIGN>
+__device__ __forceinline__ void stockham_pass(typename Cplx<R>::T *sm, int l0, int nlg, int ls, int es, const R *tw)
+{
+    typedef typename Cplx<R>::T C2;
+    constexpr int RAD = stockham_radix(N / NS);
+    constexpr int BPL = N / RAD;  // butterflies per line
+    const int l = threadIdx.x / BPL, j = threadIdx.x % BPL;
+    const bool act = l < nlg;
+    C2 v[RAD];
+    C2 *p = sm + (size_t)(l0 + (act ? l : 0)) * ls;
+    if (act) {
+#pragma unroll
+        for (int r = 0; r < RAD; r++) v[r] = p[(j + r * BPL) * es];
+        if (NS > 1) {
+            const int k = j % NS;
+#pragma unroll
+            for (int r = 1; r < RAD; r++) {
+                const int m = r * k * (N / (NS * RAD));
+                const R wr = tw[2 * m], wi = (R)SIGN * tw[2 * m + 1];
+                const R xr = v[r].x * wr - v[r].y * wi, xi = v[r].x * wi + v[r].y * wr;
+                v[r].x = xr;
+                v[r].y = xi;
+            }
+        }
+        dft_small<R, RAD, SIGN>(v);
+    }
+    __syncthreads();
+    if (act) {
+        const int d = (j / NS) * NS * RAD + j % NS;
+#pragma unroll
+        for (int r = 0; r < RAD; r++) p[(d + r * NS) * es] = v[r];
+    }
+    __syncthreads();
+    if constexpr (NS * RAD < N) stockham_pass<R, N, NS * RAD, SIGN>(sm, l0, nlg, ls, es, tw);
+}
+
+template <typename R, int N, int SIGN>
+__device__ __forceinline__ void fft_pow2_inl(typename Cplx<R>::T *sm, int nl, int ls, int es, const R *tw)
+{
+    constexpr int BPLMAX = N / stockham_min_radix(N, 1);
+    const int G = (int)blockDim.x / BPLMAX > 0 ? (int)blockDim.x / BPLMAX : 1;  // lines per round
+    for (int l0 = 0; l0 < nl; l0 += G) stockham_pass<R, N, 1, SIGN>(sm, l0, min(G, nl - l0), ls, es, tw);
+}
+
+// Out-of-line copy for kernels whose lengths are known only at run time.
+template <typename R, int N, int SIGN>
+__device__ __noinline__ void fft_pow2(typename Cplx<R>::T *sm, int nl, int ls, int es, const R *tw)
+{
+    fft_pow2_inl<R, N, SIGN>(sm, nl, ls, es, tw);
+}
+
+template <typename R, int SIGN>
+__device__ bool fft_pow2_dispatch(typename Cplx<R>::T *sm, int N, int nl, int ls, int es, const R *tw)
+{
+    switch (N) {
+    case 2: fft_pow2<R, 2, SIGN>(sm, nl, ls, es, tw); return true;
+    case 4: fft_pow2<R, 4, SIGN>(sm, nl, ls, es, tw); return true;
+    case 8: fft_pow2<R, 8, SIGN>(sm, nl, ls, es, tw); return true;
+    case 16: fft_pow2<R, 16, SIGN>(sm, nl, ls, es, tw); return true;
+    case 32: fft_pow2<R, 32, SIGN>(sm, nl, ls, es, tw); return true;
+    case 64: fft_pow2<R, 64, SIGN>(sm, nl, ls, es, tw); return true;
+    case 128: fft_pow2<R, 128, SIGN>(sm, nl, ls, es, tw); return true;
+    case 256: fft_pow2<R, 256, SIGN>(sm, nl, ls, es, tw); return true;
+    default: return false;
+    }
+}
+
 template <typename R>
 __device__ void smem_fft(typename Cplx<R>::T *sm, int N, int nl, int ls, int es, const R *tw, int sign)
 {
     typedef typename Cplx<R>::T C2;
     const int nt = blockDim.x;
-    if ((N & (N - 1)) == 0) {
-        int logn = 0;
-        while ((1 << logn) < N) logn++;
-        if (logn > 0) {
-            for (int idx = threadIdx.x; idx < nl * N; idx += nt) {
-                const int l = idx / N, n = idx % N;
-                const int r = __brev(n) >> (32 - logn);
-                if (n < r) {
-                    C2 *p = sm + l * ls;
-                    C2 u = p[n * es];
-                    p[n * es] = p[r * es];
-                    p[r * es] = u;
-                }
-            }
-            __syncthreads();
-        }
-        for (int half = 1; half < N; half <<= 1) {
-            const int tstep = N / (2 * half);
-            for (int idx = threadIdx.x; idx < nl * (N / 2); idx += nt) {
-                const int l = idx / (N / 2);
-                const int bf = idx % (N / 2);
-                const int k = bf % half;
-                const int i0 = (bf / half) * 2 * half + k, i1 = i0 + half;
-                const R wr = tw[2 * (k * tstep)], wi = (R)sign * tw[2 * (k * tstep) + 1];
-                C2 *p = sm + l * ls;
-                const C2 u = p[i0 * es], v = p[i1 * es];
-                const R vr = v.x * wr - v.y * wi, vi = v.x * wi + v.y * wr;
-                p[i0 * es].x = u.x + vr;
-                p[i0 * es].y = u.y + vi;
-                p[i1 * es].x = u.x - vr;
-                p[i1 * es].y = u.y - vi;
-            }
-            __syncthreads();
-        }
-    } else {
+    if (N == 1) return;
+    if (sign > 0 ? fft_pow2_dispatch<R, 1>(sm, N, nl, ls, es, tw) : fft_pow2_dispatch<R, -1>(sm, N, nl, ls, es, tw))
+        return;
+    {
         const int per = nt / N;  // lines per pass
         for (int l0 = 0; l0 < nl; l0 += per) {
             const int l = l0 + threadIdx.x / N, k = threadIdx.x % N;
@@ -492,6 +587,18 @@ __device__ void smem_fft(typename Cplx<R>::T *sm, int N, int nl, int ls, int es,
     }
 }
 
+// FFT of length NF known at compile time (NF > 0), else run-time N.
+template <typename R, int NF>
+__device__ __forceinline__ void line_fft(typename Cplx<R>::T *sm, int N, int nl, int ls, int es, const R *tw, int sign)
+{
+    if constexpr (NF > 0) {
+        if (sign > 0) fft_pow2_inl<R, NF, 1>(sm, nl, ls, es, tw);
+        else fft_pow2_inl<R, NF, -1>(sm, nl, ls, es, tw);
+    } else {
+        smem_fft<R>(sm, N, nl, ls, es, tw, sign);
+    }
+}
+
 template <typename R>
 __device__ __forceinline__ void load_twiddles(R *dst, const R *src, int N)
 {
@@ -500,11 +607,13 @@ __device__ __forceinline__ void load_twiddles(R *dst, const R *src, int N)
 
 // Forward transform of one (bead, c) plane along a then b; half spectrum
 // (a <= Na/2) out.  Shared: plane [Nb][Na+1] complex, twiddles.
-template <typename R>
-__global__ void __launch_bounds__(256) plane_fwd_kernel(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
+template <typename R, int NF>
+__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) plane_fwd_kernel(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
                                                         int Na, int Nb, int Nc, const R *__restrict__ twa,
                                                         const R *__restrict__ twb)
 {
+    if (NF > 0) Na = Nb = NF;  // cubic power-of-two grid known at compile time
+    (void)Nc;
     typedef typename Cplx<R>::T C2;
     extern __shared__ unsigned char smem_raw[];
     C2 *pl = (C2 *)smem_raw;
@@ -523,8 +632,8 @@ __global__ void __launch_bounds__(256) plane_fwd_kernel(const R *__restrict__ q,
         pl[(idx / Na) * ls + idx % Na] = v;
     }
     __syncthreads();
-    smem_fft<R>(pl, Na, Nb, ls, 1, ta, +1);   // along a, every row
-    smem_fft<R>(pl, Nb, Nh, 1, ls, tb, +1);   // along b, columns a <= Na/2
+    line_fft<R, NF>(pl, Na, Nb, ls, 1, ta, +1);   // along a, every row
+    line_fft<R, NF>(pl, Nb, Nh, 1, ls, tb, +1);   // along b, columns a <= Na/2
     C2 *dst = spec + plane * (size_t)Nb * Nh;
     for (int idx = threadIdx.x; idx < Nb * Nh; idx += blockDim.x) dst[idx] = pl[(idx / Nh) * ls + idx % Nh];
 }
@@ -532,11 +641,13 @@ __global__ void __launch_bounds__(256) plane_fwd_kernel(const R *__restrict__ q,
 // Inverse of plane_fwd: half spectrum in, along b, Hermitian completion of
 // each row (U(Na-a) = conj U(a) once b and c are back in real space), along
 // a, real part out.
-template <typename R>
-__global__ void __launch_bounds__(256) plane_inv_kernel(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phi,
+template <typename R, int NF>
+__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) plane_inv_kernel(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phi,
                                                         int Na, int Nb, int Nc, const R *__restrict__ twa,
                                                         const R *__restrict__ twb)
 {
+    if (NF > 0) Na = Nb = NF;  // cubic power-of-two grid known at compile time
+    (void)Nc;
     typedef typename Cplx<R>::T C2;
     extern __shared__ unsigned char smem_raw[];
     C2 *pl = (C2 *)smem_raw;
@@ -550,7 +661,7 @@ __global__ void __launch_bounds__(256) plane_inv_kernel(const typename Cplx<R>::
     const C2 *src = spec + plane * (size_t)Nb * Nh;
     for (int idx = threadIdx.x; idx < Nb * Nh; idx += blockDim.x) pl[(idx / Nh) * ls + idx % Nh] = src[idx];
     __syncthreads();
-    smem_fft<R>(pl, Nb, Nh, 1, ls, tb, -1);
+    line_fft<R, NF>(pl, Nb, Nh, 1, ls, tb, -1);
     for (int idx = threadIdx.x; idx < Nb * Na; idx += blockDim.x) {
         const int b = idx / Na, a = idx % Na;
         if (a >= Nh) {
@@ -560,7 +671,7 @@ __global__ void __launch_bounds__(256) plane_inv_kernel(const typename Cplx<R>::
         }
     }
     __syncthreads();
-    smem_fft<R>(pl, Na, Nb, ls, 1, ta, -1);
+    line_fft<R, NF>(pl, Na, Nb, ls, 1, ta, -1);
     R *dst = phi + plane * Na * Nb;
     for (int idx = threadIdx.x; idx < Na * Nb; idx += blockDim.x) dst[idx] = pl[(idx / Na) * ls + idx % Na].x;
 }
@@ -569,11 +680,12 @@ __global__ void __launch_bounds__(256) plane_inv_kernel(const typename Cplx<R>::
 // of the k-sphere terms (ewald3d_pme.c:366-425), multiplication by the
 // influence function, inverse FFT along c.  Half-spectrum points with
 // 0 < a < Na/2 stand for two full-grid points; E = 1/2 sum_full w |S|^2.
-template <typename R>
-__global__ void __launch_bounds__(256) conv_c_kernel(typename Cplx<R>::T *__restrict__ spec, const R *__restrict__ filt,
+template <typename R, int NF>
+__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) conv_c_kernel(typename Cplx<R>::T *__restrict__ spec, const R *__restrict__ filt,
                                                      int Na, int Nb, int Nc, const R *__restrict__ twc, Cell cell,
                                                      double alp, double *__restrict__ acc, int energy)
 {
+    if (NF > 0) Na = Nb = Nc = NF;  // cubic power-of-two grid known at compile time
     typedef typename Cplx<R>::T C2;
     extern __shared__ unsigned char smem_raw[];
     C2 *sl = (C2 *)smem_raw;
@@ -590,7 +702,7 @@ __global__ void __launch_bounds__(256) conv_c_kernel(typename Cplx<R>::T *__rest
         sl[c * ls + a] = base[c * cstride + a];
     }
     __syncthreads();
-    smem_fft<R>(sl, Nc, Nh, 1, ls, tc, +1);
+    line_fft<R, NF>(sl, Nc, Nh, 1, ls, tc, +1);
     double e = 0, pxx = 0, pyy = 0, pzz = 0, pxy = 0, pxz = 0, pyz = 0;
     const double kb = b <= Nb / 2 ? b : b - Nb;
     const double tpi = 2.0 * M_PI, falp2 = 4.0 * alp * alp;
@@ -620,7 +732,7 @@ __global__ void __launch_bounds__(256) conv_c_kernel(typename Cplx<R>::T *__rest
         sl[c * ls + a] = s;
     }
     __syncthreads();
-    smem_fft<R>(sl, Nc, Nh, 1, ls, tc, -1);
+    line_fft<R, NF>(sl, Nc, Nh, 1, ls, tc, -1);
     for (int idx = threadIdx.x; idx < Nc * Nh; idx += blockDim.x) {
         const int c = idx / Nh, a = idx % Nh;
         base[c * cstride + a] = sl[c * ls + a];
@@ -688,6 +800,31 @@ size_t pme_slab_smem(int Na, int Nc, bool fp64)
     return cs * (size_t)Nc * (Na / 2 + 2) + rs * 2 * (size_t)Nc;
 }
 
+// The three FFT kernels for grids of compile-time edge NF (0: run time).
+template <typename R, int NF>
+static cudaError_t launch_fft_t(pinyb200_ctx *c, const PmeArgs &a, const Cell &cell, typename Cplx<R>::T *spec,
+                                const R *filt, const R *const *tw, size_t sp, size_t ss, bool energy)
+{
+    cudaError_t err = cudaSuccess;
+    // opt in to more than 48 KB of dynamic shared memory where a plane needs it
+    if (sp > 48 * 1024) {
+        err = cudaFuncSetAttribute(plane_fwd_kernel<R, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(plane_inv_kernel<R, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp);
+        if (err != cudaSuccess) return err;
+    }
+    if (ss > 48 * 1024) {
+        err = cudaFuncSetAttribute(conv_c_kernel<R, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss);
+        if (err != cudaSuccess) return err;
+    }
+    plane_fwd_kernel<R, NF><<<a.P * a.Nc, 256, sp, c->stream>>>((const R *)a.grid, spec, a.Na, a.Nb, a.Nc, tw[0],
+                                                                tw[1]);
+    conv_c_kernel<R, NF><<<a.P * a.Nb, 256, ss, c->stream>>>(spec, filt, a.Na, a.Nb, a.Nc, tw[2], cell, c->alp_ewd,
+                                                             c->d_acc, energy ? 1 : 0);
+    plane_inv_kernel<R, NF><<<a.P * a.Nc, 256, sp, c->stream>>>(spec, (R *)a.grid, a.Na, a.Nb, a.Nc, tw[0], tw[1]);
+    return cudaGetLastError();
+}
+
 template <typename R, int NI>
 static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
 {
@@ -736,23 +873,17 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     const R *twbase = (const R *)(f64 ? (const void *)c->d_twiddle64 : (const void *)c->d_twiddle32);
     const R *tw[3] = {twbase, twbase + 2 * 256, twbase + 4 * 256};
     const size_t sp = pme_plane_smem(a.Na, a.Nb, f64), ss = pme_slab_smem(a.Na, a.Nc, f64);
-    // opt in to more than 48 KB of dynamic shared memory where a plane needs it
-    if (sp > 48 * 1024) {
-        err = cudaFuncSetAttribute(plane_fwd_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp);
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(plane_inv_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp);
-        if (err != cudaSuccess) return err;
-    }
-    if (ss > 48 * 1024) {
-        err = cudaFuncSetAttribute(conv_c_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss);
-        if (err != cudaSuccess) return err;
-    }
     C2 *spec = (C2 *)c->d_spec;
-    plane_fwd_kernel<R><<<a.P * a.Nc, 256, sp, c->stream>>>((const R *)c->d_grid, spec, a.Na, a.Nb, a.Nc, tw[0], tw[1]);
     const R *filt = f64 ? (const R *)c->d_filter : (const R *)((const double *)c->d_filter + G);
-    conv_c_kernel<R><<<a.P * a.Nb, 256, ss, c->stream>>>(spec, filt, a.Na, a.Nb, a.Nc, tw[2], cell, c->alp_ewd,
-                                                          c->d_acc, energy ? 1 : 0);
-    plane_inv_kernel<R><<<a.P * a.Nc, 256, sp, c->stream>>>(spec, (R *)c->d_grid, a.Na, a.Nb, a.Nc, tw[0], tw[1]);
+    const bool cube = a.Na == a.Nb && a.Na == a.Nc;
+    switch (cube ? a.Na : 0) {
+    case 16: err = launch_fft_t<R, 16>(c, a, cell, spec, filt, tw, sp, ss, energy); break;
+    case 32: err = launch_fft_t<R, 32>(c, a, cell, spec, filt, tw, sp, ss, energy); break;
+    case 64: err = launch_fft_t<R, 64>(c, a, cell, spec, filt, tw, sp, ss, energy); break;
+    case 128: err = launch_fft_t<R, 128>(c, a, cell, spec, filt, tw, sp, ss, energy); break;
+    default: err = launch_fft_t<R, 0>(c, a, cell, spec, filt, tw, sp, ss, energy); break;
+    }
+    if (err != cudaSuccess) return err;
     gather_tile_kernel<R, NI><<<tgrid, 256, st, c->stream>>>(a, cell, t);
     return cudaGetLastError();
 }

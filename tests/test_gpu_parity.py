@@ -86,3 +86,58 @@ def test_list_errors_and_state():
         DeviceBox(bad, 1, "fp64")
     with pytest.raises(PinyError, match="ERR_UNSUPPORTED"):
         DeviceBox(F, 3, "fp64")
+
+
+def _grid_case(case):
+    """Systems that reach each PME FFT path: compile-time 64^3 and 128^3
+    grids, and a non-cubic grid with a non-power-of-two edge (run-time path
+    with the direct DFT)."""
+    import dataclasses
+
+    from piny_b200 import system, water
+    if case == "tip4pf_512_g64":
+        spec = water.BoxSpec(water.TIP4P_F, 512, water.density_box_edge(512), 2, 298.0, 99, grid=64, order=8)
+    elif case == "spcfw_216_g128":
+        spec = water.BoxSpec(water.SPC_FW, 216, 18.64, 1, 300.0, 5, grid=128, order=8)
+    else:
+        spec = dataclasses.replace(water.named_spec("spcfw_216_p4"), nbeads=2)
+    pos = water.build_positions(spec) / water.BOHR
+    S = system.build_system(spec, pos)
+    if case == "spcfw_216_ncubic":
+        # stretch the c axis of the mesh to 40 points, B-spline weights to match
+        nc = 40
+        wa = system.bspline_weight_1d(spec.order, S["ngrid_a"])
+        wb = system.bspline_weight_1d(spec.order, S["ngrid_b"])
+        wc = system.bspline_weight_1d(spec.order, nc)
+        ka, kb, kc = S["kastr"], S["kbstr"], S["kcstr"]
+        S["ngrid_c"] = nc
+        S["bweight"] = wa[np.where(ka < 0, ka + S["ngrid_a"], ka)] * wb[np.where(kb < 0, kb + S["ngrid_b"], kb)] \
+            * wc[np.where(kc < 0, kc + nc, kc)]
+    return spec, pos, S
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["tip4pf_512_g64", "spcfw_216_g128", "spcfw_216_ncubic"])
+def test_pme_grid_paths_match_oracle(case, prec, oracle):
+    spec, pos, S = _grid_case(case)
+    from piny_b200.lib import DeviceBox, PinyError
+    if case == "spcfw_216_g128" and prec == "fp64":
+        # an FP64 plane of 128 x 129 complex points exceeds shared memory
+        with pytest.raises(PinyError, match="ERR_UNSUPPORTED"):
+            DeviceBox(S, spec.nbeads, prec)
+        return
+    xmod = pos.mean(axis=0) if spec.nbeads > 1 else None
+    pi, pj = oracle.verlist(S, pos[0], xmod, S["hmat"], S["cutskin2"])
+    fref, eref = oracle.energy_force(S, pos, xmod, S["hmat"], pi, pj)
+    box = DeviceBox(S, spec.nbeads, prec)
+    box.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+    f, e = box.energy_force(pos, xmod, S["hmat"])
+    assert rel_rms(f, fref) < TOL[prec]
+    vrec = e["vrecip"] + e["vself"] + e["vbgr"] + e["vecor"]
+    vrec_ref = eref["vrecip"] + eref["vself"] + eref["vbgr"] + eref["vecor"]
+    assert abs(vrec - vrec_ref) <= ETOL[prec] * max(1.0, abs(vrec_ref))
+    # vintert is a small difference of large terms: its mixed-precision error
+    # scales with the terms, not with the difference
+    scale = abs(eref["vvdw"]) + abs(eref["vcoul"]) + abs(eref["vrecip"]) + abs(eref["vself"]) + abs(eref["vecor"])
+    assert abs(e["vintert"] - eref["vintert"]) <= ETOL[prec] * scale
+    box.close()
