@@ -194,7 +194,8 @@ int pinyb200_destroy(pinyb200_ctx *c)
     void *ptrs[] = {c->d_row, c->d_col, c->d_rowA, c->d_colA, c->d_count, c->d_tot, c->d_posT, c->d_forceT,
                     c->d_xmod, c->d_pos_aos, c->d_force_aos, c->d_acc, c->d_grid, c->d_spec, c->d_filter, c->d_twiddle64,
                     c->d_twiddle32, c->d_err, c->d_mstart, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_chunk,
-                    c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf};
+                    c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf,
+                    c->d_pme_head, c->d_pme_w};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i < 8; i++)
@@ -322,6 +323,11 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
         CK(cudaMalloc(&c->d_pme_cnt, ((size_t)nbeads * c->pme_ntile + 1) * sizeof(int)));
         CK(cudaMalloc(&c->d_pme_bin, (size_t)nbeads * c->pme_ntile * c->pme_cap * sizeof(int)));
         CK(cudaMalloc(&c->d_pme_ovf, (size_t)std::max(1, d.nchrg) * nbeads * sizeof(int)));
+        // per (charge, bead) records: stencil origin and the six weight rows
+        const int nip = s->n_interp <= 4 ? 4 : (s->n_interp <= 8 ? 8 : 12);
+        const size_t nrec = (size_t)std::max(1, d.nchrg) * nbeads;
+        CK(cudaMalloc(&c->d_pme_head, nrec * 4 * sizeof(int)));
+        CK(cudaMalloc(&c->d_pme_w, nrec * 6 * nip * rsz));
         // twiddles exp(2 pi i m / N) per axis, 256 entries each
         std::vector<double> tw(2 * 256 * 3, 0.0);
         std::vector<float> tw32(tw.size());

@@ -119,6 +119,8 @@ struct pinyb200_ctx {
     int *d_pme_cnt = nullptr;     // [P][ntile] entries per bin, then [1] overflow count
     int *d_pme_bin = nullptr;     // [P][ntile][cap] charge numbers (index into ichrg)
     int *d_pme_ovf = nullptr;     // [nchrg*P] overflowing (charge, bead) as k*P + b
+    void *d_pme_head = nullptr;   // [nchrg*P] int4 stencil origin records
+    void *d_pme_w = nullptr;      // [nchrg*P][6][NIP] B-spline weight records
     double *d_twiddle64 = nullptr;  // per axis twiddles
     float *d_twiddle32 = nullptr;
     int *d_err = nullptr;

@@ -39,6 +39,8 @@ struct PmeArgs {
     int Na, Nb, Nc, n;
     void *grid;  // real [P][Nc][Nb][Na]
     double *forceT;
+    int4 *rhead;  // per (charge, bead) records, see RecGeom
+    void *rw;
 };
 
 // B-spline weights of order NI at the fractional offset f (ewald3d_pme.c:
@@ -108,23 +110,23 @@ __device__ __forceinline__ void stencil_origin(const PmeArgs &a, const Cell &cel
     if (lc < 0) lc += a.Nc;
 }
 
-template <typename R, int NI, bool DERIV>
-__device__ __forceinline__ void stencil(const PmeArgs &a, const Cell &cell, int at, int b, R *ma, R *mb, R *mc,
-                                        R *da, R *db, R *dc, int &la, int &lb, int &lc)
-{
-    double fa, fb, fc;
-    stencil_origin(a, cell, at, b, NI, la, lb, lc, fa, fb, fc);
-    bspline<R, NI, DERIV>((R)fa, ma, da);
-    bspline<R, NI, DERIV>((R)fb, mb, db);
-    bspline<R, NI, DERIV>((R)fc, mc, dc);
-}
-
 // Charges binned by the grid tile that holds their stencil origin, per bead.
 struct TileArgs {
     int nta, ntb, ntc, ntile, cap;
     int *cnt;  // [P][ntile], then the overflow count
-    int *bin;  // [P][ntile][cap]
-    int *ovf;  // [nchrg * P]
+    int *bin;  // [P][ntile][cap] record numbers k*P + b
+    int *ovf;  // [nchrg * P] record numbers that did not fit their bin
+};
+
+// Per (charge k, bead b) record, number idx = k*P + b, written by the bin
+// kernel and read by spread and gather:
+//   head[idx] = (atom, la, lb, lc)  stencil origin per axis
+//   w[idx][j][t], j = 0..5 for M_a, M_b, M_c, dM_a, dM_b, dM_c, t = 0..NIP-1:
+//                 weight of grid point lo + t (PINY's m[NI - t]), zero for t >= NI
+template <int NI>
+struct RecGeom {
+    static constexpr int NIP = NI <= 4 ? 4 : (NI <= 8 ? 8 : 12);
+    static constexpr int NW = 6 * NIP;
 };
 
 // Tile geometry: T^3 grid points own the charges whose stencil starts in
@@ -138,174 +140,303 @@ struct TileGeom {
     static constexpr int NPT = E * E * PA;
 };
 
-__device__ __forceinline__ int wrapi(int i, int N) { return i >= N ? i - N : i; }
+// i mod N for 0 <= i < k N with small k.
+__device__ __forceinline__ int wrapi(int i, int N)
+{
+    while (i >= N) i -= N;
+    return i;
+}
 
-template <int NI>
+// Store n consecutive values of type R (n a multiple of 4) with vector stores.
+__device__ __forceinline__ void store4(float *dst, const float *v, int n)
+{
+    for (int i = 0; i < n; i += 4) *(float4 *)(dst + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+}
+__device__ __forceinline__ void store4(double *dst, const double *v, int n)
+{
+    for (int i = 0; i < n; i += 2) *(double2 *)(dst + i) = make_double2(v[i], v[i + 1]);
+}
+template <int N>
+__device__ __forceinline__ void load4(float *v, const float *src)
+{
+#pragma unroll
+    for (int i = 0; i < N; i += 4) {
+        const float4 x = __ldg((const float4 *)(src + i));
+        v[i] = x.x;
+        v[i + 1] = x.y;
+        v[i + 2] = x.z;
+        v[i + 3] = x.w;
+    }
+}
+template <int N>
+__device__ __forceinline__ void load4(double *v, const double *src)
+{
+#pragma unroll
+    for (int i = 0; i < N; i += 2) {
+        const double2 x = __ldg((const double2 *)(src + i));
+        v[i] = x.x;
+        v[i + 1] = x.y;
+    }
+}
+
+// Bin kernel: one thread per (charge, bead).  Stencil origin in FP64 with
+// PINY's operation order, B-spline weights and derivatives in R, record
+// written in (charge, bead) order, record number filed under its tile.
+template <typename R, int NI>
 __global__ void __launch_bounds__(256) pme_bin_kernel(PmeArgs a, Cell cell, TileArgs t)
 {
+    typedef RecGeom<NI> RG;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)a.nchrg * a.P) return;
     const int b = (int)(idx % a.P);
     const int k = (int)(idx / a.P);
+    const int at = a.ichrg[k];
     int la, lb, lc;
     double fa, fb, fc;
-    stencil_origin(a, cell, a.ichrg[k], b, NI, la, lb, lc, fa, fb, fc);
+    stencil_origin(a, cell, at, b, NI, la, lb, lc, fa, fb, fc);
+    R m[NI + 1], d[NI + 1], w[RG::NIP];
+    R *out = (R *)a.rw + (size_t)idx * RG::NW;
+    const double fr[3] = {fa, fb, fc};
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) {
+        bspline<R, NI, true>((R)fr[ax], m, d);
+#pragma unroll
+        for (int s = 0; s < RG::NIP; s++) w[s] = s < NI ? m[NI - s] : (R)0;
+        store4(out + ax * RG::NIP, w, RG::NIP);
+#pragma unroll
+        for (int s = 0; s < RG::NIP; s++) w[s] = s < NI ? d[NI - s] : (R)0;
+        store4(out + (3 + ax) * RG::NIP, w, RG::NIP);
+    }
+    a.rhead[idx] = make_int4(at, la, lb, lc);
     const int T = PINYB200_PME_TILE;
     const int tile = ((lc / T) * t.ntb + lb / T) * t.nta + la / T;
     const int slot = atomicAdd(&t.cnt[b * t.ntile + tile], 1);
-    if (slot < t.cap) t.bin[((size_t)b * t.ntile + tile) * t.cap + slot] = k;
+    if (slot < t.cap) t.bin[((size_t)b * t.ntile + tile) * t.cap + slot] = (int)idx;
     else t.ovf[atomicAdd(&t.cnt[a.P * t.ntile], 1)] = (int)idx;
 }
 
-// The a-weights of lane l8 of an 8-lane group: grid points lo + l8 and
-// lo + l8 + 8 (orders above 8), picked with static indices.
-template <typename R, int NI>
-__device__ __forceinline__ void lane_weights(const R *m, int l8, R &w0, R &w1)
-{
-    w0 = (R)0;
-    w1 = (R)0;
-#pragma unroll
-    for (int t = 0; t < NI; t++) {
-        if (t == l8) w0 = m[NI - t];
-        if (t == l8 + 8) w1 = m[NI - t];
+// Weights of one record that a lane of an 8-lane group needs: its own a
+// points (l8 and l8 + 8) and all b and c points; DERIV adds the derivatives.
+template <typename R, int NI, bool DERIV>
+struct LaneW {
+    typedef RecGeom<NI> RG;
+    R wa0, wa1, da0, da1;
+    R mb[RG::NIP], mc[RG::NIP], db[DERIV ? RG::NIP : 1], dc[DERIV ? RG::NIP : 1];
+    __device__ __forceinline__ void load(const R *rw, int idx, int l8)
+    {
+        const R *w = rw + (size_t)idx * RG::NW;
+        wa0 = l8 < NI ? w[l8] : (R)0;
+        wa1 = (NI > 8 && l8 + 8 < NI) ? w[l8 + 8] : (R)0;
+        load4<RG::NIP>(mb, w + RG::NIP);
+        load4<RG::NIP>(mc, w + 2 * RG::NIP);
+        if (DERIV) {
+            da0 = l8 < NI ? w[3 * RG::NIP + l8] : (R)0;
+            da1 = (NI > 8 && l8 + 8 < NI) ? w[3 * RG::NIP + l8 + 8] : (R)0;
+            load4<RG::NIP>(db, w + 4 * RG::NIP);
+            load4<RG::NIP>(dc, w + 5 * RG::NIP);
+        }
     }
-}
+};
 
-// Spread one charge of bead b straight into the global grid (overflow
-// entries); the 8 lanes of the group share the a points.
+// Spread one record straight into the global grid (overflow entries).
 template <typename R, int NI>
-__device__ __forceinline__ void spread_global(const PmeArgs &a, R *g, int la, int lb, int lc, R wa0, R wa1,
-                                              const R *mb, const R *mc, R q, int l8)
+__device__ __forceinline__ void spread_global(const PmeArgs &a, R *g, int la, int lb, int lc,
+                                              const LaneW<R, NI, false> &lw, R q, int l8)
 {
     const int ga0 = wrapi(la + l8, a.Na), ga1 = wrapi(la + l8 + 8, a.Na);
 #pragma unroll
     for (int tc = 0; tc < NI; tc++) {
         const int gc = wrapi(lc + tc, a.Nc);
-        const R qc = q * mc[NI - tc];
+        const R qc = q * lw.mc[tc];
 #pragma unroll
         for (int tb = 0; tb < NI; tb++) {
             const int gb = wrapi(lb + tb, a.Nb);
-            const R w = mb[NI - tb] * qc;
+            const R w = lw.mb[tb] * qc;
             R *row = g + ((size_t)gc * a.Nb + gb) * a.Na;
-            if (l8 < NI) atomicAdd(row + ga0, wa0 * w);
-            if (NI > 8 && l8 + 8 < NI) atomicAdd(row + ga1, wa1 * w);
+            if (l8 < NI) atomicAdd(row + ga0, lw.wa0 * w);
+            if (NI > 8 && l8 + 8 < NI) atomicAdd(row + ga1, lw.wa1 * w);
         }
     }
 }
 
-// Spread: one block per (tile, bead).  The charges of the bin go into a
-// shared copy of the tile with shared-memory atomics (8 lanes per charge,
-// one lane per a point), then the copy is added to the grid once, with
-// 16-byte vector atomics where the rows allow.  Overflow entries are shared
-// out over all blocks and go straight to the grid.
+// Spread: one block of 8 warps per (tile, bead), no shared-memory atomics.
+// The bin's records are staged in shared memory a chunk at a time; warp w
+// owns the c-planes of the tile copy whose index is w mod 8 and adds, for
+// every staged record, the stencil rows that fall in its planes (lanes:
+// 8 a points x 4 b rows), so no two threads ever write the same point.
+// The copy is then added to the grid once, with 16-byte vector atomics
+// where the rows allow.  Records whose origin lies outside the tile (none
+// are expected) and overflow records go straight to the grid.
+template <int NI>
+struct SpreadStage {
+    static constexpr int CH = 64;  // records per staged chunk
+    static constexpr int NIP = RecGeom<NI>::NIP;
+};
+
 template <typename R, int NI>
-__global__ void __launch_bounds__(256) spread_tile_kernel(PmeArgs a, Cell cell, TileArgs t)
+size_t spread_smem()
+{
+    typedef SpreadStage<NI> SS;
+    return (size_t)TileGeom<NI>::NPT * sizeof(R) + (size_t)SS::CH * (3 * SS::NIP + 1) * sizeof(R) +
+           (size_t)SS::CH * sizeof(int);
+}
+
+template <typename R, int NI>
+__global__ void __launch_bounds__(256) spread_tile_kernel(PmeArgs a, TileArgs t)
 {
     typedef TileGeom<NI> TG;
+    typedef SpreadStage<NI> SS;
+    constexpr int NIP = SS::NIP, CH = SS::CH;
     extern __shared__ unsigned char smem_raw[];
     R *tl = (R *)smem_raw;
+    R *sw = tl + TG::NPT;        // [CH][3][NIP]: M_a, M_b, M_c
+    R *sq = sw + CH * 3 * NIP;   // [CH] charge
+    int *sh = (int *)(sq + CH);  // [CH] origin in the copy: oa | ob << 8 | oc << 16, or -1
     for (int i = threadIdx.x; i < TG::NPT; i += blockDim.x) tl[i] = (R)0;
-    __syncthreads();
     const int tile = blockIdx.x, b = blockIdx.y;
     const int ta0 = (tile % t.nta) * TG::T, tb0 = ((tile / t.nta) % t.ntb) * TG::T, tc0 = (tile / (t.nta * t.ntb)) * TG::T;
-    const int grp = threadIdx.x >> 3, l8 = threadIdx.x & 7, ngrp = blockDim.x >> 3;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int n = min(t.cnt[b * t.ntile + tile], t.cap);
     const int *list = t.bin + ((size_t)b * t.ntile + tile) * t.cap;
+    const R *rw = (const R *)a.rw;
     R *g = (R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
-    for (int e = grp; e < n; e += ngrp) {
-        const int at = a.ichrg[list[e]];
-        R ma[NI + 1], mb[NI + 1], mc[NI + 1];
-        int la, lb, lc;
-        stencil<R, NI, false>(a, cell, at, b, ma, mb, mc, nullptr, nullptr, nullptr, la, lb, lc);
-        const R q = (R)a.charge[at];
-        R wa0, wa1;
-        lane_weights<R, NI>(ma, l8, wa0, wa1);
-        const int oa = la - ta0, ob = lb - tb0, oc = lc - tc0;
-        if (oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T) {
+    const int la8 = lane & 7, lb4 = lane >> 3;
+    const int loff = lb4 * TG::PA + la8;  // this lane's point in a stencil plane
+    for (int c0 = 0; c0 < n; c0 += CH) {
+        const int nc = min(CH, n - c0);
+        __syncthreads();  // the previous chunk is done (and tl is cleared)
+        for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+            const int idx = list[c0 + i];
+            const int4 h = a.rhead[idx];
+            const int oa = h.y - ta0, ob = h.z - tb0, oc = h.w - tc0;
+            const bool in = oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T;
+            sh[i] = in ? (oa | (ob << 8) | (oc << 16)) : -1;
+            sq[i] = (R)a.charge[h.x];
+        }
+        for (int i = threadIdx.x; i < nc * 3 * NIP; i += blockDim.x) {
+            const int e = i / (3 * NIP), j = i - e * (3 * NIP);
+            sw[i] = rw[(size_t)list[c0 + e] * RecGeom<NI>::NW + j];
+        }
+        __syncthreads();
+        for (int e = 0; e < nc; e++) {
+            // lanes of this warp may update a point another lane updated for
+            // the previous record: order their shared-memory accesses
+            __syncwarp();
+            const int h = sh[e];
+            if (h < 0) continue;
+            const int oa = h & 255, ob = (h >> 8) & 255, oc = h >> 16;
+            const R *w = sw + e * 3 * NIP;
+            for (int tc = (warp - oc) & 7; tc < NI; tc += 8) {
+                const R cq = sq[e] * w[2 * NIP + tc];
+                R *base = tl + ((oc + tc) * TG::E + ob) * TG::PA + oa + loff;
 #pragma unroll
-            for (int tc = 0; tc < NI; tc++) {
-                const R qc = q * mc[NI - tc];
+                for (int sa = 0; sa < NI; sa += 8) {
+                    if (la8 + sa >= NI) continue;
+                    const R av = cq * w[la8 + sa];
 #pragma unroll
-                for (int tb = 0; tb < NI; tb++) {
-                    const R w = mb[NI - tb] * qc;
-                    R *row = tl + ((oc + tc) * TG::E + (ob + tb)) * TG::PA + oa;
-                    if (l8 < NI) atomicAdd(row + l8, wa0 * w);
-                    if (NI > 8 && l8 + 8 < NI) atomicAdd(row + l8 + 8, wa1 * w);
+                    for (int sb = 0; sb < NI; sb += 4) {
+                        if (lb4 + sb < NI) {
+                            R *p = base + sb * TG::PA + sa;
+                            *p += av * w[NIP + lb4 + sb];
+                        }
+                    }
                 }
             }
-        } else {
-            spread_global<R, NI>(a, g, la, lb, lc, wa0, wa1, mb, mc, q, l8);
         }
     }
+    // records outside the tile (not expected): straight to the grid
+    for (int e0 = 0; e0 < n; e0 += CH) {
+        // re-check from the heads; cheap, and keeps the staged loop branch-free
+        for (int i = warp; i < min(CH, n - e0); i += nwarp) {
+            const int idx = list[e0 + i];
+            const int4 h = a.rhead[idx];
+            const int oa = h.y - ta0, ob = h.z - tb0, oc = h.w - tc0;
+            if (oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T) continue;
+            if (lane < 8) {
+                LaneW<R, NI, false> lw;
+                lw.load(rw, idx, lane);
+                spread_global<R, NI>(a, g, h.y, h.z, h.w, lw, (R)a.charge[h.x], lane);
+            }
+        }
+    }
+    const int grp = threadIdx.x >> 3, l8 = threadIdx.x & 7, ngrp = blockDim.x >> 3;
     const int nov = t.cnt[a.P * t.ntile];
     const int gid = blockIdx.y * gridDim.x + blockIdx.x, nblk = gridDim.x * gridDim.y;
     for (int e = gid * ngrp + grp; e < nov; e += nblk * ngrp) {
         const int idx = t.ovf[e];
-        const int b2 = idx % a.P, at = a.ichrg[idx / a.P];
-        R ma[NI + 1], mb[NI + 1], mc[NI + 1];
-        int la, lb, lc;
-        stencil<R, NI, false>(a, cell, at, b2, ma, mb, mc, nullptr, nullptr, nullptr, la, lb, lc);
-        R wa0, wa1;
-        lane_weights<R, NI>(ma, l8, wa0, wa1);
-        R *g2 = (R *)a.grid + (size_t)b2 * a.Na * a.Nb * a.Nc;
-        spread_global<R, NI>(a, g2, la, lb, lc, wa0, wa1, mb, mc, (R)a.charge[at], l8);
+        const int4 h = a.rhead[idx];
+        LaneW<R, NI, false> lw;
+        lw.load(rw, idx, l8);
+        R *g2 = (R *)a.grid + (size_t)(idx % a.P) * a.Na * a.Nb * a.Nc;
+        spread_global<R, NI>(a, g2, h.y, h.z, h.w, lw, (R)a.charge[h.x], l8);
     }
     __syncthreads();
-    // add the shared copy to the grid
-    constexpr int NQ = TG::PA / 4;
+    // add the shared copy to the grid, a warp per row (or rows)
+    constexpr int NROW = TG::E * TG::E;
     if (sizeof(R) == 4 && (a.Na & 3) == 0) {
-        for (int i = threadIdx.x; i < TG::E * TG::E * NQ; i += blockDim.x) {
-            const int row = i / NQ, q4 = i % NQ;
-            const int cz = row / TG::E, by = row % TG::E;
-            const float4 v = ((const float4 *)tl)[i];
+        constexpr int NQ = TG::PA / 4;
+        constexpr int RPI = 32 / NQ;  // rows per warp step
+        for (int r0 = warp * RPI; r0 < NROW; r0 += nwarp * RPI) {
+            const int row = r0 + lane / NQ, q4 = lane % NQ;
+            if (lane >= RPI * NQ || row >= NROW) continue;
+            const float4 v = ((const float4 *)tl)[row * NQ + q4];
             if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
-            const int gc = (tc0 + cz) % a.Nc, gb = (tb0 + by) % a.Nb, ga = (ta0 + 4 * q4) % a.Na;
+            const int cz = row / TG::E, by = row - cz * TG::E;
+            const int gc = wrapi(tc0 + cz, a.Nc), gb = wrapi(tb0 + by, a.Nb), ga = wrapi(ta0 + 4 * q4, a.Na);
             atomicAdd((float4 *)((float *)g + ((size_t)gc * a.Nb + gb) * a.Na + ga), v);
         }
     } else {
-        for (int i = threadIdx.x; i < TG::NPT; i += blockDim.x) {
-            const R v = tl[i];
-            if (v == (R)0) continue;
-            const int row = i / TG::PA, ax = i % TG::PA;
-            const int cz = row / TG::E, by = row % TG::E;
-            const int gc = (tc0 + cz) % a.Nc, gb = (tb0 + by) % a.Nb, ga = (ta0 + ax) % a.Na;
-            atomicAdd(g + ((size_t)gc * a.Nb + gb) * a.Na + ga, v);
+        for (int row = warp; row < NROW; row += nwarp) {
+            const int cz = row / TG::E, by = row - cz * TG::E;
+            R *dst = g + ((size_t)wrapi(tc0 + cz, a.Nc) * a.Nb + wrapi(tb0 + by, a.Nb)) * a.Na;
+            for (int ax = lane; ax < TG::E; ax += 32) {
+                const R v = tl[row * TG::PA + ax];
+                if (v != (R)0) atomicAdd(dst + wrapi(ta0 + ax, a.Na), v);
+            }
         }
     }
 }
 
-// Gather sums of one charge for lane l8: d/ds_a, d/ds_b, d/ds_c of
+// Gather sums of one record for lane l8: d/ds_a, d/ds_b, d/ds_c of
 // sum M_a M_b M_c phi over the lane's a points; phi(tc, tb, ta) reads the
-// potential at stencil point (tc, tb, ta).
+// potential at stencil point (tc, tb, ta).  The a weights factor out of the
+// b and c sums, so a stencil point costs one load and two FMAs.
 template <typename R, int NI, typename PHI>
-__device__ __forceinline__ void gather_lane(PHI phi, R wa0, R wa1, R wd0, R wd1, const R *mb, const R *db,
-                                            const R *mc, const R *dc, int l8, double &ea, double &eb, double &ec)
+__device__ __forceinline__ void gather_lane(PHI phi, const LaneW<R, NI, true> &lw, int l8, double &ea, double &eb,
+                                            double &ec)
 {
     ea = eb = ec = 0.0;
     if (l8 >= NI) return;
+    R xa = 0, xb = 0, xc = 0;
 #pragma unroll
-    for (int tc = 0; tc < NI; tc++) {
-        R um = 0, udm = 0, udb = 0;
+    for (int j = 0; j < (NI > 8 ? 2 : 1); j++) {
+        if (j == 1 && l8 + 8 >= NI) break;
+        const int ta = l8 + 8 * j;
+        R sa = 0, sb = 0, sc = 0;
 #pragma unroll
-        for (int tb = 0; tb < NI; tb++) {
-            const R p0 = phi(tc, tb, l8);
-            R s0 = wa0 * p0, s1 = wd0 * p0;
-            if (NI > 8 && l8 + 8 < NI) {
-                const R p1 = phi(tc, tb, l8 + 8);
-                s0 += wa1 * p1;
-                s1 += wd1 * p1;
+        for (int tc = 0; tc < NI; tc++) {
+            R um = 0, ud = 0;
+#pragma unroll
+            for (int tb = 0; tb < NI; tb++) {
+                const R p = phi(tc, tb, ta);
+                um += lw.mb[tb] * p;
+                ud += lw.db[tb] * p;
             }
-            um += mb[NI - tb] * s0;
-            udm += mb[NI - tb] * s1;
-            udb += db[NI - tb] * s0;
+            sa += lw.mc[tc] * um;
+            sb += lw.mc[tc] * ud;
+            sc += lw.dc[tc] * um;
         }
-        ea += (double)(mc[NI - tc] * udm);
-        eb += (double)(mc[NI - tc] * udb);
-        ec += (double)(dc[NI - tc] * um);
+        const R wa = j ? lw.wa1 : lw.wa0, da = j ? lw.da1 : lw.da0;
+        xa += da * sa;
+        xb += wa * sb;
+        xc += wa * sc;
     }
+    ea = (double)xa;
+    eb = (double)xb;
+    ec = (double)xc;
 }
 
-// Force of one charge from its three sums (summed over the 8-lane group;
+// Force of one record from its three sums (summed over the 8-lane group;
 // lane 0 writes): F = -q h^-T (N_a e_a, N_b e_b, N_c e_c).
 __device__ __forceinline__ void gather_store(const PmeArgs &a, const Cell &cell, int at, int b, double ea, double eb,
                                              double ec, int l8)
@@ -331,8 +462,8 @@ __device__ __forceinline__ void gather_store(const PmeArgs &a, const Cell &cell,
 }
 
 // Gather: one block per (tile, bead); the tile's potential (with the
-// stencil reach) is copied to shared memory once and the bin's charges read
-// it there.  Overflow entries read the grid directly.  Every (charge, bead)
+// stencil reach) is copied to shared memory once and the bin's records read
+// it there.  Overflow records read the grid directly.  Every (charge, bead)
 // is handled by exactly one 8-lane group, so the force update needs no
 // atomics.
 template <typename R, int NI>
@@ -345,48 +476,62 @@ __global__ void __launch_bounds__(256) gather_tile_kernel(PmeArgs a, Cell cell, 
     const int ta0 = (tile % t.nta) * TG::T, tb0 = ((tile / t.nta) % t.ntb) * TG::T, tc0 = (tile / (t.nta * t.ntb)) * TG::T;
     const R *g = (const R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
     const int n = min(t.cnt[b * t.ntile + tile], t.cap);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     if (n > 0) {
-        for (int i = threadIdx.x; i < TG::NPT; i += blockDim.x) {
-            const int row = i / TG::PA, ax = i % TG::PA;
-            const int cz = row / TG::E, by = row % TG::E;
-            R v = (R)0;
-            if (ax < TG::E) {
-                const int gc = (tc0 + cz) % a.Nc, gb = (tb0 + by) % a.Nb, ga = (ta0 + ax) % a.Na;
-                v = g[((size_t)gc * a.Nb + gb) * a.Na + ga];
+        constexpr int NROW = TG::E * TG::E;
+        if (sizeof(R) == 4 && (a.Na & 3) == 0) {
+            // 16-byte chunks; the padding column takes whatever the grid holds there
+            constexpr int NQ = TG::PA / 4;
+            constexpr int RPI = 32 / NQ;
+            for (int r0 = warp * RPI; r0 < NROW; r0 += nwarp * RPI) {
+                const int row = r0 + lane / NQ, q4 = lane % NQ;
+                if (lane >= RPI * NQ || row >= NROW) continue;
+                const int cz = row / TG::E, by = row - cz * TG::E;
+                const float *src = (const float *)g +
+                                   ((size_t)wrapi(tc0 + cz, a.Nc) * a.Nb + wrapi(tb0 + by, a.Nb)) * a.Na +
+                                   wrapi(ta0 + 4 * q4, a.Na);
+                ((float4 *)tl)[row * NQ + q4] = __ldg((const float4 *)src);
             }
-            tl[i] = v;
+        } else {
+            for (int row = warp; row < NROW; row += nwarp) {
+                const int cz = row / TG::E, by = row - cz * TG::E;
+                const R *src = g + ((size_t)wrapi(tc0 + cz, a.Nc) * a.Nb + wrapi(tb0 + by, a.Nb)) * a.Na;
+                for (int ax = lane; ax < TG::PA; ax += 32)
+                    tl[row * TG::PA + ax] = ax < TG::E ? src[wrapi(ta0 + ax, a.Na)] : (R)0;
+            }
         }
     }
     __syncthreads();
     const int grp = threadIdx.x >> 3, l8 = threadIdx.x & 7, ngrp = blockDim.x >> 3;
     const int *list = t.bin + ((size_t)b * t.ntile + tile) * t.cap;
+    const R *rw = (const R *)a.rw;
     // every lane of a warp takes part in the group reductions: loop to the
     // same trip count in all groups of the warp
     const int nr = (n + ngrp - 1) / ngrp;
     for (int r = 0; r < nr; r++) {
         const int e = r * ngrp + grp;
         const bool act = e < n;
-        const int at = act ? a.ichrg[list[e]] : 0;
+        int at = 0;
         double ea = 0, eb = 0, ec = 0;
         if (act) {
-            R ma[NI + 1], mb[NI + 1], mc[NI + 1], da[NI + 1], db[NI + 1], dc[NI + 1];
-            int la, lb, lc;
-            stencil<R, NI, true>(a, cell, at, b, ma, mb, mc, da, db, dc, la, lb, lc);
-            R wa0, wa1, wd0, wd1;
-            lane_weights<R, NI>(ma, l8, wa0, wa1);
-            lane_weights<R, NI>(da, l8, wd0, wd1);
-            const int oa = la - ta0, ob = lb - tb0, oc = lc - tc0;
+            const int idx = list[e];
+            const int4 h = a.rhead[idx];
+            at = h.x;
+            LaneW<R, NI, true> lw;
+            lw.load(rw, idx, l8);
+            const int oa = h.y - ta0, ob = h.z - tb0, oc = h.w - tc0;
             if (oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T) {
                 const R *base = tl + (oc * TG::E + ob) * TG::PA + oa;
-                gather_lane<R, NI>([&](int tc, int tb, int ta) { return base[(tc * TG::E + tb) * TG::PA + ta]; },
-                                   wa0, wa1, wd0, wd1, mb, db, mc, dc, l8, ea, eb, ec);
+                gather_lane<R, NI>([&](int tc, int tb, int ta) { return base[(tc * TG::E + tb) * TG::PA + ta]; }, lw,
+                                   l8, ea, eb, ec);
             } else {
+                const int la = h.y, lb = h.z, lc = h.w;
                 gather_lane<R, NI>(
                     [&](int tc, int tb, int ta) {
                         return g[((size_t)wrapi(lc + tc, a.Nc) * a.Nb + wrapi(lb + tb, a.Nb)) * a.Na +
                                  wrapi(la + ta, a.Na)];
                     },
-                    wa0, wa1, wd0, wd1, mb, db, mc, dc, l8, ea, eb, ec);
+                    lw, l8, ea, eb, ec);
             }
         }
         gather_store(a, cell, at, b, ea, eb, ec, act ? l8 : 1);
@@ -401,21 +546,19 @@ __global__ void __launch_bounds__(256) gather_tile_kernel(PmeArgs a, Cell cell, 
         double ea = 0, eb = 0, ec = 0;
         if (act) {
             const int idx = t.ovf[e];
+            const int4 h = a.rhead[idx];
             b2 = idx % a.P;
-            at = a.ichrg[idx / a.P];
-            R ma[NI + 1], mb[NI + 1], mc[NI + 1], da[NI + 1], db[NI + 1], dc[NI + 1];
-            int la, lb, lc;
-            stencil<R, NI, true>(a, cell, at, b2, ma, mb, mc, da, db, dc, la, lb, lc);
-            R wa0, wa1, wd0, wd1;
-            lane_weights<R, NI>(ma, l8, wa0, wa1);
-            lane_weights<R, NI>(da, l8, wd0, wd1);
+            at = h.x;
+            LaneW<R, NI, true> lw;
+            lw.load(rw, idx, l8);
             const R *g2 = (const R *)a.grid + (size_t)b2 * a.Na * a.Nb * a.Nc;
+            const int la = h.y, lb = h.z, lc = h.w;
             gather_lane<R, NI>(
                 [&](int tc, int tb, int ta) {
                     return g2[((size_t)wrapi(lc + tc, a.Nc) * a.Nb + wrapi(lb + tb, a.Nb)) * a.Na +
                               wrapi(la + ta, a.Na)];
                 },
-                wa0, wa1, wd0, wd1, mb, db, mc, dc, l8, ea, eb, ec);
+                lw, l8, ea, eb, ec);
         }
         gather_store(a, cell, at, b2, ea, eb, ec, act ? l8 : 1);
     }
@@ -843,6 +986,8 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     a.n = s.n_interp;
     a.grid = c->d_grid;
     a.forceT = c->d_forceT;
+    a.rhead = (int4 *)c->d_pme_head;
+    a.rw = c->d_pme_w;
     const size_t G = (size_t)a.Na * a.Nb * a.Nc;
     const bool f64 = sizeof(R) == 8;
     cudaError_t err = cudaMemsetAsync(c->d_grid, 0, sizeof(R) * G * c->P, c->stream);
@@ -860,16 +1005,20 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     if (err != cudaSuccess) return err;
     const long long nt = (long long)a.nchrg * a.P;
     const int threads = 256;
-    pme_bin_kernel<NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell, t);
-    const size_t st = (size_t)TileGeom<NI>::NPT * sizeof(R);
+    pme_bin_kernel<R, NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell, t);
+    const size_t st = (size_t)TileGeom<NI>::NPT * sizeof(R), ss_spread = spread_smem<R, NI>();
+    if (ss_spread > 48 * 1024) {
+        err = cudaFuncSetAttribute(spread_tile_kernel<R, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)ss_spread);
+        if (err != cudaSuccess) return err;
+    }
     if (st > 48 * 1024) {
-        err = cudaFuncSetAttribute(spread_tile_kernel<R, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st);
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(gather_tile_kernel<R, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st);
+        err = cudaFuncSetAttribute(gather_tile_kernel<R, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st);
         if (err != cudaSuccess) return err;
     }
     const dim3 tgrid((unsigned)t.ntile, (unsigned)a.P);
-    spread_tile_kernel<R, NI><<<tgrid, 256, st, c->stream>>>(a, cell, t);
+    // 8 warps: the spread's warps own the tile's c-planes mod 8
+    spread_tile_kernel<R, NI><<<tgrid, 256, ss_spread, c->stream>>>(a, t);
     const R *twbase = (const R *)(f64 ? (const void *)c->d_twiddle64 : (const void *)c->d_twiddle32);
     const R *tw[3] = {twbase, twbase + 2 * 256, twbase + 4 * 256};
     const size_t sp = pme_plane_smem(a.Na, a.Nb, f64), ss = pme_slab_smem(a.Na, a.Nc, f64);
