@@ -259,104 +259,68 @@ __device__ __forceinline__ void spread_global(const PmeArgs &a, R *g, int la, in
     }
 }
 
-// Spread: one block of 8 warps per (tile, bead), no shared-memory atomics.
-// The bin's records are staged in shared memory a chunk at a time; warp w
-// owns the c-planes of the tile copy whose index is w mod 8 and adds, for
-// every staged record, the stencil rows that fall in its planes (lanes:
-// 8 a points x 4 b rows), so no two threads ever write the same point.
-// The copy is then added to the grid once, with 16-byte vector atomics
-// where the rows allow.  Records whose origin lies outside the tile (none
-// are expected) and overflow records go straight to the grid.
-template <int NI>
-struct SpreadStage {
-    static constexpr int CH = 64;  // records per staged chunk
-    static constexpr int NIP = RecGeom<NI>::NIP;
-};
-
+// Spread: one block per (tile, bead), one warp per record.  A warp adds its
+// record's stencil to a shared copy of the tile with shared-memory atomics;
+// its 32 lanes cover 8 a points x 4 b rows, so the 32 addresses of one
+// atomic are distinct and, with rows padded to PA = 0 mod 8 floats,
+// fall in distinct banks.  The copy is then added to the grid once, with
+// 16-byte vector atomics where the rows allow.  Records whose origin lies
+// outside the tile (none are expected) and overflow records go straight to
+// the grid.
 template <typename R, int NI>
 size_t spread_smem()
 {
-    typedef SpreadStage<NI> SS;
-    return (size_t)TileGeom<NI>::NPT * sizeof(R) + (size_t)SS::CH * (3 * SS::NIP + 1) * sizeof(R) +
-           (size_t)SS::CH * sizeof(int);
+    return (size_t)TileGeom<NI>::NPT * sizeof(R);
 }
 
 template <typename R, int NI>
 __global__ void __launch_bounds__(256) spread_tile_kernel(PmeArgs a, TileArgs t)
 {
     typedef TileGeom<NI> TG;
-    typedef SpreadStage<NI> SS;
-    constexpr int NIP = SS::NIP, CH = SS::CH;
+    typedef RecGeom<NI> RG;
+    constexpr int NIP = RG::NIP;
+    constexpr int NTB = (NI + 3) / 4;  // b rows per lane
     extern __shared__ unsigned char smem_raw[];
     R *tl = (R *)smem_raw;
-    R *sw = tl + TG::NPT;        // [CH][3][NIP]: M_a, M_b, M_c
-    R *sq = sw + CH * 3 * NIP;   // [CH] charge
-    int *sh = (int *)(sq + CH);  // [CH] origin in the copy: oa | ob << 8 | oc << 16, or -1
     for (int i = threadIdx.x; i < TG::NPT; i += blockDim.x) tl[i] = (R)0;
+    __syncthreads();
     const int tile = blockIdx.x, b = blockIdx.y;
     const int ta0 = (tile % t.nta) * TG::T, tb0 = ((tile / t.nta) % t.ntb) * TG::T, tc0 = (tile / (t.nta * t.ntb)) * TG::T;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int la8 = lane & 7, lb4 = lane >> 3;
     const int n = min(t.cnt[b * t.ntile + tile], t.cap);
     const int *list = t.bin + ((size_t)b * t.ntile + tile) * t.cap;
     const R *rw = (const R *)a.rw;
     R *g = (R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
-    const int la8 = lane & 7, lb4 = lane >> 3;
-    const int loff = lb4 * TG::PA + la8;  // this lane's point in a stencil plane
-    for (int c0 = 0; c0 < n; c0 += CH) {
-        const int nc = min(CH, n - c0);
-        __syncthreads();  // the previous chunk is done (and tl is cleared)
-        for (int i = threadIdx.x; i < nc; i += blockDim.x) {
-            const int idx = list[c0 + i];
-            const int4 h = a.rhead[idx];
-            const int oa = h.y - ta0, ob = h.z - tb0, oc = h.w - tc0;
-            const bool in = oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T;
-            sh[i] = in ? (oa | (ob << 8) | (oc << 16)) : -1;
-            sq[i] = (R)a.charge[h.x];
-        }
-        for (int i = threadIdx.x; i < nc * 3 * NIP; i += blockDim.x) {
-            const int e = i / (3 * NIP), j = i - e * (3 * NIP);
-            sw[i] = rw[(size_t)list[c0 + e] * RecGeom<NI>::NW + j];
-        }
-        __syncthreads();
-        for (int e = 0; e < nc; e++) {
-            // lanes of this warp may update a point another lane updated for
-            // the previous record: order their shared-memory accesses
-            __syncwarp();
-            const int h = sh[e];
-            if (h < 0) continue;
-            const int oa = h & 255, ob = (h >> 8) & 255, oc = h >> 16;
-            const R *w = sw + e * 3 * NIP;
-            for (int tc = (warp - oc) & 7; tc < NI; tc += 8) {
-                const R cq = sq[e] * w[2 * NIP + tc];
-                R *base = tl + ((oc + tc) * TG::E + ob) * TG::PA + oa + loff;
+    for (int e = warp; e < n; e += nwarp) {
+        const int idx = list[e];
+        const int4 h = a.rhead[idx];
+        const int oa = h.y - ta0, ob = h.z - tb0, oc = h.w - tc0;
+        const R q = (R)a.charge[h.x];
+        const R *w = rw + (size_t)idx * RG::NW;
+        if (oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T) {
+            R mc[NIP];
+            load4<NIP>(mc, w + 2 * NIP);
+            R mbl[NTB];
 #pragma unroll
-                for (int sa = 0; sa < NI; sa += 8) {
-                    if (la8 + sa >= NI) continue;
-                    const R av = cq * w[la8 + sa];
+            for (int i = 0; i < NTB; i++) mbl[i] = lb4 + 4 * i < NI ? w[NIP + lb4 + 4 * i] : (R)0;
+            R *base = tl + (oc * TG::E + ob + lb4) * TG::PA + oa + la8;
 #pragma unroll
-                    for (int sb = 0; sb < NI; sb += 4) {
-                        if (lb4 + sb < NI) {
-                            R *p = base + sb * TG::PA + sa;
-                            *p += av * w[NIP + lb4 + sb];
-                        }
-                    }
+            for (int sa = 0; sa < NI; sa += 8) {
+                if (la8 + sa >= NI) break;
+                const R qa = q * w[la8 + sa];
+#pragma unroll
+                for (int tc = 0; tc < NI; tc++) {
+                    const R cq = qa * mc[tc];
+#pragma unroll
+                    for (int i = 0; i < NTB; i++)
+                        if (lb4 + 4 * i < NI) atomicAdd(base + (tc * TG::E + 4 * i) * TG::PA + sa, cq * mbl[i]);
                 }
             }
-        }
-    }
-    // records outside the tile (not expected): straight to the grid
-    for (int e0 = 0; e0 < n; e0 += CH) {
-        // re-check from the heads; cheap, and keeps the staged loop branch-free
-        for (int i = warp; i < min(CH, n - e0); i += nwarp) {
-            const int idx = list[e0 + i];
-            const int4 h = a.rhead[idx];
-            const int oa = h.y - ta0, ob = h.z - tb0, oc = h.w - tc0;
-            if (oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T) continue;
-            if (lane < 8) {
-                LaneW<R, NI, false> lw;
-                lw.load(rw, idx, lane);
-                spread_global<R, NI>(a, g, h.y, h.z, h.w, lw, (R)a.charge[h.x], lane);
-            }
+        } else if (lane < 8) {
+            LaneW<R, NI, false> lw;
+            lw.load(rw, idx, lane);
+            spread_global<R, NI>(a, g, h.y, h.z, h.w, lw, q, lane);
         }
     }
     const int grp = threadIdx.x >> 3, l8 = threadIdx.x & 7, ngrp = blockDim.x >> 3;
@@ -1017,7 +981,6 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
         if (err != cudaSuccess) return err;
     }
     const dim3 tgrid((unsigned)t.ntile, (unsigned)a.P);
-    // 8 warps: the spread's warps own the tile's c-planes mod 8
     spread_tile_kernel<R, NI><<<tgrid, 256, ss_spread, c->stream>>>(a, t);
     const R *twbase = (const R *)(f64 ? (const void *)c->d_twiddle64 : (const void *)c->d_twiddle32);
     const R *tw[3] = {twbase, twbase + 2 * 256, twbase + 4 * 256};
