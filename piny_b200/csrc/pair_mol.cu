@@ -144,13 +144,16 @@ struct MolArgs {
     int energy;
 };
 
-// Site-pair constants of the (uniform) molecule: pair type, table row and
-// charge product of site si of molecule i with site sj of molecule j.
+// Site-pair constants of the (uniform) molecule for site si of molecule i
+// and site sj of molecule j, sp = si * NS + sj:
+//   MIXED  c = (rc^2, rmin, dri, q2)
+//   FP64   c = (rc, rmin, dr, dri), q2 separately
+//   o = (table row u * nsplin, vdW table present)
 template <typename R>
 struct PairConst {
-    R rc[16], rmin[16], dr[16], dri[16], q2[16];
-    int off[16];  // table row offset u * nsplin
-    int vdw[16];
+    typename Vec4<R>::T c[16];
+    R q2[16];
+    int2 o[16];
 };
 
 // Exact PINY image shift -NINT(h^-1 dmode) of one site pair along the
@@ -171,6 +174,64 @@ __device__ __forceinline__ double shift_exact(double dm, double hi) { return -ni
 #define PINYB200_MOL_BLOCKS64 3
 #endif
 
+// Spline knot of a MIXED site pair: t = (r - rmin) dri, k = nint(t) + 3
+// clamped to the table, offset del = t - (k - 3).
+__device__ __forceinline__ int knot32(float r, float rmin, float dri, int nsm2, float &del)
+{
+    const float t = (r - rmin) * dri;
+    int k = (int)(t + 0.5f) + 3;
+    k = k < nsm2 ? k : nsm2;
+    k = k > 3 ? k : 3;
+    del = t - (float)(k - 3);
+    return k;
+}
+
+// One site pair of one bead: force -dV/dr * r_vec / r on i (returned in
+// f), energies and virial accumulated.  r holds the separation i - j.
+// The sum is force_npol's: q2 * Coulomb table + vdW table.
+template <typename R, bool FAST, bool ENERGY>
+__device__ __forceinline__ bool site_pair(const typename Vec4<R>::T *__restrict__ tab, size_t tstride, int nsm2,
+                                          const PairConst<R> &pc, int sp, R rx, R ry, R rz, R &fx, R &fy, R &fz,
+                                          R &evs, R &ecs, R *pvs)
+{
+    typedef typename Vec4<R>::T V;
+    const V c = pc.c[sp];
+    const int2 o = pc.o[sp];
+    R del, q2;
+    int kk;
+    if constexpr (FAST) {
+        // MIXED: cutoff on r^2, r from the reciprocal square root
+        const R r2 = rx * rx + ry * ry + rz * rz;
+        if (!(r2 < c.x)) return false;
+        const R r = r2 * rsqrtf(r2);
+        kk = knot32(r, c.y, c.z, nsm2, del);
+        q2 = c.w;
+    } else {
+        const R r = Idx<R>::dist(rx, ry, rz);
+        if (!(r < c.x)) return false;
+        kk = Idx<R>::knot(r, c.y, c.z, c.w, nsm2, del);
+        q2 = pc.q2[sp];
+    }
+    const size_t off = (size_t)o.x + (kk - 1);
+    R dv = 0;
+    if (q2 != (R)0) dv = q2 * spline_eval<V, R>(ldg4(tab + T_CDV0C * tstride + off), del);
+    if (o.y) dv += spline_eval<V, R>(ldg4(tab + T_CDV0 * tstride + off), del);
+    fx = rx * dv;
+    fy = ry * dv;
+    fz = rz * dv;
+    if (ENERGY) {
+        if (q2 != (R)0) ecs += q2 * spline_eval<V, R>(ldg4(tab + T_CV0C * tstride + off), del);
+        if (o.y) evs += spline_eval<V, R>(ldg4(tab + T_CV0 * tstride + off), del);
+        pvs[0] += rx * fx;
+        pvs[1] += ry * fy;
+        pvs[2] += rz * fz;
+        pvs[3] += rx * fy;
+        pvs[4] += rx * fz;
+        pvs[5] += ry * fz;
+    }
+    return true;
+}
+
 template <typename R, int P, int NS, bool FAST, bool ENERGY>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : PINYB200_MOL_BLOCKS64)
     mol_pair_kernel(MolArgs a, Cell cell)
@@ -179,6 +240,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
     constexpr int G = P >= 32 ? 32 : P;  // lanes per molecule pair
     constexpr int JPI = 32 / G;          // molecule pairs per warp step
     __shared__ PairConst<R> pc;
+    __shared__ double sacc[8][128];      // per-thread energy / virial sums
     if (threadIdx.x < NS * NS) {
         // every molecule has the sites of molecule 0 (checked on the host)
         const int si = threadIdx.x / NS, sj = threadIdx.x % NS;
@@ -186,14 +248,25 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
         const int ia = si < nm0 ? si : 0, ja = sj < nm0 ? sj : 0;
         const int p = pair_type(a.atm_typ[ia], a.atm_typ[ja], a.ntyp);
         const int u = a.inter_map[p];
-        pc.rc[threadIdx.x] = (R)a.cutoff[p];
-        pc.off[threadIdx.x] = u * a.nsplin;
-        pc.vdw[threadIdx.x] = a.has_vdw[u];
-        pc.rmin[threadIdx.x] = (R)a.rmin[u];
-        pc.dr[threadIdx.x] = (R)a.dr[u];
-        pc.dri[threadIdx.x] = (R)a.dri[u];
-        pc.q2[threadIdx.x] = (R)(a.charge[ia] * a.charge[ja]);
+        const double q2 = a.charge[ia] * a.charge[ja];
+        V c;
+        if (FAST) {
+            c.x = (R)(a.cutoff[p] * a.cutoff[p]);
+            c.y = (R)a.rmin[u];
+            c.z = (R)a.dri[u];
+            c.w = (R)q2;
+        } else {
+            c.x = (R)a.cutoff[p];
+            c.y = (R)a.rmin[u];
+            c.z = (R)a.dr[u];
+            c.w = (R)a.dri[u];
+        }
+        pc.c[threadIdx.x] = c;
+        pc.q2[threadIdx.x] = (R)q2;
+        pc.o[threadIdx.x] = make_int2(u * a.nsplin, a.has_vdw[u]);
     }
+    if (ENERGY)
+        for (int c = 0; c < 8; c++) sacc[c][threadIdx.x] = 0.0;
     __syncthreads();
     const V *__restrict__ tab = (const V *)a.tab;
     const size_t tstride = (size_t)a.nuniq * a.nsplin;
@@ -204,21 +277,13 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
     const int b = (lane % G) + 32 * blockIdx.y;  // bead
     const int nsm2 = a.nsplin - 2;
     const double *__restrict__ posT = a.posT;
-    const double hd[3] = {cell.h[0], cell.h[4], cell.h[8]};
-    const double hid[3] = {cell.hi[0], cell.hi[4], cell.hi[8]};
-    double half_lim[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) half_lim[d] = 0.5 - 2.0 * PINYB200_MOL_EXTENT * hid[d];
-
-    double ev = 0.0, ec = 0.0, pv[6] = {0, 0, 0, 0, 0, 0};
 
     for (int ch = warp; ch < a.nchunk; ch += nwarps) {
         const int mi = a.chunk[3 * ch], beg = a.chunk[3 * ch + 1], end = a.chunk[3 * ch + 2];
         const int i0 = a.mstart[mi], ni = a.mstart[mi + 1] - i0;
-        double xi[NS][3];  // FP64 mode: all sites; MIXED: site 0 only is kept in FP64
-        R ei[NS][3];
+        double xi[NS][3];  // FP64 positions (MIXED keeps site 0 only live)
+        R ei[NS][3];       // MIXED: offsets from site 0
         R fi[NS][3];
-        double xmi0[3];
 #pragma unroll
         for (int s = 0; s < NS; s++) {
             const int i = i0 + (s < ni ? s : 0);
@@ -229,11 +294,11 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
             }
         }
 #pragma unroll
-        for (int d = 0; d < 3; d++) xmi0[d] = a.xmod[3 * (size_t)i0 + d];
-#pragma unroll
         for (int s = 0; s < NS; s++)
 #pragma unroll
             for (int d = 0; d < 3; d++) ei[s][d] = (R)(xi[s][d] - xi[0][d]);
+        const double xm0x = a.xmod[3 * (size_t)i0], xm0y = a.xmod[3 * (size_t)i0 + 1],
+                     xm0z = a.xmod[3 * (size_t)i0 + 2];
         R evs = 0, ecs = 0, pvs[6] = {0, 0, 0, 0, 0, 0};
         for (int k = beg + sub; k < end; k += JPI) {
             const int mj = a.mj[k];
@@ -253,99 +318,90 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
             // close enough to half a box for site pairs to differ from it
             double sh0[3];
             bool near = false;
+            {
+                const double dm[3] = {__dsub_rn(xm0x, a.xmod[3 * (size_t)j0]),
+                                      __dsub_rn(xm0y, a.xmod[3 * (size_t)j0 + 1]),
+                                      __dsub_rn(xm0z, a.xmod[3 * (size_t)j0 + 2])};
 #pragma unroll
-            for (int d = 0; d < 3; d++) {
-                const double dm = __dsub_rn(xmi0[d], a.xmod[3 * (size_t)j0 + d]);
-                const double t = __dmul_rn(dm, hid[d]);
-                sh0[d] = -nint_rn(t);
-                near |= fabs(t + sh0[d]) > half_lim[d];
+                for (int d = 0; d < 3; d++) {
+                    const double hid = cell.hi[4 * d];
+                    const double t = __dmul_rn(dm[d], hid);
+                    sh0[d] = -nint_rn(t);
+                    near |= fabs(t + sh0[d]) > 0.5 - 2.0 * PINYB200_MOL_EXTENT * hid;
+                }
             }
             R d0[3], ej[NS][3];
             if (FAST) {
 #pragma unroll
-                for (int d = 0; d < 3; d++) d0[d] = (R)(__dsub_rn(xi[0][d], xj[0][d]) + sh0[d] * hd[d]);
+                for (int d = 0; d < 3; d++) d0[d] = (R)(__dsub_rn(xi[0][d], xj[0][d]) + sh0[d] * cell.h[4 * d]);
 #pragma unroll
                 for (int s = 0; s < NS; s++)
 #pragma unroll
                     for (int d = 0; d < 3; d++) ej[s][d] = (R)(xj[s][d] - xj[0][d]);
             }
-            // One loop body for every site pair; per-site values are picked
-            // out of register arrays by predicated static-index loops, so the
-            // arrays stay in registers and the code stays small.
+            // j sites in a warp-uniform loop (for P >= 32 the mask is the
+            // same in every lane); i sites unrolled so their offsets and
+            // forces stay in fixed registers
 #pragma unroll 1
             for (int sj = 0; sj < NS; sj++) {
                 unsigned col = 0;
 #pragma unroll
                 for (int si = 0; si < NS; si++) col |= ((mask >> (si * NS + sj)) & 1u) << si;
                 if (!col) continue;
-                R ejx = 0, ejy = 0, ejz = 0;
+                // j-site position: MIXED d0 - e_j, FP64 x_j
+                R djx = 0, djy = 0, djz = 0;
                 double xjx = 0, xjy = 0, xjz = 0;
 #pragma unroll
                 for (int s2 = 0; s2 < NS; s2++)
                     if (sj == s2) {
-                        if (FAST) { ejx = ej[s2][0]; ejy = ej[s2][1]; ejz = ej[s2][2]; }
-                        else { xjx = xj[s2][0]; xjy = xj[s2][1]; xjz = xj[s2][2]; }
+                        if (FAST) {
+                            djx = d0[0] - ej[s2][0];
+                            djy = d0[1] - ej[s2][1];
+                            djz = d0[2] - ej[s2][2];
+                        } else {
+                            xjx = xj[s2][0];
+                            xjy = xj[s2][1];
+                            xjz = xj[s2][2];
+                        }
                     }
+                double xmj[3] = {0, 0, 0};
+                if (near)
+#pragma unroll
+                    for (int d = 0; d < 3; d++) xmj[d] = a.xmod[3 * (size_t)(j0 + sj) + d];
                 R fjx = 0, fjy = 0, fjz = 0;
-                while (col) {
-                    const int si = __ffs(col) - 1;
-                    col &= col - 1u;
-                    const int sp = si * NS + sj;
+#pragma unroll
+                for (int si = 0; si < NS; si++) {
+                    if (!((col >> si) & 1u)) continue;
                     double sh[3] = {sh0[0], sh0[1], sh0[2]};
                     if (near) {
 #pragma unroll
                         for (int d = 0; d < 3; d++)
-                            sh[d] = shift_exact(__dsub_rn(a.xmod[3 * (size_t)(i0 + si) + d],
-                                                          a.xmod[3 * (size_t)(j0 + sj) + d]), hid[d]);
+                            sh[d] = shift_exact(__dsub_rn(a.xmod[3 * (size_t)(i0 + si) + d], xmj[d]), cell.hi[4 * d]);
                     }
                     R rx, ry, rz;
                     if (FAST) {
-                        R eix = 0, eiy = 0, eiz = 0;
-#pragma unroll
-                        for (int s2 = 0; s2 < NS; s2++)
-                            if (si == s2) { eix = ei[s2][0]; eiy = ei[s2][1]; eiz = ei[s2][2]; }
-                        rx = d0[0] + (eix - ejx);
-                        ry = d0[1] + (eiy - ejy);
-                        rz = d0[2] + (eiz - ejz);
+                        rx = djx + ei[si][0];
+                        ry = djy + ei[si][1];
+                        rz = djz + ei[si][2];
                         if (near) {
-                            rx += (R)((sh[0] - sh0[0]) * hd[0]);
-                            ry += (R)((sh[1] - sh0[1]) * hd[1]);
-                            rz += (R)((sh[2] - sh0[2]) * hd[2]);
+                            rx += (R)((sh[0] - sh0[0]) * cell.h[0]);
+                            ry += (R)((sh[1] - sh0[1]) * cell.h[4]);
+                            rz += (R)((sh[2] - sh0[2]) * cell.h[8]);
                         }
                     } else {
-                        double xix = 0, xiy = 0, xiz = 0;
-#pragma unroll
-                        for (int s2 = 0; s2 < NS; s2++)
-                            if (si == s2) { xix = xi[s2][0]; xiy = xi[s2][1]; xiz = xi[s2][2]; }
-                        rx = (R)__dadd_rn(__dsub_rn(xix, xjx), __dmul_rn(sh[0], hd[0]));
-                        ry = (R)__dadd_rn(__dsub_rn(xiy, xjy), __dmul_rn(sh[1], hd[1]));
-                        rz = (R)__dadd_rn(__dsub_rn(xiz, xjz), __dmul_rn(sh[2], hd[2]));
+                        rx = (R)__dadd_rn(__dsub_rn(xi[si][0], xjx), __dmul_rn(sh[0], cell.h[0]));
+                        ry = (R)__dadd_rn(__dsub_rn(xi[si][1], xjy), __dmul_rn(sh[1], cell.h[4]));
+                        rz = (R)__dadd_rn(__dsub_rn(xi[si][2], xjz), __dmul_rn(sh[2], cell.h[8]));
                     }
-                    const R r = Idx<R>::dist(rx, ry, rz);
-                    if (!(r < pc.rc[sp])) continue;
-                    R del;
-                    const int kk = Idx<R>::knot(r, pc.rmin[sp], pc.dr[sp], pc.dri[sp], nsm2, del);
-                    const R q2 = pc.q2[sp];
-                    const size_t off = (size_t)pc.off[sp] + (kk - 1);
-                    const bool vdw = pc.vdw[sp] != 0;
-                    R dv = q2 * spline_eval<V, R>(ldg4(tab + T_CDV0C * tstride + off), del);
-                    if (vdw) dv += spline_eval<V, R>(ldg4(tab + T_CDV0 * tstride + off), del);
-                    const R fx = rx * dv, fy = ry * dv, fz = rz * dv;
-#pragma unroll
-                    for (int s2 = 0; s2 < NS; s2++)
-                        if (si == s2) { fi[s2][0] += fx; fi[s2][1] += fy; fi[s2][2] += fz; }
-                    fjx -= fx;
-                    fjy -= fy;
-                    fjz -= fz;
-                    if (ENERGY) {
-                        ecs += q2 * spline_eval<V, R>(ldg4(tab + T_CV0C * tstride + off), del);
-                        if (vdw) evs += spline_eval<V, R>(ldg4(tab + T_CV0 * tstride + off), del);
-                        pvs[0] += rx * fx;
-                        pvs[1] += ry * fy;
-                        pvs[2] += rz * fz;
-                        pvs[3] += rx * fy;
-                        pvs[4] += rx * fz;
-                        pvs[5] += ry * fz;
+                    R fx, fy, fz;
+                    if (site_pair<R, FAST, ENERGY>(tab, tstride, nsm2, pc, si * NS + sj, rx, ry, rz, fx, fy, fz, evs,
+                                                   ecs, pvs)) {
+                        fi[si][0] += fx;
+                        fi[si][1] += fy;
+                        fi[si][2] += fz;
+                        fjx -= fx;
+                        fjy -= fy;
+                        fjz -= fz;
                     }
                 }
                 if (fjx != (R)0 || fjy != (R)0 || fjz != (R)0) {
@@ -367,17 +423,18 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
                     atomicAdd(&a.forceT[(3 * (size_t)(i0 + s) + d) * P + b], v);
             }
         }
-        ev += (double)evs;
-        ec += (double)ecs;
+        if (ENERGY) {
+            sacc[0][threadIdx.x] += (double)evs;
+            sacc[1][threadIdx.x] += (double)ecs;
 #pragma unroll
-        for (int c = 0; c < 6; c++) pv[c] += (double)pvs[c];
+            for (int c = 0; c < 6; c++) sacc[2 + c][threadIdx.x] += (double)pvs[c];
+        }
     }
     if (ENERGY) {
-        double v[8] = {ev, ec, pv[0], pv[1], pv[2], pv[3], pv[4], pv[5]};
         const int slot[8] = {S_VVDW, S_VCOUL, S_PXX, S_PYY, S_PZZ, S_PXY, S_PXZ, S_PYZ};
 #pragma unroll
         for (int c = 0; c < 8; c++) {
-            double t = v[c];
+            double t = sacc[c][threadIdx.x];
             if (G < 32) t = warp_sum_strided(t, G);
             if (G == 32 || sub == 0) atomicAdd(&a.acc[(size_t)b * S_NSLOT + slot[c]], t);
         }
