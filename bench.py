@@ -397,10 +397,15 @@ def main():
 
 
 def box_launches(S, P):
-    """Kernels one evaluation launches: transpose in, ghost positions, pair,
-    spread, 6 FFT passes, convolution, gather, bond, bend, ecor, transpose
-    out (the memsets are not kernels)."""
-    return 1 + (1 if S.get("nghost", 0) else 0) + 1 + 1 + 6 + 1 + 1 + 3 + 1
+    """Kernels one evaluation launches (memsets are not kernels): transpose
+    in, ghost positions, the pair kernel, PME (bin, spread, plane FFT,
+    c-axis FFT with the convolution, inverse plane FFT, gather), bond, bend,
+    excluded-pair correction, transpose out."""
+    n = 1 + (1 if S.get("nghost", 0) else 0) + 1
+    if int(np.count_nonzero(S["charge"])) and S.get("nktot", 0):
+        n += 6
+    n += (1 if S.get("nbond", 0) else 0) + (1 if S.get("nbend", 0) else 0) + (1 if S.get("necor", 0) else 0)
+    return n + 1
 
 
 if __name__ == "__main__":
