@@ -46,6 +46,7 @@ def parse_args():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-energy", action="store_true", help="forces only (PINYB200_NO_ENERGY), for profiling")
     return ap.parse_args()
 
 
@@ -249,7 +250,7 @@ def main():
 
     def step(b, force):
         return b.energy_force_device(d_pos.data_ptr(), d_xmod.data_ptr(), hmat, force.data_ptr(),
-                                     stream=stream.cuda_stream)
+                                     stream=stream.cuda_stream, energy=not args.no_energy)
 
     for _ in range(max(3, args.warmup)):
         step(box, d_force)

@@ -170,6 +170,27 @@ int pinyb200_build_list(pinyb200_ctx *ctx, const double *pos1,
 int pinyb200_get_list(pinyb200_ctx *ctx, int *pi, int *pj, long cap,
                       long *npairs);
 
+/*
+ * Rebuild test of the current list for positions on the device, as PINY
+ * runs it each step before the force call (nbr_list_control.c:63-110):
+ *   *rmax       = max over atoms of |r(bead 1) - r(at the last build)|
+ *                 (check_ver_list, nbr_list_control.c:182-247);
+ *   *spread_now = max over beads > 1 and atoms of |r(bead) - r(bead 1)|
+ *                 (get_pimd_spread, pimd_estimators.c:121-220; 0 for P = 1);
+ *   *rebuild    = rmax > skin/2 + max(0, spread_now - spread_ref), where
+ *                 spread_ref is PINY's interact.spread (the spread when the
+ *                 list was last rebuilt; set it to spread_now on a rebuild);
+ *   cutskin2    = (cutoff + skin + spread_now)^2 per type pair (get_cut_skin,
+ *                 nbr_list_control.c:249-281), the radii for the next
+ *                 pinyb200_build_list; may be NULL.
+ * d_pos: nbeads x natm x 3 device array; stream as in
+ * pinyb200_energy_force_device.  Any output pointer may be NULL.
+ */
+int pinyb200_check_list_device(pinyb200_ctx *ctx, const double *d_pos,
+                               double spread_ref, int *rebuild, double *rmax,
+                               double *spread_now, double *cutskin2,
+                               void *stream);
+
 /* Sizes of the current list: all pairs, the force-bearing ("active") pairs
  * the pair kernel walks (a charge product or a vdW table), and capacity. */
 int pinyb200_list_info(pinyb200_ctx *ctx, long *npairs, long *nactive,

@@ -189,6 +189,20 @@ class Oracle:
         return self.lib.orc_clong(len(at), ntyp, pa, p6, pc, rheal, iswit)
 
     # -- evaluation --------------------------------------------------------
+    def check_list(self, pos, x0, skin, spread_ref, cutoff):
+        """PINY's list rebuild test (orc_check_list): (rebuild, rmax,
+        spread_now, cutskin2)."""
+        pos = np.ascontiguousarray(pos, np.float64)
+        P, natm = pos.shape[0], pos.shape[1]
+        x0 = np.ascontiguousarray(x0, np.float64).reshape(natm, 3)
+        cut = np.ascontiguousarray(cutoff, np.float64)
+        cs = np.zeros(len(cut))
+        rmax, sp = C.c_double(), C.c_double()
+        f = self.lib.orc_check_list(natm, P, pos.ctypes.data_as(_pd), x0.ctypes.data_as(_pd), C.c_double(skin),
+                                    C.c_double(spread_ref), len(cut), cut.ctypes.data_as(_pd), C.byref(rmax),
+                                    C.byref(sp), cs.ctypes.data_as(_pd))
+        return bool(f), rmax.value, sp.value, cs
+
     def verlist(self, sysd, pos1, xmod, hmat, cutskin2):
         s = self.make_struct(sysd)
         pos1 = np.ascontiguousarray(pos1, np.float64).reshape(-1, 3)

@@ -1028,3 +1028,47 @@ void orc_energy_force(const orc_system *s, int P, const double *pos_in, const do
     e->vintrat = e->vbond + e->vbend;
     for (int c = 0; c < 9; c++) e->pvten[c] = pv[c];
 }
+
+/* ------------------------------------------------------------------------ */
+/* Verlet-list rebuild test.                                                 */
+/* check_ver_list:  src/energy/inter/real_space/nbr_list_control.c:182-247 */
+/* get_pimd_spread: src/energy/pimd/pimd_estimators.c:121-220 (bead 1 is   */
+/*                  the reference, beads 2..P are compared with it)        */
+/* get_cut_skin:    nbr_list_control.c:249-281 (plain cutskin only)         */
+/* ------------------------------------------------------------------------ */
+int orc_check_list(int natm, int nbeads, const double *pos, const double *x0,
+                   double skin, double spread_ref, int ninter,
+                   const double *cutoff, double *rmax, double *spread_now,
+                   double *cutskin2)
+{
+    double r2max = 0.0, s2max = 0.0;
+    for (int i = 0; i < natm; i++) {
+        double dx = pos[3 * i] - x0[3 * i];
+        double dy = pos[3 * i + 1] - x0[3 * i + 1];
+        double dz = pos[3 * i + 2] - x0[3 * i + 2];
+        double r2 = dx * dx + dy * dy + dz * dz;
+        r2max = r2max > r2 ? r2max : r2;
+    }
+    for (int b = 1; b < nbeads; b++)
+        for (int i = 0; i < natm; i++) {
+            const double *p = pos + ((size_t)b * natm + i) * 3;
+            double dx = p[0] - pos[3 * i];
+            double dy = p[1] - pos[3 * i + 1];
+            double dz = p[2] - pos[3 * i + 2];
+            double r2 = dx * dx + dy * dy + dz * dz;
+            s2max = s2max > r2 ? s2max : r2;
+        }
+    double rm = sqrt(r2max);
+    double sp = nbeads > 1 ? sqrt(s2max) : 0.0;
+    double dspread = 0.0;
+    if (nbeads > 1) dspread = (sp - spread_ref) > 0.0 ? (sp - spread_ref) : 0.0;
+    double skin2 = skin / 2.0 + dspread;
+    if (rmax) *rmax = rm;
+    if (spread_now) *spread_now = sp;
+    if (cutskin2)
+        for (int k = 0; k < ninter; k++) {
+            double cs = cutoff[k] + skin + sp;
+            cutskin2[k] = cs * cs;
+        }
+    return rm > skin2 ? 1 : 0;
+}

@@ -146,6 +146,15 @@ long orc_verlist(const orc_system *sys, const double *x, const double *y,
                  const double *zmod, const double *hmat, const double *hmati,
                  const double *cutskin2, long cap, int *pi, int *pj);
 
+/* Verlet-list rebuild test: check_ver_list (nbr_list_control.c:182-247),
+ * get_pimd_spread (pimd_estimators.c:121-220), get_cut_skin
+ * (nbr_list_control.c:249-281).  pos: nbeads x natm x 3, x0: natm x 3 bead-1
+ * positions at the last build.  Returns the rebuild flag. */
+int orc_check_list(int natm, int nbeads, const double *pos, const double *x0,
+                   double skin, double spread_ref, int ninter,
+                   const double *cutoff, double *rmax, double *spread_now,
+                   double *cutskin2);
+
 void orc_energy_force(const orc_system *sys, int nbeads, const double *pos,
                       const double *xmod, const double *hmat,
                       long npairs, const int *pi, const int *pj,

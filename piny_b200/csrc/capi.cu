@@ -15,6 +15,12 @@
 
 using namespace pinyb200;
 
+// Molecule pairs per warp chunk of the molecule-pair kernel (per lane group
+// when P < 32): the i sites are loaded and their forces flushed once per chunk.
+#ifndef PINYB200_MOL_CHUNK
+#define PINYB200_MOL_CHUNK 8
+#endif
+
 namespace {
 
 thread_local std::string g_lib_err;
@@ -194,7 +200,7 @@ int pinyb200_destroy(pinyb200_ctx *c)
     void *ptrs[] = {c->d_row, c->d_col, c->d_rowA, c->d_colA, c->d_count, c->d_tot, c->d_posT, c->d_forceT,
                     c->d_xmod, c->d_pos_aos, c->d_force_aos, c->d_acc, c->d_grid, c->d_spec, c->d_filter, c->d_twiddle64,
                     c->d_twiddle32, c->d_err, c->d_mstart, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_chunk,
-                    c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf,
+                    c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf, c->d_x0,
                     c->d_pme_head, c->d_pme_w};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -237,6 +243,8 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
     CK(upload(&d.atm_typ, s->atm_typ, natm));
     CK(upload(&d.charge, s->charge, natm));
     c->h_charge.assign(s->charge, s->charge + natm);
+    c->h_cutoff.assign(s->cutoff, s->cutoff + s->ntyp * (s->ntyp + 1) / 2);
+    c->skin = s->skin;
     CK(upload(&d.inter_map, s->inter_map, d.npair_typ));
     CK(upload(&d.cutoff, s->cutoff, d.npair_typ));
     CK(upload(&d.rmin, s->rmin_spl, d.nuniq));
@@ -396,6 +404,7 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
     CK(cudaMalloc(&c->d_pos_aos, nb * sizeof(double)));
     CK(cudaMalloc(&c->d_force_aos, nb * sizeof(double)));
     CK(cudaMalloc(&c->d_xmod, (size_t)natm * 3 * sizeof(double)));
+    CK(cudaMalloc(&c->d_x0, (size_t)natm * 3 * sizeof(double)));
     CK(cudaMalloc(&c->d_acc, (size_t)nbeads * S_NSLOT * sizeof(double)));
     CK(cudaMalloc(&c->d_row, (size_t)(natm + 1) * sizeof(int)));
     CK(cudaMalloc(&c->d_rowA, (size_t)(natm + 1) * sizeof(int)));
@@ -484,6 +493,8 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
         c->list_cap = cap;
     }
     CK(launch_build_list(c, cell, d_p1, d_xm, d_cs, 1));
+    // the rebuild test measures displacements from these positions
+    CK(cudaMemcpyAsync(c->d_x0, d_p1, (size_t)natm * 3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->npairs = tot[0];
     c->nactive = tot[1];
@@ -513,7 +524,7 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
             std::vector<int> mrow(c->nmol + 1);
             CK(cudaMemcpy(mrow.data(), c->d_mrow, mrow.size() * sizeof(int), cudaMemcpyDeviceToHost));
             const int jpi = c->P >= 32 ? 1 : 32 / c->P;
-            const int ch = 8 * jpi;
+            const int ch = PINYB200_MOL_CHUNK * jpi;
             std::vector<int> chunks;
             for (int m = 0; m < c->nmol; m++)
                 for (int k = mrow[m]; k < mrow[m + 1]; k += ch) {
@@ -774,6 +785,39 @@ int pinyb200_count_list_device(pinyb200_ctx *c, const double *d_pos1, const doub
     CK(cudaStreamSynchronize(st));
     if (npairs) *npairs = (long)tot[0];
     if (nactive) *nactive = (long)tot[1];
+    return PINYB200_OK;
+}
+
+int pinyb200_check_list_device(pinyb200_ctx *c, const double *d_pos, double spread_ref, int *rebuild,
+                               double *rmax, double *spread_now, double *cutskin2, void *stream)
+{
+    if (!c || !d_pos) return fail(c, PINYB200_ERR_ARG, "check_list_device: NULL argument");
+    if (!c->have_list) return fail(c, PINYB200_ERR_STATE, "check_list_device: no list built yet");
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    unsigned long long *d_out = (unsigned long long *)(c->d_tot + 2);  // list totals slots, free after a build
+    CK(cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), st));
+    CK(launch_list_check(c, d_pos, d_out, st));
+    unsigned long long h[2];
+    CK(cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double r2max, s2max;
+    memcpy(&r2max, &h[0], sizeof(double));
+    memcpy(&s2max, &h[1], sizeof(double));
+    // check_ver_list (nbr_list_control.c:225-241) and get_cut_skin (:249-281)
+    const double rm = sqrt(r2max);
+    const double sp = c->P > 1 ? sqrt(s2max) : 0.0;
+    double dspread = 0.0;
+    if (c->P > 1) dspread = sp - spread_ref > 0.0 ? sp - spread_ref : 0.0;
+    const double skin2 = c->skin / 2.0 + dspread;
+    if (rebuild) *rebuild = rm > skin2 ? 1 : 0;
+    if (rmax) *rmax = rm;
+    if (spread_now) *spread_now = sp;
+    if (cutskin2)
+        for (int k = 0; k < c->sys.npair_typ; k++) {
+            const double cs = c->h_cutoff[k] + c->skin + sp;
+            cutskin2[k] = cs * cs;
+        }
     return PINYB200_OK;
 }
 

@@ -81,6 +81,8 @@ struct pinyb200_ctx {
     pinyb200::DeviceSystem sys;
     // host copies needed for energy bookkeeping
     std::vector<double> h_charge;
+    std::vector<double> h_cutoff;  // per type pair (Bohr)
+    double skin = 0;               // Verlet skin (Bohr)
     double alp_ewd = 0, self_erf = 1, clong = 0;
     int iswit_vdw = 1;
     // Verlet list: full (parity) and active (force) CSR by i, j < i
@@ -107,6 +109,7 @@ struct pinyb200_ctx {
     double *d_posT = nullptr;     // [natm][3][P]
     double *d_forceT = nullptr;   // [natm][3][P]
     double *d_xmod = nullptr;     // [natm][3]
+    double *d_x0 = nullptr;       // [natm][3] bead-1 positions at the last list build
     double *d_pos_aos = nullptr;  // [P][natm][3] staging for host calls
     double *d_force_aos = nullptr;
     double *d_acc = nullptr;      // [P][S_NSLOT]
@@ -151,6 +154,7 @@ cudaError_t launch_transpose_in(pinyb200_ctx *c, const double *d_pos_aos);
 cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_force_aos);
 cudaError_t launch_list_count(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
                               const double *d_cutskin2, int *d_count, cudaStream_t st);
+cudaError_t launch_list_check(pinyb200_ctx *c, const double *d_pos, unsigned long long *d_out, cudaStream_t st);
 cudaError_t launch_count_total(pinyb200_ctx *c, const int *d_count, unsigned long long *d_tot, cudaStream_t st);
 size_t pme_plane_smem(int Na, int Nb, bool fp64);
 size_t pme_slab_smem(int Na, int Nc, bool fp64);

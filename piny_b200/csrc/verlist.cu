@@ -207,3 +207,49 @@ cudaError_t launch_count_total(pinyb200_ctx *c, const int *d_count, unsigned lon
 }
 
 }  // namespace pinyb200
+
+namespace pinyb200 {
+
+// Rebuild test of the Verlet list on the device (check_ver_list,
+// nbr_list_control.c:182-247, and get_pimd_spread, pimd_estimators.c:
+// 121-220): out[0] = max_i |r_i(bead 1) - r_i(at the last build)|^2,
+// out[1] = max over beads b > 1 and atoms i of |r_i(b) - r_i(bead 1)|^2,
+// both as the bit patterns of non-negative doubles (ordered like the
+// values) and both zero on entry.  Squares are formed without FMA
+// contraction, in PINY's order.  pos: [P][natm][3], x0: [natm][3].
+__global__ void __launch_bounds__(256) list_check_kernel(int natm, int P, const double *__restrict__ pos,
+                                                         const double *__restrict__ x0,
+                                                         unsigned long long *__restrict__ out)
+{
+    double dmax = 0.0, smax = 0.0;
+    const long long n = (long long)natm * P;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(t / natm), i = (int)(t % natm);
+        const double *p = pos + ((size_t)b * natm + i) * 3;
+        const double *q = b == 0 ? x0 + (size_t)i * 3 : pos + (size_t)i * 3;
+        const double dx = __dsub_rn(p[0], q[0]), dy = __dsub_rn(p[1], q[1]), dz = __dsub_rn(p[2], q[2]);
+        const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        if (b == 0) dmax = fmax(dmax, r2);
+        else smax = fmax(smax, r2);
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+        dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+        smax = fmax(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&out[0], (unsigned long long)__double_as_longlong(dmax));
+        atomicMax(&out[1], (unsigned long long)__double_as_longlong(smax));
+    }
+}
+
+cudaError_t launch_list_check(pinyb200_ctx *c, const double *d_pos, unsigned long long *d_out, cudaStream_t st)
+{
+    const long long n = (long long)c->sys.natm * c->P;
+    long long blocks = (n + 255) / 256;
+    if (blocks > (long long)c->sm_count * 4) blocks = (long long)c->sm_count * 4;
+    if (blocks < 1) blocks = 1;
+    list_check_kernel<<<(unsigned)blocks, 256, 0, st>>>(c->sys.natm, c->P, d_pos, c->d_x0, d_out);
+    return cudaGetLastError();
+}
+
+}  // namespace pinyb200

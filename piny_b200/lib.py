@@ -62,7 +62,7 @@ class PinyEnergies(C.Structure):
 EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb200_destroy",
            "pinyb200_build_list", "pinyb200_get_list", "pinyb200_list_info", "pinyb200_energy_force",
            "pinyb200_energy_force_device", "pinyb200_piny_force", "pinyb200_last_timing",
-           "pinyb200_last_error", "pinyb200_count_list_device")
+           "pinyb200_last_error", "pinyb200_count_list_device", "pinyb200_check_list_device")
 
 COUNT_MAX_ATOMS = 65536       # PINYB200_COUNT_MAX_ATOMS
 COUNT_MAX_PAIR_TYPES = 64     # PINYB200_COUNT_MAX_PAIR_TYPES
@@ -100,6 +100,7 @@ def load(build_if_missing: bool = True):
     L.pinyb200_last_timing.argtypes = [C.c_void_p, C.POINTER(C.c_float), _i]
     L.pinyb200_count_list_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, _pd, C.POINTER(C.c_long),
                                              C.POINTER(C.c_long), C.c_void_p]
+    L.pinyb200_check_list_device.argtypes = [C.c_void_p, C.c_void_p, _d, _pi, _pd, _pd, _pd, C.c_void_p]
     L.pinyb200_last_error.restype = C.c_char_p
     L.pinyb200_last_error.argtypes = [C.c_void_p]
     _LIB = L
@@ -190,6 +191,18 @@ class DeviceBox:
                                                       None if stream is None else C.c_void_p(stream)),
                     "count_list_device")
         return n.value, a.value
+
+    def check_list_device(self, d_pos: int, spread_ref: float = 0.0, stream=None):
+        """PINY's list rebuild test for device-resident positions [P][natm][3]:
+        (rebuild, rmax, spread_now, cutskin2 for the next build)."""
+        reb = C.c_int()
+        rmax, spread = C.c_double(), C.c_double()
+        cs = np.zeros(self.ntyp * (self.ntyp + 1) // 2)
+        self._check(self.L.pinyb200_check_list_device(self.h, C.c_void_p(d_pos), float(spread_ref), C.byref(reb),
+                                                      C.byref(rmax), C.byref(spread), _dp(cs),
+                                                      None if stream is None else C.c_void_p(stream)),
+                    "check_list_device")
+        return bool(reb.value), rmax.value, spread.value, cs
 
     def get_list(self):
         n = C.c_long()

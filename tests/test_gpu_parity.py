@@ -141,3 +141,31 @@ def test_pme_grid_paths_match_oracle(case, prec, oracle):
     scale = abs(eref["vvdw"]) + abs(eref["vcoul"]) + abs(eref["vrecip"]) + abs(eref["vself"]) + abs(eref["vecor"])
     assert abs(e["vintert"] - eref["vintert"]) <= ETOL[prec] * scale
     box.close()
+
+
+@pytest.mark.parametrize("name", ["tip4pf_64_p4", "spcfw_64_p1"])
+def test_list_check_matches_oracle(name, oracle):
+    """Device rebuild test (check_ver_list + get_pimd_spread + get_cut_skin)
+    against the oracle, bit for bit, before and after a displacement."""
+    import torch
+
+    from piny_b200.lib import DeviceBox
+    F = load_fixture(name)
+    P = int(F["nbeads"])
+    box = DeviceBox(F, P, "fp64")
+    xmod = F.get("xmod")
+    pos = np.ascontiguousarray(F["pos"], np.float64)
+    box.build_list(pos[0], xmod, F["hmat"], F["cutskin2"])
+    x0 = pos[0].copy()
+    rng = np.random.default_rng(11)
+    cutoff = np.asarray(F["cutoff"], np.float64)
+    skin = float(F["skin"])
+    for scale, spread_ref in ((0.0, 0.0), (0.2, 0.1), (1.5, 0.0)):
+        p = pos + rng.normal(scale=scale, size=pos.shape) if scale else pos
+        d = torch.from_numpy(np.ascontiguousarray(p)).to("cuda:0")
+        torch.cuda.synchronize()
+        reb, rmax, sp, cs = box.check_list_device(d.data_ptr(), spread_ref)
+        f, r_o, s_o, cs_o = oracle.check_list(p, x0, skin, spread_ref, cutoff)
+        assert (reb, rmax, sp) == (f, r_o, s_o)
+        assert np.array_equal(cs, cs_o)
+    box.close()

@@ -73,3 +73,20 @@ def test_oracle_setup_tables(oracle):
     c6[0] = 4.0 * eps * sig ** 6
     cl = oracle.clong(F["atm_typ"], F["ntyp"], c6, F["cutoff"], 1.0 / BOHR, 1)
     assert abs(cl - F["clong"]) < 1e-12 * abs(F["clong"])
+
+
+def test_oracle_list_check_matches_numpy(oracle):
+    """The rebuild-test restatement against a direct numpy statement of
+    check_ver_list / get_pimd_spread / get_cut_skin."""
+    rng = np.random.default_rng(3)
+    for P in (1, 4):
+        x0 = rng.normal(size=(50, 3)) * 10
+        pos = x0[None] + rng.normal(scale=0.3, size=(P, 50, 3))
+        cutoff = np.array([17.0, 16.5, 15.0])
+        for skin, spread_ref in ((1.89, 0.0), (0.5, 0.2), (3.0, 5.0)):
+            f, rmax, sp, cs = oracle.check_list(pos, x0, skin, spread_ref, cutoff)
+            r = np.sqrt(((pos[0] - x0) ** 2).sum(1).max())
+            s = np.sqrt(((pos[1:] - pos[0][None]) ** 2).sum(2).max()) if P > 1 else 0.0
+            assert rmax == pytest.approx(r, rel=1e-15) and sp == pytest.approx(s, rel=1e-15)
+            assert f == (r > skin / 2 + (max(0.0, s - spread_ref) if P > 1 else 0.0))
+            assert np.allclose(cs, (cutoff + skin + s) ** 2, rtol=1e-15)
