@@ -263,9 +263,10 @@ int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
                         double *const *fy, double *const *fz,
                         double *pvten_tot, pinyb200_energies *e);
 
-/* Milliseconds of the last evaluation, from CUDA events on its stream:
- * 0 device work, 1 pair forces, 2 PME, 3 intramolecular, 4 the whole
- * host-buffer call of pinyb200_energy_force (copies included). */
+/* Milliseconds of the last evaluation, from CUDA events: 0 device work,
+ * 1 pair forces, 2 PME, 3 intramolecular, 4 the whole host-buffer call of
+ * pinyb200_energy_force (copies included).  PME runs on a second stream of
+ * the context, concurrently with 1 and 3, so 1 + 2 + 3 may exceed 0. */
 int pinyb200_last_timing(pinyb200_ctx *ctx, float *ms, int n);
 
 /* Last error text for this context (or the library if ctx is NULL). */

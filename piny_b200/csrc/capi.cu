@@ -200,12 +200,16 @@ int pinyb200_destroy(pinyb200_ctx *c)
     void *ptrs[] = {c->d_row, c->d_col, c->d_rowA, c->d_colA, c->d_count, c->d_tot, c->d_posT, c->d_forceT,
                     c->d_xmod, c->d_pos_aos, c->d_force_aos, c->d_acc, c->d_grid, c->d_spec, c->d_filter, c->d_twiddle64,
                     c->d_twiddle32, c->d_err, c->d_mstart, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_chunk,
-                    c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf, c->d_x0,
+                    c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf, c->d_x0, c->d_forceP,
                     c->d_pme_head, c->d_pme_w};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    cudaEvent_t evx[4] = {c->ev_fork, c->ev_join, c->ev_pme[0], c->ev_pme[1]};
+    for (cudaEvent_t ev : evx)
+        if (ev) cudaEventDestroy(ev);
+    if (c->pme_stream) cudaStreamDestroy(c->pme_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PINYB200_OK;
@@ -231,7 +235,11 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
     c->precision = precision;
     c->P = nbeads;
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->pme_stream, cudaStreamNonBlocking));
     for (int i = 0; i < 8; i++) CK(cudaEventCreate(&c->ev[i]));
+    CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+    for (int i = 0; i < 2; i++) CK(cudaEventCreate(&c->ev_pme[i]));
 
     DeviceSystem &d = c->sys;
     const int natm = s->natm;
@@ -335,6 +343,7 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
         const int nip = s->n_interp <= 4 ? 4 : (s->n_interp <= 8 ? 8 : 12);
         const size_t nrec = (size_t)std::max(1, d.nchrg) * nbeads;
         CK(cudaMalloc(&c->d_pme_head, nrec * 4 * sizeof(int)));
+        CK(cudaMalloc(&c->d_forceP, nrec * 3 * sizeof(double)));
         CK(cudaMalloc(&c->d_pme_w, nrec * 6 * nip * rsz));
         // twiddles exp(2 pi i m / N) per axis, 256 entries each
         std::vector<double> tw(2 * 256 * 3, 0.0);
@@ -571,14 +580,30 @@ static int evaluate(pinyb200_ctx *c, const Cell &cell, int flags, pinyb200_energ
     CK(cudaMemsetAsync(c->d_forceT, 0, nb * sizeof(double), c->stream));
     CK(cudaMemsetAsync(c->d_acc, 0, (size_t)c->P * S_NSLOT * sizeof(double), c->stream));
     CK(cudaEventRecord(c->ev[1], c->stream));
+    // PME on its own stream, concurrently with the pair and intramolecular
+    // kernels: it reads the positions, writes its own force buffer and adds
+    // its energies and virial atomically
+    CK(cudaEventRecord(c->ev_fork, c->stream));
+    CK(cudaStreamWaitEvent(c->pme_stream, c->ev_fork, 0));
+    {
+        cudaStream_t main_stream = c->stream;
+        c->stream = c->pme_stream;
+        cudaError_t perr = cudaEventRecord(c->ev_pme[0], c->stream);
+        if (perr == cudaSuccess) perr = launch_pme(c, cell, energy);
+        if (perr == cudaSuccess) perr = cudaEventRecord(c->ev_pme[1], c->stream);
+        if (perr == cudaSuccess) perr = cudaEventRecord(c->ev_join, c->stream);
+        c->stream = main_stream;
+        CK(perr);
+    }
     const bool ortho = cell.h[1] == 0.0 && cell.h[2] == 0.0 && cell.h[3] == 0.0 && cell.h[5] == 0.0 &&
                        cell.h[6] == 0.0 && cell.h[7] == 0.0;
     if (c->use_mol && c->mol_ok && ortho && !(flags & PINYB200_SITE_PAIRS)) CK(launch_mol_pair(c, cell, energy));
     else CK(launch_pair(c, cell, energy));
     CK(cudaEventRecord(c->ev[2], c->stream));
-    CK(launch_pme(c, cell, energy));
-    CK(cudaEventRecord(c->ev[3], c->stream));
     CK(launch_intra(c, cell, energy));
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    CK(launch_pme_force_add(c));
     if (flags & PINYB200_DISTRIB_GHOSTS) CK(launch_ghost_distrib(c));
     CK(cudaEventRecord(c->ev[4], c->stream));
     std::vector<double> acc;
@@ -589,8 +614,8 @@ static int evaluate(pinyb200_ctx *c, const Cell &cell, int flags, pinyb200_energ
     CK(cudaStreamSynchronize(c->stream));
     CK(cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]));
     CK(cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]));
-    CK(cudaEventElapsedTime(&c->last_ms[2], c->ev[2], c->ev[3]));
-    CK(cudaEventElapsedTime(&c->last_ms[3], c->ev[3], c->ev[4]));
+    CK(cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]));
+    CK(cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]));
     if (e) {
         memset(e, 0, sizeof(*e));
         if (energy) {

@@ -78,6 +78,8 @@ struct pinyb200_ctx {
     int P = 1;
     int sm_count = 148;
     cudaStream_t stream = nullptr;
+    cudaStream_t pme_stream = nullptr;  // PME runs here, concurrently with the pair kernel
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_pme[2] = {nullptr, nullptr};
     pinyb200::DeviceSystem sys;
     // host copies needed for energy bookkeeping
     std::vector<double> h_charge;
@@ -116,6 +118,7 @@ struct pinyb200_ctx {
     void *d_grid = nullptr;       // [P][Nc][Nb][Na] real charge / potential grid
     void *d_spec = nullptr;       // [P][Nc][Nb][Na/2+1] complex half spectrum
     void *d_filter = nullptr;     // [G] real: preg * bweight, 0 outside the sphere
+    double *d_forceP = nullptr;   // [nchrg][3][P] PME forces, added to d_forceT after the join
     // charges binned by PME grid tile (PINYB200_PME_TILE points per edge)
     int pme_nt[3] = {0, 0, 0};    // tiles per axis
     int pme_ntile = 0, pme_cap = 0;
@@ -147,6 +150,7 @@ cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_p
                             const double *d_cutskin2, int pass);
 cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_pme(pinyb200_ctx *c, const Cell &cell, bool energy);
+cudaError_t launch_pme_force_add(pinyb200_ctx *c);
 cudaError_t launch_intra(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_ghost_pos(pinyb200_ctx *c);
 cudaError_t launch_ghost_distrib(pinyb200_ctx *c);

@@ -38,7 +38,7 @@ struct PmeArgs {
     const double *posT;
     int Na, Nb, Nc, n;
     void *grid;  // real [P][Nc][Nb][Na]
-    double *forceT;
+    double *forceP;  // PME forces [nchrg][3][P]
     int4 *rhead;  // per (charge, bead) records, see RecGeom
     void *rw;
 };
@@ -401,9 +401,11 @@ __device__ __forceinline__ void gather_lane(PHI phi, const LaneW<R, NI, true> &l
 }
 
 // Force of one record from its three sums (summed over the 8-lane group;
-// lane 0 writes): F = -q h^-T (N_a e_a, N_b e_b, N_c e_c).
-__device__ __forceinline__ void gather_store(const PmeArgs &a, const Cell &cell, int at, int b, double ea, double eb,
-                                             double ec, int l8)
+// lane 0 writes): F = -q h^-T (N_a e_a, N_b e_b, N_c e_c), stored (not
+// added) at the record's slot idx = k * P + b of the PME force buffer
+// [nchrg][3][P]; every record is written exactly once per evaluation.
+__device__ __forceinline__ void gather_store(const PmeArgs &a, const Cell &cell, int at, int idx, double ea,
+                                             double eb, double ec, int l8)
 {
 #pragma unroll
     for (int o = 4; o >= 1; o >>= 1) {
@@ -419,10 +421,23 @@ __device__ __forceinline__ void gather_store(const PmeArgs &a, const Cell &cell,
     const double gx = ea * cell.hi[0] + eb * cell.hi[1] + ec * cell.hi[2];
     const double gy = ea * cell.hi[3] + eb * cell.hi[4] + ec * cell.hi[5];
     const double gz = ea * cell.hi[6] + eb * cell.hi[7] + ec * cell.hi[8];
-    double *f = a.forceT;
-    f[(3 * (size_t)at + 0) * a.P + b] -= gx * q;
-    f[(3 * (size_t)at + 1) * a.P + b] -= gy * q;
-    f[(3 * (size_t)at + 2) * a.P + b] -= gz * q;
+    const int k = idx / a.P, b = idx - k * a.P;
+    double *f = a.forceP;
+    f[(3 * (size_t)k + 0) * a.P + b] = -gx * q;
+    f[(3 * (size_t)k + 1) * a.P + b] = -gy * q;
+    f[(3 * (size_t)k + 2) * a.P + b] = -gz * q;
+}
+
+// Adds the PME forces [nchrg][3][P] to the site forces [natm][3][P].
+__global__ void __launch_bounds__(256) pme_force_add_kernel(int nchrg, int P, const int *__restrict__ ichrg,
+                                                            const double *__restrict__ fP, double *__restrict__ fT)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nchrg * 3 * P) return;
+    const long long kd = t / P;
+    const int b = (int)(t - kd * P);
+    const int k = (int)(kd / 3), d = (int)(kd - 3LL * k);
+    fT[(3 * (size_t)ichrg[k] + d) * P + b] += fP[t];
 }
 
 // Gather: one block per (tile, bead); the tile's potential (with the
@@ -475,10 +490,10 @@ __global__ void __launch_bounds__(256) gather_tile_kernel(PmeArgs a, Cell cell, 
     for (int r = 0; r < nr; r++) {
         const int e = r * ngrp + grp;
         const bool act = e < n;
-        int at = 0;
+        int at = 0, idx = 0;
         double ea = 0, eb = 0, ec = 0;
         if (act) {
-            const int idx = list[e];
+            idx = list[e];
             const int4 h = a.rhead[idx];
             at = h.x;
             LaneW<R, NI, true> lw;
@@ -498,7 +513,7 @@ __global__ void __launch_bounds__(256) gather_tile_kernel(PmeArgs a, Cell cell, 
                     lw, l8, ea, eb, ec);
             }
         }
-        gather_store(a, cell, at, b, ea, eb, ec, act ? l8 : 1);
+        gather_store(a, cell, at, idx, ea, eb, ec, act ? l8 : 1);
     }
     const int nov = t.cnt[a.P * t.ntile];
     const int gid = blockIdx.y * gridDim.x + blockIdx.x, nblk = gridDim.x * gridDim.y;
@@ -506,10 +521,10 @@ __global__ void __launch_bounds__(256) gather_tile_kernel(PmeArgs a, Cell cell, 
     for (int r = 0; r < nr2; r++) {
         const int e = (r * nblk + gid) * ngrp + grp;
         const bool act = e < nov;
-        int at = 0, b2 = 0;
+        int at = 0, b2 = 0, idx = 0;
         double ea = 0, eb = 0, ec = 0;
         if (act) {
-            const int idx = t.ovf[e];
+            idx = t.ovf[e];
             const int4 h = a.rhead[idx];
             b2 = idx % a.P;
             at = h.x;
@@ -524,7 +539,7 @@ __global__ void __launch_bounds__(256) gather_tile_kernel(PmeArgs a, Cell cell, 
                 },
                 lw, l8, ea, eb, ec);
         }
-        gather_store(a, cell, at, b2, ea, eb, ec, act ? l8 : 1);
+        gather_store(a, cell, at, idx, ea, eb, ec, act ? l8 : 1);
     }
 }
 
@@ -949,7 +964,7 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     a.Nc = s.ngrid[2];
     a.n = s.n_interp;
     a.grid = c->d_grid;
-    a.forceT = c->d_forceT;
+    a.forceP = c->d_forceP;
     a.rhead = (int4 *)c->d_pme_head;
     a.rw = c->d_pme_w;
     const size_t G = (size_t)a.Na * a.Nb * a.Nc;
@@ -1012,6 +1027,15 @@ static cudaError_t launch_pme_r(pinyb200_ctx *c, const Cell &cell, bool energy)
     case 10: return launch_pme_t<R, 10>(c, cell, energy);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_pme_force_add(pinyb200_ctx *c)
+{
+    if (c->sys.nchrg == 0 || c->sys.nktot == 0) return cudaSuccess;
+    const long long n = (long long)c->sys.nchrg * 3 * c->P;
+    pme_force_add_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->sys.nchrg, c->P, c->sys.ichrg,
+                                                                            c->d_forceP, c->d_forceT);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_pme(pinyb200_ctx *c, const Cell &cell, bool energy)
