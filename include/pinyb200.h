@@ -43,7 +43,8 @@ enum {
 enum {
     PINYB200_DISTRIB_GHOSTS = 1, /* apply distrib_ghost_force (ghost_control.c:71) */
     PINYB200_NO_ENERGY = 2,      /* skip energy/virial reductions                   */
-    PINYB200_SITE_PAIRS = 4      /* walk the site list instead of molecule pairs    */
+    PINYB200_SITE_PAIRS = 4,     /* walk the site list instead of molecule pairs    */
+    PINYB200_TUNE_AGAIN = 8      /* pinyb200_autotune: ignore remembered results    */
 };
 
 /*
@@ -262,6 +263,58 @@ int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
                         const double *hmat, double *const *fx,
                         double *const *fy, double *const *fz,
                         double *pvten_tot, pinyb200_energies *e);
+
+/*
+ * Launch shapes and the autotuner.  A context runs with four choices:
+ *   choice[0]  PME tile edge, 8 or 16 grid points (charges are binned per
+ *              tile and bead; spread and gather run one block per tile)
+ *   choice[1]  pair kernel: 0 molecule pairs (when the system is made of
+ *              identical molecules of <= 4 sites), 1 the site list
+ *   choice[2]  pair kernel grid cap, blocks per SM (1..64)
+ *   choice[3]  1: PME on a second stream, concurrent with the pair kernel
+ * pinyb200_autotune times every combination on the caller's inputs
+ * (device positions as in pinyb200_energy_force_device; `reps` timed runs
+ * each after one warm-up), keeps the fastest, returns it in choice[4] and
+ * its device time in *best_ms, and remembers it for the rest of the process
+ * for every context of the same shape (atoms, beads, mesh, order,
+ * precision); later calls for that shape only apply it (*best_ms = -1)
+ * unless flags holds PINYB200_TUNE_AGAIN.  Results do not depend on the
+ * choice beyond floating-point summation order.  No counterpart in PINY,
+ * whose force path has no launch shapes.
+ */
+int pinyb200_autotune(pinyb200_ctx *ctx, const double *d_pos,
+                      const double *d_xmod, const double *hmat, int flags,
+                      int reps, int *choice, float *best_ms);
+int pinyb200_get_tuning(pinyb200_ctx *ctx, int *choice);
+int pinyb200_set_tuning(pinyb200_ctx *ctx, const int *choice);
+
+/*
+ * Many independent boxes per call (the batched path).  A batch groups
+ * contexts on one GPU (different sizes, bead counts and meshes are fine).
+ * pinyb200_batch_energy_force_device evaluates every box, as
+ * pinyb200_energy_force_device would one by one, from per-box device arrays
+ * (d_xmod may be NULL, or hold NULL entries) and host cells, and writes
+ * e[i] for box i (e may be NULL).  All boxes run as parallel branches of one
+ * CUDA graph launched once per call; the graph is captured on the first call
+ * and again whenever a device pointer, a cell or the flags change, after one
+ * plain run of every box.  The call returns when the work is done.  PINY's
+ * Python driver reaches several replicas through one energy_control call
+ * per CLASS (python/piny/piny.pyx:426-436); this entry point has no
+ * counterpart there.
+ */
+typedef struct pinyb200_batch pinyb200_batch;
+int pinyb200_batch_create(pinyb200_ctx *const *ctx, int nbox,
+                          pinyb200_batch **out);
+int pinyb200_batch_destroy(pinyb200_batch *batch);
+int pinyb200_batch_energy_force_device(pinyb200_batch *batch,
+                                       const double *const *d_pos,
+                                       const double *const *d_xmod,
+                                       const double *const *hmat, int flags,
+                                       double *const *d_force,
+                                       pinyb200_energies *e, void *stream);
+/* Device time of the last batch call (CUDA events around the graph launch). */
+int pinyb200_batch_last_ms(pinyb200_batch *batch, float *ms);
+const char *pinyb200_batch_last_error(pinyb200_batch *batch);
 
 /* Milliseconds of the last evaluation, from CUDA events: 0 device work,
  * 1 pair forces, 2 PME, 3 intramolecular, 4 the whole host-buffer call of

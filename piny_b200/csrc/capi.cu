@@ -169,6 +169,35 @@ static constexpr int kCountMaxDevices = 64;
 static std::mutex g_count_mu;
 static unsigned char *g_count_addr[kCountMaxDevices];
 
+Cell pinyb200::cell_from_hmat(const double *hmat) { return make_cell(hmat); }
+int pinyb200::record_error(pinyb200_ctx *c, int code, const std::string &msg) { return fail(c, code, msg); }
+static int pme_tiles_setup(pinyb200_ctx *c, int T);
+int pinyb200::pme_tiles_resize(pinyb200_ctx *c, int T)
+{
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaStreamSynchronize(c->pme_stream));
+    return pme_tiles_setup(c, T);
+}
+
+// Charge bins for the PME tiles of edge T: about twice the mean occupancy
+// per (tile, bead); the rest goes to the overflow list, which can hold every
+// charge.  Called at creation and by the autotuner.
+static int pme_tiles_setup(pinyb200_ctx *c, int T)
+{
+    const int N[3] = {c->sys.ngrid[0], c->sys.ngrid[1], c->sys.ngrid[2]};
+    for (int d = 0; d < 3; d++) c->pme_nt[d] = (N[d] + T - 1) / T;
+    c->pme_tile = T;
+    c->pme_ntile = c->pme_nt[0] * c->pme_nt[1] * c->pme_nt[2];
+    const int mean = (c->sys.nchrg + c->pme_ntile - 1) / c->pme_ntile;
+    c->pme_cap = (2 * mean + 32 + 31) / 32 * 32;
+    if (c->d_pme_cnt) cudaFree(c->d_pme_cnt);
+    if (c->d_pme_bin) cudaFree(c->d_pme_bin);
+    c->d_pme_cnt = c->d_pme_bin = nullptr;
+    CK(cudaMalloc(&c->d_pme_cnt, ((size_t)c->P * c->pme_ntile + 1) * sizeof(int)));
+    CK(cudaMalloc(&c->d_pme_bin, (size_t)c->P * c->pme_ntile * c->pme_cap * sizeof(int)));
+    return PINYB200_OK;
+}
+
 extern "C" {
 
 int pinyb200_version(void) { return 1; }
@@ -328,16 +357,12 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
         const size_t csz = f64 ? sizeof(double2) : sizeof(float2);
         CK(cudaMalloc(&c->d_grid, rsz * G * nbeads));
         CK(cudaMalloc(&c->d_spec, csz * (size_t)Nc * Nb * (Na / 2 + 1) * nbeads));
-        // charge bins per grid tile and bead; about twice the mean occupancy,
-        // the rest goes to the overflow list (which can hold every charge)
-        c->pme_nt[0] = (Na + PINYB200_PME_TILE - 1) / PINYB200_PME_TILE;
-        c->pme_nt[1] = (Nb + PINYB200_PME_TILE - 1) / PINYB200_PME_TILE;
-        c->pme_nt[2] = (Nc + PINYB200_PME_TILE - 1) / PINYB200_PME_TILE;
-        c->pme_ntile = c->pme_nt[0] * c->pme_nt[1] * c->pme_nt[2];
-        const int mean = (d.nchrg + c->pme_ntile - 1) / c->pme_ntile;
-        c->pme_cap = (2 * mean + 32 + 31) / 32 * 32;
-        CK(cudaMalloc(&c->d_pme_cnt, ((size_t)nbeads * c->pme_ntile + 1) * sizeof(int)));
-        CK(cudaMalloc(&c->d_pme_bin, (size_t)nbeads * c->pme_ntile * c->pme_cap * sizeof(int)));
+        // charge bins per grid tile and bead: 16^3 tiles, or 8^3 on small
+        // meshes so that spread and gather still get enough blocks
+        {
+            const int rc2 = pme_tiles_setup(c, std::min(Na, std::min(Nb, Nc)) >= 32 ? 16 : 8);
+            if (rc2) return rc2;
+        }
         CK(cudaMalloc(&c->d_pme_ovf, (size_t)std::max(1, d.nchrg) * nbeads * sizeof(int)));
         // per (charge, bead) records: stencil origin and the six weight rows
         const int nip = s->n_interp <= 4 ? 4 : (s->n_interp <= 8 ? 8 : 12);
@@ -571,15 +596,22 @@ int pinyb200_get_list(pinyb200_ctx *c, int *pi, int *pj, long cap, long *npairs)
 }
 
 // Device evaluation on inputs already in d_posT (and d_xmod for PIMD).
-static int evaluate(pinyb200_ctx *c, const Cell &cell, int flags, pinyb200_energies *e)
+}  // extern "C"
+
+// Everything one evaluation does on the device, enqueued on c->stream (PME
+// forks to the context's PME stream and joins back); no host
+// synchronisation, so it can be captured in a CUDA graph.  timing: record
+// the phase events (not inside a graph); h_acc: where the per-bead energy
+// sums [P][S_NSLOT] are copied (NULL: not copied).
+int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, bool timing, double *h_acc)
 {
     const bool energy = !(flags & PINYB200_NO_ENERGY);
     const size_t nb = (size_t)c->sys.natm * 3 * c->P;
-    CK(cudaEventRecord(c->ev[0], c->stream));
+    if (timing) CK(cudaEventRecord(c->ev[0], c->stream));
     CK(launch_ghost_pos(c));
     CK(cudaMemsetAsync(c->d_forceT, 0, nb * sizeof(double), c->stream));
     CK(cudaMemsetAsync(c->d_acc, 0, (size_t)c->P * S_NSLOT * sizeof(double), c->stream));
-    CK(cudaEventRecord(c->ev[1], c->stream));
+    if (timing) CK(cudaEventRecord(c->ev[1], c->stream));
     // PME on its own stream, concurrently with the pair and intramolecular
     // kernels: it reads the positions, writes its own force buffer and adds
     // its energies and virial atomically
@@ -587,35 +619,38 @@ static int evaluate(pinyb200_ctx *c, const Cell &cell, int flags, pinyb200_energ
     CK(cudaStreamWaitEvent(c->pme_stream, c->ev_fork, 0));
     {
         cudaStream_t main_stream = c->stream;
-        c->stream = c->pme_stream;
-        cudaError_t perr = cudaEventRecord(c->ev_pme[0], c->stream);
+        if (c->pme_overlap) c->stream = c->pme_stream;
+        cudaError_t perr = timing ? cudaEventRecord(c->ev_pme[0], c->stream) : cudaSuccess;
         if (perr == cudaSuccess) perr = launch_pme(c, cell, energy);
-        if (perr == cudaSuccess) perr = cudaEventRecord(c->ev_pme[1], c->stream);
+        if (perr == cudaSuccess && timing) perr = cudaEventRecord(c->ev_pme[1], c->stream);
         if (perr == cudaSuccess) perr = cudaEventRecord(c->ev_join, c->stream);
         c->stream = main_stream;
         CK(perr);
     }
     const bool ortho = cell.h[1] == 0.0 && cell.h[2] == 0.0 && cell.h[3] == 0.0 && cell.h[5] == 0.0 &&
                        cell.h[6] == 0.0 && cell.h[7] == 0.0;
-    if (c->use_mol && c->mol_ok && ortho && !(flags & PINYB200_SITE_PAIRS)) CK(launch_mol_pair(c, cell, energy));
+    if (c->use_mol && c->mol_ok && ortho && c->pair_variant == 0 && !(flags & PINYB200_SITE_PAIRS))
+        CK(launch_mol_pair(c, cell, energy));
     else CK(launch_pair(c, cell, energy));
-    CK(cudaEventRecord(c->ev[2], c->stream));
+    if (timing) CK(cudaEventRecord(c->ev[2], c->stream));
     CK(launch_intra(c, cell, energy));
-    CK(cudaEventRecord(c->ev[3], c->stream));
+    if (timing) CK(cudaEventRecord(c->ev[3], c->stream));
     CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     CK(launch_pme_force_add(c));
     if (flags & PINYB200_DISTRIB_GHOSTS) CK(launch_ghost_distrib(c));
-    CK(cudaEventRecord(c->ev[4], c->stream));
-    std::vector<double> acc;
-    if (energy) {
-        acc.resize((size_t)c->P * S_NSLOT);
-        CK(cudaMemcpyAsync(acc.data(), c->d_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    }
-    CK(cudaStreamSynchronize(c->stream));
-    CK(cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]));
-    CK(cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]));
-    CK(cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]));
-    CK(cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]));
+    if (timing) CK(cudaEventRecord(c->ev[4], c->stream));
+    if (energy && h_acc)
+        CK(cudaMemcpyAsync(h_acc, c->d_acc, (size_t)c->P * S_NSLOT * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+    return PINYB200_OK;
+}
+
+// Host bookkeeping of one evaluation from the per-bead sums acc[P][S_NSLOT]
+// (energy_control_inter_real.c:141-183, energy_control_inter_recip.c:
+// 341-349, energy_control_intra.c:284-309).
+void pinyb200::evaluate_finish(pinyb200_ctx *c, const Cell &cell, int flags, const double *acc, pinyb200_energies *e)
+{
+    const bool energy = !(flags & PINYB200_NO_ENERGY);
     if (e) {
         memset(e, 0, sizeof(*e));
         if (energy) {
@@ -650,6 +685,20 @@ static int evaluate(pinyb200_ctx *c, const Cell &cell, int flags, pinyb200_energ
             e->pvten[5] = e->pvten[7] = s[S_PYZ];
         }
     }
+}
+
+static int evaluate(pinyb200_ctx *c, const Cell &cell, int flags, pinyb200_energies *e)
+{
+    const bool energy = !(flags & PINYB200_NO_ENERGY);
+    std::vector<double> acc(energy ? (size_t)c->P * S_NSLOT : 0);
+    int rc = evaluate_enqueue(c, cell, flags, true, energy ? acc.data() : nullptr);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]));
+    CK(cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]));
+    CK(cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]));
+    CK(cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]));
+    evaluate_finish(c, cell, flags, energy ? acc.data() : nullptr, e);
     return PINYB200_OK;
 }
 
@@ -662,6 +711,30 @@ __global__ void centroid_kernel(const double *__restrict__ posT, double *__restr
     for (int b = 0; b < P; b++) s += posT[t * P + b];
     xm[t] = s / (double)P;
 }
+
+// One evaluation from device-resident positions to device-resident forces,
+// enqueued on c->stream without host synchronisation (see evaluate_enqueue).
+int pinyb200::enqueue_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const Cell &cell, int flags,
+                             double *d_force, bool timing, double *h_acc)
+{
+    CK(launch_transpose_in(c, d_pos));
+    if (c->P > 1) {
+        if (d_xmod) {
+            CK(cudaMemcpyAsync(c->d_xmod, d_xmod, (size_t)c->sys.natm * 3 * sizeof(double), cudaMemcpyDeviceToDevice,
+                               c->stream));
+        } else {
+            const long long n = (long long)c->sys.natm * 3;
+            centroid_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->d_posT, c->d_xmod, c->sys.natm, c->P);
+            CK(cudaGetLastError());
+        }
+    }
+    int rc = evaluate_enqueue(c, cell, flags, timing, h_acc);
+    if (rc) return rc;
+    CK(launch_transpose_out(c, d_force));
+    return PINYB200_OK;
+}
+
+extern "C" {
 
 int pinyb200_energy_force_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const double *hmat,
                                  int flags, double *d_force, pinyb200_energies *e, void *stream)
@@ -678,21 +751,16 @@ int pinyb200_energy_force_device(pinyb200_ctx *c, const double *d_pos, const dou
         ~Restore() { c->stream = s; }
     } restore{c, own};
     Cell cell = make_cell(hmat);
-    CK(launch_transpose_in(c, d_pos));
-    if (c->P > 1) {
-        if (d_xmod) {
-            CK(cudaMemcpyAsync(c->d_xmod, d_xmod, (size_t)c->sys.natm * 3 * sizeof(double), cudaMemcpyDeviceToDevice,
-                               c->stream));
-        } else {
-            const long long n = (long long)c->sys.natm * 3;
-            centroid_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->d_posT, c->d_xmod, c->sys.natm, c->P);
-            CK(cudaGetLastError());
-        }
-    }
-    int rc = evaluate(c, cell, flags, e);
+    const bool energy = !(flags & PINYB200_NO_ENERGY);
+    std::vector<double> acc(energy ? (size_t)c->P * S_NSLOT : 0);
+    int rc = enqueue_device(c, d_pos, d_xmod, cell, flags, d_force, true, energy ? acc.data() : nullptr);
     if (rc) return rc;
-    CK(launch_transpose_out(c, d_force));
     CK(cudaStreamSynchronize(c->stream));
+    CK(cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]));
+    CK(cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]));
+    CK(cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]));
+    CK(cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]));
+    evaluate_finish(c, cell, flags, energy ? acc.data() : nullptr, e);
     return PINYB200_OK;
 }
 

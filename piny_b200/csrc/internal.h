@@ -4,7 +4,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/pinyb200.h"
@@ -79,6 +82,9 @@ struct pinyb200_ctx {
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     cudaStream_t pme_stream = nullptr;  // PME runs here, concurrently with the pair kernel
+    bool pme_overlap = true;            // false: PME on the main stream after the pair kernel
+    int pair_variant = 0;               // 0 molecule-pair kernel (when available), 1 site-list kernel
+    int pair_blocks_per_sm = 16;        // grid cap of the pair kernels, blocks per SM
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_pme[2] = {nullptr, nullptr};
     pinyb200::DeviceSystem sys;
     // host copies needed for energy bookkeeping
@@ -119,7 +125,8 @@ struct pinyb200_ctx {
     void *d_spec = nullptr;       // [P][Nc][Nb][Na/2+1] complex half spectrum
     void *d_filter = nullptr;     // [G] real: preg * bweight, 0 outside the sphere
     double *d_forceP = nullptr;   // [nchrg][3][P] PME forces, added to d_forceT after the join
-    // charges binned by PME grid tile (PINYB200_PME_TILE points per edge)
+    // charges binned by PME grid tile (pme_tile = 8 or 16 points per edge)
+    int pme_tile = 16;
     int pme_nt[3] = {0, 0, 0};    // tiles per axis
     int pme_ntile = 0, pme_cap = 0;
     int *d_pme_cnt = nullptr;     // [P][ntile] entries per bin, then [1] overflow count
@@ -139,9 +146,6 @@ struct pinyb200_ctx {
 
 namespace pinyb200 {
 
-// Edge of the PME grid tiles (grid points) that charges are binned by.
-#define PINYB200_PME_TILE 16
-
 // launchers (defined in the .cu files)
 cudaError_t launch_build_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1,
                               const double *d_xm, const double *d_cutskin2, int pass);
@@ -151,6 +155,34 @@ cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_p
 cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_pme(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_pme_force_add(pinyb200_ctx *c);
+
+// evaluation steps (capi.cu): device work of one evaluation enqueued on
+// c->stream without host synchronisation, and the host bookkeeping of its
+// per-bead sums; cell of an hmat; error recording
+int evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, bool timing, double *h_acc);
+void evaluate_finish(pinyb200_ctx *c, const Cell &cell, int flags, const double *acc, pinyb200_energies *e);
+int enqueue_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const Cell &cell, int flags,
+                   double *d_force, bool timing, double *h_acc);
+Cell cell_from_hmat(const double *hmat);
+int pme_tiles_resize(pinyb200_ctx *c, int T);
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per kernel, device
+// and size, so that repeated launches (and graph captures) do not repeat it.
+inline cudaError_t smem_optin(const void *func, int bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    int &have = done[std::make_pair(func, dev)];
+    if (have >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) have = bytes;
+    return e;
+}
+int record_error(pinyb200_ctx *c, int code, const std::string &msg);
 cudaError_t launch_intra(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_ghost_pos(pinyb200_ctx *c);
 cudaError_t launch_ghost_distrib(pinyb200_ctx *c);

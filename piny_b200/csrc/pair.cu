@@ -164,7 +164,7 @@ static void launch_pair_t(pinyb200_ctx *c, const PairArgs &a, const Cell &cell)
     const int threads = 256;
     long long rows = c->sys.natm;
     long long blocks = (rows * 32 + threads - 1) / threads;
-    long long maxb = (long long)c->sm_count * 8;
+    long long maxb = (long long)c->sm_count * c->pair_blocks_per_sm;
     if (blocks > maxb) blocks = maxb;
     pair_kernel<R, P><<<(int)blocks, threads, 0, c->stream>>>(a, cell);
 }

@@ -477,7 +477,7 @@ static void launch_mol_t(pinyb200_ctx *c, const MolArgs &a, const Cell &cell, bo
 {
     const int threads = 128;
     long long blocks = ((long long)a.nchunk * 32 + threads - 1) / threads;
-    const long long maxb = (long long)c->sm_count * 16;
+    const long long maxb = (long long)c->sm_count * c->pair_blocks_per_sm;
     if (blocks > maxb) blocks = maxb;
     if (blocks < 1) blocks = 1;
     dim3 grid((unsigned)blocks, P > 32 ? P / 32 : 1);

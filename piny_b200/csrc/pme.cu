@@ -112,6 +112,7 @@ __device__ __forceinline__ void stencil_origin(const PmeArgs &a, const Cell &cel
 
 // Charges binned by the grid tile that holds their stencil origin, per bead.
 struct TileArgs {
+    int T;  // tile edge (grid points)
     int nta, ntb, ntc, ntile, cap;
     int *cnt;  // [P][ntile], then the overflow count
     int *bin;  // [P][ntile][cap] record numbers k*P + b
@@ -132,11 +133,13 @@ struct RecGeom {
 // Tile geometry: T^3 grid points own the charges whose stencil starts in
 // them; the shared copy spans E = T + NI - 1 points per edge (the stencils
 // reach NI - 1 beyond), rows padded to PA.
-template <int NI>
+// With PA = 24 (E <= 24) the 4 b rows x 8 a points of a warp fall in 32
+// distinct banks (row offsets 0, 24, 48, 72 = 0, 24, 16, 8 mod 32).
+template <int NI, int TT>
 struct TileGeom {
-    static constexpr int T = PINYB200_PME_TILE;
+    static constexpr int T = TT;
     static constexpr int E = T + NI - 1;
-    static constexpr int PA = (E + 3) & ~3;
+    static constexpr int PA = E <= 24 ? 24 : ((E + 3) & ~3);
     static constexpr int NPT = E * E * PA;
 };
 
@@ -208,7 +211,7 @@ __global__ void __launch_bounds__(256) pme_bin_kernel(PmeArgs a, Cell cell, Tile
         store4(out + (3 + ax) * RG::NIP, w, RG::NIP);
     }
     a.rhead[idx] = make_int4(at, la, lb, lc);
-    const int T = PINYB200_PME_TILE;
+    const int T = t.T;
     const int tile = ((lc / T) * t.ntb + lb / T) * t.nta + la / T;
     const int slot = atomicAdd(&t.cnt[b * t.ntile + tile], 1);
     if (slot < t.cap) t.bin[((size_t)b * t.ntile + tile) * t.cap + slot] = (int)idx;
@@ -267,16 +270,16 @@ __device__ __forceinline__ void spread_global(const PmeArgs &a, R *g, int la, in
 // 16-byte vector atomics where the rows allow.  Records whose origin lies
 // outside the tile (none are expected) and overflow records go straight to
 // the grid.
-template <typename R, int NI>
+template <typename R, int NI, int TT>
 size_t spread_smem()
 {
-    return (size_t)TileGeom<NI>::NPT * sizeof(R);
+    return (size_t)TileGeom<NI, TT>::NPT * sizeof(R);
 }
 
-template <typename R, int NI>
+template <typename R, int NI, int TT>
 __global__ void __launch_bounds__(256) spread_tile_kernel(PmeArgs a, TileArgs t)
 {
-    typedef TileGeom<NI> TG;
+    typedef TileGeom<NI, TT> TG;
     typedef RecGeom<NI> RG;
     constexpr int NIP = RG::NIP;
     constexpr int NTB = (NI + 3) / 4;  // b rows per lane
@@ -445,10 +448,10 @@ __global__ void __launch_bounds__(256) pme_force_add_kernel(int nchrg, int P, co
 // it there.  Overflow records read the grid directly.  Every (charge, bead)
 // is handled by exactly one 8-lane group, so the force update needs no
 // atomics.
-template <typename R, int NI>
+template <typename R, int NI, int TT>
 __global__ void __launch_bounds__(256) gather_tile_kernel(PmeArgs a, Cell cell, TileArgs t)
 {
-    typedef TileGeom<NI> TG;
+    typedef TileGeom<NI, TT> TG;
     extern __shared__ unsigned char smem_raw[];
     R *tl = (R *)smem_raw;
     const int tile = blockIdx.x, b = blockIdx.y;
@@ -930,13 +933,13 @@ static cudaError_t launch_fft_t(pinyb200_ctx *c, const PmeArgs &a, const Cell &c
     cudaError_t err = cudaSuccess;
     // opt in to more than 48 KB of dynamic shared memory where a plane needs it
     if (sp > 48 * 1024) {
-        err = cudaFuncSetAttribute(plane_fwd_kernel<R, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp);
+        err = smem_optin((const void *)plane_fwd_kernel<R, NF>, (int)sp);
         if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(plane_inv_kernel<R, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp);
+            err = smem_optin((const void *)plane_inv_kernel<R, NF>, (int)sp);
         if (err != cudaSuccess) return err;
     }
     if (ss > 48 * 1024) {
-        err = cudaFuncSetAttribute(conv_c_kernel<R, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss);
+        err = smem_optin((const void *)conv_c_kernel<R, NF>, (int)ss);
         if (err != cudaSuccess) return err;
     }
     plane_fwd_kernel<R, NF><<<a.P * a.Nc, 256, sp, c->stream>>>((const R *)a.grid, spec, a.Na, a.Nb, a.Nc, tw[0],
@@ -947,7 +950,7 @@ static cudaError_t launch_fft_t(pinyb200_ctx *c, const PmeArgs &a, const Cell &c
     return cudaGetLastError();
 }
 
-template <typename R, int NI>
+template <typename R, int NI, int TT>
 static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
 {
     typedef typename Cplx<R>::T C2;
@@ -972,6 +975,7 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     cudaError_t err = cudaMemsetAsync(c->d_grid, 0, sizeof(R) * G * c->P, c->stream);
     if (err != cudaSuccess) return err;
     TileArgs t;
+    t.T = TT;
     t.nta = c->pme_nt[0];
     t.ntb = c->pme_nt[1];
     t.ntc = c->pme_nt[2];
@@ -985,18 +989,17 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     const long long nt = (long long)a.nchrg * a.P;
     const int threads = 256;
     pme_bin_kernel<R, NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell, t);
-    const size_t st = (size_t)TileGeom<NI>::NPT * sizeof(R), ss_spread = spread_smem<R, NI>();
+    const size_t st = (size_t)TileGeom<NI, TT>::NPT * sizeof(R), ss_spread = spread_smem<R, NI, TT>();
     if (ss_spread > 48 * 1024) {
-        err = cudaFuncSetAttribute(spread_tile_kernel<R, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)ss_spread);
+        err = smem_optin((const void *)spread_tile_kernel<R, NI, TT>, (int)ss_spread);
         if (err != cudaSuccess) return err;
     }
     if (st > 48 * 1024) {
-        err = cudaFuncSetAttribute(gather_tile_kernel<R, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st);
+        err = smem_optin((const void *)gather_tile_kernel<R, NI, TT>, (int)st);
         if (err != cudaSuccess) return err;
     }
     const dim3 tgrid((unsigned)t.ntile, (unsigned)a.P);
-    spread_tile_kernel<R, NI><<<tgrid, 256, ss_spread, c->stream>>>(a, t);
+    spread_tile_kernel<R, NI, TT><<<tgrid, 256, ss_spread, c->stream>>>(a, t);
     const R *twbase = (const R *)(f64 ? (const void *)c->d_twiddle64 : (const void *)c->d_twiddle32);
     const R *tw[3] = {twbase, twbase + 2 * 256, twbase + 4 * 256};
     const size_t sp = pme_plane_smem(a.Na, a.Nb, f64), ss = pme_slab_smem(a.Na, a.Nc, f64);
@@ -1011,22 +1014,28 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     default: err = launch_fft_t<R, 0>(c, a, cell, spec, filt, tw, sp, ss, energy); break;
     }
     if (err != cudaSuccess) return err;
-    gather_tile_kernel<R, NI><<<tgrid, 256, st, c->stream>>>(a, cell, t);
+    gather_tile_kernel<R, NI, TT><<<tgrid, 256, st, c->stream>>>(a, cell, t);
     return cudaGetLastError();
+}
+
+template <typename R, int TT>
+static cudaError_t launch_pme_rt(pinyb200_ctx *c, const Cell &cell, bool energy)
+{
+    switch (c->sys.n_interp) {
+    case 4: return launch_pme_t<R, 4, TT>(c, cell, energy);
+    case 5: return launch_pme_t<R, 5, TT>(c, cell, energy);
+    case 6: return launch_pme_t<R, 6, TT>(c, cell, energy);
+    case 7: return launch_pme_t<R, 7, TT>(c, cell, energy);
+    case 8: return launch_pme_t<R, 8, TT>(c, cell, energy);
+    case 10: return launch_pme_t<R, 10, TT>(c, cell, energy);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 template <typename R>
 static cudaError_t launch_pme_r(pinyb200_ctx *c, const Cell &cell, bool energy)
 {
-    switch (c->sys.n_interp) {
-    case 4: return launch_pme_t<R, 4>(c, cell, energy);
-    case 5: return launch_pme_t<R, 5>(c, cell, energy);
-    case 6: return launch_pme_t<R, 6>(c, cell, energy);
-    case 7: return launch_pme_t<R, 7>(c, cell, energy);
-    case 8: return launch_pme_t<R, 8>(c, cell, energy);
-    case 10: return launch_pme_t<R, 10>(c, cell, energy);
-    default: return cudaErrorInvalidValue;
-    }
+    return c->pme_tile == 8 ? launch_pme_rt<R, 8>(c, cell, energy) : launch_pme_rt<R, 16>(c, cell, energy);
 }
 
 cudaError_t launch_pme_force_add(pinyb200_ctx *c)

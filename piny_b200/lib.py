@@ -23,6 +23,7 @@ PINYB200_MIXED = 1
 DISTRIB_GHOSTS = 1
 NO_ENERGY = 2
 SITE_PAIRS = 4
+TUNE_AGAIN = 8
 
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NO_DEVICE", 4: "ERR_LIST_OVERFLOW", 5: "ERR_CUTOFF",
           6: "ERR_TIMEOUT", 7: "ERR_NAN", 8: "ERR_UNSUPPORTED", 9: "ERR_STATE"}
@@ -62,7 +63,10 @@ class PinyEnergies(C.Structure):
 EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb200_destroy",
            "pinyb200_build_list", "pinyb200_get_list", "pinyb200_list_info", "pinyb200_energy_force",
            "pinyb200_energy_force_device", "pinyb200_piny_force", "pinyb200_last_timing",
-           "pinyb200_last_error", "pinyb200_count_list_device", "pinyb200_check_list_device")
+           "pinyb200_last_error", "pinyb200_count_list_device", "pinyb200_check_list_device",
+           "pinyb200_autotune", "pinyb200_get_tuning", "pinyb200_set_tuning", "pinyb200_batch_create",
+           "pinyb200_batch_destroy", "pinyb200_batch_energy_force_device", "pinyb200_batch_last_ms",
+           "pinyb200_batch_last_error")
 
 COUNT_MAX_ATOMS = 65536       # PINYB200_COUNT_MAX_ATOMS
 COUNT_MAX_PAIR_TYPES = 64     # PINYB200_COUNT_MAX_PAIR_TYPES
@@ -101,6 +105,17 @@ def load(build_if_missing: bool = True):
     L.pinyb200_count_list_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, _pd, C.POINTER(C.c_long),
                                              C.POINTER(C.c_long), C.c_void_p]
     L.pinyb200_check_list_device.argtypes = [C.c_void_p, C.c_void_p, _d, _pi, _pd, _pd, _pd, C.c_void_p]
+    L.pinyb200_autotune.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, _i, _i, _pi, C.POINTER(C.c_float)]
+    L.pinyb200_get_tuning.argtypes = [C.c_void_p, _pi]
+    L.pinyb200_set_tuning.argtypes = [C.c_void_p, _pi]
+    L.pinyb200_batch_create.argtypes = [C.POINTER(C.c_void_p), _i, C.POINTER(C.c_void_p)]
+    L.pinyb200_batch_destroy.argtypes = [C.c_void_p]
+    L.pinyb200_batch_energy_force_device.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                                     C.POINTER(_pd), _i, C.POINTER(C.c_void_p),
+                                                     C.POINTER(PinyEnergies), C.c_void_p]
+    L.pinyb200_batch_last_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
+    L.pinyb200_batch_last_error.restype = C.c_char_p
+    L.pinyb200_batch_last_error.argtypes = [C.c_void_p]
     L.pinyb200_last_error.restype = C.c_char_p
     L.pinyb200_last_error.argtypes = [C.c_void_p]
     _LIB = L
@@ -243,7 +258,75 @@ class DeviceBox:
                     "energy_force_device")
         return energies_dict(e)
 
+    def autotune(self, d_pos: int, d_xmod, hmat, reps=3, again=False, energy=True):
+        """Time every launch shape on these inputs and keep the fastest:
+        returns (choice [tile, pair kernel, blocks/SM, overlap], best ms or -1
+        when a remembered result was applied)."""
+        hmat = np.ascontiguousarray(hmat, np.float64)
+        ch = (C.c_int * 4)()
+        ms = C.c_float()
+        flags = (TUNE_AGAIN if again else 0) | (0 if energy else NO_ENERGY)
+        self._check(self.L.pinyb200_autotune(self.h, C.c_void_p(d_pos), None if d_xmod is None else C.c_void_p(d_xmod),
+                                             _dp(hmat), flags, int(reps), ch, C.byref(ms)), "autotune")
+        return list(ch), ms.value
+
+    def tuning(self):
+        ch = (C.c_int * 4)()
+        self._check(self.L.pinyb200_get_tuning(self.h, ch), "get_tuning")
+        return list(ch)
+
+    def set_tuning(self, choice):
+        ch = (C.c_int * 4)(*[int(v) for v in choice])
+        self._check(self.L.pinyb200_set_tuning(self.h, ch), "set_tuning")
+
     def last_timing(self):
         ms = (C.c_float * 5)()
         self._check(self.L.pinyb200_last_timing(self.h, ms, 5), "last_timing")
         return list(ms)
+
+
+class DeviceBatch:
+    """Several DeviceBox contexts evaluated together as one CUDA graph launch
+    (pinyb200_batch_*)."""
+
+    def __init__(self, boxes):
+        self.L = load()
+        self.boxes = list(boxes)
+        arr = (C.c_void_p * len(self.boxes))(*[b.h.value for b in self.boxes])
+        h = C.c_void_p()
+        rc = self.L.pinyb200_batch_create(arr, len(self.boxes), C.byref(h))
+        if rc != 0:
+            raise PinyError("pinyb200_batch_create: %s %s" % (STATUS.get(rc, rc),
+                                                              self.L.pinyb200_last_error(None).decode()))
+        self.h = h
+
+    def energy_force_device(self, d_pos, d_xmod, hmats, d_force, stream=None, energy=True):
+        n = len(self.boxes)
+        P = (C.c_void_p * n)(*[int(p) for p in d_pos])
+        X = (C.c_void_p * n)(*[None if x is None else int(x) for x in d_xmod]) if d_xmod is not None else None
+        F = (C.c_void_p * n)(*[int(p) for p in d_force])
+        hm = [np.ascontiguousarray(h, np.float64) for h in hmats]
+        H = (_pd * n)(*[_dp(h) for h in hm])
+        E = (PinyEnergies * n)()
+        rc = self.L.pinyb200_batch_energy_force_device(self.h, P, X, H, 0 if energy else NO_ENERGY, F, E,
+                                                       None if stream is None else C.c_void_p(stream))
+        if rc != 0:
+            raise PinyError("batch_energy_force_device: %s %s" % (STATUS.get(rc, rc),
+                                                                  self.L.pinyb200_batch_last_error(self.h).decode()))
+        return [energies_dict(e) for e in E]
+
+    def last_ms(self):
+        ms = C.c_float()
+        self.L.pinyb200_batch_last_ms(self.h, C.byref(ms))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pinyb200_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -341,6 +341,24 @@ def density_box_edge(nmol, density_per_A3=0.03342):
     return (nmol / density_per_A3) ** (1.0 / 3.0)
 
 
+def c4_specs(nbox: int = 64, seed: int = 2024, nmin: int = 64, nmax: int = 2048):
+    """The batched configuration: `nbox` independent q-TIP4P/F boxes with
+    molecule counts drawn log-uniformly from [nmin, nmax] and bead counts from
+    {1, 4, 8, 16, 32, 64} (seeded), each at 0.997 g/cm^3 (L = (n/0.03342)^(1/3)
+    Angstrom) with a PME mesh of the next power of two >= 1 point per
+    Angstrom, order 8, and the shared cutoff / skin / alpha.  Box i uses seed
+    seed + i for its geometry."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(nbox):
+        n = int(round(float(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))))
+        P = int(rng.choice([1, 4, 8, 16, 32, 64]))
+        L = density_box_edge(n)
+        grid = 1 << int(np.ceil(np.log2(L)))
+        out.append(BoxSpec(TIP4P_F, n, L, P, 298.0, seed + i, grid=grid, order=8))
+    return out
+
+
 def named_spec(name: str) -> BoxSpec:
     if name == "spcfw_256_p1":
         return BoxSpec(SPC_FW, 256, 19.73, 1, 300.0, 12345, grid=32, order=6)

@@ -1,0 +1,128 @@
+"""Batched boxes (one CUDA graph per call) and launch shapes: every path
+gives the forces and energies of the one-box path.
+
+Tolerances: FP64 force relative RMS 1e-12 (the kernels are the same; only
+atomic summation order differs), MIXED 1e-5 against the FP64 one-box result.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_rms
+
+pytestmark = pytest.mark.gpu
+
+
+def _boxes(nbox=4, seed=77):
+    from piny_b200 import system, water
+    specs = water.c4_specs(nbox=nbox, seed=seed, nmin=64, nmax=300)
+    out = []
+    for sp in specs:
+        pos = water.build_positions(sp) / water.BOHR
+        S = system.build_system(sp, pos)
+        out.append((sp, pos, S))
+    return out
+
+
+def _single(S, pos, P, prec, choice=None):
+    import torch
+
+    from piny_b200.lib import DeviceBox
+    box = DeviceBox(S, P, prec)
+    xmod = pos.mean(axis=0) if P > 1 else None
+    box.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+    if choice is not None:
+        box.set_tuning(choice)
+    d = torch.from_numpy(pos).to("cuda:0")
+    dx = torch.from_numpy(xmod).to("cuda:0") if xmod is not None else None
+    f = torch.empty_like(d)
+    e = box.energy_force_device(d.data_ptr(), None if dx is None else dx.data_ptr(), S["hmat"], f.data_ptr())
+    return box, f.cpu().numpy(), e
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_batch_matches_single_boxes(prec):
+    import torch
+
+    from piny_b200.lib import DeviceBatch, DeviceBox
+    boxes = _boxes()
+    ref = [_single(S, pos, sp.nbeads, "fp64") for sp, pos, S in boxes]
+    ctxs, d_pos, d_xm, d_f, hm = [], [], [], [], []
+    keep = []
+    for sp, pos, S in boxes:
+        b = DeviceBox(S, sp.nbeads, prec)
+        xmod = pos.mean(axis=0) if sp.nbeads > 1 else None
+        b.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+        d = torch.from_numpy(pos).to("cuda:0")
+        dx = torch.from_numpy(xmod).to("cuda:0") if xmod is not None else None
+        f = torch.zeros_like(d)
+        keep += [d, dx, f]
+        ctxs.append(b)
+        d_pos.append(d.data_ptr())
+        d_xm.append(None if dx is None else dx.data_ptr())
+        d_f.append(f.data_ptr())
+        hm.append(S["hmat"])
+    torch.cuda.synchronize()
+    batch = DeviceBatch(ctxs)
+    tol = 1e-12 if prec == "fp64" else 1e-5
+    etol = 1e-11 if prec == "fp64" else 1e-6
+    for call in range(2):  # capture, then replay of the graph
+        es = batch.energy_force_device(d_pos, d_xm, hm, d_f)
+        torch.cuda.synchronize()
+        for i, (sp, pos, S) in enumerate(boxes):
+            f = keep[3 * i + 2].cpu().numpy()
+            assert rel_rms(f, ref[i][1]) < tol, (call, i)
+            e0 = ref[i][2]
+            scale = abs(e0["vvdw"]) + abs(e0["vcoul"]) + abs(e0["vrecip"]) + abs(e0["vself"])
+            assert abs(es[i]["vintert"] - e0["vintert"]) <= etol * scale
+            assert abs(es[i]["vintrat"] - e0["vintrat"]) <= etol * max(1.0, abs(e0["vintrat"]))
+    assert batch.last_ms() > 0
+    # a changed cell is a new graph; an unchanged call replays
+    hm2 = [h * 1.001 for h in hm]
+    es2 = batch.energy_force_device(d_pos, d_xm, hm2, d_f)
+    assert all(np.isfinite(e["vintert"]) for e in es2)
+    batch.close()
+    for b in ctxs:
+        b.close()
+    for r in ref:
+        r[0].close()
+
+
+def test_every_launch_shape_gives_the_same_forces():
+    boxes = _boxes(nbox=2, seed=5)
+    for sp, pos, S in boxes:
+        b0, f0, e0 = _single(S, pos, sp.nbeads, "fp64")
+        b0.close()
+        for choice in ([8, 0, 4, 0], [16, 1, 32, 1], [8, 1, 8, 1], [16, 0, 16, 0]):
+            if choice[0] == 16 and min(S["ngrid_a"], S["ngrid_b"], S["ngrid_c"]) < 16:
+                continue
+            b, f, e = _single(S, pos, sp.nbeads, "fp64", choice)
+            assert b.tuning() == choice
+            assert rel_rms(f, f0) < 1e-12, choice
+            assert abs(e["vintert"] - e0["vintert"]) <= 1e-11 * max(1.0, abs(e0["vintert"]))
+            b.close()
+
+
+def test_autotune_picks_a_valid_shape_and_remembers_it():
+    import torch
+
+    from piny_b200.lib import DeviceBox, PinyError
+    sp, pos, S = _boxes(nbox=1, seed=9)[0]
+    P = sp.nbeads
+    box = DeviceBox(S, P, "mixed")
+    xmod = pos.mean(axis=0) if P > 1 else None
+    box.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+    d = torch.from_numpy(pos).to("cuda:0")
+    dx = torch.from_numpy(xmod).to("cuda:0") if xmod is not None else None
+    choice, ms = box.autotune(d.data_ptr(), None if dx is None else dx.data_ptr(), S["hmat"], reps=2, again=True)
+    assert choice[0] in (8, 16) and choice[1] in (0, 1) and choice[2] in (4, 8, 16, 32) and choice[3] in (0, 1)
+    assert ms > 0
+    assert box.tuning() == choice
+    # a second context of the same shape applies the remembered result
+    box2 = DeviceBox(S, P, "mixed")
+    box2.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+    choice2, ms2 = box2.autotune(d.data_ptr(), None if dx is None else dx.data_ptr(), S["hmat"])
+    assert choice2 == choice and ms2 == -1.0
+    with pytest.raises(PinyError, match="ERR_ARG"):
+        box2.set_tuning([12, 0, 8, 1])
+    box.close()
+    box2.close()
