@@ -316,6 +316,45 @@ int pinyb200_batch_energy_force_device(pinyb200_batch *batch,
 int pinyb200_batch_last_ms(pinyb200_batch *batch, float *ms);
 const char *pinyb200_batch_last_error(pinyb200_batch *batch);
 
+/*
+ * Parameter gradients (adjoint).  A tangent holds the derivative of the
+ * set-up data with respect to one model parameter theta_k; NULL parts are
+ * zero.  Array sizes as the matching pinyb200_system fields:
+ *   dcharge      natm                  d charge
+ *   dcv0, dcdv0  ninter_unique*nsplin  d vdW tables (cv0, cdv0)
+ *   dghost_coef  nghost*ghost_ncomp    d ghost coefficients (moves the ghosts)
+ *   dbond_eq     nbond_typ             d bond equilibrium length
+ *   dbond_c      nbond_typ*7           d bond series c_0..c_6
+ *   dbend_c/s/dc/ds  nbend_typ*7 each  d bend series (all four, or none)
+ *   dclong       d clong (LJ tail, energy clong/volume)
+ * pinyb200_grad_prepare copies up to 16 tangents to the device (it
+ * allocates; call it when the parameters change).  pinyb200_grad then runs
+ * one forward evaluation at d_pos / d_xmod / hmat (as
+ * pinyb200_energy_force_device) and one adjoint pass, and returns for every
+ * tangent
+ *   dE[k] = d(vintert + vintrat) / d theta_k
+ *   dF[k] = sum over beads and atoms of fbar . dF / d theta_k
+ * where F are the forces with the ghost force distributed
+ * (PINYB200_DISTRIB_GHOSTS) and fbar (device, nbeads x natm x 3, or NULL
+ * for energy derivatives only) is the caller's upstream gradient, e.g.
+ * 2 (F - F_target) for a force-matching loss.  Pair terms are recomputed
+ * from the list, not stored.  No counterpart in PINY, which has no
+ * parameter derivatives.
+ */
+typedef struct pinyb200_tangent {
+    const double *dcharge;
+    const double *dcv0, *dcdv0;
+    const double *dghost_coef;
+    const double *dbond_eq, *dbond_c;
+    const double *dbend_c, *dbend_s, *dbend_dc, *dbend_ds;
+    double dclong;
+} pinyb200_tangent;
+int pinyb200_grad_prepare(pinyb200_ctx *ctx, int ntan,
+                          const pinyb200_tangent *tan);
+int pinyb200_grad(pinyb200_ctx *ctx, const double *d_pos, const double *d_xmod,
+                  const double *hmat, const double *d_fbar, double *dE,
+                  double *dF, void *stream);
+
 /* Milliseconds of the last evaluation, from CUDA events: 0 device work,
  * 1 pair forces, 2 PME, 3 intramolecular, 4 the whole host-buffer call of
  * pinyb200_energy_force (copies included).  PME runs on a second stream of

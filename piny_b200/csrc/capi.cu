@@ -172,6 +172,7 @@ static unsigned char *g_count_addr[kCountMaxDevices];
 Cell pinyb200::cell_from_hmat(const double *hmat) { return make_cell(hmat); }
 int pinyb200::record_error(pinyb200_ctx *c, int code, const std::string &msg) { return fail(c, code, msg); }
 static int pme_tiles_setup(pinyb200_ctx *c, int T);
+void pinyb200::table_coefs(const double *t, int nsplin, std::vector<double> &out) { cubic_coefs(t, nsplin, out); }
 int pinyb200::pme_tiles_resize(pinyb200_ctx *c, int T)
 {
     CK(cudaStreamSynchronize(c->stream));
@@ -235,6 +236,8 @@ int pinyb200_destroy(pinyb200_ctx *c)
         if (p) cudaFree(p);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    for (void *p : c->grad.dev) cudaFree(p);
+    c->grad.dev.clear();
     cudaEvent_t evx[4] = {c->ev_fork, c->ev_join, c->ev_pme[0], c->ev_pme[1]};
     for (cudaEvent_t ev : evx)
         if (ev) cudaEventDestroy(ev);
@@ -282,6 +285,8 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
     c->h_charge.assign(s->charge, s->charge + natm);
     c->h_cutoff.assign(s->cutoff, s->cutoff + s->ntyp * (s->ntyp + 1) / 2);
     c->skin = s->skin;
+    c->nbond_typ = s->nbond_typ;
+    c->nbend_typ = s->nbend_typ;
     CK(upload(&d.inter_map, s->inter_map, d.npair_typ));
     CK(upload(&d.cutoff, s->cutoff, d.npair_typ));
     CK(upload(&d.rmin, s->rmin_spl, d.nuniq));

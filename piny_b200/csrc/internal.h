@@ -73,6 +73,41 @@ struct DeviceSystem {
     double *ghost_coef = nullptr;
 };
 
+// Parameter derivatives (tangent channels) for the adjoint.  Channel k
+// holds the derivative of the set-up data with respect to one parameter;
+// absent parts are NULL.
+#define PINYB200_MAX_TAN 16
+struct GradChan {
+    const double *dq;        // [natm] d charge
+    const void *ttab;        // [2][nuniq][nsplin] cubic coefficients of d cv0, d cdv0 (double4 / float4)
+    const double *dcoef;     // [nghost][ncomp] d ghost coefficient
+    double *w;               // [natm][3][P] d site position (ghost rows), filled on the device
+    const double *bond_deq;  // [nbond_typ] d equilibrium length
+    const double *bond_dc;   // [nbond_typ][7] d power-series coefficients
+    const double *bend_c, *bend_s, *bend_dc, *bend_ds;  // [nbend_typ][7] d bend series
+};
+struct GradArgs {
+    int K;
+    GradChan ch[PINYB200_MAX_TAN];
+    const double *uT;        // [natm][3][P] adjoint of the raw site forces
+    double *gacc;            // [K][2] FP64 sums: energy derivative, force contraction
+};
+// host copies of the tangent data (owned by the context)
+struct GradHost {
+    int K = 0;
+    std::vector<void *> dev;  // every device allocation of the tangents
+    GradChan ch[PINYB200_MAX_TAN];
+    double dq_dot_q[PINYB200_MAX_TAN];  // sum_i q_i dq_i
+    double dq_sum[PINYB200_MAX_TAN];    // sum_i dq_i
+    double dclong[PINYB200_MAX_TAN];
+    double *d_u = nullptr;              // [natm][3][P]
+    double *d_gacc = nullptr;           // [K][2]
+    void *d_grid2 = nullptr;            // PME: dipole spread of u, then its convolution
+};
+
+cudaError_t launch_pme_adjoint(pinyb200_ctx *c, const Cell &cell, const GradArgs &g);
+cudaError_t launch_grad_terms(pinyb200_ctx *c, const Cell &cell, const GradArgs &g, const double *d_fbar);
+
 }  // namespace pinyb200
 
 struct pinyb200_ctx {
@@ -91,6 +126,7 @@ struct pinyb200_ctx {
     std::vector<double> h_charge;
     std::vector<double> h_cutoff;  // per type pair (Bohr)
     double skin = 0;               // Verlet skin (Bohr)
+    int nbond_typ = 0, nbend_typ = 0;
     double alp_ewd = 0, self_erf = 1, clong = 0;
     int iswit_vdw = 1;
     // Verlet list: full (parity) and active (force) CSR by i, j < i
@@ -141,6 +177,7 @@ struct pinyb200_ctx {
     bool filter_ok = false;
     cudaEvent_t ev[8];
     float last_ms[5] = {0, 0, 0, 0, 0};
+    pinyb200::GradHost grad;      // tangent channels of pinyb200_grad_prepare
     std::string err;
 };
 
@@ -165,6 +202,7 @@ int enqueue_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, c
                    double *d_force, bool timing, double *h_acc);
 Cell cell_from_hmat(const double *hmat);
 int pme_tiles_resize(pinyb200_ctx *c, int T);
+void table_coefs(const double *t, int nsplin, std::vector<double> &out);
 
 // cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per kernel, device
 // and size, so that repeated launches (and graph captures) do not repeat it.

@@ -1065,3 +1065,301 @@ cudaError_t launch_pme(pinyb200_ctx *c, const Cell &cell, bool energy)
 }
 
 }  // namespace pinyb200
+
+namespace pinyb200 {
+
+// ---------------------------------------------------------------------------
+// Adjoint of the reciprocal-space term (parameter gradients).
+//
+// With u the adjoint of the raw site forces, Q_u(g) = sum_s q_s u_s . grad
+// M_s(g) is spread, convolved with the same influence function as the charge
+// grid (chi = theta * Q_u), and gathered; with phi the forward potential:
+//   charge tangent dq:   dE += sum_s dq_s phi_s
+//                        dF += -sum_s dq_s (u_s . grad phi_s + chi_s)
+//   ghost position w:    dF += -sum_s q_s (w_s . grad chi_s + u_s^T (grad grad phi)_s w_s)
+// (symmetry of the influence function moves the convolution onto Q_u).
+
+// Second-derivative weights of the order-NI B-spline at offset f, PINY's
+// index j = 1..NI: d2[j] = m[j] - 2 m[j-1] + m[j-2] with m of order NI-2.
+template <typename R, int NI>
+__device__ __forceinline__ void bspline_d2(R f, R *d2)
+{
+    R u[NI + 1], m[NI + 1];
+#pragma unroll
+    for (int j = 1; j <= NI; j++) u[j] = f + (R)(j - 1);
+    m[0] = (R)0;
+    m[1] = (R)1 - fabs(u[1] - (R)1);
+    m[2] = (R)1 - fabs(u[2] - (R)1);
+#pragma unroll
+    for (int j = 3; j <= NI; j++) m[j] = (R)0;
+#pragma unroll
+    for (int nn = 3; nn <= NI - 2; nn++) {
+        const R rn = (R)nn, rn1 = (R)1 / (R)(nn - 1);
+#pragma unroll
+        for (int j = nn; j >= 2; j--) m[j] = (u[j] * m[j] + (rn - u[j]) * m[j - 1]) * rn1;
+        m[1] = u[1] * m[1] * rn1;
+    }
+#pragma unroll
+    for (int j = 1; j <= NI; j++) d2[j] = m[j] - (R)2 * (j >= 2 ? m[j - 1] : (R)0) + (j >= 3 ? m[j - 2] : (R)0);
+}
+
+// u (or w) in scaled-grid units: t_d = N_d sum_alpha hi[d + 3 alpha] v_alpha.
+__device__ __forceinline__ void scaled_vec(const PmeArgs &a, const Cell &cell, double vx, double vy, double vz,
+                                           double *t)
+{
+    const int N[3] = {a.Na, a.Nb, a.Nc};
+#pragma unroll
+    for (int d = 0; d < 3; d++) t[d] = N[d] * (cell.hi[d] * vx + cell.hi[d + 3] * vy + cell.hi[d + 6] * vz);
+}
+
+// Q_u: one warp per record, lanes 8 a points x 4 b rows, FP32/FP64 atomics.
+template <typename R, int NI>
+__global__ void __launch_bounds__(256) pme_dipole_spread_kernel(PmeArgs a, Cell cell, const double *__restrict__ uT,
+                                                                R *__restrict__ grid2)
+{
+    typedef RecGeom<NI> RG;
+    const int lane = threadIdx.x & 31;
+    const int ta = lane & 7, tq = lane >> 3;
+    const long long nrec = (long long)a.nchrg * a.P;
+    const size_t G = (size_t)a.Na * a.Nb * a.Nc;
+    for (long long idx = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; idx < nrec;
+         idx += ((long long)gridDim.x * blockDim.x) >> 5) {
+        const int b = (int)(idx % a.P);
+        const int4 h = a.rhead[idx];
+        const int at = h.x;
+        const double ux = uT[(3 * (size_t)at + 0) * a.P + b], uy = uT[(3 * (size_t)at + 1) * a.P + b],
+                     uz = uT[(3 * (size_t)at + 2) * a.P + b];
+        if (ux == 0.0 && uy == 0.0 && uz == 0.0) continue;
+        double ut[3];
+        scaled_vec(a, cell, ux, uy, uz, ut);
+        const R q = (R)a.charge[at];
+        const R *w = (const R *)a.rw + (size_t)idx * RG::NW;
+        R *g = grid2 + (size_t)b * G;
+        for (int sa = 0; sa < NI; sa += 8) {
+            const int t_a = ta + sa;
+            if (t_a >= NI) break;
+            const R ma = w[t_a], da = w[3 * RG::NIP + t_a];
+            const int ga = wrapi(h.y + t_a, a.Na);
+            for (int tb = tq; tb < NI; tb += 4) {
+                const R mb = w[RG::NIP + tb], db = w[4 * RG::NIP + tb];
+                const int gb = wrapi(h.z + tb, a.Nb);
+                const R cab = q * ((R)ut[0] * da * mb + (R)ut[1] * ma * db), cc = q * (R)ut[2] * ma * mb;
+                for (int tc = 0; tc < NI; tc++) {
+                    const R val = cab * w[2 * RG::NIP + tc] + cc * w[5 * RG::NIP + tc];
+                    atomicAdd(g + ((size_t)wrapi(h.w + tc, a.Nc) * a.Nb + gb) * a.Na + ga, val);
+                }
+            }
+        }
+    }
+}
+
+// Gathers phi, grad phi, chi, grad chi (and grad grad phi at sites with a
+// ghost tangent) per record and contracts them with every channel.
+template <typename R, int NI>
+__global__ void __launch_bounds__(128) pme_adjoint_gather_kernel(PmeArgs a, Cell cell, GradArgs g,
+                                                                 const R *__restrict__ phi, const R *__restrict__ chi)
+{
+    typedef RecGeom<NI> RG;
+    __shared__ double sh[2 * PINYB200_MAX_TAN];
+    double acc[2 * PINYB200_MAX_TAN];
+    for (int k = 0; k < 2 * g.K; k++) acc[k] = 0.0;
+    const long long nrec = (long long)a.nchrg * a.P;
+    const size_t G = (size_t)a.Na * a.Nb * a.Nc;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < nrec;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(idx % a.P);
+        const int4 h = a.rhead[idx];
+        const int at = h.x;
+        R m[6][RG::NIP];
+        const R *w = (const R *)a.rw + (size_t)idx * RG::NW;
+#pragma unroll
+        for (int j = 0; j < 6; j++) load4<RG::NIP>(m[j], w + j * RG::NIP);
+        const R *pg = phi + (size_t)b * G, *cg = chi + (size_t)b * G;
+        double P0 = 0, Pa = 0, Pb = 0, Pc = 0, X0 = 0, Xa = 0, Xb = 0, Xc = 0;
+#pragma unroll 1
+        for (int tc = 0; tc < NI; tc++) {
+            const int gc = wrapi(h.w + tc, a.Nc);
+            R p0 = 0, pa = 0, pb = 0, pc = 0, x0 = 0, xa = 0, xb = 0, xc = 0;
+#pragma unroll
+            for (int tb = 0; tb < NI; tb++) {
+                const size_t row = ((size_t)gc * a.Nb + wrapi(h.z + tb, a.Nb)) * a.Na;
+                R sp = 0, sdp = 0, sx = 0, sdx = 0;
+#pragma unroll
+                for (int t_a = 0; t_a < NI; t_a++) {
+                    const int ga = wrapi(h.y + t_a, a.Na);
+                    const R pv = pg[row + ga], xv = cg[row + ga];
+                    sp += m[0][t_a] * pv;
+                    sdp += m[3][t_a] * pv;
+                    sx += m[0][t_a] * xv;
+                    sdx += m[3][t_a] * xv;
+                }
+                p0 += m[1][tb] * sp;
+                pa += m[1][tb] * sdp;
+                pb += m[4][tb] * sp;
+                x0 += m[1][tb] * sx;
+                xa += m[1][tb] * sdx;
+                xb += m[4][tb] * sx;
+                (void)pc;
+                (void)xc;
+            }
+            P0 += (double)(m[2][tc] * p0);
+            Pa += (double)(m[2][tc] * pa);
+            Pb += (double)(m[2][tc] * pb);
+            Pc += (double)(m[5][tc] * p0);
+            X0 += (double)(m[2][tc] * x0);
+            Xa += (double)(m[2][tc] * xa);
+            Xb += (double)(m[2][tc] * xb);
+            Xc += (double)(m[5][tc] * x0);
+        }
+        const double ux = g.uT[(3 * (size_t)at + 0) * a.P + b], uy = g.uT[(3 * (size_t)at + 1) * a.P + b],
+                     uz = g.uT[(3 * (size_t)at + 2) * a.P + b];
+        double ut[3];
+        scaled_vec(a, cell, ux, uy, uz, ut);
+        const double udphi = ut[0] * Pa + ut[1] * Pb + ut[2] * Pc;
+        const double q = a.charge[at];
+        // the ghost-position tangents of this site, if any
+        bool need_h = false;
+        for (int k = 0; k < g.K; k++)
+            if (g.ch[k].w) {
+                const double *wv = g.ch[k].w;
+                if (wv[(3 * (size_t)at) * a.P + b] != 0.0 || wv[(3 * (size_t)at + 1) * a.P + b] != 0.0 ||
+                    wv[(3 * (size_t)at + 2) * a.P + b] != 0.0)
+                    need_h = true;
+            }
+        double H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        if (need_h) {
+            int la, lb, lc;
+            double fa, fb, fc;
+            stencil_origin(a, cell, at, b, NI, la, lb, lc, fa, fb, fc);
+            R d2[3][NI + 1];
+            bspline_d2<R, NI>((R)fa, d2[0]);
+            bspline_d2<R, NI>((R)fb, d2[1]);
+            bspline_d2<R, NI>((R)fc, d2[2]);
+            // grid order: point lo + t carries index NI - t
+            double haa = 0, hbb = 0, hcc = 0, hab = 0, hac = 0, hbc = 0;
+            for (int tc = 0; tc < NI; tc++) {
+                const int gc = wrapi(h.w + tc, a.Nc);
+                for (int tb = 0; tb < NI; tb++) {
+                    const size_t row = ((size_t)gc * a.Nb + wrapi(h.z + tb, a.Nb)) * a.Na;
+                    for (int t_a = 0; t_a < NI; t_a++) {
+                        const double pv = (double)pg[row + wrapi(h.y + t_a, a.Na)];
+                        const double ma = m[0][t_a], mb = m[1][tb], mc = m[2][tc];
+                        const double da = m[3][t_a], db = m[4][tb], dc = m[5][tc];
+                        haa += (double)d2[0][NI - t_a] * mb * mc * pv;
+                        hbb += ma * (double)d2[1][NI - tb] * mc * pv;
+                        hcc += ma * mb * (double)d2[2][NI - tc] * pv;
+                        hab += da * db * mc * pv;
+                        hac += da * mb * dc * pv;
+                        hbc += ma * db * dc * pv;
+                    }
+                }
+            }
+            H[0][0] = haa;
+            H[1][1] = hbb;
+            H[2][2] = hcc;
+            H[0][1] = H[1][0] = hab;
+            H[0][2] = H[2][0] = hac;
+            H[1][2] = H[2][1] = hbc;
+        }
+        for (int k = 0; k < g.K; k++) {
+            const GradChan &ch = g.ch[k];
+            if (ch.dq) {
+                const double dq = ch.dq[at];
+                if (dq != 0.0) {
+                    acc[2 * k] += dq * P0 / (double)a.P;
+                    acc[2 * k + 1] += -dq * (udphi + X0);
+                }
+            }
+            if (ch.w && need_h) {
+                const double wx = ch.w[(3 * (size_t)at) * a.P + b], wy = ch.w[(3 * (size_t)at + 1) * a.P + b],
+                             wz = ch.w[(3 * (size_t)at + 2) * a.P + b];
+                double wt[3];
+                scaled_vec(a, cell, wx, wy, wz, wt);
+                double uhw = 0;
+                for (int d = 0; d < 3; d++)
+                    for (int e = 0; e < 3; e++) uhw += ut[d] * H[d][e] * wt[e];
+                acc[2 * k + 1] += -q * (wt[0] * Xa + wt[1] * Xb + wt[2] * Xc + uhw);
+            }
+        }
+    }
+    // block flush
+    for (int i = threadIdx.x; i < 2 * g.K; i += blockDim.x) sh[i] = 0.0;
+    __syncthreads();
+    for (int i = 0; i < 2 * g.K; i++)
+        if (acc[i] != 0.0) atomicAdd(&sh[i], acc[i]);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * g.K; i += blockDim.x)
+        if (sh[i] != 0.0) atomicAdd(&g.gacc[i], sh[i]);
+}
+
+template <typename R, int NI>
+static cudaError_t launch_pme_adjoint_t(pinyb200_ctx *c, const Cell &cell, const GradArgs &g)
+{
+    typedef typename Cplx<R>::T C2;
+    const DeviceSystem &s = c->sys;
+    PmeArgs a;
+    a.natm = s.natm;
+    a.P = c->P;
+    a.nchrg = s.nchrg;
+    a.ichrg = s.ichrg;
+    a.charge = s.charge;
+    a.posT = c->d_posT;
+    a.Na = s.ngrid[0];
+    a.Nb = s.ngrid[1];
+    a.Nc = s.ngrid[2];
+    a.n = s.n_interp;
+    a.grid = c->grad.d_grid2;
+    a.forceP = c->d_forceP;
+    a.rhead = (int4 *)c->d_pme_head;
+    a.rw = c->d_pme_w;
+    const size_t G = (size_t)a.Na * a.Nb * a.Nc;
+    const bool f64 = sizeof(R) == 8;
+    cudaError_t err = cudaMemsetAsync(c->grad.d_grid2, 0, sizeof(R) * G * c->P, c->stream);
+    if (err != cudaSuccess) return err;
+    const long long nrec = (long long)a.nchrg * a.P;
+    long long blocks = (nrec * 32 + 255) / 256;
+    if (blocks > (long long)c->sm_count * 16) blocks = (long long)c->sm_count * 16;
+    pme_dipole_spread_kernel<R, NI><<<(unsigned)blocks, 256, 0, c->stream>>>(a, cell, g.uT, (R *)c->grad.d_grid2);
+    const R *twbase = (const R *)(f64 ? (const void *)c->d_twiddle64 : (const void *)c->d_twiddle32);
+    const R *tw[3] = {twbase, twbase + 2 * 256, twbase + 4 * 256};
+    const size_t sp = pme_plane_smem(a.Na, a.Nb, f64), ss = pme_slab_smem(a.Na, a.Nc, f64);
+    C2 *spec = (C2 *)c->d_spec;
+    const R *filt = f64 ? (const R *)c->d_filter : (const R *)((const double *)c->d_filter + G);
+    const bool cube = a.Na == a.Nb && a.Na == a.Nc;
+    switch (cube ? a.Na : 0) {
+    case 16: err = launch_fft_t<R, 16>(c, a, cell, spec, filt, tw, sp, ss, false); break;
+    case 32: err = launch_fft_t<R, 32>(c, a, cell, spec, filt, tw, sp, ss, false); break;
+    case 64: err = launch_fft_t<R, 64>(c, a, cell, spec, filt, tw, sp, ss, false); break;
+    case 128: err = launch_fft_t<R, 128>(c, a, cell, spec, filt, tw, sp, ss, false); break;
+    default: err = launch_fft_t<R, 0>(c, a, cell, spec, filt, tw, sp, ss, false); break;
+    }
+    if (err != cudaSuccess) return err;
+    long long gb = (nrec + 127) / 128;
+    if (gb > (long long)c->sm_count * 8) gb = (long long)c->sm_count * 8;
+    pme_adjoint_gather_kernel<R, NI><<<(unsigned)(gb < 1 ? 1 : gb), 128, 0, c->stream>>>(
+        a, cell, g, (const R *)c->d_grid, (const R *)c->grad.d_grid2);
+    return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t launch_pme_adjoint_r(pinyb200_ctx *c, const Cell &cell, const GradArgs &g)
+{
+    switch (c->sys.n_interp) {
+    case 4: return launch_pme_adjoint_t<R, 4>(c, cell, g);
+    case 5: return launch_pme_adjoint_t<R, 5>(c, cell, g);
+    case 6: return launch_pme_adjoint_t<R, 6>(c, cell, g);
+    case 7: return launch_pme_adjoint_t<R, 7>(c, cell, g);
+    case 8: return launch_pme_adjoint_t<R, 8>(c, cell, g);
+    case 10: return launch_pme_adjoint_t<R, 10>(c, cell, g);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_pme_adjoint(pinyb200_ctx *c, const Cell &cell, const GradArgs &g)
+{
+    if (c->sys.nchrg == 0 || c->sys.nktot == 0 || !c->grad.d_grid2) return cudaSuccess;
+    if (c->precision == PINYB200_FP64) return launch_pme_adjoint_r<double>(c, cell, g);
+    return launch_pme_adjoint_r<float>(c, cell, g);
+}
+
+}  // namespace pinyb200

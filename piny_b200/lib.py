@@ -59,6 +59,13 @@ class PinyEnergies(C.Structure):
     _fields_ = [(n, _d) for n in ENERGY_NAMES] + [("pvten", _d * 9)]
 
 
+class PinyTangent(C.Structure):
+    """pinyb200_tangent: derivative of the set-up data along one parameter."""
+    _fields_ = [("dcharge", _pd), ("dcv0", _pd), ("dcdv0", _pd), ("dghost_coef", _pd), ("dbond_eq", _pd),
+                ("dbond_c", _pd), ("dbend_c", _pd), ("dbend_s", _pd), ("dbend_dc", _pd), ("dbend_ds", _pd),
+                ("dclong", _d)]
+
+
 # every symbol include/pinyb200.h declares
 EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb200_destroy",
            "pinyb200_build_list", "pinyb200_get_list", "pinyb200_list_info", "pinyb200_energy_force",
@@ -66,7 +73,7 @@ EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb
            "pinyb200_last_error", "pinyb200_count_list_device", "pinyb200_check_list_device",
            "pinyb200_autotune", "pinyb200_get_tuning", "pinyb200_set_tuning", "pinyb200_batch_create",
            "pinyb200_batch_destroy", "pinyb200_batch_energy_force_device", "pinyb200_batch_last_ms",
-           "pinyb200_batch_last_error")
+           "pinyb200_batch_last_error", "pinyb200_grad_prepare", "pinyb200_grad")
 
 COUNT_MAX_ATOMS = 65536       # PINYB200_COUNT_MAX_ATOMS
 COUNT_MAX_PAIR_TYPES = 64     # PINYB200_COUNT_MAX_PAIR_TYPES
@@ -116,6 +123,8 @@ def load(build_if_missing: bool = True):
     L.pinyb200_batch_last_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
     L.pinyb200_batch_last_error.restype = C.c_char_p
     L.pinyb200_batch_last_error.argtypes = [C.c_void_p]
+    L.pinyb200_grad_prepare.argtypes = [C.c_void_p, _i, C.POINTER(PinyTangent)]
+    L.pinyb200_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, C.c_void_p, _pd, _pd, C.c_void_p]
     L.pinyb200_last_error.restype = C.c_char_p
     L.pinyb200_last_error.argtypes = [C.c_void_p]
     _LIB = L
@@ -278,6 +287,38 @@ class DeviceBox:
     def set_tuning(self, choice):
         ch = (C.c_int * 4)(*[int(v) for v in choice])
         self._check(self.L.pinyb200_set_tuning(self.h, ch), "set_tuning")
+
+    def grad_prepare(self, tangents):
+        """Upload tangent channels: a list of dicts with keys of PinyTangent
+        (arrays or scalars; missing keys are zero)."""
+        arr = (PinyTangent * max(1, len(tangents)))()
+        keep = []
+        for k, t in enumerate(tangents):
+            for name, ctype in PinyTangent._fields_:
+                v = t.get(name)
+                if ctype is _pd:
+                    if v is None:
+                        setattr(arr[k], name, None)
+                    else:
+                        a = np.ascontiguousarray(v, np.float64)
+                        keep.append(a)
+                        setattr(arr[k], name, _dp(a))
+                else:
+                    setattr(arr[k], name, float(v or 0.0))
+        self._check(self.L.pinyb200_grad_prepare(self.h, len(tangents), arr), "grad_prepare")
+        self._ntan = len(tangents)
+
+    def grad(self, d_pos: int, d_xmod, hmat, d_fbar=None, stream=None):
+        """(dE, dF) per prepared tangent (see pinyb200_grad)."""
+        hmat = np.ascontiguousarray(hmat, np.float64)
+        n = max(1, getattr(self, "_ntan", 0))
+        dE = np.zeros(n)
+        dF = np.zeros(n)
+        self._check(self.L.pinyb200_grad(self.h, C.c_void_p(d_pos), None if d_xmod is None else C.c_void_p(d_xmod),
+                                         _dp(hmat), None if d_fbar is None else C.c_void_p(d_fbar), _dp(dE), _dp(dF),
+                                         None if stream is None else C.c_void_p(stream)), "grad")
+        k = getattr(self, "_ntan", 0)
+        return dE[:k], dF[:k]
 
     def last_timing(self):
         ms = (C.c_float * 5)()
