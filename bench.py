@@ -43,11 +43,13 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="tip4pf_4096_p32",
-                    help="a named box, or c4_batch64: 64 uneven boxes in one graph launch per step")
+                    help="a named box; c4_batch64: 64 uneven boxes in one graph launch per step; "
+                         "c5_grad: parameter gradients of 1024 TIP4P/F x 16 beads")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-energy", action="store_true", help="forces only (PINYB200_NO_ENERGY), for profiling")
+    ap.add_argument("--fd", action="store_true", help="c5_grad: also check against central differences")
     return ap.parse_args()
 
 
@@ -221,6 +223,109 @@ def alg_bytes_per_bead_eval(S, P, nlist, precision):
     return 48.0 * S["natm"] + 4.0 * nlist / P + 6.0 * G * bg
 
 
+def run_grad(args, ws, rank, local):
+    """Gradients of the energy and of a force-matching loss with respect to
+    the 9 q-TIP4P/F parameters (1024 molecules, 16 beads, 32^3 mesh): one
+    step = forward evaluation + adjoint pass; MIXED timed, checked against
+    the FP64 adjoint and against central differences of the FP64 device
+    forward (h = 1e-5 relative)."""
+    import dataclasses
+
+    import torch
+
+    from piny_b200 import params, water
+    from piny_b200.params import PinyForceField
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    spec = water.named_spec("tip4pf_1024_p16")
+    if ws > 1:
+        spec = dataclasses.replace(spec, seed=spec.seed + rank)
+    pos_A = water.build_positions(spec)
+    theta = params.theta_of(spec.model)
+    rng = np.random.default_rng(2024)
+    theta_t = theta * (1.0 + rng.uniform(-0.02, 0.02, size=theta.shape))
+    f64 = PinyForceField(spec, pos_A, "fp64", device=str(dev))
+    _, f_target = f64.energy_forces(theta_t)
+    E64, F64 = f64.energy_forces(theta)
+    fbar = 2.0 * (F64 - f_target)
+    g64 = f64.adjoint(theta, 1.0, fbar)
+    mixed = PinyForceField(spec, pos_A, args.precision, device=str(dev))
+    E, F = mixed.energy_forces(theta)
+    d_fbar = torch.from_numpy(2.0 * (F - f_target)).to(dev)
+    box = mixed.box
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        return box.grad(mixed.d_pos.data_ptr(), None if mixed.d_xmod is None else mixed.d_xmod.data_ptr(),
+                        mixed.hmat, d_fbar.data_ptr(), stream=stream.cuda_stream)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if ws > 1:
+        torch.distributed.barrier()
+    ms_list = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dE, dF = step()
+        e1.record(stream)
+        e1.synchronize()
+        ms_list.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    ms = float(np.mean(ms_list))
+    if ws > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    g_mixed = dE + dF
+    rel_mixed = float(np.abs(g_mixed - g64).max() / np.abs(g64).max())
+    fd = None
+    if getattr(args, "fd", False):
+        gfd = np.zeros(len(theta))
+        for k in range(len(theta)):
+            h = 1e-5 * abs(theta[k])
+            tp, tm = theta.copy(), theta.copy()
+            tp[k] += h
+            tm[k] -= h
+            Ep, Fp = f64.energy_forces(tp)
+            Em, Fm = f64.energy_forces(tm)
+            gfd[k] = (Ep - Em) / (2 * h) + (((Fp - f_target) ** 2).sum() - ((Fm - f_target) ** 2).sum()) / (2 * h)
+        fd = {params.PARAMS[k]: {"adjoint_fp64": float(g64[k]), "central_difference": float(gfd[k]),
+                                 "rel": float(abs(g64[k] - gfd[k]) / max(abs(gfd[k]), 1e-300))}
+              for k in range(len(theta))}
+    if rank == 0:
+        line = {
+            "metric": "parameter-gradient evals/s (9 q-TIP4P/F parameters; energy + force-matching loss; "
+                      "1024 mol x 16 beads)", "value": ws * 1e3 / ms, "unit": "gradient evals/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64acc" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": "c5_grad", "molecules": spec.nmol, "beads": spec.nbeads, "pme_grid": spec.grid,
+                       "parameters": list(params.PARAMS), "target": "theta perturbed by seeded +-2 %",
+                       "step": "forward evaluation + adjoint (pinyb200_grad)",
+                       "l2": "256 MiB buffer written between timed steps; CUDA events on the launch stream"},
+            "gradient": {"theta": theta.tolist(), "mixed": g_mixed.tolist(), "fp64": g64.tolist(),
+                         "max_rel_mixed_vs_fp64": rel_mixed, "finite_differences_fp64": fd},
+            "roofline": None, "cpu_baseline": None, "e2e": None,
+            "gpu_launches": None, "clocks": clocks,
+        }
+        print(json.dumps(line))
+    f64.close()
+    mixed.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def run_batch(args, ws, rank, local):
     """64 uneven TIP4P/F boxes, all beads, one CUDA graph launch per step."""
     import torch
@@ -355,6 +460,8 @@ def main():
         return run_reference(args, ws, rank)
     if args.config.startswith("c4_batch"):
         return run_batch(args, ws, rank, local)
+    if args.config == "c5_grad":
+        return run_grad(args, ws, rank, local)
 
     import torch
 
