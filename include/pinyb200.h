@@ -26,9 +26,9 @@ typedef enum pinyb200_status {
     PINYB200_ERR_CUDA = 2,           /* a CUDA runtime call failed              */
     PINYB200_ERR_NO_DEVICE = 3,      /* no usable GPU                           */
     PINYB200_ERR_LIST_OVERFLOW = 4,  /* Verlet list larger than its capacity    */
-    PINYB200_ERR_CUTOFF = 5,         /* cutoff exceeds half the box (warning)   */
-    PINYB200_ERR_TIMEOUT = 6,        /* a bounded device wait gave up           */
-    PINYB200_ERR_NAN = 7,            /* non-finite positions or forces          */
+    PINYB200_ERR_CUTOFF = 5,         /* reserved (PINY only warns; not checked) */
+    PINYB200_ERR_TIMEOUT = 6,        /* reserved (no kernel waits on another)   */
+    PINYB200_ERR_NAN = 7,            /* non-finite energy (forces are written)  */
     PINYB200_ERR_UNSUPPORTED = 8,    /* option not built for this path          */
     PINYB200_ERR_STATE = 9           /* call order violated (e.g. no list yet)  */
 } pinyb200_status;

@@ -704,6 +704,8 @@ static int evaluate(pinyb200_ctx *c, const Cell &cell, int flags, pinyb200_energ
     CK(cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]));
     CK(cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]));
     evaluate_finish(c, cell, flags, energy ? acc.data() : nullptr, e);
+    if (energy && e && !std::isfinite(e->vintert + e->vintrat))
+        return fail(c, PINYB200_ERR_NAN, "non-finite energy: check the positions (forces were written)");
     return PINYB200_OK;
 }
 
@@ -766,6 +768,8 @@ int pinyb200_energy_force_device(pinyb200_ctx *c, const double *d_pos, const dou
     CK(cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]));
     CK(cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]));
     evaluate_finish(c, cell, flags, energy ? acc.data() : nullptr, e);
+    if (energy && e && !std::isfinite(e->vintert + e->vintrat))
+        return fail(c, PINYB200_ERR_NAN, "non-finite energy: check the positions (forces were written)");
     return PINYB200_OK;
 }
 

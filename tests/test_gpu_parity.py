@@ -169,3 +169,20 @@ def test_list_check_matches_oracle(name, oracle):
         assert (reb, rmax, sp) == (f, r_o, s_o)
         assert np.array_equal(cs, cs_o)
     box.close()
+
+
+def test_non_finite_positions_are_reported():
+    """A NaN position gives PINYB200_ERR_NAN from the host-buffer call (the
+    device work itself runs on the NaN and finishes normally)."""
+    F = load_fixture("spcfw_64_p1")
+    from piny_b200.lib import DeviceBox, PinyError
+    box = DeviceBox(F, 1, "fp64")
+    box.build_list(F["pos"][0], None, F["hmat"], F["cutskin2"])
+    pos = np.array(F["pos"], np.float64)
+    pos[0, 5, 1] = np.nan
+    with pytest.raises(PinyError, match="ERR_NAN"):
+        box.energy_force(pos, None, F["hmat"])
+    # the context stays usable
+    force, e = box.energy_force(F["pos"], None, F["hmat"])
+    assert np.isfinite(e["vintert"])
+    box.close()
