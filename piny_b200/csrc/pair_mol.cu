@@ -168,7 +168,7 @@ __device__ __forceinline__ double shift_exact(double dm, double hi) { return -ni
 
 // Resident blocks of 128 threads per SM the register allocation aims at.
 #ifndef PINYB200_MOL_BLOCKS32
-#define PINYB200_MOL_BLOCKS32 4
+#define PINYB200_MOL_BLOCKS32 5
 #endif
 #ifndef PINYB200_MOL_BLOCKS64
 #define PINYB200_MOL_BLOCKS64 3
@@ -230,6 +230,51 @@ __device__ __forceinline__ bool site_pair(const typename Vec4<R>::T *__restrict_
         pvs[5] += ry * fz;
     }
     return true;
+}
+
+// One molecule pair whose site-0 separation is within twice the molecular
+// extent of half a box, so that its site pairs may take different images:
+// every site pair gets its own period_pimd shift (period.c:163-176) and its
+// separation in FP64; forces go straight to the force array.  Kept out of
+// line: it is rare in large boxes and would otherwise burden the main
+// loop with its registers.
+template <typename R, int P, int NS, bool FAST, bool ENERGY>
+__device__ __noinline__ void mol_pair_near(const double *__restrict__ posT, const double *__restrict__ xmod,
+                                           double *__restrict__ forceT, const PairConst<R> *pc,
+                                           const typename Vec4<R>::T *__restrict__ tab, size_t tstride, int nsm2,
+                                           int i0, int j0, unsigned mask, int b, double hx, double hy, double hz,
+                                           double hix, double hiy, double hiz, double *sacc)
+{
+    const double hd[3] = {hx, hy, hz}, hid[3] = {hix, hiy, hiz};
+    R evs = 0, ecs = 0, pvs[6] = {0, 0, 0, 0, 0, 0};
+    for (unsigned m = mask; m; m &= m - 1u) {
+        const int sp = __ffs(m) - 1;
+        const int si = sp / NS, sj = sp % NS;
+        const int i = i0 + si, j = j0 + sj;
+        double r[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double sh = shift_exact(__dsub_rn(xmod[3 * (size_t)i + d], xmod[3 * (size_t)j + d]), hid[d]);
+            r[d] = __dadd_rn(__dsub_rn(posT[(3 * (size_t)i + d) * P + b], posT[(3 * (size_t)j + d) * P + b]),
+                             __dmul_rn(sh, hd[d]));
+        }
+        R fx, fy, fz;
+        if (site_pair<R, FAST, ENERGY>(tab, tstride, nsm2, *pc, sp, (R)r[0], (R)r[1], (R)r[2], fx, fy, fz, evs, ecs,
+                                       pvs)) {
+            atomicAdd(&forceT[(3 * (size_t)i + 0) * P + b], (double)fx);
+            atomicAdd(&forceT[(3 * (size_t)i + 1) * P + b], (double)fy);
+            atomicAdd(&forceT[(3 * (size_t)i + 2) * P + b], (double)fz);
+            atomicAdd(&forceT[(3 * (size_t)j + 0) * P + b], -(double)fx);
+            atomicAdd(&forceT[(3 * (size_t)j + 1) * P + b], -(double)fy);
+            atomicAdd(&forceT[(3 * (size_t)j + 2) * P + b], -(double)fz);
+        }
+    }
+    if (ENERGY) {
+        sacc[0] += (double)evs;
+        sacc[128] += (double)ecs;
+#pragma unroll
+        for (int c = 0; c < 6; c++) sacc[128 * (2 + c)] += (double)pvs[c];
+    }
 }
 
 template <typename R, int P, int NS, bool FAST, bool ENERGY>
@@ -301,8 +346,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
                      xm0z = a.xmod[3 * (size_t)i0 + 2];
         R evs = 0, ecs = 0, pvs[6] = {0, 0, 0, 0, 0, 0};
         for (int k = beg + sub; k < end; k += JPI) {
-            const int mj = a.mj[k];
-            const unsigned mask = a.mask[k];
+            const int mj = __ldcg(a.mj + k);
+            const unsigned mask = __ldcg(a.mask + k);
             const int j0 = a.mstart[mj];
             unsigned jm = 1u;
 #pragma unroll
@@ -312,16 +357,16 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
             for (int s = 0; s < NS; s++) {
                 const int j = j0 + (((jm >> s) & 1u) ? s : 0);
 #pragma unroll
-                for (int d = 0; d < 3; d++) xj[s][d] = posT[(3 * (size_t)j + d) * P + b];
+                for (int d = 0; d < 3; d++) xj[s][d] = __ldcg(posT + (3 * (size_t)j + d) * P + b);
             }
             // site-0 image (mode-1 separation, FP64) and whether the pair is
             // close enough to half a box for site pairs to differ from it
             double sh0[3];
             bool near = false;
             {
-                const double dm[3] = {__dsub_rn(xm0x, a.xmod[3 * (size_t)j0]),
-                                      __dsub_rn(xm0y, a.xmod[3 * (size_t)j0 + 1]),
-                                      __dsub_rn(xm0z, a.xmod[3 * (size_t)j0 + 2])};
+                const double dm[3] = {__dsub_rn(xm0x, __ldcg(a.xmod + 3 * (size_t)j0)),
+                                      __dsub_rn(xm0y, __ldcg(a.xmod + 3 * (size_t)j0 + 1)),
+                                      __dsub_rn(xm0z, __ldcg(a.xmod + 3 * (size_t)j0 + 2))};
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
                     const double hid = cell.hi[4 * d];
@@ -329,6 +374,12 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
                     sh0[d] = -nint_rn(t);
                     near |= fabs(t + sh0[d]) > 0.5 - 2.0 * PINYB200_MOL_EXTENT * hid;
                 }
+            }
+            if (near) {
+                mol_pair_near<R, P, NS, FAST, ENERGY>(posT, a.xmod, a.forceT, &pc, tab, tstride, nsm2, i0, j0, mask, b,
+                                                      cell.h[0], cell.h[4], cell.h[8], cell.hi[0], cell.hi[4],
+                                                      cell.hi[8], &sacc[0][threadIdx.x]);
+                continue;
             }
             R d0[3], ej[NS][3];
             if (FAST) {
@@ -364,34 +415,20 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
                             xjz = xj[s2][2];
                         }
                     }
-                double xmj[3] = {0, 0, 0};
-                if (near)
-#pragma unroll
-                    for (int d = 0; d < 3; d++) xmj[d] = a.xmod[3 * (size_t)(j0 + sj) + d];
                 R fjx = 0, fjy = 0, fjz = 0;
 #pragma unroll
                 for (int si = 0; si < NS; si++) {
                     if (!((col >> si) & 1u)) continue;
-                    double sh[3] = {sh0[0], sh0[1], sh0[2]};
-                    if (near) {
-#pragma unroll
-                        for (int d = 0; d < 3; d++)
-                            sh[d] = shift_exact(__dsub_rn(a.xmod[3 * (size_t)(i0 + si) + d], xmj[d]), cell.hi[4 * d]);
-                    }
+                    // away from half a box every site pair takes the site-0 image
                     R rx, ry, rz;
                     if (FAST) {
                         rx = djx + ei[si][0];
                         ry = djy + ei[si][1];
                         rz = djz + ei[si][2];
-                        if (near) {
-                            rx += (R)((sh[0] - sh0[0]) * cell.h[0]);
-                            ry += (R)((sh[1] - sh0[1]) * cell.h[4]);
-                            rz += (R)((sh[2] - sh0[2]) * cell.h[8]);
-                        }
                     } else {
-                        rx = (R)__dadd_rn(__dsub_rn(xi[si][0], xjx), __dmul_rn(sh[0], cell.h[0]));
-                        ry = (R)__dadd_rn(__dsub_rn(xi[si][1], xjy), __dmul_rn(sh[1], cell.h[4]));
-                        rz = (R)__dadd_rn(__dsub_rn(xi[si][2], xjz), __dmul_rn(sh[2], cell.h[8]));
+                        rx = (R)__dadd_rn(__dsub_rn(xi[si][0], xjx), __dmul_rn(sh0[0], cell.h[0]));
+                        ry = (R)__dadd_rn(__dsub_rn(xi[si][1], xjy), __dmul_rn(sh0[1], cell.h[4]));
+                        rz = (R)__dadd_rn(__dsub_rn(xi[si][2], xjz), __dmul_rn(sh0[2], cell.h[8]));
                     }
                     R fx, fy, fz;
                     if (site_pair<R, FAST, ENERGY>(tab, tstride, nsm2, pc, si * NS + sj, rx, ry, rz, fx, fy, fz, evs,
