@@ -50,6 +50,7 @@ def parse_args():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-energy", action="store_true", help="forces only (PINYB200_NO_ENERGY), for profiling")
     ap.add_argument("--fd", action="store_true", help="c5_grad: also check against central differences")
+    ap.add_argument("--tuning", default="", help="pin a launch shape: tile,pair_kernel,blocks_per_sm,overlap")
     return ap.parse_args()
 
 
@@ -486,6 +487,8 @@ def main():
     t0 = time.perf_counter()
     npairs = box.build_list(pos[0], xmod, hmat, S["cutskin2"])
     list_s = time.perf_counter() - t0
+    if args.tuning:
+        box.set_tuning([int(v) for v in args.tuning.split(",")])
 
     stream = torch.cuda.current_stream(dev)
     d_pos = torch.from_numpy(pos).to(dev)
