@@ -302,8 +302,9 @@ def _pair_index(ti, tj, ntyp):
     return ((jj - 1) * ((ntyp + 1) * 2 - jj)) // 2 + ii - jj
 
 
-def build_system(spec: "water.BoxSpec", pos_bohr, rheal_A=1.0):
-    """Set-up arrays for ``spec`` given bead positions (P, natm, 3) in Bohr.
+def build_system(spec: "water.BoxSpec", pos_bohr, rheal_A=1.0, hmat=None):
+    """Set-up arrays for ``spec`` given bead positions (P, natm, 3) in Bohr;
+    ``hmat`` (9, column-major, Bohr) replaces the cubic cell of edge spec.L.
 
     The bead positions fix the two configuration-dependent set-up values
     PINY derives at start-up: the bead spread that pads the Verlet cutoff
@@ -326,8 +327,11 @@ def build_system(spec: "water.BoxSpec", pos_bohr, rheal_A=1.0):
     S["charge"] = np.tile(np.array(model.charges, np.float64), nmol)
 
     L = spec.L
-    hmat = np.zeros(9)
-    hmat[0] = hmat[4] = hmat[8] = L / BOHR
+    if hmat is None:
+        hmat = np.zeros(9)
+        hmat[0] = hmat[4] = hmat[8] = L / BOHR
+    else:
+        hmat = np.array(hmat, np.float64)
     hi, vol = gethinv(hmat)
     S["hmat"] = hmat
     S["hmati"] = hi

@@ -186,3 +186,48 @@ def test_non_finite_positions_are_reported():
     force, e = box.energy_force(F["pos"], None, F["hmat"])
     assert np.isfinite(e["vintert"])
     box.close()
+
+
+def _oracle_case(oracle, spec, S, pos):
+    xmod = pos.mean(axis=0) if spec.nbeads > 1 else None
+    pi, pj = oracle.verlist(S, pos[0], xmod, S["hmat"], S["cutskin2"])
+    fref, eref = oracle.energy_force(S, pos, xmod, S["hmat"], pi, pj)
+    return xmod, pi, pj, fref, eref
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["triclinic", "beads64", "uncharged"])
+def test_more_systems_match_oracle(case, prec, oracle):
+    """A sheared (triclinic) cell: the site-list kernel, general minimum
+    image and general-cell PME; 64 beads; a system without charges (no
+    PME, no Ewald correction)."""
+    import dataclasses
+
+    from piny_b200 import system, water
+    from piny_b200.lib import DeviceBox
+    if case == "triclinic":
+        spec = dataclasses.replace(water.named_spec("spcfw_216_p4"), nbeads=2)
+        pos = water.build_positions(spec) / water.BOHR
+        L = spec.L / water.BOHR
+        h = np.array([L, 0.0, 0.0, 0.12 * L, L, 0.0, -0.07 * L, 0.05 * L, L])
+        S = system.build_system(spec, pos, hmat=h)
+    elif case == "beads64":
+        spec = water.BoxSpec(water.TIP4P_F, 64, water.density_box_edge(64), 64, 298.0, 8, grid=16, order=8)
+        pos = water.build_positions(spec) / water.BOHR
+        S = system.build_system(spec, pos)
+    else:
+        model = dataclasses.replace(water.SPC_FW, charges=[0.0, 0.0, 0.0])
+        spec = water.BoxSpec(model, 216, 18.64, 2, 300.0, 12, grid=32, order=6)
+        pos = water.build_positions(spec) / water.BOHR
+        S = system.build_system(spec, pos)
+    xmod, pi, pj, fref, eref = _oracle_case(oracle, spec, S, pos)
+    box = DeviceBox(S, spec.nbeads, prec)
+    n = box.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+    gi, gj = box.get_list()
+    assert n == len(pi) and pair_hash(gi, gj) == pair_hash(pi, pj)
+    f, e = box.energy_force(pos, xmod, S["hmat"])
+    assert rel_rms(f, fref) < TOL[prec]
+    scale = abs(eref["vvdw"]) + abs(eref["vcoul"]) + abs(eref["vrecip"]) + abs(eref["vself"]) + abs(eref["vecor"])
+    assert abs(e["vintert"] - eref["vintert"]) <= ETOL[prec] * max(scale, 1.0)
+    assert abs(e["vintrat"] - eref["vintrat"]) <= ETOL[prec] * max(1.0, abs(eref["vintrat"]))
+    box.close()
