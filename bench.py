@@ -609,6 +609,20 @@ def main():
             "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
             "algorithmic_bytes_per_launch": alg_bytes, "bytes_model": unit_note,
             "phase_ms": {names[i]: float(phase[i]) for i in range(4)}}
+    # the bound that applies to the pair kernel: FP32 issue, not HBM
+    alu = None
+    try:
+        from piny_b200.lib import fma_peak_gflops
+        npc = in_cutoff_pairs(box, S, pos[0], xmod)
+        flops = 40.0 * npc * P
+        peak32 = fma_peak_gflops(fp64=args.precision == "fp64")
+        ach = flops / (phase[1] * 1e-3) / 1e9
+        alu = {"bound": "fp32" if args.precision == "mixed" else "fp64", "kernel": "pair phase",
+               "achieved": ach, "peak": peak32, "unit": "GFLOP/s", "frac": ach / peak32, "peak_kind": "measured",
+               "flops_per_launch": flops, "in_cutoff_site_pairs": int(npc),
+               "flops_model": "40 flops per in-cutoff site pair and bead (bead-1 pair count x beads)"}
+    except Exception as exc:  # reported, not fatal
+        alu = {"error": str(exc)}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -629,6 +643,7 @@ def main():
                        "l2": "256 MiB buffer written between timed steps; per-step CUDA events on the launch stream",
                        "parallelism": "replica per GPU" if ws > 1 else "single GPU"},
             "roofline": roof,
+            "alu_roofline": alu,
             "cpu_baseline": cpu,
             "e2e": {"value": ws * P / (e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e},
@@ -643,6 +658,32 @@ def main():
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+def in_cutoff_pairs(box, S, pos1, xmod):
+    """Force-bearing site pairs of the list within their cutoff on bead 1
+    (minimum image through the mode-1 positions, as the kernels take it)."""
+    pi, pj = box.get_list()
+    q = S["charge"]
+    typ = S["atm_typ"]
+    ntyp = S["ntyp"]
+    a, b = np.minimum(typ[pi], typ[pj]) + 1, np.maximum(typ[pi], typ[pj]) + 1
+    pt = ((a - 1) * ((ntyp + 1) * 2 - a)) // 2 + b - a
+    u = S["inter_map"][pt]
+    nspl = S["nsplin"]
+    has_vdw = np.array([np.any(S["cdv0"][k * nspl:(k + 1) * nspl] != 0) for k in range(S["ninter_unique"])])
+    act = (q[pi] * q[pj] != 0) | has_vdw[u]
+    pi, pj, pt = pi[act], pj[act], pt[act]
+    h = np.asarray(S["hmat"]).reshape(3, 3, order="F")
+    hi = np.linalg.inv(h)
+    d = pos1[pi] - pos1[pj]
+    if xmod is not None:
+        dm = xmod[pi] - xmod[pj]
+        d -= (h @ np.round(hi @ dm.T)).T
+    else:
+        d -= (h @ np.round(hi @ d.T)).T
+    r = np.sqrt((d * d).sum(1))
+    return int(np.count_nonzero(r < S["cutoff"][pt]))
 
 
 def box_launches(S, P):

@@ -361,6 +361,11 @@ int pinyb200_grad(pinyb200_ctx *ctx, const double *d_pos, const double *d_xmod,
  * the context, concurrently with 1 and 3, so 1 + 2 + 3 may exceed 0. */
 int pinyb200_last_timing(pinyb200_ctx *ctx, float *ms, int n);
 
+/* FMA throughput of the current GPU in GFLOP/s (fp64 = 0: FP32, 1: FP64),
+ * best of `reps` timed launches of a register-only probe: the ALU peak the
+ * benchmark's roofline divides by.  No counterpart in PINY. */
+int pinyb200_fma_peak(int fp64, int reps, double *gflops);
+
 /* Last error text for this context (or the library if ctx is NULL). */
 const char *pinyb200_last_error(pinyb200_ctx *ctx);
 

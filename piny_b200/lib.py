@@ -73,7 +73,8 @@ EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb
            "pinyb200_last_error", "pinyb200_count_list_device", "pinyb200_check_list_device",
            "pinyb200_autotune", "pinyb200_get_tuning", "pinyb200_set_tuning", "pinyb200_batch_create",
            "pinyb200_batch_destroy", "pinyb200_batch_energy_force_device", "pinyb200_batch_last_ms",
-           "pinyb200_batch_last_error", "pinyb200_grad_prepare", "pinyb200_grad")
+           "pinyb200_batch_last_error", "pinyb200_grad_prepare", "pinyb200_grad",
+           "pinyb200_fma_peak")
 
 COUNT_MAX_ATOMS = 65536       # PINYB200_COUNT_MAX_ATOMS
 COUNT_MAX_PAIR_TYPES = 64     # PINYB200_COUNT_MAX_PAIR_TYPES
@@ -125,10 +126,21 @@ def load(build_if_missing: bool = True):
     L.pinyb200_batch_last_error.argtypes = [C.c_void_p]
     L.pinyb200_grad_prepare.argtypes = [C.c_void_p, _i, C.POINTER(PinyTangent)]
     L.pinyb200_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, C.c_void_p, _pd, _pd, C.c_void_p]
+    L.pinyb200_fma_peak.argtypes = [_i, _i, _pd]
     L.pinyb200_last_error.restype = C.c_char_p
     L.pinyb200_last_error.argtypes = [C.c_void_p]
     _LIB = L
     return L
+
+
+def fma_peak_gflops(fp64=False, reps=5):
+    """Measured FMA throughput of the current GPU (GFLOP/s)."""
+    L = load()
+    g = C.c_double()
+    rc = L.pinyb200_fma_peak(1 if fp64 else 0, int(reps), C.byref(g))
+    if rc != 0:
+        raise PinyError("pinyb200_fma_peak: %s %s" % (STATUS.get(rc, rc), L.pinyb200_last_error(None).decode()))
+    return g.value
 
 
 def _dp(a):
