@@ -366,6 +366,31 @@ int pinyb200_last_timing(pinyb200_ctx *ctx, float *ms, int n);
  * benchmark's roofline divides by.  No counterpart in PINY. */
 int pinyb200_fma_peak(int fp64, int reps, double *gflops);
 
+/* Ring-polymer transforms of PINY's PIMD integrators, in FP64, in place on
+ * the device array d_x[nbeads][natm][3] (the bead-major layout of
+ * pinyb200_energy_force_device), enqueued on `stream`.  No context needed.
+ *   kind  PINYB200_STAGING      staging (pi_md_typ 1),
+ *         PINYB200_NORMAL_MODES centroid normal modes (pi_md_typ 2);
+ *   what  PINYB200_TO_MODES       positions -> modes
+ *           (convert_pimd_mode_stag, transform_stg.c:92;
+ *            convert_pimd_mode_cent, transform_cnt.c:240),
+ *         PINYB200_TO_BEADS       modes -> positions
+ *           (convert_pimd_pos_stag, transform_stg.c:164;
+ *            convert_pimd_pos_cent, transform_cnt.c:321),
+ *         PINYB200_FORCE_TO_MODES bead forces -> mode forces
+ *           (convert_pimd_force_stag, transform_stg.c:31;
+ *            convert_pimd_force_cent, transform_cnt.c:415).
+ * Normal modes use PINY's packing: mode 1 = Re X_0, mode 2m = Re X_m,
+ * mode 2m+1 = Im X_m, mode P = Re X_{P/2}, X_k = (1/P) sum_j x_j e^{2 pi i jk/P}.
+ * Staging is bit-identical to PINY; normal modes agree to rounding.
+ * nbeads 1 is a no-op (PINY skips it); else 2, 4, ..., 64. */
+#define PINYB200_STAGING 1
+#define PINYB200_NORMAL_MODES 2
+#define PINYB200_TO_MODES 0
+#define PINYB200_TO_BEADS 1
+#define PINYB200_FORCE_TO_MODES 2
+int pinyb200_pimd_transform(int natm, int nbeads, int kind, int what, double *d_x, void *stream);
+
 /* Last error text for this context (or the library if ctx is NULL). */
 const char *pinyb200_last_error(pinyb200_ctx *ctx);
 

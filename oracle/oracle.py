@@ -71,6 +71,8 @@ class Oracle:
         L.orc_kvec_fill.argtypes = [_d, _pi, _pd, _pi, _pi, _pi]
         L.orc_pme_grid.argtypes = [_d, _d, _pd, _pi, _i, _pi]
         L.orc_pme_bweight.argtypes = [_i, _pi, _pi, _pi, _pi, _i, _pd]
+        L.orc_pimd_transform.restype = _i
+        L.orc_pimd_transform.argtypes = [_i, _i, _i, _i, _pd]
         L.orc_ecor_table.argtypes = [_i, _d, _d, _d, _pd, _pd, _pd, _pd, _pd]
         L.orc_gauss_legendre.argtypes = [_i, _pd, _pd]
         L.orc_bond_power.argtypes = [_d, _d, _d, _pd, _pd]
@@ -202,6 +204,17 @@ class Oracle:
                                     C.c_double(spread_ref), len(cut), cut.ctypes.data_as(_pd), C.byref(rmax),
                                     C.byref(sp), cs.ctypes.data_as(_pd))
         return bool(f), rmax.value, sp.value, cs
+
+    def pimd_transform(self, x, kind, what):
+        """PINY's ring-polymer transform (orc_pimd_transform) of x[P][natm][3]:
+        kind 1 staging / 2 normal modes; what 0 positions->modes,
+        1 modes->positions, 2 forces->mode forces.  Returns a new array."""
+        y = np.array(x, dtype=np.float64, order="C", copy=True)
+        P, natm = y.shape[0], y.shape[1]
+        rc = self.lib.orc_pimd_transform(natm, P, int(kind), int(what), y.ctypes.data_as(_pd))
+        if rc != 0:
+            raise ValueError("orc_pimd_transform: bad arguments")
+        return y
 
     def verlist(self, sysd, pos1, xmod, hmat, cutskin2):
         s = self.make_struct(sysd)

@@ -1072,3 +1072,100 @@ int orc_check_list(int natm, int nbeads, const double *pos, const double *x0,
         }
     return rm > skin2 ? 1 : 0;
 }
+
+/* --------------------------------------------------------------------------
+ * Ring-polymer transforms, one (atom, direction) row of P beads at a time.
+ * Staging: src/energy/pimd/transform_stg.c:31-85 (forces), :92-153 (modes),
+ * :164-222 (positions), with rat1[ip] = (ip-1)/ip, rat2[ip] = 1/ip from
+ * path_integral_init (transform_cnt.c:206-216); the loops and the grouping
+ * of each update are PINY's, so the results are bit-identical to it.
+ * Normal modes: transform_cnt.c:240-316 (modes: backward FFT, i.e.
+ * e^{+2 pi i jk/P}, then /P), :321-410 (positions: forward FFT of the
+ * Hermitian-completed modes), :415-489 (forces: backward FFT, x2 on the
+ * paired modes).  PINY packs mode 1 = Re X_0, mode 2m = Re X_m,
+ * mode 2m+1 = Im X_m (m = 1..P/2-1), mode P = Re X_{P/2}.  Here the DFTs are
+ * direct sums, so they agree with PINY's FFT to rounding only.
+ * ------------------------------------------------------------------------ */
+static void orc_stage_row(int P, int what, double *v /* 1-based, v[1..P] */)
+{
+    double rat1[65], rat2[65];
+    for (int ip = 2; ip <= P; ip++) {
+        rat1[ip] = ((double)(ip - 1)) / ((double)(ip));
+        rat2[ip] = 1.0 / ((double)(ip));
+    }
+    if (what == 0) {
+        for (int ip = 2; ip <= P - 1; ip++) {
+            double star = rat1[ip] * v[ip + 1] + rat2[ip] * v[1];
+            v[ip] -= star;
+        }
+        double star = rat1[P] * v[1] + rat2[P] * v[1];
+        v[P] -= star;
+    } else if (what == 1) {
+        v[P] += v[1];
+        for (int ip = P - 1; ip >= 2; ip--) {
+            double add = rat1[ip] * v[ip + 1] + v[1] * rat2[ip];
+            v[ip] += add;
+        }
+    } else {
+        for (int ip = 2; ip <= P; ip++) v[1] += v[ip];
+        for (int ip = 2; ip <= P - 1; ip++) v[ip + 1] += (rat1[ip] * v[ip]);
+    }
+}
+
+static void orc_mode_row(int P, int what, double *v /* 0-based, v[0..P-1] */)
+{
+    double out[64], cs[64], sn[64];
+    const int np2 = P / 2;
+    for (int m = 0; m < P; m++) {
+        double a = 2.0 * M_PI * (double)m / (double)P;
+        cs[m] = cos(a);
+        sn[m] = sin(a);
+    }
+    if (what == 0 || what == 2) {
+        for (int k = 0; k <= np2; k++) {
+            double re = 0.0, im = 0.0;
+            for (int j = 0; j < P; j++) {
+                int m = (j * k) % P;
+                re += v[j] * cs[m];
+                im += v[j] * sn[m];
+            }
+            if (what == 0) {
+                re /= P;
+                im /= P;
+            }
+            double f2 = what == 2 ? 2.0 : 1.0;
+            if (k == 0) out[0] = re;
+            else if (k == np2) out[P - 1] = re;
+            else {
+                out[2 * k - 1] = re * f2;
+                out[2 * k] = im * f2;
+            }
+        }
+    } else {
+        for (int j = 0; j < P; j++) {
+            double s = v[0] + ((j & 1) ? -v[P - 1] : v[P - 1]);
+            for (int k = 1; k < np2; k++) {
+                int m = (j * k) % P;
+                s += 2.0 * (v[2 * k - 1] * cs[m] + v[2 * k] * sn[m]);
+            }
+            out[j] = s;
+        }
+    }
+    for (int j = 0; j < P; j++) v[j] = out[j];
+}
+
+int orc_pimd_transform(int natm, int nbeads, int kind, int what, double *x)
+{
+    if (natm < 1 || nbeads < 1 || nbeads > 64 || (kind != 1 && kind != 2) || what < 0 || what > 2) return -1;
+    if (kind == 2 && (nbeads & (nbeads - 1))) return -1;
+    if (nbeads == 1) return 0;
+    const size_t stride = (size_t)natm * 3;
+    double row[65];
+    for (size_t t = 0; t < stride; t++) {
+        for (int b = 0; b < nbeads; b++) row[b + 1] = x[b * stride + t];
+        if (kind == 1) orc_stage_row(nbeads, what, row);
+        else orc_mode_row(nbeads, what, row + 1);
+        for (int b = 0; b < nbeads; b++) x[b * stride + t] = row[b + 1];
+    }
+    return 0;
+}

@@ -155,6 +155,11 @@ int orc_check_list(int natm, int nbeads, const double *pos, const double *x0,
                    const double *cutoff, double *rmax, double *spread_now,
                    double *cutskin2);
 
+/* Ring-polymer transforms, in place on x[P][natm][3] (bead-major).
+ * kind 1 staging (transform_stg.c), 2 normal modes (transform_cnt.c);
+ * what 0 positions -> modes, 1 modes -> positions, 2 forces -> mode forces. */
+int orc_pimd_transform(int natm, int nbeads, int kind, int what, double *x);
+
 void orc_energy_force(const orc_system *sys, int nbeads, const double *pos,
                       const double *xmod, const double *hmat,
                       long npairs, const int *pi, const int *pj,

@@ -14,6 +14,12 @@
  *   piny_ref recip <dir> <input>                      print bead-1 PME energy
  *   piny_ref time  <dir> <input> <reps> <nbeads>      time <reps> evaluations
  *                                                     of the first <nbeads>
+ *   piny_ref pimd  <typ> <in.bin> <out.bin>           PINY's ring-polymer
+ *                 transforms (typ 1 staging, 2 normal modes) on given beads:
+ *                 path_integral_init (transform_cnt.c:23), then
+ *                 convert_pimd_mode_*, convert_pimd_pos_* on the modes, and
+ *                 convert_pimd_force_* on given forces.  in.bin: int32 P,
+ *                 natm, then doubles mass[natm], x[P][natm][3], f[P][natm][3].
  *
  * The dump is a flat record file: for each record a 32-byte name, a one-byte
  * kind ('d' double, 'i' int32), 7 pad bytes, an int64 count, then the data.
@@ -324,8 +330,116 @@ static void dump_all(const char *path)
     fclose(g_out);
 }
 
+void path_integral_init(CLATOMS_INFO *, CLATOMS_POS *, CLATOMS_TRAN *, GHOST_ATOMS *, SIMOPTS *, ATOMMAPS *,
+                        COMMUNICATE *);
+void convert_pimd_mode_cent(CLATOMS_INFO *, CLATOMS_POS *, CLATOMS_TRAN *);
+void convert_pimd_pos_cent(CLATOMS_INFO *, CLATOMS_POS *, CLATOMS_TRAN *);
+void convert_pimd_force_cent(CLATOMS_INFO *, CLATOMS_POS *, CLATOMS_TRAN *);
+void convert_pimd_mode_stag(CLATOMS_INFO *, CLATOMS_POS *, CLATOMS_TRAN *);
+void convert_pimd_pos_stag(CLATOMS_INFO *, CLATOMS_POS *, CLATOMS_TRAN *);
+void convert_pimd_force_stag(CLATOMS_INFO *, CLATOMS_POS *, CLATOMS_TRAN *);
+
+/* Bead-major [P][natm][3] <-> PINY's per-bead 1-based x/y/z (or fx/fy/fz). */
+static void load_beads(CLATOMS_POS *cp, int P, int n, const double *a, int force)
+{
+    for (int b = 0; b < P; b++)
+        for (int i = 0; i < n; i++) {
+            double *x = force ? cp[b + 1].fx : cp[b + 1].x, *y = force ? cp[b + 1].fy : cp[b + 1].y,
+                   *z = force ? cp[b + 1].fz : cp[b + 1].z;
+            x[i + 1] = a[(b * n + i) * 3 + 0];
+            y[i + 1] = a[(b * n + i) * 3 + 1];
+            z[i + 1] = a[(b * n + i) * 3 + 2];
+        }
+}
+static void store_beads(CLATOMS_POS *cp, int P, int n, double *a, int force)
+{
+    for (int b = 0; b < P; b++)
+        for (int i = 0; i < n; i++) {
+            const double *x = force ? cp[b + 1].fx : cp[b + 1].x, *y = force ? cp[b + 1].fy : cp[b + 1].y,
+                         *z = force ? cp[b + 1].fz : cp[b + 1].z;
+            a[(b * n + i) * 3 + 0] = x[i + 1];
+            a[(b * n + i) * 3 + 1] = y[i + 1];
+            a[(b * n + i) * 3 + 2] = z[i + 1];
+        }
+}
+
+static int run_pimd(int typ, const char *inpath, const char *outpath)
+{
+    FILE *fi = fopen(inpath, "rb");
+    int hdr[2];
+    if (!fi || fread(hdr, sizeof(int), 2, fi) != 2) return 2;
+    const int P = hdr[0], n = hdr[1];
+    double *mass = malloc(sizeof(double) * n), *x = malloc(sizeof(double) * P * n * 3),
+           *f = malloc(sizeof(double) * P * n * 3);
+    if (fread(mass, sizeof(double), n, fi) != (size_t)n || fread(x, sizeof(double), (size_t)P * n * 3, fi) != (size_t)P * n * 3 ||
+        fread(f, sizeof(double), (size_t)P * n * 3, fi) != (size_t)P * n * 3)
+        return 2;
+    fclose(fi);
+
+    static CLATOMS_INFO info;
+    static CLATOMS_TRAN tran;
+    static GHOST_ATOMS ghost;
+    static SIMOPTS sim;
+    static ATOMMAPS maps;
+    static COMMUNICATE comm;
+    CLATOMS_POS *cp = calloc(P + 1, sizeof(CLATOMS_POS));
+    info.pi_beads = P;
+    info.pi_beads_proc = P;
+    info.pi_beads_proc_st = 1;
+    info.natm_tot = n;
+    info.myatm_start = 1;
+    info.myatm_end = n;
+    info.gamma_adb = 1.0;
+    info.pi_temperature = 300.0;
+    info.mass = calloc(n + 1, sizeof(double));
+    info.prekf = calloc(n + 1, sizeof(double));
+    for (int i = 0; i < n; i++) info.mass[i + 1] = mass[i];
+    for (int b = 1; b <= P; b++) {
+        cp[b].mass = calloc(n + 1, sizeof(double));
+        cp[b].x = calloc(n + 1, sizeof(double));
+        cp[b].y = calloc(n + 1, sizeof(double));
+        cp[b].z = calloc(n + 1, sizeof(double));
+        cp[b].fx = calloc(n + 1, sizeof(double));
+        cp[b].fy = calloc(n + 1, sizeof(double));
+        cp[b].fz = calloc(n + 1, sizeof(double));
+    }
+    sim.pi_md_typ = typ;
+    comm.np_beads = 1;
+    path_integral_init(&info, cp, &tran, &ghost, &sim, &maps, &comm);
+
+    g_out = fopen(outpath, "wb");
+    if (!g_out) return 2;
+    double *buf = malloc(sizeof(double) * P * n * 3);
+    load_beads(cp, P, n, x, 0);
+    if (typ == 2) convert_pimd_mode_cent(&info, cp, &tran);
+    else convert_pimd_mode_stag(&info, cp, &tran);
+    store_beads(cp, P, n, buf, 0);
+    put("modes", 'd', buf, (int64_t)P * n * 3);
+    if (typ == 2) convert_pimd_pos_cent(&info, cp, &tran);
+    else convert_pimd_pos_stag(&info, cp, &tran);
+    store_beads(cp, P, n, buf, 0);
+    put("back", 'd', buf, (int64_t)P * n * 3);
+    load_beads(cp, P, n, f, 1);
+    if (typ == 2) convert_pimd_force_cent(&info, cp, &tran);
+    else convert_pimd_force_stag(&info, cp, &tran);
+    store_beads(cp, P, n, buf, 1);
+    put("fmodes", 'd', buf, (int64_t)P * n * 3);
+    putd("path_eig", tran.path_eig, P);
+    for (int b = 0; b < P; b++)
+        for (int i = 0; i < n; i++) buf[b * n + i] = cp[b + 1].mass[i + 1];
+    put("bead_mass", 'd', buf, (int64_t)P * n);
+    putd("prekf", info.prekf, n);
+    if (typ == 1) {
+        putd("rat1", tran.rat1_stag + 1, P - 1);
+        putd("rat2", tran.rat2_stag + 1, P - 1);
+    }
+    fclose(g_out);
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
+    if (argc == 5 && strcmp(argv[1], "pimd") == 0) return run_pimd(atoi(argv[2]), argv[3], argv[4]);
     if (argc < 4) {
         fprintf(stderr, "usage: piny_ref dump|recip|time <dir> <input> [...]\n");
         return 2;

@@ -74,7 +74,10 @@ EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb
            "pinyb200_autotune", "pinyb200_get_tuning", "pinyb200_set_tuning", "pinyb200_batch_create",
            "pinyb200_batch_destroy", "pinyb200_batch_energy_force_device", "pinyb200_batch_last_ms",
            "pinyb200_batch_last_error", "pinyb200_grad_prepare", "pinyb200_grad",
-           "pinyb200_fma_peak")
+           "pinyb200_fma_peak", "pinyb200_pimd_transform")
+
+STAGING, NORMAL_MODES = 1, 2                      # PINYB200_STAGING / _NORMAL_MODES
+TO_MODES, TO_BEADS, FORCE_TO_MODES = 0, 1, 2      # PINYB200_TO_MODES / _TO_BEADS / _FORCE_TO_MODES
 
 COUNT_MAX_ATOMS = 65536       # PINYB200_COUNT_MAX_ATOMS
 COUNT_MAX_PAIR_TYPES = 64     # PINYB200_COUNT_MAX_PAIR_TYPES
@@ -127,6 +130,7 @@ def load(build_if_missing: bool = True):
     L.pinyb200_grad_prepare.argtypes = [C.c_void_p, _i, C.POINTER(PinyTangent)]
     L.pinyb200_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, C.c_void_p, _pd, _pd, C.c_void_p]
     L.pinyb200_fma_peak.argtypes = [_i, _i, _pd]
+    L.pinyb200_pimd_transform.argtypes = [_i, _i, _i, _i, C.c_void_p, C.c_void_p]
     L.pinyb200_last_error.restype = C.c_char_p
     L.pinyb200_last_error.argtypes = [C.c_void_p]
     _LIB = L
@@ -141,6 +145,19 @@ def fma_peak_gflops(fp64=False, reps=5):
     if rc != 0:
         raise PinyError("pinyb200_fma_peak: %s %s" % (STATUS.get(rc, rc), L.pinyb200_last_error(None).decode()))
     return g.value
+
+
+def pimd_transform(d_x, natm, nbeads, kind, what, stream=None):
+    """PINY's ring-polymer transform (staging or normal modes), in place on
+    the device array at address d_x, shaped [nbeads][natm][3] FP64:
+    what TO_MODES (positions -> modes), TO_BEADS (modes -> positions) or
+    FORCE_TO_MODES (bead forces -> mode forces).  Enqueued on `stream`
+    (a CUDA stream handle; None for the default stream)."""
+    L = load()
+    rc = L.pinyb200_pimd_transform(int(natm), int(nbeads), int(kind), int(what), C.c_void_p(d_x),
+                                   C.c_void_p(stream) if stream else None)
+    if rc != 0:
+        raise PinyError("pinyb200_pimd_transform: %s %s" % (STATUS.get(rc, rc), L.pinyb200_last_error(None).decode()))
 
 
 def _dp(a):

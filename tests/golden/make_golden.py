@@ -11,7 +11,13 @@ and stores, per configuration, a compressed .npz with
 * PINY's outputs (per-bead forces before and after the M-site
   redistribution, energy components, pressure tensor, the Verlet pair set).
 
+It also stores pimd_transforms.npz: PINY's own ring-polymer transforms
+(``piny_ref pimd``: path_integral_init, convert_pimd_mode/pos/force_* of
+transform_stg.c and transform_cnt.c) of seeded bead positions and forces,
+for staging and normal modes at several bead counts.
+
 Run in a container that has the PINY tree:  python tests/golden/make_golden.py
+(``--pimd-only`` regenerates just the transform fixture)
 The GPU tests only read the .npz files.
 """
 from __future__ import annotations
@@ -188,10 +194,50 @@ def golden_specs():
     ]
 
 
+PIMD_CASES = [(1, 2), (1, 4), (1, 6), (1, 8), (1, 32), (1, 64), (2, 2), (2, 4), (2, 8), (2, 16), (2, 32), (2, 64)]
+PIMD_NATM = 6
+
+
+def pimd_fixture(tmp):
+    """PINY's transforms of seeded ring polymers: per (kind, P) the inputs
+    x, f ([P][natm][3]) and PINY's modes, positions back from the modes,
+    mode forces, path eigenvalues and bead masses."""
+    rng = np.random.default_rng(7)
+    mass = np.array([29156.9, 1837.4, 1837.4, 29156.9, 1837.4, 1837.4])[:PIMD_NATM]
+    out = {"natm": PIMD_NATM, "mass": mass}
+    for kind, P in PIMD_CASES:
+        centre = rng.uniform(0.0, 20.0, size=(1, PIMD_NATM, 3))
+        x = centre + rng.normal(0.0, 0.3, size=(P, PIMD_NATM, 3))
+        f = rng.normal(0.0, 0.05, size=(P, PIMD_NATM, 3))
+        inp = os.path.join(tmp, "pimd_in.bin")
+        with open(inp, "wb") as fh:
+            fh.write(struct.pack("<ii", P, PIMD_NATM))
+            fh.write(mass.astype("<f8").tobytes())
+            fh.write(x.astype("<f8").tobytes())
+            fh.write(f.astype("<f8").tobytes())
+        res = os.path.join(tmp, "pimd_out.bin")
+        subprocess.run([PINY_REF, "pimd", str(kind), inp, res], check=True, capture_output=True)
+        D = read_dump(res)
+        tag = "k%d_p%d_" % (kind, P)
+        out[tag + "x"] = x
+        out[tag + "f"] = f
+        for k in ("modes", "back", "fmodes"):
+            out[tag + k] = D[k].reshape(P, PIMD_NATM, 3)
+        out[tag + "path_eig"] = D["path_eig"]
+        out[tag + "bead_mass"] = D["bead_mass"].reshape(P, PIMD_NATM)
+    path = os.path.join(HERE, "pimd_transforms.npz")
+    np.savez_compressed(path, **{k: np.asarray(v) for k, v in out.items()})
+    print("pimd_transforms", os.path.getsize(path), "bytes")
+
+
 def main():
     if not os.path.exists(PINY_REF):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     tmp = tempfile.mkdtemp(prefix="piny_golden_")
+    pimd_fixture(tmp)
+    if "--pimd-only" in sys.argv[1:]:
+        shutil.rmtree(tmp, ignore_errors=True)
+        return
     for name, spec, keep in golden_specs():
         pos = water.build_positions(spec)
         D = run_piny(spec, pos, tmp)
