@@ -391,6 +391,84 @@ int pinyb200_fma_peak(int fp64, int reps, double *gflops);
 #define PINYB200_FORCE_TO_MODES 2
 int pinyb200_pimd_transform(int natm, int nbeads, int kind, int what, double *d_x, void *stream);
 
+/*
+ * Path-integral MD around the force path, on the device, in FP64: PINY's
+ * NVT ring-polymer step (int_NVT_pimd, src/integrate/pimd/int_NVT_pimd.c:
+ * 142-217, with every RESPA count 1) as one call per step.
+ *
+ * A Nose-Hoover chain set is PINY's THERM_INFO (typedefs_class.h) for one
+ * set of beads: the class set thermostats bead 1 (with the atom masses),
+ * the bead set each of beads 2..P (with the bead masses; one chain state
+ * per bead).  Chains are 0-based; chain num_nhc is the null chain.
+ */
+typedef struct pinyb200_nhc_set {
+    int num_nhc;             /* chains (therm_info.num_nhc)                  */
+    int len_nhc;             /* links per chain, 1..8                        */
+    int nres_nhc;            /* RESPA steps of the chain operator            */
+    int nyosh_nhc;           /* Yoshida-Suzuki stages, 1..9                  */
+    const double *wdti;      /* [nyosh_nhc] stage weights x dti_nhc
+                                (therm_info.wdti, from set_yosh)             */
+    const int *inhc;         /* [3][natm] chain of each coordinate
+                                (inhc_x, inhc_y, inhc_z)                    */
+    const double *mass_nhc;  /* [len_nhc][num_nhc]                           */
+    const double *gkt;       /* [len_nhc][num_nhc]                           */
+} pinyb200_nhc_set;
+
+typedef struct pinyb200_pimd_setup {
+    int natm;                /* sites, ghosts included (as the force path)  */
+    int nbeads;
+    int kind;                /* PINYB200_STAGING or PINYB200_NORMAL_MODES    */
+    const double *mass;      /* [natm] clatoms_info.mass                     */
+    const double *bead_mass; /* [nbeads][natm] clatoms_pos[ip].mass          */
+    const double *prekf;     /* [natm] clatoms_info.prekf                    */
+    const double *path_eig;  /* [nbeads] clatoms_tran.path_eig (veig)        */
+    double wght_pimd;        /* clatoms_info.wght_pimd (1 for NVT)           */
+    double dt;               /* time step                                    */
+    double beta;             /* BOLTZ / pi_temperature                       */
+    int nfree_atoms;         /* natm - nghost - nfreeze (virial estimator)   */
+    pinyb200_nhc_set class_nhc;
+    pinyb200_nhc_set bead_nhc;
+} pinyb200_pimd_setup;
+
+typedef struct pinyb200_pimd_energies {
+    pinyb200_energies force; /* the force path's, pvten = its bead sum        */
+    double kin_harm;         /* sum of spring energies (stat_avg.kin_harm)    */
+    double akvirx;           /* virial kinetic estimator (0.5 x PINY's sum)   */
+    double pvten[9];         /* pvten / P with the centroid virial correction */
+    double pvten_tot[9];     /* pvten_tot / P, likewise                       */
+    double pvten_mode_tot[9];/* spring tensor (ptens.pvten_mode_tot)          */
+} pinyb200_pimd_energies;
+
+typedef struct pinyb200_pimd pinyb200_pimd;
+
+/* Set up a step for one box; chain positions and velocities start at zero. */
+int pinyb200_pimd_create(const pinyb200_pimd_setup *setup, pinyb200_pimd **out);
+int pinyb200_pimd_destroy(pinyb200_pimd *pm);
+
+/* Chain state, host arrays: set 0 (class) [len][num]; set 1 (bead)
+ * [nbeads-1][len][num] for beads 2..P (therm_class / therm_bead[ip]). */
+int pinyb200_pimd_set_nhc(pinyb200_pimd *pm, int set, const double *x_nhc, const double *v_nhc);
+int pinyb200_pimd_get_nhc(pinyb200_pimd *pm, int set, double *x_nhc, double *v_nhc);
+
+/* Mode forces of the bead positions d_x ([P][natm][3]): spring forces of
+ * the modes (mode_energy_control, pimd_estimators.c:31), the force path
+ * with the mode-1 image positions, and the post-processing of
+ * energy_control_pimd.c:113-218 (bead forces / P, centroid virial
+ * correction, forces to modes, springs added) into d_f.  Ghost positions in
+ * d_x are recomputed (get_ghost_pos).  Work goes to `stream` (NULL: the
+ * force context's own stream); the call blocks until it is done. */
+int pinyb200_pimd_forces(pinyb200_pimd *pm, pinyb200_ctx *ctx, double *d_x, double *d_f,
+                         const double *hmat, pinyb200_pimd_energies *e, void *stream);
+
+/* One NVT step: chains and half kick (int_0_to_dt2_nvt_pimd,
+ * int_0_to_dt2_pimd.c:34-190), positions to modes, drift, springs, modes
+ * to positions, pinyb200_pimd_forces, half kick and chains
+ * (int_dt2_to_dt_nvt_pimd, int_dt2_to_dt_pimd.c).  d_x: bead positions,
+ * d_v: mode velocities, d_f: mode forces of d_x on entry, of the new d_x
+ * on return.  Blocks until done. */
+int pinyb200_pimd_step(pinyb200_pimd *pm, pinyb200_ctx *ctx, double *d_x, double *d_v, double *d_f,
+                       const double *hmat, pinyb200_pimd_energies *e, void *stream);
+
 /* Last error text for this context (or the library if ctx is NULL). */
 const char *pinyb200_last_error(pinyb200_ctx *ctx);
 

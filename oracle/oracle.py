@@ -73,6 +73,11 @@ class Oracle:
         L.orc_pme_bweight.argtypes = [_i, _pi, _pi, _pi, _pi, _i, _pd]
         L.orc_pimd_transform.restype = _i
         L.orc_pimd_transform.argtypes = [_i, _i, _i, _i, _pd]
+        L.orc_nhc_apply.argtypes = [_i, _pi, _pd, _pd, _i, _i, _i, _i, _pd, _pd, _pd, _pd, _pd]
+        L.orc_pimd_springs.restype = _d
+        L.orc_pimd_springs.argtypes = [_i, _i, _pd, _pd, _pd, _d, _pd, _pd]
+        L.orc_pimd_force_post.restype = _d
+        L.orc_pimd_force_post.argtypes = [_i, _i, _i, _pd, _pd, _pd, _pd, _i, _d, _pd, _pd]
         L.orc_ecor_table.argtypes = [_i, _d, _d, _d, _pd, _pd, _pd, _pd, _pd]
         L.orc_gauss_legendre.argtypes = [_i, _pd, _pd]
         L.orc_bond_power.argtypes = [_d, _d, _d, _pd, _pd]
@@ -259,3 +264,114 @@ class Oracle:
         out = {n: getattr(e, n) for n, _ in OrcEnergies._fields_ if n != "pvten"}
         out["pvten"] = np.array(e.pvten[:])
         return force, out
+
+
+# -- path-integral MD bookkeeping (pimd_oracle.c) and its composition -------
+
+def _c(a, dt=np.float64):
+    return np.ascontiguousarray(a, dt)
+
+
+def nhc_apply(orc, v, m, chains, x_nhc, v_nhc):
+    """apply_NHC_par on one bead's velocities v [natm][3] (copies returned)."""
+    v, m = _c(v).copy(), _c(m)
+    x_nhc, v_nhc = _c(x_nhc).copy(), _c(v_nhc).copy()
+    inhc = _c(chains["inhc"], np.int32)
+    w = _c(chains["wdti"])
+    orc.lib.orc_nhc_apply(v.shape[0], inhc.ctypes.data_as(_pi), m.ctypes.data_as(_pd), v.ctypes.data_as(_pd),
+                          int(chains["num_nhc"]), int(chains["len_nhc"]), int(chains["nres_nhc"]), len(w),
+                          w.ctypes.data_as(_pd), _c(chains["mass_nhc"]).ctypes.data_as(_pd),
+                          _c(chains["gkt"]).ctypes.data_as(_pd), x_nhc.ctypes.data_as(_pd), v_nhc.ctypes.data_as(_pd))
+    return v, x_nhc, v_nhc
+
+
+def pimd_springs(orc, u, prekf, veig, wght):
+    """mode_energy_control: (fm, kin_harm, pvten_mode_tot)."""
+    u = _c(u)
+    fm = np.zeros_like(u)
+    pv = np.zeros(9)
+    prekf, veig = _c(prekf), _c(veig)
+    ake = orc.lib.orc_pimd_springs(u.shape[1], u.shape[0], u.ctypes.data_as(_pd), prekf.ctypes.data_as(_pd),
+                                   veig.ctypes.data_as(_pd), float(wght), fm.ctypes.data_as(_pd), pv.ctypes.data_as(_pd))
+    return fm, ake, pv
+
+
+def pimd_force_post(orc, kind, f, x, xmod, fm, nfree, beta, pvten, pvten_tot):
+    """energy_control_pimd's post-processing: (mode forces, akvirx, pvten,
+    pvten_tot)."""
+    f = _c(f).copy()
+    x, xmod, fm = _c(x), _c(xmod), _c(fm)
+    pv, pvt = _c(pvten).copy(), _c(pvten_tot).copy()
+    akv = orc.lib.orc_pimd_force_post(f.shape[1], f.shape[0], int(kind), f.ctypes.data_as(_pd), x.ctypes.data_as(_pd),
+                                      xmod.ctypes.data_as(_pd), fm.ctypes.data_as(_pd), int(nfree), float(beta),
+                                      pv.ctypes.data_as(_pd), pvt.ctypes.data_as(_pd))
+    return f, akv, pv, pvt
+
+
+def ghost_positions(sysd, x):
+    """get_ghost_pos on every bead of x [P][natm][3] (a copy), in PINY's
+    operation order: sum over components of coef * position."""
+    x = _c(x).copy()
+    ng = int(sysd.get("nghost", 0))
+    if ng == 0:
+        return x
+    nc = int(sysd["ghost_ncomp"])
+    comp = np.asarray(sysd["ghost_comp"]).reshape(ng, nc)
+    coef = np.asarray(sysd["ghost_coef"], np.float64).reshape(ng, nc)
+    acc = np.zeros((x.shape[0], ng, 3))
+    for c in range(nc):
+        ok = comp[:, c] >= 0
+        term = coef[:, c][None, :, None] * x[:, np.where(ok, comp[:, c], 0), :]
+        acc = np.where(ok[None, :, None], acc + term, acc)
+    x[:, np.asarray(sysd["ghost_atom"]), :] = acc
+    return x
+
+
+def pimd_forces(orc, sysd, setup, x, pi, pj):
+    """pinyb200_pimd_forces restated: (x with ghosts, mode forces, energies)."""
+    P, kind = int(setup["nbeads"]), int(setup["kind"])
+    x = ghost_positions(sysd, x)
+    u = orc.pimd_transform(x, kind, 0) if P > 1 else x.copy()
+    return (x,) + _forces_core(orc, sysd, setup, x, u, u[0].copy(), pi, pj)
+
+
+def _forces_core(orc, sysd, setup, x, u, xmod, pi, pj):
+    P, kind = int(setup["nbeads"]), int(setup["kind"])
+    fm, ake, pvm = pimd_springs(orc, u, setup["prekf"], setup["path_eig"], setup.get("wght_pimd", 1.0))
+    f, e = orc.energy_force(sysd, x, xmod if P > 1 else None, sysd["hmat"], pi, pj, distribute_ghosts=True)
+    fmode, akv, pv, pvt = pimd_force_post(orc, kind, f, x, xmod, fm, setup["nfree_atoms"], setup["beta"],
+                                          e["pvten"], e["pvten"])
+    e = dict(e)
+    e.update(kin_harm=ake, akvirx=akv if P > 1 else 0.0, pvten_corr=pv, pvten_tot_corr=pvt, pvten_mode_tot=pvm)
+    return fmode, e
+
+
+def pimd_apply_chains(orc, setup, v, state):
+    """Class chains on bead 1 (atom masses), bead chains on beads 2..P."""
+    v = _c(v).copy()
+    cls, bead = setup.get("class_nhc"), setup.get("bead_nhc")
+    if cls is not None and int(cls["num_nhc"]):
+        v[0], state["cx"], state["cv"] = nhc_apply(orc, v[0], setup["mass"], cls, state["cx"], state["cv"])
+    if bead is not None and int(bead["num_nhc"]):
+        for b in range(1, v.shape[0]):
+            v[b], state["bx"][b - 1], state["bv"][b - 1] = nhc_apply(orc, v[b], setup["bead_mass"][b], bead,
+                                                                     state["bx"][b - 1], state["bv"][b - 1])
+    return v
+
+
+def pimd_step(orc, sysd, setup, x, v, f, state, pi, pj):
+    """pinyb200_pimd_step restated (int_NVT_pimd with RESPA counts 1):
+    returns new (x, v, f, energies); `state` (chain x/v) is updated."""
+    P, kind, dt = int(setup["nbeads"]), int(setup["kind"]), float(setup["dt"])
+    bm = np.asarray(setup["bead_mass"], np.float64)[:, :, None]
+    v = pimd_apply_chains(orc, setup, v, state)
+    v = v + (f * (dt / 2.0)) / bm
+    u = orc.pimd_transform(x, kind, 0) if P > 1 else _c(x).copy()
+    u = u + v * dt
+    xmod = u[0].copy()
+    xn = orc.pimd_transform(u, kind, 1) if P > 1 else u.copy()
+    xn = ghost_positions(sysd, xn)
+    fn, e = _forces_core(orc, sysd, setup, xn, u, xmod, pi, pj)
+    v = v + (fn * (dt / 2.0)) / bm
+    v = pimd_apply_chains(orc, setup, v, state)
+    return xn, v, fn, e

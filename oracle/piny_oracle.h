@@ -160,6 +160,15 @@ int orc_check_list(int natm, int nbeads, const double *pos, const double *x0,
  * what 0 positions -> modes, 1 modes -> positions, 2 forces -> mode forces. */
 int orc_pimd_transform(int natm, int nbeads, int kind, int what, double *x);
 
+/* PIMD bookkeeping around the force call (pimd_oracle.c). */
+void orc_nhc_apply(int natm, const int *inhc, const double *m, double *v, int num_nhc, int len_nhc,
+                   int nres_nhc, int nyosh, const double *wdti, const double *mass_nhc, const double *gkt,
+                   double *x_nhc, double *v_nhc);
+double orc_pimd_springs(int natm, int P, const double *u, const double *prekf, const double *veig, double wght,
+                        double *fm, double *pvten_mode_tot);
+double orc_pimd_force_post(int natm, int P, int kind, double *f, const double *x, const double *xmod,
+                           const double *fm, int nfree_atoms, double beta, double *pvten, double *pvten_tot);
+
 void orc_energy_force(const orc_system *sys, int nbeads, const double *pos,
                       const double *xmod, const double *hmat,
                       long npairs, const int *pi, const int *pj,

@@ -20,6 +20,19 @@
  *                 convert_pimd_mode_*, convert_pimd_pos_* on the modes, and
  *                 convert_pimd_force_* on given forces.  in.bin: int32 P,
  *                 natm, then doubles mass[natm], x[P][natm][3], f[P][natm][3].
+ *   piny_ref nhc <in.bin> <out.bin>   apply_NHC_par (int_NVT.c:144) once on
+ *                 given velocities and chains, weights from set_yosh
+ *                 (int_utils.c:244).  in.bin: int32 natm, num_nhc, len_nhc,
+ *                 nres_nhc, nyosh, inhc[3][natm] (1-based, num_nhc+1 null);
+ *                 doubles dti, mass[natm], v[natm][3], mass_nhc, gkt, x_nhc,
+ *                 v_nhc (each [len_nhc][num_nhc]).
+ *   piny_ref springs <in.bin> <out.bin>  mode_energy_control
+ *                 (pimd_estimators.c:31) on modes u, then pimd_pvten_forc_corr
+ *                 (pimd_estimators.c:223) on positions x with forces f (also
+ *                 the virial forces).  in.bin: int32 P, natm, nfree_atoms
+ *                 unused; doubles pi_temperature, wght, prekf[natm],
+ *                 veig[P], u, x, f ([P][natm][3]), xmod[natm][3], pvten[9],
+ *                 pvten_tot[9].
  *
  * The dump is a flat record file: for each record a 32-byte name, a one-byte
  * kind ('d' double, 'i' int32), 7 pad bytes, an int64 count, then the data.
@@ -437,8 +450,218 @@ static int run_pimd(int typ, const char *inpath, const char *outpath)
     return 0;
 }
 
+void apply_NHC_par(CLATOMS_INFO *, CLATOMS_POS *, THERM_INFO *, THERM_POS *, INT_SCR *, int, CLASS_COMM_FORC_PKG *);
+void set_yosh(int, double, double *, double *, double *, double *, double *);
+void mode_energy_control(CLASS *, GENERAL_DATA *);
+void pimd_pvten_forc_corr(CLASS *, GENERAL_DATA *, double *);
+
+static int read_all(FILE *f, void *p, size_t sz, size_t n) { return fread(p, sz, n, f) == n; }
+
+/* 1-based [len][num] table from a 0-based row-major block */
+static double **chain_table(int len, int num, const double *src)
+{
+    double **t = calloc(len + 1, sizeof(double *));
+    for (int c = 1; c <= len; c++) {
+        t[c] = calloc(num + 2, sizeof(double));
+        if (src)
+            for (int k = 1; k <= num; k++) t[c][k] = src[(size_t)(c - 1) * num + (k - 1)];
+    }
+    return t;
+}
+static void chain_dump(const char *name, double **t, int len, int num)
+{
+    double *buf = malloc(sizeof(double) * len * num);
+    for (int c = 1; c <= len; c++)
+        for (int k = 1; k <= num; k++) buf[(size_t)(c - 1) * num + (k - 1)] = t[c][k];
+    put(name, 'd', buf, (int64_t)len * num);
+    free(buf);
+}
+
+static int run_nhc(const char *inpath, const char *outpath)
+{
+    FILE *fi = fopen(inpath, "rb");
+    int h[5];
+    if (!fi || !read_all(fi, h, sizeof(int), 5)) return 2;
+    const int n = h[0], num = h[1], len = h[2];
+    int *inhc = malloc(sizeof(int) * 3 * n);
+    double dti;
+    double *m = malloc(sizeof(double) * n), *v = malloc(sizeof(double) * 3 * n);
+    double *blk[4];
+    if (!read_all(fi, inhc, sizeof(int), 3 * (size_t)n) || !read_all(fi, &dti, sizeof(double), 1) ||
+        !read_all(fi, m, sizeof(double), n) || !read_all(fi, v, sizeof(double), 3 * (size_t)n))
+        return 2;
+    for (int k = 0; k < 4; k++) {
+        blk[k] = malloc(sizeof(double) * len * num);
+        if (!read_all(fi, blk[k], sizeof(double), (size_t)len * num)) return 2;
+    }
+    fclose(fi);
+
+    static CLATOMS_INFO info;
+    static CLATOMS_POS pos;
+    static THERM_INFO ti;
+    static THERM_POS tp;
+    static INT_SCR scr;
+    static CLASS_COMM_FORC_PKG pkg;
+    info.natm_tot = n;
+    info.myatm_start = 1;
+    info.myatm_end = n;
+    info.mass = calloc(n + 1, sizeof(double));
+    pos.mass = calloc(n + 1, sizeof(double));
+    pos.vx = calloc(n + 1, sizeof(double));
+    pos.vy = calloc(n + 1, sizeof(double));
+    pos.vz = calloc(n + 1, sizeof(double));
+    for (int i = 0; i < n; i++) {
+        info.mass[i + 1] = pos.mass[i + 1] = m[i];
+        pos.vx[i + 1] = v[3 * i];
+        pos.vy[i + 1] = v[3 * i + 1];
+        pos.vz[i + 1] = v[3 * i + 2];
+    }
+    ti.num_nhc = num;
+    ti.len_nhc = len;
+    ti.nres_nhc = h[3];
+    ti.nyosh_nhc = h[4];
+    ti.mytherm_start = 1;
+    ti.mytherm_end = num;
+    ti.inhc_x = calloc(n + 1, sizeof(int));
+    ti.inhc_y = calloc(n + 1, sizeof(int));
+    ti.inhc_z = calloc(n + 1, sizeof(int));
+    for (int i = 0; i < n; i++) {
+        ti.inhc_x[i + 1] = inhc[i];
+        ti.inhc_y[i + 1] = inhc[n + i];
+        ti.inhc_z[i + 1] = inhc[2 * n + i];
+    }
+    ti.wdti = calloc(10, sizeof(double));
+    ti.wdti2 = calloc(10, sizeof(double));
+    ti.wdti4 = calloc(10, sizeof(double));
+    ti.wdti8 = calloc(10, sizeof(double));
+    ti.wdti16 = calloc(10, sizeof(double));
+    set_yosh(ti.nyosh_nhc, dti, ti.wdti, ti.wdti2, ti.wdti4, ti.wdti8, ti.wdti16);
+    ti.mass_nhc = chain_table(len, num, blk[0]);
+    ti.gkt = chain_table(len, num, blk[1]);
+    tp.x_nhc = chain_table(len, num, blk[2]);
+    tp.v_nhc = chain_table(len, num, blk[3]);
+    tp.f_nhc = chain_table(len, num, NULL);
+    scr.atm_kin = calloc(num + 2, sizeof(double));
+    scr.sc = calloc(num + 2, sizeof(double));
+    scr.sc_temp = calloc(num + 2, sizeof(double));
+    pkg.num_proc = 1;
+    apply_NHC_par(&info, &pos, &ti, &tp, &scr, 2, &pkg);
+
+    g_out = fopen(outpath, "wb");
+    if (!g_out) return 2;
+    for (int i = 0; i < n; i++) {
+        v[3 * i] = pos.vx[i + 1];
+        v[3 * i + 1] = pos.vy[i + 1];
+        v[3 * i + 2] = pos.vz[i + 1];
+    }
+    put("v", 'd', v, 3 * (int64_t)n);
+    chain_dump("x_nhc", tp.x_nhc, len, num);
+    chain_dump("v_nhc", tp.v_nhc, len, num);
+    putd("wdti", ti.wdti, ti.nyosh_nhc);
+    fclose(g_out);
+    return 0;
+}
+
+static int run_springs(const char *inpath, const char *outpath)
+{
+    FILE *fi = fopen(inpath, "rb");
+    int h[3];
+    double sc2[2];
+    if (!fi || !read_all(fi, h, sizeof(int), 3) || !read_all(fi, sc2, sizeof(double), 2)) return 2;
+    const int P = h[0], n = h[1];
+    const size_t nb = (size_t)P * n * 3;
+    double *prekf = malloc(sizeof(double) * n), *veig = malloc(sizeof(double) * P);
+    double *u = malloc(sizeof(double) * nb), *x = malloc(sizeof(double) * nb), *f = malloc(sizeof(double) * nb);
+    double *xm = malloc(sizeof(double) * 3 * n), pv[9], pvt[9];
+    if (!read_all(fi, prekf, sizeof(double), n) || !read_all(fi, veig, sizeof(double), P) ||
+        !read_all(fi, u, sizeof(double), nb) || !read_all(fi, x, sizeof(double), nb) ||
+        !read_all(fi, f, sizeof(double), nb) || !read_all(fi, xm, sizeof(double), 3 * (size_t)n) ||
+        !read_all(fi, pv, sizeof(double), 9) || !read_all(fi, pvt, sizeof(double), 9))
+        return 2;
+    fclose(fi);
+
+    static CLASS cl;
+    static GENERAL_DATA gd;
+    CLATOMS_POS *cp = calloc(P + 1, sizeof(CLATOMS_POS));
+    cl.clatoms_pos = cp;
+    cl.clatoms_info.pi_beads = P;
+    cl.clatoms_info.pi_beads_proc = P;
+    cl.clatoms_info.pi_beads_proc_st = 1;
+    cl.clatoms_info.natm_tot = n;
+    cl.clatoms_info.myatm_start = 1;
+    cl.clatoms_info.myatm_end = n;
+    cl.clatoms_info.pi_temperature = sc2[0];
+    cl.clatoms_info.wght_pimd = sc2[1];
+    cl.clatoms_info.prekf = calloc(n + 1, sizeof(double));
+    cl.clatoms_info.xmod = calloc(n + 1, sizeof(double));
+    cl.clatoms_info.ymod = calloc(n + 1, sizeof(double));
+    cl.clatoms_info.zmod = calloc(n + 1, sizeof(double));
+    for (int i = 0; i < n; i++) {
+        cl.clatoms_info.prekf[i + 1] = prekf[i];
+        cl.clatoms_info.xmod[i + 1] = xm[3 * i];
+        cl.clatoms_info.ymod[i + 1] = xm[3 * i + 1];
+        cl.clatoms_info.zmod[i + 1] = xm[3 * i + 2];
+    }
+    cl.clatoms_tran.path_eig = calloc(P + 1, sizeof(double));
+    for (int b = 0; b < P; b++) cl.clatoms_tran.path_eig[b + 1] = veig[b];
+    cl.communicate.np_forc = 1;
+    cl.energy_ctrl.iget_full_inter = 1;
+    cl.energy_ctrl.iget_full_intra = 1;
+    cl.ewd_scr.x = calloc(n + 1, sizeof(double));
+    cl.ewd_scr.y = calloc(n + 1, sizeof(double));
+    cl.ewd_scr.z = calloc(n + 1, sizeof(double));
+    for (int b = 1; b <= P; b++) {
+        cp[b].x = calloc(n + 1, sizeof(double));
+        cp[b].y = calloc(n + 1, sizeof(double));
+        cp[b].z = calloc(n + 1, sizeof(double));
+        cp[b].fx = calloc(n + 1, sizeof(double));
+        cp[b].fy = calloc(n + 1, sizeof(double));
+        cp[b].fz = calloc(n + 1, sizeof(double));
+        cp[b].fxt = cp[b].fx;
+        cp[b].fyt = cp[b].fy;
+        cp[b].fzt = cp[b].fz;
+        cp[b].fxm = calloc(n + 1, sizeof(double));
+        cp[b].fym = calloc(n + 1, sizeof(double));
+        cp[b].fzm = calloc(n + 1, sizeof(double));
+    }
+    gd.ptens.pvten = calloc(10, sizeof(double));
+    gd.ptens.pvten_tot = calloc(10, sizeof(double));
+    gd.ptens.pvten_mode = calloc(10, sizeof(double));
+    gd.ptens.pvten_mode_tot = calloc(10, sizeof(double));
+    for (int k = 0; k < 9; k++) {
+        gd.ptens.pvten[k + 1] = pv[k];
+        gd.ptens.pvten_tot[k + 1] = pvt[k];
+    }
+    load_beads(cp, P, n, u, 0);
+    mode_energy_control(&cl, &gd);
+    load_beads(cp, P, n, x, 0);
+    load_beads(cp, P, n, f, 1);
+    double akvirx = 0.0;
+    pimd_pvten_forc_corr(&cl, &gd, &akvirx);
+
+    g_out = fopen(outpath, "wb");
+    if (!g_out) return 2;
+    double *buf = malloc(sizeof(double) * nb);
+    for (int b = 0; b < P; b++)
+        for (int i = 0; i < n; i++) {
+            buf[((size_t)b * n + i) * 3 + 0] = cp[b + 1].fxm[i + 1];
+            buf[((size_t)b * n + i) * 3 + 1] = cp[b + 1].fym[i + 1];
+            buf[((size_t)b * n + i) * 3 + 2] = cp[b + 1].fzm[i + 1];
+        }
+    put("fm", 'd', buf, (int64_t)nb);
+    put1d("kin_harm", gd.stat_avg.kin_harm);
+    putd("pvten_mode_tot", gd.ptens.pvten_mode_tot, 9);
+    putd("pvten", gd.ptens.pvten, 9);
+    putd("pvten_tot", gd.ptens.pvten_tot, 9);
+    put1d("akvirx", akvirx);
+    fclose(g_out);
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
+    if (argc == 4 && strcmp(argv[1], "nhc") == 0) return run_nhc(argv[2], argv[3]);
+    if (argc == 4 && strcmp(argv[1], "springs") == 0) return run_springs(argv[2], argv[3]);
     if (argc == 5 && strcmp(argv[1], "pimd") == 0) return run_pimd(atoi(argv[2]), argv[3], argv[4]);
     if (argc < 4) {
         fprintf(stderr, "usage: piny_ref dump|recip|time <dir> <input> [...]\n");

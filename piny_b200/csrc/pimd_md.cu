@@ -1,0 +1,578 @@
+// Path-integral MD bookkeeping around the force call, on the device, FP64:
+// PINY's NVT ring-polymer step (int_NVT_pimd with every RESPA count 1).
+//
+// Per step (src/integrate/pimd/int_NVT_pimd.c:142-217):
+//   chains, half kick            int_0_to_dt2_nvt_pimd (int_0_to_dt2_pimd.c:34-190)
+//   positions -> modes, drift    control_pimd_trans_mode, x += v dt
+//   springs on the modes         mode_energy_control (pimd_estimators.c:31-110)
+//   mode 1 -> xmod, modes -> positions, ghost positions
+//                                control_pimd_trans_pos (control_pimd_trans.c:146-250)
+//   force path, post-processing  energy_control_pimd.c:113-218: forces / P,
+//                                centroid virial correction (pimd_pvten_forc_corr,
+//                                pimd_estimators.c:223-305), forces -> modes,
+//                                spring forces added
+//   half kick, chains            int_dt2_to_dt_nvt_pimd (int_dt2_to_dt_pimd.c)
+// The chain operator is apply_NHC_par (src/integrate/md/int_NVT.c:144-353):
+// one thread per chain runs the RESPA x Yoshida-Suzuki loop; the kinetic
+// energy of each chain is summed with FP64 atomics and the velocities are
+// scaled afterwards.  Layouts: bead arrays [P][natm][3]; chain state
+// [beads of the set][len_nhc][num_nhc].
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int kMaxLen = 8;   // links per chain
+constexpr int kMaxYosh = 9;  // Yoshida-Suzuki stages
+
+// accumulator slots (doubles)
+enum Acc {
+    A_KIN = 0,     // spring energy
+    A_PVM = 1,     // spring tensor xx yy zz xy xz yz (6)
+    A_VIR = 7,     // sum of d . f (virial estimator)
+    A_PVC = 8,     // sum of d (x) f, 9 components row-major
+    A_N = 17
+};
+
+struct NhcDev {
+    int num = 0, len = 0, nres = 0, nyosh = 0, nb = 0;
+    double w[kMaxYosh] = {0};
+    int *inhc = nullptr;
+    double *mass = nullptr, *gkt = nullptr;  // [len][num]
+    double *x = nullptr, *v = nullptr;       // [nb][len][num]
+    double *kin = nullptr, *sc = nullptr;    // [nb][num + 1]
+};
+
+struct ChainArgs {
+    int num, len, nres, nyosh, nb;
+    double w[kMaxYosh];
+    const double *mass, *gkt;
+    double *x, *v, *kin, *sc;
+};
+
+__global__ void nhc_kin_kernel(const double *__restrict__ v, int nb, int natm, const double *__restrict__ m,
+                               size_t m_stride, const int *__restrict__ inhc, double *__restrict__ kin, int num)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n3 = (long long)natm * 3;
+    if (t >= n3 * nb) return;
+    const int b = (int)(t / n3);
+    const int r = (int)(t - (long long)b * n3);
+    const int i = r / 3, d = r - 3 * (r / 3);
+    const double vv = v[t];
+    const double e = __dmul_rn(__dmul_rn(m[(size_t)b * m_stride + i], vv), vv);
+    atomicAdd(&kin[(size_t)b * (num + 1) + inhc[d * natm + i]], e);
+}
+
+__global__ void nhc_chain_kernel(ChainArgs a)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)a.nb * a.num) return;
+    const int b = (int)(t / a.num), k = (int)(t - (long long)b * a.num);
+    const int num = a.num, L = a.len - 1;
+    double *x = a.x + (size_t)b * a.len * num + k;
+    double *v = a.v + (size_t)b * a.len * num + k;
+    double vn[kMaxLen], f[kMaxLen], ms[kMaxLen], gk[kMaxLen];
+    for (int c = 0; c <= L; c++) {
+        vn[c] = v[(size_t)c * num];
+        ms[c] = a.mass[(size_t)c * num + k];
+        gk[c] = a.gkt[(size_t)c * num + k];
+    }
+    double kin = a.kin[(size_t)b * (num + 1) + k], sc = 1.0;
+    f[0] = (kin - gk[0]) / ms[0];
+    for (int c = 0; c < L; c++) f[c + 1] = (ms[c] * vn[c] * vn[c] - gk[c + 1]) / ms[c + 1];
+    double xs[kMaxLen];
+    for (int c = 0; c <= L; c++) xs[c] = x[(size_t)c * num];
+    for (int r = 0; r < a.nres; r++)
+        for (int y = 0; y < a.nyosh; y++) {
+            const double w2 = a.w[y] / 2.0, w4 = a.w[y] / 4.0, w8 = a.w[y] / 8.0;
+            vn[L] += f[L] * w4;
+            for (int c = L - 1; c >= 0; c--) {
+                const double aa = exp(-w8 * vn[c + 1]);
+                vn[c] = vn[c] * aa * aa + w4 * f[c] * aa;
+            }
+            const double aa = exp(-w2 * vn[0]);
+            sc *= aa;
+            kin *= aa * aa;
+            for (int c = 0; c <= L; c++) xs[c] += vn[c] * w2;
+            f[0] = (kin - gk[0]) / ms[0];
+            for (int c = 0; c < L; c++) {
+                const double ab = exp(-w8 * vn[c + 1]);
+                vn[c] = vn[c] * ab * ab + w4 * f[c] * ab;
+                f[c + 1] = (ms[c] * vn[c] * vn[c] - gk[c + 1]) / ms[c + 1];
+            }
+            vn[L] += f[L] * w4;
+        }
+    for (int c = 0; c <= L; c++) {
+        x[(size_t)c * num] = xs[c];
+        v[(size_t)c * num] = vn[c];
+    }
+    a.sc[(size_t)b * (num + 1) + k] = sc;
+    if (k == 0) a.sc[(size_t)b * (num + 1) + num] = 1.0;  // null chain
+}
+
+__global__ void nhc_scale_kernel(double *__restrict__ v, int nb, int natm, const int *__restrict__ inhc,
+                                 const double *__restrict__ sc, int num)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n3 = (long long)natm * 3;
+    if (t >= n3 * nb) return;
+    const int b = (int)(t / n3);
+    const int r = (int)(t - (long long)b * n3);
+    const int i = r / 3, d = r - 3 * (r / 3);
+    v[t] *= sc[(size_t)b * (num + 1) + inhc[d * natm + i]];
+}
+
+// v += f dt2 / m_bead
+__global__ void kick_kernel(double *__restrict__ v, const double *__restrict__ f, const double *__restrict__ bm,
+                            long long n, double dt2)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const long long bi = t / 3;  // b * natm + i
+    v[t] = __dadd_rn(v[t], __ddiv_rn(__dmul_rn(f[t], dt2), bm[bi]));
+}
+
+// x += v dt
+__global__ void drift_kernel(double *__restrict__ x, const double *__restrict__ v, long long n, double dt)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    x[t] = __dadd_rn(x[t], __dmul_rn(v[t], dt));
+}
+
+__global__ void add_kernel(double *__restrict__ f, const double *__restrict__ g, long long n)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    f[t] = __dadd_rn(f[t], g[t]);
+}
+
+// Block sum of NV values per thread into acc[0..NV) with FP64 atomics.
+template <int NV>
+__device__ __forceinline__ void block_accumulate(double (&val)[NV], double *acc)
+{
+    __shared__ double red[NV][8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+        double s = val[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) red[q][wid] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[threadIdx.x][w];
+        atomicAdd(acc + threadIdx.x, s);
+    }
+}
+
+// Spring forces on the modes and their energy and tensor (mode_energy_control).
+__global__ void __launch_bounds__(256) springs_kernel(const double *__restrict__ u, const double *__restrict__ prekf,
+                                                      const double *__restrict__ veig, double wght, int natm, int P,
+                                                      double *__restrict__ fm, double *__restrict__ acc)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double val[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (t < (long long)natm * P) {
+        const int b = (int)(t / natm), i = (int)(t - (long long)b * natm);
+        const double *p = u + 3 * t;
+        const double fk = __dmul_rn(prekf[i], veig[b]);
+        const double x = p[0], y = p[1], z = p[2];
+        val[0] = __dmul_rn(fk, __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+        const double g = -2.0 * fk;
+        const double gx = __dmul_rn(g, x), gy = __dmul_rn(g, y), gz = __dmul_rn(g, z);
+        val[1] = __dmul_rn(x, gx);
+        val[2] = __dmul_rn(y, gy);
+        val[3] = __dmul_rn(z, gz);
+        val[4] = __dmul_rn(x, gy);
+        val[5] = __dmul_rn(x, gz);
+        val[6] = __dmul_rn(y, gz);
+        double *q = fm + 3 * t;
+        q[0] = __dmul_rn(gx, wght);
+        q[1] = __dmul_rn(gy, wght);
+        q[2] = __dmul_rn(gz, wght);
+    }
+    block_accumulate<7>(val, acc + A_KIN);
+}
+
+// Bead forces / P and the centroid virial sums (d = x - xmod).
+__global__ void __launch_bounds__(256) post_kernel(double *__restrict__ f, const double *__restrict__ x,
+                                                   const double *__restrict__ xmod, int natm, int P, int correct,
+                                                   double *__restrict__ acc)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double val[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (t < (long long)natm * P) {
+        const int i = (int)(t % natm);
+        double *g = f + 3 * t;
+        const double dP = (double)P;
+        const double g0 = __ddiv_rn(g[0], dP), g1 = __ddiv_rn(g[1], dP), g2 = __ddiv_rn(g[2], dP);
+        g[0] = g0;
+        g[1] = g1;
+        g[2] = g2;
+        if (correct) {
+            const double *p = x + 3 * t;
+            const double d0 = __dsub_rn(p[0], xmod[3 * i]), d1 = __dsub_rn(p[1], xmod[3 * i + 1]),
+                         d2 = __dsub_rn(p[2], xmod[3 * i + 2]);
+            val[0] = __dadd_rn(__dadd_rn(__dmul_rn(d0, g0), __dmul_rn(d1, g1)), __dmul_rn(d2, g2));
+            val[1] = __dmul_rn(d0, g0);
+            val[2] = __dmul_rn(d0, g1);
+            val[3] = __dmul_rn(d0, g2);
+            val[4] = __dmul_rn(d1, g0);
+            val[5] = __dmul_rn(d1, g1);
+            val[6] = __dmul_rn(d1, g2);
+            val[7] = __dmul_rn(d2, g0);
+            val[8] = __dmul_rn(d2, g1);
+            val[9] = __dmul_rn(d2, g2);
+        }
+    }
+    block_accumulate<10>(val, acc + A_VIR);
+}
+
+// Ghost positions from their components (get_ghost_pos) in the [P][natm][3]
+// layout, with the force path's operation order.
+__global__ void ghost_pos_aos_kernel(double *__restrict__ x, int natm, int P, int nghost, int ncomp,
+                                     const int *__restrict__ gatom, const int *__restrict__ gcomp,
+                                     const double *__restrict__ gcoef)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nghost * P) return;
+    const int b = (int)(t / nghost), g = (int)(t - (long long)b * nghost);
+    double *xb = x + (size_t)b * natm * 3;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        double v = 0.0;
+        for (int c = 0; c < ncomp; c++) {
+            const int at = gcomp[g * ncomp + c];
+            if (at < 0) continue;
+            v = __dadd_rn(v, __dmul_rn(gcoef[g * ncomp + c], xb[3 * (size_t)at + d]));
+        }
+        xb[3 * (size_t)gatom[g] + d] = v;
+    }
+}
+
+inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+}  // namespace
+
+struct pinyb200_pimd {
+    int device = 0;
+    int natm = 0, P = 1, kind = PINYB200_STAGING;
+    double wght = 1.0, dt = 0.0, beta = 1.0;
+    int nfree = 0;
+    double *d_mass = nullptr, *d_bmass = nullptr, *d_prekf = nullptr, *d_veig = nullptr;
+    double *d_fm = nullptr, *d_u = nullptr, *d_xmod = nullptr, *d_acc = nullptr;
+    double *h_acc = nullptr;
+    NhcDev set[2];  // 0: class (bead 1), 1: bead (beads 2..P)
+    std::string err;
+};
+
+namespace {
+
+int pimd_fail(pinyb200_pimd *pm, int code, const std::string &msg)
+{
+    if (pm) pm->err = msg;
+    return pinyb200::record_error(nullptr, code, msg);
+}
+
+#define PCK(call)                                                                                     \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) return pimd_fail(pm, PINYB200_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+void free_set(NhcDev &s)
+{
+    cudaFree(s.inhc);
+    cudaFree(s.mass);
+    cudaFree(s.gkt);
+    cudaFree(s.x);
+    cudaFree(s.v);
+    cudaFree(s.kin);
+    cudaFree(s.sc);
+    s = NhcDev();
+}
+
+int upload_set(pinyb200_pimd *pm, NhcDev &s, const pinyb200_nhc_set &h, int nb)
+{
+    s.nb = nb;
+    if (nb == 0 || h.num_nhc == 0) {
+        s.num = 0;
+        return PINYB200_OK;
+    }
+    if (h.num_nhc < 0 || h.len_nhc < 1 || h.len_nhc > kMaxLen || h.nres_nhc < 1 || h.nyosh_nhc < 1 ||
+        h.nyosh_nhc > kMaxYosh || !h.wdti || !h.inhc || !h.mass_nhc || !h.gkt)
+        return pimd_fail(pm, PINYB200_ERR_ARG, "pimd: chain set needs num>=0, len 1..8, nres>=1, nyosh 1..9 and its arrays");
+    for (int k = 0; k < 3 * pm->natm; k++)
+        if (h.inhc[k] < 0 || h.inhc[k] > h.num_nhc) return pimd_fail(pm, PINYB200_ERR_ARG, "pimd: chain index out of range");
+    s.num = h.num_nhc;
+    s.len = h.len_nhc;
+    s.nres = h.nres_nhc;
+    s.nyosh = h.nyosh_nhc;
+    for (int y = 0; y < s.nyosh; y++) s.w[y] = h.wdti[y];
+    const size_t tab = (size_t)s.len * s.num, st = tab * nb;
+    PCK(cudaMalloc(&s.inhc, sizeof(int) * 3 * pm->natm));
+    PCK(cudaMalloc(&s.mass, sizeof(double) * tab));
+    PCK(cudaMalloc(&s.gkt, sizeof(double) * tab));
+    PCK(cudaMalloc(&s.x, sizeof(double) * st));
+    PCK(cudaMalloc(&s.v, sizeof(double) * st));
+    PCK(cudaMalloc(&s.kin, sizeof(double) * (size_t)nb * (s.num + 1)));
+    PCK(cudaMalloc(&s.sc, sizeof(double) * (size_t)nb * (s.num + 1)));
+    PCK(cudaMemcpy(s.inhc, h.inhc, sizeof(int) * 3 * pm->natm, cudaMemcpyHostToDevice));
+    PCK(cudaMemcpy(s.mass, h.mass_nhc, sizeof(double) * tab, cudaMemcpyHostToDevice));
+    PCK(cudaMemcpy(s.gkt, h.gkt, sizeof(double) * tab, cudaMemcpyHostToDevice));
+    PCK(cudaMemset(s.x, 0, sizeof(double) * st));
+    PCK(cudaMemset(s.v, 0, sizeof(double) * st));
+    return PINYB200_OK;
+}
+
+// apply_NHC_par on every bead of one set: bead0 is the set's first bead in
+// the velocity array; m is the per-bead mass row (stride 0 for atom masses).
+int apply_nhc(pinyb200_pimd *pm, NhcDev &s, double *d_v, int bead0, const double *m, size_t m_stride,
+              cudaStream_t st)
+{
+    if (s.num == 0 || s.nb == 0) return PINYB200_OK;
+    const long long n = (long long)pm->natm * 3 * s.nb;
+    double *v = d_v + (size_t)bead0 * pm->natm * 3;
+    PCK(cudaMemsetAsync(s.kin, 0, sizeof(double) * (size_t)s.nb * (s.num + 1), st));
+    nhc_kin_kernel<<<blocks_for(n, 256), 256, 0, st>>>(v, s.nb, pm->natm, m, m_stride, s.inhc, s.kin, s.num);
+    ChainArgs a;
+    a.num = s.num;
+    a.len = s.len;
+    a.nres = s.nres;
+    a.nyosh = s.nyosh;
+    a.nb = s.nb;
+    for (int y = 0; y < kMaxYosh; y++) a.w[y] = s.w[y];
+    a.mass = s.mass;
+    a.gkt = s.gkt;
+    a.x = s.x;
+    a.v = s.v;
+    a.kin = s.kin;
+    a.sc = s.sc;
+    nhc_chain_kernel<<<blocks_for((long long)s.nb * s.num, 128), 128, 0, st>>>(a);
+    nhc_scale_kernel<<<blocks_for(n, 256), 256, 0, st>>>(v, s.nb, pm->natm, s.inhc, s.sc, s.num);
+    PCK(cudaGetLastError());
+    return PINYB200_OK;
+}
+
+int apply_all_nhc(pinyb200_pimd *pm, double *d_v, cudaStream_t st)
+{
+    int rc = apply_nhc(pm, pm->set[0], d_v, 0, pm->d_mass, 0, st);
+    if (rc) return rc;
+    return apply_nhc(pm, pm->set[1], d_v, 1, pm->d_bmass + pm->natm, (size_t)pm->natm, st);
+}
+
+int ghost_positions(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, cudaStream_t st)
+{
+    const pinyb200::DeviceSystem &s = c->sys;
+    if (s.nghost == 0) return PINYB200_OK;
+    ghost_pos_aos_kernel<<<blocks_for((long long)s.nghost * pm->P, 256), 256, 0, st>>>(
+        d_x, pm->natm, pm->P, s.nghost, s.ghost_ncomp, s.ghost_atom, s.ghost_comp, s.ghost_coef);
+    PCK(cudaGetLastError());
+    return PINYB200_OK;
+}
+
+// Force path and post-processing; springs already in d_fm and acc.
+int forces_core(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, const double *d_xmod, double *d_f,
+                const double *hmat, pinyb200_pimd_energies *e, cudaStream_t st)
+{
+    pinyb200_energies fe;
+    int rc = pinyb200_energy_force_device(c, d_x, pm->P > 1 ? d_xmod : nullptr, hmat, PINYB200_DISTRIB_GHOSTS, d_f,
+                                          &fe, st);
+    if (rc) return rc;
+    const long long nb = (long long)pm->natm * pm->P, n = nb * 3;
+    post_kernel<<<blocks_for(nb, 256), 256, 0, st>>>(d_f, d_x, d_xmod, pm->natm, pm->P, pm->P > 1, pm->d_acc);
+    PCK(cudaGetLastError());
+    if (pm->P > 1) {
+        rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_FORCE_TO_MODES, d_f, st);
+        if (rc) return rc;
+    }
+    add_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_f, pm->d_fm, n);
+    PCK(cudaGetLastError());
+    PCK(cudaMemcpyAsync(pm->h_acc, pm->d_acc, sizeof(double) * A_N, cudaMemcpyDeviceToHost, st));
+    PCK(cudaStreamSynchronize(st));
+    if (e) {
+        const double *a = pm->h_acc;
+        e->force = fe;
+        e->kin_harm = a[A_KIN];
+        const double P = (double)pm->P;
+        const double akv = 3.0 * (double)pm->nfree / pm->beta;
+        e->akvirx = pm->P > 1 ? 0.5 * (akv - a[A_VIR]) : 0.0;  // PINY corrects only with beads
+        for (int k = 0; k < 9; k++) {
+            const double base = fe.pvten[k] / P;
+            e->pvten[k] = base - a[A_PVC + k];
+            e->pvten_tot[k] = base - a[A_PVC + k];
+        }
+        const double *m = a + A_PVM;  // xx yy zz xy xz yz
+        const double pm9[9] = {m[0], m[3], m[4], m[3], m[1], m[5], m[4], m[5], m[2]};
+        std::memcpy(e->pvten_mode_tot, pm9, sizeof pm9);
+    }
+    return PINYB200_OK;
+}
+
+int springs(pinyb200_pimd *pm, const double *d_u, cudaStream_t st)
+{
+    const long long nb = (long long)pm->natm * pm->P;
+    springs_kernel<<<blocks_for(nb, 256), 256, 0, st>>>(d_u, pm->d_prekf, pm->d_veig, pm->wght, pm->natm, pm->P,
+                                                        pm->d_fm, pm->d_acc);
+    PCK(cudaGetLastError());
+    return PINYB200_OK;
+}
+
+int check_ctx(pinyb200_pimd *pm, pinyb200_ctx *c)
+{
+    if (!pm || !c) return pimd_fail(pm, PINYB200_ERR_ARG, "pimd: null handle");
+    if (c->sys.natm != pm->natm || c->P != pm->P)
+        return pimd_fail(pm, PINYB200_ERR_ARG, "pimd: force context has other sites or beads");
+    return PINYB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pinyb200_pimd_create(const pinyb200_pimd_setup *s, pinyb200_pimd **out)
+{
+    pinyb200_pimd *pm = nullptr;
+    if (!s || !out || s->natm < 1 || s->nbeads < 1 || !s->mass || !s->bead_mass || !s->prekf || !s->path_eig ||
+        !(s->kind == PINYB200_STAGING || s->kind == PINYB200_NORMAL_MODES) || !(s->beta > 0.0))
+        return pimd_fail(nullptr, PINYB200_ERR_ARG, "pimd_create: bad setup");
+    if (s->nbeads > 64 || (s->nbeads & (s->nbeads - 1)))
+        return pimd_fail(nullptr, PINYB200_ERR_UNSUPPORTED, "pimd_create: beads 1..64, powers of 2");
+    *out = nullptr;
+    pm = new pinyb200_pimd();
+    cudaGetDevice(&pm->device);
+    pm->natm = s->natm;
+    pm->P = s->nbeads;
+    pm->kind = s->kind;
+    pm->wght = s->wght_pimd;
+    pm->dt = s->dt;
+    pm->beta = s->beta;
+    pm->nfree = s->nfree_atoms;
+    const size_t na = (size_t)s->natm, nb = na * s->nbeads;
+    auto cleanup = [&](int rc) {
+        pinyb200_pimd_destroy(pm);
+        return rc;
+    };
+#define CCK(call)                                                                                          \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) return cleanup(pimd_fail(nullptr, PINYB200_ERR_CUDA, cudaGetErrorString(e_))); \
+    } while (0)
+    CCK(cudaMalloc(&pm->d_mass, sizeof(double) * na));
+    CCK(cudaMalloc(&pm->d_bmass, sizeof(double) * nb));
+    CCK(cudaMalloc(&pm->d_prekf, sizeof(double) * na));
+    CCK(cudaMalloc(&pm->d_veig, sizeof(double) * s->nbeads));
+    CCK(cudaMalloc(&pm->d_fm, sizeof(double) * nb * 3));
+    CCK(cudaMalloc(&pm->d_u, sizeof(double) * nb * 3));
+    CCK(cudaMalloc(&pm->d_xmod, sizeof(double) * na * 3));
+    CCK(cudaMalloc(&pm->d_acc, sizeof(double) * A_N));
+    CCK(cudaMallocHost(&pm->h_acc, sizeof(double) * A_N));
+    CCK(cudaMemcpy(pm->d_mass, s->mass, sizeof(double) * na, cudaMemcpyHostToDevice));
+    CCK(cudaMemcpy(pm->d_bmass, s->bead_mass, sizeof(double) * nb, cudaMemcpyHostToDevice));
+    CCK(cudaMemcpy(pm->d_prekf, s->prekf, sizeof(double) * na, cudaMemcpyHostToDevice));
+    CCK(cudaMemcpy(pm->d_veig, s->path_eig, sizeof(double) * s->nbeads, cudaMemcpyHostToDevice));
+#undef CCK
+    int rc = upload_set(pm, pm->set[0], s->class_nhc, 1);
+    if (!rc) rc = upload_set(pm, pm->set[1], s->bead_nhc, s->nbeads - 1);
+    if (rc) return cleanup(rc);
+    *out = pm;
+    return PINYB200_OK;
+}
+
+int pinyb200_pimd_destroy(pinyb200_pimd *pm)
+{
+    if (!pm) return PINYB200_OK;
+    cudaFree(pm->d_mass);
+    cudaFree(pm->d_bmass);
+    cudaFree(pm->d_prekf);
+    cudaFree(pm->d_veig);
+    cudaFree(pm->d_fm);
+    cudaFree(pm->d_u);
+    cudaFree(pm->d_xmod);
+    cudaFree(pm->d_acc);
+    cudaFreeHost(pm->h_acc);
+    free_set(pm->set[0]);
+    free_set(pm->set[1]);
+    delete pm;
+    return PINYB200_OK;
+}
+
+int pinyb200_pimd_set_nhc(pinyb200_pimd *pm, int set, const double *x_nhc, const double *v_nhc)
+{
+    if (!pm || set < 0 || set > 1 || !x_nhc || !v_nhc) return pimd_fail(pm, PINYB200_ERR_ARG, "pimd_set_nhc: bad arguments");
+    NhcDev &s = pm->set[set];
+    if (s.num == 0) return PINYB200_OK;
+    const size_t n = (size_t)s.nb * s.len * s.num;
+    PCK(cudaMemcpy(s.x, x_nhc, sizeof(double) * n, cudaMemcpyHostToDevice));
+    PCK(cudaMemcpy(s.v, v_nhc, sizeof(double) * n, cudaMemcpyHostToDevice));
+    return PINYB200_OK;
+}
+
+int pinyb200_pimd_get_nhc(pinyb200_pimd *pm, int set, double *x_nhc, double *v_nhc)
+{
+    if (!pm || set < 0 || set > 1 || !x_nhc || !v_nhc) return pimd_fail(pm, PINYB200_ERR_ARG, "pimd_get_nhc: bad arguments");
+    NhcDev &s = pm->set[set];
+    if (s.num == 0) return PINYB200_OK;
+    const size_t n = (size_t)s.nb * s.len * s.num;
+    PCK(cudaMemcpy(x_nhc, s.x, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    PCK(cudaMemcpy(v_nhc, s.v, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    return PINYB200_OK;
+}
+
+int pinyb200_pimd_forces(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double *d_f, const double *hmat,
+                         pinyb200_pimd_energies *e, void *stream)
+{
+    int rc = check_ctx(pm, c);
+    if (rc) return rc;
+    if (!d_x || !d_f || !hmat) return pimd_fail(pm, PINYB200_ERR_ARG, "pimd_forces: null pointer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;  // NULL: the force context's stream
+    const size_t nbytes = sizeof(double) * (size_t)pm->natm * pm->P * 3;
+    if ((rc = ghost_positions(pm, c, d_x, st))) return rc;
+    PCK(cudaMemcpyAsync(pm->d_u, d_x, nbytes, cudaMemcpyDeviceToDevice, st));
+    if (pm->P > 1 && (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_MODES, pm->d_u, st)))
+        return rc;
+    PCK(cudaMemsetAsync(pm->d_acc, 0, sizeof(double) * A_N, st));
+    if ((rc = springs(pm, pm->d_u, st))) return rc;
+    return forces_core(pm, c, d_x, pm->d_u, d_f, hmat, e, st);
+}
+
+int pinyb200_pimd_step(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double *d_v, double *d_f, const double *hmat,
+                       pinyb200_pimd_energies *e, void *stream)
+{
+    int rc = check_ctx(pm, c);
+    if (rc) return rc;
+    if (!d_x || !d_v || !d_f || !hmat) return pimd_fail(pm, PINYB200_ERR_ARG, "pimd_step: null pointer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;  // NULL: the force context's stream
+    const long long n = (long long)pm->natm * pm->P * 3;
+    const double dt2 = pm->dt / 2.0;
+    // t = 0 -> dt/2: chains, half kick
+    if ((rc = apply_all_nhc(pm, d_v, st))) return rc;
+    kick_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_v, d_f, pm->d_bmass, n, dt2);
+    PCK(cudaGetLastError());
+    // positions -> modes, drift, springs, modes -> positions
+    if (pm->P > 1 && (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_MODES, d_x, st))) return rc;
+    drift_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_x, d_v, n, pm->dt);
+    PCK(cudaGetLastError());
+    PCK(cudaMemsetAsync(pm->d_acc, 0, sizeof(double) * A_N, st));
+    if ((rc = springs(pm, d_x, st))) return rc;
+    PCK(cudaMemcpyAsync(pm->d_xmod, d_x, sizeof(double) * (size_t)pm->natm * 3, cudaMemcpyDeviceToDevice, st));
+    if (pm->P > 1 && (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_BEADS, d_x, st))) return rc;
+    if ((rc = ghost_positions(pm, c, d_x, st))) return rc;
+    // forces of the new positions, as mode forces
+    if ((rc = forces_core(pm, c, d_x, pm->d_xmod, d_f, hmat, e, st))) return rc;
+    // dt/2 -> dt: half kick, chains
+    kick_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_v, d_f, pm->d_bmass, n, dt2);
+    PCK(cudaGetLastError());
+    if ((rc = apply_all_nhc(pm, d_v, st))) return rc;
+    PCK(cudaStreamSynchronize(st));
+    return PINYB200_OK;
+}
+
+}  // extern "C"

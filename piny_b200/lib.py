@@ -59,6 +59,25 @@ class PinyEnergies(C.Structure):
     _fields_ = [(n, _d) for n in ENERGY_NAMES] + [("pvten", _d * 9)]
 
 
+class PinyNhcSet(C.Structure):
+    """pinyb200_nhc_set: one Nose-Hoover chain set (PINY THERM_INFO)."""
+    _fields_ = [("num_nhc", _i), ("len_nhc", _i), ("nres_nhc", _i), ("nyosh_nhc", _i), ("wdti", _pd), ("inhc", _pi),
+                ("mass_nhc", _pd), ("gkt", _pd)]
+
+
+class PinyPimdSetup(C.Structure):
+    """pinyb200_pimd_setup."""
+    _fields_ = [("natm", _i), ("nbeads", _i), ("kind", _i), ("mass", _pd), ("bead_mass", _pd), ("prekf", _pd),
+                ("path_eig", _pd), ("wght_pimd", _d), ("dt", _d), ("beta", _d), ("nfree_atoms", _i),
+                ("class_nhc", PinyNhcSet), ("bead_nhc", PinyNhcSet)]
+
+
+class PinyPimdEnergies(C.Structure):
+    """pinyb200_pimd_energies."""
+    _fields_ = [("force", PinyEnergies), ("kin_harm", _d), ("akvirx", _d), ("pvten", _d * 9), ("pvten_tot", _d * 9),
+                ("pvten_mode_tot", _d * 9)]
+
+
 class PinyTangent(C.Structure):
     """pinyb200_tangent: derivative of the set-up data along one parameter."""
     _fields_ = [("dcharge", _pd), ("dcv0", _pd), ("dcdv0", _pd), ("dghost_coef", _pd), ("dbond_eq", _pd),
@@ -74,7 +93,8 @@ EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb
            "pinyb200_autotune", "pinyb200_get_tuning", "pinyb200_set_tuning", "pinyb200_batch_create",
            "pinyb200_batch_destroy", "pinyb200_batch_energy_force_device", "pinyb200_batch_last_ms",
            "pinyb200_batch_last_error", "pinyb200_grad_prepare", "pinyb200_grad",
-           "pinyb200_fma_peak", "pinyb200_pimd_transform")
+           "pinyb200_fma_peak", "pinyb200_pimd_transform", "pinyb200_pimd_create", "pinyb200_pimd_destroy",
+           "pinyb200_pimd_set_nhc", "pinyb200_pimd_get_nhc", "pinyb200_pimd_forces", "pinyb200_pimd_step")
 
 STAGING, NORMAL_MODES = 1, 2                      # PINYB200_STAGING / _NORMAL_MODES
 TO_MODES, TO_BEADS, FORCE_TO_MODES = 0, 1, 2      # PINYB200_TO_MODES / _TO_BEADS / _FORCE_TO_MODES
@@ -131,6 +151,14 @@ def load(build_if_missing: bool = True):
     L.pinyb200_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, C.c_void_p, _pd, _pd, C.c_void_p]
     L.pinyb200_fma_peak.argtypes = [_i, _i, _pd]
     L.pinyb200_pimd_transform.argtypes = [_i, _i, _i, _i, C.c_void_p, C.c_void_p]
+    L.pinyb200_pimd_create.argtypes = [C.POINTER(PinyPimdSetup), C.POINTER(C.c_void_p)]
+    L.pinyb200_pimd_destroy.argtypes = [C.c_void_p]
+    L.pinyb200_pimd_set_nhc.argtypes = [C.c_void_p, _i, _pd, _pd]
+    L.pinyb200_pimd_get_nhc.argtypes = [C.c_void_p, _i, _pd, _pd]
+    L.pinyb200_pimd_forces.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _pd,
+                                       C.POINTER(PinyPimdEnergies), C.c_void_p]
+    L.pinyb200_pimd_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _pd,
+                                     C.POINTER(PinyPimdEnergies), C.c_void_p]
     L.pinyb200_last_error.restype = C.c_char_p
     L.pinyb200_last_error.argtypes = [C.c_void_p]
     _LIB = L
@@ -393,6 +421,100 @@ class DeviceBatch:
     def close(self):
         if getattr(self, "h", None):
             self.L.pinyb200_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _pimd_energies(e):
+    out = {k: getattr(e.force, k) for k in ENERGY_NAMES}
+    out["force_pvten"] = np.array(e.force.pvten[:])
+    out["kin_harm"] = e.kin_harm
+    out["akvirx"] = e.akvirx
+    for k in ("pvten", "pvten_tot", "pvten_mode_tot"):
+        out[k] = np.array(getattr(e, k)[:])
+    return out
+
+
+class DevicePimd:
+    """PINY's NVT ring-polymer step on the device (pinyb200_pimd_*), driving
+    the force path of a DeviceBox.  `setup` holds the numpy arrays of
+    pinyb200_pimd_setup (see piny_b200.pimd.nvt_setup)."""
+
+    def __init__(self, setup: dict):
+        self.L = load()
+        self._keep = []
+        self.natm, self.P = int(setup["natm"]), int(setup["nbeads"])
+
+        def dp(a, dt=np.float64):
+            a = np.ascontiguousarray(a, dt)
+            self._keep.append(a)
+            return a.ctypes.data_as(_pd if dt == np.float64 else _pi)
+
+        def nhc(c):
+            if c is None or int(c["num_nhc"]) == 0:
+                return PinyNhcSet(0, 0, 0, 0, None, None, None, None)
+            return PinyNhcSet(int(c["num_nhc"]), int(c["len_nhc"]), int(c["nres_nhc"]), len(c["wdti"]),
+                              dp(c["wdti"]), dp(c["inhc"], np.int32), dp(c["mass_nhc"]), dp(c["gkt"]))
+
+        self.sets = (setup.get("class_nhc"), setup.get("bead_nhc"))
+        st = PinyPimdSetup(self.natm, self.P, int(setup["kind"]), dp(setup["mass"]), dp(setup["bead_mass"]),
+                           dp(setup["prekf"]), dp(setup["path_eig"]), float(setup.get("wght_pimd", 1.0)),
+                           float(setup["dt"]), float(setup["beta"]), int(setup["nfree_atoms"]),
+                           nhc(self.sets[0]), nhc(self.sets[1]))
+        h = C.c_void_p()
+        self._check(self.L.pinyb200_pimd_create(C.byref(st), C.byref(h)), "pinyb200_pimd_create")
+        self.h = h
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise PinyError("%s: %s %s" % (what, STATUS.get(rc, rc), self.L.pinyb200_last_error(None).decode()))
+
+    def _shape(self, s):
+        c = self.sets[s]
+        if c is None or int(c["num_nhc"]) == 0:
+            return None
+        nb = 1 if s == 0 else self.P - 1
+        return (nb, int(c["len_nhc"]), int(c["num_nhc"])) if s == 1 else (int(c["len_nhc"]), int(c["num_nhc"]))
+
+    def set_nhc(self, s, x_nhc, v_nhc):
+        if self._shape(s) is None:
+            return
+        x = np.ascontiguousarray(x_nhc, np.float64).reshape(self._shape(s))
+        v = np.ascontiguousarray(v_nhc, np.float64).reshape(self._shape(s))
+        self._check(self.L.pinyb200_pimd_set_nhc(self.h, s, _dp(x), _dp(v)), "pinyb200_pimd_set_nhc")
+
+    def get_nhc(self, s):
+        shp = self._shape(s)
+        if shp is None:
+            return None, None
+        x, v = np.zeros(shp), np.zeros(shp)
+        self._check(self.L.pinyb200_pimd_get_nhc(self.h, s, _dp(x), _dp(v)), "pinyb200_pimd_get_nhc")
+        return x, v
+
+    def forces(self, box, d_x, d_f, hmat, stream=None):
+        hm = np.ascontiguousarray(hmat, np.float64)
+        e = PinyPimdEnergies()
+        self._check(self.L.pinyb200_pimd_forces(self.h, box.h, C.c_void_p(d_x), C.c_void_p(d_f), _dp(hm),
+                                                C.byref(e), C.c_void_p(stream) if stream else None),
+                    "pinyb200_pimd_forces")
+        return _pimd_energies(e)
+
+    def step(self, box, d_x, d_v, d_f, hmat, stream=None):
+        hm = np.ascontiguousarray(hmat, np.float64)
+        e = PinyPimdEnergies()
+        self._check(self.L.pinyb200_pimd_step(self.h, box.h, C.c_void_p(d_x), C.c_void_p(d_v), C.c_void_p(d_f),
+                                              _dp(hm), C.byref(e), C.c_void_p(stream) if stream else None),
+                    "pinyb200_pimd_step")
+        return _pimd_energies(e)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pinyb200_pimd_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -11,7 +11,9 @@ and stores, per configuration, a compressed .npz with
 * PINY's outputs (per-bead forces before and after the M-site
   redistribution, energy components, pressure tensor, the Verlet pair set).
 
-It also stores pimd_transforms.npz: PINY's own ring-polymer transforms
+pimd_md.npz holds PINY's Nose-Hoover chain operator and its spring and
+centroid-virial routines (``piny_ref nhc`` / ``piny_ref springs``) on seeded
+inputs.  It also stores pimd_transforms.npz: PINY's own ring-polymer transforms
 (``piny_ref pimd``: path_integral_init, convert_pimd_mode/pos/force_* of
 transform_stg.c and transform_cnt.c) of seeded bead positions and forces,
 for staging and normal modes at several bead counts.
@@ -225,9 +227,82 @@ def pimd_fixture(tmp):
             out[tag + k] = D[k].reshape(P, PIMD_NATM, 3)
         out[tag + "path_eig"] = D["path_eig"]
         out[tag + "bead_mass"] = D["bead_mass"].reshape(P, PIMD_NATM)
+        out[tag + "prekf"] = D["prekf"]
     path = os.path.join(HERE, "pimd_transforms.npz")
     np.savez_compressed(path, **{k: np.asarray(v) for k, v in out.items()})
     print("pimd_transforms", os.path.getsize(path), "bytes")
+
+
+NHC_CASES = [  # (num chains, len, nres, nyosh, shared): shared maps several coordinates to one chain
+    (15, 4, 1, 3, False), (2, 2, 2, 5, True), (15, 1, 1, 1, False)]
+
+
+def pimd_md_fixture(tmp):
+    """PINY's chain operator (apply_NHC_par, weights from set_yosh) and its
+    spring / centroid-virial routines (mode_energy_control,
+    pimd_pvten_forc_corr) on seeded inputs."""
+    rng = np.random.default_rng(11)
+    n = PIMD_NATM
+    out = {"natm": n}
+    for c, (num, ln, nres, nyosh, shared) in enumerate(NHC_CASES):
+        if shared:  # atoms 0-2 on chain 0, 3-4 on chain 1, atom 5 (a ghost) on the null chain
+            per_atom = np.array([1, 1, 1, 2, 2, num + 1])
+            inhc = np.tile(per_atom, 3).astype(np.int32)
+        else:  # one chain per coordinate of atoms 0-4, atom 5 null
+            inhc = np.full(3 * n, num + 1, np.int32)
+            for d in range(3):
+                inhc[d * n:d * n + 5] = 1 + 3 * np.arange(5) + d
+        dti = 41.3 / nres
+        m = rng.uniform(1800.0, 30000.0, n)
+        v = rng.normal(0.0, 4e-4, (n, 3))
+        mass_nhc = rng.uniform(5e3, 5e4, (ln, num))
+        gkt = rng.uniform(5e-4, 3e-3, (ln, num))
+        x_nhc = rng.normal(0.0, 0.1, (ln, num))
+        v_nhc = rng.normal(0.0, 2e-4, (ln, num))
+        inp = os.path.join(tmp, "nhc_in.bin")
+        with open(inp, "wb") as fh:
+            fh.write(struct.pack("<5i", n, num, ln, nres, nyosh))
+            fh.write(inhc.astype("<i4").tobytes())
+            fh.write(struct.pack("<d", dti))
+            for a in (m, v, mass_nhc, gkt, x_nhc, v_nhc):
+                fh.write(np.ascontiguousarray(a, "<f8").tobytes())
+        res = os.path.join(tmp, "nhc_out.bin")
+        subprocess.run([PINY_REF, "nhc", inp, res], check=True, capture_output=True)
+        D = read_dump(res)
+        t = "nhc%d_" % c
+        out.update({t + "num": num, t + "len": ln, t + "nres": nres, t + "nyosh": nyosh, t + "dti": dti,
+                    t + "inhc": (inhc - 1).reshape(3, n), t + "mass": m, t + "v": v, t + "mass_nhc": mass_nhc,
+                    t + "gkt": gkt, t + "x_nhc": x_nhc, t + "v_nhc": v_nhc, t + "wdti": D["wdti"],
+                    t + "ref_v": D["v"].reshape(n, 3), t + "ref_x_nhc": D["x_nhc"].reshape(ln, num),
+                    t + "ref_v_nhc": D["v_nhc"].reshape(ln, num)})
+    for P in (4, 8):
+        T, wght = 300.0, 1.0
+        prekf = rng.uniform(1e3, 1e4, n)
+        prekf[5] = 0.0
+        veig = np.concatenate([[0.0], rng.uniform(1.0, 30.0, P - 1)])
+        u = rng.normal(0.0, 0.3, (P, n, 3))
+        xmod = rng.uniform(0.0, 20.0, (n, 3))
+        x = xmod[None] + rng.normal(0.0, 0.3, (P, n, 3))
+        f = rng.normal(0.0, 0.02, (P, n, 3))
+        pv, pvt = rng.normal(0.0, 1e-3, 9), rng.normal(0.0, 1e-3, 9)
+        inp = os.path.join(tmp, "spr_in.bin")
+        with open(inp, "wb") as fh:
+            fh.write(struct.pack("<3i", P, n, n))
+            fh.write(struct.pack("<2d", T, wght))
+            for a in (prekf, veig, u, x, f, xmod, pv, pvt):
+                fh.write(np.ascontiguousarray(a, "<f8").tobytes())
+        res = os.path.join(tmp, "spr_out.bin")
+        subprocess.run([PINY_REF, "springs", inp, res], check=True, capture_output=True)
+        D = read_dump(res)
+        t = "spr_p%d_" % P
+        out.update({t + "T": T, t + "wght": wght, t + "prekf": prekf, t + "veig": veig, t + "u": u, t + "x": x,
+                    t + "f": f, t + "xmod": xmod, t + "pvten": pv, t + "pvten_tot": pvt,
+                    t + "ref_fm": D["fm"].reshape(P, n, 3), t + "ref_kin_harm": D["kin_harm"][0],
+                    t + "ref_pvten_mode_tot": D["pvten_mode_tot"], t + "ref_pvten": D["pvten"],
+                    t + "ref_pvten_tot": D["pvten_tot"], t + "ref_akvirx": D["akvirx"][0]})
+    path = os.path.join(HERE, "pimd_md.npz")
+    np.savez_compressed(path, **{k: np.asarray(v) for k, v in out.items()})
+    print("pimd_md", os.path.getsize(path), "bytes")
 
 
 def main():
@@ -235,6 +310,7 @@ def main():
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     tmp = tempfile.mkdtemp(prefix="piny_golden_")
     pimd_fixture(tmp)
+    pimd_md_fixture(tmp)
     if "--pimd-only" in sys.argv[1:]:
         shutil.rmtree(tmp, ignore_errors=True)
         return

@@ -82,3 +82,65 @@ def test_bad_arguments(oracle):
         oracle.pimd_transform(np.zeros((4, 2, 3)), 3, 0)
     x = np.arange(6.0).reshape(1, 2, 3)
     assert np.array_equal(oracle.pimd_transform(x, 1, 0), x)  # one bead: untouched
+
+
+# -- chains, springs, centroid virial, set-up (pimd_md.npz) ------------------
+
+MD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "pimd_md.npz")
+
+
+@pytest.fixture(scope="module")
+def md():
+    return np.load(MD)
+
+
+def _chains(g, t):
+    return {"num_nhc": int(g[t + "num"]), "len_nhc": int(g[t + "len"]), "nres_nhc": int(g[t + "nres"]),
+            "wdti": g[t + "wdti"], "inhc": g[t + "inhc"], "mass_nhc": g[t + "mass_nhc"], "gkt": g[t + "gkt"]}
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_oracle_chains_match_piny(md, oracle, case):
+    from oracle.oracle import nhc_apply
+    t = "nhc%d_" % case
+    v, x, vn = nhc_apply(oracle, md[t + "v"], md[t + "mass"], _chains(md, t), md[t + "x_nhc"], md[t + "v_nhc"])
+    assert np.array_equal(v, md[t + "ref_v"])
+    assert np.array_equal(x, md[t + "ref_x_nhc"])
+    assert np.array_equal(vn, md[t + "ref_v_nhc"])
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_yoshida_weights_match_piny(md, case):
+    from piny_b200.pimd import yoshida_weights
+    t = "nhc%d_" % case
+    assert np.array_equal(yoshida_weights(int(md[t + "nyosh"]), float(md[t + "dti"])), md[t + "wdti"])
+
+
+@pytest.mark.parametrize("P", [4, 8])
+def test_oracle_springs_and_virial_match_piny(md, oracle, P):
+    from oracle.oracle import pimd_force_post, pimd_springs
+    from piny_b200.water import BOLTZ
+    t = "spr_p%d_" % P
+    fm, ake, pvm = pimd_springs(oracle, md[t + "u"], md[t + "prekf"], md[t + "veig"], float(md[t + "wght"]))
+    assert np.array_equal(fm, md[t + "ref_fm"])
+    assert ake == md[t + "ref_kin_harm"]
+    assert np.array_equal(pvm, md[t + "ref_pvten_mode_tot"])
+    # PINY's routine takes forces and tensors already divided by P; P is a
+    # power of two, so scaling the inputs by P first is exact
+    natm = md[t + "u"].shape[1]
+    _, akv, pv, pvt = pimd_force_post(oracle, 1, md[t + "f"] * P, md[t + "x"], md[t + "xmod"], np.zeros_like(fm), natm,
+                                      BOLTZ / float(md[t + "T"]), md[t + "pvten"] * P, md[t + "pvten_tot"] * P)
+    assert np.array_equal(pv, md[t + "ref_pvten"])
+    assert np.array_equal(pvt, md[t + "ref_pvten_tot"])
+    assert akv == md[t + "ref_akvirx"]
+
+
+@pytest.mark.parametrize("kind,P", CASES)
+def test_path_integral_setup_matches_piny(gold, kind, P):
+    from piny_b200.pimd import path_integral_setup
+    t = "k%d_p%d_" % (kind, P)
+    mass = gold["mass"]
+    s = path_integral_setup(mass, P, kind, 300.0)
+    assert np.allclose(s["path_eig"], gold[t + "path_eig"], rtol=1e-15, atol=0)
+    assert np.allclose(s["bead_mass"], gold[t + "bead_mass"], rtol=1e-15, atol=0)
+    assert np.array_equal(s["prekf"], gold[t + "prekf"])
