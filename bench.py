@@ -44,7 +44,8 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="tip4pf_4096_p32",
                     help="a named box; c4_batch64: 64 uneven boxes in one graph launch per step; "
-                         "c5_grad: parameter gradients of 1024 TIP4P/F x 16 beads")
+                         "c5_grad: parameter gradients of 1024 TIP4P/F x 16 beads; "
+                         "pimd_nvt: PINY's NVT ring-polymer MD step of 4096 TIP4P/F x 32 beads")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
@@ -327,6 +328,133 @@ def run_grad(args, ws, rank, local):
     return 0
 
 
+def run_pimd(args, ws, rank, local):
+    """PINY's NVT ring-polymer MD step on the device (pinyb200_pimd_step):
+    4096 q-TIP4P/F x 32 beads, normal modes, chains of 4 on every
+    coordinate, dt = 20 a.u.; a step is the chains and half kicks, the
+    mode transforms, drift, springs, one force evaluation of all beads, the
+    force post-processing, and PINY's per-step list test
+    (pinyb200_check_list_device).  The transform kernel is timed alone for
+    its HBM roofline."""
+    import dataclasses
+
+    import torch
+
+    from piny_b200 import pimd, system, water
+    from piny_b200.lib import NORMAL_MODES, TO_MODES, DeviceBox, DevicePimd, pimd_transform
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    spec = water.named_spec("tip4pf_4096_p32")
+    if ws > 1:
+        spec = dataclasses.replace(spec, seed=spec.seed + rank)
+    pos = water.build_positions(spec) / water.BOHR
+    S = system.build_system(spec, pos)
+    natm, P = int(S["natm"]), spec.nbeads
+    ghost = np.zeros(natm, bool)
+    ghost[np.asarray(S["ghost_atom"])] = True
+    mass = np.tile(np.asarray(spec.model.masses, np.float64), spec.nmol) * 1822.888486
+    dt = 20.0
+    setup = pimd.nvt_setup(mass, ghost, P, NORMAL_MODES, spec.temperature, dt, 800.0, len_nhc=4, nyosh=3)
+    rng = np.random.default_rng(spec.seed)
+    v = rng.normal(size=(P, natm, 3)) * np.sqrt(spec.temperature / water.BOLTZ / setup["bead_mass"])[:, :, None]
+    v[:, ghost, :] = 0.0
+    box = DeviceBox(S, P, args.precision)
+    xmod0 = pos.mean(axis=0)
+    box.build_list(pos[0], xmod0, S["hmat"], S["cutskin2"])
+    pm = DevicePimd(setup)
+    stream = torch.cuda.current_stream(dev)
+    d_x = torch.from_numpy(pos.copy()).to(dev)
+    d_v = torch.from_numpy(v).to(dev)
+    d_f = torch.zeros_like(d_x)
+    pm.forces(box, d_x.data_ptr(), d_f.data_ptr(), S["hmat"], stream=stream.cuda_stream)
+    # the list was built from these positions: their bead spread is the reference
+    spread_ref = box.check_list_device(d_x.data_ptr(), 0.0, stream=stream.cuda_stream)[2]
+    rebuilds = 0
+
+    def step():
+        nonlocal spread_ref, rebuilds
+        e = pm.step(box, d_x.data_ptr(), d_v.data_ptr(), d_f.data_ptr(), S["hmat"], stream=stream.cuda_stream)
+        rebuild, _, spread_now, cutskin2 = box.check_list_device(d_x.data_ptr(), spread_ref,
+                                                                 stream=stream.cuda_stream)
+        if rebuild:
+            x = d_x.cpu().numpy()
+            box.build_list(x[0], x.mean(axis=0), S["hmat"], cutskin2)
+            spread_ref = spread_now
+            rebuilds += 1
+        return e
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if ws > 1:
+        torch.distributed.barrier()
+    ms_list, force_ms = [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e = step()
+        e1.record(stream)
+        e1.synchronize()
+        ms_list.append(e0.elapsed_time(e1))
+        force_ms.append(box.last_timing()[0])
+    clocks = sampler.stop()
+    ms = float(np.mean(ms_list))
+    # the transform alone: positions -> modes of all beads (HBM roofline)
+    tr = torch.empty_like(d_x)
+    tr.copy_(d_x)
+    tms = []
+    for r in range(13):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pimd_transform(tr.data_ptr(), natm, P, NORMAL_MODES, TO_MODES, stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        if r >= 3:
+            tms.append(e0.elapsed_time(e1))
+    t_ms = float(np.mean(tms))
+    t_bytes = 2.0 * P * natm * 3 * 8
+    if ws > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    hbm, peak_kind = peaks()
+    if rank == 0:
+        line = {
+            "metric": "PIMD NVT steps/s (TIP4P/F 4096 mol x 32 beads, normal modes)", "value": ws * 1e3 / ms,
+            "unit": "MD steps/s", "n_gpus": ws, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (step) + " + ("f32+f64acc" if args.precision == "mixed" else "f64") + " (forces)",
+            "data": "synthetic",
+            "config": {"workload": "pimd_nvt", "molecules": spec.nmol, "beads": P, "dt_au": dt,
+                       "chains": "4 links on every coordinate, 3 Yoshida stages", "pme_grid": spec.grid,
+                       "bead_force_evals_per_s": ws * P * 1e3 / ms, "force_ms_per_step": float(np.mean(force_ms)),
+                       "pimd_bookkeeping_ms_per_step": ms - float(np.mean(force_ms)), "list_rebuilds": rebuilds,
+                       "energies_last_step": {k: e[k] for k in ("vintert", "vintrat", "kin_harm", "akvirx")},
+                       "l2": "256 MiB buffer written between timed steps; CUDA events on the launch stream"},
+            "roofline": {"bound": "hbm", "kernel": "normal-mode transform (positions -> modes, all beads)",
+                         "achieved": t_bytes / (t_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": t_bytes / (t_ms * 1e-3) / 1e9 / hbm, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": t_bytes, "ms": t_ms},
+            "cpu_baseline": None, "e2e": None, "gpu_launches": None, "clocks": clocks,
+        }
+        print(json.dumps(line))
+    pm.close()
+    box.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def run_batch(args, ws, rank, local):
     """64 uneven TIP4P/F boxes, all beads, one CUDA graph launch per step."""
     import torch
@@ -463,6 +591,8 @@ def main():
         return run_batch(args, ws, rank, local)
     if args.config == "c5_grad":
         return run_grad(args, ws, rank, local)
+    if args.config == "pimd_nvt":
+        return run_pimd(args, ws, rank, local)
 
     import torch
 

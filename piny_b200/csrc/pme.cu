@@ -611,14 +611,20 @@ __host__ __device__ constexpr int stockham_min_radix(int n, int ns)
 }
 
 // One Stockham pass (stride NS) over lines l0 .. l0+nlg-1, then the next.
+// Consecutive threads take consecutive lines (G lines per round) and share
+// the butterfly index j: a half-warp then touches 16 different lines at the
+// same position, which fall in 16 different bank pairs both for lines along
+// the fast axis (odd line stride) and across it (line stride 1), and reads
+// one twiddle (a broadcast).
 template <typename R, int N, int NS, int SIGN>
-__device__ __forceinline__ void stockham_pass(typename Cplx<R>::T *sm, int l0, int nlg, int ls, int es, const R *tw)
+__device__ __forceinline__ void stockham_pass(typename Cplx<R>::T *sm, int l0, int nlg, int G, int ls, int es,
+                                              const R *tw)
 {
     typedef typename Cplx<R>::T C2;
     constexpr int RAD = stockham_radix(N / NS);
     constexpr int BPL = N / RAD;  // butterflies per line
-    const int l = threadIdx.x / BPL, j = threadIdx.x % BPL;
-    const bool act = l < nlg;
+    const int l = threadIdx.x % G, j = threadIdx.x / G;
+    const bool act = l < nlg && j < BPL;
     C2 v[RAD];
     C2 *p = sm + (size_t)(l0 + (act ? l : 0)) * ls;
     if (act) {
@@ -644,7 +650,7 @@ __device__ __forceinline__ void stockham_pass(typename Cplx<R>::T *sm, int l0, i
         for (int r = 0; r < RAD; r++) p[(d + r * NS) * es] = v[r];
     }
     __syncthreads();
-    if constexpr (NS * RAD < N) stockham_pass<R, N, NS * RAD, SIGN>(sm, l0, nlg, ls, es, tw);
+    if constexpr (NS * RAD < N) stockham_pass<R, N, NS * RAD, SIGN>(sm, l0, nlg, G, ls, es, tw);
 }
 
 template <typename R, int N, int SIGN>
@@ -652,7 +658,7 @@ __device__ __forceinline__ void fft_pow2_inl(typename Cplx<R>::T *sm, int nl, in
 {
     constexpr int BPLMAX = N / stockham_min_radix(N, 1);
     const int G = (int)blockDim.x / BPLMAX > 0 ? (int)blockDim.x / BPLMAX : 1;  // lines per round
-    for (int l0 = 0; l0 < nl; l0 += G) stockham_pass<R, N, 1, SIGN>(sm, l0, min(G, nl - l0), ls, es, tw);
+    for (int l0 = 0; l0 < nl; l0 += G) stockham_pass<R, N, 1, SIGN>(sm, l0, min(G, nl - l0), G, ls, es, tw);
 }
 
 // Out-of-line copy for kernels whose lengths are known only at run time.
