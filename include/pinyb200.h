@@ -44,7 +44,8 @@ enum {
     PINYB200_DISTRIB_GHOSTS = 1, /* apply distrib_ghost_force (ghost_control.c:71) */
     PINYB200_NO_ENERGY = 2,      /* skip energy/virial reductions                   */
     PINYB200_SITE_PAIRS = 4,     /* walk the site list instead of molecule pairs    */
-    PINYB200_TUNE_AGAIN = 8      /* pinyb200_autotune: ignore remembered results    */
+    PINYB200_TUNE_AGAIN = 8,     /* pinyb200_autotune: ignore remembered results    */
+    PINYB200_UPDATE_LIST = 16    /* device list test and rebuild before the forces  */
 };
 
 /*
@@ -366,6 +367,42 @@ int pinyb200_last_timing(pinyb200_ctx *ctx, float *ms, int n);
  * benchmark's roofline divides by.  No counterpart in PINY. */
 int pinyb200_fma_peak(int fp64, int reps, double *gflops);
 
+/*
+ * PINY's per-step list update on the device: the rebuild test of
+ * check_ver_list (nbr_list_control.c:182-247, with the PIMD spread) and,
+ * when it fires, the list build of verlist_control (verlist_control.c:
+ * 30-128) with get_cut_skin's cutskin^2 -- all enqueued on `stream`, no
+ * host round trip, capturable in a CUDA graph (call it once outside a
+ * capture first: that call sets up the device state).  d_pos: [P][natm][3]
+ * with current ghost positions (PINY runs get_ghost_pos first); d_xmod: the
+ * mode-1 positions (NULL for one bead).  The reference spread is kept on
+ * the device (pinyb200_list_set_spread sets it; unset, the first call takes
+ * the current spread).  The list must have been built once on the host
+ * (pinyb200_build_list): device builds reuse its reservations (25 % slack);
+ * a build that does not fit sets a sticky flag, the next evaluation returns
+ * PINYB200_ERR_NAN and pinyb200_list_status PINYB200_ERR_LIST_OVERFLOW --
+ * rebuild on the host then.  The same update runs inside
+ * pinyb200_energy_force_device and the batch graph with
+ * PINYB200_UPDATE_LIST, and inside every pinyb200_pimd_step.  No
+ * counterpart call in PINY (it tests and rebuilds inside energy_control).
+ */
+typedef struct pinyb200_list_state {
+    long rebuilds;           /* device rebuilds so far                       */
+    int rebuilt_last;        /* the last update rebuilt                      */
+    int overflow, mismatch;  /* sticky error flags                           */
+    double rmax;             /* largest bead-1 displacement at the last test */
+    double spread_now;       /* bead spread at the last test                 */
+    double spread_ref;       /* bead spread of the current list              */
+    long npairs, nactive;    /* site pairs (all, with a force) of the list   */
+    long nmol_pairs;         /* molecule pairs of the list                   */
+} pinyb200_list_state;
+
+int pinyb200_update_list_device(pinyb200_ctx *ctx, const double *d_pos, const double *d_xmod,
+                                const double *hmat, void *stream);
+int pinyb200_list_set_spread(pinyb200_ctx *ctx, double spread_ref);
+/* Reads the device state (waits for `stream`, NULL = the context's). */
+int pinyb200_list_status(pinyb200_ctx *ctx, void *stream, pinyb200_list_state *out);
+
 /* Ring-polymer transforms of PINY's PIMD integrators, in FP64, in place on
  * the device array d_x[nbeads][natm][3] (the bead-major layout of
  * pinyb200_energy_force_device), enqueued on `stream`.  No context needed.
@@ -462,7 +499,8 @@ int pinyb200_pimd_forces(pinyb200_pimd *pm, pinyb200_ctx *ctx, double *d_x, doub
 
 /* One NVT step: chains and half kick (int_0_to_dt2_nvt_pimd,
  * int_0_to_dt2_pimd.c:34-190), positions to modes, drift, springs, modes
- * to positions, pinyb200_pimd_forces, half kick and chains
+ * to positions, the device list update (pinyb200_update_list_device),
+ * the forces as in pinyb200_pimd_forces, half kick and chains
  * (int_dt2_to_dt_nvt_pimd, int_dt2_to_dt_pimd.c).  d_x: bead positions,
  * d_v: mode velocities, d_f: mode forces of d_x on entry, of the new d_x
  * on return.  Blocks until done. */

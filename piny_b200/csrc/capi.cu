@@ -15,12 +15,6 @@
 
 using namespace pinyb200;
 
-// Molecule pairs per warp chunk of the molecule-pair kernel (per lane group
-// when P < 32): the i sites are loaded and their forces flushed once per chunk.
-#ifndef PINYB200_MOL_CHUNK
-#define PINYB200_MOL_CHUNK 8
-#endif
-
 namespace {
 
 thread_local std::string g_lib_err;
@@ -231,7 +225,7 @@ int pinyb200_destroy(pinyb200_ctx *c)
                     c->d_xmod, c->d_pos_aos, c->d_force_aos, c->d_acc, c->d_grid, c->d_spec, c->d_filter, c->d_twiddle64,
                     c->d_twiddle32, c->d_err, c->d_mstart, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_chunk,
                     c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf, c->d_x0, c->d_forceP,
-                    c->d_pme_head, c->d_pme_w};
+                    c->d_pme_head, c->d_pme_w, c->d_nchunk, c->d_ls, c->d_cs, c->d_mchunk};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i < 8; i++)
@@ -448,7 +442,7 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
     CK(cudaMalloc(&c->d_row, (size_t)(natm + 1) * sizeof(int)));
     CK(cudaMalloc(&c->d_rowA, (size_t)(natm + 1) * sizeof(int)));
     CK(cudaMalloc(&c->d_count, (size_t)2 * natm * sizeof(int)));
-    CK(cudaMalloc(&c->d_tot, 4 * sizeof(long long)));
+    CK(cudaMalloc(&c->d_tot, 8 * sizeof(long long)));  // list totals [4], chunk total, spare
     // molecules: connected components of the exclusion graph, each a run of
     // at most 4 consecutive sites (water); otherwise the site kernel is used
     {
@@ -526,7 +520,7 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
         if (c->d_col) cudaFree(c->d_col);
         if (c->d_colA) cudaFree(c->d_colA);
         c->d_col = c->d_colA = nullptr;
-        long long cap = tot[0] + tot[0] / 8 + 1024;
+        long long cap = tot[0] + tot[0] / 4 + 1024;
         CK(cudaMalloc(&c->d_col, cap * sizeof(int)));
         CK(cudaMalloc(&c->d_colA, cap * sizeof(int)));
         c->list_cap = cap;
@@ -549,7 +543,7 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
             if (c->d_mmask) cudaFree(c->d_mmask);
             c->d_mj = nullptr;
             c->d_mmask = nullptr;
-            long long cap = mt[0] + mt[0] / 8 + 1024;
+            long long cap = mt[0] + mt[0] / 4 + 1024;
             CK(cudaMalloc(&c->d_mj, cap * sizeof(int)));
             CK(cudaMalloc(&c->d_mmask, cap * sizeof(unsigned)));
             c->mlist_cap = cap;
@@ -571,15 +565,24 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
                     chunks.push_back(k);
                     chunks.push_back(std::min(k + ch, mrow[m + 1]));
                 }
-            if (c->d_chunk) cudaFree(c->d_chunk);
-            c->d_chunk = nullptr;
             c->nchunk = (int)(chunks.size() / 3);
-            CK(upload(&c->d_chunk, chunks.data(), chunks.size()));
+            if (!c->d_chunk || c->nchunk > c->chunk_cap) {
+                // room for lists that grow between host builds (device updates)
+                if (c->d_chunk) cudaFree(c->d_chunk);
+                c->d_chunk = nullptr;
+                const long long cap = c->nchunk + c->nchunk / 4 + 256;
+                CK(cudaMalloc(&c->d_chunk, (size_t)cap * 3 * sizeof(int)));
+                c->chunk_cap = cap;
+            }
+            CK(cudaMemcpy(c->d_chunk, chunks.data(), chunks.size() * sizeof(int), cudaMemcpyHostToDevice));
+            if (!c->d_nchunk) CK(cudaMalloc(&c->d_nchunk, sizeof(int)));
+            CK(cudaMemcpy(c->d_nchunk, &c->nchunk, sizeof(int), cudaMemcpyHostToDevice));
             c->mol_ok = true;
         }
     }
     cudaFree(d_cs);
     c->have_list = true;
+    if (int rc = list_reset_flags(c)) return rc;
     if (npairs) *npairs = (long)tot[0];
     return PINYB200_OK;
 }
@@ -588,6 +591,8 @@ int pinyb200_get_list(pinyb200_ctx *c, int *pi, int *pj, long cap, long *npairs)
 {
     if (!c) return fail(c, PINYB200_ERR_ARG, "NULL context");
     if (!c->have_list) return fail(c, PINYB200_ERR_STATE, "no list built yet");
+    CK(cudaSetDevice(c->device));
+    if (int rc = list_sync_counts(c)) return rc;
     if (npairs) *npairs = (long)c->npairs;
     if (!pi || !pj) return PINYB200_OK;
     if (cap < c->npairs) return fail(c, PINYB200_ERR_ARG, "get_list: capacity too small");
@@ -734,6 +739,11 @@ int pinyb200::enqueue_device(pinyb200_ctx *c, const double *d_pos, const double 
             centroid_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->d_posT, c->d_xmod, c->sys.natm, c->P);
             CK(cudaGetLastError());
         }
+    }
+    if (flags & PINYB200_UPDATE_LIST) {
+        // PINY's list test (and rebuild) from these positions, on the device
+        int rc = list_update_enqueue(c, d_pos, c->P > 1 ? c->d_xmod : nullptr, cell, c->stream);
+        if (rc) return rc;
     }
     int rc = evaluate_enqueue(c, cell, flags, timing, h_acc);
     if (rc) return rc;
@@ -926,6 +936,10 @@ int pinyb200_check_list_device(pinyb200_ctx *c, const double *d_pos, double spre
 int pinyb200_list_info(pinyb200_ctx *c, long *npairs, long *nactive, long *capacity)
 {
     if (!c) return fail(c, PINYB200_ERR_ARG, "list_info: NULL context");
+    if (c->have_list) {
+        CK(cudaSetDevice(c->device));
+        if (int rc = list_sync_counts(c)) return rc;
+    }
     if (npairs) *npairs = (long)c->npairs;
     if (nactive) *nactive = (long)c->nactive;
     if (capacity) *capacity = (long)c->list_cap;

@@ -37,6 +37,26 @@ struct Cell {
 // Table kinds in the coefficient arrays.
 enum TabKind { T_CV0 = 0, T_CDV0 = 1, T_CV0C = 2, T_CDV0C = 3 };
 
+// Molecule pairs per warp chunk of the molecule-pair kernel (per lane group
+// when P < 32): the i sites are loaded and their forces flushed once per chunk.
+#ifndef PINYB200_MOL_CHUNK
+#define PINYB200_MOL_CHUNK 8
+#endif
+
+// Device state of the list update (pinyb200_update_list_device).
+struct ListState {
+    int rebuild;                   // this step's decision (gates the build kernels)
+    int overflow;                  // a build needed more room than reserved (sticky)
+    int mismatch;                  // molecule masks and active site list disagree (sticky)
+    int spread_set;                // spread_ref holds a value
+    double spread_ref;             // bead spread at the last build (PINY interact.spread)
+    double spread_now, rmax;
+    unsigned long long r2s2[2];    // max displacement^2, max spread^2 (bit patterns)
+    long long rebuilds;            // builds done on the device
+    long long site_tot[2];         // full, active site pairs of the last build
+    long long mol_tot[2];          // molecule pairs, site pairs in their masks
+};
+
 struct DeviceSystem {
     int natm, ntyp, npair_typ, nsplin, nuniq;
     int *atm_typ = nullptr;
@@ -148,7 +168,13 @@ struct pinyb200_ctx {
     unsigned *d_mmask = nullptr;
     long long mlist_cap = 0, nmp = 0;
     int nchunk = 0;
-    int *d_chunk = nullptr;    // [nchunk][3]
+    int *d_chunk = nullptr;    // [chunk_cap][3]
+    long long chunk_cap = 0;
+    int *d_nchunk = nullptr;   // device copy of the chunk count (the pair kernel reads it)
+    // device list update (pinyb200_update_list_device)
+    pinyb200::ListState *d_ls = nullptr;
+    double *d_cs = nullptr;    // [npair_typ] cutskin^2 of the last device decision
+    int *d_mchunk = nullptr;   // [nmol] chunks per molecule row, then [nmol + 1] offsets
     // work buffers
     double *d_posT = nullptr;     // [natm][3][P]
     double *d_forceT = nullptr;   // [natm][3][P]
@@ -184,11 +210,15 @@ struct pinyb200_ctx {
 namespace pinyb200 {
 
 // launchers (defined in the .cu files)
+// gate: device flag, 0 = skip (the device list update); st: nullptr = the
+// context's stream
 cudaError_t launch_build_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1,
-                              const double *d_xm, const double *d_cutskin2, int pass);
+                              const double *d_xm, const double *d_cutskin2, int pass, const int *gate = nullptr,
+                              cudaStream_t st = nullptr);
 cudaError_t launch_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
-                            const double *d_cutskin2, int pass);
+                            const double *d_cutskin2, int pass, const int *gate = nullptr,
+                            cudaStream_t st = nullptr);
 cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_pme(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_pme_force_add(pinyb200_ctx *c);
@@ -229,6 +259,13 @@ cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_force_aos);
 cudaError_t launch_list_count(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
                               const double *d_cutskin2, int *d_count, cudaStream_t st);
 cudaError_t launch_list_check(pinyb200_ctx *c, const double *d_pos, unsigned long long *d_out, cudaStream_t st);
+__global__ void __launch_bounds__(1024) mol_scan_kernel(const int *gate, int n, const int *count, int *row,
+                                                         long long *tot);
+// device list update (update.cu)
+int list_update_prepare(pinyb200_ctx *c);
+int list_update_enqueue(pinyb200_ctx *c, const double *d_pos, const double *d_xm, const Cell &cell, cudaStream_t st);
+int list_sync_counts(pinyb200_ctx *c);
+int list_reset_flags(pinyb200_ctx *c);
 cudaError_t launch_count_total(pinyb200_ctx *c, const int *d_count, unsigned long long *d_tot, cudaStream_t st);
 size_t pme_plane_smem(int Na, int Nb, bool fp64);
 size_t pme_slab_smem(int Na, int Nc, bool fp64);

@@ -17,6 +17,8 @@
 // shuffles; the reaction on j is one coalesced FP64 red.add per component.
 // MIXED: separations are formed in FP64 (positions and image shift), the
 // rest of the pair arithmetic is FP32, every accumulation is FP64.
+#include <cstddef>
+
 #include "common.cuh"
 
 namespace pinyb200 {
@@ -35,11 +37,17 @@ struct PairArgs {
     double *forceT;
     double *acc;
     int energy;
+    const int *bad;  // device flags (overflow, mismatch) of the list update, or nullptr
 };
 
 template <typename R, int P>
 __global__ void __launch_bounds__(256) pair_kernel(PairArgs a, Cell cell)
 {
+    if (a.bad && (a.bad[0] | a.bad[1])) {
+        // the list update could not hold the new list: fail loudly
+        if (blockIdx.x == 0 && threadIdx.x == 0) a.acc[S_VVDW] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
     typedef typename Vec4<R>::T V;
     constexpr int JPI = P >= 32 ? 1 : 32 / P;  // neighbours per warp step
     constexpr int BPL = P >= 32 ? P / 32 : 1;  // beads per lane
@@ -209,6 +217,7 @@ cudaError_t launch_pair(pinyb200_ctx *c, const Cell &cell, bool energy)
     a.forceT = c->d_forceT;
     a.acc = c->d_acc;
     a.energy = energy ? 1 : 0;
+    a.bad = c->d_ls ? (const int *)((const char *)c->d_ls + offsetof(ListState, overflow)) : nullptr;
     if (c->precision == PINYB200_FP64) {
         a.tab = s.tab64;
         return launch_pair_r<double>(c, a, cell);

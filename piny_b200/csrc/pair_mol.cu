@@ -19,6 +19,8 @@
 //     is evaluated from the mode-1 separations the same way.
 //   * FP64: every site-pair separation and image shift in FP64 with PINY's
 //     operation order, as in the site kernel.
+#include <cstddef>
+
 #include "common.cuh"
 
 namespace pinyb200 {
@@ -26,7 +28,8 @@ namespace pinyb200 {
 // ---------------------------------------------------------------------------
 // molecule-pair list build (count / fill), FP64 criterion of the site list
 template <int FILL, int NS>
-__global__ void __launch_bounds__(256) mol_list_kernel(int nmol, const int *__restrict__ mstart, int ntyp,
+__global__ void __launch_bounds__(256) mol_list_kernel(const int *__restrict__ gate, int nmol,
+                                                       const int *__restrict__ mstart, int ntyp,
                                                        const double *__restrict__ pos1, const double *__restrict__ xm,
                                                        int use_xm, Cell cell, const double *__restrict__ cutskin2,
                                                        const int *__restrict__ atm_typ,
@@ -37,6 +40,7 @@ __global__ void __launch_bounds__(256) mol_list_kernel(int nmol, const int *__re
                                                        unsigned *__restrict__ mask_out, long long cap,
                                                        unsigned long long *__restrict__ nsite)
 {
+    if (gate && *gate == 0) return;  // device list update: no rebuild this step
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -93,9 +97,11 @@ __global__ void __launch_bounds__(256) mol_list_kernel(int nmol, const int *__re
     }
 }
 
-__global__ void __launch_bounds__(1024) mol_scan_kernel(int n, const int *__restrict__ count, int *__restrict__ row,
+__global__ void __launch_bounds__(1024) mol_scan_kernel(const int *__restrict__ gate, int n,
+                                                         const int *__restrict__ count, int *__restrict__ row,
                                                          long long *__restrict__ tot)
 {
+    if (gate && *gate == 0) return;
     __shared__ long long part[1024];
     const int t = threadIdx.x;
     const int chunk = (n + blockDim.x - 1) / blockDim.x;
@@ -125,8 +131,9 @@ __global__ void __launch_bounds__(1024) mol_scan_kernel(int n, const int *__rest
 // force kernel
 
 struct MolArgs {
-    int nchunk;
-    const int *chunk;  // [nchunk][3]: mi, begin, end
+    const int *nchunk;  // device: chunks of the current list
+    const int *chunk;   // [nchunk][3]: mi, begin, end
+    const int *bad;     // device flags (overflow, mismatch) of the list update, or nullptr
     const int *mj;
     const unsigned *mask;
     const int *mstart;
@@ -313,6 +320,12 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
     if (ENERGY)
         for (int c = 0; c < 8; c++) sacc[c][threadIdx.x] = 0.0;
     __syncthreads();
+    if (a.bad && (a.bad[0] | a.bad[1])) {
+        // the list update could not hold the new list: make the evaluation
+        // fail loudly (non-finite energy) instead of using a stale list
+        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) a.acc[S_VVDW] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
     const V *__restrict__ tab = (const V *)a.tab;
     const size_t tstride = (size_t)a.nuniq * a.nsplin;
     const int lane = threadIdx.x & 31;
@@ -323,7 +336,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
     const int nsm2 = a.nsplin - 2;
     const double *__restrict__ posT = a.posT;
 
-    for (int ch = warp; ch < a.nchunk; ch += nwarps) {
+    const int nch = *a.nchunk;
+    for (int ch = warp; ch < nch; ch += nwarps) {
         const int mi = a.chunk[3 * ch], beg = a.chunk[3 * ch + 1], end = a.chunk[3 * ch + 2];
         const int i0 = a.mstart[mi], ni = a.mstart[mi + 1] - i0;
         double xi[NS][3];  // FP64 positions (MIXED keeps site 0 only live)
@@ -482,8 +496,9 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
 // launchers
 
 cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
-                            const double *d_cutskin2, int pass)
+                            const double *d_cutskin2, int pass, const int *gate, cudaStream_t st)
 {
+    if (!st) st = c->stream;
     const DeviceSystem &s = c->sys;
     const int threads = 256;
     int blocks = (c->nmol * 32 + threads - 1) / threads;
@@ -492,13 +507,13 @@ cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_p
     if (blocks < 1) blocks = 1;
 #define MOL_LIST(NSV)                                                                                            \
     if (pass == 0) {                                                                                             \
-        mol_list_kernel<0, NSV><<<blocks, threads, 0, c->stream>>>(                                              \
-            c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell, d_cutskin2, s.atm_typ, s.charge, \
+        mol_list_kernel<0, NSV><<<blocks, threads, 0, st>>>(                                                     \
+            gate, c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell, d_cutskin2, s.atm_typ, s.charge, \
             s.inter_map, s.has_vdw, c->d_mcount, nullptr, nullptr, nullptr, 0, nullptr);                         \
-        mol_scan_kernel<<<1, 1024, 0, c->stream>>>(c->nmol, c->d_mcount, c->d_mrow, c->d_tot + 2);               \
+        mol_scan_kernel<<<1, 1024, 0, st>>>(gate, c->nmol, c->d_mcount, c->d_mrow, c->d_tot + 2);                \
     } else {                                                                                                     \
-        mol_list_kernel<1, NSV><<<blocks, threads, 0, c->stream>>>(                                              \
-            c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell, d_cutskin2, s.atm_typ, s.charge, \
+        mol_list_kernel<1, NSV><<<blocks, threads, 0, st>>>(                                                     \
+            gate, c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell, d_cutskin2, s.atm_typ, s.charge, \
             s.inter_map, s.has_vdw, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->mlist_cap,                  \
             (unsigned long long *)(c->d_tot + 3));                                                               \
     }
@@ -513,7 +528,7 @@ template <typename R, int P, int NS>
 static void launch_mol_t(pinyb200_ctx *c, const MolArgs &a, const Cell &cell, bool fast)
 {
     const int threads = 128;
-    long long blocks = ((long long)a.nchunk * 32 + threads - 1) / threads;
+    long long blocks = ((long long)c->chunk_cap * 32 + threads - 1) / threads;
     const long long maxb = (long long)c->sm_count * c->pair_blocks_per_sm;
     if (blocks > maxb) blocks = maxb;
     if (blocks < 1) blocks = 1;
@@ -549,8 +564,9 @@ cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy)
 {
     const DeviceSystem &s = c->sys;
     MolArgs a;
-    a.nchunk = c->nchunk;
+    a.nchunk = c->d_nchunk;
     a.chunk = c->d_chunk;
+    a.bad = c->d_ls ? (const int *)((const char *)c->d_ls + offsetof(ListState, overflow)) : nullptr;
     a.mj = c->d_mj;
     a.mask = c->d_mmask;
     a.mstart = c->d_mstart;

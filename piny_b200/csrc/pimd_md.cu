@@ -7,6 +7,7 @@
 //   springs on the modes         mode_energy_control (pimd_estimators.c:31-110)
 //   mode 1 -> xmod, modes -> positions, ghost positions
 //                                control_pimd_trans_pos (control_pimd_trans.c:146-250)
+//   list test and rebuild        check_ver_list / verlist_control, on the device
 //   force path, post-processing  energy_control_pimd.c:113-218: forces / P,
 //                                centroid virial correction (pimd_pvten_forc_corr,
 //                                pimd_estimators.c:223-305), forces -> modes,
@@ -565,6 +566,9 @@ int pinyb200_pimd_step(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double *
     PCK(cudaMemcpyAsync(pm->d_xmod, d_x, sizeof(double) * (size_t)pm->natm * 3, cudaMemcpyDeviceToDevice, st));
     if (pm->P > 1 && (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_BEADS, d_x, st))) return rc;
     if ((rc = ghost_positions(pm, c, d_x, st))) return rc;
+    // PINY's list test and, when due, the rebuild -- on the device
+    if ((rc = pinyb200::list_update_enqueue(c, d_x, pm->P > 1 ? pm->d_xmod : nullptr, pinyb200::cell_from_hmat(hmat), st)))
+        return rc;
     // forces of the new positions, as mode forces
     if ((rc = forces_core(pm, c, d_x, pm->d_xmod, d_f, hmat, e, st))) return rc;
     // dt/2 -> dt: half kick, chains

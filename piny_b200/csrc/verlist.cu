@@ -16,7 +16,8 @@
 namespace pinyb200 {
 
 template <int FILL>
-__global__ void __launch_bounds__(256) list_kernel(int natm, int ntyp, const double *__restrict__ pos1,
+__global__ void __launch_bounds__(256) list_kernel(const int *__restrict__ gate, int natm, int ntyp,
+                                                   const double *__restrict__ pos1,
                                                    const double *__restrict__ xm, int use_xm, Cell cell,
                                                    const double *__restrict__ cutskin2,
                                                    const int *__restrict__ atm_typ,
@@ -29,6 +30,7 @@ __global__ void __launch_bounds__(256) list_kernel(int natm, int ntyp, const dou
                                                    const int *__restrict__ rowA, int *__restrict__ colA,
                                                    long long cap)
 {
+    if (gate && *gate == 0) return;  // device list update: no rebuild this step
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -87,9 +89,11 @@ __global__ void __launch_bounds__(256) list_kernel(int natm, int ntyp, const dou
 
 // Exclusive scan of two count arrays (full, active) into row pointers; one
 // block, each thread sums a contiguous chunk.
-__global__ void __launch_bounds__(1024) scan_kernel(int n, const int *__restrict__ count, int *__restrict__ row,
-                                                     int *__restrict__ rowA, long long *__restrict__ tot)
+__global__ void __launch_bounds__(1024) scan_kernel(const int *__restrict__ gate, int n, const int *__restrict__ count,
+                                                     int *__restrict__ row, int *__restrict__ rowA,
+                                                     long long *__restrict__ tot)
 {
+    if (gate && *gate == 0) return;
     __shared__ long long part[2][1024];
     const int t = threadIdx.x;
     const int chunk = (n + blockDim.x - 1) / blockDim.x;
@@ -122,21 +126,22 @@ __global__ void __launch_bounds__(1024) scan_kernel(int n, const int *__restrict
 }
 
 cudaError_t launch_build_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
-                              const double *d_cutskin2, int pass)
+                              const double *d_cutskin2, int pass, const int *gate, cudaStream_t st)
 {
+    if (!st) st = c->stream;
     const DeviceSystem &s = c->sys;
     const int threads = 256;
     int blocks = (s.natm * 32 + threads - 1) / threads;
     const int maxb = c->sm_count * 8;
     if (blocks > maxb) blocks = maxb;
     if (pass == 0) {
-        list_kernel<0><<<blocks, threads, 0, c->stream>>>(s.natm, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell,
+        list_kernel<0><<<blocks, threads, 0, st>>>(gate, s.natm, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell,
                                                           d_cutskin2, s.atm_typ, s.charge, s.inter_map, s.has_vdw,
                                                           s.excl_off, s.excl_j, c->d_count, nullptr, nullptr,
                                                           nullptr, nullptr, 0);
-        scan_kernel<<<1, 1024, 0, c->stream>>>(s.natm, c->d_count, c->d_row, c->d_rowA, c->d_tot);
+        scan_kernel<<<1, 1024, 0, st>>>(gate, s.natm, c->d_count, c->d_row, c->d_rowA, c->d_tot);
     } else {
-        list_kernel<1><<<blocks, threads, 0, c->stream>>>(s.natm, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell,
+        list_kernel<1><<<blocks, threads, 0, st>>>(gate, s.natm, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell,
                                                           d_cutskin2, s.atm_typ, s.charge, s.inter_map, s.has_vdw,
                                                           s.excl_off, s.excl_j, c->d_count, c->d_row, c->d_col,
                                                           c->d_rowA, c->d_colA, c->list_cap);
@@ -158,7 +163,7 @@ cudaError_t launch_list_count(pinyb200_ctx *c, const Cell &cell, const double *d
     int blocks = (s.natm * 32 + threads - 1) / threads;
     const int maxb = c->sm_count * 8;
     if (blocks > maxb) blocks = maxb;
-    list_kernel<0><<<blocks, threads, 0, st>>>(s.natm, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell, d_cutskin2,
+    list_kernel<0><<<blocks, threads, 0, st>>>(nullptr, s.natm, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell, d_cutskin2,
                                                s.atm_typ, s.charge, s.inter_map, s.has_vdw, s.excl_off, s.excl_j,
                                                d_count, nullptr, nullptr, nullptr, nullptr, 0);
     return cudaGetLastError();

@@ -24,6 +24,7 @@ DISTRIB_GHOSTS = 1
 NO_ENERGY = 2
 SITE_PAIRS = 4
 TUNE_AGAIN = 8
+UPDATE_LIST = 16       # PINYB200_UPDATE_LIST
 
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NO_DEVICE", 4: "ERR_LIST_OVERFLOW", 5: "ERR_CUTOFF",
           6: "ERR_TIMEOUT", 7: "ERR_NAN", 8: "ERR_UNSUPPORTED", 9: "ERR_STATE"}
@@ -57,6 +58,13 @@ ENERGY_NAMES = ("vreal", "vvdw", "vcoul", "vrecip", "vself", "vbgr", "vecor", "v
 
 class PinyEnergies(C.Structure):
     _fields_ = [(n, _d) for n in ENERGY_NAMES] + [("pvten", _d * 9)]
+
+
+class PinyListState(C.Structure):
+    """pinyb200_list_state."""
+    _fields_ = [("rebuilds", C.c_long), ("rebuilt_last", _i), ("overflow", _i), ("mismatch", _i), ("rmax", _d),
+                ("spread_now", _d), ("spread_ref", _d), ("npairs", C.c_long), ("nactive", C.c_long),
+                ("nmol_pairs", C.c_long)]
 
 
 class PinyNhcSet(C.Structure):
@@ -94,7 +102,8 @@ EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb
            "pinyb200_batch_destroy", "pinyb200_batch_energy_force_device", "pinyb200_batch_last_ms",
            "pinyb200_batch_last_error", "pinyb200_grad_prepare", "pinyb200_grad",
            "pinyb200_fma_peak", "pinyb200_pimd_transform", "pinyb200_pimd_create", "pinyb200_pimd_destroy",
-           "pinyb200_pimd_set_nhc", "pinyb200_pimd_get_nhc", "pinyb200_pimd_forces", "pinyb200_pimd_step")
+           "pinyb200_pimd_set_nhc", "pinyb200_pimd_get_nhc", "pinyb200_pimd_forces", "pinyb200_pimd_step",
+           "pinyb200_update_list_device", "pinyb200_list_set_spread", "pinyb200_list_status")
 
 STAGING, NORMAL_MODES = 1, 2                      # PINYB200_STAGING / _NORMAL_MODES
 TO_MODES, TO_BEADS, FORCE_TO_MODES = 0, 1, 2      # PINYB200_TO_MODES / _TO_BEADS / _FORCE_TO_MODES
@@ -151,6 +160,9 @@ def load(build_if_missing: bool = True):
     L.pinyb200_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, C.c_void_p, _pd, _pd, C.c_void_p]
     L.pinyb200_fma_peak.argtypes = [_i, _i, _pd]
     L.pinyb200_pimd_transform.argtypes = [_i, _i, _i, _i, C.c_void_p, C.c_void_p]
+    L.pinyb200_update_list_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, C.c_void_p]
+    L.pinyb200_list_set_spread.argtypes = [C.c_void_p, _d]
+    L.pinyb200_list_status.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(PinyListState)]
     L.pinyb200_pimd_create.argtypes = [C.POINTER(PinyPimdSetup), C.POINTER(C.c_void_p)]
     L.pinyb200_pimd_destroy.argtypes = [C.c_void_p]
     L.pinyb200_pimd_set_nhc.argtypes = [C.c_void_p, _i, _pd, _pd]
@@ -285,6 +297,25 @@ class DeviceBox:
                     "check_list_device")
         return bool(reb.value), rmax.value, spread.value, cs
 
+    def update_list_device(self, d_pos: int, d_xmod, hmat, stream=None):
+        """PINY's list test and, when due, rebuild on the device (no host
+        round trip); d_pos [P][natm][3] with current ghost positions."""
+        hm = np.ascontiguousarray(hmat, np.float64)
+        self._check(self.L.pinyb200_update_list_device(self.h, C.c_void_p(d_pos),
+                                                       C.c_void_p(d_xmod) if d_xmod else None, _dp(hm),
+                                                       C.c_void_p(stream) if stream else None),
+                    "update_list_device")
+
+    def list_set_spread(self, spread_ref: float):
+        self._check(self.L.pinyb200_list_set_spread(self.h, float(spread_ref)), "list_set_spread")
+
+    def list_status(self, stream=None, check=True):
+        st = PinyListState()
+        rc = self.L.pinyb200_list_status(self.h, C.c_void_p(stream) if stream else None, C.byref(st))
+        if check:
+            self._check(rc, "list_status")
+        return {k: getattr(st, k) for k, _ in PinyListState._fields_}
+
     def get_list(self):
         n = C.c_long()
         self._check(self.L.pinyb200_get_list(self.h, None, None, 0, C.byref(n)), "get_list")
@@ -312,11 +343,13 @@ class DeviceBox:
         return force, energies_dict(e)
 
     def energy_force_device(self, d_pos: int, d_xmod, hmat, d_force: int, stream=None, distribute_ghosts=False,
-                            energy=True):
-        """Device-pointer variant; pointers are integers (e.g. tensor.data_ptr())."""
+                            energy=True, update_list=False):
+        """Device-pointer variant; pointers are integers (e.g. tensor.data_ptr()).
+        update_list: PINY's list test and rebuild on the device first."""
         hmat = np.ascontiguousarray(hmat, np.float64)
         e = PinyEnergies()
-        flags = (DISTRIB_GHOSTS if distribute_ghosts else 0) | (0 if energy else NO_ENERGY)
+        flags = (DISTRIB_GHOSTS if distribute_ghosts else 0) | (0 if energy else NO_ENERGY) | \
+            (UPDATE_LIST if update_list else 0)
         self._check(self.L.pinyb200_energy_force_device(self.h, C.c_void_p(d_pos),
                                                         None if d_xmod is None else C.c_void_p(d_xmod), _dp(hmat),
                                                         flags, C.c_void_p(d_force), C.byref(e),
@@ -398,7 +431,7 @@ class DeviceBatch:
                                                               self.L.pinyb200_last_error(None).decode()))
         self.h = h
 
-    def energy_force_device(self, d_pos, d_xmod, hmats, d_force, stream=None, energy=True):
+    def energy_force_device(self, d_pos, d_xmod, hmats, d_force, stream=None, energy=True, update_list=False):
         n = len(self.boxes)
         P = (C.c_void_p * n)(*[int(p) for p in d_pos])
         X = (C.c_void_p * n)(*[None if x is None else int(x) for x in d_xmod]) if d_xmod is not None else None
@@ -406,7 +439,8 @@ class DeviceBatch:
         hm = [np.ascontiguousarray(h, np.float64) for h in hmats]
         H = (_pd * n)(*[_dp(h) for h in hm])
         E = (PinyEnergies * n)()
-        rc = self.L.pinyb200_batch_energy_force_device(self.h, P, X, H, 0 if energy else NO_ENERGY, F, E,
+        flags = (0 if energy else NO_ENERGY) | (UPDATE_LIST if update_list else 0)
+        rc = self.L.pinyb200_batch_energy_force_device(self.h, P, X, H, flags, F, E,
                                                        None if stream is None else C.c_void_p(stream))
         if rc != 0:
             raise PinyError("batch_energy_force_device: %s %s" % (STATUS.get(rc, rc),
