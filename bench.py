@@ -332,10 +332,10 @@ def run_pimd(args, ws, rank, local):
     """PINY's NVT ring-polymer MD step on the device (pinyb200_pimd_step):
     4096 q-TIP4P/F x 32 beads, normal modes, chains of 4 on every
     coordinate, dt = 20 a.u.; a step is the chains and half kicks, the
-    mode transforms, drift, springs, one force evaluation of all beads, the
-    force post-processing, and PINY's per-step list test
-    (pinyb200_check_list_device).  The transform kernel is timed alone for
-    its HBM roofline."""
+    mode transforms, drift, springs, PINY's list test and (when due) list
+    rebuild on the device, one force evaluation of all beads, and the force
+    post-processing.  The transform kernel is timed alone for its HBM
+    roofline."""
     import dataclasses
 
     import torch
@@ -368,21 +368,12 @@ def run_pimd(args, ws, rank, local):
     d_v = torch.from_numpy(v).to(dev)
     d_f = torch.zeros_like(d_x)
     pm.forces(box, d_x.data_ptr(), d_f.data_ptr(), S["hmat"], stream=stream.cuda_stream)
-    # the list was built from these positions: their bead spread is the reference
-    spread_ref = box.check_list_device(d_x.data_ptr(), 0.0, stream=stream.cuda_stream)[2]
-    rebuilds = 0
+    # the list was built from these positions: their bead spread is the
+    # reference of the device list test that every step runs
+    box.list_set_spread(box.check_list_device(d_x.data_ptr(), 0.0, stream=stream.cuda_stream)[2])
 
     def step():
-        nonlocal spread_ref, rebuilds
-        e = pm.step(box, d_x.data_ptr(), d_v.data_ptr(), d_f.data_ptr(), S["hmat"], stream=stream.cuda_stream)
-        rebuild, _, spread_now, cutskin2 = box.check_list_device(d_x.data_ptr(), spread_ref,
-                                                                 stream=stream.cuda_stream)
-        if rebuild:
-            x = d_x.cpu().numpy()
-            box.build_list(x[0], x.mean(axis=0), S["hmat"], cutskin2)
-            spread_ref = spread_now
-            rebuilds += 1
-        return e
+        return pm.step(box, d_x.data_ptr(), d_v.data_ptr(), d_f.data_ptr(), S["hmat"], stream=stream.cuda_stream)
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     for _ in range(max(3, args.warmup)):
@@ -406,6 +397,7 @@ def run_pimd(args, ws, rank, local):
         force_ms.append(box.last_timing()[0])
     clocks = sampler.stop()
     ms = float(np.mean(ms_list))
+    rebuilds = box.list_status(stream=stream.cuda_stream)["rebuilds"]
     # the transform alone: positions -> modes of all beads (HBM roofline)
     tr = torch.empty_like(d_x)
     tr.copy_(d_x)
@@ -437,7 +429,8 @@ def run_pimd(args, ws, rank, local):
             "config": {"workload": "pimd_nvt", "molecules": spec.nmol, "beads": P, "dt_au": dt,
                        "chains": "4 links on every coordinate, 3 Yoshida stages", "pme_grid": spec.grid,
                        "bead_force_evals_per_s": ws * P * 1e3 / ms, "force_ms_per_step": float(np.mean(force_ms)),
-                       "pimd_bookkeeping_ms_per_step": ms - float(np.mean(force_ms)), "list_rebuilds": rebuilds,
+                       "pimd_bookkeeping_ms_per_step": ms - float(np.mean(force_ms)), "list_rebuilds_incl_warmup": rebuilds,
+                       "step_ms_median": float(np.median(ms_list)), "step_ms_max": float(np.max(ms_list)),
                        "energies_last_step": {k: e[k] for k in ("vintert", "vintrat", "kin_harm", "akvirx")},
                        "l2": "256 MiB buffer written between timed steps; CUDA events on the launch stream"},
             "roofline": {"bound": "hbm", "kernel": "normal-mode transform (positions -> modes, all beads)",

@@ -225,7 +225,8 @@ int pinyb200_destroy(pinyb200_ctx *c)
                     c->d_xmod, c->d_pos_aos, c->d_force_aos, c->d_acc, c->d_grid, c->d_spec, c->d_filter, c->d_twiddle64,
                     c->d_twiddle32, c->d_err, c->d_mstart, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_chunk,
                     c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf, c->d_x0, c->d_forceP,
-                    c->d_pme_head, c->d_pme_w, c->d_nchunk, c->d_ls, c->d_cs, c->d_mchunk};
+                    c->d_pme_head, c->d_pme_w, c->d_nchunk, c->d_ls, c->d_cs, c->d_mchunk, c->d_mmaskf,
+                    c->d_reach};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i < 8; i++)
@@ -475,6 +476,16 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
             for (int k = 0; ok && k < nm; k++)
                 if (s->atm_typ[mstart[m] + k] != s->atm_typ[k] || s->charge[mstart[m] + k] != s->charge[k]) ok = false;
         }
+        // every pair inside a molecule must be excluded: the molecule lists
+        // hold pairs of different molecules only
+        for (size_t m = 0; ok && m + 1 < mstart.size(); m++)
+            for (int i = mstart[m]; ok && i < mstart[m + 1]; i++)
+                for (int j = mstart[m]; ok && j < i; j++) {
+                    bool ex = false;
+                    for (int e = s->excl_off[i]; e < s->excl_off[i + 1]; e++) ex |= s->excl_j[e] == j;
+                    for (int e = s->excl_off[j]; e < s->excl_off[j + 1]; e++) ex |= s->excl_j[e] == i;
+                    if (!ex) ok = false;
+                }
         if (ok && maxn <= 4 && s->ntyp <= 8) {
             c->use_mol = true;
             c->nmol = (int)mstart.size() - 1;
@@ -506,54 +517,55 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
     }
     double *d_cs = nullptr;
     CK(cudaMalloc(&d_cs, c->sys.npair_typ * sizeof(double)));
+    struct FreeCs {
+        double *p;
+        ~FreeCs() { cudaFree(p); }
+    } free_cs{d_cs};
     CK(cudaMemcpyAsync(d_cs, cutskin2, c->sys.npair_typ * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CK(launch_build_list(c, cell, d_p1, d_xm, d_cs, 0));
-    long long tot[2];
-    CK(cudaMemcpyAsync(tot, c->d_tot, sizeof(tot), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    if (tot[0] > 0x7fffffffLL) {
-        cudaFree(d_cs);
-        return fail(c, PINYB200_ERR_LIST_OVERFLOW, "Verlet list exceeds 2^31 pairs");
-    }
-    if (tot[0] > c->list_cap) {
-        // grow like ver_list_mem_check (verlist_control.c:87-110), with slack
+    // grow like ver_list_mem_check (verlist_control.c:87-110), with slack
+    // for lists that grow between host builds (device updates)
+    auto grow_sites = [&](long long need) -> int {
+        if (need <= c->list_cap && c->d_col) return PINYB200_OK;
         if (c->d_col) cudaFree(c->d_col);
         if (c->d_colA) cudaFree(c->d_colA);
         c->d_col = c->d_colA = nullptr;
-        long long cap = tot[0] + tot[0] / 4 + 1024;
+        const long long cap = need + need / 4 + 1024;
         CK(cudaMalloc(&c->d_col, cap * sizeof(int)));
         CK(cudaMalloc(&c->d_colA, cap * sizeof(int)));
         c->list_cap = cap;
-    }
-    CK(launch_build_list(c, cell, d_p1, d_xm, d_cs, 1));
-    // the rebuild test measures displacements from these positions
-    CK(cudaMemcpyAsync(c->d_x0, d_p1, (size_t)natm * 3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    c->npairs = tot[0];
-    c->nactive = tot[1];
+        return PINYB200_OK;
+    };
+    long long tot[4] = {0, 0, 0, 0};
     c->mol_ok = false;
     if (c->use_mol) {
-        CK(cudaMemsetAsync(c->d_tot + 2, 0, 2 * sizeof(long long), c->stream));
+        // molecule-pair list first; the site lists are expanded from its masks
+        if (!c->d_reach) CK(cudaMalloc(&c->d_reach, sizeof(double)));
+        CK(cudaMemsetAsync(c->d_tot, 0, 4 * sizeof(long long), c->stream));
         CK(launch_mol_list(c, cell, d_p1, d_xm, d_cs, 0));
-        long long mt[2];
-        CK(cudaMemcpyAsync(mt, c->d_tot + 2, sizeof(mt), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(tot, c->d_tot, sizeof(tot), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        if (mt[0] > c->mlist_cap) {
+        if (tot[2] > c->mlist_cap || !c->d_mj) {
             if (c->d_mj) cudaFree(c->d_mj);
             if (c->d_mmask) cudaFree(c->d_mmask);
+            if (c->d_mmaskf) cudaFree(c->d_mmaskf);
             c->d_mj = nullptr;
-            c->d_mmask = nullptr;
-            long long cap = mt[0] + mt[0] / 4 + 1024;
+            c->d_mmask = c->d_mmaskf = nullptr;
+            const long long cap = tot[2] + tot[2] / 4 + 1024;
             CK(cudaMalloc(&c->d_mj, cap * sizeof(int)));
             CK(cudaMalloc(&c->d_mmask, cap * sizeof(unsigned)));
+            CK(cudaMalloc(&c->d_mmaskf, cap * sizeof(unsigned)));
             c->mlist_cap = cap;
         }
         CK(launch_mol_list(c, cell, d_p1, d_xm, d_cs, 1));
-        CK(cudaMemcpyAsync(mt, c->d_tot + 2, sizeof(mt), cudaMemcpyDeviceToHost, c->stream));
+        CK(launch_site_from_mol(c, 0));
+        CK(cudaMemcpyAsync(tot, c->d_tot, sizeof(tot), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        c->nmp = mt[0];
-        // the molecule masks must hold exactly the active site pairs
-        if (mt[1] == c->nactive) {
+        if (tot[0] > 0x7fffffffLL) return fail(c, PINYB200_ERR_LIST_OVERFLOW, "Verlet list exceeds 2^31 pairs");
+        if (int rc = grow_sites(tot[0])) return rc;
+        CK(launch_site_from_mol(c, 1));
+        c->nmp = tot[2];
+        // the active site pairs of the masks are the active site list
+        if (tot[3] == tot[1]) {
             std::vector<int> mrow(c->nmol + 1);
             CK(cudaMemcpy(mrow.data(), c->d_mrow, mrow.size() * sizeof(int), cudaMemcpyDeviceToHost));
             const int jpi = c->P >= 32 ? 1 : 32 / c->P;
@@ -567,7 +579,6 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
                 }
             c->nchunk = (int)(chunks.size() / 3);
             if (!c->d_chunk || c->nchunk > c->chunk_cap) {
-                // room for lists that grow between host builds (device updates)
                 if (c->d_chunk) cudaFree(c->d_chunk);
                 c->d_chunk = nullptr;
                 const long long cap = c->nchunk + c->nchunk / 4 + 256;
@@ -579,8 +590,19 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
             CK(cudaMemcpy(c->d_nchunk, &c->nchunk, sizeof(int), cudaMemcpyHostToDevice));
             c->mol_ok = true;
         }
+    } else {
+        CK(launch_build_list(c, cell, d_p1, d_xm, d_cs, 0));
+        CK(cudaMemcpyAsync(tot, c->d_tot, 2 * sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (tot[0] > 0x7fffffffLL) return fail(c, PINYB200_ERR_LIST_OVERFLOW, "Verlet list exceeds 2^31 pairs");
+        if (int rc = grow_sites(tot[0])) return rc;
+        CK(launch_build_list(c, cell, d_p1, d_xm, d_cs, 1));
     }
-    cudaFree(d_cs);
+    // the rebuild test measures displacements from these positions
+    CK(cudaMemcpyAsync(c->d_x0, d_p1, (size_t)natm * 3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->npairs = tot[0];
+    c->nactive = tot[1];
     c->have_list = true;
     if (int rc = list_reset_flags(c)) return rc;
     if (npairs) *npairs = (long)tot[0];

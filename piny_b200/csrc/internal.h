@@ -165,7 +165,9 @@ struct pinyb200_ctx {
     int *d_mcount = nullptr;   // [nmol]
     int *d_mrow = nullptr;     // [nmol+1]
     int *d_mj = nullptr;       // [nmp]
-    unsigned *d_mmask = nullptr;
+    unsigned *d_mmask = nullptr;   // active site pairs of each molecule pair
+    unsigned *d_mmaskf = nullptr;  // all site pairs (PINY's list) of each molecule pair
+    double *d_reach = nullptr;     // list build: reach of the molecule bound
     long long mlist_cap = 0, nmp = 0;
     int nchunk = 0;
     int *d_chunk = nullptr;    // [chunk_cap][3]
@@ -220,6 +222,9 @@ cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_p
                             const double *d_cutskin2, int pass, const int *gate = nullptr,
                             cudaStream_t st = nullptr);
 cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
+cudaError_t launch_site_from_mol(pinyb200_ctx *c, int pass, const int *gate = nullptr, cudaStream_t st = nullptr);
+__global__ void __launch_bounds__(1024) scan_kernel(const int *gate, int n, const int *count, int *row, int *rowA,
+                                                     long long *tot);
 cudaError_t launch_pme(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_pme_force_add(pinyb200_ctx *c);
 

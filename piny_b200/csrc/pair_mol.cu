@@ -26,7 +26,88 @@
 namespace pinyb200 {
 
 // ---------------------------------------------------------------------------
-// molecule-pair list build (count / fill), FP64 criterion of the site list
+// molecule-pair list build (count / fill), FP64 criterion of the site list.
+//
+// Each molecule pair (mi > mj) gets two masks of site pairs (si, sj) with
+// r^2 < cutskin^2 on PINY's image: the full mask (PINY's list) and the
+// active one (pairs that carry a force).  A molecule pair is kept when its
+// full mask is not empty.  The site lists (full and active, rows i with
+// ascending j < i) are expanded from the masks afterwards, so the FP64
+// criterion is evaluated once per site pair.  Every pair inside a molecule
+// is excluded (checked when the context is made), so no site pair is lost.
+//
+// A molecule pair is skipped without looking at its sites when a lower
+// bound of the distance between any images of the two site-0 mode-1
+// positions exceeds the reach R = max cutskin + 2 (e + d), e = largest
+// distance of a site from its molecule's site 0 and d = largest distance of
+// a bead-1 position from its mode-1 position (mode-1 positions: xm, or the
+// bead-1 positions for one bead).  Any site pair of a pair so skipped is
+// farther apart than max cutskin on every image.
+
+// Lower bound of |dx + h n| over all lattice vectors h n: along each cell
+// axis the wrapped fractional separation times the lattice-plane spacing.
+__device__ __forceinline__ double image_lower_bound(double dx, double dy, double dz, const Cell &c)
+{
+    double lb = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double b0 = c.hi[d], b1 = c.hi[3 + d], b2 = c.hi[6 + d];
+        const double sd = dx * b0 + dy * b1 + dz * b2;
+        const double w = fabs(sd - rint(sd)) * rsqrt(b0 * b0 + b1 * b1 + b2 * b2);
+        lb = fmax(lb, w);
+    }
+    return lb;
+}
+
+// The reach R (above) into *reach; one block.
+__global__ void __launch_bounds__(1024) mol_reach_kernel(const int *__restrict__ gate, int nmol,
+                                                          const int *__restrict__ mstart,
+                                                          const double *__restrict__ pos1,
+                                                          const double *__restrict__ xm, int use_xm,
+                                                          const double *__restrict__ cs, int npt,
+                                                          double *__restrict__ reach)
+{
+    if (gate && *gate == 0) return;
+    __shared__ double red[3][32];
+    double ext = 0.0, dev = 0.0, cmax = 0.0;
+    for (int k = threadIdx.x; k < npt; k += blockDim.x) cmax = fmax(cmax, cs[k]);
+    for (int m = threadIdx.x; m < nmol; m += blockDim.x) {
+        const int i0 = mstart[m], i1 = mstart[m + 1];
+        const double *x0 = (use_xm ? xm : pos1) + 3 * (size_t)i0;
+        for (int i = i0; i < i1; i++) {
+            const double *xi = (use_xm ? xm : pos1) + 3 * (size_t)i;
+            const double ex = xi[0] - x0[0], ey = xi[1] - x0[1], ez = xi[2] - x0[2];
+            ext = fmax(ext, sqrt(ex * ex + ey * ey + ez * ez));
+            if (use_xm) {
+                const double *p = pos1 + 3 * (size_t)i;
+                const double qx = p[0] - xi[0], qy = p[1] - xi[1], qz = p[2] - xi[2];
+                dev = fmax(dev, sqrt(qx * qx + qy * qy + qz * qz));
+            }
+        }
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+        ext = fmax(ext, __shfl_xor_sync(0xffffffffu, ext, o));
+        dev = fmax(dev, __shfl_xor_sync(0xffffffffu, dev, o));
+        cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[0][w] = ext;
+        red[1][w] = dev;
+        red[2][w] = cmax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); k++) {
+            ext = fmax(ext, red[0][k]);
+            dev = fmax(dev, red[1][k]);
+            cmax = fmax(cmax, red[2][k]);
+        }
+        // rounding of the bound and of the criterion: a generous margin
+        *reach = (sqrt(cmax) + 2.0 * (ext + dev)) * (1.0 + 1e-12) + 1e-9;
+    }
+}
+
 template <int FILL, int NS>
 __global__ void __launch_bounds__(256) mol_list_kernel(const int *__restrict__ gate, int nmol,
                                                        const int *__restrict__ mstart, int ntyp,
@@ -35,55 +116,68 @@ __global__ void __launch_bounds__(256) mol_list_kernel(const int *__restrict__ g
                                                        const int *__restrict__ atm_typ,
                                                        const double *__restrict__ charge,
                                                        const int *__restrict__ inter_map,
-                                                       const int *__restrict__ has_vdw, int *__restrict__ count,
+                                                       const int *__restrict__ has_vdw,
+                                                       const double *__restrict__ reach, int *__restrict__ count,
                                                        const int *__restrict__ row, int *__restrict__ mj_out,
-                                                       unsigned *__restrict__ mask_out, long long cap,
-                                                       unsigned long long *__restrict__ nsite)
+                                                       unsigned *__restrict__ mask_out, unsigned *__restrict__ maskf_out,
+                                                       long long cap, unsigned long long *__restrict__ nsite)
 {
     if (gate && *gate == 0) return;  // device list update: no rebuild this step
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const double R = *reach;
+    const double *x0 = use_xm ? xm : pos1;  // site-0 mode-1 positions for the bound
     unsigned long long sites = 0;
     for (int mi = warp; mi < nmol; mi += nwarps) {
         const int i0 = mstart[mi], ni = mstart[mi + 1] - i0;
+        const double bx = x0[3 * (size_t)i0], by = x0[3 * (size_t)i0 + 1], bz = x0[3 * (size_t)i0 + 2];
         int n = 0;
         const long long w0 = FILL ? row[mi] : 0;
         for (int m0 = 0; m0 < mi; m0 += 32) {
             const int mj = m0 + lane;
-            unsigned mask = 0;
+            unsigned mask = 0, maskf = 0;
             if (mj < mi) {
                 const int j0 = mstart[mj], nj = mstart[mj + 1] - j0;
-                for (int si = 0; si < ni; si++) {
-                    const int i = i0 + si;
-                    const double xi = pos1[3 * i], yi = pos1[3 * i + 1], zi = pos1[3 * i + 2];
-                    const int ti = atm_typ[i];
-                    const double qi = charge[i];
-                    for (int sj = 0; sj < nj; sj++) {
-                        const int j = j0 + sj;
-                        double dx = __dsub_rn(xi, pos1[3 * j]);
-                        double dy = __dsub_rn(yi, pos1[3 * j + 1]);
-                        double dz = __dsub_rn(zi, pos1[3 * j + 2]);
-                        if (use_xm)
-                            period_pimd_exact(dx, dy, dz, __dsub_rn(xm[3 * i], xm[3 * j]),
-                                              __dsub_rn(xm[3 * i + 1], xm[3 * j + 1]),
-                                              __dsub_rn(xm[3 * i + 2], xm[3 * j + 2]), cell);
-                        else
-                            period_exact(dx, dy, dz, cell);
-                        const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-                        const int pt = pair_type(ti, atm_typ[j], ntyp);
-                        if (r2 < cutskin2[pt] && (has_vdw[inter_map[pt]] || qi * charge[j] != 0.0))
-                            mask |= 1u << (si * NS + sj);
+                const double lb = image_lower_bound(bx - x0[3 * (size_t)j0], by - x0[3 * (size_t)j0 + 1],
+                                                    bz - x0[3 * (size_t)j0 + 2], cell);
+                if (!(lb > R)) {
+                    for (int si = 0; si < ni; si++) {
+                        const int i = i0 + si;
+                        const double xi = pos1[3 * i], yi = pos1[3 * i + 1], zi = pos1[3 * i + 2];
+                        const int ti = atm_typ[i];
+                        const double qi = charge[i];
+                        for (int sj = 0; sj < nj; sj++) {
+                            const int j = j0 + sj;
+                            double dx = __dsub_rn(xi, pos1[3 * j]);
+                            double dy = __dsub_rn(yi, pos1[3 * j + 1]);
+                            double dz = __dsub_rn(zi, pos1[3 * j + 2]);
+                            if (use_xm)
+                                period_pimd_exact(dx, dy, dz, __dsub_rn(xm[3 * i], xm[3 * j]),
+                                                  __dsub_rn(xm[3 * i + 1], xm[3 * j + 1]),
+                                                  __dsub_rn(xm[3 * i + 2], xm[3 * j + 2]), cell);
+                            else
+                                period_exact(dx, dy, dz, cell);
+                            const double r2 =
+                                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+                            const int pt = pair_type(ti, atm_typ[j], ntyp);
+                            if (r2 < cutskin2[pt]) {
+                                const unsigned bit = 1u << (si * NS + sj);
+                                maskf |= bit;
+                                if (has_vdw[inter_map[pt]] || qi * charge[j] != 0.0) mask |= bit;
+                            }
+                        }
                     }
                 }
             }
-            const bool keep = mask != 0;
+            const bool keep = maskf != 0;
             const unsigned bk = __ballot_sync(0xffffffffu, keep);
             if (FILL && keep) {
                 const long long p = w0 + n + __popc(bk & ((1u << lane) - 1u));
                 if (p < cap) {
                     mj_out[p] = mj;
                     mask_out[p] = mask;
+                    maskf_out[p] = maskf;
                 }
             }
             if (FILL) sites += __popc(mask);
@@ -94,6 +188,102 @@ __global__ void __launch_bounds__(256) mol_list_kernel(const int *__restrict__ g
     if (FILL) {
         for (int o = 16; o >= 1; o >>= 1) sites += __shfl_xor_sync(0xffffffffu, sites, o);
         if (lane == 0) atomicAdd(nsite, sites);
+    }
+}
+
+// Site lists from the molecule masks.  Count: per site, the full and active
+// pairs with lower-index sites; one warp per molecule row.
+template <int NS>
+__global__ void __launch_bounds__(256) site_count_kernel(const int *__restrict__ gate, int nmol, int natm,
+                                                         const int *__restrict__ mstart, const int *__restrict__ mrow,
+                                                         const unsigned *__restrict__ maskf,
+                                                         const unsigned *__restrict__ mask, long long cap,
+                                                         int *__restrict__ count)
+{
+    if (gate && *gate == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    constexpr unsigned RM = (1u << NS) - 1u;
+    for (int mi = warp; mi < nmol; mi += nwarps) {
+        const int i0 = mstart[mi], ni = mstart[mi + 1] - i0;
+        const int k1 = (int)(mrow[mi + 1] < cap ? mrow[mi + 1] : cap);
+        int cf[NS], ca[NS];
+#pragma unroll
+        for (int si = 0; si < NS; si++) cf[si] = ca[si] = 0;
+        for (int k = mrow[mi] + lane; k < k1; k += 32) {
+            const unsigned f = maskf[k], a = mask[k];
+#pragma unroll
+            for (int si = 0; si < NS; si++) {
+                cf[si] += __popc((f >> (si * NS)) & RM);
+                ca[si] += __popc((a >> (si * NS)) & RM);
+            }
+        }
+#pragma unroll
+        for (int si = 0; si < NS; si++) {
+            for (int o = 16; o >= 1; o >>= 1) {
+                cf[si] += __shfl_xor_sync(0xffffffffu, cf[si], o);
+                ca[si] += __shfl_xor_sync(0xffffffffu, ca[si], o);
+            }
+            if (lane == 0 && si < ni) {
+                count[i0 + si] = cf[si];
+                count[natm + i0 + si] = ca[si];
+            }
+        }
+    }
+}
+
+// Fill: row i lists j = mstart[mj] + sj in molecule-row order (mj
+// ascending), sj ascending within a molecule pair: ascending j.
+template <int NS>
+__global__ void __launch_bounds__(256) site_fill_kernel(const int *__restrict__ gate, int nmol,
+                                                        const int *__restrict__ mstart, const int *__restrict__ mrow,
+                                                        const int *__restrict__ mj, const unsigned *__restrict__ maskf,
+                                                        const unsigned *__restrict__ mask, long long mcap,
+                                                        const int *__restrict__ row, const int *__restrict__ rowA,
+                                                        int *__restrict__ col, int *__restrict__ colA, long long cap)
+{
+    if (gate && *gate == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    constexpr unsigned RM = (1u << NS) - 1u;
+    for (int mi = warp; mi < nmol; mi += nwarps) {
+        const int i0 = mstart[mi], ni = mstart[mi + 1] - i0;
+        const int k1 = (int)(mrow[mi + 1] < mcap ? mrow[mi + 1] : mcap);
+        for (int si = 0; si < ni; si++) {
+            long long wf = row[i0 + si], wa = rowA[i0 + si];
+            for (int k0 = mrow[mi]; k0 < k1; k0 += 32) {
+                const int k = k0 + lane;
+                unsigned f = 0, a = 0;
+                int j0 = 0;
+                if (k < k1) {
+                    f = (maskf[k] >> (si * NS)) & RM;
+                    a = (mask[k] >> (si * NS)) & RM;
+                    j0 = mstart[mj[k]];
+                }
+                // exclusive prefix sums of the per-lane counts
+                int nf = __popc(f), na = __popc(a), pf = nf, pa = na;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int tf = __shfl_up_sync(0xffffffffu, pf, o), ta = __shfl_up_sync(0xffffffffu, pa, o);
+                    if (lane >= o) {
+                        pf += tf;
+                        pa += ta;
+                    }
+                }
+                long long qf = wf + pf - nf, qa = wa + pa - na;
+                for (unsigned m = f; m; m &= m - 1u) {
+                    if (qf < cap) col[qf] = j0 + __ffs(m) - 1;
+                    qf++;
+                }
+                for (unsigned m = a; m; m &= m - 1u) {
+                    if (qa < cap) colA[qa] = j0 + __ffs(m) - 1;
+                    qa++;
+                }
+                wf += __shfl_sync(0xffffffffu, pf, 31);
+                wa += __shfl_sync(0xffffffffu, pa, 31);
+            }
+        }
     }
 }
 
@@ -495,6 +685,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
 // ---------------------------------------------------------------------------
 // launchers
 
+// pass 0: reach, counts, row offsets and the molecule-pair total (tot[2]);
+// pass 1: the fill, adding the active site pairs into tot[3].
 cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
                             const double *d_cutskin2, int pass, const int *gate, cudaStream_t st)
 {
@@ -505,22 +697,54 @@ cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_p
     const int maxb = c->sm_count * 8;
     if (blocks > maxb) blocks = maxb;
     if (blocks < 1) blocks = 1;
-#define MOL_LIST(NSV)                                                                                            \
-    if (pass == 0) {                                                                                             \
-        mol_list_kernel<0, NSV><<<blocks, threads, 0, st>>>(                                                     \
-            gate, c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell, d_cutskin2, s.atm_typ, s.charge, \
-            s.inter_map, s.has_vdw, c->d_mcount, nullptr, nullptr, nullptr, 0, nullptr);                         \
-        mol_scan_kernel<<<1, 1024, 0, st>>>(gate, c->nmol, c->d_mcount, c->d_mrow, c->d_tot + 2);                \
-    } else {                                                                                                     \
-        mol_list_kernel<1, NSV><<<blocks, threads, 0, st>>>(                                                     \
-            gate, c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell, d_cutskin2, s.atm_typ, s.charge, \
-            s.inter_map, s.has_vdw, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->mlist_cap,                  \
-            (unsigned long long *)(c->d_tot + 3));                                                               \
+    const int use_xm = d_xm != nullptr;
+    if (pass == 0)
+        mol_reach_kernel<<<1, 1024, 0, st>>>(gate, c->nmol, c->d_mstart, d_pos1, d_xm, use_xm, d_cutskin2,
+                                             s.npair_typ, c->d_reach);
+#define MOL_LIST(NSV)                                                                                             \
+    if (pass == 0) {                                                                                              \
+        mol_list_kernel<0, NSV><<<blocks, threads, 0, st>>>(                                                      \
+            gate, c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, use_xm, cell, d_cutskin2, s.atm_typ, s.charge,      \
+            s.inter_map, s.has_vdw, c->d_reach, c->d_mcount, nullptr, nullptr, nullptr, nullptr, 0, nullptr);    \
+        mol_scan_kernel<<<1, 1024, 0, st>>>(gate, c->nmol, c->d_mcount, c->d_mrow, c->d_tot + 2);                 \
+    } else {                                                                                                      \
+        mol_list_kernel<1, NSV><<<blocks, threads, 0, st>>>(                                                      \
+            gate, c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, use_xm, cell, d_cutskin2, s.atm_typ, s.charge,      \
+            s.inter_map, s.has_vdw, c->d_reach, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_mmaskf,         \
+            c->mlist_cap, (unsigned long long *)(c->d_tot + 3));                                                  \
     }
     if (c->mol_ns == 3) { MOL_LIST(3) }
     else if (c->mol_ns == 4) { MOL_LIST(4) }
     else return cudaErrorInvalidValue;
 #undef MOL_LIST
+    return cudaGetLastError();
+}
+
+// Site lists from the molecule list.  pass 0: counts, row offsets, totals
+// (tot[0], tot[1]); pass 1: the fill.
+cudaError_t launch_site_from_mol(pinyb200_ctx *c, int pass, const int *gate, cudaStream_t st)
+{
+    if (!st) st = c->stream;
+    const int threads = 256;
+    int blocks = (c->nmol * 32 + threads - 1) / threads;
+    const int maxb = c->sm_count * 8;
+    if (blocks > maxb) blocks = maxb;
+    if (blocks < 1) blocks = 1;
+    const int natm = c->sys.natm;
+#define SITE_LIST(NSV)                                                                                             \
+    if (pass == 0) {                                                                                               \
+        site_count_kernel<NSV><<<blocks, threads, 0, st>>>(gate, c->nmol, natm, c->d_mstart, c->d_mrow, c->d_mmaskf, \
+                                                           c->d_mmask, c->mlist_cap, c->d_count);                 \
+        scan_kernel<<<1, 1024, 0, st>>>(gate, natm, c->d_count, c->d_row, c->d_rowA, c->d_tot);                   \
+    } else {                                                                                                       \
+        site_fill_kernel<NSV><<<blocks, threads, 0, st>>>(gate, c->nmol, c->d_mstart, c->d_mrow, c->d_mj,          \
+                                                          c->d_mmaskf, c->d_mmask, c->mlist_cap, c->d_row,        \
+                                                          c->d_rowA, c->d_col, c->d_colA, c->list_cap);           \
+    }
+    if (c->mol_ns == 3) { SITE_LIST(3) }
+    else if (c->mol_ns == 4) { SITE_LIST(4) }
+    else return cudaErrorInvalidValue;
+#undef SITE_LIST
     return cudaGetLastError();
 }
 

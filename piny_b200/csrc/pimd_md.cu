@@ -18,6 +18,7 @@
 // energy of each chain is summed with FP64 atomics and the velocities are
 // scaled afterwards.  Layouts: bead arrays [P][natm][3]; chain state
 // [beads of the set][len_nhc][num_nhc].
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -68,45 +69,58 @@ __global__ void nhc_kin_kernel(const double *__restrict__ v, int nb, int natm, c
     atomicAdd(&kin[(size_t)b * (num + 1) + inhc[d * natm + i]], e);
 }
 
-__global__ void nhc_chain_kernel(ChainArgs a)
+// One thread per chain; LEN links known at compile time, so the chain stays
+// in registers.
+template <int LEN>
+__global__ void __launch_bounds__(128) nhc_chain_kernel(ChainArgs a)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)a.nb * a.num) return;
     const int b = (int)(t / a.num), k = (int)(t - (long long)b * a.num);
-    const int num = a.num, L = a.len - 1;
-    double *x = a.x + (size_t)b * a.len * num + k;
-    double *v = a.v + (size_t)b * a.len * num + k;
-    double vn[kMaxLen], f[kMaxLen], ms[kMaxLen], gk[kMaxLen];
+    const int num = a.num;
+    constexpr int L = LEN - 1;
+    double *x = a.x + (size_t)b * LEN * num + k;
+    double *v = a.v + (size_t)b * LEN * num + k;
+    double vn[LEN], f[LEN], ms[LEN], gk[LEN], xs[LEN];
+#pragma unroll
     for (int c = 0; c <= L; c++) {
         vn[c] = v[(size_t)c * num];
+        xs[c] = x[(size_t)c * num];
         ms[c] = a.mass[(size_t)c * num + k];
         gk[c] = a.gkt[(size_t)c * num + k];
     }
     double kin = a.kin[(size_t)b * (num + 1) + k], sc = 1.0;
     f[0] = (kin - gk[0]) / ms[0];
+#pragma unroll
     for (int c = 0; c < L; c++) f[c + 1] = (ms[c] * vn[c] * vn[c] - gk[c + 1]) / ms[c + 1];
-    double xs[kMaxLen];
-    for (int c = 0; c <= L; c++) xs[c] = x[(size_t)c * num];
     for (int r = 0; r < a.nres; r++)
         for (int y = 0; y < a.nyosh; y++) {
             const double w2 = a.w[y] / 2.0, w4 = a.w[y] / 4.0, w8 = a.w[y] / 8.0;
             vn[L] += f[L] * w4;
+            // the upward sweep needs exp(-w8 v[c+1]) of the same v[c+1] as
+            // the downward one (nothing changes it in between): keep them
+            double ex[LEN];
+#pragma unroll
             for (int c = L - 1; c >= 0; c--) {
                 const double aa = exp(-w8 * vn[c + 1]);
+                ex[c] = aa;
                 vn[c] = vn[c] * aa * aa + w4 * f[c] * aa;
             }
             const double aa = exp(-w2 * vn[0]);
             sc *= aa;
             kin *= aa * aa;
+#pragma unroll
             for (int c = 0; c <= L; c++) xs[c] += vn[c] * w2;
             f[0] = (kin - gk[0]) / ms[0];
+#pragma unroll
             for (int c = 0; c < L; c++) {
-                const double ab = exp(-w8 * vn[c + 1]);
+                const double ab = ex[c];
                 vn[c] = vn[c] * ab * ab + w4 * f[c] * ab;
                 f[c + 1] = (ms[c] * vn[c] * vn[c] - gk[c + 1]) / ms[c + 1];
             }
             vn[L] += f[L] * w4;
         }
+#pragma unroll
     for (int c = 0; c <= L; c++) {
         x[(size_t)c * num] = xs[c];
         v[(size_t)c * num] = vn[c];
@@ -270,6 +284,7 @@ struct pinyb200_pimd {
     double *d_mass = nullptr, *d_bmass = nullptr, *d_prekf = nullptr, *d_veig = nullptr;
     double *d_fm = nullptr, *d_u = nullptr, *d_xmod = nullptr, *d_acc = nullptr;
     double *h_acc = nullptr;
+    double *h_facc = nullptr;  // the force path's per-bead sums (pinned)
     NhcDev set[2];  // 0: class (bead 1), 1: bead (beads 2..P)
     std::string err;
 };
@@ -356,7 +371,17 @@ int apply_nhc(pinyb200_pimd *pm, NhcDev &s, double *d_v, int bead0, const double
     a.v = s.v;
     a.kin = s.kin;
     a.sc = s.sc;
-    nhc_chain_kernel<<<blocks_for((long long)s.nb * s.num, 128), 128, 0, st>>>(a);
+    const unsigned nbk = blocks_for((long long)s.nb * s.num, 128);
+    switch (s.len) {
+    case 1: nhc_chain_kernel<1><<<nbk, 128, 0, st>>>(a); break;
+    case 2: nhc_chain_kernel<2><<<nbk, 128, 0, st>>>(a); break;
+    case 3: nhc_chain_kernel<3><<<nbk, 128, 0, st>>>(a); break;
+    case 4: nhc_chain_kernel<4><<<nbk, 128, 0, st>>>(a); break;
+    case 5: nhc_chain_kernel<5><<<nbk, 128, 0, st>>>(a); break;
+    case 6: nhc_chain_kernel<6><<<nbk, 128, 0, st>>>(a); break;
+    case 7: nhc_chain_kernel<7><<<nbk, 128, 0, st>>>(a); break;
+    default: nhc_chain_kernel<8><<<nbk, 128, 0, st>>>(a); break;
+    }
     nhc_scale_kernel<<<blocks_for(n, 256), 256, 0, st>>>(v, s.nb, pm->natm, s.inhc, s.sc, s.num);
     PCK(cudaGetLastError());
     return PINYB200_OK;
@@ -379,13 +404,18 @@ int ghost_positions(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, cudaStream_
     return PINYB200_OK;
 }
 
-// Force path and post-processing; springs already in d_fm and acc.
-int forces_core(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, const double *d_xmod, double *d_f,
-                const double *hmat, pinyb200_pimd_energies *e, cudaStream_t st)
+// Force path and post-processing, enqueued on st (springs already in d_fm
+// and acc): the force evaluation, forces / P with the centroid virial sums,
+// forces to modes, springs added, and the sums copied to the host.  Nothing
+// waits here; pimd_finish does, once per call.
+int forces_enqueue(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, const double *d_xmod, double *d_f,
+                   const pinyb200::Cell &cell, cudaStream_t st)
 {
-    pinyb200_energies fe;
-    int rc = pinyb200_energy_force_device(c, d_x, pm->P > 1 ? d_xmod : nullptr, hmat, PINYB200_DISTRIB_GHOSTS, d_f,
-                                          &fe, st);
+    cudaStream_t own = c->stream;
+    c->stream = st;  // the evaluation runs on the caller's stream
+    int rc = pinyb200::enqueue_device(c, d_x, pm->P > 1 ? d_xmod : nullptr, cell, PINYB200_DISTRIB_GHOSTS, d_f, true,
+                                      pm->h_facc);
+    c->stream = own;
     if (rc) return rc;
     const long long nb = (long long)pm->natm * pm->P, n = nb * 3;
     post_kernel<<<blocks_for(nb, 256), 256, 0, st>>>(d_f, d_x, d_xmod, pm->natm, pm->P, pm->P > 1, pm->d_acc);
@@ -397,7 +427,23 @@ int forces_core(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, const double *d
     add_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_f, pm->d_fm, n);
     PCK(cudaGetLastError());
     PCK(cudaMemcpyAsync(pm->h_acc, pm->d_acc, sizeof(double) * A_N, cudaMemcpyDeviceToHost, st));
+    return PINYB200_OK;
+}
+
+// Wait for st, then the energies: the force path's bookkeeping
+// (evaluate_finish) and the PIMD sums.
+int pimd_finish(pinyb200_pimd *pm, pinyb200_ctx *c, const pinyb200::Cell &cell, pinyb200_pimd_energies *e,
+                cudaStream_t st)
+{
     PCK(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]);
+    cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]);
+    cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]);
+    pinyb200_energies fe;
+    pinyb200::evaluate_finish(c, cell, PINYB200_DISTRIB_GHOSTS, pm->h_facc, &fe);
+    if (!std::isfinite(fe.vintert + fe.vintrat))
+        return pimd_fail(pm, PINYB200_ERR_NAN, "pimd: non-finite energy (positions, or a list that outgrew its room)");
     if (e) {
         const double *a = pm->h_acc;
         e->force = fe;
@@ -431,6 +477,8 @@ int check_ctx(pinyb200_pimd *pm, pinyb200_ctx *c)
     if (!pm || !c) return pimd_fail(pm, PINYB200_ERR_ARG, "pimd: null handle");
     if (c->sys.natm != pm->natm || c->P != pm->P)
         return pimd_fail(pm, PINYB200_ERR_ARG, "pimd: force context has other sites or beads");
+    if (!c->have_list) return pimd_fail(pm, PINYB200_ERR_STATE, "pimd: build the force context's list first");
+    if (cudaSetDevice(c->device) != cudaSuccess) return pimd_fail(pm, PINYB200_ERR_CUDA, "pimd: cannot select the device");
     return PINYB200_OK;
 }
 
@@ -475,6 +523,7 @@ int pinyb200_pimd_create(const pinyb200_pimd_setup *s, pinyb200_pimd **out)
     CCK(cudaMalloc(&pm->d_xmod, sizeof(double) * na * 3));
     CCK(cudaMalloc(&pm->d_acc, sizeof(double) * A_N));
     CCK(cudaMallocHost(&pm->h_acc, sizeof(double) * A_N));
+    CCK(cudaMallocHost(&pm->h_facc, sizeof(double) * (size_t)s->nbeads * pinyb200::S_NSLOT));
     CCK(cudaMemcpy(pm->d_mass, s->mass, sizeof(double) * na, cudaMemcpyHostToDevice));
     CCK(cudaMemcpy(pm->d_bmass, s->bead_mass, sizeof(double) * nb, cudaMemcpyHostToDevice));
     CCK(cudaMemcpy(pm->d_prekf, s->prekf, sizeof(double) * na, cudaMemcpyHostToDevice));
@@ -499,6 +548,7 @@ int pinyb200_pimd_destroy(pinyb200_pimd *pm)
     cudaFree(pm->d_xmod);
     cudaFree(pm->d_acc);
     cudaFreeHost(pm->h_acc);
+    cudaFreeHost(pm->h_facc);
     free_set(pm->set[0]);
     free_set(pm->set[1]);
     delete pm;
@@ -541,7 +591,9 @@ int pinyb200_pimd_forces(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double
         return rc;
     PCK(cudaMemsetAsync(pm->d_acc, 0, sizeof(double) * A_N, st));
     if ((rc = springs(pm, pm->d_u, st))) return rc;
-    return forces_core(pm, c, d_x, pm->d_u, d_f, hmat, e, st);
+    const pinyb200::Cell cell = pinyb200::cell_from_hmat(hmat);
+    if ((rc = forces_enqueue(pm, c, d_x, pm->d_u, d_f, cell, st))) return rc;
+    return pimd_finish(pm, c, cell, e, st);
 }
 
 int pinyb200_pimd_step(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double *d_v, double *d_f, const double *hmat,
@@ -567,16 +619,15 @@ int pinyb200_pimd_step(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double *
     if (pm->P > 1 && (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_BEADS, d_x, st))) return rc;
     if ((rc = ghost_positions(pm, c, d_x, st))) return rc;
     // PINY's list test and, when due, the rebuild -- on the device
-    if ((rc = pinyb200::list_update_enqueue(c, d_x, pm->P > 1 ? pm->d_xmod : nullptr, pinyb200::cell_from_hmat(hmat), st)))
-        return rc;
+    const pinyb200::Cell cell = pinyb200::cell_from_hmat(hmat);
+    if ((rc = pinyb200::list_update_enqueue(c, d_x, pm->P > 1 ? pm->d_xmod : nullptr, cell, st))) return rc;
     // forces of the new positions, as mode forces
-    if ((rc = forces_core(pm, c, d_x, pm->d_xmod, d_f, hmat, e, st))) return rc;
+    if ((rc = forces_enqueue(pm, c, d_x, pm->d_xmod, d_f, cell, st))) return rc;
     // dt/2 -> dt: half kick, chains
     kick_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_v, d_f, pm->d_bmass, n, dt2);
     PCK(cudaGetLastError());
     if ((rc = apply_all_nhc(pm, d_v, st))) return rc;
-    PCK(cudaStreamSynchronize(st));
-    return PINYB200_OK;
+    return pimd_finish(pm, c, cell, e, st);
 }
 
 }  // extern "C"

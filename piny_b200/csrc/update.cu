@@ -1,8 +1,9 @@
 // PINY's per-step Verlet list update entirely on the device: the rebuild
 // test of check_ver_list (nbr_list_control.c:182-247) with the PIMD spread
 // and get_cut_skin (:249-281), and, when the test fires, the list build of
-// verlist_control (verlist_control.c:30-128) -- site list, molecule-pair
-// list and its work chunks -- gated on the device flag, so a step needs no
+// verlist_control (verlist_control.c:30-128) -- molecule-pair list, the
+// site lists expanded from it, and the work chunks (or the site list alone
+// for systems without such molecules) -- gated on the device flag, so a step needs no
 // host round trip and can sit inside a CUDA graph.  The reserved capacities
 // of the last host build bound the device builds; a build that would not
 // fit sets a sticky flag, writes nothing past the reservation, and the pair
@@ -134,6 +135,7 @@ int list_update_prepare(pinyb200_ctx *c)
     if (e == cudaSuccess) e = cudaMemset(c->d_ls, 0, sizeof(ListState));
     if (e == cudaSuccess) e = cudaMalloc(&c->d_cs, sizeof(double) * (size_t)c->sys.npair_typ);
     if (e == cudaSuccess && c->nmol > 0) e = cudaMalloc(&c->d_mchunk, sizeof(int) * (2 * (size_t)c->nmol + 1));
+    if (e == cudaSuccess && c->use_mol && !c->d_reach) e = cudaMalloc(&c->d_reach, sizeof(double));
     if (e != cudaSuccess) return record_error(c, PINYB200_ERR_CUDA, std::string("list update: ") + cudaGetErrorString(e));
     return PINYB200_OK;
 }
@@ -155,13 +157,13 @@ int list_update_enqueue(pinyb200_ctx *c, const double *d_pos, const double *d_xm
     ls_decide_kernel<<<1, 64, 0, st>>>(ls, c->P, c->skin, c->sys.npair_typ, c->sys.cutoff, c->d_cs);
     ls_prep_kernel<<<1, 1, 0, st>>>(gate, c->d_tot, chunk_tot);
     const double *xm = c->P > 1 ? d_xm : nullptr;
-    if ((e = launch_build_list(c, cell, d_pos, xm, c->d_cs, 0, gate, st)) != cudaSuccess ||
-        (e = launch_build_list(c, cell, d_pos, xm, c->d_cs, 1, gate, st)) != cudaSuccess)
-        return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
-    const bool mol = c->use_mol && c->d_chunk && c->d_nchunk;
+    const bool mol = c->use_mol && c->d_mj && c->d_chunk && c->d_nchunk;
     if (mol) {
+        // molecule-pair list, the site lists expanded from its masks, chunks
         if ((e = launch_mol_list(c, cell, d_pos, xm, c->d_cs, 0, gate, st)) != cudaSuccess ||
-            (e = launch_mol_list(c, cell, d_pos, xm, c->d_cs, 1, gate, st)) != cudaSuccess)
+            (e = launch_mol_list(c, cell, d_pos, xm, c->d_cs, 1, gate, st)) != cudaSuccess ||
+            (e = launch_site_from_mol(c, 0, gate, st)) != cudaSuccess ||
+            (e = launch_site_from_mol(c, 1, gate, st)) != cudaSuccess)
             return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
         const int jpi = c->P >= 32 ? 1 : 32 / c->P;
         const int ch = PINYB200_MOL_CHUNK * jpi;
@@ -170,6 +172,9 @@ int list_update_enqueue(pinyb200_ctx *c, const double *d_pos, const double *d_xm
         mol_scan_kernel<<<1, 1024, 0, st>>>(gate, c->nmol, c->d_mchunk, c->d_mchunk + c->nmol, chunk_tot);
         ls_chunk_fill_kernel<<<blocks, 256, 0, st>>>(gate, c->nmol, c->d_mrow, ch, c->d_mchunk,
                                                      c->d_mchunk + c->nmol, c->d_chunk, c->chunk_cap);
+    } else if ((e = launch_build_list(c, cell, d_pos, xm, c->d_cs, 0, gate, st)) != cudaSuccess ||
+               (e = launch_build_list(c, cell, d_pos, xm, c->d_cs, 1, gate, st)) != cudaSuccess) {
+        return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
     }
     ls_finish_kernel<<<1, 1, 0, st>>>(gate, ls, c->d_tot, chunk_tot, c->list_cap, c->mlist_cap, c->chunk_cap,
                                       mol ? 1 : 0, c->d_nchunk);
@@ -201,7 +206,9 @@ int list_sync_counts(pinyb200_ctx *c)
     cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e == cudaSuccess) e = cudaMemcpy(&h, c->d_ls, sizeof(h), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
-    if (h.rebuilds > 0) {
+    if (h.overflow) {  // the rows were emptied
+        c->npairs = c->nactive = c->nmp = 0;
+    } else if (h.rebuilds > 0) {
         c->npairs = h.site_tot[0];
         c->nactive = h.site_tot[1];
         c->nmp = h.mol_tot[0];
