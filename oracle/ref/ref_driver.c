@@ -26,6 +26,10 @@
  *                 nres_nhc, nyosh, inhc[3][natm] (1-based, num_nhc+1 null);
  *                 doubles dti, mass[natm], v[natm][3], mass_nhc, gkt, x_nhc,
  *                 v_nhc (each [len_nhc][num_nhc]).
+ *   piny_ref io <dir> <input> <outdir> <binary 0|1>   after one evaluation,
+ *                 PINY's restart dump (write_dump_file_pimd, output_pimd.c:786)
+ *                 and configuration files (write_config_files_pimd, :1093)
+ *                 into <outdir>, and <outdir>/state.bin with what they hold.
  *   piny_ref springs <in.bin> <out.bin>  mode_energy_control
  *                 (pimd_estimators.c:31) on modes u, then pimd_pvten_forc_corr
  *                 (pimd_estimators.c:223) on positions x with forces f (also
@@ -65,7 +69,7 @@ static void put(const char *name, char kind, const void *data, int64_t n)
     hdr[32] = kind;
     fwrite(hdr, 1, 40, g_out);
     fwrite(&n, sizeof(int64_t), 1, g_out);
-    if (n > 0) fwrite(data, kind == 'd' ? 8 : 4, (size_t)n, g_out);
+    if (n > 0) fwrite(data, kind == 'd' ? 8 : kind == 'c' ? 1 : 4, (size_t)n, g_out);
 }
 static void putd(const char *name, const double *one_based, int64_t n) { put(name, 'd', one_based + 1, n); }
 static void puti(const char *name, const int *one_based, int64_t n) { put(name, 'i', one_based + 1, n); }
@@ -658,8 +662,101 @@ static int run_springs(const char *inpath, const char *outpath)
     return 0;
 }
 
+void write_dump_file_pimd(CLASS *, BONDED *, GENERAL_DATA *);
+void write_config_files_pimd(CLASS *, BONDED *, GENERAL_DATA *);
+
+static char *path_in(const char *dir, const char *name)
+{
+    char *p = malloc(strlen(dir) + strlen(name) + 2);
+    sprintf(p, "%s/%s", dir, name);
+    return p;
+}
+
+static int run_io(const char *dir, const char *input, const char *outdir_rel, int binary)
+{
+    char *outdir = realpath(outdir_rel, NULL);
+    if (!outdir) return 2;
+    setup(dir, input);
+    evaluate();
+    CLASS *cl = &class_;
+    GENERAL_DATA *g = &gd_;
+    const int P = cl->clatoms_info.pi_beads, n = cl->clatoms_info.natm_tot;
+    g->filenames.dname = path_in(outdir, "dump");
+    g->filenames.cpname = path_in(outdir, "conf_pos");
+    g->filenames.cvname = path_in(outdir, "conf_vel");
+    g->filenames.centname = path_in(outdir, "conf_cent");
+    g->filenames.forcename = path_in(outdir, "conf_force");
+    g->filenames.cpparname = path_in(outdir, "conf_par");
+    g->filenames.iwrite_confp = g->filenames.iwrite_confv = g->filenames.iwrite_path_cent = 1;
+    g->filenames.iwrite_atm_for = g->filenames.iwrite_par_confp = 1;
+    g->filenames.low_lim_par = 2;
+    g->filenames.high_lim_par = n < 6 ? n : 6;
+    g->filenames.iwrite_conf_binary = binary;
+    g->timeinfo.itime = 0;
+    write_dump_file_pimd(cl, &bonded_, g);
+    write_config_files_pimd(cl, &bonded_, g);
+
+    g_out = fopen(path_in(outdir, "state.bin"), "wb");
+    if (!g_out) return 2;
+    double *buf = malloc(sizeof(double) * 3 * (size_t)n * P);
+    const char *what[3] = {"pos", "vel", "fxt"};
+    for (int w = 0; w < 3; w++) {
+        for (int b = 0; b < P; b++)
+            for (int i = 0; i < n; i++) {
+                CLATOMS_POS *cp = &cl->clatoms_pos[b + 1];
+                const double *x = w == 0 ? cp->x : w == 1 ? cp->vx : cp->fxt, *y = w == 0 ? cp->y : w == 1 ? cp->vy : cp->fyt,
+                             *z = w == 0 ? cp->z : w == 1 ? cp->vz : cp->fzt;
+                buf[((size_t)b * n + i) * 3 + 0] = x[i + 1];
+                buf[((size_t)b * n + i) * 3 + 1] = y[i + 1];
+                buf[((size_t)b * n + i) * 3 + 2] = z[i + 1];
+            }
+        put(what[w], 'd', buf, 3 * (int64_t)n * P);
+    }
+    putd("hmat", g->cell.hmat, 9);
+    putd("hmat_ewd", g->cell.hmat_ewd, 9);
+    putd("vgmat", g->par_rahman.vgmat, 9);
+    put1d("x_lnv", g->baro.x_lnv);
+    put1d("v_lnv", g->baro.v_lnv);
+    put1d("dt", g->timeinfo.dt);
+    put1d("t_ext", g->statepoint.t_ext);
+    put1d("pext", g->statepoint.pext);
+    put1d("stens_ext", g->statepoint.stens_ext);
+    put1i("nfree", cl->clatoms_info.nfree);
+    int ens[5] = {g->ensopts.nve, g->ensopts.nvt, g->ensopts.npt_i, g->ensopts.npt_f, g->ensopts.nst};
+    put("ens", 'i', ens, 5);
+    int fr[3] = {bonded_.bond_free.num, bonded_.bend_free.num, bonded_.tors_free.num};
+    put("free", 'i', fr, 3);
+    const int cn = cl->therm_info_class.num_nhc, cl_len = cl->therm_info_class.len_nhc;
+    const int bn = cl->therm_info_bead.num_nhc, bl = cl->therm_info_bead.len_nhc;
+    int nh[4] = {cn, cl_len, bn, bl};
+    put("nhc_dims", 'i', nh, 4);
+    double *v = malloc(sizeof(double) * ((size_t)cn * cl_len + (size_t)bn * bl * P + cl_len + 1));
+    size_t k = 0;
+    for (int j = 1; j <= cl_len; j++)
+        for (int i = 1; i <= cn; i++) v[k++] = cl->therm_class.v_nhc[j][i];
+    put("class_v_nhc", 'd', v, (int64_t)k);
+    k = 0;
+    for (int b = 2; b <= P; b++)
+        for (int j = 1; j <= bl; j++)
+            for (int i = 1; i <= bn; i++) v[k++] = cl->therm_bead[b].v_nhc[j][i];
+    put("bead_v_nhc", 'd', v, (int64_t)k);
+    putd("v_vol_nhc", g->baro.v_vol_nhc, cl_len);
+    /* names: atom, residue, molecule type of each atom, then molecule numbers */
+    char *names = malloc((size_t)n * 3 * 64 + 1);
+    size_t off = 0;
+    for (int i = 1; i <= n; i++)
+        off += sprintf(names + off, "%s %s %s\n", cl->atommaps.atm_typ[cl->atommaps.iatm_atm_typ[i]],
+                       cl->atommaps.res_typ[cl->atommaps.iatm_res_typ[i]],
+                       cl->atommaps.mol_typ[cl->atommaps.iatm_mol_typ[i]]);
+    put("names", 'c', names, (int64_t)off);
+    puti("mol_num", cl->atommaps.iatm_mol_num, n);
+    fclose(g_out);
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
+    if (argc == 6 && strcmp(argv[1], "io") == 0) return run_io(argv[2], argv[3], argv[4], atoi(argv[5]));
     if (argc == 4 && strcmp(argv[1], "nhc") == 0) return run_nhc(argv[2], argv[3]);
     if (argc == 4 && strcmp(argv[1], "springs") == 0) return run_springs(argv[2], argv[3]);
     if (argc == 5 && strcmp(argv[1], "pimd") == 0) return run_pimd(atoi(argv[2]), argv[3], argv[4]);

@@ -11,7 +11,9 @@ and stores, per configuration, a compressed .npz with
 * PINY's outputs (per-bead forces before and after the M-site
   redistribution, energy components, pressure tensor, the Verlet pair set).
 
-pimd_md.npz holds PINY's Nose-Hoover chain operator and its spring and
+piny_io.npz holds PINY's restart dump and configuration files (text and
+binary) for tip4pf_64_p4 with the state they were written from
+(``piny_ref io``).  pimd_md.npz holds PINY's Nose-Hoover chain operator and its spring and
 centroid-virial routines (``piny_ref nhc`` / ``piny_ref springs``) on seeded
 inputs.  It also stores pimd_transforms.npz: PINY's own ring-polymer transforms
 (``piny_ref pimd``: path_integral_init, convert_pimd_mode/pos/force_* of
@@ -53,6 +55,9 @@ def read_dump(path):
             name = h[:32].split(b"\0")[0].decode()
             kind = chr(h[32])
             n = struct.unpack("<q", f.read(8))[0]
+            if kind == "c":
+                out[name] = f.read(n).decode()
+                continue
             dt = np.float64 if kind == "d" else np.int32
             out[name] = np.frombuffer(f.read(n * np.dtype(dt).itemsize), dtype=dt).copy()
     return out
@@ -305,12 +310,45 @@ def pimd_md_fixture(tmp):
     print("pimd_md", os.path.getsize(path), "bytes")
 
 
+IO_FILES = ("dump", "conf_pos", "conf_vel", "conf_cent", "conf_force", "conf_par")
+
+
+def io_fixture(tmp):
+    """PINY's restart dump and configuration files (``piny_ref io``: after one
+    evaluation of tip4pf_64_p4, write_dump_file_pimd and
+    write_config_files_pimd, text and binary) with the state they hold."""
+    spec = [s for n, s, k in golden_specs() if n == "tip4pf_64_p4"][0]
+    pos = water.build_positions(spec)
+    out = {}
+    for binary in (0, 1):
+        d = os.path.join(tmp, "io_inp%d" % binary)
+        shutil.rmtree(d, ignore_errors=True)
+        water.write_piny_input(d, spec, pos)
+        od = os.path.join(tmp, "io_out%d" % binary)
+        shutil.rmtree(od, ignore_errors=True)
+        os.makedirs(od)
+        subprocess.run([PINY_REF, "io", d, "water.input", od, str(binary)], check=True, capture_output=True)
+        if binary == 0:
+            D = read_dump(os.path.join(od, "state.bin"))
+            for k, v in D.items():
+                out["state_" + k] = np.asarray(v)
+        for f in IO_FILES:
+            if binary == 1 and f == "dump":
+                continue
+            with open(os.path.join(od, f), "rb") as fh:
+                out["file%d_%s" % (binary, f)] = np.frombuffer(fh.read(), np.uint8)
+    path = os.path.join(HERE, "piny_io.npz")
+    np.savez_compressed(path, **out)
+    print("piny_io", os.path.getsize(path), "bytes")
+
+
 def main():
     if not os.path.exists(PINY_REF):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     tmp = tempfile.mkdtemp(prefix="piny_golden_")
     pimd_fixture(tmp)
     pimd_md_fixture(tmp)
+    io_fixture(tmp)
     if "--pimd-only" in sys.argv[1:]:
         shutil.rmtree(tmp, ignore_errors=True)
         return
