@@ -834,29 +834,33 @@ __global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) conv_c_kernel(typename Cp
     }
     __syncthreads();
     line_fft<R, NF>(sl, Nc, Nh, 1, ls, tc, +1);
+    // per-point energy and virial terms in R (FP32 for MIXED), summed in FP64
     double e = 0, pxx = 0, pyy = 0, pzz = 0, pxy = 0, pxz = 0, pyz = 0;
-    const double kb = b <= Nb / 2 ? b : b - Nb;
-    const double tpi = 2.0 * M_PI, falp2 = 4.0 * alp * alp;
+    const R kb = (R)(b <= Nb / 2 ? b : b - Nb);
+    const R tpi = (R)(2.0 * M_PI), falp2 = (R)(4.0 * alp * alp);
+    R hi[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) hi[k] = (R)cell.hi[k];
     for (int idx = threadIdx.x; idx < Nc * Nh; idx += blockDim.x) {
         const int c = idx / Nh, a = idx % Nh;
         const R w = filt[((size_t)c * Nb + b) * Na + a];
         C2 s = sl[c * ls + a];
         if (w != (R)0 && energy) {
-            const double ka = a, kc = c <= Nc / 2 ? c : c - Nc;
-            const double xk = tpi * (ka * cell.hi[0] + kb * cell.hi[1] + kc * cell.hi[2]);
-            const double yk = tpi * (ka * cell.hi[3] + kb * cell.hi[4] + kc * cell.hi[5]);
-            const double zk = tpi * (ka * cell.hi[6] + kb * cell.hi[7] + kc * cell.hi[8]);
-            const double g2 = xk * xk + yk * yk + zk * zk;
-            const double mult = (a == 0 || 2 * a == Na) ? 0.5 : 1.0;
-            const double sm = mult * ((double)s.x * (double)s.x + (double)s.y * (double)s.y) * (double)w;
-            const double prep = -2.0 * ((g2 / falp2) + 1.0) / g2 * sm;
-            e += sm;
-            pxx += prep * xk * xk;
-            pyy += prep * yk * yk;
-            pzz += prep * zk * zk;
-            pxy += prep * xk * yk;
-            pxz += prep * xk * zk;
-            pyz += prep * yk * zk;
+            const R ka = (R)a, kc = (R)(c <= Nc / 2 ? c : c - Nc);
+            const R xk = tpi * (ka * hi[0] + kb * hi[1] + kc * hi[2]);
+            const R yk = tpi * (ka * hi[3] + kb * hi[4] + kc * hi[5]);
+            const R zk = tpi * (ka * hi[6] + kb * hi[7] + kc * hi[8]);
+            const R g2 = xk * xk + yk * yk + zk * zk;
+            const R mult = (a == 0 || 2 * a == Na) ? (R)0.5 : (R)1.0;
+            const R sm = mult * (s.x * s.x + s.y * s.y) * w;
+            const R prep = (R)-2.0 * ((g2 / falp2) + (R)1.0) / g2 * sm;
+            e += (double)sm;
+            pxx += (double)(prep * xk * xk);
+            pyy += (double)(prep * yk * yk);
+            pzz += (double)(prep * zk * zk);
+            pxy += (double)(prep * xk * yk);
+            pxz += (double)(prep * xk * zk);
+            pyz += (double)(prep * yk * zk);
         }
         s.x *= w;
         s.y *= w;
