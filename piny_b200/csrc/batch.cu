@@ -57,6 +57,7 @@ int set_choice(pinyb200_ctx *c, const int *ch)
     c->pair_variant = ch[1];
     c->pair_blocks_per_sm = ch[2];
     c->pme_overlap = ch[3] != 0;
+    c->gen++;
     return PINYB200_OK;
 }
 
@@ -261,6 +262,7 @@ int pinyb200_batch_energy_force_device(pinyb200_batch *bt, const double *const *
         kp.push_back(d_xmod ? d_xmod[i] : nullptr);
         kp.push_back(d_force[i]);
         kh.insert(kh.end(), hmat[i], hmat[i] + 9);
+        kh.push_back((double)bt->box[i]->gen);  // a list build or retune invalidates the graph
     }
     if (!bt->exec || kp != bt->key_ptr || kh != bt->key_h || flags != bt->key_flags) {
         drop_graph(bt);

@@ -182,6 +182,7 @@ static int pme_tiles_setup(pinyb200_ctx *c, int T)
     const int N[3] = {c->sys.ngrid[0], c->sys.ngrid[1], c->sys.ngrid[2]};
     for (int d = 0; d < 3; d++) c->pme_nt[d] = (N[d] + T - 1) / T;
     c->pme_tile = T;
+    c->gen++;
     c->pme_ntile = c->pme_nt[0] * c->pme_nt[1] * c->pme_nt[2];
     const int mean = (c->sys.nchrg + c->pme_ntile - 1) / c->pme_ntile;
     c->pme_cap = (2 * mean + 32 + 31) / 32 * 32;
@@ -506,6 +507,7 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
 {
     if (!c || !pos1 || !hmat || !cutskin2) return fail(c, PINYB200_ERR_ARG, "build_list: NULL argument");
     CK(cudaSetDevice(c->device));
+    c->gen++;  // the list arrays may move
     const int natm = c->sys.natm;
     Cell cell = make_cell(hmat);
     double *d_p1 = c->d_pos_aos;  // bead-1 positions in the staging buffer

@@ -205,6 +205,9 @@ struct pinyb200_ctx {
     bool filter_ok = false;
     cudaEvent_t ev[8];
     float last_ms[5] = {0, 0, 0, 0, 0};
+    // bumped whenever launch shapes or device buffers may change (list
+    // builds, tuning, PME tiles): captured graphs compare it before replay
+    unsigned long long gen = 0;
     pinyb200::GradHost grad;      // tangent channels of pinyb200_grad_prepare
     std::string err;
 };

@@ -19,6 +19,7 @@
 // scaled afterwards.  Layouts: bead arrays [P][natm][3]; chain state
 // [beads of the set][len_nhc][num_nhc].
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -285,7 +286,14 @@ struct pinyb200_pimd {
     double *d_fm = nullptr, *d_u = nullptr, *d_xmod = nullptr, *d_acc = nullptr;
     double *h_acc = nullptr;
     double *h_facc = nullptr;  // the force path's per-bead sums (pinned)
-    NhcDev set[2];  // 0: class (bead 1), 1: bead (beads 2..P)
+    NhcDev set[2];
+    // the step as a CUDA graph, for the arguments it was captured with
+    cudaStream_t cap = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<double> key;     // pointers, cell, context and its generation
+    std::vector<double> eager;   // key of the last eager step (the capture follows it)
+    bool graph_mode = false;     // the last step ran as a graph (no per-phase timing)  // 0: class (bead 1), 1: bead (beads 2..P)
     std::string err;
 };
 
@@ -409,11 +417,11 @@ int ghost_positions(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, cudaStream_
 // forces to modes, springs added, and the sums copied to the host.  Nothing
 // waits here; pimd_finish does, once per call.
 int forces_enqueue(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, const double *d_xmod, double *d_f,
-                   const pinyb200::Cell &cell, cudaStream_t st)
+                   const pinyb200::Cell &cell, cudaStream_t st, bool timing)
 {
     cudaStream_t own = c->stream;
     c->stream = st;  // the evaluation runs on the caller's stream
-    int rc = pinyb200::enqueue_device(c, d_x, pm->P > 1 ? d_xmod : nullptr, cell, PINYB200_DISTRIB_GHOSTS, d_f, true,
+    int rc = pinyb200::enqueue_device(c, d_x, pm->P > 1 ? d_xmod : nullptr, cell, PINYB200_DISTRIB_GHOSTS, d_f, timing,
                                       pm->h_facc);
     c->stream = own;
     if (rc) return rc;
@@ -436,10 +444,12 @@ int pimd_finish(pinyb200_pimd *pm, pinyb200_ctx *c, const pinyb200::Cell &cell, 
                 cudaStream_t st)
 {
     PCK(cudaStreamSynchronize(st));
-    cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]);
-    cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]);
-    cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]);
-    cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]);
+    if (!pm->graph_mode) {  // a replayed graph records no phase events
+        cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]);
+        cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]);
+        cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]);
+        cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]);
+    }
     pinyb200_energies fe;
     pinyb200::evaluate_finish(c, cell, PINYB200_DISTRIB_GHOSTS, pm->h_facc, &fe);
     if (!std::isfinite(fe.vintert + fe.vintrat))
@@ -470,6 +480,46 @@ int springs(pinyb200_pimd *pm, const double *d_u, cudaStream_t st)
                                                         pm->d_fm, pm->d_acc);
     PCK(cudaGetLastError());
     return PINYB200_OK;
+}
+
+void drop_graph(pinyb200_pimd *pm)
+{
+    if (pm->exec) cudaGraphExecDestroy(pm->exec);
+    if (pm->graph) cudaGraphDestroy(pm->graph);
+    pm->exec = nullptr;
+    pm->graph = nullptr;
+    pm->key.clear();
+}
+
+// Everything of one step up to the host read of its sums, enqueued on st
+// with no waits (capturable).
+int step_enqueue(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double *d_v, double *d_f,
+                 const pinyb200::Cell &cell, cudaStream_t st, bool timing)
+{
+    int rc;
+    const long long n = (long long)pm->natm * pm->P * 3;
+    const double dt2 = pm->dt / 2.0;
+    // t = 0 -> dt/2: chains, half kick
+    if ((rc = apply_all_nhc(pm, d_v, st))) return rc;
+    kick_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_v, d_f, pm->d_bmass, n, dt2);
+    PCK(cudaGetLastError());
+    // positions -> modes, drift, springs, modes -> positions
+    if (pm->P > 1 && (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_MODES, d_x, st))) return rc;
+    drift_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_x, d_v, n, pm->dt);
+    PCK(cudaGetLastError());
+    PCK(cudaMemsetAsync(pm->d_acc, 0, sizeof(double) * A_N, st));
+    if ((rc = springs(pm, d_x, st))) return rc;
+    PCK(cudaMemcpyAsync(pm->d_xmod, d_x, sizeof(double) * (size_t)pm->natm * 3, cudaMemcpyDeviceToDevice, st));
+    if (pm->P > 1 && (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_BEADS, d_x, st))) return rc;
+    if ((rc = ghost_positions(pm, c, d_x, st))) return rc;
+    // PINY's list test and, when due, the rebuild -- on the device
+    if ((rc = pinyb200::list_update_enqueue(c, d_x, pm->P > 1 ? pm->d_xmod : nullptr, cell, st))) return rc;
+    // forces of the new positions, as mode forces
+    if ((rc = forces_enqueue(pm, c, d_x, pm->d_xmod, d_f, cell, st, timing))) return rc;
+    // dt/2 -> dt: half kick, chains
+    kick_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_v, d_f, pm->d_bmass, n, dt2);
+    PCK(cudaGetLastError());
+    return apply_all_nhc(pm, d_v, st);
 }
 
 int check_ctx(pinyb200_pimd *pm, pinyb200_ctx *c)
@@ -551,6 +601,8 @@ int pinyb200_pimd_destroy(pinyb200_pimd *pm)
     cudaFreeHost(pm->h_facc);
     free_set(pm->set[0]);
     free_set(pm->set[1]);
+    drop_graph(pm);
+    if (pm->cap) cudaStreamDestroy(pm->cap);
     delete pm;
     return PINYB200_OK;
 }
@@ -592,7 +644,8 @@ int pinyb200_pimd_forces(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double
     PCK(cudaMemsetAsync(pm->d_acc, 0, sizeof(double) * A_N, st));
     if ((rc = springs(pm, pm->d_u, st))) return rc;
     const pinyb200::Cell cell = pinyb200::cell_from_hmat(hmat);
-    if ((rc = forces_enqueue(pm, c, d_x, pm->d_u, d_f, cell, st))) return rc;
+    if ((rc = forces_enqueue(pm, c, d_x, pm->d_u, d_f, cell, st, true))) return rc;
+    pm->graph_mode = false;
     return pimd_finish(pm, c, cell, e, st);
 }
 
@@ -603,30 +656,36 @@ int pinyb200_pimd_step(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double *
     if (rc) return rc;
     if (!d_x || !d_v || !d_f || !hmat) return pimd_fail(pm, PINYB200_ERR_ARG, "pimd_step: null pointer");
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;  // NULL: the force context's stream
-    const long long n = (long long)pm->natm * pm->P * 3;
-    const double dt2 = pm->dt / 2.0;
-    // t = 0 -> dt/2: chains, half kick
-    if ((rc = apply_all_nhc(pm, d_v, st))) return rc;
-    kick_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_v, d_f, pm->d_bmass, n, dt2);
-    PCK(cudaGetLastError());
-    // positions -> modes, drift, springs, modes -> positions
-    if (pm->P > 1 && (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_MODES, d_x, st))) return rc;
-    drift_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_x, d_v, n, pm->dt);
-    PCK(cudaGetLastError());
-    PCK(cudaMemsetAsync(pm->d_acc, 0, sizeof(double) * A_N, st));
-    if ((rc = springs(pm, d_x, st))) return rc;
-    PCK(cudaMemcpyAsync(pm->d_xmod, d_x, sizeof(double) * (size_t)pm->natm * 3, cudaMemcpyDeviceToDevice, st));
-    if (pm->P > 1 && (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_BEADS, d_x, st))) return rc;
-    if ((rc = ghost_positions(pm, c, d_x, st))) return rc;
-    // PINY's list test and, when due, the rebuild -- on the device
     const pinyb200::Cell cell = pinyb200::cell_from_hmat(hmat);
-    if ((rc = pinyb200::list_update_enqueue(c, d_x, pm->P > 1 ? pm->d_xmod : nullptr, cell, st))) return rc;
-    // forces of the new positions, as mode forces
-    if ((rc = forces_enqueue(pm, c, d_x, pm->d_xmod, d_f, cell, st))) return rc;
-    // dt/2 -> dt: half kick, chains
-    kick_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_v, d_f, pm->d_bmass, n, dt2);
-    PCK(cudaGetLastError());
-    if ((rc = apply_all_nhc(pm, d_v, st))) return rc;
+    // Steps with the same arguments replay one CUDA graph: the first such
+    // step runs eagerly (it sets up everything the work needs), the second
+    // is captured and launched, later ones are launched.
+    std::vector<double> key = {(double)(uintptr_t)d_x, (double)(uintptr_t)d_v, (double)(uintptr_t)d_f,
+                               (double)(uintptr_t)c, (double)c->gen};
+    key.insert(key.end(), hmat, hmat + 9);
+    if (pm->exec && key != pm->key) drop_graph(pm);
+    if (!pm->exec && key != pm->eager) {
+        if ((rc = step_enqueue(pm, c, d_x, d_v, d_f, cell, st, true))) return rc;
+        pm->eager = key;
+        pm->graph_mode = false;
+        return pimd_finish(pm, c, cell, e, st);
+    }
+    if (!pm->exec) {
+        if (!pm->cap) PCK(cudaStreamCreateWithFlags(&pm->cap, cudaStreamNonBlocking));
+        PCK(cudaStreamBeginCapture(pm->cap, cudaStreamCaptureModeRelaxed));
+        rc = step_enqueue(pm, c, d_x, d_v, d_f, cell, pm->cap, false);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(pm->cap, &g);
+        if (rc || ee != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return rc ? rc : pimd_fail(pm, PINYB200_ERR_CUDA, std::string("pimd step capture: ") + cudaGetErrorString(ee));
+        }
+        pm->graph = g;
+        PCK(cudaGraphInstantiate(&pm->exec, pm->graph, 0));
+        pm->key = key;
+    }
+    PCK(cudaGraphLaunch(pm->exec, st));
+    pm->graph_mode = true;
     return pimd_finish(pm, c, cell, e, st);
 }
 
