@@ -73,7 +73,7 @@ __global__ void nhc_kin_kernel(const double *__restrict__ v, int nb, int natm, c
 // One thread per chain; LEN links known at compile time, so the chain stays
 // in registers.
 template <int LEN>
-__global__ void __launch_bounds__(128) nhc_chain_kernel(ChainArgs a)
+__global__ void __launch_bounds__(128, 6) nhc_chain_kernel(ChainArgs a)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)a.nb * a.num) return;
