@@ -230,6 +230,7 @@ int pinyb200_destroy(pinyb200_ctx *c)
                     c->d_reach};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    if (c->h_acc_pin) cudaFreeHost(c->h_acc_pin);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (void *p : c->grad.dev) cudaFree(p);
@@ -721,23 +722,6 @@ void pinyb200::evaluate_finish(pinyb200_ctx *c, const Cell &cell, int flags, con
     }
 }
 
-static int evaluate(pinyb200_ctx *c, const Cell &cell, int flags, pinyb200_energies *e)
-{
-    const bool energy = !(flags & PINYB200_NO_ENERGY);
-    std::vector<double> acc(energy ? (size_t)c->P * S_NSLOT : 0);
-    int rc = evaluate_enqueue(c, cell, flags, true, energy ? acc.data() : nullptr);
-    if (rc) return rc;
-    CK(cudaStreamSynchronize(c->stream));
-    CK(cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]));
-    CK(cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]));
-    CK(cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]));
-    CK(cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]));
-    evaluate_finish(c, cell, flags, energy ? acc.data() : nullptr, e);
-    if (energy && e && !std::isfinite(e->vintert + e->vintrat))
-        return fail(c, PINYB200_ERR_NAN, "non-finite energy: check the positions (forces were written)");
-    return PINYB200_OK;
-}
-
 // mode-1 positions for a PIMD call without xmod: the bead centroid
 __global__ void centroid_kernel(const double *__restrict__ posT, double *__restrict__ xm, int natm, int P)
 {
@@ -828,13 +812,25 @@ int pinyb200_energy_force(pinyb200_ctx *c, const double *pos, const double *xmod
             CK(cudaGetLastError());
         }
     }
-    int rc = evaluate(c, cell, flags, e);
+    // everything enqueued, one wait: the forces come back right behind the
+    // evaluation
+    const bool energy = !(flags & PINYB200_NO_ENERGY);
+    if (energy && !c->h_acc_pin) CK(cudaMallocHost(&c->h_acc_pin, (size_t)c->P * S_NSLOT * sizeof(double)));
+    double *acc = energy ? c->h_acc_pin : nullptr;  // pinned: the copy is queued, not waited for
+    int rc = evaluate_enqueue(c, cell, flags, true, acc);
     if (rc) return rc;
     CK(launch_transpose_out(c, c->d_force_aos));
     CK(cudaMemcpyAsync(force, c->d_force_aos, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaEventRecord(c->ev[7], c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    CK(cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]));
+    CK(cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]));
+    CK(cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]));
+    CK(cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]));
     CK(cudaEventElapsedTime(&c->last_ms[4], c->ev[6], c->ev[7]));
+    evaluate_finish(c, cell, flags, acc, e);
+    if (energy && e && !std::isfinite(e->vintert + e->vintrat))
+        return fail(c, PINYB200_ERR_NAN, "non-finite energy: check the positions (forces were written)");
     return PINYB200_OK;
 }
 

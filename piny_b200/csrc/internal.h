@@ -208,6 +208,7 @@ struct pinyb200_ctx {
     // bumped whenever launch shapes or device buffers may change (list
     // builds, tuning, PME tiles): captured graphs compare it before replay
     unsigned long long gen = 0;
+    double *h_acc_pin = nullptr;  // pinned per-bead sums of the host-buffer call
     pinyb200::GradHost grad;      // tangent channels of pinyb200_grad_prepare
     std::string err;
 };
