@@ -264,8 +264,10 @@ def read_config(path, natm, pi_beads, binary=False, centroid=False):
 
 
 def dump_from_run(setup, pos, vel, hmat, names, mol_num, itime=0, pimd=None, t_ext=None, dt=None):
-    """A write_dump state for a run driven here: chain velocities read from
-    a ``lib.DevicePimd`` (pimd), everything volume-related zero (NVT)."""
+    """A write_dump state for a run driven here (``pimd.nvt_setup``'s
+    ``setup``): chain velocities read from a ``lib.DevicePimd`` (pimd),
+    everything volume-related zero (NVT), nfree = 3 per non-ghost atom (PINY's
+    count without constraints)."""
     P, n = np.asarray(pos).shape[:2]
     cv = bv = np.zeros((0, 0))
     if pimd is not None:

@@ -115,5 +115,5 @@ def nvt_setup(mass, ghost, nbeads: int, kind: int, temperature: float, dt: float
         pre = BOLTZ * BOLTZ * gamma_adb * gamma_adb / float(nbeads)
         bead = massive_chains(natm, ghost, T, pre / (T * T), len_nhc, nres_nhc, w, True)
     return {"natm": natm, "nbeads": int(nbeads), "kind": int(kind), "mass": mass, **pis, "wght_pimd": 1.0,
-            "dt": float(dt), "beta": BOLTZ / T, "nfree_atoms": int((~ghost).sum()), "class_nhc": cls,
-            "bead_nhc": bead}
+            "dt": float(dt), "beta": BOLTZ / T, "temperature": T, "nfree_atoms": int((~ghost).sum()),
+            "class_nhc": cls, "bead_nhc": bead}

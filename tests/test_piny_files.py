@@ -116,3 +116,27 @@ def test_initial_file(tmp_path):
     assert np.abs(x * files.BOHR - pos).max() <= 1e-9 * np.abs(pos).max()
     x1, _, _ = files.read_initial(str(d / "water.initial"), spread=True)
     assert x1.shape == (1, spec.natm, 3)
+
+
+def test_dump_from_a_run_reads_back(tmp_path):
+    """A dump written from a run driven here is a restart_all file PINY's
+    reader layout accepts (our reader: every field back)."""
+    from piny_b200 import files, pimd
+    from piny_b200.lib import NORMAL_MODES
+    natm, P = 6, 4
+    rng = np.random.default_rng(0)
+    mass = np.array([29164.4, 1837.5, 1837.5, 29164.4, 1837.5, 1837.5])
+    setup = pimd.nvt_setup(mass, None, P, NORMAL_MODES, 300.0, 20.0, 800.0, len_nhc=2)
+    pos, vel = rng.normal(size=(P, natm, 3)), rng.normal(size=(P, natm, 3)) * 1e-3
+    h = np.diag([20.0, 21.0, 22.0]).reshape(9)
+    names = [("O", "water", "water"), ("H", "water", "water"), ("H", "water", "water")] * 2
+    s = files.dump_from_run(setup, pos, vel, h, names, [1, 1, 1, 2, 2, 2], itime=7)
+    s["class_v_nhc"] = rng.normal(size=(2, 18))
+    s["bead_v_nhc"] = rng.normal(size=(P - 1, 2, 18))
+    s["v_vol_nhc"] = np.zeros(2)
+    p = tmp_path / "dump"
+    files.write_dump(str(p), s)
+    r = files.read_dump(str(p))
+    assert r["itime"] == 7 and r["pi_beads"] == P and r["t_ext"] == 300.0 and r["nfree"] == 18
+    assert np.abs(r["pos"] - pos).max() <= 1e-12 and np.abs(r["vel"] - vel).max() <= 1e-15
+    assert r["class_v_nhc"].shape == (2, 18) and r["bead_v_nhc"].shape == (P - 1, 2, 18)
