@@ -142,3 +142,22 @@ def test_list_that_outgrows_its_reservation_is_reported():
     box.list_status()
     box.energy_force_device(d2.data_ptr(), xm2.data_ptr(), F["hmat"], df.data_ptr())
     box.close()
+
+
+def test_update_arguments_and_state():
+    import torch
+
+    from piny_b200.lib import DeviceBox, PinyError
+    F = load_fixture(NAME)
+    P = int(F["nbeads"])
+    box = DeviceBox(F, P, "fp64")
+    d = torch.from_numpy(np.ascontiguousarray(F["pos"], np.float64)).to("cuda:0")
+    xm = torch.from_numpy(np.ascontiguousarray(F["xmod"], np.float64)).to("cuda:0")
+    with pytest.raises(PinyError, match="ERR_STATE"):  # no host build yet
+        box.update_list_device(d.data_ptr(), xm.data_ptr(), F["hmat"])
+    box.build_list(F["pos"][0], F["xmod"], F["hmat"], F["cutskin2"])
+    with pytest.raises(PinyError, match="ERR_ARG"):  # beads without mode-1 positions
+        box.update_list_device(d.data_ptr(), None, F["hmat"])
+    st = box.list_status()
+    assert st["rebuilds"] == 0 and st["overflow"] == 0 and st["npairs"] == box.list_info()["npairs"]
+    box.close()
