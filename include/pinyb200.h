@@ -256,7 +256,10 @@ int pinyb200_energy_force_device(pinyb200_ctx *ctx, const double *d_pos,
  * PINY's 1-based per-bead arrays (clatoms_pos[ip+1].x etc., element 1 is the
  * first atom); xmod/ymod/zmod are clatoms_info.xmod etc. (1-based) or NULL;
  * hmat is cell.hmat (1-based).  Forces and pvten_tot (1-based, 9) are ADDED
- * to, as PINY's routines do; energies are returned in *e.
+ * to, as PINY's routines do; energies are returned in *e.  PINY also adds
+ * every one of these forces to the virial forces fxt/fyt/fzt (force_npol,
+ * the reciprocal sum, bond, bend, ecor); without RESPA they equal the forces
+ * added here, so a PIMD shim adds the same values to fxt.
  */
 int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
                         double *const *y, double *const *z, const double *xmod,
