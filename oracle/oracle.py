@@ -50,6 +50,14 @@ class OrcEnergies(C.Structure):
                                   "vlong", "vbond", "vbend", "vintert", "vintrat")] + [("pvten", _d * 9)]
 
 
+class OrcRespa(C.Structure):
+    _fields_ = [
+        ("wght_ter", _d), ("wght_ter_res", _d), ("wght_tra_res", _d),
+        ("int_res_ter", _i), ("int_res_inter", _i), ("ires_bond", _i),
+        ("cutoff_res", _pd), ("rheal_res", _d), ("bond_eq_res", _pd),
+    ]
+
+
 def build():
     """Compile the oracle restatement (plain gcc)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
@@ -89,6 +97,8 @@ class Oracle:
                                   C.c_long, _pi, _pi]
         L.orc_energy_force.argtypes = [C.POINTER(OrcSystem), _i, _pd, _pd, _pd, C.c_long, _pi, _pi, _i,
                                        _pd, C.POINTER(OrcEnergies)]
+        L.orc_respa_force.argtypes = [C.POINTER(OrcSystem), C.POINTER(OrcRespa), _i, _i, _pd, _pd, _pd,
+                                      C.c_long, _pi, _pi, _i, _pd, _pd]
 
     # -- helpers -----------------------------------------------------------
     @staticmethod
@@ -264,6 +274,37 @@ class Oracle:
         out = {n: getattr(e, n) for n, _ in OrcEnergies._fields_ if n != "pvten"}
         out["pvten"] = np.array(e.pvten[:])
         return force, out
+
+    def respa_force(self, sysd, respa, level, pos, xmod, hmat, pi, pj, distribute_ghosts=False):
+        """orc_respa_force: PINY's weighted forces at one RESPA level and, at
+        a full inter level, the virial forces (else None).  ``respa`` holds
+        wght_ter, wght_ter_res, wght_tra_res, int_res_ter, int_res_inter,
+        ires_bond, cutoff_res [npair_typ], rheal_res, bond_eq_res."""
+        s = self.make_struct(sysd)
+        r = OrcRespa()
+        keep = []
+        for name, ctype in OrcRespa._fields_:
+            v = respa[name]
+            if ctype is _pd:
+                a, p = self._d(v)
+                keep.append(a)
+                setattr(r, name, p)
+            else:
+                setattr(r, name, v)
+        pos = np.ascontiguousarray(pos, np.float64)
+        P = pos.shape[0]
+        force = np.zeros_like(pos)
+        forcet = np.zeros_like(pos)
+        xm = None if xmod is None else np.ascontiguousarray(xmod, np.float64)
+        hmat, ph = self._d(hmat)
+        pi, ppi = self._i(pi)
+        pj, ppj = self._i(pj)
+        self.lib.orc_respa_force(C.byref(s), C.byref(r), int(level), P, pos.ctypes.data_as(_pd),
+                                 xm.ctypes.data_as(_pd) if xm is not None else None, ph, len(pi), ppi, ppj,
+                                 1 if distribute_ghosts else 0, force.ctypes.data_as(_pd),
+                                 forcet.ctypes.data_as(_pd))
+        del keep
+        return force, (forcet if level & 1 else None)
 
 
 # -- path-integral MD bookkeeping (pimd_oracle.c) and its composition -------

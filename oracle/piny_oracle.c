@@ -1030,6 +1030,228 @@ void orc_energy_force(const orc_system *s, int P, const double *pos_in, const do
 }
 
 /* ------------------------------------------------------------------------ */
+/* RESPA split of the force at one level (orc_respa in piny_oracle.h).       */
+/* force = PINY's weighted clatoms fx; forcet = the virial forces fxt,       */
+/* written only at a full inter level (bead 1..P, unweighted).               */
+/* ------------------------------------------------------------------------ */
+static void add3(double *f, int a, double fx, double fy, double fz)
+{
+    f[3 * a] += fx; f[3 * a + 1] += fy; f[3 * a + 2] += fz;
+}
+
+static void distrib_ghosts(const orc_system *s, double *f)
+{
+    for (int g = 0; g < s->nghost; g++) {
+        int gl = s->ghost_atom[g];
+        for (int c = 0; c < s->ghost_ncomp; c++) {
+            int a = s->ghost_comp[g * s->ghost_ncomp + c];
+            if (a < 0) continue;
+            double cf = s->ghost_coef[g * s->ghost_ncomp + c];
+            add3(f, a, cf * f[3 * gl], cf * f[3 * gl + 1], cf * f[3 * gl + 2]);
+        }
+        f[3 * gl] = f[3 * gl + 1] = f[3 * gl + 2] = 0.0;
+    }
+}
+
+void orc_respa_force(const orc_system *s, const orc_respa *r, int level, int P,
+                     const double *pos_in, const double *xmod, const double *h,
+                     long npairs, const int *pi, const int *pj,
+                     int distribute_ghosts, double *force, double *forcet)
+{
+    const int full_inter = (level & ORC_FULL_INTER) != 0, res_inter = (level & ORC_RES_INTER) != 0;
+    const int intra = (level & (ORC_FULL_INTRA | ORC_RES_INTRA)) != 0;
+    double hi[9];
+    double vol = cell_inverse(h, hi);
+    int cubic = is_cubic(h);
+    long natm = s->natm;
+    double *pos = malloc(sizeof(double) * 3 * natm);
+    double *tmp = malloc(sizeof(double) * 3 * natm);
+    const double w_full = r->wght_ter, w_res = r->wght_ter_res, w_tra_res = r->wght_tra_res;
+    const double rheal_resi = 1.0 / r->rheal_res;
+    /* bond_both.c:156-161 */
+    const double wfor_both = r->int_res_inter ? r->wght_ter_res : r->wght_ter;
+
+    for (int b = 0; b < P; b++) {
+        memcpy(pos, pos_in + 3 * natm * b, sizeof(double) * 3 * natm);
+        double *f = force + 3 * natm * b;
+        double *ft = full_inter ? forcet + 3 * natm * b : NULL;
+        memset(f, 0, sizeof(double) * 3 * natm);
+        if (ft) memset(ft, 0, sizeof(double) * 3 * natm);
+        for (int g = 0; g < s->nghost; g++) {
+            int gl = s->ghost_atom[g];
+            double gx = 0.0, gy = 0.0, gz = 0.0;
+            for (int c = 0; c < s->ghost_ncomp; c++) {
+                int a = s->ghost_comp[g * s->ghost_ncomp + c];
+                if (a < 0) continue;
+                double cf = s->ghost_coef[g * s->ghost_ncomp + c];
+                gx += cf * pos[3 * a];
+                gy += cf * pos[3 * a + 1];
+                gz += cf * pos[3 * a + 2];
+            }
+            pos[3 * gl] = gx; pos[3 * gl + 1] = gy; pos[3 * gl + 2] = gz;
+        }
+
+        /* real space (force_npol.c): shave at cutoff (full) or cutoff_res
+         * (res only, npol_shave_skin :1309-1319), switch over the last
+         * rheal_res before cutoff_res (:807-816), multiplier (:1030-1060) */
+        if (full_inter || res_inter) {
+            for (long p = 0; p < npairs; p++) {
+                int i = pi[p], j = pj[p];
+                double dx = pos[3 * i] - pos[3 * j], dy = pos[3 * i + 1] - pos[3 * j + 1],
+                       dz = pos[3 * i + 2] - pos[3 * j + 2];
+                if (P > 1)
+                    period_pimd_one(&dx, &dy, &dz, xmod[3 * i] - xmod[3 * j], xmod[3 * i + 1] - xmod[3 * j + 1],
+                                    xmod[3 * i + 2] - xmod[3 * j + 2], h, hi, cubic);
+                else
+                    period_one(&dx, &dy, &dz, h, hi, cubic);
+                double rr = sqrt((dx * dx + dy * dy + dz * dz));
+                int pt = pair_type(s->atm_typ[i], s->atm_typ[j], s->ntyp);
+                double cut = full_inter ? s->cutoff[pt] : r->cutoff_res[pt];
+                if (!(rr < cut)) continue;
+                int u = s->inter_map[pt];
+                double rmin = s->rmin_spl[u], dr = s->dr_spl[u], dri = s->dri_spl[u];
+                int k = (int)(((rr - rmin) * dri) + 0.5) + 3;
+                k = k < s->nsplin - 2 ? k : s->nsplin - 2;
+                k = k > 3 ? k : 3;
+                double rsp = ((double)(k - 3)) * dr + rmin;
+                double del = (rr - rsp) * dri;
+                long off = (long)u * s->nsplin;
+                double q2 = s->charge[i] * s->charge[j];
+                double dvtemp = (q2 * vspl(s->cdv0_c + off, k, del) + vspl(s->cdv0 + off, k, del));
+                double fx = dx * dvtemp, fy = dy * dvtemp, fz = dz * dvtemp;
+                double fmult = w_full;
+                if (res_inter) {
+                    double br = (rr - r->cutoff_res[pt] + r->rheal_res) * rheal_resi;
+                    br = br > 0.0 ? br : 0.0;
+                    br = br < 1.0 ? br : 1.0;
+                    double swit = br * br * (br * 2.0 - 3.0) + 1.0;
+                    fmult = full_inter ? (swit * w_res + (1.0 - swit) * w_full) : swit * w_res;
+                }
+                add3(f, i, fx * fmult, fy * fmult, fz * fmult);
+                add3(f, j, -(fx * fmult), -(fy * fmult), -(fz * fmult));
+                if (ft) {
+                    add3(ft, i, fx, fy, fz);
+                    add3(ft, j, -fx, -fy, -fz);
+                }
+            }
+        }
+
+        /* reciprocal space and the exclusion correction: full steps only,
+         * weight wght_ter (energy_control_inter_recip.c:184-214, :281-292;
+         * ewald3d_pme.c forces x wght_now, ecorr.c:100 wfor) */
+        if (full_inter) {
+            if (s->nktot > 0) {
+                double pvr[10] = {0};
+                memset(tmp, 0, sizeof(double) * 3 * natm);
+                pme_bead(s, pos, h, hi, vol, tmp, pvr);
+                for (long a = 0; a < 3 * natm; a++) {
+                    ft[a] += tmp[a];
+                    f[a] += tmp[a] * w_full;
+                }
+            }
+            for (int c = 0; c < s->necor; c++) {
+                int a = s->ecor_j1[c], bb = s->ecor_j2[c];
+                double dx = pos[3 * a] - pos[3 * bb], dy = pos[3 * a + 1] - pos[3 * bb + 1],
+                       dz = pos[3 * a + 2] - pos[3 * bb + 2];
+                double rr = sqrt(dx * dx + dy * dy + dz * dz);
+                int k = (int)(((rr - s->ecor_rmin) * s->ecor_dri) + 0.5) + 3;
+                k = k < s->ecor_nsplin - 2 ? k : s->ecor_nsplin - 2;
+                k = k > 3 ? k : 3;
+                double rsp = ((double)(k - 3)) * s->ecor_dr + s->ecor_rmin;
+                double del = (rr - rsp) * s->ecor_dri;
+                double q12 = s->charge[a] * s->charge[bb];
+                double dvt = vspl(s->ecor_cdv0, k, del) * q12;
+                double fx = dx * dvt, fy = dy * dvt, fz = dz * dvt;
+                add3(ft, a, fx, fy, fz);
+                add3(ft, bb, -fx, -fy, -fz);
+                add3(f, a, fx * w_full, fy * w_full, fz * w_full);
+                add3(f, bb, -(fx * w_full), -(fy * w_full), -(fz * w_full));
+            }
+        }
+
+        if (intra) {
+            /* bonds: bond_both at inter levels (bond_both.c:270-420), else
+             * bond() with the res equilibrium when ires_bond (bond.c:113-118) */
+            for (int c = 0; c < s->nbond; c++) {
+                int a = s->bond_j1[c], bb = s->bond_j2[c], t = s->bond_typ[c];
+                const double *dc = s->bond_dc + 7 * t;
+                double dx = pos[3 * a] - pos[3 * bb], dy = pos[3 * a + 1] - pos[3 * bb + 1],
+                       dz = pos[3 * a + 2] - pos[3 * bb + 2];
+                double rr = sqrt(dx * dx + dy * dy + dz * dz);
+                if (full_inter || res_inter) {
+                    double rr0 = rr - s->bond_eq[t], rr0r = rr - r->bond_eq_res[t];
+                    double dv = ((((dc[6] * rr0 + dc[5]) * rr0 + dc[4]) * rr0 + dc[3]) * rr0 + dc[2]) * rr0 + dc[1];
+                    double dvr =
+                        ((((dc[6] * rr0r + dc[5]) * rr0r + dc[4]) * rr0r + dc[3]) * rr0r + dc[2]) * rr0r + dc[1];
+                    double pre = -dv / rr, prer = -dvr / rr;
+                    double f1[3] = {dx * pre, dy * pre, dz * pre}, f2[3] = {dx * prer, dy * prer, dz * prer};
+                    double fw[3];
+                    for (int d = 0; d < 3; d++) fw[d] = w_tra_res * f2[d] + wfor_both * (f1[d] - f2[d]);
+                    if (ft) {
+                        add3(ft, a, f1[0], f1[1], f1[2]);
+                        add3(ft, bb, -f1[0], -f1[1], -f1[2]);
+                    }
+                    add3(f, a, fw[0], fw[1], fw[2]);
+                    add3(f, bb, -fw[0], -fw[1], -fw[2]);
+                } else {
+                    double rr0 = rr - (r->ires_bond ? r->bond_eq_res[t] : s->bond_eq[t]);
+                    double dv = ((((dc[6] * rr0 + dc[5]) * rr0 + dc[4]) * rr0 + dc[3]) * rr0 + dc[2]) * rr0 + dc[1];
+                    double pre = -dv / rr;
+                    double fx = dx * pre * w_tra_res, fy = dy * pre * w_tra_res, fz = dz * pre * w_tra_res;
+                    add3(f, a, fx, fy, fz);
+                    add3(f, bb, -fx, -fy, -fz);
+                }
+            }
+            /* bends x wght_tra_res (bend.c:144, :380-393) */
+            for (int c = 0; c < s->nbend; c++) {
+                int a1 = s->bend_j1[c], a2 = s->bend_j2[c], a3 = s->bend_j3[c], t = s->bend_typ[c];
+                const double *bs = s->bend_s + 7 * t;
+                const double *bdc = s->bend_dc + 7 * t, *bds = s->bend_ds + 7 * t;
+                double x2 = pos[3 * a2], y2 = pos[3 * a2 + 1], z2 = pos[3 * a2 + 2];
+                double dx12 = pos[3 * a1] - x2, dy12 = pos[3 * a1 + 1] - y2, dz12 = pos[3 * a1 + 2] - z2;
+                double dx23 = pos[3 * a3] - x2, dy23 = pos[3 * a3 + 1] - y2, dz23 = pos[3 * a3 + 2] - z2;
+                double r122i = 1.0 / (dx12 * dx12 + dy12 * dy12 + dz12 * dz12);
+                double r12i = sqrt(r122i);
+                double r322i = 1.0 / (dx23 * dx23 + dy23 * dy23 + dz23 * dz23);
+                double r32i = sqrt(r322i);
+                double rpmag = r12i * r32i;
+                double cost = (dx12 * dx23 + dy12 * dy23 + dz12 * dz23) * rpmag;
+                cost = (cost < 1.0 ? cost : 1.0);
+                cost = (cost > -1.0 ? cost : -1.0);
+                double sint = sqrt(1.0 - cost * cost);
+                sint = (sint > 1.0e-8 ? sint : 1.0e-8);
+                double cos122 = cost * r122i, cos322 = cost * r322i;
+                double sisum = (((((bs[6] * sint + bs[5]) * sint + bs[4]) * sint + bs[3]) * sint + bs[2]) * sint);
+                double dvbendc = (((((bdc[6] * cost + bdc[5]) * cost + bdc[4]) * cost + bdc[3]) * cost + bdc[2]) *
+                                      cost + bdc[1]);
+                double dvbends = ((((bds[6] * sint + bds[5]) * sint + bds[4]) * sint + bds[3]) * sint + bds[2]);
+                dvbends = dvbends * cost + bds[1];
+                double pre = -(dvbendc + sisum - dvbends * cost / sint);
+                double g1[3] = {(dx23 * rpmag - dx12 * cos122) * pre, (dy23 * rpmag - dy12 * cos122) * pre,
+                                (dz23 * rpmag - dz12 * cos122) * pre};
+                double g3[3] = {(dx12 * rpmag - dx23 * cos322) * pre, (dy12 * rpmag - dy23 * cos322) * pre,
+                                (dz12 * rpmag - dz23 * cos322) * pre};
+                double g2[3] = {-(g1[0] + g3[0]), -(g1[1] + g3[1]), -(g1[2] + g3[2])};
+                if (ft) {
+                    add3(ft, a1, g1[0], g1[1], g1[2]);
+                    add3(ft, a2, g2[0], g2[1], g2[2]);
+                    add3(ft, a3, g3[0], g3[1], g3[2]);
+                }
+                add3(f, a1, g1[0] * w_tra_res, g1[1] * w_tra_res, g1[2] * w_tra_res);
+                add3(f, a2, g2[0] * w_tra_res, g2[1] * w_tra_res, g2[2] * w_tra_res);
+                add3(f, a3, g3[0] * w_tra_res, g3[1] * w_tra_res, g3[2] * w_tra_res);
+            }
+        }
+        if (distribute_ghosts) {
+            distrib_ghosts(s, f);
+            if (ft) distrib_ghosts(s, ft);
+        }
+    }
+    free(pos);
+    free(tmp);
+}
+
+/* ------------------------------------------------------------------------ */
 /* Verlet-list rebuild test.                                                 */
 /* check_ver_list:  src/energy/inter/real_space/nbr_list_control.c:182-247 */
 /* get_pimd_spread: src/energy/pimd/pimd_estimators.c:121-220 (bead 1 is   */

@@ -116,6 +116,28 @@ typedef struct orc_energies {
     double pvten[9];   /* bead-summed pressure tensor (PINY pvten_tot)      */
 } orc_energies;
 
+/* RESPA split of the force (energy_control_initial.c:211-243 weights,
+ * force_npol.c:805-816 / :1030-1060 switch and multipliers, bond_both.c,
+ * bond.c, bend.c, ecorr.c, ewald3d_pme.c weights).  Level bits are the
+ * energy_ctrl flags int_NVT_pimd sets (int_NVT_pimd.c:175-189). */
+typedef struct orc_respa {
+    double wght_ter, wght_ter_res, wght_tra_res;
+    int int_res_ter;            /* energy_ctrl.int_res_ter                  */
+    int int_res_inter;          /* intra_scr.int_res_inter (nres_ter > 1)   */
+    int ires_bond;              /* bond() irespa: nres_tra*nres_tor > 1     */
+    const double *cutoff_res;   /* [npair_typ] interact.cutoff_res (Bohr)   */
+    double rheal_res;           /* interact.rheal_res (Bohr)                */
+    const double *bond_eq_res;  /* [nbond_typ] bond.eq_pow_res              */
+} orc_respa;
+#define ORC_FULL_INTER 1
+#define ORC_RES_INTER 2
+#define ORC_FULL_INTRA 4
+#define ORC_RES_INTRA 8
+void orc_respa_force(const orc_system *s, const orc_respa *r, int level, int P,
+                     const double *pos, const double *xmod, const double *h,
+                     long npairs, const int *pi, const int *pj,
+                     int distribute_ghosts, double *force, double *forcet);
+
 /* ---- setup restatements -------------------------------------------------*/
 void orc_spline_table(int nsplin, double rmin, double rmax, int itype,
                       double sig, double eps, double alp, double rheal,

@@ -30,6 +30,13 @@
  *                 PINY's restart dump (write_dump_file_pimd, output_pimd.c:786)
  *                 and configuration files (write_config_files_pimd, :1093)
  *                 into <outdir>, and <outdir>/state.bin with what they hold.
+ *   piny_ref respa <dir> <input> <out.bin>   an input with RESPA keys
+ *                 (respa_steps_lrf / _intra / _pimd, respa_rheal, res_dist,
+ *                 eq_res): the four force sub-steps with the energy flags
+ *                 int_NVT_pimd sets at each RESPA level (int_NVT_pimd.c:
+ *                 175-189), then the full step dumped as in dump, plus per
+ *                 level the raw forces (and at the full level the virial
+ *                 forces fxt) and the RESPA set-up.
  *   piny_ref springs <in.bin> <out.bin>  mode_energy_control
  *                 (pimd_estimators.c:31) on modes u, then pimd_pvten_forc_corr
  *                 (pimd_estimators.c:223) on positions x with forces f (also
@@ -665,6 +672,102 @@ static int run_springs(const char *inpath, const char *outpath)
 void write_dump_file_pimd(CLASS *, BONDED *, GENERAL_DATA *);
 void write_config_files_pimd(CLASS *, BONDED *, GENERAL_DATA *);
 
+/* absolute path of an output file that may not exist yet (setup chdirs) */
+static char *resolve_out(const char *arg)
+{
+    char *outpath = realpath(arg, NULL);
+    if (!outpath) {
+        char *tmp = strdup(arg);
+        char *slash = strrchr(tmp, '/');
+        char *d = slash ? (*slash = 0, realpath(tmp[0] ? tmp : "/", NULL)) : realpath(".", NULL);
+        const char *base = slash ? slash + 1 : arg;
+        outpath = malloc(strlen(d) + strlen(base) + 2);
+        sprintf(outpath, "%s/%s", d, base);
+    }
+    return outpath;
+}
+
+/* RESPA levels as int_NVT_pimd sets the flags (int_NVT_pimd.c:175-189):
+ * iget_full_inter, iget_res_inter, iget_full_intra, iget_res_intra. */
+static const int k_levels[4][4] = {{1, -1, 1, 1}, {0, 1, 1, 1}, {0, 0, 1, 1}, {0, 0, 0, 1}};
+
+static void set_level(int l)
+{
+    class_.energy_ctrl.iget_full_inter = k_levels[l][0];
+    class_.energy_ctrl.iget_res_inter = k_levels[l][1] < 0 ? gd_.timeinfo.int_res_ter : k_levels[l][1];
+    class_.energy_ctrl.iget_full_intra = k_levels[l][2];
+    class_.energy_ctrl.iget_res_intra = k_levels[l][3];
+}
+
+static void gather_forces(double *buf, int t)
+{
+    CLATOMS_INFO *ci = &class_.clatoms_info;
+    int n = ci->natm_tot, P = ci->pi_beads;
+    for (int ip = 1; ip <= P; ip++)
+        for (int i = 1; i <= n; i++) {
+            size_t o = ((size_t)(ip - 1) * n + (i - 1)) * 3;
+            CLATOMS_POS *cp = &class_.clatoms_pos[ip];
+            buf[o] = t ? cp->fxt[i] : cp->fx[i];
+            buf[o + 1] = t ? cp->fyt[i] : cp->fy[i];
+            buf[o + 2] = t ? cp->fzt[i] : cp->fz[i];
+        }
+}
+
+static int run_respa(const char *dir, const char *input, const char *outpath)
+{
+    setup(dir, input);
+    CLATOMS_INFO *ci = &class_.clatoms_info;
+    const size_t nb = (size_t)ci->natm_tot * ci->pi_beads * 3;
+    double *f[4], *ft = (double *)malloc(sizeof(double) * nb + 8);
+    double e[4][2];
+    for (int l = 0; l < 4; l++) {
+        f[l] = (double *)malloc(sizeof(double) * nb + 8);
+        set_level(l);
+        evaluate();
+        gather_forces(f[l], 0);
+        if (l == 0 && ci->pi_beads > 1) gather_forces(ft, 1);
+        e[l][0] = gd_.stat_avg.vintert;
+        e[l][1] = gd_.stat_avg.vintrat;
+    }
+    set_level(0);
+    evaluate();
+    dump_all(outpath);
+    g_out = fopen(outpath, "ab");
+    if (!g_out) return 2;
+    TIMEINFO *ti = &gd_.timeinfo;
+    put1i("nres_ter", ti->nres_ter);
+    put1i("nres_tor", ti->nres_tor);
+    put1i("nres_tra", ti->nres_tra);
+    put1i("nres_pimd", ti->nres_pimd);
+    put1i("int_res_ter", ti->int_res_ter);
+    put1i("int_res_tra", ti->int_res_tra);
+    put1d("wght_ter", class_.for_scr.wght_ter);
+    put1d("wght_ter_res", class_.for_scr.wght_ter_res);
+    put1d("wght_tra", class_.for_scr.wght_tra);
+    put1d("wght_tra_res", class_.for_scr.wght_tra_res);
+    if (bonded_.bond.npow > 0) putd("bond_eq_res", bonded_.bond.eq_pow_res, bonded_.bond.ntyp_pow);
+    for (int l = 0; l < 4; l++) {
+        char nm[32];
+        snprintf(nm, sizeof nm, "L%d_force_raw", l);
+        put(nm, 'd', f[l], (int64_t)nb);
+        snprintf(nm, sizeof nm, "L%d_flags", l);
+        int fl[4];
+        set_level(l);
+        fl[0] = class_.energy_ctrl.iget_full_inter;
+        fl[1] = class_.energy_ctrl.iget_res_inter;
+        fl[2] = class_.energy_ctrl.iget_full_intra;
+        fl[3] = class_.energy_ctrl.iget_res_intra;
+        put(nm, 'i', fl, 4);
+        snprintf(nm, sizeof nm, "L%d_energies", l);
+        put(nm, 'd', e[l], 2);
+        free(f[l]);
+    }
+    if (ci->pi_beads > 1) put("L0_forcet_raw", 'd', ft, (int64_t)nb);
+    free(ft);
+    fclose(g_out);
+    return 0;
+}
+
 static char *path_in(const char *dir, const char *name)
 {
     char *p = malloc(strlen(dir) + strlen(name) + 2);
@@ -757,6 +860,7 @@ static int run_io(const char *dir, const char *input, const char *outdir_rel, in
 int main(int argc, char **argv)
 {
     if (argc == 6 && strcmp(argv[1], "io") == 0) return run_io(argv[2], argv[3], argv[4], atoi(argv[5]));
+    if (argc == 5 && strcmp(argv[1], "respa") == 0) return run_respa(argv[2], argv[3], resolve_out(argv[4]));
     if (argc == 4 && strcmp(argv[1], "nhc") == 0) return run_nhc(argv[2], argv[3]);
     if (argc == 4 && strcmp(argv[1], "springs") == 0) return run_springs(argv[2], argv[3]);
     if (argc == 5 && strcmp(argv[1], "pimd") == 0) return run_pimd(atoi(argv[2]), argv[3], argv[4]);
@@ -768,16 +872,7 @@ int main(int argc, char **argv)
     char *outpath = NULL;
     if (strcmp(mode, "dump") == 0) {
         if (argc < 5) return 2;
-        outpath = realpath(argv[4], NULL);
-        if (!outpath) {
-            /* file does not exist yet: resolve its directory */
-            char *tmp = strdup(argv[4]);
-            char *slash = strrchr(tmp, '/');
-            char *d = slash ? (*slash = 0, realpath(tmp[0] ? tmp : "/", NULL)) : realpath(".", NULL);
-            const char *base = slash ? slash + 1 : argv[4];
-            outpath = malloc(strlen(d) + strlen(base) + 2);
-            sprintf(outpath, "%s/%s", d, base);
-        }
+        outpath = resolve_out(argv[4]);
     }
     setup(argv[2], argv[3]);
 

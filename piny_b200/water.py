@@ -226,8 +226,13 @@ def _fmt(x):
     return repr(float(x))
 
 
-def piny_input_files(spec: BoxSpec, pos_angstrom, sim_typ=None):
-    """Return {filename: text} for a PINY run of ``spec`` at ``pos_angstrom``."""
+def piny_input_files(spec: BoxSpec, pos_angstrom, sim_typ=None, respa=None):
+    """Return {filename: text} for a PINY run of ``spec`` at ``pos_angstrom``.
+
+    ``respa`` (optional) switches on PINY's RESPA split: a dict with the step
+    counts ``lrf``, ``intra``, ``pimd`` (respa_steps_lrf / _intra / _pimd),
+    ``rheal`` (respa_rheal, Angstrom) and ``eq_res`` (the bond's eq_res
+    shift, Angstrom); the inner cutoff is each pair's ``res_dist``."""
     model = spec.model
     P = spec.nbeads
     L = spec.L
@@ -243,7 +248,11 @@ def piny_input_files(spec: BoxSpec, pos_angstrom, sim_typ=None):
     if P > 1:
         sections.append(("sim_pimd_def", {
             "path_int_beads": P, "path_int_md_typ": "centroid",
-            "initial_spread_opt": "off", "respa_steps_pimd": 1}))
+            "initial_spread_opt": "off", "respa_steps_pimd": int(respa["pimd"]) if respa else 1}))
+    if respa:
+        sections.append(("sim_run_def", {
+            "respa_steps_lrf": int(respa["lrf"]), "respa_steps_torsion": 1,
+            "respa_steps_intra": int(respa["intra"]), "respa_rheal": _fmt(respa["rheal"])}))
     sections += [
         ("sim_list_def", {"neighbor_list": "ver_list", "verlist_skin": _fmt(spec.skin),
                           "update_type": spec.update_type}),
@@ -289,6 +298,8 @@ def piny_input_files(spec: BoxSpec, pos_angstrom, sim_typ=None):
         a = b["a"]
         bond = {"atom1": "O", "atom2": "H", "pot_type": "power", "eq": _fmt(b["r0"]),
                 "p2": _fmt(D * a ** 2), "p3": _fmt(-D * a ** 3), "p4": _fmt(7.0 * D * a ** 4 / 12.0)}
+    if respa:
+        bond["eq_res"] = _fmt(respa["eq_res"])
     files["water.bond"] = _input_str([("bond_parm", bond)])
     files["water.bend"] = _input_str([("bend_parm", {
         "atom1": "H", "atom2": "O", "atom3": "H", "pot_type_bend": "harm",
@@ -326,9 +337,9 @@ def piny_input_files(spec: BoxSpec, pos_angstrom, sim_typ=None):
     return files
 
 
-def write_piny_input(directory, spec: BoxSpec, pos_angstrom, sim_typ=None):
+def write_piny_input(directory, spec: BoxSpec, pos_angstrom, sim_typ=None, respa=None):
     os.makedirs(directory, exist_ok=True)
-    for name, text in piny_input_files(spec, pos_angstrom, sim_typ).items():
+    for name, text in piny_input_files(spec, pos_angstrom, sim_typ, respa).items():
         with open(os.path.join(directory, name), "w") as f:
             f.write(text)
     return os.path.join(directory, "water.input")

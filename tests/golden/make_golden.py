@@ -18,10 +18,13 @@ centroid-virial routines (``piny_ref nhc`` / ``piny_ref springs``) on seeded
 inputs.  It also stores pimd_transforms.npz: PINY's own ring-polymer transforms
 (``piny_ref pimd``: path_integral_init, convert_pimd_mode/pos/force_* of
 transform_stg.c and transform_cnt.c) of seeded bead positions and forces,
-for staging and normal modes at several bead counts.
+for staging and normal modes at several bead counts.  respa_*.npz hold
+PINY's forces at each RESPA level (``piny_ref respa``) for boxes whose inputs
+switch the split on.
 
 Run in a container that has the PINY tree:  python tests/golden/make_golden.py
-(``--pimd-only`` regenerates just the transform fixture)
+(``--pimd-only`` regenerates just the transform, MD-bookkeeping, I/O and
+RESPA fixtures)
 The GPU tests only read the .npz files.
 """
 from __future__ import annotations
@@ -342,6 +345,57 @@ def io_fixture(tmp):
     print("piny_io", os.path.getsize(path), "bytes")
 
 
+RESPA_CASES = [
+    # (name, spec, RESPA keys)
+    ("respa_tip4pf_64_p4",
+     water.BoxSpec(water.TIP4P_F, 64, 12.416, 4, 298.0, 105, cutoff=6.0, grid=16, order=8, kmax=6),
+     {"lrf": 2, "intra": 2, "pimd": 2, "rheal": 0.8, "eq_res": 0.02}),
+    ("respa_spcfw_64_p1",
+     water.BoxSpec(water.SPC_FW, 64, 12.416, 1, 300.0, 106, cutoff=6.0, grid=16, order=6, kmax=6),
+     {"lrf": 3, "intra": 2, "pimd": 1, "rheal": 1.0, "eq_res": -0.01}),
+]
+
+
+def respa_fixture(tmp):
+    """PINY's forces at each RESPA level (``piny_ref respa``): the flags
+    int_NVT_pimd sets at the outer step, an inner inter step, an intra step
+    and the innermost step, on seeded boxes with RESPA inputs."""
+    for name, spec, rk in RESPA_CASES:
+        pos = water.build_positions(spec)
+        d = os.path.join(tmp, "respa_inp")
+        shutil.rmtree(d, ignore_errors=True)
+        water.write_piny_input(d, spec, pos, respa=rk)
+        out = os.path.join(tmp, "respa.bin")
+        subprocess.run([PINY_REF, "respa", d, "water.input", out], check=True, capture_output=True)
+        D = read_dump(out)
+        fx = dump_to_fixture(D, False)
+        n, P = fx["natm"], fx["nbeads"]
+        for k in ("nres_ter", "nres_tor", "nres_tra", "nres_pimd", "int_res_ter"):
+            fx[k] = int(D[k][0])
+        for k in ("wght_ter", "wght_ter_res", "wght_tra_res"):
+            fx[k] = float(D[k][0])
+        fx["cutoff_res"] = D["cutoff_res"]
+        fx["rheal_res"] = float(D["rheal_res"][0])
+        fx["bond_eq_res"] = D["bond_eq_res"]
+        for lv in range(4):
+            fx["L%d_flags" % lv] = D["L%d_flags" % lv]
+            fx["ref_L%d_force_raw" % lv] = D["L%d_force_raw" % lv].reshape(P, n, 3)
+        if P > 1:
+            fx["ref_L0_forcet_raw"] = D["L0_forcet_raw"].reshape(P, n, 3)
+        fx["spec_nmol"] = spec.nmol
+        fx["spec_L"] = spec.L
+        fx["spec_model"] = "tip4pf" if spec.model is water.TIP4P_F else "spcfw"
+        fx["spec_cutoff"] = spec.cutoff
+        fx["spec_kmax"] = spec.kmax_ewald
+        fx["spec_kmax_pme"] = spec.kmax_pme
+        fx["spec_order"] = spec.order
+        fx["spec_nsplin"] = spec.nsplin
+        fx["spec_temperature"] = spec.temperature
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **{k: np.asarray(v) for k, v in fx.items()})
+        print(name, os.path.getsize(path), "bytes")
+
+
 def main():
     if not os.path.exists(PINY_REF):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
@@ -349,6 +403,7 @@ def main():
     pimd_fixture(tmp)
     pimd_md_fixture(tmp)
     io_fixture(tmp)
+    respa_fixture(tmp)
     if "--pimd-only" in sys.argv[1:]:
         shutil.rmtree(tmp, ignore_errors=True)
         return

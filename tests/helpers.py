@@ -30,3 +30,20 @@ def pair_hash(pi, pj):
 
 def rel_rms(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+RESPA_NAMES = ["respa_tip4pf_64_p4", "respa_spcfw_64_p1"]
+
+
+def respa_from_fixture(F):
+    """pinyb200_set_respa's inputs for a RESPA fixture, formed from its step
+    counts the way PINY forms them."""
+    from piny_b200.respa import respa_setup
+    return respa_setup(int(F["nres_ter"]), int(F["nres_tor"]), int(F["nres_tra"]), int(F["nres_pimd"]),
+                       int(F["nbeads"]) > 1, bool(F["int_res_ter"]), F["cutoff_res"], float(F["rheal_res"]),
+                       F["bond_eq_res"])
+
+
+def fixture_level(F, lv):
+    from piny_b200.respa import level_bits
+    return level_bits(*[int(v) for v in F["L%d_flags" % lv]])

@@ -1,0 +1,50 @@
+"""The RESPA split: the oracle restatement against PINY's own forces at each
+RESPA level (fixtures made by tests/golden/make_golden.py, ``piny_ref respa``)
+and the host-side set-up against the values PINY formed."""
+import numpy as np
+import pytest
+
+from helpers import RESPA_NAMES, fixture_level, load_fixture, pair_hash, respa_from_fixture, rel_rms
+from piny_b200 import respa as R
+
+
+@pytest.mark.parametrize("name", RESPA_NAMES)
+def test_respa_weights_match_piny(name):
+    F = load_fixture(name)
+    r = respa_from_fixture(F)
+    for k in ("wght_ter", "wght_ter_res", "wght_tra_res"):
+        assert r[k] == F[k], k
+
+
+@pytest.mark.parametrize("name", RESPA_NAMES)
+def test_respa_oracle_matches_piny(name, oracle):
+    F = load_fixture(name)
+    r = respa_from_fixture(F)
+    xmod = F.get("xmod")
+    pi, pj = oracle.verlist(F, F["pos"][0], xmod, F["hmat"], F["cutskin2"])
+    assert pair_hash(pi, pj) == F["pairs_sha256"]
+    for lv in range(4):
+        f, ft = oracle.respa_force(F, r, fixture_level(F, lv), F["pos"], xmod, F["hmat"], pi, pj)
+        assert rel_rms(f, F["ref_L%d_force_raw" % lv]) < 1e-13, lv
+        if lv == 0 and "ref_L0_forcet_raw" in F:
+            assert rel_rms(ft, F["ref_L0_forcet_raw"]) < 1e-13
+    # the full level with every weight 1 is the plain evaluation, and so are
+    # PINY's virial forces of the full level
+    plain, _ = oracle.energy_force(F, F["pos"], xmod, F["hmat"], pi, pj)
+    one = dict(r, wght_ter=1.0, wght_ter_res=1.0, wght_tra_res=1.0)
+    f, ft = oracle.respa_force(F, one, R.FULL_INTER | R.FULL_INTRA | R.RES_INTRA, F["pos"], xmod, F["hmat"], pi, pj)
+    assert rel_rms(f, plain) < 1e-13
+    assert rel_rms(ft, plain) < 1e-13
+    if "ref_L0_forcet_raw" in F:
+        assert rel_rms(plain, F["ref_L0_forcet_raw"]) < 1e-13
+
+
+def test_respa_loop_levels():
+    """int_NVT_pimd's nesting: the last call of a step is the full level,
+    inner inter calls close each (tor, tra) sweep, the rest are innermost."""
+    lv = R.loop_levels(2, 1, 2, 1, True)
+    full = R.FULL_INTER | R.RES_INTER | R.FULL_INTRA | R.RES_INTRA
+    inner = R.RES_INTER | R.FULL_INTRA | R.RES_INTRA
+    assert lv == [R.RES_INTRA, inner, R.RES_INTRA, full]
+    assert R.loop_levels(1, 1, 1, 3, False) == [0, 0, R.FULL_INTER | R.FULL_INTRA | R.RES_INTRA]
+    assert R.loop_levels(1, 1, 2, 2, False) == [0, R.RES_INTRA, 0, R.FULL_INTER | R.FULL_INTRA | R.RES_INTRA]
