@@ -269,6 +269,72 @@ int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
                         double *pvten_tot, pinyb200_energies *e);
 
 /*
+ * RESPA split of the force (PINY's respa_steps_lrf / _intra / _pimd).
+ * PINY's integrators nest RESPA loops and ask the force routines for one
+ * level per inner step through four energy_ctrl flags (int_NVT_pimd.c:
+ * 175-189); each term is weighted by the number of inner steps its impulse
+ * spans (energy_control_initial.c:211-243).  pinyb200_set_respa stores the
+ * split's set-up (NULL switches it off):
+ *   wght_ter, wght_ter_res, wght_tra_res   for_scr.wght_* as
+ *                  energy_control_initial sets them
+ *   int_res_ter    energy_ctrl.int_res_ter (respa_steps_lrf given)
+ *   int_res_inter  intra_scr.int_res_inter (nres_ter > 1): bond_both's
+ *                  outer weight is wght_ter_res when set, else wght_ter
+ *   ires_bond      energy_control_intra.c:116-119 (nres_tra*nres_tor > 1):
+ *                  intra-only levels use the bonds' RESPA equilibria
+ *   cutoff_res     interact.cutoff_res per pair type (npair_typ, Bohr)
+ *   rheal_res      interact.rheal_res (Bohr), the switch width
+ *   bond_eq_res    bond.eq_pow_res per bond type (nbond_typ, Bohr)
+ * pinyb200_respa_force_device evaluates one level, `level` being the OR of
+ * the PINYB200_* flag bits below that PINY has set: one of
+ *   RES_INTRA; FULL_INTRA|RES_INTRA; RES_INTER|FULL_INTRA|RES_INTRA (needs
+ *   int_res_ter); FULL_INTER|FULL_INTRA|RES_INTRA, with RES_INTER exactly
+ *   when int_res_ter (the levels int_NVT_pimd's loops produce).
+ * d_force receives PINY's weighted forces fx: real-space pairs x the RESPA
+ * multiplier (inner levels shave at cutoff_res; force_npol.c:805-816,
+ * :1030-1060), PME and the exclusion correction x wght_ter at the outer
+ * level only, bonds as bond_both / bond, bends x wght_tra_res.  At the outer
+ * level d_forcet (may be NULL) receives the unweighted forces PINY adds to
+ * the virial forces fxt, and *e the energies and pvten_tot of
+ * pinyb200_energy_force_device; at inner levels *e is zeroed (PINY books
+ * energies at the outer step).  flags: PINYB200_DISTRIB_GHOSTS,
+ * PINYB200_UPDATE_LIST.  The inner levels use the active site list shaved
+ * at cutoff_res in place of PINY's separate RESPA Verlet list (pairs within
+ * cutoff_res + skin + spread at the build); under the list's own validity
+ * rule the two hold the same pairs inside cutoff_res.  The reciprocal-space
+ * RESPA set (ewald_respa_kmax, PINY's nktot_res > 0) is not supported.
+ */
+#define PINYB200_FULL_INTER 1
+#define PINYB200_RES_INTER 2
+#define PINYB200_FULL_INTRA 4
+#define PINYB200_RES_INTRA 8
+typedef struct pinyb200_respa {
+    double wght_ter, wght_ter_res, wght_tra_res;
+    int int_res_ter, int_res_inter, ires_bond;
+    const double *cutoff_res;
+    double rheal_res;
+    const double *bond_eq_res;
+} pinyb200_respa;
+int pinyb200_set_respa(pinyb200_ctx *ctx, const pinyb200_respa *r);
+int pinyb200_respa_force_device(pinyb200_ctx *ctx, const double *d_pos,
+                                const double *d_xmod, const double *hmat,
+                                int level, int flags, double *d_force,
+                                double *d_forcet, pinyb200_energies *e,
+                                void *stream);
+/* PINY-layout form (arrays as pinyb200_piny_force): forces ADDED to fx/fy/fz
+ * and, at the outer level, the virial forces to fxt/fyt/fzt (may be NULL)
+ * and pvten_tot; ghost forces are left on the ghost sites, as PINY's force
+ * routines leave them for energy_control_final. */
+int pinyb200_piny_force_respa(pinyb200_ctx *ctx, int level, double *const *x,
+                              double *const *y, double *const *z,
+                              const double *xmod, const double *ymod,
+                              const double *zmod, const double *hmat,
+                              double *const *fx, double *const *fy,
+                              double *const *fz, double *const *fxt,
+                              double *const *fyt, double *const *fzt,
+                              double *pvten_tot, pinyb200_energies *e);
+
+/*
  * Launch shapes and the autotuner.  A context runs with four choices:
  *   choice[0]  PME tile edge, 8 or 16 grid points (charges are binned per
  *              tile and bead; spread and gather run one block per tile)

@@ -227,7 +227,7 @@ int pinyb200_destroy(pinyb200_ctx *c)
                     c->d_twiddle32, c->d_err, c->d_mstart, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_chunk,
                     c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf, c->d_x0, c->d_forceP,
                     c->d_pme_head, c->d_pme_w, c->d_nchunk, c->d_ls, c->d_cs, c->d_mchunk, c->d_mmaskf,
-                    c->d_reach};
+                    c->d_reach, c->d_cut_res, c->d_bond_eq_res, c->d_forceW, c->d_forcet_aos};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->h_acc_pin) cudaFreeHost(c->h_acc_pin);
@@ -737,9 +737,24 @@ __global__ void centroid_kernel(const double *__restrict__ posT, double *__restr
 int pinyb200::enqueue_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const Cell &cell, int flags,
                              double *d_force, bool timing, double *h_acc)
 {
+    int rc = stage_positions(c, d_pos, d_xmod, cell, flags);
+    if (rc) return rc;
+    rc = evaluate_enqueue(c, cell, flags, timing, h_acc);
+    if (rc) return rc;
+    CK(launch_transpose_out(c, d_force));
+    return PINYB200_OK;
+}
+
+// Positions into the internal [atom][xyz][bead] layout, the mode-1
+// positions (given, or the bead centroid), and the device list update when
+// flags ask for it; enqueued on c->stream.
+int pinyb200::stage_positions(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const Cell &cell, int flags)
+{
     CK(launch_transpose_in(c, d_pos));
     if (c->P > 1) {
-        if (d_xmod) {
+        if (d_xmod == c->d_xmod) {
+            // already in place
+        } else if (d_xmod) {
             CK(cudaMemcpyAsync(c->d_xmod, d_xmod, (size_t)c->sys.natm * 3 * sizeof(double), cudaMemcpyDeviceToDevice,
                                c->stream));
         } else {
@@ -753,9 +768,6 @@ int pinyb200::enqueue_device(pinyb200_ctx *c, const double *d_pos, const double 
         int rc = list_update_enqueue(c, d_pos, c->P > 1 ? c->d_xmod : nullptr, cell, c->stream);
         if (rc) return rc;
     }
-    int rc = evaluate_enqueue(c, cell, flags, timing, h_acc);
-    if (rc) return rc;
-    CK(launch_transpose_out(c, d_force));
     return PINYB200_OK;
 }
 

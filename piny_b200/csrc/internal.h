@@ -209,6 +209,14 @@ struct pinyb200_ctx {
     // builds, tuning, PME tiles): captured graphs compare it before replay
     unsigned long long gen = 0;
     double *h_acc_pin = nullptr;  // pinned per-bead sums of the host-buffer call
+    // RESPA split (pinyb200_set_respa): PINY's weights and switches
+    bool respa_on = false;
+    double r_wter = 1, r_wter_res = 1, r_wtra_res = 1, r_rheal = 1;
+    int r_int_res_ter = 0, r_int_res_inter = 0, r_ires_bond = 0;
+    double *d_cut_res = nullptr;      // [npair_typ] inner cutoffs (Bohr)
+    double *d_bond_eq_res = nullptr;  // [nbond_typ] RESPA bond equilibria
+    double *d_forceW = nullptr;       // [natm][3][P] weighted forces of one level
+    double *d_forcet_aos = nullptr;   // [P][natm][3] staging of the virial forces
     pinyb200::GradHost grad;      // tangent channels of pinyb200_grad_prepare
     std::string err;
 };
@@ -222,6 +230,10 @@ cudaError_t launch_build_list(pinyb200_ctx *c, const Cell &cell, const double *d
                               const double *d_xm, const double *d_cutskin2, int pass, const int *gate = nullptr,
                               cudaStream_t st = nullptr);
 cudaError_t launch_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
+cudaError_t launch_pair_respa(pinyb200_ctx *c, const Cell &cell, int mode, double *target);
+cudaError_t launch_intra_respa(pinyb200_ctx *c, bool both, double *target);
+cudaError_t launch_ecor_weighted(pinyb200_ctx *c, double w, double *target);
+cudaError_t launch_pme_force_add_scaled(pinyb200_ctx *c, double w, double *target);
 cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
                             const double *d_cutskin2, int pass, const int *gate = nullptr,
                             cudaStream_t st = nullptr);
@@ -236,6 +248,7 @@ cudaError_t launch_pme_force_add(pinyb200_ctx *c);
 // c->stream without host synchronisation, and the host bookkeeping of its
 // per-bead sums; cell of an hmat; error recording
 int evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, bool timing, double *h_acc);
+int stage_positions(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const Cell &cell, int flags);
 void evaluate_finish(pinyb200_ctx *c, const Cell &cell, int flags, const double *acc, pinyb200_energies *e);
 int enqueue_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const Cell &cell, int flags,
                    double *d_force, bool timing, double *h_acc);
@@ -262,9 +275,9 @@ inline cudaError_t smem_optin(const void *func, int bytes)
 int record_error(pinyb200_ctx *c, int code, const std::string &msg);
 cudaError_t launch_intra(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_ghost_pos(pinyb200_ctx *c);
-cudaError_t launch_ghost_distrib(pinyb200_ctx *c);
+cudaError_t launch_ghost_distrib(pinyb200_ctx *c, double *fT = nullptr);
 cudaError_t launch_transpose_in(pinyb200_ctx *c, const double *d_pos_aos);
-cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_force_aos);
+cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_force_aos, const double *fT = nullptr);
 cudaError_t launch_list_count(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
                               const double *d_cutskin2, int *d_count, cudaStream_t st);
 cudaError_t launch_list_check(pinyb200_ctx *c, const double *d_pos, unsigned long long *d_out, cudaStream_t st);

@@ -149,6 +149,54 @@ __global__ void __launch_bounds__(256) bond_kernel(IntraArgs a, int nbond, const
     }
 }
 
+// One bend of one bead (bend.c:186-330): forces on the outer atoms f1, f3
+// (the middle atom takes -(f1 + f3)), the bond vectors for the virial, and
+// the energy.
+struct BendTerm {
+    double dx12, dy12, dz12, dx23, dy23, dz23;
+    double fx1, fy1, fz1, fx3, fy3, fz3;
+    double v;
+};
+
+__device__ __forceinline__ void bend_term(const double *posT, int P, int a1, int a2, int a3, int b,
+                                          const double *c, const double *s, const double *dc, const double *ds,
+                                          BendTerm &t)
+{
+    double x1, y1, z1, x2, y2, z2, x3, y3, z3;
+    load_x(posT, P, a1, b, x1, y1, z1);
+    load_x(posT, P, a2, b, x2, y2, z2);
+    load_x(posT, P, a3, b, x3, y3, z3);
+    const double dx12 = x1 - x2, dy12 = y1 - y2, dz12 = z1 - z2;
+    const double dx23 = x3 - x2, dy23 = y3 - y2, dz23 = z3 - z2;
+    const double r122i = 1.0 / (dx12 * dx12 + dy12 * dy12 + dz12 * dz12);
+    const double r12i = sqrt(r122i);
+    const double r322i = 1.0 / (dx23 * dx23 + dy23 * dy23 + dz23 * dz23);
+    const double r32i = sqrt(r322i);
+    const double rpmag = r12i * r32i;
+    double cost = (dx12 * dx23 + dy12 * dy23 + dz12 * dz23) * rpmag;
+    cost = cost < 1.0 ? cost : 1.0;
+    cost = cost > -1.0 ? cost : -1.0;
+    double sint = sqrt(1.0 - cost * cost);
+    sint = sint > 1.0e-8 ? sint : 1.0e-8;
+    const double cos122 = cost * r122i, cos322 = cost * r322i;
+    const double vc = ((((((c[6] * cost + c[5]) * cost + c[4]) * cost + c[3]) * cost + c[2]) * cost + c[1]) * cost +
+                       c[0]);
+    const double sisum = (((((s[6] * sint + s[5]) * sint + s[4]) * sint + s[3]) * sint + s[2]) * sint);
+    t.v = vc + (sisum * cost + s[1] * sint);
+    const double dvc = (((((dc[6] * cost + dc[5]) * cost + dc[4]) * cost + dc[3]) * cost + dc[2]) * cost + dc[1]);
+    double dvs = ((((ds[6] * sint + ds[5]) * sint + ds[4]) * sint + ds[3]) * sint + ds[2]);
+    dvs = dvs * cost + ds[1];
+    const double pre = -(dvc + sisum - dvs * cost / sint);
+    t.fx1 = (dx23 * rpmag - dx12 * cos122) * pre;
+    t.fy1 = (dy23 * rpmag - dy12 * cos122) * pre;
+    t.fz1 = (dz23 * rpmag - dz12 * cos122) * pre;
+    t.fx3 = (dx12 * rpmag - dx23 * cos322) * pre;
+    t.fy3 = (dy12 * rpmag - dy23 * cos322) * pre;
+    t.fz3 = (dz12 * rpmag - dz23 * cos322) * pre;
+    t.dx12 = dx12; t.dy12 = dy12; t.dz12 = dz12;
+    t.dx23 = dx23; t.dy23 = dy23; t.dz23 = dz23;
+}
+
 __global__ void __launch_bounds__(256) bend_kernel(IntraArgs a, int nbend, const int *__restrict__ bj,
                                                    const double *__restrict__ bc, const double *__restrict__ bs,
                                                    const double *__restrict__ bdc, const double *__restrict__ bds)
@@ -161,45 +209,18 @@ __global__ void __launch_bounds__(256) bend_kernel(IntraArgs a, int nbend, const
     for (long long t = t0; t < (long long)nbend * a.P; t += stride) {
         const int ib = (int)(t / a.P);
         const int a1 = bj[4 * ib], a2 = bj[4 * ib + 1], a3 = bj[4 * ib + 2], ty = bj[4 * ib + 3];
-        double x1, y1, z1, x2, y2, z2, x3, y3, z3;
-        load_x(a.posT, a.P, a1, b, x1, y1, z1);
-        load_x(a.posT, a.P, a2, b, x2, y2, z2);
-        load_x(a.posT, a.P, a3, b, x3, y3, z3);
-        const double dx12 = x1 - x2, dy12 = y1 - y2, dz12 = z1 - z2;
-        const double dx23 = x3 - x2, dy23 = y3 - y2, dz23 = z3 - z2;
-        const double r122i = 1.0 / (dx12 * dx12 + dy12 * dy12 + dz12 * dz12);
-        const double r12i = sqrt(r122i);
-        const double r322i = 1.0 / (dx23 * dx23 + dy23 * dy23 + dz23 * dz23);
-        const double r32i = sqrt(r322i);
-        const double rpmag = r12i * r32i;
-        double cost = (dx12 * dx23 + dy12 * dy23 + dz12 * dz23) * rpmag;
-        cost = cost < 1.0 ? cost : 1.0;
-        cost = cost > -1.0 ? cost : -1.0;
-        double sint = sqrt(1.0 - cost * cost);
-        sint = sint > 1.0e-8 ? sint : 1.0e-8;
-        const double cos122 = cost * r122i, cos322 = cost * r322i;
-        const double *c = bc + 7 * ty, *s = bs + 7 * ty, *dc = bdc + 7 * ty, *ds = bds + 7 * ty;
-        const double vc = ((((((c[6] * cost + c[5]) * cost + c[4]) * cost + c[3]) * cost + c[2]) * cost + c[1]) * cost +
-                           c[0]);
-        const double sisum = (((((s[6] * sint + s[5]) * sint + s[4]) * sint + s[3]) * sint + s[2]) * sint);
-        v += vc + (sisum * cost + s[1] * sint);
-        const double dvc = (((((dc[6] * cost + dc[5]) * cost + dc[4]) * cost + dc[3]) * cost + dc[2]) * cost + dc[1]);
-        double dvs = ((((ds[6] * sint + ds[5]) * sint + ds[4]) * sint + ds[3]) * sint + ds[2]);
-        dvs = dvs * cost + ds[1];
-        const double pre = -(dvc + sisum - dvs * cost / sint);
-        const double fx1 = (dx23 * rpmag - dx12 * cos122) * pre, fy1 = (dy23 * rpmag - dy12 * cos122) * pre,
-                     fz1 = (dz23 * rpmag - dz12 * cos122) * pre;
-        const double fx3 = (dx12 * rpmag - dx23 * cos322) * pre, fy3 = (dy12 * rpmag - dy23 * cos322) * pre,
-                     fz3 = (dz12 * rpmag - dz23 * cos322) * pre;
-        add_f(a.forceT, a.P, a1, b, fx1, fy1, fz1);
-        add_f(a.forceT, a.P, a2, b, -(fx1 + fx3), -(fy1 + fy3), -(fz1 + fz3));
-        add_f(a.forceT, a.P, a3, b, fx3, fy3, fz3);
-        p[0] += dx12 * fx1 + dx23 * fx3;
-        p[1] += dy12 * fy1 + dy23 * fy3;
-        p[2] += dz12 * fz1 + dz23 * fz3;
-        p[3] += dx12 * fy1 + dx23 * fy3;
-        p[4] += dx12 * fz1 + dx23 * fz3;
-        p[5] += dy12 * fz1 + dy23 * fz3;
+        BendTerm g;
+        bend_term(a.posT, a.P, a1, a2, a3, b, bc + 7 * ty, bs + 7 * ty, bdc + 7 * ty, bds + 7 * ty, g);
+        v += g.v;
+        add_f(a.forceT, a.P, a1, b, g.fx1, g.fy1, g.fz1);
+        add_f(a.forceT, a.P, a2, b, -(g.fx1 + g.fx3), -(g.fy1 + g.fy3), -(g.fz1 + g.fz3));
+        add_f(a.forceT, a.P, a3, b, g.fx3, g.fy3, g.fz3);
+        p[0] += g.dx12 * g.fx1 + g.dx23 * g.fx3;
+        p[1] += g.dy12 * g.fy1 + g.dy23 * g.fy3;
+        p[2] += g.dz12 * g.fz1 + g.dz23 * g.fz3;
+        p[3] += g.dx12 * g.fy1 + g.dx23 * g.fy3;
+        p[4] += g.dx12 * g.fz1 + g.dx23 * g.fz3;
+        p[5] += g.dy12 * g.fz1 + g.dy23 * g.fz3;
     }
     if (a.energy) {
         const int slot[7] = {S_VBEND, S_PXX, S_PYY, S_PZZ, S_PXY, S_PXZ, S_PYZ};
@@ -245,6 +266,96 @@ __global__ void __launch_bounds__(256) ecor_kernel(IntraArgs a, int necor, const
     }
 }
 
+// ---- RESPA: weighted intramolecular forces, no energies -------------------
+// Bonds at an inter level (bond_both.c:270-420): the full series at eq and
+// the RESPA series at eq_res, combined as w_res F_res + w_both (F - F_res).
+// At an intra-only level (bond.c:113-118, :270-278): one series, at eq_res
+// when use_res, times w_res.
+__global__ void __launch_bounds__(256) bond_w_kernel(int P, const double *__restrict__ posT, double *__restrict__ fW,
+                                                     int nbond, const int *__restrict__ bj,
+                                                     const double *__restrict__ eq, const double *__restrict__ eq_res,
+                                                     const double *__restrict__ dc, int both, int use_res,
+                                                     double w_res, double w_both)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nbond * P) return;
+    const int ib = (int)(t / P), b = (int)(t % P);
+    const int j1 = bj[3 * ib], j2 = bj[3 * ib + 1], ty = bj[3 * ib + 2];
+    double x1, y1, z1, x2, y2, z2;
+    load_x(posT, P, j1, b, x1, y1, z1);
+    load_x(posT, P, j2, b, x2, y2, z2);
+    const double dx = x1 - x2, dy = y1 - y2, dz = z1 - z2;
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const double *d = dc + 7 * ty;
+    double fx, fy, fz;
+    if (both) {
+        const double rr0 = r - eq[ty], rr0r = r - eq_res[ty];
+        const double dv = ((((d[6] * rr0 + d[5]) * rr0 + d[4]) * rr0 + d[3]) * rr0 + d[2]) * rr0 + d[1];
+        const double dvr = ((((d[6] * rr0r + d[5]) * rr0r + d[4]) * rr0r + d[3]) * rr0r + d[2]) * rr0r + d[1];
+        const double pre = -dv / r, prer = -dvr / r;
+        const double f1x = dx * pre, f1y = dy * pre, f1z = dz * pre;
+        const double f2x = dx * prer, f2y = dy * prer, f2z = dz * prer;
+        fx = w_res * f2x + w_both * (f1x - f2x);
+        fy = w_res * f2y + w_both * (f1y - f2y);
+        fz = w_res * f2z + w_both * (f1z - f2z);
+    } else {
+        const double rr0 = r - (use_res ? eq_res[ty] : eq[ty]);
+        const double dv = ((((d[6] * rr0 + d[5]) * rr0 + d[4]) * rr0 + d[3]) * rr0 + d[2]) * rr0 + d[1];
+        const double pre = -dv / r;
+        fx = dx * pre * w_res;
+        fy = dy * pre * w_res;
+        fz = dz * pre * w_res;
+    }
+    add_f(fW, P, j1, b, fx, fy, fz);
+    add_f(fW, P, j2, b, -fx, -fy, -fz);
+}
+
+// Bends x w (bend.c:144, :380-393).
+__global__ void __launch_bounds__(256) bend_w_kernel(int P, const double *__restrict__ posT, double *__restrict__ fW,
+                                                     int nbend, const int *__restrict__ bj,
+                                                     const double *__restrict__ bc, const double *__restrict__ bs,
+                                                     const double *__restrict__ bdc, const double *__restrict__ bds,
+                                                     double w)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nbend * P) return;
+    const int ib = (int)(t / P), b = (int)(t % P);
+    const int a1 = bj[4 * ib], a2 = bj[4 * ib + 1], a3 = bj[4 * ib + 2], ty = bj[4 * ib + 3];
+    BendTerm g;
+    bend_term(posT, P, a1, a2, a3, b, bc + 7 * ty, bs + 7 * ty, bdc + 7 * ty, bds + 7 * ty, g);
+    const double fx2 = -(g.fx1 + g.fx3), fy2 = -(g.fy1 + g.fy3), fz2 = -(g.fz1 + g.fz3);
+    add_f(fW, P, a1, b, g.fx1 * w, g.fy1 * w, g.fz1 * w);
+    add_f(fW, P, a2, b, fx2 * w, fy2 * w, fz2 * w);
+    add_f(fW, P, a3, b, g.fx3 * w, g.fy3 * w, g.fz3 * w);
+}
+
+// Ewald exclusion correction x w (ecorr.c:100, :229-245).
+__global__ void __launch_bounds__(256) ecor_w_kernel(int P, const double *__restrict__ posT, double *__restrict__ fW,
+                                                     const double *__restrict__ charge, int necor,
+                                                     const int *__restrict__ j1s, const int *__restrict__ j2s,
+                                                     int nsplin, double rmin, double dr, double dri,
+                                                     const double4 *__restrict__ tab, double w)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)necor * P) return;
+    const int ie = (int)(t / P), b = (int)(t % P);
+    const int j1 = j1s[ie], j2 = j2s[ie];
+    double x1, y1, z1, x2, y2, z2;
+    load_x(posT, P, j1, b, x1, y1, z1);
+    load_x(posT, P, j2, b, x2, y2, z2);
+    const double dx = x1 - x2, dy = y1 - y2, dz = z1 - z2;
+    const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+    int k = __double2int_rz(__dadd_rn(__dmul_rn(__dsub_rn(r, rmin), dri), 0.5)) + 3;
+    k = k < nsplin - 2 ? k : nsplin - 2;
+    k = k > 3 ? k : 3;
+    const double rsp = __dadd_rn(__dmul_rn((double)(k - 3), dr), rmin);
+    const double del = __dmul_rn(__dsub_rn(r, rsp), dri);
+    const double dvt = spline_eval<double4, double>(tab[nsplin + k - 1], del) * (charge[j1] * charge[j2]);
+    const double fx = dx * dvt * w, fy = dy * dvt * w, fz = dz * dvt * w;
+    add_f(fW, P, j1, b, fx, fy, fz);
+    add_f(fW, P, j2, b, -fx, -fy, -fz);
+}
+
 static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // grid-stride launch size for the intramolecular kernels
@@ -261,10 +372,10 @@ cudaError_t launch_transpose_in(pinyb200_ctx *c, const double *d_aos)
     return cudaGetLastError();
 }
 
-cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_aos)
+cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_aos, const double *fT)
 {
     const long long n = (long long)c->sys.natm * 3 * c->P;
-    transpose_out_kernel<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_forceT, d_aos, c->sys.natm, c->P);
+    transpose_out_kernel<<<nblk(n, 256), 256, 0, c->stream>>>(fT ? fT : c->d_forceT, d_aos, c->sys.natm, c->P);
     return cudaGetLastError();
 }
 
@@ -277,12 +388,12 @@ cudaError_t launch_ghost_pos(pinyb200_ctx *c)
     return cudaGetLastError();
 }
 
-cudaError_t launch_ghost_distrib(pinyb200_ctx *c)
+cudaError_t launch_ghost_distrib(pinyb200_ctx *c, double *fT)
 {
     const DeviceSystem &s = c->sys;
     if (s.nghost == 0) return cudaSuccess;
     ghost_distrib_kernel<<<nblk((long long)s.nghost * c->P, 256), 256, 0, c->stream>>>(
-        c->d_forceT, c->P, s.nghost, s.ghost_ncomp, s.ghost_atom, s.ghost_comp, s.ghost_coef);
+        fT ? fT : c->d_forceT, c->P, s.nghost, s.ghost_ncomp, s.ghost_atom, s.ghost_comp, s.ghost_coef);
     return cudaGetLastError();
 }
 
@@ -307,6 +418,33 @@ cudaError_t launch_intra(pinyb200_ctx *c, const Cell &cell, bool energy)
     if (s.necor)
         ecor_kernel<<<nblk_gs(c, (long long)s.necor * c->P), 256, 0, c->stream>>>(
             a, s.necor, s.ecor_j1, s.ecor_j2, s.ecor_nsplin, s.ecor_rmin, s.ecor_dr, s.ecor_dri, s.ecor_tab);
+    return cudaGetLastError();
+}
+
+// Weighted bonds and bends of one RESPA level into target: bond_both's
+// combination when both (inter levels), else bond() with PINY's ires_bond
+// choice of equilibrium; bends x wght_tra_res.
+cudaError_t launch_intra_respa(pinyb200_ctx *c, bool both, double *target)
+{
+    const DeviceSystem &s = c->sys;
+    const double w_both = c->r_int_res_inter ? c->r_wter_res : c->r_wter;  // bond_both.c:156-161
+    if (s.nbond)
+        bond_w_kernel<<<nblk((long long)s.nbond * c->P, 256), 256, 0, c->stream>>>(
+            c->P, c->d_posT, target, s.nbond, s.bond_j, s.bond_eq, c->d_bond_eq_res, s.bond_dc, both ? 1 : 0,
+            c->r_ires_bond, c->r_wtra_res, w_both);
+    if (s.nbend)
+        bend_w_kernel<<<nblk((long long)s.nbend * c->P, 256), 256, 0, c->stream>>>(
+            c->P, c->d_posT, target, s.nbend, s.bend_j, s.bend_c, s.bend_s, s.bend_dc, s.bend_ds, c->r_wtra_res);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ecor_weighted(pinyb200_ctx *c, double w, double *target)
+{
+    const DeviceSystem &s = c->sys;
+    if (!s.necor) return cudaSuccess;
+    ecor_w_kernel<<<nblk((long long)s.necor * c->P, 256), 256, 0, c->stream>>>(
+        c->P, c->d_posT, target, s.charge, s.necor, s.ecor_j1, s.ecor_j2, s.ecor_nsplin, s.ecor_rmin, s.ecor_dr,
+        s.ecor_dri, s.ecor_tab, w);
     return cudaGetLastError();
 }
 

@@ -38,9 +38,17 @@ struct PairArgs {
     double *acc;
     int energy;
     const int *bad;  // device flags (overflow, mismatch) of the list update, or nullptr
+    // RESPA split (force_npol.c:805-816, :1030-1060): 0 off; 1 inner level
+    // (shave at cut_res, force x swit w_res); 2 outer level with the switch
+    // (force x (swit w_res + (1 - swit) w_full)); 3 outer level without
+    // inter RESPA (force x w_full).  swit = 1 - 3 br^2 + 2 br^3 with
+    // br = clamp((r - cut_res + rheal) / rheal, 0, 1).
+    int respa;
+    const double *cut_res;
+    double rheal, rheali, w_res, w_full;
 };
 
-template <typename R, int P>
+template <typename R, int P, bool RSP>
 __global__ void __launch_bounds__(256) pair_kernel(PairArgs a, Cell cell)
 {
     if (a.bad && (a.bad[0] | a.bad[1])) {
@@ -88,7 +96,7 @@ __global__ void __launch_bounds__(256) pair_kernel(PairArgs a, Cell cell)
             const int j = a.col[jj];
             const int pt = pair_type(ti, a.atm_typ[j], a.ntyp);
             const int u = a.inter_map[pt];
-            const R rc = (R)a.cutoff[pt];
+            const R rc = (R)((RSP && a.respa == 1) ? a.cut_res[pt] : a.cutoff[pt]);
             const R rmin = (R)a.rmin[u], dr = (R)a.dr[u], dri = (R)a.dri[u];
             const int vdw = a.has_vdw[u];
             const R q2 = (R)(qi * a.charge[j]);
@@ -122,7 +130,20 @@ __global__ void __launch_bounds__(256) pair_kernel(PairArgs a, Cell cell)
                 const int k = Idx<R>::knot(r, rmin, dr, dri, nsm2, del);
                 R dv = q2 * spline_eval<V, R>(ldg4(tF + (k - 1)), del);
                 if (vdw) dv += spline_eval<V, R>(ldg4(tV + (k - 1)), del);
-                const R fx = rx * dv, fy = ry * dv, fz = rz * dv;
+                R fx = rx * dv, fy = ry * dv, fz = rz * dv;
+                if (RSP) {
+                    R fm = (R)a.w_full;
+                    if (a.respa != 3) {
+                        R br = (r - (R)a.cut_res[pt] + (R)a.rheal) * (R)a.rheali;
+                        br = br > (R)0 ? br : (R)0;
+                        br = br < (R)1 ? br : (R)1;
+                        const R swit = br * br * (br * (R)2 - (R)3) + (R)1;
+                        fm = a.respa == 1 ? swit * (R)a.w_res : swit * (R)a.w_res + ((R)1 - swit) * (R)a.w_full;
+                    }
+                    fx *= fm;
+                    fy *= fm;
+                    fz *= fm;
+                }
                 fi[s][0] += (double)fx;
                 fi[s][1] += (double)fy;
                 fi[s][2] += (double)fz;
@@ -166,7 +187,7 @@ __global__ void __launch_bounds__(256) pair_kernel(PairArgs a, Cell cell)
     }
 }
 
-template <typename R, int P>
+template <typename R, int P, bool RSP>
 static void launch_pair_t(pinyb200_ctx *c, const PairArgs &a, const Cell &cell)
 {
     const int threads = 256;
@@ -174,26 +195,26 @@ static void launch_pair_t(pinyb200_ctx *c, const PairArgs &a, const Cell &cell)
     long long blocks = (rows * 32 + threads - 1) / threads;
     long long maxb = (long long)c->sm_count * c->pair_blocks_per_sm;
     if (blocks > maxb) blocks = maxb;
-    pair_kernel<R, P><<<(int)blocks, threads, 0, c->stream>>>(a, cell);
+    pair_kernel<R, P, RSP><<<(int)blocks, threads, 0, c->stream>>>(a, cell);
 }
 
-template <typename R>
+template <typename R, bool RSP>
 static cudaError_t launch_pair_r(pinyb200_ctx *c, const PairArgs &a, const Cell &cell)
 {
     switch (c->P) {
-    case 1: launch_pair_t<R, 1>(c, a, cell); break;
-    case 2: launch_pair_t<R, 2>(c, a, cell); break;
-    case 4: launch_pair_t<R, 4>(c, a, cell); break;
-    case 8: launch_pair_t<R, 8>(c, a, cell); break;
-    case 16: launch_pair_t<R, 16>(c, a, cell); break;
-    case 32: launch_pair_t<R, 32>(c, a, cell); break;
-    case 64: launch_pair_t<R, 64>(c, a, cell); break;
+    case 1: launch_pair_t<R, 1, RSP>(c, a, cell); break;
+    case 2: launch_pair_t<R, 2, RSP>(c, a, cell); break;
+    case 4: launch_pair_t<R, 4, RSP>(c, a, cell); break;
+    case 8: launch_pair_t<R, 8, RSP>(c, a, cell); break;
+    case 16: launch_pair_t<R, 16, RSP>(c, a, cell); break;
+    case 32: launch_pair_t<R, 32, RSP>(c, a, cell); break;
+    case 64: launch_pair_t<R, 64, RSP>(c, a, cell); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_pair(pinyb200_ctx *c, const Cell &cell, bool energy)
+static PairArgs pair_args(pinyb200_ctx *c, bool energy)
 {
     const DeviceSystem &s = c->sys;
     PairArgs a;
@@ -218,12 +239,34 @@ cudaError_t launch_pair(pinyb200_ctx *c, const Cell &cell, bool energy)
     a.acc = c->d_acc;
     a.energy = energy ? 1 : 0;
     a.bad = c->d_ls ? (const int *)((const char *)c->d_ls + offsetof(ListState, overflow)) : nullptr;
-    if (c->precision == PINYB200_FP64) {
-        a.tab = s.tab64;
-        return launch_pair_r<double>(c, a, cell);
-    }
-    a.tab = s.tab32;
-    return launch_pair_r<float>(c, a, cell);
+    a.tab = c->precision == PINYB200_FP64 ? (const void *)s.tab64 : (const void *)s.tab32;
+    a.respa = 0;
+    a.cut_res = nullptr;
+    a.rheal = a.rheali = a.w_res = a.w_full = 1.0;
+    return a;
+}
+
+cudaError_t launch_pair(pinyb200_ctx *c, const Cell &cell, bool energy)
+{
+    const PairArgs a = pair_args(c, energy);
+    if (c->precision == PINYB200_FP64) return launch_pair_r<double, false>(c, a, cell);
+    return launch_pair_r<float, false>(c, a, cell);
+}
+
+// One RESPA pass of the real-space pair forces over the active site list
+// into target ([natm][3][P]); no energies.  mode as PairArgs::respa.
+cudaError_t launch_pair_respa(pinyb200_ctx *c, const Cell &cell, int mode, double *target)
+{
+    PairArgs a = pair_args(c, false);
+    a.forceT = target;
+    a.respa = mode;
+    a.cut_res = c->d_cut_res;
+    a.rheal = c->r_rheal;
+    a.rheali = 1.0 / c->r_rheal;
+    a.w_res = c->r_wter_res;
+    a.w_full = c->r_wter;
+    if (c->precision == PINYB200_FP64) return launch_pair_r<double, true>(c, a, cell);
+    return launch_pair_r<float, true>(c, a, cell);
 }
 
 }  // namespace pinyb200

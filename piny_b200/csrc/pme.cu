@@ -443,6 +443,20 @@ __global__ void __launch_bounds__(256) pme_force_add_kernel(int nchrg, int P, co
     fT[(3 * (size_t)ichrg[k] + d) * P + b] += fP[t];
 }
 
+// RESPA outer level: PME forces x wght_ter into another buffer
+// (ewald3d_pme.c: forces x wght_now before they are added).
+__global__ void __launch_bounds__(256) pme_force_add_scaled_kernel(int nchrg, int P, const int *__restrict__ ichrg,
+                                                                   const double *__restrict__ fP, double w,
+                                                                   double *__restrict__ fT)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nchrg * 3 * P) return;
+    const long long kd = t / P;
+    const int b = (int)(t - kd * P);
+    const int k = (int)(kd / 3), d = (int)(kd - 3LL * k);
+    fT[(3 * (size_t)ichrg[k] + d) * P + b] += fP[t] * w;
+}
+
 // Gather: one block per (tile, bead); the tile's potential (with the
 // stencil reach) is copied to shared memory once and the bin's records read
 // it there.  Overflow records read the grid directly.  Every (charge, bead)
@@ -1054,6 +1068,16 @@ cudaError_t launch_pme_force_add(pinyb200_ctx *c)
     const long long n = (long long)c->sys.nchrg * 3 * c->P;
     pme_force_add_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->sys.nchrg, c->P, c->sys.ichrg,
                                                                             c->d_forceP, c->d_forceT);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pme_force_add_scaled(pinyb200_ctx *c, double w, double *target)
+{
+    if (c->sys.nchrg == 0 || c->sys.nktot == 0) return cudaSuccess;
+    const long long n = (long long)c->sys.nchrg * 3 * c->P;
+    pme_force_add_scaled_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->sys.nchrg, c->P,
+                                                                                   c->sys.ichrg, c->d_forceP, w,
+                                                                                   target);
     return cudaGetLastError();
 }
 

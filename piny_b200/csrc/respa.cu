@@ -1,0 +1,220 @@
+// PINY's RESPA split of the force path (respa_steps_lrf / _intra / _pimd).
+//
+// int_NVT_pimd (int_NVT_pimd.c:142-223) nests inter, torsion, intra and bead
+// RESPA loops and asks the force routines for one level per inner step
+// through energy_ctrl's iget_full_inter / iget_res_inter / iget_full_intra /
+// iget_res_intra (:175-189).  Each term carries the number of inner steps its
+// impulse spans (energy_control_initial.c:211-243):
+//   real space   outer level: x (swit wght_ter_res + (1 - swit) wght_ter),
+//                or x wght_ter without inter RESPA; inner inter level:
+//                shave at cutoff_res, x swit wght_ter_res (force_npol.c)
+//   PME, ecor    outer level only, x wght_ter (energy_control_inter_recip.c)
+//   bonds        inter levels: bond_both, wght_tra_res F_res + w (F - F_res);
+//                intra levels: bond() x wght_tra_res at the RESPA equilibrium
+//                when nres_tra nres_tor > 1 (energy_control_intra.c:116-140)
+//   bends        x wght_tra_res at every intra level (bend.c)
+// The outer level also yields the unweighted forces PINY adds to the virial
+// forces fxt, its energies and pvten_tot: that is the plain evaluation, run
+// into the context's force buffer, while the weighted forces go to a second
+// buffer ([atom][xyz][bead] like the first).
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+using namespace pinyb200;
+
+namespace {
+
+int check_level(pinyb200_ctx *c, int level)
+{
+    const int intra = PINYB200_FULL_INTRA | PINYB200_RES_INTRA;
+    const bool ok = level == PINYB200_RES_INTRA || level == intra ||
+                    (level == (PINYB200_RES_INTER | intra) && c->r_int_res_ter) ||
+                    level == (PINYB200_FULL_INTER | intra | (c->r_int_res_ter ? PINYB200_RES_INTER : 0));
+    if (ok) return PINYB200_OK;
+    return record_error(c, PINYB200_ERR_ARG,
+                        "respa_force: level " + std::to_string(level) +
+                            " is not one PINY's RESPA loops set (int_res_ter = " + std::to_string(c->r_int_res_ter) +
+                            ")");
+}
+
+#define RK(x)                                                                          \
+    do {                                                                               \
+        cudaError_t e_ = (x);                                                          \
+        if (e_ != cudaSuccess) return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e_)); \
+    } while (0)
+
+// One level, enqueued on c->stream; the weighted forces end in c->d_forceW,
+// the outer level's unweighted ones in c->d_forceT (and its per-bead sums
+// are copied to h_acc).
+int respa_enqueue(pinyb200_ctx *c, const Cell &cell, int level, int flags, double *h_acc)
+{
+    const size_t nb = (size_t)c->sys.natm * 3 * c->P;
+    const bool outer = level & PINYB200_FULL_INTER;
+    const bool inter = level & (PINYB200_FULL_INTER | PINYB200_RES_INTER);
+    const bool distrib = flags & PINYB200_DISTRIB_GHOSTS;
+    if (outer) {
+        int rc = evaluate_enqueue(c, cell, flags & ~PINYB200_DISTRIB_GHOSTS, false, h_acc);
+        if (rc) return rc;
+    } else {
+        RK(launch_ghost_pos(c));
+    }
+    RK(cudaMemsetAsync(c->d_forceW, 0, nb * sizeof(double), c->stream));
+    if (inter) RK(launch_pair_respa(c, cell, outer ? (c->r_int_res_ter ? 2 : 3) : 1, c->d_forceW));
+    if (outer) {
+        RK(launch_pme_force_add_scaled(c, c->r_wter, c->d_forceW));
+        RK(launch_ecor_weighted(c, c->r_wter, c->d_forceW));
+    }
+    RK(launch_intra_respa(c, inter, c->d_forceW));
+    if (distrib) {
+        RK(launch_ghost_distrib(c, c->d_forceW));
+        if (outer) RK(launch_ghost_distrib(c, c->d_forceT));
+    }
+    return PINYB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pinyb200_set_respa(pinyb200_ctx *c, const pinyb200_respa *r)
+{
+    if (!c) return record_error(c, PINYB200_ERR_ARG, "set_respa: NULL context");
+    RK(cudaSetDevice(c->device));
+    if (!r) {
+        c->respa_on = false;
+        return PINYB200_OK;
+    }
+    if (!r->cutoff_res || (c->sys.nbond && !r->bond_eq_res))
+        return record_error(c, PINYB200_ERR_ARG, "set_respa: cutoff_res / bond_eq_res missing");
+    if (!(r->rheal_res > 0.0)) return record_error(c, PINYB200_ERR_ARG, "set_respa: rheal_res must be > 0");
+    if (!(r->wght_ter >= 1.0 && r->wght_ter_res >= 1.0 && r->wght_tra_res >= 1.0))
+        return record_error(c, PINYB200_ERR_ARG, "set_respa: RESPA weights are step counts (>= 1)");
+    const int npt = c->sys.npair_typ;
+    for (int k = 0; k < npt; k++)
+        if (!(r->cutoff_res[k] > 0.0) || r->cutoff_res[k] > c->h_cutoff[k])
+            return record_error(c, PINYB200_ERR_ARG, "set_respa: cutoff_res must lie in (0, cutoff]");
+    if (!c->d_cut_res) RK(cudaMalloc(&c->d_cut_res, (size_t)npt * sizeof(double)));
+    RK(cudaMemcpy(c->d_cut_res, r->cutoff_res, (size_t)npt * sizeof(double), cudaMemcpyHostToDevice));
+    if (c->sys.nbond) {
+        if (!c->d_bond_eq_res) RK(cudaMalloc(&c->d_bond_eq_res, (size_t)c->nbond_typ * sizeof(double)));
+        RK(cudaMemcpy(c->d_bond_eq_res, r->bond_eq_res, (size_t)c->nbond_typ * sizeof(double),
+                      cudaMemcpyHostToDevice));
+    }
+    if (!c->d_forceW) RK(cudaMalloc(&c->d_forceW, (size_t)c->sys.natm * 3 * c->P * sizeof(double)));
+    c->r_wter = r->wght_ter;
+    c->r_wter_res = r->wght_ter_res;
+    c->r_wtra_res = r->wght_tra_res;
+    c->r_int_res_ter = r->int_res_ter ? 1 : 0;
+    c->r_int_res_inter = r->int_res_inter ? 1 : 0;
+    c->r_ires_bond = r->ires_bond ? 1 : 0;
+    c->r_rheal = r->rheal_res;
+    c->respa_on = true;
+    return PINYB200_OK;
+}
+
+int pinyb200_respa_force_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const double *hmat,
+                                int level, int flags, double *d_force, double *d_forcet, pinyb200_energies *e,
+                                void *stream)
+{
+    if (!c || !d_pos || !hmat || !d_force) return record_error(c, PINYB200_ERR_ARG, "respa_force: NULL argument");
+    if (!c->have_list) return record_error(c, PINYB200_ERR_STATE, "respa_force: build the Verlet list first");
+    if (!c->respa_on) return record_error(c, PINYB200_ERR_STATE, "respa_force: pinyb200_set_respa first");
+    if (int rc = check_level(c, level)) return rc;
+    RK(cudaSetDevice(c->device));
+    cudaStream_t own = c->stream;
+    if (stream) c->stream = (cudaStream_t)stream;
+    struct Restore {
+        pinyb200_ctx *c;
+        cudaStream_t s;
+        ~Restore() { c->stream = s; }
+    } restore{c, own};
+    const Cell cell = cell_from_hmat(hmat);
+    const bool outer = level & PINYB200_FULL_INTER;
+    const bool energy = outer && !(flags & PINYB200_NO_ENERGY);
+    std::vector<double> acc(outer ? (size_t)c->P * S_NSLOT : 0);
+    int rc = stage_positions(c, d_pos, d_xmod, cell, flags);
+    if (rc) return rc;
+    rc = respa_enqueue(c, cell, level, flags, outer ? acc.data() : nullptr);
+    if (rc) return rc;
+    RK(launch_transpose_out(c, d_force, c->d_forceW));
+    if (outer && d_forcet) RK(launch_transpose_out(c, d_forcet, c->d_forceT));
+    RK(cudaStreamSynchronize(c->stream));
+    if (e) {
+        if (energy) {
+            evaluate_finish(c, cell, flags, acc.data(), e);
+            if (!std::isfinite(e->vintert + e->vintrat))
+                return record_error(c, PINYB200_ERR_NAN, "non-finite energy: check the positions");
+        } else {
+            memset(e, 0, sizeof(*e));
+        }
+    }
+    return PINYB200_OK;
+}
+
+int pinyb200_piny_force_respa(pinyb200_ctx *c, int level, double *const *x, double *const *y, double *const *z,
+                              const double *xmod, const double *ymod, const double *zmod, const double *hmat,
+                              double *const *fx, double *const *fy, double *const *fz, double *const *fxt,
+                              double *const *fyt, double *const *fzt, double *pvten_tot, pinyb200_energies *e)
+{
+    if (!c || !x || !y || !z || !hmat || !fx || !fy || !fz)
+        return record_error(c, PINYB200_ERR_ARG, "piny_force_respa: NULL argument");
+    const int natm = c->sys.natm, P = c->P;
+    const size_t nb = (size_t)P * natm * 3;
+    std::vector<double> pos(nb), frc(nb), frt;
+    for (int b = 0; b < P; b++)
+        for (int i = 0; i < natm; i++) {
+            pos[((size_t)b * natm + i) * 3 + 0] = x[b][i + 1];
+            pos[((size_t)b * natm + i) * 3 + 1] = y[b][i + 1];
+            pos[((size_t)b * natm + i) * 3 + 2] = z[b][i + 1];
+        }
+    RK(cudaSetDevice(c->device));
+    const bool outer = level & PINYB200_FULL_INTER;
+    const bool want_t = outer && fxt && fyt && fzt;
+    if (want_t && !c->d_forcet_aos) RK(cudaMalloc(&c->d_forcet_aos, nb * sizeof(double)));
+    double *d_xm = nullptr;
+    if (P > 1 && xmod && ymod && zmod) {
+        std::vector<double> xm((size_t)natm * 3);
+        for (int i = 0; i < natm; i++) {
+            xm[3 * i] = xmod[i + 1];
+            xm[3 * i + 1] = ymod[i + 1];
+            xm[3 * i + 2] = zmod[i + 1];
+        }
+        // the mode-1 positions go straight to the context's own buffer
+        RK(cudaMemcpy(c->d_xmod, xm.data(), xm.size() * sizeof(double), cudaMemcpyHostToDevice));
+        d_xm = c->d_xmod;
+    }
+    RK(cudaMemcpy(c->d_pos_aos, pos.data(), nb * sizeof(double), cudaMemcpyHostToDevice));
+    double h[9];
+    for (int k = 0; k < 9; k++) h[k] = hmat[k + 1];
+    pinyb200_energies en;
+    int rc = pinyb200_respa_force_device(c, c->d_pos_aos, d_xm, h, level, 0, c->d_force_aos,
+                                         want_t ? c->d_forcet_aos : nullptr, &en, nullptr);
+    if (rc) return rc;
+    RK(cudaMemcpy(frc.data(), c->d_force_aos, nb * sizeof(double), cudaMemcpyDeviceToHost));
+    if (want_t) {
+        frt.resize(nb);
+        RK(cudaMemcpy(frt.data(), c->d_forcet_aos, nb * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    for (int b = 0; b < P; b++)
+        for (int i = 0; i < natm; i++) {
+            const size_t o = ((size_t)b * natm + i) * 3;
+            fx[b][i + 1] += frc[o];
+            fy[b][i + 1] += frc[o + 1];
+            fz[b][i + 1] += frc[o + 2];
+            if (want_t) {
+                fxt[b][i + 1] += frt[o];
+                fyt[b][i + 1] += frt[o + 1];
+                fzt[b][i + 1] += frt[o + 2];
+            }
+        }
+    if (outer && pvten_tot)
+        for (int k = 0; k < 9; k++) pvten_tot[k + 1] += en.pvten[k];
+    if (e) *e = en;
+    return PINYB200_OK;
+}
+
+}  // extern "C"

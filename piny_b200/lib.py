@@ -86,6 +86,12 @@ class PinyPimdEnergies(C.Structure):
                 ("pvten_mode_tot", _d * 9)]
 
 
+class PinyRespa(C.Structure):
+    _fields_ = [("wght_ter", _d), ("wght_ter_res", _d), ("wght_tra_res", _d),
+                ("int_res_ter", _i), ("int_res_inter", _i), ("ires_bond", _i),
+                ("cutoff_res", _pd), ("rheal_res", _d), ("bond_eq_res", _pd)]
+
+
 class PinyTangent(C.Structure):
     """pinyb200_tangent: derivative of the set-up data along one parameter."""
     _fields_ = [("dcharge", _pd), ("dcv0", _pd), ("dcdv0", _pd), ("dghost_coef", _pd), ("dbond_eq", _pd),
@@ -103,7 +109,8 @@ EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb
            "pinyb200_batch_last_error", "pinyb200_grad_prepare", "pinyb200_grad",
            "pinyb200_fma_peak", "pinyb200_pimd_transform", "pinyb200_pimd_create", "pinyb200_pimd_destroy",
            "pinyb200_pimd_set_nhc", "pinyb200_pimd_get_nhc", "pinyb200_pimd_forces", "pinyb200_pimd_step",
-           "pinyb200_update_list_device", "pinyb200_list_set_spread", "pinyb200_list_status")
+           "pinyb200_update_list_device", "pinyb200_list_set_spread", "pinyb200_list_status",
+           "pinyb200_set_respa", "pinyb200_respa_force_device", "pinyb200_piny_force_respa")
 
 STAGING, NORMAL_MODES = 1, 2                      # PINYB200_STAGING / _NORMAL_MODES
 TO_MODES, TO_BEADS, FORCE_TO_MODES = 0, 1, 2      # PINYB200_TO_MODES / _TO_BEADS / _FORCE_TO_MODES
@@ -172,6 +179,11 @@ def load(build_if_missing: bool = True):
     L.pinyb200_pimd_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _pd,
                                      C.POINTER(PinyPimdEnergies), C.c_void_p]
     L.pinyb200_last_error.restype = C.c_char_p
+    L.pinyb200_set_respa.argtypes = [C.c_void_p, C.POINTER(PinyRespa)]
+    L.pinyb200_respa_force_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, _i, _i, C.c_void_p,
+                                              C.c_void_p, C.POINTER(PinyEnergies), C.c_void_p]
+    L.pinyb200_piny_force_respa.argtypes = [C.c_void_p, _i] + [C.c_void_p] * 3 + [_pd] * 3 + [_pd] + \
+        [C.c_void_p] * 6 + [_pd, C.POINTER(PinyEnergies)]
     L.pinyb200_last_error.argtypes = [C.c_void_p]
     _LIB = L
     return L
@@ -355,6 +367,37 @@ class DeviceBox:
                                                         flags, C.c_void_p(d_force), C.byref(e),
                                                         None if stream is None else C.c_void_p(stream)),
                     "energy_force_device")
+        return energies_dict(e)
+
+    def set_respa(self, respa):
+        """PINY's RESPA split (a dict as piny_b200.respa.respa_setup makes;
+        None switches it off)."""
+        if respa is None:
+            self._check(self.L.pinyb200_set_respa(self.h, None), "set_respa")
+            return
+        cut = np.ascontiguousarray(respa["cutoff_res"], np.float64)
+        eqr = np.ascontiguousarray(respa["bond_eq_res"], np.float64)
+        r = PinyRespa(float(respa["wght_ter"]), float(respa["wght_ter_res"]), float(respa["wght_tra_res"]),
+                      int(respa["int_res_ter"]), int(respa["int_res_inter"]), int(respa["ires_bond"]), _dp(cut),
+                      float(respa["rheal_res"]), _dp(eqr))
+        self._check(self.L.pinyb200_set_respa(self.h, C.byref(r)), "set_respa")
+
+    def respa_force_device(self, d_pos: int, d_xmod, hmat, level: int, d_force: int, d_forcet=None, stream=None,
+                           distribute_ghosts=False, energy=True, update_list=False):
+        """One RESPA level (piny_b200.respa bits) from device positions:
+        PINY's weighted forces into d_force and, at the outer level, the
+        unweighted virial forces into d_forcet; returns the energies (zero
+        at inner levels)."""
+        hmat = np.ascontiguousarray(hmat, np.float64)
+        e = PinyEnergies()
+        flags = (DISTRIB_GHOSTS if distribute_ghosts else 0) | (0 if energy else NO_ENERGY) | \
+            (UPDATE_LIST if update_list else 0)
+        self._check(self.L.pinyb200_respa_force_device(self.h, C.c_void_p(d_pos),
+                                                       None if d_xmod is None else C.c_void_p(d_xmod), _dp(hmat),
+                                                       int(level), flags, C.c_void_p(d_force),
+                                                       None if d_forcet is None else C.c_void_p(d_forcet),
+                                                       C.byref(e), None if stream is None else C.c_void_p(stream)),
+                    "respa_force_device")
         return energies_dict(e)
 
     def autotune(self, d_pos: int, d_xmod, hmat, reps=3, again=False, energy=True):
