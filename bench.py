@@ -45,7 +45,9 @@ def parse_args():
     ap.add_argument("--config", default="tip4pf_4096_p32",
                     help="a named box; c4_batch64: 64 uneven boxes in one graph launch per step; "
                          "c5_grad: parameter gradients of 1024 TIP4P/F x 16 beads; "
-                         "pimd_nvt: PINY's NVT ring-polymer MD step of 4096 TIP4P/F x 32 beads")
+                         "pimd_nvt: PINY's NVT ring-polymer MD step of 4096 TIP4P/F x 32 beads; "
+                         "respa: the force calls of one PINY RESPA step (respa_steps_lrf 2, respa_steps_intra 2) "
+                         "of 4096 TIP4P/F x 32 beads")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
@@ -457,6 +459,114 @@ def run_pimd(args, ws, rank, local):
     return 0
 
 
+def run_respa(args, ws, rank, local):
+    """The force calls of one PINY RESPA step on the device: 4096 q-TIP4P/F
+    x 32 beads, respa_steps_lrf 2, respa_steps_intra 2 (inner cutoff 5 A,
+    switch width 1 A), so int_NVT_pimd's loops ask for the levels
+    [innermost, inner inter, innermost, outer] (piny_b200.respa.loop_levels).
+    A step is those four calls; the plain evaluation, which a run without
+    RESPA makes at each of the four inner time steps, is timed beside it."""
+    import dataclasses
+
+    import torch
+
+    from piny_b200 import respa as R
+    from piny_b200 import system, water
+    from piny_b200.lib import DeviceBox
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    spec = water.named_spec("tip4pf_4096_p32")
+    if ws > 1:
+        spec = dataclasses.replace(spec, seed=spec.seed + rank)
+    pos = water.build_positions(spec) / water.BOHR
+    S = system.build_system(spec, pos)
+    P = spec.nbeads
+    xmod = pos.mean(axis=0)
+    box = DeviceBox(S, P, args.precision)
+    box.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+    nres = (2, 1, 2, 1)
+    cut_res = np.minimum(np.asarray(S["cutoff"]), 5.0 / water.BOHR)
+    rs = R.respa_setup(*nres, True, True, cut_res, 1.0 / water.BOHR, np.asarray(S["bond_eq"]))
+    box.set_respa(rs)
+    levels = [lv for lv in R.loop_levels(*nres, True) if lv]
+    stream = torch.cuda.current_stream(dev)
+    d_pos = torch.from_numpy(pos).to(dev)
+    d_xm = torch.from_numpy(xmod).to(dev)
+    d_f = torch.empty_like(d_pos)
+    d_ft = torch.empty_like(d_pos)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def call(lv):
+        box.respa_force_device(d_pos.data_ptr(), d_xm.data_ptr(), S["hmat"], lv, d_f.data_ptr(),
+                               d_ft.data_ptr() if lv & R.FULL_INTER else None, stream=stream.cuda_stream,
+                               distribute_ghosts=True)
+
+    def timed(fn):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(max(3, args.warmup)):
+        for lv in levels:
+            call(lv)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if ws > 1:
+        torch.distributed.barrier()
+    per_level = {lv: [] for lv in set(levels)}
+    steps = []
+    for _ in range(args.steps):
+        tot = 0.0
+        for lv in levels:
+            t = timed(lambda: call(lv))
+            per_level[lv].append(t)
+            tot += t
+        steps.append(tot)
+    plain = [timed(lambda: box.energy_force_device(d_pos.data_ptr(), d_xm.data_ptr(), S["hmat"], d_f.data_ptr(),
+                                                   stream=stream.cuda_stream, distribute_ghosts=True))
+             for _ in range(max(3, args.steps))]
+    clocks = sampler.stop()
+    ms = float(np.mean(steps))
+    if ws > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    names = {R.RES_INTRA: "innermost (bonds, bends)", R.RES_INTER | R.FULL_INTRA | R.RES_INTRA:
+             "inner inter (pairs inside 5 A, bonds, bends)", R.FULL_INTER | R.RES_INTER | R.FULL_INTRA | R.RES_INTRA:
+             "outer (everything, weighted and plain)"}
+    if rank == 0:
+        plain_ms = float(np.mean(plain))
+        line = {
+            "metric": "RESPA steps/s (force calls of one PINY step, TIP4P/F 4096 mol x 32 beads)",
+            "value": ws * 1e3 / ms, "unit": "RESPA steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64acc" if args.precision == "mixed" else "f64",
+            "data": "synthetic",
+            "config": {"workload": "respa", "molecules": spec.nmol, "beads": P, "respa_steps_lrf": nres[0],
+                       "respa_steps_intra": nres[2], "cutoff_res_A": 5.0, "rheal_A": 1.0,
+                       "calls_per_step": len(levels),
+                       "ms_per_level": {names[lv]: float(np.mean(v)) for lv, v in per_level.items()},
+                       "plain_evaluation_ms": plain_ms,
+                       "plain_ms_for_the_same_inner_steps": plain_ms * len(levels),
+                       "l2": "256 MiB buffer written before each timed call; CUDA events on the launch stream"},
+            "roofline": None, "cpu_baseline": None, "e2e": None, "gpu_launches": None, "clocks": clocks,
+        }
+        print(json.dumps(line))
+    box.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def run_batch(args, ws, rank, local):
     """64 uneven TIP4P/F boxes, all beads, one CUDA graph launch per step."""
     import torch
@@ -595,6 +705,8 @@ def main():
         return run_grad(args, ws, rank, local)
     if args.config == "pimd_nvt":
         return run_pimd(args, ws, rank, local)
+    if args.config == "respa":
+        return run_respa(args, ws, rank, local)
 
     import torch
 

@@ -227,7 +227,8 @@ int pinyb200_destroy(pinyb200_ctx *c)
                     c->d_twiddle32, c->d_err, c->d_mstart, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_chunk,
                     c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf, c->d_x0, c->d_forceP,
                     c->d_pme_head, c->d_pme_w, c->d_nchunk, c->d_ls, c->d_cs, c->d_mchunk, c->d_mmaskf,
-                    c->d_reach, c->d_cut_res, c->d_bond_eq_res, c->d_forceW, c->d_forcet_aos};
+                    c->d_reach, c->d_cut_res, c->d_bond_eq_res, c->d_forceW, c->d_forcet_aos, c->d_rowR,
+                    c->d_colR, c->d_rtot, c->d_xm0, c->d_cs0};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->h_acc_pin) cudaFreeHost(c->h_acc_pin);
@@ -603,6 +604,14 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
     }
     // the rebuild test measures displacements from these positions
     CK(cudaMemcpyAsync(c->d_x0, d_p1, (size_t)natm * 3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    // mode-1 positions and cutskin^2 of this build, for the RESPA list
+    if (!c->d_xm0) CK(cudaMalloc(&c->d_xm0, (size_t)natm * 3 * sizeof(double)));
+    if (!c->d_cs0) CK(cudaMalloc(&c->d_cs0, (size_t)c->sys.npair_typ * sizeof(double)));
+    CK(launch_keep_build_state(c, nullptr, d_p1, d_xm, d_cs, c->stream));
+    c->build_cell = cell;
+    c->build_cell_ok = true;
+    if (c->respa_on)
+        if (int rc = respa_list_reserve(c, cell)) return rc;
     CK(cudaStreamSynchronize(c->stream));
     c->npairs = tot[0];
     c->nactive = tot[1];
@@ -638,7 +647,8 @@ int pinyb200_get_list(pinyb200_ctx *c, int *pi, int *pj, long cap, long *npairs)
 // synchronisation, so it can be captured in a CUDA graph.  timing: record
 // the phase events (not inside a graph); h_acc: where the per-bead energy
 // sums [P][S_NSLOT] are copied (NULL: not copied).
-int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, bool timing, double *h_acc)
+int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, bool timing, double *h_acc,
+                               double *respa_w)
 {
     const bool energy = !(flags & PINYB200_NO_ENERGY);
     const size_t nb = (size_t)c->sys.natm * 3 * c->P;
@@ -667,12 +677,27 @@ int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, boo
     if (c->use_mol && c->mol_ok && ortho && c->pair_variant == 0 && !(flags & PINYB200_SITE_PAIRS))
         CK(launch_mol_pair(c, cell, energy));
     else CK(launch_pair(c, cell, energy));
+    if (respa_w) {
+        // RESPA outer level: the weighted pair forces from the plain ones
+        // (so far the only forces in the buffer) and the switched pairs
+        // inside cutoff_res: w_ter F + (w_ter_res - w_ter) swit F
+        CK(launch_respa_scale_copy(c, c->r_wter, respa_w));
+        if (c->r_int_res_ter) CK(launch_pair_respa(c, cell, 4, respa_w));
+    }
     if (timing) CK(cudaEventRecord(c->ev[2], c->stream));
     CK(launch_intra(c, cell, energy));
+    if (respa_w) {
+        CK(launch_intra_respa(c, true, respa_w));
+        CK(launch_ecor_weighted(c, c->r_wter, respa_w));
+    }
     if (timing) CK(cudaEventRecord(c->ev[3], c->stream));
     CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     CK(launch_pme_force_add(c));
-    if (flags & PINYB200_DISTRIB_GHOSTS) CK(launch_ghost_distrib(c));
+    if (respa_w) CK(launch_pme_force_add_scaled(c, c->r_wter, respa_w));
+    if (flags & PINYB200_DISTRIB_GHOSTS) {
+        CK(launch_ghost_distrib(c));
+        if (respa_w) CK(launch_ghost_distrib(c, respa_w));
+    }
     if (timing) CK(cudaEventRecord(c->ev[4], c->stream));
     if (energy && h_acc)
         CK(cudaMemcpyAsync(h_acc, c->d_acc, (size_t)c->P * S_NSLOT * sizeof(double), cudaMemcpyDeviceToHost,

@@ -217,6 +217,13 @@ struct pinyb200_ctx {
     double *d_bond_eq_res = nullptr;  // [nbond_typ] RESPA bond equilibria
     double *d_forceW = nullptr;       // [natm][3][P] weighted forces of one level
     double *d_forcet_aos = nullptr;   // [P][natm][3] staging of the virial forces
+    int *d_rowR = nullptr, *d_colR = nullptr;  // RESPA pair list (CSR by i, j < i), capacity res_cap
+    long long res_cap = 0;
+    long long *d_rtot = nullptr;      // [2] RESPA list totals
+    double *d_xm0 = nullptr;          // [natm][3] mode-1 positions at the last list build
+    double *d_cs0 = nullptr;          // [npair_typ] cutskin^2 of the last list build
+    pinyb200::Cell build_cell{};      // cell of the last host list build
+    bool build_cell_ok = false;
     pinyb200::GradHost grad;      // tangent channels of pinyb200_grad_prepare
     std::string err;
 };
@@ -247,7 +254,17 @@ cudaError_t launch_pme_force_add(pinyb200_ctx *c);
 // evaluation steps (capi.cu): device work of one evaluation enqueued on
 // c->stream without host synchronisation, and the host bookkeeping of its
 // per-bead sums; cell of an hmat; error recording
-int evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, bool timing, double *h_acc);
+int evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, bool timing, double *h_acc,
+                     double *respa_w = nullptr);
+// RESPA pair list: the active pairs within cutoff_res + skin + spread at the
+// last list build (PINY's jter_res), rebuilt with every list build
+int respa_list_enqueue(pinyb200_ctx *c, const Cell &cell, const int *gate, cudaStream_t st);
+int respa_list_reserve(pinyb200_ctx *c, const Cell &cell);
+cudaError_t launch_respa_scale_copy(pinyb200_ctx *c, double w, double *target);
+// bead-1 and mode-1 positions and cutskin^2 of a list build, kept for the
+// RESPA list (gated like the build on the device)
+cudaError_t launch_keep_build_state(pinyb200_ctx *c, const int *gate, const double *d_pos1, const double *d_xm,
+                                    const double *d_cs, cudaStream_t st);
 int stage_positions(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const Cell &cell, int flags);
 void evaluate_finish(pinyb200_ctx *c, const Cell &cell, int flags, const double *acc, pinyb200_energies *e);
 int enqueue_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const Cell &cell, int flags,

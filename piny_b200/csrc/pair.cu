@@ -38,10 +38,11 @@ struct PairArgs {
     double *acc;
     int energy;
     const int *bad;  // device flags (overflow, mismatch) of the list update, or nullptr
-    // RESPA split (force_npol.c:805-816, :1030-1060): 0 off; 1 inner level
-    // (shave at cut_res, force x swit w_res); 2 outer level with the switch
-    // (force x (swit w_res + (1 - swit) w_full)); 3 outer level without
-    // inter RESPA (force x w_full).  swit = 1 - 3 br^2 + 2 br^3 with
+    // RESPA split (force_npol.c:805-816, :1030-1060), over the RESPA pair
+    // list and shaved at cut_res: 0 off; 1 inner level, force x swit w_res;
+    // 2 the outer level's switched part, force x swit (w_res - w_full),
+    // added to w_full times the plain forces (PINY's multiplier
+    // swit w_res + (1 - swit) w_full).  swit = 1 - 3 br^2 + 2 br^3 with
     // br = clamp((r - cut_res + rheal) / rheal, 0, 1).
     int respa;
     const double *cut_res;
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(256) pair_kernel(PairArgs a, Cell cell)
             const int j = a.col[jj];
             const int pt = pair_type(ti, a.atm_typ[j], a.ntyp);
             const int u = a.inter_map[pt];
-            const R rc = (R)((RSP && a.respa == 1) ? a.cut_res[pt] : a.cutoff[pt]);
+            const R rc = (R)(RSP ? a.cut_res[pt] : a.cutoff[pt]);
             const R rmin = (R)a.rmin[u], dr = (R)a.dr[u], dri = (R)a.dri[u];
             const int vdw = a.has_vdw[u];
             const R q2 = (R)(qi * a.charge[j]);
@@ -132,14 +133,11 @@ __global__ void __launch_bounds__(256) pair_kernel(PairArgs a, Cell cell)
                 if (vdw) dv += spline_eval<V, R>(ldg4(tV + (k - 1)), del);
                 R fx = rx * dv, fy = ry * dv, fz = rz * dv;
                 if (RSP) {
-                    R fm = (R)a.w_full;
-                    if (a.respa != 3) {
-                        R br = (r - (R)a.cut_res[pt] + (R)a.rheal) * (R)a.rheali;
-                        br = br > (R)0 ? br : (R)0;
-                        br = br < (R)1 ? br : (R)1;
-                        const R swit = br * br * (br * (R)2 - (R)3) + (R)1;
-                        fm = a.respa == 1 ? swit * (R)a.w_res : swit * (R)a.w_res + ((R)1 - swit) * (R)a.w_full;
-                    }
+                    R br = (r - rc + (R)a.rheal) * (R)a.rheali;
+                    br = br > (R)0 ? br : (R)0;
+                    br = br < (R)1 ? br : (R)1;
+                    const R swit = br * br * (br * (R)2 - (R)3) + (R)1;
+                    const R fm = a.respa == 1 ? swit * (R)a.w_res : swit * (R)(a.w_res - a.w_full);
                     fx *= fm;
                     fy *= fm;
                     fz *= fm;
@@ -253,11 +251,13 @@ cudaError_t launch_pair(pinyb200_ctx *c, const Cell &cell, bool energy)
     return launch_pair_r<float, false>(c, a, cell);
 }
 
-// One RESPA pass of the real-space pair forces over the active site list
+// One RESPA pass of the real-space pair forces over the RESPA pair list
 // into target ([natm][3][P]); no energies.  mode as PairArgs::respa.
 cudaError_t launch_pair_respa(pinyb200_ctx *c, const Cell &cell, int mode, double *target)
 {
     PairArgs a = pair_args(c, false);
+    a.row = c->d_rowR;
+    a.col = c->d_colR;
     a.forceT = target;
     a.respa = mode;
     a.cut_res = c->d_cut_res;

@@ -18,11 +18,152 @@
 // into the context's force buffer, while the weighted forces go to a second
 // buffer ([atom][xyz][bead] like the first).
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "common.cuh"
+
+namespace pinyb200 {
+
+// RESPA pair list (PINY's jter_res, verlist_create.c:409-491): the active
+// pairs whose bead-1 separation at the list build lies within
+// cutskin_res = min(cutoff_res + skin + spread, cutskin) (nbr_list_control.c:
+// 265-275), i.e. cutoff_res plus the build's own cutskin - cutoff.  One warp
+// per row i; separations as the list build forms them.
+template <int FILL>
+__global__ void __launch_bounds__(256) respa_list_kernel(const int *__restrict__ gate, int natm, int ntyp,
+                                                         const double *__restrict__ pos1,
+                                                         const double *__restrict__ xm, int use_xm, Cell cell,
+                                                         const double *__restrict__ cs,
+                                                         const double *__restrict__ cutoff,
+                                                         const double *__restrict__ cut_res,
+                                                         const int *__restrict__ atm_typ,
+                                                         const int *__restrict__ rowA, const int *__restrict__ colA,
+                                                         int *__restrict__ count, const int *__restrict__ rowR,
+                                                         int *__restrict__ colR, long long cap)
+{
+    if (gate && *gate == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < natm; i += nwarps) {
+        const double xi = pos1[3 * i], yi = pos1[3 * i + 1], zi = pos1[3 * i + 2];
+        double xmi = 0, ymi = 0, zmi = 0;
+        if (use_xm) { xmi = xm[3 * i]; ymi = xm[3 * i + 1]; zmi = xm[3 * i + 2]; }
+        const int ti = atm_typ[i];
+        const int beg = rowA[i], end = rowA[i + 1];
+        const long long w = FILL ? rowR[i] : 0;
+        int n = 0;
+        for (int jj0 = beg; jj0 < end; jj0 += 32) {
+            const int jj = jj0 + lane;
+            bool keep = false;
+            int j = 0;
+            if (jj < end) {
+                j = colA[jj];
+                double dx = __dsub_rn(xi, pos1[3 * j]);
+                double dy = __dsub_rn(yi, pos1[3 * j + 1]);
+                double dz = __dsub_rn(zi, pos1[3 * j + 2]);
+                if (use_xm)
+                    period_pimd_exact(dx, dy, dz, __dsub_rn(xmi, xm[3 * j]), __dsub_rn(ymi, xm[3 * j + 1]),
+                                      __dsub_rn(zmi, xm[3 * j + 2]), cell);
+                else
+                    period_exact(dx, dy, dz, cell);
+                const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+                const int pt = pair_type(ti, atm_typ[j], ntyp);
+                const double margin = fmax(sqrt(cs[pt]) - cutoff[pt], 0.0);
+                const double cr = fmin(cut_res[pt] + margin, sqrt(cs[pt]));
+                keep = r2 < cr * cr;
+            }
+            const unsigned b = __ballot_sync(0xffffffffu, keep);
+            if (FILL && keep) {
+                const long long p = w + n + __popc(b & ((1u << lane) - 1u));
+                if (p < cap) colR[p] = j;
+            }
+            n += __popc(b);
+        }
+        if (!FILL && lane == 0) {
+            count[i] = n;
+            count[natm + i] = n;  // the scan fills two row arrays: both are rowR
+        }
+    }
+}
+
+__global__ void keep_build_state_kernel(const int *gate, const double *__restrict__ xm, double *__restrict__ xm0,
+                                        long long n, const double *__restrict__ cs, double *__restrict__ cs0, int npt)
+{
+    if (gate && *gate == 0) return;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        xm0[i] = xm[i];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) cs0[i] = cs[i];
+}
+
+__global__ void scale_copy_kernel(const double *__restrict__ src, double w, double *__restrict__ dst, long long n)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) dst[t] = src[t] * w;
+}
+
+cudaError_t launch_keep_build_state(pinyb200_ctx *c, const int *gate, const double *d_pos1, const double *d_xm,
+                                    const double *d_cs, cudaStream_t st)
+{
+    (void)d_pos1;  // bead-1 positions are kept in d_x0 by the list build itself
+    if (!c->d_xm0 || !c->d_cs0) return cudaSuccess;
+    const long long n = d_xm ? (long long)c->sys.natm * 3 : 0;
+    keep_build_state_kernel<<<(unsigned)((n + 255) / 256 + 1), 256, 0, st>>>(gate, d_xm, c->d_xm0, n, d_cs, c->d_cs0,
+                                                                             c->sys.npair_typ);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_respa_scale_copy(pinyb200_ctx *c, double w, double *target)
+{
+    const long long n = (long long)c->sys.natm * 3 * c->P;
+    scale_copy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->d_forceT, w, target, n);
+    return cudaGetLastError();
+}
+
+// Count, scan and fill of the RESPA list on st (gated like a device build).
+int respa_list_enqueue(pinyb200_ctx *c, const Cell &cell, const int *gate, cudaStream_t st)
+{
+    if (!c->respa_on || !c->d_rowR || !c->d_colR) return PINYB200_OK;
+    const DeviceSystem &s = c->sys;
+    const int threads = 256;
+    const int blocks = (int)(((long long)s.natm * 32 + threads - 1) / threads);
+    const bool use_xm = c->P > 1;
+    respa_list_kernel<0><<<blocks, threads, 0, st>>>(gate, s.natm, s.ntyp, c->d_x0, c->d_xm0, use_xm, cell, c->d_cs0,
+                                                     s.cutoff, c->d_cut_res, s.atm_typ, c->d_rowA, c->d_colA,
+                                                     c->d_count, nullptr, nullptr, 0);
+    scan_kernel<<<1, 1024, 0, st>>>(gate, s.natm, c->d_count, c->d_rowR, c->d_rowR, c->d_rtot);
+    respa_list_kernel<1><<<blocks, threads, 0, st>>>(gate, s.natm, s.ntyp, c->d_x0, c->d_xm0, use_xm, cell, c->d_cs0,
+                                                     s.cutoff, c->d_cut_res, s.atm_typ, c->d_rowA, c->d_colA,
+                                                     nullptr, c->d_rowR, c->d_colR, c->res_cap);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
+    return PINYB200_OK;
+}
+
+// RESPA list storage for the current list capacity, and the list itself
+// from the state of the last list build (host side, outside graphs).
+int respa_list_reserve(pinyb200_ctx *c, const Cell &cell)
+{
+    if (!c->d_rowR) {
+        cudaError_t e = cudaMalloc(&c->d_rowR, ((size_t)c->sys.natm + 1) * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&c->d_rtot, 2 * sizeof(long long));
+        if (e != cudaSuccess) return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (c->res_cap < c->list_cap || !c->d_colR) {
+        if (c->d_colR) cudaFree(c->d_colR);
+        c->d_colR = nullptr;
+        c->res_cap = 0;
+        cudaError_t e = cudaMalloc(&c->d_colR, (size_t)c->list_cap * sizeof(int));
+        if (e != cudaSuccess) return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
+        c->res_cap = c->list_cap;
+    }
+    return respa_list_enqueue(c, cell, nullptr, c->stream);
+}
+
+}  // namespace pinyb200
 
 using namespace pinyb200;
 
@@ -49,30 +190,31 @@ int check_level(pinyb200_ctx *c, int level)
 
 // One level, enqueued on c->stream; the weighted forces end in c->d_forceW,
 // the outer level's unweighted ones in c->d_forceT (and its per-bead sums
-// are copied to h_acc).
+// are copied to h_acc).  The outer level is the plain evaluation with the
+// weighted buffer formed alongside (evaluate_enqueue); the inner levels run
+// only their own terms.
 int respa_enqueue(pinyb200_ctx *c, const Cell &cell, int level, int flags, double *h_acc)
 {
+    if (level & PINYB200_FULL_INTER) return evaluate_enqueue(c, cell, flags, false, h_acc, c->d_forceW);
     const size_t nb = (size_t)c->sys.natm * 3 * c->P;
-    const bool outer = level & PINYB200_FULL_INTER;
-    const bool inter = level & (PINYB200_FULL_INTER | PINYB200_RES_INTER);
-    const bool distrib = flags & PINYB200_DISTRIB_GHOSTS;
-    if (outer) {
-        int rc = evaluate_enqueue(c, cell, flags & ~PINYB200_DISTRIB_GHOSTS, false, h_acc);
-        if (rc) return rc;
-    } else {
-        RK(launch_ghost_pos(c));
-    }
+    const bool inter = level & PINYB200_RES_INTER;
+    RK(launch_ghost_pos(c));
     RK(cudaMemsetAsync(c->d_forceW, 0, nb * sizeof(double), c->stream));
-    if (inter) RK(launch_pair_respa(c, cell, outer ? (c->r_int_res_ter ? 2 : 3) : 1, c->d_forceW));
-    if (outer) {
-        RK(launch_pme_force_add_scaled(c, c->r_wter, c->d_forceW));
-        RK(launch_ecor_weighted(c, c->r_wter, c->d_forceW));
-    }
+    if (inter) RK(launch_pair_respa(c, cell, 1, c->d_forceW));
     RK(launch_intra_respa(c, inter, c->d_forceW));
-    if (distrib) {
-        RK(launch_ghost_distrib(c, c->d_forceW));
-        if (outer) RK(launch_ghost_distrib(c, c->d_forceT));
-    }
+    if (flags & PINYB200_DISTRIB_GHOSTS) RK(launch_ghost_distrib(c, c->d_forceW));
+    return PINYB200_OK;
+}
+
+// The list update's sticky failure flags (a device rebuild that did not fit)
+int check_list_flags(pinyb200_ctx *c)
+{
+    if (!c->d_ls) return PINYB200_OK;
+    int fl[2] = {0, 0};
+    RK(cudaMemcpy(fl, (const char *)c->d_ls + offsetof(ListState, overflow), sizeof(fl), cudaMemcpyDeviceToHost));
+    if (fl[0] | fl[1])
+        return record_error(c, PINYB200_ERR_LIST_OVERFLOW,
+                            "respa_force: a device list rebuild exceeded the reserved list; rebuild on the host");
     return PINYB200_OK;
 }
 
@@ -105,6 +247,8 @@ int pinyb200_set_respa(pinyb200_ctx *c, const pinyb200_respa *r)
                       cudaMemcpyHostToDevice));
     }
     if (!c->d_forceW) RK(cudaMalloc(&c->d_forceW, (size_t)c->sys.natm * 3 * c->P * sizeof(double)));
+    if (c->have_list && !c->build_cell_ok)
+        return record_error(c, PINYB200_ERR_STATE, "set_respa: the list build state is missing");
     c->r_wter = r->wght_ter;
     c->r_wter_res = r->wght_ter_res;
     c->r_wtra_res = r->wght_tra_res;
@@ -113,6 +257,13 @@ int pinyb200_set_respa(pinyb200_ctx *c, const pinyb200_respa *r)
     c->r_ires_bond = r->ires_bond ? 1 : 0;
     c->r_rheal = r->rheal_res;
     c->respa_on = true;
+    c->gen++;  // captured graphs must pick up the RESPA list build
+    if (c->have_list) {
+        // the RESPA list of the current Verlet list, from its build state
+        int rc = respa_list_reserve(c, c->build_cell);
+        if (rc) return rc;
+        RK(cudaStreamSynchronize(c->stream));
+    }
     return PINYB200_OK;
 }
 
@@ -143,6 +294,7 @@ int pinyb200_respa_force_device(pinyb200_ctx *c, const double *d_pos, const doub
     RK(launch_transpose_out(c, d_force, c->d_forceW));
     if (outer && d_forcet) RK(launch_transpose_out(c, d_forcet, c->d_forceT));
     RK(cudaStreamSynchronize(c->stream));
+    if (int rc2 = check_list_flags(c)) return rc2;
     if (e) {
         if (energy) {
             evaluate_finish(c, cell, flags, acc.data(), e);

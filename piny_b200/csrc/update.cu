@@ -182,6 +182,10 @@ int list_update_enqueue(pinyb200_ctx *c, const double *d_pos, const double *d_xm
                                                               mol ? c->d_mrow : nullptr);
     const long long n = (long long)natm * 3;
     ls_copy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(gate, d_pos, c->d_x0, n);
+    if ((e = launch_keep_build_state(c, gate, d_pos, xm, c->d_cs, st)) != cudaSuccess)
+        return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
+    if (c->respa_on)
+        if ((rc = respa_list_enqueue(c, cell, gate, st))) return rc;
     if ((e = cudaGetLastError()) != cudaSuccess) return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
     return PINYB200_OK;
 }

@@ -191,3 +191,45 @@ def test_piny_layout_calls():
     assert rel_rms(gt, F["ref_L0_forcet_raw"]) < 1e-12
     assert np.abs(pv2[1:] - pv[1:]).max() <= 1e-12 * np.abs(pv[1:]).max()
     box.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64"])
+def test_respa_list_follows_device_rebuild(prec, oracle):
+    """A list rebuild on the device (PINYB200_UPDATE_LIST) rebuilds the RESPA
+    pair list with it: after the atoms move past the skin, the inner and
+    outer levels match the oracle on a list built afresh."""
+    import torch
+
+    from piny_b200 import respa as R
+    from piny_b200.lib import DeviceBox
+    F = load_fixture("tip4pf_128_p2")
+    P, n = int(F["nbeads"]), int(F["natm"])
+    rs = R.respa_setup(2, 1, 1, 1, True, True, np.asarray(F["cutoff"]) - 1.5, 1.2, np.asarray(F["bond_eq"]))
+    box = DeviceBox(F, P, prec)
+    box.build_list(F["pos"][0], F["xmod"], F["hmat"], F["cutskin2"])
+    box.set_respa(rs)
+    d0 = _dev(F["pos"])
+    box.list_set_spread(box.check_list_device(d0.data_ptr(), 0.0)[2])
+    rng = np.random.default_rng(11)
+    nsite = 4  # q-TIP4P/F: O, H, H, M; molecules move rigidly
+    shift = rng.normal(size=(n // nsite, 3))
+    shift *= (0.7 * float(F["skin"]) / np.linalg.norm(shift, axis=1))[:, None]
+    pos = F["pos"] + np.repeat(shift, nsite, axis=0)[None, :, :]
+    xmod = pos.mean(axis=0)
+    d_pos, d_xm = _dev(pos), _dev(xmod)
+    inner = R.RES_INTER | R.FULL_INTRA | R.RES_INTRA
+    f = torch.zeros_like(d_pos)
+    box.respa_force_device(d_pos.data_ptr(), d_xm.data_ptr(), F["hmat"], inner, f.data_ptr(), update_list=True)
+    st = box.list_status()
+    assert st["rebuilds"] == 1 and not st["overflow"]
+    cs = np.asarray(F["cutskin2"])
+    pi, pj = oracle.verlist(F, pos[0], xmod, F["hmat"], cs)
+    fref, _ = oracle.respa_force(F, rs, inner, pos, xmod, F["hmat"], pi, pj)
+    assert rel_rms(f.cpu().numpy(), fref) < TOL[prec]
+    outer = R.FULL_INTER | R.RES_INTER | R.FULL_INTRA | R.RES_INTRA
+    ft = torch.zeros_like(d_pos)
+    box.respa_force_device(d_pos.data_ptr(), d_xm.data_ptr(), F["hmat"], outer, f.data_ptr(), ft.data_ptr())
+    fref, ftref = oracle.respa_force(F, rs, outer, pos, xmod, F["hmat"], pi, pj)
+    assert rel_rms(f.cpu().numpy(), fref) < TOL[prec]
+    assert rel_rms(ft.cpu().numpy(), ftref) < TOL[prec]
+    box.close()
