@@ -285,6 +285,9 @@ int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
  *   cutoff_res     interact.cutoff_res per pair type (npair_typ, Bohr)
  *   rheal_res      interact.rheal_res (Bohr), the switch width
  *   bond_eq_res    bond.eq_pow_res per bond type (nbond_typ, Bohr)
+ *   nktot_res      ewald.nktot_res: the reciprocal-space RESPA set
+ *                  (ewald_respa_kmax) is not supported; > 0 is refused
+ *                  with PINYB200_ERR_UNSUPPORTED
  * pinyb200_respa_force_device evaluates one level, `level` being the OR of
  * the PINYB200_* flag bits below that PINY has set: one of
  *   RES_INTRA; FULL_INTRA|RES_INTRA; RES_INTER|FULL_INTRA|RES_INTRA (needs
@@ -301,8 +304,7 @@ int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
  * PINYB200_UPDATE_LIST.  The inner levels use the active site list shaved
  * at cutoff_res in place of PINY's separate RESPA Verlet list (pairs within
  * cutoff_res + skin + spread at the build); under the list's own validity
- * rule the two hold the same pairs inside cutoff_res.  The reciprocal-space
- * RESPA set (ewald_respa_kmax, PINY's nktot_res > 0) is not supported.
+ * rule the two hold the same pairs inside cutoff_res.
  */
 #define PINYB200_FULL_INTER 1
 #define PINYB200_RES_INTER 2
@@ -314,6 +316,7 @@ typedef struct pinyb200_respa {
     const double *cutoff_res;
     double rheal_res;
     const double *bond_eq_res;
+    int nktot_res;
 } pinyb200_respa;
 int pinyb200_set_respa(pinyb200_ctx *ctx, const pinyb200_respa *r);
 int pinyb200_respa_force_device(pinyb200_ctx *ctx, const double *d_pos,

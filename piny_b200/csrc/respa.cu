@@ -230,6 +230,9 @@ int pinyb200_set_respa(pinyb200_ctx *c, const pinyb200_respa *r)
         c->respa_on = false;
         return PINYB200_OK;
     }
+    if (r->nktot_res > 0)
+        return record_error(c, PINYB200_ERR_UNSUPPORTED,
+                            "set_respa: the reciprocal-space RESPA set (ewald_respa_kmax) is not supported");
     if (!r->cutoff_res || (c->sys.nbond && !r->bond_eq_res))
         return record_error(c, PINYB200_ERR_ARG, "set_respa: cutoff_res / bond_eq_res missing");
     if (!(r->rheal_res > 0.0)) return record_error(c, PINYB200_ERR_ARG, "set_respa: rheal_res must be > 0");

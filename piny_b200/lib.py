@@ -89,7 +89,7 @@ class PinyPimdEnergies(C.Structure):
 class PinyRespa(C.Structure):
     _fields_ = [("wght_ter", _d), ("wght_ter_res", _d), ("wght_tra_res", _d),
                 ("int_res_ter", _i), ("int_res_inter", _i), ("ires_bond", _i),
-                ("cutoff_res", _pd), ("rheal_res", _d), ("bond_eq_res", _pd)]
+                ("cutoff_res", _pd), ("rheal_res", _d), ("bond_eq_res", _pd), ("nktot_res", _i)]
 
 
 class PinyTangent(C.Structure):
@@ -379,7 +379,7 @@ class DeviceBox:
         eqr = np.ascontiguousarray(respa["bond_eq_res"], np.float64)
         r = PinyRespa(float(respa["wght_ter"]), float(respa["wght_ter_res"]), float(respa["wght_tra_res"]),
                       int(respa["int_res_ter"]), int(respa["int_res_inter"]), int(respa["ires_bond"]), _dp(cut),
-                      float(respa["rheal_res"]), _dp(eqr))
+                      float(respa["rheal_res"]), _dp(eqr), int(respa.get("nktot_res", 0)))
         self._check(self.L.pinyb200_set_respa(self.h, C.byref(r)), "set_respa")
 
     def respa_force_device(self, d_pos: int, d_xmod, hmat, level: int, d_force: int, d_forcet=None, stream=None,
