@@ -285,9 +285,18 @@ int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
  *   cutoff_res     interact.cutoff_res per pair type (npair_typ, Bohr)
  *   rheal_res      interact.rheal_res (Bohr), the switch width
  *   bond_eq_res    bond.eq_pow_res per bond type (nbond_typ, Bohr)
- *   nktot_res      ewald.nktot_res: the reciprocal-space RESPA set
- *                  (ewald_respa_kmax) is not supported; > 0 is refused
- *                  with PINYB200_ERR_UNSUPPORTED
+ *   nktot_res      ewald.nktot_res (> 0: ewald_respa_kmax given).  With
+ *                  one PME grid (pme_res_on 0; PINY then demands
+ *                  kmax_res = kmax) the reciprocal sum moves to the inner
+ *                  inter level: PME x wght_ter_res at every RES_INTER level
+ *                  (energy_control_inter_recip.c:184-213), the exclusion
+ *                  correction at the inner level from ecor_cdv0_res x
+ *                  wght_ter_res (ecorr.c:97-106) and at the outer level as
+ *                  ecor_both, wght_ter F + (wght_ter_res - wght_ter) F_res
+ *                  (ecorr.c:349-351, :497-505)
+ *   pme_res_on     part_mesh.pme_res_on: a separate RESPA PME grid; not
+ *                  supported (PINYB200_ERR_UNSUPPORTED)
+ *   ecor_cdv0_res  ecor.cdv0_res (ecor_nsplin entries) when nktot_res > 0
  * pinyb200_respa_force_device evaluates one level, `level` being the OR of
  * the PINYB200_* flag bits below that PINY has set: one of
  *   RES_INTRA; FULL_INTRA|RES_INTRA; RES_INTER|FULL_INTRA|RES_INTRA (needs
@@ -296,7 +305,8 @@ int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
  * d_force receives PINY's weighted forces fx: real-space pairs x the RESPA
  * multiplier (inner levels shave at cutoff_res; force_npol.c:805-816,
  * :1030-1060), PME and the exclusion correction x wght_ter at the outer
- * level only, bonds as bond_both / bond, bends x wght_tra_res.  At the outer
+ * level only (nktot_res = 0; see above otherwise), bonds as bond_both /
+ * bond, bends x wght_tra_res.  At the outer
  * level d_forcet (may be NULL) receives the unweighted forces PINY adds to
  * the virial forces fxt, and *e the energies and pvten_tot of
  * pinyb200_energy_force_device; at inner levels *e is zeroed (PINY books
@@ -317,6 +327,8 @@ typedef struct pinyb200_respa {
     double rheal_res;
     const double *bond_eq_res;
     int nktot_res;
+    int pme_res_on;
+    const double *ecor_cdv0_res;
 } pinyb200_respa;
 int pinyb200_set_respa(pinyb200_ctx *ctx, const pinyb200_respa *r);
 int pinyb200_respa_force_device(pinyb200_ctx *ctx, const double *d_pos,

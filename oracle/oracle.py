@@ -55,6 +55,7 @@ class OrcRespa(C.Structure):
         ("wght_ter", _d), ("wght_ter_res", _d), ("wght_tra_res", _d),
         ("int_res_ter", _i), ("int_res_inter", _i), ("ires_bond", _i),
         ("cutoff_res", _pd), ("rheal_res", _d), ("bond_eq_res", _pd),
+        ("nktot_res", _i), ("ecor_cdv0_res", _pd),
     ]
 
 
@@ -284,7 +285,9 @@ class Oracle:
         r = OrcRespa()
         keep = []
         for name, ctype in OrcRespa._fields_:
-            v = respa[name]
+            v = respa.get(name)
+            if v is None:
+                v = np.zeros(1) if ctype is _pd else 0
             if ctype is _pd:
                 a, p = self._d(v)
                 keep.append(a)

@@ -1136,10 +1136,52 @@ void orc_respa_force(const orc_system *s, const orc_respa *r, int level, int P,
             }
         }
 
-        /* reciprocal space and the exclusion correction: full steps only,
-         * weight wght_ter (energy_control_inter_recip.c:184-214, :281-292;
-         * ewald3d_pme.c forces x wght_now, ecorr.c:100 wfor) */
-        if (full_inter) {
+        /* reciprocal space and the exclusion correction
+         * (energy_control_inter_recip.c:184-214, :278-323): without the
+         * reciprocal RESPA set at full steps only, x wght_ter (ewald3d_pme.c
+         * forces x wght_now, ecorr.c:100 wfor); with it (one grid) PME at
+         * every inner inter step x wght_ter_res, ecor from the RESPA table
+         * x wght_ter_res (ecorr.c:103-106) or, at full steps, ecor_both
+         * (ecorr.c:349-351, :497-505) */
+        const int kres = r->nktot_res > 0;
+        if (kres && res_inter) {
+            if (s->nktot > 0) {
+                double pvr[10] = {0};
+                memset(tmp, 0, sizeof(double) * 3 * natm);
+                pme_bead(s, pos, h, hi, vol, tmp, pvr);
+                for (long a = 0; a < 3 * natm; a++) {
+                    if (ft) ft[a] += tmp[a];
+                    f[a] += tmp[a] * w_res;
+                }
+            }
+            for (int c = 0; c < s->necor; c++) {
+                int a = s->ecor_j1[c], bb = s->ecor_j2[c];
+                double dx = pos[3 * a] - pos[3 * bb], dy = pos[3 * a + 1] - pos[3 * bb + 1],
+                       dz = pos[3 * a + 2] - pos[3 * bb + 2];
+                double rr = sqrt(dx * dx + dy * dy + dz * dz);
+                int k = (int)(((rr - s->ecor_rmin) * s->ecor_dri) + 0.5) + 3;
+                k = k < s->ecor_nsplin - 2 ? k : s->ecor_nsplin - 2;
+                k = k > 3 ? k : 3;
+                double rsp = ((double)(k - 3)) * s->ecor_dr + s->ecor_rmin;
+                double del = (rr - rsp) * s->ecor_dri;
+                double q12 = s->charge[a] * s->charge[bb];
+                double dvr = vspl(r->ecor_cdv0_res, k, del) * q12;
+                double g[3];
+                if (full_inter) {
+                    double dvt = vspl(s->ecor_cdv0, k, del) * q12;
+                    double d[3] = {dx, dy, dz};
+                    for (int e = 0; e < 3; e++) g[e] = w_full * (d[e] * dvt) + (w_res - w_full) * (d[e] * dvr);
+                    add3(ft, a, dx * dvt, dy * dvt, dz * dvt);
+                    add3(ft, bb, -(dx * dvt), -(dy * dvt), -(dz * dvt));
+                } else {
+                    g[0] = dx * dvr * w_res;
+                    g[1] = dy * dvr * w_res;
+                    g[2] = dz * dvr * w_res;
+                }
+                add3(f, a, g[0], g[1], g[2]);
+                add3(f, bb, -g[0], -g[1], -g[2]);
+            }
+        } else if (full_inter) {
             if (s->nktot > 0) {
                 double pvr[10] = {0};
                 memset(tmp, 0, sizeof(double) * 3 * natm);

@@ -128,6 +128,8 @@ typedef struct orc_respa {
     const double *cutoff_res;   /* [npair_typ] interact.cutoff_res (Bohr)   */
     double rheal_res;           /* interact.rheal_res (Bohr)                */
     const double *bond_eq_res;  /* [nbond_typ] bond.eq_pow_res              */
+    int nktot_res;              /* ewald.nktot_res (one PME grid)           */
+    const double *ecor_cdv0_res; /* [ecor_nsplin] ecor.cdv0_res             */
 } orc_respa;
 #define ORC_FULL_INTER 1
 #define ORC_RES_INTER 2

@@ -746,6 +746,12 @@ static int run_respa(const char *dir, const char *input, const char *outpath)
     put1d("wght_tra", class_.for_scr.wght_tra);
     put1d("wght_tra_res", class_.for_scr.wght_tra_res);
     if (bonded_.bond.npow > 0) putd("bond_eq_res", bonded_.bond.eq_pow_res, bonded_.bond.ntyp_pow);
+    put1i("nktot_res", gd_.ewald.nktot_res);
+    put1i("pme_res_on", class_.part_mesh.pme_res_on);
+    if (bonded_.ecor.num > 0 && bonded_.ecor.nktot_res > 0) {
+        putd("ecor_cdv0_res", bonded_.ecor.cdv0_res, bonded_.ecor.nsplin);
+        put1d("ecor_ecut_res", bonded_.ecor.ecut_res);
+    }
     for (int l = 0; l < 4; l++) {
         char nm[32];
         snprintf(nm, sizeof nm, "L%d_force_raw", l);

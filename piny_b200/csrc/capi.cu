@@ -228,7 +228,7 @@ int pinyb200_destroy(pinyb200_ctx *c)
                     c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf, c->d_x0, c->d_forceP,
                     c->d_pme_head, c->d_pme_w, c->d_nchunk, c->d_ls, c->d_cs, c->d_mchunk, c->d_mmaskf,
                     c->d_reach, c->d_cut_res, c->d_bond_eq_res, c->d_forceW, c->d_forcet_aos, c->d_rowR,
-                    c->d_colR, c->d_rtot, c->d_xm0, c->d_cs0};
+                    c->d_colR, c->d_rtot, c->d_xm0, c->d_cs0, c->d_ecor_res_tab};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->h_acc_pin) cudaFreeHost(c->h_acc_pin);
@@ -688,12 +688,12 @@ int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, boo
     CK(launch_intra(c, cell, energy));
     if (respa_w) {
         CK(launch_intra_respa(c, true, respa_w));
-        CK(launch_ecor_weighted(c, c->r_wter, respa_w));
+        CK(launch_ecor_weighted(c, c->r_wter, respa_w, c->r_kres ? 2 : 0));
     }
     if (timing) CK(cudaEventRecord(c->ev[3], c->stream));
     CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     CK(launch_pme_force_add(c));
-    if (respa_w) CK(launch_pme_force_add_scaled(c, c->r_wter, respa_w));
+    if (respa_w) CK(launch_pme_force_add_scaled(c, c->r_kres ? c->r_wter_res : c->r_wter, respa_w));
     if (flags & PINYB200_DISTRIB_GHOSTS) {
         CK(launch_ghost_distrib(c));
         if (respa_w) CK(launch_ghost_distrib(c, respa_w));

@@ -213,6 +213,8 @@ struct pinyb200_ctx {
     bool respa_on = false;
     double r_wter = 1, r_wter_res = 1, r_wtra_res = 1, r_rheal = 1;
     int r_int_res_ter = 0, r_int_res_inter = 0, r_ires_bond = 0;
+    int r_kres = 0;                   // reciprocal-space RESPA on one grid (nktot_res > 0)
+    double *d_ecor_res_tab = nullptr; // [ecor_nsplin][4] cubic coefficients of ecor.cdv0_res
     double *d_cut_res = nullptr;      // [npair_typ] inner cutoffs (Bohr)
     double *d_bond_eq_res = nullptr;  // [nbond_typ] RESPA bond equilibria
     double *d_forceW = nullptr;       // [natm][3][P] weighted forces of one level
@@ -239,7 +241,7 @@ cudaError_t launch_build_list(pinyb200_ctx *c, const Cell &cell, const double *d
 cudaError_t launch_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_pair_respa(pinyb200_ctx *c, const Cell &cell, int mode, double *target);
 cudaError_t launch_intra_respa(pinyb200_ctx *c, bool both, double *target);
-cudaError_t launch_ecor_weighted(pinyb200_ctx *c, double w, double *target);
+cudaError_t launch_ecor_weighted(pinyb200_ctx *c, double w, double *target, int table = 0);
 cudaError_t launch_pme_force_add_scaled(pinyb200_ctx *c, double w, double *target);
 cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
                             const double *d_cutskin2, int pass, const int *gate = nullptr,

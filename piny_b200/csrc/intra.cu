@@ -329,12 +329,16 @@ __global__ void __launch_bounds__(256) bend_w_kernel(int P, const double *__rest
     add_f(fW, P, a3, b, g.fx3 * w, g.fy3 * w, g.fz3 * w);
 }
 
-// Ewald exclusion correction x w (ecorr.c:100, :229-245).
+// Ewald exclusion correction (ecorr.c): table 0, the force table x w
+// (:100, :229-245); 1, the RESPA table x w (:103-106); 2, ecor_both's
+// w F + (w_res - w) F_res with w_res = wght_ter_res (:349-351, :497-505).
 __global__ void __launch_bounds__(256) ecor_w_kernel(int P, const double *__restrict__ posT, double *__restrict__ fW,
                                                      const double *__restrict__ charge, int necor,
                                                      const int *__restrict__ j1s, const int *__restrict__ j2s,
                                                      int nsplin, double rmin, double dr, double dri,
-                                                     const double4 *__restrict__ tab, double w)
+                                                     const double4 *__restrict__ tab,
+                                                     const double4 *__restrict__ tab_res, int table, double w,
+                                                     double w_res)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)necor * P) return;
@@ -350,8 +354,21 @@ __global__ void __launch_bounds__(256) ecor_w_kernel(int P, const double *__rest
     k = k > 3 ? k : 3;
     const double rsp = __dadd_rn(__dmul_rn((double)(k - 3), dr), rmin);
     const double del = __dmul_rn(__dsub_rn(r, rsp), dri);
-    const double dvt = spline_eval<double4, double>(tab[nsplin + k - 1], del) * (charge[j1] * charge[j2]);
-    const double fx = dx * dvt * w, fy = dy * dvt * w, fz = dz * dvt * w;
+    const double q12 = charge[j1] * charge[j2];
+    double fx, fy, fz;
+    if (table == 0 || table == 1) {
+        const double dvt = spline_eval<double4, double>(table == 0 ? tab[nsplin + k - 1] : tab_res[k - 1], del) * q12;
+        fx = dx * dvt * w;
+        fy = dy * dvt * w;
+        fz = dz * dvt * w;
+    } else {
+        const double dvt = spline_eval<double4, double>(tab[nsplin + k - 1], del) * q12;
+        const double dvr = spline_eval<double4, double>(tab_res[k - 1], del) * q12;
+        const double wd = w_res - w;
+        fx = w * (dx * dvt) + wd * (dx * dvr);
+        fy = w * (dy * dvt) + wd * (dy * dvr);
+        fz = w * (dz * dvt) + wd * (dz * dvr);
+    }
     add_f(fW, P, j1, b, fx, fy, fz);
     add_f(fW, P, j2, b, -fx, -fy, -fz);
 }
@@ -438,13 +455,13 @@ cudaError_t launch_intra_respa(pinyb200_ctx *c, bool both, double *target)
     return cudaGetLastError();
 }
 
-cudaError_t launch_ecor_weighted(pinyb200_ctx *c, double w, double *target)
+cudaError_t launch_ecor_weighted(pinyb200_ctx *c, double w, double *target, int table)
 {
     const DeviceSystem &s = c->sys;
     if (!s.necor) return cudaSuccess;
     ecor_w_kernel<<<nblk((long long)s.necor * c->P, 256), 256, 0, c->stream>>>(
         c->P, c->d_posT, target, s.charge, s.necor, s.ecor_j1, s.ecor_j2, s.ecor_nsplin, s.ecor_rmin, s.ecor_dr,
-        s.ecor_dri, s.ecor_tab, w);
+        s.ecor_dri, s.ecor_tab, (const double4 *)c->d_ecor_res_tab, table, w, c->r_wter_res);
     return cudaGetLastError();
 }
 

@@ -201,6 +201,13 @@ int respa_enqueue(pinyb200_ctx *c, const Cell &cell, int level, int flags, doubl
     RK(launch_ghost_pos(c));
     RK(cudaMemsetAsync(c->d_forceW, 0, nb * sizeof(double), c->stream));
     if (inter) RK(launch_pair_respa(c, cell, 1, c->d_forceW));
+    if (inter && c->r_kres) {
+        // reciprocal-space RESPA with one grid: the reciprocal sum and the
+        // exclusion correction (RESPA table) belong to this level
+        RK(launch_pme(c, cell, false));
+        RK(launch_pme_force_add_scaled(c, c->r_wter_res, c->d_forceW));
+        RK(launch_ecor_weighted(c, c->r_wter_res, c->d_forceW, 1));
+    }
     RK(launch_intra_respa(c, inter, c->d_forceW));
     if (flags & PINYB200_DISTRIB_GHOSTS) RK(launch_ghost_distrib(c, c->d_forceW));
     return PINYB200_OK;
@@ -230,9 +237,11 @@ int pinyb200_set_respa(pinyb200_ctx *c, const pinyb200_respa *r)
         c->respa_on = false;
         return PINYB200_OK;
     }
-    if (r->nktot_res > 0)
+    if (r->nktot_res > 0 && r->pme_res_on)
         return record_error(c, PINYB200_ERR_UNSUPPORTED,
-                            "set_respa: the reciprocal-space RESPA set (ewald_respa_kmax) is not supported");
+                            "set_respa: a separate RESPA PME grid (ewald_respa_pme_opt on) is not supported");
+    if (r->nktot_res > 0 && c->sys.necor > 0 && !r->ecor_cdv0_res)
+        return record_error(c, PINYB200_ERR_ARG, "set_respa: ecor_cdv0_res missing (nktot_res > 0)");
     if (!r->cutoff_res || (c->sys.nbond && !r->bond_eq_res))
         return record_error(c, PINYB200_ERR_ARG, "set_respa: cutoff_res / bond_eq_res missing");
     if (!(r->rheal_res > 0.0)) return record_error(c, PINYB200_ERR_ARG, "set_respa: rheal_res must be > 0");
@@ -250,6 +259,13 @@ int pinyb200_set_respa(pinyb200_ctx *c, const pinyb200_respa *r)
                       cudaMemcpyHostToDevice));
     }
     if (!c->d_forceW) RK(cudaMalloc(&c->d_forceW, (size_t)c->sys.natm * 3 * c->P * sizeof(double)));
+    c->r_kres = r->nktot_res > 0 ? 1 : 0;
+    if (c->r_kres && c->sys.necor > 0) {
+        std::vector<double> coef;
+        table_coefs(r->ecor_cdv0_res, c->sys.ecor_nsplin, coef);
+        if (!c->d_ecor_res_tab) RK(cudaMalloc(&c->d_ecor_res_tab, coef.size() * sizeof(double)));
+        RK(cudaMemcpy(c->d_ecor_res_tab, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
     if (c->have_list && !c->build_cell_ok)
         return record_error(c, PINYB200_ERR_STATE, "set_respa: the list build state is missing");
     c->r_wter = r->wght_ter;

@@ -89,7 +89,8 @@ class PinyPimdEnergies(C.Structure):
 class PinyRespa(C.Structure):
     _fields_ = [("wght_ter", _d), ("wght_ter_res", _d), ("wght_tra_res", _d),
                 ("int_res_ter", _i), ("int_res_inter", _i), ("ires_bond", _i),
-                ("cutoff_res", _pd), ("rheal_res", _d), ("bond_eq_res", _pd), ("nktot_res", _i)]
+                ("cutoff_res", _pd), ("rheal_res", _d), ("bond_eq_res", _pd), ("nktot_res", _i),
+                ("pme_res_on", _i), ("ecor_cdv0_res", _pd)]
 
 
 class PinyTangent(C.Structure):
@@ -377,9 +378,12 @@ class DeviceBox:
             return
         cut = np.ascontiguousarray(respa["cutoff_res"], np.float64)
         eqr = np.ascontiguousarray(respa["bond_eq_res"], np.float64)
+        ecr = respa.get("ecor_cdv0_res")
+        ecr = None if ecr is None else np.ascontiguousarray(ecr, np.float64)
         r = PinyRespa(float(respa["wght_ter"]), float(respa["wght_ter_res"]), float(respa["wght_tra_res"]),
                       int(respa["int_res_ter"]), int(respa["int_res_inter"]), int(respa["ires_bond"]), _dp(cut),
-                      float(respa["rheal_res"]), _dp(eqr), int(respa.get("nktot_res", 0)))
+                      float(respa["rheal_res"]), _dp(eqr), int(respa.get("nktot_res", 0)),
+                      int(respa.get("pme_res_on", 0)), None if ecr is None else _dp(ecr))
         self._check(self.L.pinyb200_set_respa(self.h, C.byref(r)), "set_respa")
 
     def respa_force_device(self, d_pos: int, d_xmod, hmat, level: int, d_force: int, d_forcet=None, stream=None,

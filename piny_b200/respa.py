@@ -30,19 +30,26 @@ def respa_weights(nres_ter: int, nres_tor: int, nres_tra: int, nres_pimd: int, p
 
 
 def respa_setup(nres_ter: int, nres_tor: int, nres_tra: int, nres_pimd: int, pimd_on: bool, int_res_ter: bool,
-                cutoff_res, rheal_res: float, bond_eq_res):
+                cutoff_res, rheal_res: float, bond_eq_res, nktot_res: int = 0, ecor_cdv0_res=None):
     """Everything pinyb200_set_respa takes: the weights, PINY's switches
     int_res_ter (``respa_steps_lrf`` given), int_res_inter (nres_ter > 1,
     energy_control_initial.c:223-229) and the bond RESPA flag of
     energy_control_intra.c:116-119 (nres_tra*nres_tor > 1), the inner
-    cutoffs per pair type (Bohr), the switch width (Bohr) and the bonds'
-    RESPA equilibrium lengths per bond type (Bohr)."""
+    cutoffs per pair type (Bohr), the switch width (Bohr), the bonds' RESPA
+    equilibrium lengths per bond type (Bohr) and, for the reciprocal-space
+    RESPA set on the one PME grid (``ewald_respa_kmax`` = ``ewald_kmax``),
+    its k-vector count and the exclusion correction's RESPA force table
+    (``system.ecor_res_table``)."""
     w_ter, w_ter_res, w_tra_res = respa_weights(nres_ter, nres_tor, nres_tra, nres_pimd, pimd_on)
-    return {"wght_ter": w_ter, "wght_ter_res": w_ter_res, "wght_tra_res": w_tra_res,
-            "int_res_ter": int(bool(int_res_ter)), "int_res_inter": int(nres_ter > 1),
-            "ires_bond": int(nres_tra * nres_tor > 1),
-            "cutoff_res": np.ascontiguousarray(cutoff_res, np.float64), "rheal_res": float(rheal_res),
-            "bond_eq_res": np.ascontiguousarray(bond_eq_res, np.float64)}
+    out = {"wght_ter": w_ter, "wght_ter_res": w_ter_res, "wght_tra_res": w_tra_res,
+           "int_res_ter": int(bool(int_res_ter)), "int_res_inter": int(nres_ter > 1),
+           "ires_bond": int(nres_tra * nres_tor > 1),
+           "cutoff_res": np.ascontiguousarray(cutoff_res, np.float64), "rheal_res": float(rheal_res),
+           "bond_eq_res": np.ascontiguousarray(bond_eq_res, np.float64), "nktot_res": int(nktot_res),
+           "pme_res_on": 0}
+    if ecor_cdv0_res is not None:
+        out["ecor_cdv0_res"] = np.ascontiguousarray(ecor_cdv0_res, np.float64)
+    return out
 
 
 def level_bits(iget_full_inter: int, iget_res_inter: int, iget_full_intra: int, iget_res_intra: int) -> int:

@@ -277,6 +277,33 @@ def ecor_table(nsplin, rmax, alp, ecut):
     return cv0, cdv0, dr, dri, self_erf
 
 
+def ecor_res_table(nsplin, rmax, alp, ecut, ecut_res):
+    """ecor.cdv0_res of splin_ecor (set_exclude.c:670-745) for the
+    reciprocal-space RESPA set: the force table of ``ecor_table`` without its
+    finite-k correction, plus the correction for the RESPA k cutoff
+    sqrt(2 ecut_res) (ecut_res = ecor.ecut_res, 4x the RESPA k-list cutoff)."""
+    _, cdv0, dr, _, _ = ecor_table(nsplin, rmax, alp, ecut)
+    rmin = 0.1
+    i = np.arange(1, nsplin + 1, dtype=np.float64)
+    r12 = dr * (i - 3.0) + rmin
+    node, weight = gauss_legendre_128()
+    alp2 = alp * alp
+    kmax = 15.0 * alp
+
+    def dchi(kc):
+        if not kmax > kc:
+            return np.zeros_like(r12)
+        dk, pk = kmax - kc, kmax + kc
+        know = 0.5 * (node * dk + pk)
+        fknow = (dk / math.pi) * np.exp(-0.25 * know * know / alp2) * weight
+        a = know[None, :] * r12[:, None]
+        s = np.sin(a)
+        j1 = (s / a - np.cos(a)) / a
+        return (know[None, :] * fknow[None, :] * j1 / r12[:, None]).sum(axis=1)
+
+    return cdv0 - dchi(math.sqrt(2.0 * ecut)) + dchi(math.sqrt(2.0 * ecut_res))
+
+
 def bend_harm_coefs(fk, theta0):
     """bend_coef "harm" (intra_coefs.c:240-276) and derivatives (:355-371)."""
     cn1, cn2, cn3, cn4 = 49.0 / 72.0, 3.0 / 4.0, 3.0 / 40.0, 1.0 / 180.0

@@ -232,7 +232,10 @@ def piny_input_files(spec: BoxSpec, pos_angstrom, sim_typ=None, respa=None):
     ``respa`` (optional) switches on PINY's RESPA split: a dict with the step
     counts ``lrf``, ``intra``, ``pimd`` (respa_steps_lrf / _intra / _pimd),
     ``rheal`` (respa_rheal, Angstrom) and ``eq_res`` (the bond's eq_res
-    shift, Angstrom); the inner cutoff is each pair's ``res_dist``."""
+    shift, Angstrom), and optionally ``kmax_res`` (ewald_respa_kmax, the
+    reciprocal-space RESPA set) with ``pme_res`` = (ewald_respa_kmax_pme,
+    ewald_respa_interp_pme) for PINY's separate RESPA PME grid; the inner
+    cutoff is each pair's ``res_dist``."""
     model = spec.model
     P = spec.nbeads
     L = spec.L
@@ -262,7 +265,10 @@ def piny_input_files(spec: BoxSpec, pos_angstrom, sim_typ=None, respa=None):
             "ewald_alpha": _fmt(spec.alpha * L), "ewald_kmax": spec.kmax_ewald,
             "ewald_pme_opt": "on", "ewald_kmax_pme": spec.kmax_pme,
             "ewald_interp_pme": spec.order, "ewald_respa_pme_opt": "off",
-            "inter_PE_calc_freq": 1, "sep_VanderWaals": "on"}),
+            "inter_PE_calc_freq": 1, "sep_VanderWaals": "on",
+            **({"ewald_respa_kmax": int(respa["kmax_res"])} if respa and respa.get("kmax_res") else {}),
+            **({"ewald_respa_pme_opt": "on", "ewald_respa_kmax_pme": int(respa["pme_res"][0]),
+                "ewald_respa_interp_pme": int(respa["pme_res"][1])} if respa and respa.get("pme_res") else {})}),
         ("sim_nhc_def", {"atm_nhc_tau_def": 20.0, "atm_nhc_len": 4, "respa_steps_nhc": 1,
                          "yosh_steps_nhc": 3, "respa_xi_opt": 1}),
         ("sim_write_def", {

@@ -353,14 +353,25 @@ RESPA_CASES = [
     ("respa_spcfw_64_p1",
      water.BoxSpec(water.SPC_FW, 64, 12.416, 1, 300.0, 106, cutoff=6.0, grid=16, order=6, kmax=6),
      {"lrf": 3, "intra": 2, "pimd": 1, "rheal": 1.0, "eq_res": -0.01}),
+    # the reciprocal-space RESPA set on the one PME grid (PINY demands
+    # ewald_respa_kmax = ewald_kmax when ewald_respa_pme_opt is off)
+    ("respa_kspace_tip4pf_64_p4",
+     water.BoxSpec(water.TIP4P_F, 64, 12.416, 4, 298.0, 107, cutoff=6.0, grid=16, order=8, kmax=6),
+     {"lrf": 2, "intra": 2, "pimd": 1, "rheal": 0.8, "eq_res": 0.02, "kmax_res": 6}),
 ]
+
+# PINY's separate RESPA PME grid (ewald_respa_pme_opt on, kmax_res < kmax):
+# only its set-up products are kept (the exclusion correction's RESPA table)
+RESPA_GRID_CASE = ("respa_pmegrid_tip4pf_64_p4",
+                   water.BoxSpec(water.TIP4P_F, 64, 12.416, 4, 298.0, 108, cutoff=6.0, grid=16, order=8, kmax=6),
+                   {"lrf": 2, "intra": 1, "pimd": 1, "rheal": 0.8, "eq_res": 0.0, "kmax_res": 3, "pme_res": (4, 4)})
 
 
 def respa_fixture(tmp):
     """PINY's forces at each RESPA level (``piny_ref respa``): the flags
     int_NVT_pimd sets at the outer step, an inner inter step, an intra step
     and the innermost step, on seeded boxes with RESPA inputs."""
-    for name, spec, rk in RESPA_CASES:
+    for name, spec, rk in RESPA_CASES + [RESPA_GRID_CASE]:
         pos = water.build_positions(spec)
         d = os.path.join(tmp, "respa_inp")
         shutil.rmtree(d, ignore_errors=True)
@@ -377,6 +388,11 @@ def respa_fixture(tmp):
         fx["cutoff_res"] = D["cutoff_res"]
         fx["rheal_res"] = float(D["rheal_res"][0])
         fx["bond_eq_res"] = D["bond_eq_res"]
+        fx["nktot_res"] = int(D["nktot_res"][0])
+        fx["pme_res_on"] = int(D["pme_res_on"][0])
+        if "ecor_cdv0_res" in D:
+            fx["ecor_cdv0_res"] = D["ecor_cdv0_res"]
+            fx["ecor_ecut_res"] = float(D["ecor_ecut_res"][0])
         for lv in range(4):
             fx["L%d_flags" % lv] = D["L%d_flags" % lv]
             fx["ref_L%d_force_raw" % lv] = D["L%d_force_raw" % lv].reshape(P, n, 3)
@@ -391,6 +407,10 @@ def respa_fixture(tmp):
         fx["spec_order"] = spec.order
         fx["spec_nsplin"] = spec.nsplin
         fx["spec_temperature"] = spec.temperature
+        if name == RESPA_GRID_CASE[0]:
+            keep = ("ecor_nsplin", "ecor_rmax", "alp_ewd", "ecor_ecut", "ecor_ecut_res", "ecor_cdv0",
+                    "ecor_cdv0_res", "nktot", "nktot_res", "pme_res_on", "natm", "nbeads")
+            fx = {k: fx[k] for k in keep}
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **{k: np.asarray(v) for k, v in fx.items()})
         print(name, os.path.getsize(path), "bytes")

@@ -32,7 +32,7 @@ def rel_rms(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
 
 
-RESPA_NAMES = ["respa_tip4pf_64_p4", "respa_spcfw_64_p1"]
+RESPA_NAMES = ["respa_tip4pf_64_p4", "respa_spcfw_64_p1", "respa_kspace_tip4pf_64_p4"]
 
 
 def respa_from_fixture(F):
@@ -41,7 +41,7 @@ def respa_from_fixture(F):
     from piny_b200.respa import respa_setup
     return respa_setup(int(F["nres_ter"]), int(F["nres_tor"]), int(F["nres_tra"]), int(F["nres_pimd"]),
                        int(F["nbeads"]) > 1, bool(F["int_res_ter"]), F["cutoff_res"], float(F["rheal_res"]),
-                       F["bond_eq_res"])
+                       F["bond_eq_res"], nktot_res=int(F["nktot_res"]), ecor_cdv0_res=F.get("ecor_cdv0_res"))
 
 
 def fixture_level(F, lv):

@@ -115,7 +115,9 @@ def test_respa_arguments():
     with pytest.raises(PinyError, match="ERR_ARG"):
         box.set_respa(bad)
     with pytest.raises(PinyError, match="ERR_UNSUPPORTED"):
-        box.set_respa(dict(rs, nktot_res=12))
+        box.set_respa(dict(rs, nktot_res=12, pme_res_on=1))
+    with pytest.raises(PinyError, match="ERR_ARG"):
+        box.set_respa(dict(rs, nktot_res=12))  # the RESPA exclusion table is needed
     box.set_respa(rs)
     # levels PINY's loops never set are refused
     for lv in (R.FULL_INTER, R.RES_INTER, R.FULL_INTER | R.FULL_INTRA | R.RES_INTRA):

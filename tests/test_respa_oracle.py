@@ -39,6 +39,23 @@ def test_respa_oracle_matches_piny(name, oracle):
         assert rel_rms(plain, F["ref_L0_forcet_raw"]) < 1e-13
 
 
+@pytest.mark.parametrize("name", ["respa_kspace_tip4pf_64_p4", "respa_pmegrid_tip4pf_64_p4"])
+def test_ecor_res_table_matches_piny(name):
+    """The exclusion correction's RESPA force table from piny_b200.system
+    against PINY's ecor.cdv0_res: RESPA k cutoff equal to the full one (one
+    PME grid) and smaller (PINY's separate RESPA grid)."""
+    from piny_b200 import system
+    F = load_fixture(name)
+    t = system.ecor_res_table(int(F["ecor_nsplin"]), float(F["ecor_rmax"]), float(F["alp_ewd"]),
+                              float(F["ecor_ecut"]), float(F["ecor_ecut_res"]))
+    ref = F["ecor_cdv0_res"]
+    # as for the plain table: Gauss-Legendre nodes computed here, PINY's
+    # are tabulated (weights_nodes_128.h)
+    assert np.abs(t - ref).max() <= 1e-10 * np.abs(ref).max()
+    if name == "respa_pmegrid_tip4pf_64_p4":
+        assert np.abs(ref - F["ecor_cdv0"]).max() > 1e-6 * np.abs(ref).max()
+
+
 def test_respa_loop_levels():
     """int_NVT_pimd's nesting: the last call of a step is the full level,
     inner inter calls close each (tor, tra) sweep, the rest are innermost."""
