@@ -486,6 +486,7 @@ def run_respa(args, ws, rank, local):
     box = DeviceBox(S, P, args.precision)
     box.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
     nres = (2, 1, 2, 1)
+    rk = {"lrf": nres[0], "intra": nres[2], "pimd": nres[3], "rheal": 1.0, "eq_res": 0.0}
     cut_res = np.minimum(np.asarray(S["cutoff"]), 5.0 / water.BOHR)
     rs = R.respa_setup(*nres, True, True, cut_res, 1.0 / water.BOHR, np.asarray(S["bond_eq"]))
     box.set_respa(rs)
@@ -544,6 +545,9 @@ def run_respa(args, ws, rank, local):
              "outer (everything, weighted and plain)"}
     if rank == 0:
         plain_ms = float(np.mean(plain))
+        cpu = None
+        if not args.no_cpu_baseline and ws == 1:
+            cpu = respa_cpu_baseline(spec, pos * water.BOHR, rk, levels)
         line = {
             "metric": "RESPA steps/s (force calls of one PINY step, TIP4P/F 4096 mol x 32 beads)",
             "value": ws * 1e3 / ms, "unit": "RESPA steps/s", "n_gpus": ws, "steps": args.steps,
@@ -557,7 +561,7 @@ def run_respa(args, ws, rank, local):
                        "plain_evaluation_ms": plain_ms,
                        "plain_ms_for_the_same_inner_steps": plain_ms * len(levels),
                        "l2": "256 MiB buffer written before each timed call; CUDA events on the launch stream"},
-            "roofline": None, "cpu_baseline": None, "e2e": None, "gpu_launches": None, "clocks": clocks,
+            "roofline": None, "cpu_baseline": cpu, "e2e": None, "gpu_launches": None, "clocks": clocks,
         }
         print(json.dumps(line))
     box.close()
@@ -565,6 +569,33 @@ def run_respa(args, ws, rank, local):
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+def respa_cpu_baseline(spec, pos_A, rk, levels):
+    """PINY's own CPU path (oracle/_ref/piny_ref respa_time) on the same box
+    with the same RESPA input: each level once on 2 of the beads, 1 core,
+    after one warm-up round; one RESPA step = the step's levels, scaled to
+    all beads."""
+    from piny_b200 import respa as R
+    from piny_b200 import water
+    exe = piny_ref_binary()
+    if not exe:
+        return None
+    d = tempfile.mkdtemp(prefix="piny_respa_")
+    water.write_piny_input(d, spec, pos_A, respa=rk)
+    r = subprocess.run([exe, "respa_time", d, "water.input", "1", "2"], capture_output=True, text=True)
+    shutil.rmtree(d, ignore_errors=True)
+    if r.returncode != 0:
+        return None
+    t = {int(l.split()[1]): float(l.split()[2]) for l in r.stdout.splitlines() if l.startswith("level")}
+    # piny_ref's level order: outer, inner inter, full intra, innermost
+    code = {R.FULL_INTER | R.RES_INTER | R.FULL_INTRA | R.RES_INTRA: 0, R.RES_INTER | R.FULL_INTRA | R.RES_INTRA: 1,
+            R.FULL_INTRA | R.RES_INTRA: 2, R.RES_INTRA: 3}
+    step_s = sum(t[code[lv]] for lv in levels) * spec.nbeads / 2.0
+    return {"value": 1.0 / step_s, "unit": "RESPA steps/s", "cores": 1, "kind": "reference",
+            "sample": "PINY's energy_control sub-steps at each RESPA level (oracle/_ref/piny_ref respa_time), "
+                      "2 of 32 beads per level, 1 host core, after one warm-up round; scaled to 32 beads",
+            "seconds_per_level_2_beads": {str(k): v for k, v in t.items()}}
 
 
 def run_batch(args, ws, rank, local):

@@ -37,6 +37,9 @@
  *                 175-189), then the full step dumped as in dump, plus per
  *                 level the raw forces (and at the full level the virial
  *                 forces fxt) and the RESPA set-up.
+ *   piny_ref respa_time <dir> <input> <reps> <nbeads>   with a RESPA input:
+ *                 time <reps> rounds of the four RESPA levels on the first
+ *                 <nbeads> beads (one line "level L seconds" per call)
  *   piny_ref springs <in.bin> <out.bin>  mode_energy_control
  *                 (pimd_estimators.c:31) on modes u, then pimd_pvten_forc_corr
  *                 (pimd_estimators.c:223) on positions x with forces f (also
@@ -713,6 +716,27 @@ static void gather_forces(double *buf, int t)
         }
 }
 
+static int run_respa_time(const char *dir, const char *input, int reps, int nb)
+{
+    setup(dir, input);
+    CLATOMS_INFO *ci = &class_.clatoms_info;
+    if (nb < 1 || nb > ci->pi_beads) nb = ci->pi_beads;
+    ci->pi_beads_proc = nb;
+    for (int l = 0; l < 4; l++) { /* warm-up */
+        set_level(l);
+        evaluate();
+    }
+    for (int r = 0; r < reps; r++)
+        for (int l = 0; l < 4; l++) {
+            set_level(l);
+            double t0 = now_s();
+            evaluate();
+            printf("level %d %.6f s\n", l, now_s() - t0);
+            fflush(stdout);
+        }
+    return 0;
+}
+
 static int run_respa(const char *dir, const char *input, const char *outpath)
 {
     setup(dir, input);
@@ -866,6 +890,8 @@ static int run_io(const char *dir, const char *input, const char *outdir_rel, in
 int main(int argc, char **argv)
 {
     if (argc == 6 && strcmp(argv[1], "io") == 0) return run_io(argv[2], argv[3], argv[4], atoi(argv[5]));
+    if (argc == 6 && strcmp(argv[1], "respa_time") == 0)
+        return run_respa_time(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]));
     if (argc == 5 && strcmp(argv[1], "respa") == 0) return run_respa(argv[2], argv[3], resolve_out(argv[4]));
     if (argc == 4 && strcmp(argv[1], "nhc") == 0) return run_nhc(argv[2], argv[3]);
     if (argc == 4 && strcmp(argv[1], "springs") == 0) return run_springs(argv[2], argv[3]);
