@@ -549,6 +549,13 @@ typedef struct pinyb200_pimd_setup {
     int nfree_atoms;         /* natm - nghost - nfreeze (virial estimator)   */
     pinyb200_nhc_set class_nhc;
     pinyb200_nhc_set bead_nhc;
+    /* RESPA (timeinfo.nres_ter, nres_tor, nres_tra, nres_pimd; 0 reads as 1)
+     * and the level whose steps carry the chains (timeinfo.ix_respa, 1..5;
+     * 0 reads as 1).  With a count above 1 the force context needs
+     * pinyb200_set_respa; the chains' wdti must then be formed from PINY's
+     * dt_nhc for ix_respa (int_NVT_pimd.c:96-125). */
+    int nres_ter, nres_tor, nres_tra, nres_pimd;
+    int ix_respa;
 } pinyb200_pimd_setup;
 
 typedef struct pinyb200_pimd_energies {
@@ -585,9 +592,18 @@ int pinyb200_pimd_forces(pinyb200_pimd *pm, pinyb200_ctx *ctx, double *d_x, doub
  * int_0_to_dt2_pimd.c:34-190), positions to modes, drift, springs, modes
  * to positions, the device list update (pinyb200_update_list_device),
  * the forces as in pinyb200_pimd_forces, half kick and chains
- * (int_dt2_to_dt_nvt_pimd, int_dt2_to_dt_pimd.c).  d_x: bead positions,
- * d_v: mode velocities, d_f: mode forces of d_x on entry, of the new d_x
- * on return.  Blocks until done. */
+ * (int_dt2_to_dt_nvt_pimd, int_dt2_to_dt_pimd.c).  With RESPA counts above
+ * 1 the step is int_NVT_pimd's nested loops (int_NVT_pimd.c:142-223): every
+ * inner step of dt / (nres_ter nres_tor nres_tra nres_pimd) kicks with the
+ * current mode forces, the chains run at the inner steps that open / close
+ * a loop of level <= ix_respa, positions go to modes at ir_pimd = 1 and back
+ * at ir_pimd = nres_pimd, where the force path is asked for the level of
+ * :175-189 (pinyb200_respa_force_device; the virial estimator from the
+ * outer level's virial forces), and the other inner steps use the spring
+ * forces alone.  d_x: bead positions, d_v: mode velocities, d_f: mode
+ * forces of d_x on entry, of the new d_x on return (the outer level's
+ * weighted forces with RESPA).  Energies are those of the outer level.
+ * Blocks until done. */
 int pinyb200_pimd_step(pinyb200_pimd *pm, pinyb200_ctx *ctx, double *d_x, double *d_v, double *d_f,
                        const double *hmat, pinyb200_pimd_energies *e, void *stream);
 

@@ -87,6 +87,8 @@ class Oracle:
         L.orc_pimd_springs.argtypes = [_i, _i, _pd, _pd, _pd, _d, _pd, _pd]
         L.orc_pimd_force_post.restype = _d
         L.orc_pimd_force_post.argtypes = [_i, _i, _i, _pd, _pd, _pd, _pd, _i, _d, _pd, _pd]
+        L.orc_pimd_force_post_respa.restype = _d
+        L.orc_pimd_force_post_respa.argtypes = [_i, _i, _i, _pd, _pd, _pd, _pd, _pd, _i, _d, _i, _pd, _pd]
         L.orc_ecor_table.argtypes = [_i, _d, _d, _d, _pd, _pd, _pd, _pd, _pd]
         L.orc_gauss_legendre.argtypes = [_i, _pd, _pd]
         L.orc_bond_power.argtypes = [_d, _d, _d, _pd, _pd]
@@ -401,6 +403,94 @@ def pimd_apply_chains(orc, setup, v, state):
             v[b], state["bx"][b - 1], state["bv"][b - 1] = nhc_apply(orc, v[b], setup["bead_mass"][b], bead,
                                                                      state["bx"][b - 1], state["bv"][b - 1])
     return v
+
+
+def pimd_force_post_respa(orc, kind, f, ft, x, xmod, fm, nfree, beta, full, pvten, pvten_tot):
+    """energy_control_pimd's post-processing at one RESPA level: (mode
+    forces, akvirx, pvten, pvten_tot); ft = the virial forces (full level)."""
+    f = _c(f).copy()
+    ftc = None if ft is None else _c(ft).copy()
+    x, xmod, fm = _c(x), _c(xmod), _c(fm)
+    pv, pvt = _c(pvten).copy(), _c(pvten_tot).copy()
+    akv = orc.lib.orc_pimd_force_post_respa(f.shape[1], f.shape[0], int(kind), f.ctypes.data_as(_pd),
+                                            None if ftc is None else ftc.ctypes.data_as(_pd), x.ctypes.data_as(_pd),
+                                            xmod.ctypes.data_as(_pd), fm.ctypes.data_as(_pd), int(nfree), float(beta),
+                                            1 if full else 0, pv.ctypes.data_as(_pd), pvt.ctypes.data_as(_pd))
+    return f, akv, pv, pvt
+
+
+def pimd_step_respa(orc, sysd, setup, respa, x, v, f, state, pi, pj):
+    """pinyb200_pimd_step with RESPA counts setup["nres"] = (nres_ter,
+    nres_tor, nres_tra, nres_pimd) and chains at level setup["ix_respa"]:
+    int_NVT_pimd's nested loops (int_NVT_pimd.c:142-223) with
+    int_0_to_dt2_nvt_pimd / int_dt2_to_dt_nvt_pimd (int_0_to_dt2_pimd.c:
+    34-190, int_dt2_to_dt_pimd.c) and the force path at each level
+    (orc_respa_force, then orc_pimd_force_post_respa).  Returns new (x, v,
+    f, energies of the outer level); `state` is updated."""
+    P, kind, dt = int(setup["nbeads"]), int(setup["kind"]), float(setup["dt"])
+    nt, no, na, npi = (int(k) for k in setup["nres"])
+    ixr = int(setup.get("ix_respa", 1))
+    dti = dt / float(nt * no * na * npi)
+    bm = np.asarray(setup["bead_mass"], np.float64)[:, :, None]
+    x, v, f = _c(x).copy(), _c(v).copy(), _c(f).copy()
+    u = None
+    e = None
+    for ir_ter in range(1, nt + 1):
+        for ir_tor in range(1, no + 1):
+            for ir_tra in range(1, na + 1):
+                for ir_pimd in range(1, npi + 1):
+                    ix = 5
+                    if ir_pimd == 1:
+                        ix = 4
+                        if ir_tra == 1:
+                            ix = 3
+                            if ir_tor == 1:
+                                ix = 1 if ir_ter == 1 else 2
+                    if ixr >= ix:
+                        v = pimd_apply_chains(orc, setup, v, state)
+                    v = v + (f * (dti / 2.0)) / bm
+                    if ir_pimd == 1:
+                        u = orc.pimd_transform(x, kind, 0) if P > 1 else x.copy()
+                    u = u + v * dti
+                    fm, ake, pvm = pimd_springs(orc, u, setup["prekf"], setup["path_eig"], setup.get("wght_pimd", 1.0))
+                    if ir_pimd == npi:
+                        xmod = u[0].copy()
+                        x = orc.pimd_transform(u, kind, 1) if P > 1 else u.copy()
+                        x = ghost_positions(sysd, x)
+                        last_tra = ir_tra == na
+                        level = 8 | (4 if last_tra else 0)
+                        if respa["int_res_ter"] and ir_tor == no and last_tra:
+                            level |= 2
+                        full = ir_ter == nt and ir_tor == no and last_tra
+                        if full:
+                            level |= 1
+                        fw, ft = orc.respa_force(sysd, respa, level, x, xmod if P > 1 else None, sysd["hmat"], pi, pj,
+                                                 distribute_ghosts=True)
+                        if full:
+                            _, ef = orc.energy_force(sysd, x, xmod if P > 1 else None, sysd["hmat"], pi, pj,
+                                                     distribute_ghosts=True)
+                            pv0 = ef["pvten"]
+                        else:
+                            pv0 = np.zeros(9)
+                        f, akv, pv, pvt = pimd_force_post_respa(orc, kind, fw, ft, x, xmod, fm, setup["nfree_atoms"],
+                                                                setup["beta"], full, pv0, pv0)
+                        if full:
+                            e = dict(ef)
+                            e.update(kin_harm=ake, akvirx=akv if P > 1 else 0.0, pvten_tot_corr=pvt,
+                                     pvten_mode_tot=pvm)
+                    else:
+                        f = fm
+                    v = v + (f * (dti / 2.0)) / bm
+                    ix = 5
+                    if ir_pimd == npi:
+                        ix = 4
+                        if ir_tra == na:
+                            ix = 3
+                            if ir_tor == no:
+                                ix = 1 if ir_ter == nt else 2
+                    if ixr >= ix:
+                        v = pimd_apply_chains(orc, setup, v, state)
+    return x, v, f, e
 
 
 def pimd_step(orc, sysd, setup, x, v, f, state, pi, pj):

@@ -146,3 +146,44 @@ double orc_pimd_force_post(int natm, int P, int kind, double *f, const double *x
     for (size_t k = 0; k < (size_t)P * n3; k++) f[k] += fm[k];
     return 0.5 * akvirx;
 }
+
+/* energy_control_pimd's post-processing at one RESPA level
+ * (energy_control_pimd.c:113-218, pimd_pvten_forc_corr pimd_estimators.c:
+ * 223-305): forces / P; pvten corrected with the (weighted) forces f at
+ * every level; at a full level (iget_full_inter and iget_full_intra) the
+ * virial forces ft / P give akvirx and the pvten_tot correction; forces to
+ * modes, springs added.  ft may be NULL when full is 0.  Returns 0.5 akvirx
+ * (0 below the full level). */
+double orc_pimd_force_post_respa(int natm, int P, int kind, double *f, double *ft, const double *x,
+                                 const double *xmod, const double *fm, int nfree_atoms, double beta, int full,
+                                 double *pvten, double *pvten_tot)
+{
+    const size_t n3 = (size_t)natm * 3;
+    for (size_t k = 0; k < (size_t)P * n3; k++) f[k] /= P;
+    if (full && ft)
+        for (size_t k = 0; k < (size_t)P * n3; k++) ft[k] /= P;
+    for (int k = 0; k < 9; k++) {
+        pvten[k] /= P;
+        pvten_tot[k] /= P;
+    }
+    double akvirx = full ? 3.0 * (double)nfree_atoms / beta : 0.0;
+    for (int b = 0; b < (P > 1 ? P : 0); b++) {
+        for (int i = 0; i < natm; i++) {
+            const double *p = x + b * n3 + 3 * (size_t)i, *g = f + b * n3 + 3 * (size_t)i;
+            double d[3] = {p[0] - xmod[3 * i], p[1] - xmod[3 * i + 1], p[2] - xmod[3 * i + 2]};
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) pvten[3 * r + c] -= d[r] * g[c];
+        }
+        if (!full) continue;
+        for (int i = 0; i < natm; i++) {
+            const double *p = x + b * n3 + 3 * (size_t)i, *g = ft + b * n3 + 3 * (size_t)i;
+            double d[3] = {p[0] - xmod[3 * i], p[1] - xmod[3 * i + 1], p[2] - xmod[3 * i + 2]};
+            akvirx -= (d[0] * g[0] + d[1] * g[1] + d[2] * g[2]);
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) pvten_tot[3 * r + c] -= d[r] * g[c];
+        }
+    }
+    if (P > 1) orc_pimd_transform(natm, P, kind, 2, f);
+    for (size_t k = 0; k < (size_t)P * n3; k++) f[k] += fm[k];
+    return 0.5 * akvirx;
+}

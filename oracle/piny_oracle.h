@@ -199,6 +199,10 @@ void orc_energy_force(const orc_system *sys, int nbeads, const double *pos,
                       int distribute_ghosts, double *force,
                       orc_energies *e);
 
+double orc_pimd_force_post_respa(int natm, int P, int kind, double *f, double *ft, const double *x,
+                                 const double *xmod, const double *fm, int nfree_atoms, double beta, int full,
+                                 double *pvten, double *pvten_tot);
+
 #ifdef __cplusplus
 }
 #endif

@@ -262,6 +262,8 @@ int evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, bool timing, 
 // last list build (PINY's jter_res), rebuilt with every list build
 int respa_list_enqueue(pinyb200_ctx *c, const Cell &cell, const int *gate, cudaStream_t st);
 int respa_list_reserve(pinyb200_ctx *c, const Cell &cell);
+// one RESPA level on c->stream (see respa.cu); PINYB200_* level bits
+int respa_level_enqueue(pinyb200_ctx *c, const Cell &cell, int level, int flags, double *h_acc);
 cudaError_t launch_respa_scale_copy(pinyb200_ctx *c, double w, double *target);
 // bead-1 and mode-1 positions and cutskin^2 of a list build, kept for the
 // RESPA list (gated like the build on the device)

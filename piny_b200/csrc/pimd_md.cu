@@ -1,7 +1,7 @@
 // Path-integral MD bookkeeping around the force call, on the device, FP64:
-// PINY's NVT ring-polymer step (int_NVT_pimd with every RESPA count 1).
+// PINY's NVT ring-polymer step (int_NVT_pimd), RESPA loops included.
 //
-// Per step (src/integrate/pimd/int_NVT_pimd.c:142-217):
+// Per step with every RESPA count 1 (src/integrate/pimd/int_NVT_pimd.c:142-217):
 //   chains, half kick            int_0_to_dt2_nvt_pimd (int_0_to_dt2_pimd.c:34-190)
 //   positions -> modes, drift    control_pimd_trans_mode, x += v dt
 //   springs on the modes         mode_energy_control (pimd_estimators.c:31-110)
@@ -16,8 +16,9 @@
 // The chain operator is apply_NHC_par (src/integrate/md/int_NVT.c:144-353):
 // one thread per chain runs the RESPA x Yoshida-Suzuki loop; the kinetic
 // energy of each chain is summed with FP64 atomics and the velocities are
-// scaled afterwards.  Layouts: bead arrays [P][natm][3]; chain state
-// [beads of the set][len_nhc][num_nhc].
+// scaled afterwards.  With RESPA counts above 1 these are the inner steps of
+// int_NVT_pimd's four nested loops (step_enqueue).  Layouts: bead arrays
+// [P][natm][3]; chain state [beads of the set][len_nhc][num_nhc].
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -293,7 +294,10 @@ struct pinyb200_pimd {
     cudaGraphExec_t exec = nullptr;
     std::vector<double> key;     // pointers, cell, context and its generation
     std::vector<double> eager;   // key of the last eager step (the capture follows it)
-    bool graph_mode = false;     // the last step ran as a graph (no per-phase timing)  // 0: class (bead 1), 1: bead (beads 2..P)
+    bool graph_mode = false;     // the last step ran as a graph (no per-phase timing)
+    int nres[4] = {1, 1, 1, 1};  // RESPA counts: inter, torsion, intra, bead
+    int ix_respa = 1;            // chains at the inner steps of loops of level <= ix_respa
+    double *d_ft = nullptr;      // [P][natm][3] virial forces of the outer RESPA level
     std::string err;
 };
 
@@ -414,20 +418,44 @@ int ghost_positions(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, cudaStream_
 
 // Force path and post-processing, enqueued on st (springs already in d_fm
 // and acc): the force evaluation, forces / P with the centroid virial sums,
-// forces to modes, springs added, and the sums copied to the host.  Nothing
-// waits here; pimd_finish does, once per call.
+// forces to modes, springs added, and the sums copied to the host.  level 0
+// is the plain evaluation; otherwise the RESPA level (PINYB200_* bits) of
+// the force context's split, whose weighted forces are the step's forces
+// and, at the outer level, whose virial forces feed the virial sums
+// (pimd_pvten_forc_corr, pimd_estimators.c:262-301).  Nothing waits here;
+// pimd_finish does, once per call.
 int forces_enqueue(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, const double *d_xmod, double *d_f,
-                   const pinyb200::Cell &cell, cudaStream_t st, bool timing)
+                   const pinyb200::Cell &cell, cudaStream_t st, bool timing, int level = 0)
 {
     cudaStream_t own = c->stream;
     c->stream = st;  // the evaluation runs on the caller's stream
-    int rc = pinyb200::enqueue_device(c, d_x, pm->P > 1 ? d_xmod : nullptr, cell, PINYB200_DISTRIB_GHOSTS, d_f, timing,
-                                      pm->h_facc);
-    c->stream = own;
-    if (rc) return rc;
     const long long nb = (long long)pm->natm * pm->P, n = nb * 3;
-    post_kernel<<<blocks_for(nb, 256), 256, 0, st>>>(d_f, d_x, d_xmod, pm->natm, pm->P, pm->P > 1, pm->d_acc);
-    PCK(cudaGetLastError());
+    int rc;
+    if (level == 0) {
+        rc = pinyb200::enqueue_device(c, d_x, pm->P > 1 ? d_xmod : nullptr, cell, PINYB200_DISTRIB_GHOSTS, d_f,
+                                      timing, pm->h_facc);
+        c->stream = own;
+        if (rc) return rc;
+        post_kernel<<<blocks_for(nb, 256), 256, 0, st>>>(d_f, d_x, d_xmod, pm->natm, pm->P, pm->P > 1, pm->d_acc);
+        PCK(cudaGetLastError());
+    } else {
+        const bool outer = level & PINYB200_FULL_INTER;
+        rc = pinyb200::stage_positions(c, d_x, pm->P > 1 ? d_xmod : nullptr, cell, 0);
+        if (!rc) rc = pinyb200::respa_level_enqueue(c, cell, level, PINYB200_DISTRIB_GHOSTS, outer ? pm->h_facc : nullptr);
+        cudaError_t e = cudaSuccess;
+        if (!rc) e = pinyb200::launch_transpose_out(c, d_f, c->d_forceW);
+        if (!rc && e == cudaSuccess && outer) e = pinyb200::launch_transpose_out(c, pm->d_ft, c->d_forceT);
+        c->stream = own;
+        if (rc) return rc;
+        PCK(e);
+        // the virial estimator from the outer level's virial forces; the
+        // weighted forces are only divided by P
+        if (outer)
+            post_kernel<<<blocks_for(nb, 256), 256, 0, st>>>(pm->d_ft, d_x, d_xmod, pm->natm, pm->P, pm->P > 1,
+                                                             pm->d_acc);
+        post_kernel<<<blocks_for(nb, 256), 256, 0, st>>>(d_f, d_x, d_xmod, pm->natm, pm->P, 0, pm->d_acc);
+        PCK(cudaGetLastError());
+    }
     if (pm->P > 1) {
         rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_FORCE_TO_MODES, d_f, st);
         if (rc) return rc;
@@ -492,34 +520,84 @@ void drop_graph(pinyb200_pimd *pm)
 }
 
 // Everything of one step up to the host read of its sums, enqueued on st
-// with no waits (capturable).
+// with no waits (capturable): int_NVT_pimd's loops over the inter, torsion,
+// intra and bead RESPA levels (int_NVT_pimd.c:142-223), one pass when every
+// count is 1.
 int step_enqueue(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double *d_v, double *d_f,
                  const pinyb200::Cell &cell, cudaStream_t st, bool timing)
 {
     int rc;
     const long long n = (long long)pm->natm * pm->P * 3;
-    const double dt2 = pm->dt / 2.0;
-    // t = 0 -> dt/2: chains, half kick
-    if ((rc = apply_all_nhc(pm, d_v, st))) return rc;
-    kick_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_v, d_f, pm->d_bmass, n, dt2);
-    PCK(cudaGetLastError());
-    // positions -> modes, drift, springs, modes -> positions
-    if (pm->P > 1 && (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_MODES, d_x, st))) return rc;
-    drift_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_x, d_v, n, pm->dt);
-    PCK(cudaGetLastError());
-    PCK(cudaMemsetAsync(pm->d_acc, 0, sizeof(double) * A_N, st));
-    if ((rc = springs(pm, d_x, st))) return rc;
-    PCK(cudaMemcpyAsync(pm->d_xmod, d_x, sizeof(double) * (size_t)pm->natm * 3, cudaMemcpyDeviceToDevice, st));
-    if (pm->P > 1 && (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_BEADS, d_x, st))) return rc;
-    if ((rc = ghost_positions(pm, c, d_x, st))) return rc;
-    // PINY's list test and, when due, the rebuild -- on the device
-    if ((rc = pinyb200::list_update_enqueue(c, d_x, pm->P > 1 ? pm->d_xmod : nullptr, cell, st))) return rc;
-    // forces of the new positions, as mode forces
-    if ((rc = forces_enqueue(pm, c, d_x, pm->d_xmod, d_f, cell, st, timing))) return rc;
-    // dt/2 -> dt: half kick, chains
-    kick_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_v, d_f, pm->d_bmass, n, dt2);
-    PCK(cudaGetLastError());
-    return apply_all_nhc(pm, d_v, st);
+    const int nt = pm->nres[0], no = pm->nres[1], na = pm->nres[2], np = pm->nres[3];
+    const bool respa = nt * no * na * np > 1;
+    const double dti = pm->dt / (double)(nt * no * na * np), dti2 = dti / 2.0;
+    for (int ir_ter = 1; ir_ter <= nt; ir_ter++)
+        for (int ir_tor = 1; ir_tor <= no; ir_tor++)
+            for (int ir_tra = 1; ir_tra <= na; ir_tra++)
+                for (int ir_pimd = 1; ir_pimd <= np; ir_pimd++) {
+                    // t -> t + dti/2: chains at the start of a loop of
+                    // level <= ix_respa, half kick (int_0_to_dt2_pimd.c:~75-145)
+                    int ix = 5;
+                    if (ir_pimd == 1) {
+                        ix = 4;
+                        if (ir_tra == 1) {
+                            ix = 3;
+                            if (ir_tor == 1) ix = ir_ter == 1 ? 1 : 2;
+                        }
+                    }
+                    if (pm->ix_respa >= ix && (rc = apply_all_nhc(pm, d_v, st))) return rc;
+                    kick_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_v, d_f, pm->d_bmass, n, dti2);
+                    PCK(cudaGetLastError());
+                    // positions -> modes (first bead step), drift, springs
+                    if (pm->P > 1 && ir_pimd == 1 &&
+                        (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_MODES, d_x, st)))
+                        return rc;
+                    drift_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_x, d_v, n, dti);
+                    PCK(cudaGetLastError());
+                    PCK(cudaMemsetAsync(pm->d_acc, 0, sizeof(double) * A_N, st));
+                    if ((rc = springs(pm, d_x, st))) return rc;
+                    if (ir_pimd == np) {
+                        // mode 1 -> xmod, modes -> positions, ghosts; the forces
+                        PCK(cudaMemcpyAsync(pm->d_xmod, d_x, sizeof(double) * (size_t)pm->natm * 3,
+                                            cudaMemcpyDeviceToDevice, st));
+                        if (pm->P > 1 &&
+                            (rc = pinyb200_pimd_transform(pm->natm, pm->P, pm->kind, PINYB200_TO_BEADS, d_x, st)))
+                            return rc;
+                        if ((rc = ghost_positions(pm, c, d_x, st))) return rc;
+                        int level = 0;
+                        if (respa) {  // int_NVT_pimd.c:175-189
+                            const bool last_tra = ir_tra == na;
+                            if (ir_ter == nt && ir_tor == no && last_tra) level |= PINYB200_FULL_INTER;
+                            if (c->r_int_res_ter && ir_tor == no && last_tra) level |= PINYB200_RES_INTER;
+                            if (last_tra) level |= PINYB200_FULL_INTRA;
+                            level |= PINYB200_RES_INTRA;
+                        }
+                        // PINY's list test and, when due, the rebuild -- on the device,
+                        // where the level asks for the intermolecular forces
+                        if ((!respa || (level & (PINYB200_FULL_INTER | PINYB200_RES_INTER))) &&
+                            (rc = pinyb200::list_update_enqueue(c, d_x, pm->P > 1 ? pm->d_xmod : nullptr, cell, st)))
+                            return rc;
+                        if ((rc = forces_enqueue(pm, c, d_x, pm->d_xmod, d_f, cell, st, timing && !respa, level)))
+                            return rc;
+                    } else {
+                        // no force call: the spring forces alone (int_NVT_pimd.c:193-207)
+                        PCK(cudaMemcpyAsync(d_f, pm->d_fm, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+                    }
+                    // t + dti/2 -> t + dti: half kick, chains at the end of a
+                    // loop of level <= ix_respa (int_dt2_to_dt_pimd.c)
+                    kick_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_v, d_f, pm->d_bmass, n, dti2);
+                    PCK(cudaGetLastError());
+                    ix = 5;
+                    if (ir_pimd == np) {
+                        ix = 4;
+                        if (ir_tra == na) {
+                            ix = 3;
+                            if (ir_tor == no) ix = ir_ter == nt ? 1 : 2;
+                        }
+                    }
+                    if (pm->ix_respa >= ix && (rc = apply_all_nhc(pm, d_v, st))) return rc;
+                }
+    return PINYB200_OK;
 }
 
 int check_ctx(pinyb200_pimd *pm, pinyb200_ctx *c)
@@ -528,6 +606,8 @@ int check_ctx(pinyb200_pimd *pm, pinyb200_ctx *c)
     if (c->sys.natm != pm->natm || c->P != pm->P)
         return pimd_fail(pm, PINYB200_ERR_ARG, "pimd: force context has other sites or beads");
     if (!c->have_list) return pimd_fail(pm, PINYB200_ERR_STATE, "pimd: build the force context's list first");
+    if (pm->nres[0] * pm->nres[1] * pm->nres[2] * pm->nres[3] > 1 && !c->respa_on)
+        return pimd_fail(pm, PINYB200_ERR_STATE, "pimd: RESPA counts > 1 need pinyb200_set_respa on the force context");
     if (cudaSetDevice(c->device) != cudaSuccess) return pimd_fail(pm, PINYB200_ERR_CUDA, "pimd: cannot select the device");
     return PINYB200_OK;
 }
@@ -554,6 +634,19 @@ int pinyb200_pimd_create(const pinyb200_pimd_setup *s, pinyb200_pimd **out)
     pm->dt = s->dt;
     pm->beta = s->beta;
     pm->nfree = s->nfree_atoms;
+    const int nres[4] = {s->nres_ter, s->nres_tor, s->nres_tra, s->nres_pimd};
+    for (int k = 0; k < 4; k++) {
+        if (nres[k] < 0 || nres[k] > 64) {
+            delete pm;
+            return pimd_fail(nullptr, PINYB200_ERR_ARG, "pimd_create: RESPA counts 0..64");
+        }
+        pm->nres[k] = nres[k] > 0 ? nres[k] : 1;
+    }
+    if (s->ix_respa < 0 || s->ix_respa > 5) {
+        delete pm;
+        return pimd_fail(nullptr, PINYB200_ERR_ARG, "pimd_create: ix_respa 1..5");
+    }
+    pm->ix_respa = s->ix_respa > 0 ? s->ix_respa : 1;
     const size_t na = (size_t)s->natm, nb = na * s->nbeads;
     auto cleanup = [&](int rc) {
         pinyb200_pimd_destroy(pm);
@@ -572,6 +665,7 @@ int pinyb200_pimd_create(const pinyb200_pimd_setup *s, pinyb200_pimd **out)
     CCK(cudaMalloc(&pm->d_u, sizeof(double) * nb * 3));
     CCK(cudaMalloc(&pm->d_xmod, sizeof(double) * na * 3));
     CCK(cudaMalloc(&pm->d_acc, sizeof(double) * A_N));
+    if (pm->nres[0] * pm->nres[1] * pm->nres[2] * pm->nres[3] > 1) CCK(cudaMalloc(&pm->d_ft, sizeof(double) * nb * 3));
     CCK(cudaMallocHost(&pm->h_acc, sizeof(double) * A_N));
     CCK(cudaMallocHost(&pm->h_facc, sizeof(double) * (size_t)s->nbeads * pinyb200::S_NSLOT));
     CCK(cudaMemcpy(pm->d_mass, s->mass, sizeof(double) * na, cudaMemcpyHostToDevice));
@@ -597,6 +691,7 @@ int pinyb200_pimd_destroy(pinyb200_pimd *pm)
     cudaFree(pm->d_u);
     cudaFree(pm->d_xmod);
     cudaFree(pm->d_acc);
+    cudaFree(pm->d_ft);
     cudaFreeHost(pm->h_acc);
     cudaFreeHost(pm->h_facc);
     free_set(pm->set[0]);

@@ -188,12 +188,14 @@ int check_level(pinyb200_ctx *c, int level)
         if (e_ != cudaSuccess) return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e_)); \
     } while (0)
 
+}  // namespace
+
 // One level, enqueued on c->stream; the weighted forces end in c->d_forceW,
 // the outer level's unweighted ones in c->d_forceT (and its per-bead sums
 // are copied to h_acc).  The outer level is the plain evaluation with the
 // weighted buffer formed alongside (evaluate_enqueue); the inner levels run
 // only their own terms.
-int respa_enqueue(pinyb200_ctx *c, const Cell &cell, int level, int flags, double *h_acc)
+int pinyb200::respa_level_enqueue(pinyb200_ctx *c, const Cell &cell, int level, int flags, double *h_acc)
 {
     if (level & PINYB200_FULL_INTER) return evaluate_enqueue(c, cell, flags, false, h_acc, c->d_forceW);
     const size_t nb = (size_t)c->sys.natm * 3 * c->P;
@@ -212,6 +214,8 @@ int respa_enqueue(pinyb200_ctx *c, const Cell &cell, int level, int flags, doubl
     if (flags & PINYB200_DISTRIB_GHOSTS) RK(launch_ghost_distrib(c, c->d_forceW));
     return PINYB200_OK;
 }
+
+namespace {
 
 // The list update's sticky failure flags (a device rebuild that did not fit)
 int check_list_flags(pinyb200_ctx *c)
@@ -308,7 +312,7 @@ int pinyb200_respa_force_device(pinyb200_ctx *c, const double *d_pos, const doub
     std::vector<double> acc(outer ? (size_t)c->P * S_NSLOT : 0);
     int rc = stage_positions(c, d_pos, d_xmod, cell, flags);
     if (rc) return rc;
-    rc = respa_enqueue(c, cell, level, flags, outer ? acc.data() : nullptr);
+    rc = respa_level_enqueue(c, cell, level, flags, outer ? acc.data() : nullptr);
     if (rc) return rc;
     RK(launch_transpose_out(c, d_force, c->d_forceW));
     if (outer && d_forcet) RK(launch_transpose_out(c, d_forcet, c->d_forceT));

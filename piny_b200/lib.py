@@ -77,7 +77,8 @@ class PinyPimdSetup(C.Structure):
     """pinyb200_pimd_setup."""
     _fields_ = [("natm", _i), ("nbeads", _i), ("kind", _i), ("mass", _pd), ("bead_mass", _pd), ("prekf", _pd),
                 ("path_eig", _pd), ("wght_pimd", _d), ("dt", _d), ("beta", _d), ("nfree_atoms", _i),
-                ("class_nhc", PinyNhcSet), ("bead_nhc", PinyNhcSet)]
+                ("class_nhc", PinyNhcSet), ("bead_nhc", PinyNhcSet),
+                ("nres_ter", _i), ("nres_tor", _i), ("nres_tra", _i), ("nres_pimd", _i), ("ix_respa", _i)]
 
 
 class PinyPimdEnergies(C.Structure):
@@ -546,7 +547,8 @@ class DevicePimd:
         st = PinyPimdSetup(self.natm, self.P, int(setup["kind"]), dp(setup["mass"]), dp(setup["bead_mass"]),
                            dp(setup["prekf"]), dp(setup["path_eig"]), float(setup.get("wght_pimd", 1.0)),
                            float(setup["dt"]), float(setup["beta"]), int(setup["nfree_atoms"]),
-                           nhc(self.sets[0]), nhc(self.sets[1]))
+                           nhc(self.sets[0]), nhc(self.sets[1]), *[int(v) for v in setup.get("nres", (1, 1, 1, 1))],
+                           int(setup.get("ix_respa", 1)))
         h = C.c_void_p()
         self._check(self.L.pinyb200_pimd_create(C.byref(st), C.byref(h)), "pinyb200_pimd_create")
         self.h = h

@@ -98,16 +98,26 @@ def massive_chains(natm: int, ghost, temperature: float, first_mass: float, len_
             "inhc": inhc, "mass_nhc": mass_nhc, "gkt": gkt}
 
 
+def nhc_time_step(dt: float, nres=(1, 1, 1, 1), ix_respa: int = 1) -> float:
+    """dt_nhc of the chains for RESPA level ix_respa (int_NVT_pimd.c:96-122):
+    dt divided by the step counts of the levels down to ix_respa."""
+    nt, no, na, np_ = (int(v) for v in nres)
+    div = [1, nt, nt * no, nt * no * na, nt * no * na * np_][int(ix_respa) - 1]
+    return dt / float(div)
+
+
 def nvt_setup(mass, ghost, nbeads: int, kind: int, temperature: float, dt: float, tau_nhc: float,
-              len_nhc: int = 4, nres_nhc: int = 1, nyosh: int = 3, gamma_adb: float = 1.0):
+              len_nhc: int = 4, nres_nhc: int = 1, nyosh: int = 3, gamma_adb: float = 1.0,
+              nres=(1, 1, 1, 1), ix_respa: int = 1):
     """Everything pinyb200_pimd_create takes for one box: the class set
     thermostats bead 1 per coordinate (PINY option 6), the bead set beads
-    2..P (PINY's bead thermostats)."""
+    2..P (PINY's bead thermostats).  nres = (nres_ter, nres_tor, nres_tra,
+    nres_pimd) and ix_respa set PINY's RESPA loops; dt is the outer step."""
     mass = np.asarray(mass, np.float64)
     natm = len(mass)
     ghost = np.zeros(natm, bool) if ghost is None else np.asarray(ghost, bool)
     pis = path_integral_setup(mass, nbeads, kind, temperature, gamma_adb, ghost)
-    w = yoshida_weights(nyosh, dt / nres_nhc)
+    w = yoshida_weights(nyosh, nhc_time_step(dt, nres, ix_respa) / nres_nhc)
     T = float(temperature)
     cls = massive_chains(natm, ghost, T, tau_nhc * tau_nhc * T, len_nhc, nres_nhc, w, False)
     bead = None
@@ -116,4 +126,4 @@ def nvt_setup(mass, ghost, nbeads: int, kind: int, temperature: float, dt: float
         bead = massive_chains(natm, ghost, T, pre / (T * T), len_nhc, nres_nhc, w, True)
     return {"natm": natm, "nbeads": int(nbeads), "kind": int(kind), "mass": mass, **pis, "wght_pimd": 1.0,
             "dt": float(dt), "beta": BOLTZ / T, "temperature": T, "nfree_atoms": int((~ghost).sum()),
-            "class_nhc": cls, "bead_nhc": bead}
+            "class_nhc": cls, "bead_nhc": bead, "nres": tuple(int(v) for v in nres), "ix_respa": int(ix_respa)}

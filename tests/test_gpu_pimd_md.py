@@ -140,3 +140,58 @@ def test_step_arguments():
     bad["class_nhc"] = dict(setup["class_nhc"], len_nhc=9)
     with pytest.raises(PinyError, match="ERR_ARG"):
         DevicePimd(bad)
+
+
+@pytest.mark.parametrize("kind,ix_respa", [(2, 1), (1, 3), (2, 5)])
+def test_device_respa_step_matches_oracle(oracle, kind, ix_respa):
+    """int_NVT_pimd's RESPA loops on the device (counts inter 2, intra 2,
+    switch 1 Bohr below an inner cutoff 1.5 Bohr short of the full one,
+    bonds' RESPA equilibrium 0.01 Bohr longer; chains at the level
+    ix_respa) against the oracle's composition of the pinned pieces and the
+    RESPA force split, over two outer steps (eight inner steps)."""
+    import torch
+
+    from oracle import oracle as O
+    from piny_b200 import pimd, respa
+    from piny_b200.lib import DeviceBox, DevicePimd
+    spec, S, pos, v0, setup, rng = _problem(kind)
+    P = setup["nbeads"]
+    natm = int(S["natm"])
+    nres = (2, 1, 2, 1)
+    ghost = np.zeros(natm, bool)
+    ghost[np.asarray(S["ghost_atom"])] = True
+    setup = pimd.nvt_setup(setup["mass"], ghost, P, kind, spec.temperature, 2 * DT, TAU, len_nhc=3, nres_nhc=1,
+                           nyosh=3, nres=nres, ix_respa=ix_respa)
+    rs = respa.respa_setup(*nres, True, True, np.asarray(S["cutoff"]) - 1.5, 1.0, np.asarray(S["bond_eq"]) + 0.01)
+    state = _chain_state(setup, rng)
+    x0 = O.ghost_positions(S, pos)
+    u0 = oracle.pimd_transform(x0, kind, 0)
+    pi, pj = oracle.verlist(S, x0[0], u0[0], S["hmat"], S["cutskin2"])
+
+    box = DeviceBox(S, P, "fp64")
+    box.build_list(x0[0], u0[0], S["hmat"], S["cutskin2"])
+    box.set_respa(rs)
+    pm = DevicePimd(setup)
+    pm.set_nhc(0, state["cx"], state["cv"])
+    pm.set_nhc(1, state["bx"], state["bv"])
+    dx = torch.from_numpy(pos.copy()).to("cuda:0")
+    dv = torch.from_numpy(v0.copy()).to("cuda:0")
+    df = torch.zeros_like(dx)
+    pm.forces(box, dx.data_ptr(), df.data_ptr(), S["hmat"])
+    x, f = O.pimd_forces(oracle, S, setup, pos, pi, pj)[:2]
+    v = v0.copy()
+    for step in range(2):
+        ed = pm.step(box, dx.data_ptr(), dv.data_ptr(), df.data_ptr(), S["hmat"])
+        x, v, f, eo = O.pimd_step_respa(oracle, S, setup, rs, x, v, f, state, pi, pj)
+        assert _close(dx.cpu().numpy(), x, 1e-13), step
+        assert _close(dv.cpu().numpy(), v, 1e-11), step
+        assert _close(df.cpu().numpy(), f, 1e-11), step
+        assert abs(ed["kin_harm"] - eo["kin_harm"]) <= 1e-11 * abs(eo["kin_harm"])
+        assert abs(ed["akvirx"] - eo["akvirx"]) <= 1e-10 * abs(eo["akvirx"])
+        assert abs(ed["vintert"] - eo["vintert"]) <= 1e-11 * abs(eo["vintert"])
+        cx, cv = pm.get_nhc(0)
+        bx, bv = pm.get_nhc(1)
+        assert _close(cx, state["cx"], 1e-11) and _close(cv, state["cv"], 1e-10)
+        assert _close(bx, state["bx"], 1e-11) and _close(bv, state["bv"], 1e-10)
+    pm.close()
+    box.close()

@@ -65,3 +65,38 @@ def test_respa_loop_levels():
     assert lv == [R.RES_INTRA, inner, R.RES_INTRA, full]
     assert R.loop_levels(1, 1, 1, 3, False) == [0, 0, R.FULL_INTER | R.FULL_INTRA | R.RES_INTRA]
     assert R.loop_levels(1, 1, 2, 2, False) == [0, R.RES_INTRA, 0, R.FULL_INTER | R.FULL_INTRA | R.RES_INTRA]
+
+
+def test_oracle_respa_step_reduces_to_plain(oracle):
+    """The oracle's RESPA step with every count 1 and unit weights is its
+    plain NVT step."""
+    from oracle import oracle as O
+    from piny_b200 import pimd, system, water
+    spec = water.BoxSpec(water.TIP4P_F, 27, water.density_box_edge(27), 4, 298.0, 21, grid=16, order=8,
+                         cutoff=4.5)
+    pos = water.build_positions(spec) / water.BOHR
+    S = system.build_system(spec, pos)
+    natm = int(S["natm"])
+    ghost = np.zeros(natm, bool)
+    ghost[np.asarray(S["ghost_atom"])] = True
+    mass = np.tile(np.asarray(spec.model.masses, np.float64), spec.nmol) * 1822.888486
+    setup = pimd.nvt_setup(mass, ghost, 4, 2, spec.temperature, 20.0, 800.0, len_nhc=3)
+    rs = R.respa_setup(1, 1, 1, 1, True, False, np.asarray(S["cutoff"]), 1.0, np.asarray(S["bond_eq"]))
+    rng = np.random.default_rng(2)
+    v = rng.normal(size=(4, natm, 3)) * 1e-4
+    v[:, ghost, :] = 0.0
+    c, b = setup["class_nhc"], setup["bead_nhc"]
+    st = {"cx": rng.normal(0, 0.05, (c["len_nhc"], c["num_nhc"])), "cv": rng.normal(0, 1e-4, (c["len_nhc"], c["num_nhc"])),
+          "bx": rng.normal(0, 0.05, (3, b["len_nhc"], b["num_nhc"])), "bv": rng.normal(0, 1e-4, (3, b["len_nhc"], b["num_nhc"]))}
+    st2 = {k: a.copy() for k, a in st.items()}
+    x0 = O.ghost_positions(S, pos)
+    u0 = oracle.pimd_transform(x0, 2, 0)
+    pi, pj = oracle.verlist(S, x0[0], u0[0], S["hmat"], S["cutskin2"])
+    x, f = O.pimd_forces(oracle, S, setup, pos, pi, pj)[:2]
+    a = O.pimd_step(oracle, S, setup, x, v, f, st, pi, pj)
+    b2 = O.pimd_step_respa(oracle, S, setup, rs, x, v, f, st2, pi, pj)
+    for k in range(3):
+        assert np.abs(a[k] - b2[k]).max() <= 1e-12 * np.abs(a[k]).max(), k
+    assert abs(a[3]["akvirx"] - b2[3]["akvirx"]) <= 1e-12 * abs(a[3]["akvirx"])
+    for k in st:
+        assert np.abs(st[k] - st2[k]).max() <= 1e-12 * max(np.abs(st[k]).max(), 1e-30), k
