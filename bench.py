@@ -47,7 +47,7 @@ def parse_args():
                          "c5_grad: parameter gradients of 1024 TIP4P/F x 16 beads; "
                          "pimd_nvt: PINY's NVT ring-polymer MD step of 4096 TIP4P/F x 32 beads; "
                          "respa: the force calls of one PINY RESPA step (respa_steps_lrf 2, respa_steps_intra 2) "
-                         "of 4096 TIP4P/F x 32 beads")
+                         "of 4096 TIP4P/F x 32 beads; pimd_nvt_respa: the NVT PIMD step with those RESPA loops")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
@@ -343,8 +343,10 @@ def run_pimd(args, ws, rank, local):
     import torch
 
     from piny_b200 import pimd, system, water
+    from piny_b200 import respa as R
     from piny_b200.lib import NORMAL_MODES, TO_MODES, DeviceBox, DevicePimd, pimd_transform
 
+    use_respa = args.config == "pimd_nvt_respa"
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     spec = water.named_spec("tip4pf_4096_p32")
@@ -357,13 +359,24 @@ def run_pimd(args, ws, rank, local):
     ghost[np.asarray(S["ghost_atom"])] = True
     mass = np.tile(np.asarray(spec.model.masses, np.float64), spec.nmol) * 1822.888486
     dt = 20.0
-    setup = pimd.nvt_setup(mass, ghost, P, NORMAL_MODES, spec.temperature, dt, 800.0, len_nhc=4, nyosh=3)
+    nres = (2, 1, 2, 1) if use_respa else (1, 1, 1, 1)
+    if use_respa:
+        dt = 20.0 * 4  # outer step of four 20 a.u. inner steps
+    # with RESPA the chains run at every inner step (ix_respa 5): the bead
+    # chains of 32 beads (tuned to the ring polymer's frequency) do not stay
+    # stable over the 80 a.u. outer step
+    ix_respa = 5 if use_respa else 1
+    setup = pimd.nvt_setup(mass, ghost, P, NORMAL_MODES, spec.temperature, dt, 800.0, len_nhc=4, nyosh=3, nres=nres,
+                           ix_respa=ix_respa)
     rng = np.random.default_rng(spec.seed)
     v = rng.normal(size=(P, natm, 3)) * np.sqrt(spec.temperature / water.BOLTZ / setup["bead_mass"])[:, :, None]
     v[:, ghost, :] = 0.0
     box = DeviceBox(S, P, args.precision)
     xmod0 = pos.mean(axis=0)
     box.build_list(pos[0], xmod0, S["hmat"], S["cutskin2"])
+    if use_respa:
+        box.set_respa(R.respa_setup(*nres, True, True, np.minimum(np.asarray(S["cutoff"]), 5.0 / water.BOHR),
+                                    1.0 / water.BOHR, np.asarray(S["bond_eq"])))
     pm = DevicePimd(setup)
     stream = torch.cuda.current_stream(dev)
     d_x = torch.from_numpy(pos.copy()).to(dev)
@@ -431,16 +444,25 @@ def run_pimd(args, ws, rank, local):
         ms = float(t.item())
     hbm, peak_kind = peaks()
     if rank == 0:
+        inner = int(np.prod(nres))
         line = {
-            "metric": "PIMD NVT steps/s (TIP4P/F 4096 mol x 32 beads, normal modes)", "value": ws * 1e3 / ms,
+            "metric": ("PIMD NVT RESPA steps/s (TIP4P/F 4096 mol x 32 beads, normal modes, 4 inner steps)"
+                       if use_respa else "PIMD NVT steps/s (TIP4P/F 4096 mol x 32 beads, normal modes)"),
+            "value": ws * 1e3 / ms,
             "unit": "MD steps/s", "n_gpus": ws, "steps": args.steps, "warmup": max(3, args.warmup),
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 (step) + " + ("f32+f64acc" if args.precision == "mixed" else "f64") + " (forces)",
             "data": "synthetic",
-            "config": {"workload": "pimd_nvt", "molecules": spec.nmol, "beads": P, "dt_au": dt,
+            "config": {"workload": args.config, "molecules": spec.nmol, "beads": P, "dt_au": dt,
+                       "respa": {"nres_ter_tor_tra_pimd": list(nres), "ix_respa": ix_respa, "cutoff_res_A": 5.0,
+                                 "rheal_A": 1.0, "inner_dt_au": dt / inner,
+                                 "inner_steps_per_s": ws * inner * 1e3 / ms} if use_respa else None,
                        "chains": "4 links on every coordinate, 3 Yoshida stages", "pme_grid": spec.grid,
-                       "bead_force_evals_per_s": ws * P * 1e3 / ms, "force_ms_per_step": float(np.mean(force_ms)),
-                       "pimd_bookkeeping_ms_per_step": ms - float(np.mean(force_ms)), "list_rebuilds_incl_warmup": rebuilds,
+                       "plain_force_evaluation_ms": float(np.mean(force_ms)),
+                       **({} if use_respa else {
+                           "bead_force_evals_per_s": ws * P * 1e3 / ms, "force_ms_per_step": float(np.mean(force_ms)),
+                           "pimd_bookkeeping_ms_per_step": ms - float(np.mean(force_ms))}),
+                       "list_rebuilds_incl_warmup": rebuilds,
                        "step_ms_median": float(np.median(ms_list)), "step_ms_max": float(np.max(ms_list)),
                        "energies_last_step": {k: e[k] for k in ("vintert", "vintrat", "kin_harm", "akvirx")},
                        "l2": "256 MiB buffer written between timed steps; CUDA events on the launch stream"},
@@ -734,7 +756,7 @@ def main():
         return run_batch(args, ws, rank, local)
     if args.config == "c5_grad":
         return run_grad(args, ws, rank, local)
-    if args.config == "pimd_nvt":
+    if args.config in ("pimd_nvt", "pimd_nvt_respa"):
         return run_pimd(args, ws, rank, local)
     if args.config == "respa":
         return run_respa(args, ws, rank, local)
