@@ -48,6 +48,7 @@ struct NhcDev {
     double *mass = nullptr, *gkt = nullptr;  // [len][num]
     double *x = nullptr, *v = nullptr;       // [nb][len][num]
     double *kin = nullptr, *sc = nullptr;    // [nb][num + 1]
+    int *coord = nullptr;  // massive sets (one coordinate per chain): chain -> 3 i + d
 };
 
 struct ChainArgs {
@@ -71,14 +72,13 @@ __global__ void nhc_kin_kernel(const double *__restrict__ v, int nb, int natm, c
     atomicAdd(&kin[(size_t)b * (num + 1) + inhc[d * natm + i]], e);
 }
 
-// One thread per chain; LEN links known at compile time, so the chain stays
+// The chain operator of one chain (apply_NHC_par, int_NVT.c:144-353)
+// on the chain's kinetic energy kin: updates the chain's x and v and returns
+// the velocity scale.  LEN links known at compile time, so the chain stays
 // in registers.
 template <int LEN>
-__global__ void __launch_bounds__(128, 6) nhc_chain_kernel(ChainArgs a)
+__device__ __forceinline__ double chain_run(const ChainArgs &a, int b, int k, double kin)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)a.nb * a.num) return;
-    const int b = (int)(t / a.num), k = (int)(t - (long long)b * a.num);
     const int num = a.num;
     constexpr int L = LEN - 1;
     double *x = a.x + (size_t)b * LEN * num + k;
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(128, 6) nhc_chain_kernel(ChainArgs a)
         ms[c] = a.mass[(size_t)c * num + k];
         gk[c] = a.gkt[(size_t)c * num + k];
     }
-    double kin = a.kin[(size_t)b * (num + 1) + k], sc = 1.0;
+    double sc = 1.0;
     f[0] = (kin - gk[0]) / ms[0];
 #pragma unroll
     for (int c = 0; c < L; c++) f[c + 1] = (ms[c] * vn[c] * vn[c] - gk[c + 1]) / ms[c + 1];
@@ -127,8 +127,39 @@ __global__ void __launch_bounds__(128, 6) nhc_chain_kernel(ChainArgs a)
         x[(size_t)c * num] = xs[c];
         v[(size_t)c * num] = vn[c];
     }
-    a.sc[(size_t)b * (num + 1) + k] = sc;
-    if (k == 0) a.sc[(size_t)b * (num + 1) + num] = 1.0;  // null chain
+    return sc;
+}
+
+// One thread per chain, kinetic energies summed beforehand (nhc_kin_kernel).
+template <int LEN>
+__global__ void __launch_bounds__(128, 6) nhc_chain_kernel(ChainArgs a)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)a.nb * a.num) return;
+    const int b = (int)(t / a.num), k = (int)(t - (long long)b * a.num);
+    const double sc = chain_run<LEN>(a, b, k, a.kin[(size_t)b * (a.num + 1) + k]);
+    a.sc[(size_t)b * (a.num + 1) + k] = sc;
+    if (k == 0) a.sc[(size_t)b * (a.num + 1) + a.num] = 1.0;  // null chain
+}
+
+// Massive sets (every chain thermostats one coordinate, as PINY's bead and
+// option-6 class thermostats): kinetic energy, chain and velocity scaling in
+// one thread per chain, with the operations of the three-kernel path (the
+// kinetic energy m v v of the one coordinate, v x scale).
+template <int LEN>
+__global__ void __launch_bounds__(128, 6) nhc_massive_kernel(ChainArgs a, double *__restrict__ v0, int natm,
+                                                             const double *__restrict__ m, size_t m_stride,
+                                                             const int *__restrict__ coord)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)a.nb * a.num) return;
+    const int b = (int)(t / a.num), k = (int)(t - (long long)b * a.num);
+    const int r = coord[k];
+    double *vp = v0 + (size_t)b * natm * 3 + r;
+    const double vv = *vp;
+    const double kin = __dmul_rn(__dmul_rn(m[(size_t)b * m_stride + r / 3], vv), vv);
+    const double sc = chain_run<LEN>(a, b, k, kin);
+    *vp = vv * sc;
 }
 
 __global__ void nhc_scale_kernel(double *__restrict__ v, int nb, int natm, const int *__restrict__ inhc,
@@ -324,6 +355,7 @@ void free_set(NhcDev &s)
     cudaFree(s.v);
     cudaFree(s.kin);
     cudaFree(s.sc);
+    cudaFree(s.coord);
     s = NhcDev();
 }
 
@@ -357,6 +389,21 @@ int upload_set(pinyb200_pimd *pm, NhcDev &s, const pinyb200_nhc_set &h, int nb)
     PCK(cudaMemcpy(s.gkt, h.gkt, sizeof(double) * tab, cudaMemcpyHostToDevice));
     PCK(cudaMemset(s.x, 0, sizeof(double) * st));
     PCK(cudaMemset(s.v, 0, sizeof(double) * st));
+    // one coordinate per chain: the fused chain kernel applies
+    std::vector<int> coord(s.num, -1);
+    bool massive = true;
+    for (int d = 0; d < 3 && massive; d++)
+        for (int i = 0; i < pm->natm && massive; i++) {
+            const int k = h.inhc[d * pm->natm + i];
+            if (k == s.num) continue;  // the null chain
+            if (coord[k] >= 0) massive = false;
+            else coord[k] = 3 * i + d;
+        }
+    for (int k = 0; k < s.num && massive; k++) massive = coord[k] >= 0;
+    if (massive) {
+        PCK(cudaMalloc(&s.coord, sizeof(int) * (size_t)s.num));
+        PCK(cudaMemcpy(s.coord, coord.data(), sizeof(int) * (size_t)s.num, cudaMemcpyHostToDevice));
+    }
     return PINYB200_OK;
 }
 
@@ -368,8 +415,10 @@ int apply_nhc(pinyb200_pimd *pm, NhcDev &s, double *d_v, int bead0, const double
     if (s.num == 0 || s.nb == 0) return PINYB200_OK;
     const long long n = (long long)pm->natm * 3 * s.nb;
     double *v = d_v + (size_t)bead0 * pm->natm * 3;
-    PCK(cudaMemsetAsync(s.kin, 0, sizeof(double) * (size_t)s.nb * (s.num + 1), st));
-    nhc_kin_kernel<<<blocks_for(n, 256), 256, 0, st>>>(v, s.nb, pm->natm, m, m_stride, s.inhc, s.kin, s.num);
+    if (!s.coord) {
+        PCK(cudaMemsetAsync(s.kin, 0, sizeof(double) * (size_t)s.nb * (s.num + 1), st));
+        nhc_kin_kernel<<<blocks_for(n, 256), 256, 0, st>>>(v, s.nb, pm->natm, m, m_stride, s.inhc, s.kin, s.num);
+    }
     ChainArgs a;
     a.num = s.num;
     a.len = s.len;
@@ -384,6 +433,20 @@ int apply_nhc(pinyb200_pimd *pm, NhcDev &s, double *d_v, int bead0, const double
     a.kin = s.kin;
     a.sc = s.sc;
     const unsigned nbk = blocks_for((long long)s.nb * s.num, 128);
+    if (s.coord) {
+        switch (s.len) {
+        case 1: nhc_massive_kernel<1><<<nbk, 128, 0, st>>>(a, v, pm->natm, m, m_stride, s.coord); break;
+        case 2: nhc_massive_kernel<2><<<nbk, 128, 0, st>>>(a, v, pm->natm, m, m_stride, s.coord); break;
+        case 3: nhc_massive_kernel<3><<<nbk, 128, 0, st>>>(a, v, pm->natm, m, m_stride, s.coord); break;
+        case 4: nhc_massive_kernel<4><<<nbk, 128, 0, st>>>(a, v, pm->natm, m, m_stride, s.coord); break;
+        case 5: nhc_massive_kernel<5><<<nbk, 128, 0, st>>>(a, v, pm->natm, m, m_stride, s.coord); break;
+        case 6: nhc_massive_kernel<6><<<nbk, 128, 0, st>>>(a, v, pm->natm, m, m_stride, s.coord); break;
+        case 7: nhc_massive_kernel<7><<<nbk, 128, 0, st>>>(a, v, pm->natm, m, m_stride, s.coord); break;
+        default: nhc_massive_kernel<8><<<nbk, 128, 0, st>>>(a, v, pm->natm, m, m_stride, s.coord); break;
+        }
+        PCK(cudaGetLastError());
+        return PINYB200_OK;
+    }
     switch (s.len) {
     case 1: nhc_chain_kernel<1><<<nbk, 128, 0, st>>>(a); break;
     case 2: nhc_chain_kernel<2><<<nbk, 128, 0, st>>>(a); break;
