@@ -182,6 +182,19 @@ def test_piny_layout_calls():
     assert rel_rms(got, want) < 1e-12
     gt = np.stack([np.stack([Ft[d][0][b][1:] for b in range(P)]) for d in range(3)], axis=-1)
     assert rel_rms(gt, F["ref_L0_forcet_raw"]) < 1e-12
+    # an inner level adds its weighted forces and leaves the virial forces
+    for d in range(3):
+        for b in range(P):
+            Fa[d][0][b][:] = 0.0
+    before = [[Ft[d][0][b].copy() for b in range(P)] for d in range(3)]
+    rc = box.L.pinyb200_piny_force_respa(box.h, fixture_level(F, 1), X[0], X[1], X[2],
+                                          *[a.ctypes.data_as(dp) for a in xm], h1.ctypes.data_as(dp),
+                                          Fa[0][1], Fa[1][1], Fa[2][1], Ft[0][1], Ft[1][1], Ft[2][1],
+                                          None, C.byref(e))
+    assert rc == 0
+    got = np.stack([np.stack([Fa[d][0][b][1:] for b in range(P)]) for d in range(3)], axis=-1)
+    assert rel_rms(got, F["ref_L1_force_raw"]) < 1e-12
+    assert all(np.array_equal(Ft[d][0][b], before[d][b]) for d in range(3) for b in range(P))
     # plain PINY-layout call: the unweighted forces, added to zeros
     for d in range(3):
         for b in range(P):
