@@ -300,8 +300,9 @@ int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
  * pinyb200_respa_force_device evaluates one level, `level` being the OR of
  * the PINYB200_* flag bits below that PINY has set: one of
  *   RES_INTRA; FULL_INTRA|RES_INTRA; RES_INTER|FULL_INTRA|RES_INTRA (needs
- *   int_res_ter); FULL_INTER|FULL_INTRA|RES_INTRA, with RES_INTER exactly
- *   when int_res_ter (the levels int_NVT_pimd's loops produce).
+ *   int_res_ter); FULL_INTER|FULL_INTRA with or without RES_INTRA, with
+ *   RES_INTER exactly when int_res_ter (the levels int_NVT_pimd's loops
+ *   and control_pimd's first force call produce).
  * d_force receives PINY's weighted forces fx: real-space pairs x the RESPA
  * multiplier (inner levels shave at cutoff_res; force_npol.c:805-816,
  * :1030-1060), PME and the exclusion correction x wght_ter at the outer
@@ -582,8 +583,10 @@ int pinyb200_pimd_get_nhc(pinyb200_pimd *pm, int set, double *x_nhc, double *v_n
  * the modes (mode_energy_control, pimd_estimators.c:31), the force path
  * with the mode-1 image positions, and the post-processing of
  * energy_control_pimd.c:113-218 (bead forces / P, centroid virial
- * correction, forces to modes, springs added) into d_f.  Ghost positions in
- * d_x are recomputed (get_ghost_pos).  Work goes to `stream` (NULL: the
+ * correction, forces to modes, springs added) into d_f.  With RESPA counts
+ * above 1 the force path is asked for the outer level, as PINY's first
+ * force call is (control_pimd.c:297-317).  Ghost positions in d_x are
+ * recomputed (get_ghost_pos).  Work goes to `stream` (NULL: the
  * force context's own stream); the call blocks until it is done. */
 int pinyb200_pimd_forces(pinyb200_pimd *pm, pinyb200_ctx *ctx, double *d_x, double *d_f,
                          const double *hmat, pinyb200_pimd_energies *e, void *stream);

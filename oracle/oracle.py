@@ -419,6 +419,26 @@ def pimd_force_post_respa(orc, kind, f, ft, x, xmod, fm, nfree, beta, full, pvte
     return f, akv, pv, pvt
 
 
+def pimd_forces_respa(orc, sysd, setup, respa, x, pi, pj):
+    """pinyb200_pimd_forces with RESPA counts > 1: the outer level, as
+    PINY's first force call (control_pimd.c:297-317).  Returns (x with
+    ghosts, mode forces, energies)."""
+    P, kind = int(setup["nbeads"]), int(setup["kind"])
+    x = ghost_positions(sysd, x)
+    u = orc.pimd_transform(x, kind, 0) if P > 1 else x.copy()
+    xmod = u[0].copy()
+    fm, ake, pvm = pimd_springs(orc, u, setup["prekf"], setup["path_eig"], setup.get("wght_pimd", 1.0))
+    level = 1 | 4 | 8 | (2 if respa["int_res_ter"] else 0)
+    fw, ft = orc.respa_force(sysd, respa, level, x, xmod if P > 1 else None, sysd["hmat"], pi, pj,
+                             distribute_ghosts=True)
+    _, ef = orc.energy_force(sysd, x, xmod if P > 1 else None, sysd["hmat"], pi, pj, distribute_ghosts=True)
+    f, akv, pv, pvt = pimd_force_post_respa(orc, kind, fw, ft, x, xmod, fm, setup["nfree_atoms"], setup["beta"],
+                                            True, ef["pvten"], ef["pvten"])
+    e = dict(ef)
+    e.update(kin_harm=ake, akvirx=akv if P > 1 else 0.0, pvten_tot_corr=pvt, pvten_mode_tot=pvm)
+    return x, f, e
+
+
 def pimd_step_respa(orc, sysd, setup, respa, x, v, f, state, pi, pj):
     """pinyb200_pimd_step with RESPA counts setup["nres"] = (nres_ter,
     nres_tor, nres_tra, nres_pimd) and chains at level setup["ix_respa"]:

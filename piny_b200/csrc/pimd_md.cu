@@ -329,6 +329,7 @@ struct pinyb200_pimd {
     int nres[4] = {1, 1, 1, 1};  // RESPA counts: inter, torsion, intra, bead
     int ix_respa = 1;            // chains at the inner steps of loops of level <= ix_respa
     double *d_ft = nullptr;      // [P][natm][3] virial forces of the outer RESPA level
+    bool timed = false;          // this call recorded the force path's phase events
     std::string err;
 };
 
@@ -497,6 +498,7 @@ int forces_enqueue(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, const double
     if (level == 0) {
         rc = pinyb200::enqueue_device(c, d_x, pm->P > 1 ? d_xmod : nullptr, cell, PINYB200_DISTRIB_GHOSTS, d_f,
                                       timing, pm->h_facc);
+        pm->timed = pm->timed || timing;
         c->stream = own;
         if (rc) return rc;
         post_kernel<<<blocks_for(nb, 256), 256, 0, st>>>(d_f, d_x, d_xmod, pm->natm, pm->P, pm->P > 1, pm->d_acc);
@@ -535,7 +537,7 @@ int pimd_finish(pinyb200_pimd *pm, pinyb200_ctx *c, const pinyb200::Cell &cell, 
                 cudaStream_t st)
 {
     PCK(cudaStreamSynchronize(st));
-    if (!pm->graph_mode) {  // a replayed graph records no phase events
+    if (!pm->graph_mode && pm->timed) {  // a replayed graph (or a RESPA step) records no phase events
         cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]);
         cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]);
         cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]);
@@ -793,6 +795,7 @@ int pinyb200_pimd_forces(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double
     int rc = check_ctx(pm, c);
     if (rc) return rc;
     if (!d_x || !d_f || !hmat) return pimd_fail(pm, PINYB200_ERR_ARG, "pimd_forces: null pointer");
+    pm->timed = false;
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;  // NULL: the force context's stream
     const size_t nbytes = sizeof(double) * (size_t)pm->natm * pm->P * 3;
     if ((rc = ghost_positions(pm, c, d_x, st))) return rc;
@@ -802,7 +805,12 @@ int pinyb200_pimd_forces(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double
     PCK(cudaMemsetAsync(pm->d_acc, 0, sizeof(double) * A_N, st));
     if ((rc = springs(pm, pm->d_u, st))) return rc;
     const pinyb200::Cell cell = pinyb200::cell_from_hmat(hmat);
-    if ((rc = forces_enqueue(pm, c, d_x, pm->d_u, d_f, cell, st, true))) return rc;
+    // with RESPA, the outer level (control_pimd.c:297-317)
+    const int level = pm->nres[0] * pm->nres[1] * pm->nres[2] * pm->nres[3] > 1
+                          ? PINYB200_FULL_INTER | PINYB200_FULL_INTRA | PINYB200_RES_INTRA |
+                                (c->r_int_res_ter ? PINYB200_RES_INTER : 0)
+                          : 0;
+    if ((rc = forces_enqueue(pm, c, d_x, pm->d_u, d_f, cell, st, level == 0, level))) return rc;
     pm->graph_mode = false;
     return pimd_finish(pm, c, cell, e, st);
 }
@@ -813,6 +821,7 @@ int pinyb200_pimd_step(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double *
     int rc = check_ctx(pm, c);
     if (rc) return rc;
     if (!d_x || !d_v || !d_f || !hmat) return pimd_fail(pm, PINYB200_ERR_ARG, "pimd_step: null pointer");
+    pm->timed = false;
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;  // NULL: the force context's stream
     const pinyb200::Cell cell = pinyb200::cell_from_hmat(hmat);
     // Steps with the same arguments replay one CUDA graph: the first such

@@ -172,9 +172,12 @@ namespace {
 int check_level(pinyb200_ctx *c, int level)
 {
     const int intra = PINYB200_FULL_INTRA | PINYB200_RES_INTRA;
+    const int outer = PINYB200_FULL_INTER | PINYB200_FULL_INTRA | (c->r_int_res_ter ? PINYB200_RES_INTER : 0);
+    // the outer level with or without RES_INTRA: PINY's first call sets it
+    // only with intra RESPA (control_pimd.c:297-306); the forces agree
     const bool ok = level == PINYB200_RES_INTRA || level == intra ||
-                    (level == (PINYB200_RES_INTER | intra) && c->r_int_res_ter) ||
-                    level == (PINYB200_FULL_INTER | intra | (c->r_int_res_ter ? PINYB200_RES_INTER : 0));
+                    (level == (PINYB200_RES_INTER | intra) && c->r_int_res_ter) || level == outer ||
+                    level == (outer | PINYB200_RES_INTRA);
     if (ok) return PINYB200_OK;
     return record_error(c, PINYB200_ERR_ARG,
                         "respa_force: level " + std::to_string(level) +

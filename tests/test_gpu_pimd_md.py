@@ -178,7 +178,8 @@ def test_device_respa_step_matches_oracle(oracle, kind, ix_respa):
     dv = torch.from_numpy(v0.copy()).to("cuda:0")
     df = torch.zeros_like(dx)
     pm.forces(box, dx.data_ptr(), df.data_ptr(), S["hmat"])
-    x, f = O.pimd_forces(oracle, S, setup, pos, pi, pj)[:2]
+    x, f = O.pimd_forces_respa(oracle, S, setup, rs, pos, pi, pj)[:2]
+    assert _close(df.cpu().numpy(), f, 1e-11)  # PINY's first call: the outer level
     v = v0.copy()
     for step in range(2):
         ed = pm.step(box, dx.data_ptr(), dv.data_ptr(), df.data_ptr(), S["hmat"])

@@ -123,6 +123,12 @@ def test_respa_arguments():
     for lv in (R.FULL_INTER, R.RES_INTER, R.FULL_INTER | R.FULL_INTRA | R.RES_INTRA):
         with pytest.raises(PinyError, match="ERR_ARG"):
             box.respa_force_device(d_pos.data_ptr(), None, F["hmat"], lv, f.data_ptr())
+    # PINY's first call sets RES_INTRA only with intra RESPA: same forces
+    f2 = torch.zeros_like(d_pos)
+    box.respa_force_device(d_pos.data_ptr(), None, F["hmat"], R.FULL_INTER | R.RES_INTER | R.FULL_INTRA, f.data_ptr())
+    box.respa_force_device(d_pos.data_ptr(), None, F["hmat"], R.FULL_INTER | R.RES_INTER | R.FULL_INTRA | R.RES_INTRA,
+                           f2.data_ptr())
+    assert rel_rms(f.cpu().numpy(), f2.cpu().numpy()) < 1e-13  # up to the atomics' summation order
     box.set_respa(dict(rs, int_res_ter=0))
     with pytest.raises(PinyError, match="ERR_ARG"):
         box.respa_force_device(d_pos.data_ptr(), None, F["hmat"], R.RES_INTER | R.FULL_INTRA | R.RES_INTRA,
