@@ -142,13 +142,14 @@ def test_step_arguments():
         DevicePimd(bad)
 
 
-@pytest.mark.parametrize("kind,ix_respa", [(2, 1), (1, 3), (2, 5)])
-def test_device_respa_step_matches_oracle(oracle, kind, ix_respa):
-    """int_NVT_pimd's RESPA loops on the device (counts inter 2, intra 2,
-    switch 1 Bohr below an inner cutoff 1.5 Bohr short of the full one,
-    bonds' RESPA equilibrium 0.01 Bohr longer; chains at the level
-    ix_respa) against the oracle's composition of the pinned pieces and the
-    RESPA force split, over two outer steps (eight inner steps)."""
+@pytest.mark.parametrize("kind,ix_respa,nres", [(2, 1, (2, 1, 2, 1)), (1, 3, (2, 1, 2, 1)), (2, 5, (2, 1, 2, 1)),
+                                               (2, 5, (1, 1, 1, 2)), (1, 4, (2, 1, 1, 2))])
+def test_device_respa_step_matches_oracle(oracle, kind, ix_respa, nres):
+    """int_NVT_pimd's RESPA loops on the device (inter, intra and bead
+    counts as given; switch 1 Bohr below an inner cutoff 1.5 Bohr short of
+    the full one, bonds' RESPA equilibrium 0.01 Bohr longer; chains at the
+    level ix_respa) against the oracle's composition of the pinned pieces
+    and the RESPA force split, over two outer steps."""
     import torch
 
     from oracle import oracle as O
@@ -157,12 +158,12 @@ def test_device_respa_step_matches_oracle(oracle, kind, ix_respa):
     spec, S, pos, v0, setup, rng = _problem(kind)
     P = setup["nbeads"]
     natm = int(S["natm"])
-    nres = (2, 1, 2, 1)
     ghost = np.zeros(natm, bool)
     ghost[np.asarray(S["ghost_atom"])] = True
-    setup = pimd.nvt_setup(setup["mass"], ghost, P, kind, spec.temperature, 2 * DT, TAU, len_nhc=3, nres_nhc=1,
-                           nyosh=3, nres=nres, ix_respa=ix_respa)
-    rs = respa.respa_setup(*nres, True, True, np.asarray(S["cutoff"]) - 1.5, 1.0, np.asarray(S["bond_eq"]) + 0.01)
+    setup = pimd.nvt_setup(setup["mass"], ghost, P, kind, spec.temperature, DT * int(np.prod(nres)) / 2, TAU,
+                           len_nhc=3, nres_nhc=1, nyosh=3, nres=nres, ix_respa=ix_respa)
+    rs = respa.respa_setup(*nres, True, nres[0] > 1, np.asarray(S["cutoff"]) - 1.5, 1.0,
+                           np.asarray(S["bond_eq"]) + 0.01)
     state = _chain_state(setup, rng)
     x0 = O.ghost_positions(S, pos)
     u0 = oracle.pimd_transform(x0, kind, 0)
