@@ -197,3 +197,39 @@ def test_device_respa_step_matches_oracle(oracle, kind, ix_respa, nres):
         assert _close(bx, state["bx"], 1e-11) and _close(bv, state["bv"], 1e-10)
     pm.close()
     box.close()
+
+
+def test_mixed_respa_step_tracks_fp64():
+    """One RESPA step (counts 2, 1, 2, 1) with MIXED forces against FP64:
+    mode forces within 1e-5 (relative RMS), positions within 1e-9."""
+    import torch
+
+    from oracle import oracle as O
+    from piny_b200 import pimd, respa
+    from piny_b200.lib import DeviceBox, DevicePimd
+    spec, S, pos, v0, setup, rng = _problem(2)
+    P, natm = setup["nbeads"], int(S["natm"])
+    nres = (2, 1, 2, 1)
+    ghost = np.zeros(natm, bool)
+    ghost[np.asarray(S["ghost_atom"])] = True
+    setup = pimd.nvt_setup(setup["mass"], ghost, P, 2, spec.temperature, 2 * DT, TAU, len_nhc=3, nres=nres,
+                           ix_respa=5)
+    rs = respa.respa_setup(*nres, True, True, np.asarray(S["cutoff"]) - 1.5, 1.0, np.asarray(S["bond_eq"]))
+    out = {}
+    for prec in ("fp64", "mixed"):
+        box = DeviceBox(S, P, prec)
+        x0 = O.ghost_positions(S, pos)
+        box.build_list(x0[0], x0.mean(axis=0), S["hmat"], S["cutskin2"])
+        box.set_respa(rs)
+        pm = DevicePimd(setup)
+        dx = torch.from_numpy(pos.copy()).to("cuda:0")
+        dv = torch.from_numpy(v0.copy()).to("cuda:0")
+        df = torch.zeros_like(dx)
+        pm.forces(box, dx.data_ptr(), df.data_ptr(), S["hmat"])
+        pm.step(box, dx.data_ptr(), dv.data_ptr(), df.data_ptr(), S["hmat"])
+        out[prec] = (df.cpu().numpy(), dx.cpu().numpy())
+        pm.close()
+        box.close()
+    f64, f32 = out["fp64"][0], out["mixed"][0]
+    assert np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()) <= 1e-5
+    assert np.abs(out["mixed"][1] - out["fp64"][1]).max() <= 1e-9 * np.abs(out["fp64"][1]).max()
