@@ -210,7 +210,8 @@ int pinyb200_list_info(pinyb200_ctx *ctx, long *npairs, long *nactive,
  *   stream         : opaque CUDA stream handle, NULL = the context's stream;
  *                    the call returns after that stream is idle.
  * It calls no cudaMalloc/cudaFree: its scratch is one fixed device array per
- * GPU (about 1 MiB) inside the library, so
+ * GPU inside the library (4096 B + 8 B per atom of the limit: 528,384 B,
+ * about 0.5 MiB), so
  *   - it accepts natm <= PINYB200_COUNT_MAX_ATOMS and at most
  *     PINYB200_COUNT_MAX_PAIR_TYPES pair types (ntyp(ntyp+1)/2), and returns
  *     PINYB200_ERR_ARG beyond them;

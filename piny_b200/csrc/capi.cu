@@ -228,7 +228,7 @@ int pinyb200_destroy(pinyb200_ctx *c)
                     c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf, c->d_x0, c->d_forceP,
                     c->d_pme_head, c->d_pme_w, c->d_nchunk, c->d_ls, c->d_cs, c->d_mchunk, c->d_mmaskf,
                     c->d_reach, c->d_cut_res, c->d_bond_eq_res, c->d_forceW, c->d_forcet_aos, c->d_rowR,
-                    c->d_colR, c->d_rtot, c->d_xm0, c->d_cs0, c->d_ecor_res_tab};
+                    c->d_colR, c->d_rtot, c->d_xm0, c->d_cs0, c->d_ecor_res_tab, c->d_cs_in};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->h_acc_pin) cudaFreeHost(c->h_acc_pin);
@@ -447,6 +447,7 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
     CK(cudaMalloc(&c->d_rowA, (size_t)(natm + 1) * sizeof(int)));
     CK(cudaMalloc(&c->d_count, (size_t)2 * natm * sizeof(int)));
     CK(cudaMalloc(&c->d_tot, 8 * sizeof(long long)));  // list totals [4], chunk total, spare
+    CK(cudaMalloc(&c->d_cs_in, (size_t)d.npair_typ * sizeof(double)));
     // molecules: connected components of the exclusion graph, each a run of
     // at most 4 consecutive sites (water); otherwise the site kernel is used
     {
@@ -519,12 +520,7 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
         CK(cudaMemcpyAsync(c->d_xmod, xmod, (size_t)natm * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         d_xm = c->d_xmod;
     }
-    double *d_cs = nullptr;
-    CK(cudaMalloc(&d_cs, c->sys.npair_typ * sizeof(double)));
-    struct FreeCs {
-        double *p;
-        ~FreeCs() { cudaFree(p); }
-    } free_cs{d_cs};
+    double *d_cs = c->d_cs_in;  // reserved at creation: no allocation per build
     CK(cudaMemcpyAsync(d_cs, cutskin2, c->sys.npair_typ * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     // grow like ver_list_mem_check (verlist_control.c:87-110), with slack
     // for lists that grow between host builds (device updates)

@@ -224,6 +224,7 @@ struct pinyb200_ctx {
     long long *d_rtot = nullptr;      // [2] RESPA list totals
     double *d_xm0 = nullptr;          // [natm][3] mode-1 positions at the last list build
     double *d_cs0 = nullptr;          // [npair_typ] cutskin^2 of the last list build
+    double *d_cs_in = nullptr;        // [npair_typ] cutskin^2 passed to the current host list build
     pinyb200::Cell build_cell{};      // cell of the last host list build
     bool build_cell_ok = false;
     pinyb200::GradHost grad;      // tangent channels of pinyb200_grad_prepare

@@ -805,9 +805,13 @@ int pinyb200_pimd_forces(pinyb200_pimd *pm, pinyb200_ctx *c, double *d_x, double
     PCK(cudaMemsetAsync(pm->d_acc, 0, sizeof(double) * A_N, st));
     if ((rc = springs(pm, pm->d_u, st))) return rc;
     const pinyb200::Cell cell = pinyb200::cell_from_hmat(hmat);
-    // with RESPA, the outer level (control_pimd.c:297-317)
+    // with RESPA, the outer level (control_pimd.c:297-317): RES_INTER with
+    // inter RESPA, RES_INTRA with intra RESPA (PINY's int_res_tra, set by
+    // respa_steps_intra, set_sim_params.c:1626-1637).  Beside FULL_INTRA the
+    // RES_INTRA bit changes only PINY's RESPA pressure guesses in pvten
+    // (energy_control_inter_real.c:270-279), not the forces or pvten_tot.
     const int level = pm->nres[0] * pm->nres[1] * pm->nres[2] * pm->nres[3] > 1
-                          ? PINYB200_FULL_INTER | PINYB200_FULL_INTRA | PINYB200_RES_INTRA |
+                          ? PINYB200_FULL_INTER | PINYB200_FULL_INTRA | (pm->nres[2] > 1 ? PINYB200_RES_INTRA : 0) |
                                 (c->r_int_res_ter ? PINYB200_RES_INTER : 0)
                           : 0;
     if ((rc = forces_enqueue(pm, c, d_x, pm->d_u, d_f, cell, st, level == 0, level))) return rc;

@@ -4,8 +4,8 @@ Builds, from a :class:`piny_b200.water.BoxSpec` and bead positions, every
 table PINY's input stage builds for its force routines, as plain numpy arrays
 in PINY internal units (Bohr, Hartree), 0-based.  The dict keys are the
 field names of ``pinyb200_system`` in include/pinyb200.h.  A PINY host fills
-the same structure straight from its CLASS/BONDED/GENERAL_DATA instead (the
-binding is shown in INTEGRATION.md); this module is the standalone path.
+the same structure straight from its CLASS/BONDED/GENERAL_DATA instead; this
+module is the standalone path.
 
 Each step cites the PINY set-up routine whose arithmetic it restates.
 """

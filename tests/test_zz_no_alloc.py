@@ -78,6 +78,47 @@ def test_count_rejects_sizes_beyond_the_scratch():
     box = DeviceBox(S, 1, "fp64")
     d = torch.from_numpy(np.ascontiguousarray(pos[0])).to("cuda:0")
     torch.cuda.synchronize()
-    with pytest.raises(PinyError, match="PINYB200_COUNT_MAX_ATOMS"):
+    with pytest.raises(PinyError, match=r"count_list_device: ERR_ARG .*PINYB200_COUNT_MAX_ATOMS"):
         box.count_list_device(d.data_ptr(), None, S["hmat"], S["cutskin2"])
+    box.close()
+
+
+def _split_types(F, per_kind=6):
+    """The same box with every atom type split into ``per_kind`` types
+    (molecule index mod per_kind): the pair set is unchanged, the number of
+    pair types ntyp(ntyp+1)/2 grows past the count's fixed limit."""
+    from piny_b200.system import _pair_index
+
+    nt0 = int(F["ntyp"])
+    nt = nt0 * per_kind
+    old = np.repeat(np.arange(nt0), per_kind)          # old type of each new type
+    typ0 = np.asarray(F["atm_typ"])
+    mol = np.arange(len(typ0)) // 3
+    typ = (typ0 * per_kind + mol % per_kind).astype(np.int32)
+    npt = nt * (nt + 1) // 2
+    imap, cut, cs = np.zeros(npt, np.int32), np.zeros(npt), np.zeros(npt)
+    for a in range(nt):
+        for b in range(a, nt):
+            p, p0 = _pair_index(a, b, nt), _pair_index(old[a], old[b], nt0)
+            imap[p], cut[p], cs[p] = F["inter_map"][p0], F["cutoff"][p0], F["cutskin2"][p0]
+    G = dict(F)
+    G.update(ntyp=nt, atm_typ=typ, inter_map=imap, cutoff=cut, cutskin2=cs)
+    return G
+
+
+def test_count_rejects_too_many_pair_types():
+    import torch
+
+    from piny_b200.lib import COUNT_MAX_PAIR_TYPES, DeviceBox, PinyError
+
+    F = load_fixture("spcfw_64_p1")
+    G = _split_types(F)
+    assert G["ntyp"] * (G["ntyp"] + 1) // 2 > COUNT_MAX_PAIR_TYPES
+    box = DeviceBox(G, 1, "fp64")
+    # the split box still builds PINY's list through the allocating entry
+    assert box.build_list(F["pos"][0], None, G["hmat"], G["cutskin2"]) == F["npairs"]
+    d = torch.from_numpy(np.ascontiguousarray(F["pos"][0])).to("cuda:0")
+    torch.cuda.synchronize()
+    with pytest.raises(PinyError, match=r"count_list_device: ERR_ARG .*PINYB200_COUNT_MAX_PAIR_TYPES"):
+        box.count_list_device(d.data_ptr(), None, G["hmat"], G["cutskin2"])
     box.close()
