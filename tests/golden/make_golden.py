@@ -24,7 +24,8 @@ switch the split on.
 
 Run in a container that has the PINY tree:  python tests/golden/make_golden.py
 (``--pimd-only`` regenerates just the transform, MD-bookkeeping, I/O and
-RESPA fixtures)
+RESPA fixtures; ``--headline-only`` just the benchmark configurations
+evaluated in full: spcfw_256_p32, tip4pf_4096_p32, tip4pf_1024_p16)
 The GPU tests only read the .npz files.
 """
 from __future__ import annotations
@@ -416,7 +417,75 @@ def respa_fixture(tmp):
         print(name, os.path.getsize(path), "bytes")
 
 
+# Benchmark configurations evaluated by PINY in full (all beads): the 256
+# q-SPC/Fw x 32-bead box, the 4096 q-TIP4P/F x 32-bead box (64^3 mesh, order
+# 8) and the 1024 q-TIP4P/F x 16-bead box (32^3 mesh, order 8).
+HEADLINE_NAMES = ("spcfw_256_p32", "tip4pf_4096_p32", "tip4pf_1024_p16")
+
+
+def ulp_offsets(actual, generated):
+    """actual - generated in units in the last place (int8), for positions
+    PINY used that differ from the seeded generator's by its Angstrom->Bohr
+    read and its bead -> mode -> bead round trip."""
+    d = actual.view(np.int64) - generated.view(np.int64)
+    if np.abs(d).max() > 127:
+        raise ValueError("positions differ by more than 127 ulps")
+    return d.astype(np.int8)
+
+
+def headline_fixture(name, tmp):
+    """PINY's evaluation of a benchmark configuration, stored compactly: the
+    bead positions and mode-1 positions PINY used as ulp offsets from
+    water.build_positions (Bohr) and from its bead mean, PINY's raw forces
+    (M sites still loaded) of the first and the last bead, every energy
+    component (bead averages over all P beads), pvten_tot, the pair count and
+    sorted-pair SHA-256 of PINY's Verlet list, PINY's cutskin^2, and digests
+    of its set-up (k list SHA-256, every 16th B-spline weight, the spline
+    tables)."""
+    spec = water.named_spec(name)
+    pos_A = water.build_positions(spec)
+    D = run_piny(spec, pos_A, tmp)
+    n, P = int(D["natm_tot"][0]), int(D["pi_beads"][0])
+    gen = pos_A / water.BOHR
+    f = {"spec_name": name, "natm": n, "nbeads": P}
+    f["pos_ulp"] = ulp_offsets(D["pos"].reshape(P, n, 3), gen)
+    if P > 1:
+        xm = np.stack([D["xmod"], D["ymod"], D["zmod"]], axis=1)
+        f["xmod_ulp"] = ulp_offsets(xm, gen.mean(axis=0))
+    f["hmat"] = D["hmat"]
+    f["cutskin2"] = D["cutskin"]
+    f["spread"] = float(D["spread"][0])
+    beads = np.array([0, P - 1]) if P > 1 else np.array([0])
+    f["ref_beads"] = beads
+    f["ref_force_raw"] = D["force_raw"].reshape(P, n, 3)[beads]
+    for k in ("vintert", "vintrat", "vvdw", "vcoul", "vrecip", "vlong", "vbondt", "vbendt"):
+        f["ref_" + k] = float(D[k][0])
+    f["ref_pvten_tot"] = D["pvten_tot"]
+    pairs = D["verlist_pairs"].reshape(-1, 2) - 1
+    f["npairs"] = pairs.shape[0]
+    f["pairs_sha256"] = pair_hash(pairs[:, 0], pairs[:, 1])
+    kv = np.stack([D["kastr"], D["kbstr"], D["kcstr"]], axis=1).astype(np.int32)
+    f["nktot"] = int(D["nktot"][0])
+    f["kvec_sha256"] = hashlib.sha256(kv.tobytes()).hexdigest()
+    f["bweight_every16"] = D["bweight_tot"][::16]
+    f["ngrid"] = np.array([int(D["ngrid_a"][0]), int(D["ngrid_b"][0]), int(D["ngrid_c"][0])])
+    for k in ("cv0", "cdv0", "cv0_c", "cdv0_c"):
+        f[k] = D[k]
+    f["inter_map"] = D["inter_map_index"] - 1
+    f["alp_ewd"] = float(D["alp_ewd"][0])
+    f["clong"] = float(D["clong"][0])
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **{k: np.asarray(v) for k, v in f.items()})
+    print(name, os.path.getsize(path), "bytes", f["npairs"], "pairs")
+
+
 def main():
+    if "--headline-only" in sys.argv[1:]:
+        tmp = tempfile.mkdtemp(prefix="piny_golden_")
+        for name in HEADLINE_NAMES:
+            headline_fixture(name, tmp)
+        shutil.rmtree(tmp, ignore_errors=True)
+        return
     if not os.path.exists(PINY_REF):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     tmp = tempfile.mkdtemp(prefix="piny_golden_")
@@ -443,6 +512,8 @@ def main():
         out = os.path.join(HERE, name + ".npz")
         np.savez_compressed(out, **{k: np.asarray(v) for k, v in fx.items()})
         print(name, os.path.getsize(out), "bytes", fx["npairs"], "pairs")
+    for name in HEADLINE_NAMES:
+        headline_fixture(name, tmp)
     shutil.rmtree(tmp, ignore_errors=True)
 
 

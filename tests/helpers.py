@@ -47,3 +47,24 @@ def respa_from_fixture(F):
 def fixture_level(F, lv):
     from piny_b200.respa import level_bits
     return level_bits(*[int(v) for v in F["L%d_flags" % lv]])
+
+
+HEADLINE_NAMES = ["spcfw_256_p32", "tip4pf_4096_p32", "tip4pf_1024_p16"]
+
+
+def headline_inputs(name):
+    """A benchmark configuration exactly as PINY evaluated it: the fixture,
+    the spec, the bead positions [P][natm][3] and mode-1 positions (Bohr)
+    PINY used -- the seeded generator's positions moved by the stored ulp
+    offsets -- and the host set-up built from them."""
+    from piny_b200 import system
+
+    F = load_fixture(name)
+    spec = water.named_spec(name)
+    gen = water.build_positions(spec) / water.BOHR
+    pos = (gen.view(np.int64) + F["pos_ulp"].astype(np.int64)).view(np.float64)
+    xmod = None
+    if "xmod_ulp" in F:
+        xmod = (gen.mean(axis=0).view(np.int64) + F["xmod_ulp"].astype(np.int64)).view(np.float64)
+    S = system.build_system(spec, pos)
+    return F, spec, pos, xmod, S
