@@ -356,7 +356,10 @@ int pinyb200_piny_force_respa(pinyb200_ctx *ctx, int level, double *const *x,
  *   choice[0]  PME tile edge, 8 or 16 grid points (charges are binned per
  *              tile and bead; spread and gather run one block per tile)
  *   choice[1]  pair kernel: 0 molecule pairs (when the system is made of
- *              identical molecules of <= 4 sites), 1 the site list
+ *              identical molecules of <= 4 sites; in MIXED, when all their
+ *              site pairs share one cutoff and spline grid, with combined
+ *              per-site-pair force and energy rows), 1 the site list,
+ *              2 molecule pairs with PINY's per-table rows
  *   choice[2]  pair kernel grid cap, blocks per SM (1..64)
  *   choice[3]  1: PME on a second stream, concurrent with the pair kernel
  * pinyb200_autotune times every combination on the caller's inputs

@@ -1,16 +1,22 @@
-"""Build the in-tree CUDA library libpinyb200.so for sm_100a with nvcc."""
+"""Build the in-tree CUDA library libpinyb200.so for sm_100a with nvcc.
+
+Each .cu file is compiled to an object in parallel (piny_b200/_build/), then
+the objects are linked into the shared library once.
+"""
 from __future__ import annotations
 
 import glob
 import os
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpinyb200.so")
+OBJDIR = os.path.join(HERE, "_build")
 
 NVCC_FLAGS = [
-    "-O3", "-std=c++17", "-lineinfo", "-shared",
+    "-O3", "-std=c++17", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
 ]
@@ -32,11 +38,31 @@ def needs_build():
     return any(os.path.getmtime(f) > t for f in sources() + headers())
 
 
+def _obj(src):
+    return os.path.join(OBJDIR, os.path.basename(src)[:-3] + ".o")
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB + ".tmp"] + sources()
+    os.makedirs(OBJDIR, exist_ok=True)
+    hdr_t = max(os.path.getmtime(h) for h in headers())
+
+    def compile_one(src):
+        obj = _obj(src)
+        if not force and os.path.exists(obj) and os.path.getmtime(obj) > max(os.path.getmtime(src), hdr_t):
+            return
+        cmd = [nvcc] + NVCC_FLAGS + ["-c", "-o", obj + ".tmp", src]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        os.replace(obj + ".tmp", obj)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(sources()), os.cpu_count() or 1))) as ex:
+        list(ex.map(compile_one, sources()))
+    cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB + ".tmp"] + \
+        [_obj(s) for s in sources()]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -47,9 +47,10 @@ void get_choice(const pinyb200_ctx *c, int *ch)
 
 int set_choice(pinyb200_ctx *c, const int *ch)
 {
-    if (!(ch[0] == 8 || ch[0] == 16) || !(ch[1] == 0 || ch[1] == 1) || ch[2] < 1 || ch[2] > 64 ||
+    if (!(ch[0] == 8 || ch[0] == 16) || !(ch[1] >= 0 && ch[1] <= 2) || ch[2] < 1 || ch[2] > 64 ||
         !(ch[3] == 0 || ch[3] == 1))
-        return record_error(c, PINYB200_ERR_ARG, "tuning: expected {tile 8|16, pair 0|1, blocks/SM 1..64, overlap 0|1}");
+        return record_error(c, PINYB200_ERR_ARG,
+                            "tuning: expected {tile 8|16, pair 0|1|2, blocks/SM 1..64, overlap 0|1}");
     if (c->sys.nchrg > 0 && c->sys.nktot > 0 && ch[0] != c->pme_tile) {
         int rc = pme_tiles_resize(c, ch[0]);
         if (rc) return rc;
@@ -150,7 +151,8 @@ int pinyb200_autotune(pinyb200_ctx *c, const double *d_pos, const double *d_xmod
     if (has_pme && nmin >= 16) tiles.push_back(16);
     std::vector<int> variants = {1};
     if (c->use_mol && c->mol_ok) variants.insert(variants.begin(), 0);
-    const int bps[4] = {4, 8, 16, 32};
+    if (c->use_mol && c->mol_ok && c->mix_ok) variants.push_back(2);
+    const int bps[5] = {4, 6, 8, 16, 32};
     int best[4];
     get_choice(c, best);
     float tbest = 1e30f;

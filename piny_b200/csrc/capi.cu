@@ -194,6 +194,48 @@ static int pme_tiles_setup(pinyb200_ctx *c, int T)
     return PINYB200_OK;
 }
 
+// Per-site-pair parameters of the MIXED molecule-pair kernel
+// (mol_pair_mixed_kernel): for site pair (si, sj) of the uniform molecule
+// with pair type p and table u = inter_map[p], its row offset u * nsplin + 2,
+// charge product and which of the tables (Coulomb, vdW) it reads
+// (force_npol.c:339-375).  Set only when every site pair shares the cutoff
+// and the spline grid; otherwise mix_ok stays false and mol_pair_kernel runs.
+static void mixed_setup(pinyb200_ctx *c, const pinyb200_system *s, int n0)
+{
+    const int NS = c->mol_ns;
+    const size_t per = (size_t)s->nsplin;
+    int p0 = -1;
+    for (int si = 0; si < NS; si++)
+        for (int sj = 0; sj < NS; sj++) {
+            const int sp = si * NS + sj;
+            const int ia = si < n0 ? si : 0, ja = sj < n0 ? sj : 0;
+            const int ti = s->atm_typ[ia], tj = s->atm_typ[ja];
+            const int i2 = ti + 1, i3 = tj + 1, jj = std::min(i2, i3), ii = i2 + i3 - jj;
+            const int p = ((jj - 1) * ((s->ntyp + 1) * 2 - jj)) / 2 + ii - jj;
+            if (p0 < 0) p0 = p;
+            const int u = s->inter_map[p], u0 = s->inter_map[p0];
+            if (s->cutoff[p] != s->cutoff[p0] || s->rmin_spl[u] != s->rmin_spl[u0] ||
+                s->dri_spl[u] != s->dri_spl[u0] || s->dr_spl[u] != s->dr_spl[u0])
+                return;  // not uniform: mol_pair_kernel
+            bool vdw = false;
+            for (size_t k = 0; k < per; k++)
+                vdw |= s->cv0[(size_t)u * per + k] != 0.0 || s->cdv0[(size_t)u * per + k] != 0.0;
+            const double q2 = s->charge[ia] * s->charge[ja];
+            c->mix_eflag[sp] = (vdw ? 1 : 0) | (q2 != 0.0 ? 2 : 0);
+            c->mix_q2[sp] = (float)q2;
+            c->mix_toff[sp] = (int)((size_t)u * per + 2);  // knot k = nint(t) + 3, coefficients at k - 1
+        }
+    const int u0 = s->inter_map[p0];
+    c->mix_rc2 = (float)(s->cutoff[p0] * s->cutoff[p0]);
+    c->mix_dri = (float)s->dri_spl[u0];
+    c->mix_rmd = (float)(s->rmin_spl[u0] * s->dri_spl[u0]);
+    c->mix_tmax = (float)(s->nsplin - 5);
+    c->mix_ok = (size_t)c->sys.nuniq * per * 4 < (size_t)0x7fffffff;
+    // one wave of resident blocks (6 per SM at its register count) serves
+    // the grid-strided chunks best at the benchmark sizes
+    if (c->mix_ok) c->pair_blocks_per_sm = 6;
+}
+
 extern "C" {
 
 int pinyb200_version(void) { return 1; }
@@ -497,6 +539,11 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
             CK(upload(&c->d_mstart, mstart.data(), mstart.size()));
             CK(cudaMalloc(&c->d_mcount, (size_t)c->nmol * sizeof(int)));
             CK(cudaMalloc(&c->d_mrow, (size_t)(c->nmol + 1) * sizeof(int)));
+            const int n0 = mstart[1];
+            bool strided = true;
+            for (size_t m = 0; m < mstart.size(); m++) strided &= mstart[m] == (int)m * n0;
+            c->mol_stride = strided ? n0 : 0;
+            if (strided && precision == PINYB200_MIXED) mixed_setup(c, s, n0);
         }
     }
     CK(cudaMalloc(&c->d_err, sizeof(int)));
@@ -670,7 +717,9 @@ int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, boo
     }
     const bool ortho = cell.h[1] == 0.0 && cell.h[2] == 0.0 && cell.h[3] == 0.0 && cell.h[5] == 0.0 &&
                        cell.h[6] == 0.0 && cell.h[7] == 0.0;
-    if (c->use_mol && c->mol_ok && ortho && c->pair_variant == 0 && !(flags & PINYB200_SITE_PAIRS))
+    if (c->use_mol && c->mol_ok && ortho && c->pair_variant == 0 && !(flags & PINYB200_SITE_PAIRS) && c->mix_ok)
+        CK(launch_mol_pair_mixed(c, cell, energy));
+    else if (c->use_mol && c->mol_ok && ortho && c->pair_variant != 1 && !(flags & PINYB200_SITE_PAIRS))
         CK(launch_mol_pair(c, cell, energy));
     else CK(launch_pair(c, cell, energy));
     if (respa_w) {

@@ -140,6 +140,7 @@ struct pinyb200_ctx {
     bool pme_overlap = true;            // false: PME on the main stream after the pair kernel
     int pair_variant = 0;               // 0 molecule-pair kernel (when available), 1 site-list kernel
     int pair_blocks_per_sm = 16;        // grid cap of the pair kernels, blocks per SM
+    int pair_carveout = 25;             // shared-memory share (%) the MIXED molecule-pair kernel asks for
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_pme[2] = {nullptr, nullptr};
     pinyb200::DeviceSystem sys;
     // host copies needed for energy bookkeeping
@@ -159,6 +160,13 @@ struct pinyb200_ctx {
     bool have_list = false;
     // molecule-pair list (sites grouped into molecules of <= 4 consecutive sites)
     bool use_mol = false;      // the system splits into such molecules
+    int mol_stride = 0;        // sites per molecule when molecule m starts at site m * mol_stride, else 0
+    // MIXED molecule-pair kernel with unrolled site pairs: usable when every
+    // site pair of the molecule shares one cutoff and spline grid
+    bool mix_ok = false;
+    int mix_toff[16] = {0}, mix_eflag[16] = {0};
+    float mix_q2[16] = {0};
+    float mix_rc2 = 0, mix_dri = 0, mix_rmd = 0, mix_tmax = 0;
     bool mol_ok = false;       // the current molecule list matches the site list
     int nmol = 0, mol_ns = 0;
     int *d_mstart = nullptr;   // [nmol+1]
@@ -248,6 +256,7 @@ cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_p
                             const double *d_cutskin2, int pass, const int *gate = nullptr,
                             cudaStream_t st = nullptr);
 cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
+cudaError_t launch_mol_pair_mixed(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_site_from_mol(pinyb200_ctx *c, int pass, const int *gate = nullptr, cudaStream_t st = nullptr);
 __global__ void __launch_bounds__(1024) scan_kernel(const int *gate, int n, const int *count, int *row, int *rowA,
                                                      long long *tot);
@@ -292,6 +301,23 @@ inline cudaError_t smem_optin(const void *func, int bytes)
     if (have >= bytes) return cudaSuccess;
     e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) have = bytes;
+    return e;
+}
+// cudaFuncSetAttribute(PreferredSharedMemoryCarveout) once per kernel and
+// device: a kernel that gathers from tables held in L1 asks for a small
+// shared-memory share, leaving the rest of the unified cache to L1.
+inline cudaError_t carveout_pref(const void *func, int percent)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    int &have = done[std::make_pair(func, dev)];
+    if (have == percent + 1) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, percent);
+    if (e == cudaSuccess) have = percent + 1;
     return e;
 }
 int record_error(pinyb200_ctx *c, int code, const std::string &msg);

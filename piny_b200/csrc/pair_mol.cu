@@ -683,6 +683,253 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
 }
 
 // ---------------------------------------------------------------------------
+// MIXED kernel with unrolled site pairs.
+//
+// Same pairs, images, tables and accumulation scheme as mol_pair_kernel
+// (lanes = beads, one molecule pair per lane group, i-site forces in
+// registers over a chunk, one FP64 red.add per j site), with the per-pair
+// work cut down for a molecular system whose pair types all share one
+// cutoff and one spline grid (every PINY water input):
+//   * the site-pair loops are unrolled and each site pair's table offset,
+//     charge product and which tables it uses (q_i q_j cdv0_c / cv0_c, the
+//     vdW cdv0 / cv0; force_npol.c:339-375) are kernel parameters (constant
+//     bank): no shared-memory constant load and no address arithmetic on
+//     the pair type is left per pair.  The rows stay PINY's per-table ones:
+//     every charged pair reads the same Coulomb table, so the tables that
+//     32 beads' knots scatter over stay few enough for L1;
+//   * the knot nint((r - rmin) dri) (force_npol.c:345-352) is taken with the
+//     1.5 * 2^23 rounding constant instead of float <-> int conversions, t
+//     clamped to the table's intervals (what clamping the knot does for
+//     every r inside the cutoff);
+//   * molecules are uniform runs of sites: the j site index is mj * stride,
+//     not a load.
+// Pairs whose site-0 separation is within twice the molecular extent of half
+// a box go through mol_pair_near (per-site-pair FP64 image), as in
+// mol_pair_kernel.
+
+// Table row load that asks L1 to keep the line (evict_last): the four
+// tables a water system reads stay resident while positions stream past.
+__device__ __forceinline__ float4 ldg_keep(const float4 *p)
+{
+    float4 v;
+    asm("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(p));
+    return v;
+}
+
+struct MixArgs {
+    const int *nchunk, *chunk, *bad, *mj;
+    const unsigned *mask;
+    const int *mstart;
+    int ntyp, nuniq, nsplin, stride;
+    const double *posT, *xmod;
+    const int *atm_typ;
+    const double *charge;
+    const int *inter_map;
+    const double *cutoff, *rmin, *dri;
+    const int *has_vdw;
+    const float4 *tab;   // [4][nuniq][nsplin] interval coefficients (TabKind order)
+    double *forceT;
+    double *acc;
+    int toff[16];        // per site pair si * NS + sj: u * nsplin + 2, its rows at nint(t) = 0
+    float q2[16];        // charge product of the site pair
+    int eflag[16];       // tables the site pair uses: 1 vdW, 2 Coulomb
+    int tstride;         // nuniq * nsplin, the distance between table kinds
+    float rc2, dri_f, rmd, tmax;  // cutoff^2, 1/dr, rmin/dr, last interval
+};
+
+#ifndef PINYB200_MIX_BLOCKS
+#define PINYB200_MIX_BLOCKS 6
+#endif
+
+template <int P, int NS, bool ENERGY>
+__global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kernel(MixArgs a, Cell cell)
+{
+    constexpr int G = P >= 32 ? 32 : P;  // lanes per molecule pair
+    constexpr int JPI = 32 / G;          // molecule pairs per warp step
+    __shared__ PairConst<float> pc;      // per-kind constants of the near path
+    __shared__ double sacc[8][128];
+    if (threadIdx.x < NS * NS) {
+        const int si = threadIdx.x / NS, sj = threadIdx.x % NS;
+        const int nm0 = a.mstart[1];
+        const int ia = si < nm0 ? si : 0, ja = sj < nm0 ? sj : 0;
+        const int p = pair_type(a.atm_typ[ia], a.atm_typ[ja], a.ntyp);
+        const int u = a.inter_map[p];
+        const double q2 = a.charge[ia] * a.charge[ja];
+        float4 c;
+        c.x = (float)(a.cutoff[p] * a.cutoff[p]);
+        c.y = (float)a.rmin[u];
+        c.z = (float)a.dri[u];
+        c.w = (float)q2;
+        pc.c[threadIdx.x] = c;
+        pc.q2[threadIdx.x] = (float)q2;
+        pc.o[threadIdx.x] = make_int2(u * a.nsplin, a.has_vdw[u]);
+    }
+    if (ENERGY)
+        for (int c = 0; c < 8; c++) sacc[c][threadIdx.x] = 0.0;
+    __syncthreads();
+    if (a.bad && (a.bad[0] | a.bad[1])) {
+        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) a.acc[S_VVDW] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
+    const float4 *__restrict__ tab = a.tab;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int sub = lane / G;
+    const int b = (lane % G) + 32 * blockIdx.y;  // bead
+    const double *__restrict__ posT = a.posT;
+    const float rc2 = a.rc2, dri = a.dri_f, rmd = a.rmd, tmax = a.tmax;
+    constexpr float kRound = 12582912.0f;  // 1.5 * 2^23: x + kRound - kRound = nearest integer of x
+
+    const int nch = *a.nchunk;
+    for (int ch = warp; ch < nch; ch += nwarps) {
+        const int mi = a.chunk[3 * ch], beg = a.chunk[3 * ch + 1], end = a.chunk[3 * ch + 2];
+        const int i0 = mi * a.stride, ni = a.stride;
+        float ei[NS][3], fi[NS][3];
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            const int i = i0 + (s < ni ? s : 0);
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                ei[s][d] = (float)(posT[(3 * (size_t)i + d) * P + b] - posT[(3 * (size_t)i0 + d) * P + b]);
+                fi[s][d] = 0.0f;
+            }
+        }
+        float evs = 0.0f, ecs = 0.0f, pvs[6] = {0, 0, 0, 0, 0, 0};
+        for (int k = beg + sub; k < end; k += JPI) {
+            const int mj = __ldcg(a.mj + k);
+            const unsigned mask = __ldcg(a.mask + k);
+            const int j0 = mj * a.stride;
+            // site-0 image from the mode-1 separation (FP64) and whether site
+            // pairs may take other images
+            double sh0[3];
+            bool near = false;
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const double hid = cell.hi[4 * d];
+                const double t = __dmul_rn(__dsub_rn(a.xmod[3 * (size_t)i0 + d], __ldcg(a.xmod + 3 * (size_t)j0 + d)), hid);
+                sh0[d] = -nint_rn(t);
+                near |= fabs(t + sh0[d]) > 0.5 - 2.0 * PINYB200_MOL_EXTENT * hid;
+            }
+            if (near) {
+                mol_pair_near<float, P, NS, true, ENERGY>(posT, a.xmod, a.forceT, &pc, a.tab,
+                                                           (size_t)a.nuniq * a.nsplin, a.nsplin - 2, i0, j0, mask, b,
+                                                           cell.h[0], cell.h[4], cell.h[8], cell.hi[0], cell.hi[4],
+                                                           cell.hi[8], &sacc[0][threadIdx.x]);
+                continue;
+            }
+            unsigned jm = 1u;
+#pragma unroll
+            for (int si = 0; si < NS; si++) jm |= (mask >> (si * NS)) & ((1u << NS) - 1u);
+            // dj[s] = x_i0 - x_j(s) + image, in FP32 from the FP64 site-0 separation
+            float dj[NS][3];
+            {
+                // the i anchor is re-read (an L1 hit) rather than held over the chunk
+                double xj0[3];
+#pragma unroll
+                for (int d = 0; d < 3; d++) xj0[d] = __ldcg(posT + (3 * (size_t)j0 + d) * P + b);
+#pragma unroll
+                for (int d = 0; d < 3; d++)
+                    dj[0][d] = (float)(__dsub_rn(posT[(3 * (size_t)i0 + d) * P + b], xj0[d]) + sh0[d] * cell.h[4 * d]);
+#pragma unroll
+                for (int s = 1; s < NS; s++) {
+                    const int j = j0 + (((jm >> s) & 1u) ? s : 0);
+#pragma unroll
+                    for (int d = 0; d < 3; d++)
+                        dj[s][d] = dj[0][d] - (float)(__ldcg(posT + (3 * (size_t)j + d) * P + b) - xj0[d]);
+                }
+            }
+#pragma unroll
+            for (int sj = 0; sj < NS; sj++) {
+                if (!((jm >> sj) & 1u)) continue;
+                float fjx = 0.0f, fjy = 0.0f, fjz = 0.0f;
+#pragma unroll
+                for (int si = 0; si < NS; si++) {
+                    const int sp = si * NS + sj;
+                    if (!((mask >> sp) & 1u)) continue;
+                    const float rx = dj[sj][0] + ei[si][0];
+                    const float ry = dj[sj][1] + ei[si][1];
+                    const float rz = dj[sj][2] + ei[si][2];
+                    const float r2 = rx * rx + ry * ry + rz * rz;
+                    if (r2 < rc2) {
+                        const float r = r2 * rsqrtf(r2);
+                        const float t = fminf(fmaxf(fmaf(r, dri, -rmd), 0.0f), tmax);
+                        const float tr = __fadd_rn(t, kRound);
+                        const int kn = __float_as_int(tr) - __float_as_int(kRound);
+                        const float del = t - __fsub_rn(tr, kRound);
+                        const float4 *row = tab + (a.toff[sp] + kn);
+                        float dv = 0.0f;
+                        if (a.eflag[sp] & 2) {
+                            const float4 cf = ldg_keep(row + T_CDV0C * a.tstride);
+                            dv = a.q2[sp] * (cf.x + del * (cf.y + del * (cf.z + del * cf.w)));
+                        }
+                        if (a.eflag[sp] & 1) {
+                            const float4 cf = ldg_keep(row + T_CDV0 * a.tstride);
+                            dv += cf.x + del * (cf.y + del * (cf.z + del * cf.w));
+                        }
+                        const float fx = rx * dv, fy = ry * dv, fz = rz * dv;
+                        fi[si][0] += fx;
+                        fi[si][1] += fy;
+                        fi[si][2] += fz;
+                        fjx -= fx;
+                        fjy -= fy;
+                        fjz -= fz;
+                        if (ENERGY) {
+                            if (a.eflag[sp] & 1) {
+                                const float4 ce = ldg_keep(row + T_CV0 * a.tstride);
+                                evs += ce.x + del * (ce.y + del * (ce.z + del * ce.w));
+                            }
+                            if (a.eflag[sp] & 2) {
+                                const float4 ce = ldg_keep(row + T_CV0C * a.tstride);
+                                ecs += a.q2[sp] * (ce.x + del * (ce.y + del * (ce.z + del * ce.w)));
+                            }
+                            pvs[0] += rx * fx;
+                            pvs[1] += ry * fy;
+                            pvs[2] += rz * fz;
+                            pvs[3] += rx * fy;
+                            pvs[4] += rx * fz;
+                            pvs[5] += ry * fz;
+                        }
+                    }
+                }
+                if (fjx != 0.0f || fjy != 0.0f || fjz != 0.0f) {
+                    const int j = j0 + sj;
+                    atomicAdd(&a.forceT[(3 * (size_t)j + 0) * P + b], (double)fjx);
+                    atomicAdd(&a.forceT[(3 * (size_t)j + 1) * P + b], (double)fjy);
+                    atomicAdd(&a.forceT[(3 * (size_t)j + 2) * P + b], (double)fjz);
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                double v = (double)fi[s][d];
+                if (G < 32) v = warp_sum_strided(v, G);
+                if ((G == 32 || sub == 0) && s < ni && v != 0.0) atomicAdd(&a.forceT[(3 * (size_t)(i0 + s) + d) * P + b], v);
+            }
+        }
+        if (ENERGY) {
+            sacc[0][threadIdx.x] += (double)evs;
+            sacc[1][threadIdx.x] += (double)ecs;
+#pragma unroll
+            for (int c = 0; c < 6; c++) sacc[2 + c][threadIdx.x] += (double)pvs[c];
+        }
+    }
+    if (ENERGY) {
+        const int slot[8] = {S_VVDW, S_VCOUL, S_PXX, S_PYY, S_PZZ, S_PXY, S_PXZ, S_PYZ};
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            double t = sacc[c][threadIdx.x];
+            if (G < 32) t = warp_sum_strided(t, G);
+            if (G == 32 || sub == 0) atomicAdd(&a.acc[(size_t)b * S_NSLOT + slot[c]], t);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 
 // pass 0: reach, counts, row offsets and the molecule-pair total (tot[2]);
@@ -820,6 +1067,82 @@ cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy)
     a.tab = s.tab32;
     if (c->mol_ns == 3) return launch_mol_ns<float, 3>(c, a, cell, true);
     return launch_mol_ns<float, 4>(c, a, cell, true);
+}
+
+
+template <int P, int NS>
+static void launch_mix_t(pinyb200_ctx *c, const MixArgs &a, const Cell &cell, bool energy)
+{
+    const int threads = 128;
+    long long blocks = ((long long)c->chunk_cap * 32 + threads - 1) / threads;
+    const long long maxb = (long long)c->sm_count * c->pair_blocks_per_sm;
+    if (blocks > maxb) blocks = maxb;
+    if (blocks < 1) blocks = 1;
+    dim3 grid((unsigned)blocks, P > 32 ? P / 32 : 1);
+    if (energy) {
+        carveout_pref((const void *)mol_pair_mixed_kernel<P, NS, true>, c->pair_carveout);
+        mol_pair_mixed_kernel<P, NS, true><<<grid, threads, 0, c->stream>>>(a, cell);
+    } else {
+        carveout_pref((const void *)mol_pair_mixed_kernel<P, NS, false>, c->pair_carveout);
+        mol_pair_mixed_kernel<P, NS, false><<<grid, threads, 0, c->stream>>>(a, cell);
+    }
+}
+
+template <int NS>
+static cudaError_t launch_mix_ns(pinyb200_ctx *c, const MixArgs &a, const Cell &cell, bool energy)
+{
+    switch (c->P) {
+    case 1: launch_mix_t<1, NS>(c, a, cell, energy); break;
+    case 2: launch_mix_t<2, NS>(c, a, cell, energy); break;
+    case 4: launch_mix_t<4, NS>(c, a, cell, energy); break;
+    case 8: launch_mix_t<8, NS>(c, a, cell, energy); break;
+    case 16: launch_mix_t<16, NS>(c, a, cell, energy); break;
+    case 32: launch_mix_t<32, NS>(c, a, cell, energy); break;
+    case 64: launch_mix_t<64, NS>(c, a, cell, energy); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+// The MIXED kernel with combined per-site-pair tables (pinyb200_ctx::mix_ok).
+cudaError_t launch_mol_pair_mixed(pinyb200_ctx *c, const Cell &cell, bool energy)
+{
+    const DeviceSystem &s = c->sys;
+    MixArgs a;
+    a.nchunk = c->d_nchunk;
+    a.chunk = c->d_chunk;
+    a.bad = c->d_ls ? (const int *)((const char *)c->d_ls + offsetof(ListState, overflow)) : nullptr;
+    a.mj = c->d_mj;
+    a.mask = c->d_mmask;
+    a.mstart = c->d_mstart;
+    a.ntyp = s.ntyp;
+    a.nuniq = s.nuniq;
+    a.nsplin = s.nsplin;
+    a.stride = c->mol_stride;
+    a.posT = c->d_posT;
+    a.xmod = c->P > 1 ? c->d_xmod : c->d_posT;
+    a.atm_typ = s.atm_typ;
+    a.charge = s.charge;
+    a.inter_map = s.inter_map;
+    a.cutoff = s.cutoff;
+    a.rmin = s.rmin;
+    a.dri = s.dri;
+    a.has_vdw = s.has_vdw;
+    a.tab = s.tab32;
+    a.forceT = c->d_forceT;
+    a.acc = c->d_acc;
+    for (int k = 0; k < 16; k++) {
+        a.toff[k] = c->mix_toff[k];
+        a.q2[k] = c->mix_q2[k];
+        a.eflag[k] = c->mix_eflag[k];
+    }
+    a.tstride = s.nuniq * s.nsplin;
+    a.rc2 = c->mix_rc2;
+    a.dri_f = c->mix_dri;
+    a.rmd = c->mix_rmd;
+    a.tmax = c->mix_tmax;
+    if (c->mol_ns == 3) return launch_mix_ns<3>(c, a, cell, energy);
+    return launch_mix_ns<4>(c, a, cell, energy);
 }
 
 }  // namespace pinyb200

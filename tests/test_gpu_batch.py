@@ -114,7 +114,7 @@ def test_autotune_picks_a_valid_shape_and_remembers_it():
     d = torch.from_numpy(pos).to("cuda:0")
     dx = torch.from_numpy(xmod).to("cuda:0") if xmod is not None else None
     choice, ms = box.autotune(d.data_ptr(), None if dx is None else dx.data_ptr(), S["hmat"], reps=2, again=True)
-    assert choice[0] in (8, 16) and choice[1] in (0, 1) and choice[2] in (4, 8, 16, 32) and choice[3] in (0, 1)
+    assert choice[0] in (8, 16) and choice[1] in (0, 1, 2) and choice[2] in (4, 8, 16, 32) and choice[3] in (0, 1)
     assert ms > 0
     assert box.tuning() == choice
     # a second context of the same shape applies the remembered result
@@ -189,3 +189,22 @@ def test_c4_set_matches_oracle_box_by_box(prec, oracle):
     batch.close()
     for bx in boxes:
         bx[-1].close()
+
+
+def test_mixed_pair_kernels_agree_with_fp64():
+    """MIXED: the unrolled molecule-pair kernel (pair choice 0), the
+    per-table molecule-pair kernel (2) and the site-list kernel (1) all give
+    the FP64 forces within 1e-5 relative RMS."""
+    boxes = _boxes(nbox=2, seed=5)
+    for sp, pos, S in boxes:
+        b0, f0, e0 = _single(S, pos, sp.nbeads, "fp64")
+        b0.close()
+        for choice in ([16, 0, 6, 1], [8, 2, 16, 0], [8, 1, 8, 1]):
+            if choice[0] == 16 and min(S["ngrid_a"], S["ngrid_b"], S["ngrid_c"]) < 16:
+                choice = [8] + choice[1:]
+            b, f, e = _single(S, pos, sp.nbeads, "mixed", choice)
+            assert b.tuning() == choice
+            assert rel_rms(f, f0) < 1e-5, choice
+            scale = abs(e0["vvdw"]) + abs(e0["vcoul"]) + abs(e0["vrecip"]) + abs(e0["vself"])
+            assert abs(e["vintert"] - e0["vintert"]) <= 1e-6 * scale
+            b.close()
