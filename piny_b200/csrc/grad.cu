@@ -616,7 +616,9 @@ int pinyb200_grad(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, co
     const GradHost &gh = c->grad;
     const int K = gh.K;
     // forward: raw site forces (ghosts not distributed), potential grid, records
+    c->pme_full_records = true;
     int rc = enqueue_device(c, d_pos, d_xmod, cell, 0, c->d_force_aos, false, nullptr);
+    c->pme_full_records = false;
     if (rc) return rc;
     if (cudaMemsetAsync(gh.d_gacc, 0, (size_t)2 * PINYB200_MAX_TAN * sizeof(double), c->stream) != cudaSuccess)
         return record_error(c, PINYB200_ERR_CUDA, "grad: memset failed");

@@ -140,6 +140,7 @@ struct pinyb200_ctx {
     bool pme_overlap = true;            // false: PME on the main stream after the pair kernel
     int pair_variant = 0;               // 0 molecule-pair kernel (when available), 1 site-list kernel
     int pair_blocks_per_sm = 16;        // grid cap of the pair kernels, blocks per SM
+    bool pme_full_records = false;      // forward PME writes the full weight records (the adjoint reads them)
     int pair_carveout = 25;             // shared-memory share (%) the MIXED molecule-pair kernel asks for
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_pme[2] = {nullptr, nullptr};
     pinyb200::DeviceSystem sys;

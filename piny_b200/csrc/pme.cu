@@ -561,6 +561,426 @@ __global__ void __launch_bounds__(256) gather_tile_kernel(PmeArgs a, Cell cell, 
 }
 
 // ---------------------------------------------------------------------------
+// Compact forward path: bin, spread and gather without weight records.
+//
+// B-spline weights as polynomials of the fractional offset.  PINY's
+// recursion (ewald3d_pme.c:301-338) makes the weight m[j] of order NI (at
+// u = f + j - 1) a polynomial of degree NI - 1 in f on [0, 1), and the
+// derivative weight dm[j] = m'[j] - m'[j - 1] formed from the order NI - 1
+// splines (:512-532) one of degree NI - 2.  BsplinePoly runs that recursion
+// on coefficient arrays at compile time; the kernels evaluate each lane's
+// weights by Horner from a shared-memory copy.  The bin kernel writes, per
+// (charge, bead), only the stencil origin and the three fractional offsets
+// with the charge (32 bytes in FP32) instead of the 6 x NIP weights, and
+// spread and gather read the next record while they work on the current one.
+template <int NI>
+struct BsplinePoly {
+    double m[NI][NI];   // m[p][d]: coefficient of f^d of PINY's m[p + 1]
+    double dm[NI][NI];  // dm[p][d]: of PINY's dm[p + 1]
+    constexpr BsplinePoly() : m(), dm()
+    {
+        double cur[NI + 1][NI + 1] = {};
+        cur[1][1] = 1.0;   // m[1] = 1 - |u_1 - 1| = f
+        cur[2][0] = 1.0;   // m[2] = 1 - |u_2 - 1| = 1 - f
+        cur[2][1] = -1.0;
+        for (int nn = 3; nn <= NI; nn++) {
+            const double rn1 = 1.0 / (double)(nn - 1);
+            // m[j] = (u_j m[j] + (nn - u_j) m[j - 1]) / (nn - 1), u_j = f + j - 1
+            for (int j = nn; j >= 2; j--) {
+                double nw[NI + 1] = {};
+                for (int d = 0; d < NI; d++) {
+                    nw[d] += (double)(j - 1) * cur[j][d] + (double)(nn - j + 1) * cur[j - 1][d];
+                    nw[d + 1] += cur[j][d] - cur[j - 1][d];
+                }
+                for (int d = 0; d <= NI; d++) cur[j][d] = nw[d] * rn1;
+            }
+            double nw1[NI + 1] = {};
+            for (int d = 0; d < NI; d++) nw1[d + 1] = cur[1][d];
+            for (int d = 0; d <= NI; d++) cur[1][d] = nw1[d] * rn1;
+            if (nn == NI - 1)
+                for (int j = 1; j <= NI; j++)
+                    for (int d = 0; d < NI; d++) dm[j - 1][d] = cur[j][d] - (j >= 2 ? cur[j - 1][d] : 0.0);
+        }
+        for (int j = 1; j <= NI; j++)
+            for (int d = 0; d < NI; d++) m[j - 1][d] = cur[j][d];
+    }
+};
+
+template <int NI>
+__constant__ BsplinePoly<NI> kBspline = BsplinePoly<NI>();
+
+// Shared copy of the polynomials in R, rows padded to a multiple of 4.
+template <typename R, int NI>
+struct PolyTab {
+    static constexpr int NP4 = (NI + 3) & ~3;
+    R m[NI][NP4], dm[NI][NP4];
+    __device__ __forceinline__ void fill(bool deriv)
+    {
+        for (int i = threadIdx.x; i < NI * NP4; i += blockDim.x) {
+            const int p = i / NP4, d = i - p * NP4;
+            m[p][d] = d < NI ? (R)kBspline<NI>.m[p][d] : (R)0;
+            if (deriv) dm[p][d] = d < NI ? (R)kBspline<NI>.dm[p][d] : (R)0;
+        }
+    }
+};
+
+// Weight of stencil point t (grid index lo + t carries PINY's m[NI - t],
+// piece NI - 1 - t) from its coefficient row, by Horner.
+template <typename R, int NI>
+__device__ __forceinline__ R poly_eval(const R (&row)[PolyTab<R, NI>::NP4], R f)
+{
+    constexpr int NP4 = PolyTab<R, NI>::NP4;
+    R c[NP4];
+    if constexpr (sizeof(R) == 4) {
+#pragma unroll
+        for (int i = 0; i < NP4; i += 4) {
+            const float4 v = *(const float4 *)&row[i];
+            c[i] = v.x;
+            c[i + 1] = v.y;
+            c[i + 2] = v.z;
+            c[i + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < NP4; i += 2) {
+            const double2 v = *(const double2 *)&row[i];
+            c[i] = v.x;
+            c[i + 1] = v.y;
+        }
+    }
+    R w = c[NI - 1];
+#pragma unroll
+    for (int d = NI - 2; d >= 0; d--) w = w * f + c[d];
+    return w;
+}
+
+template <typename R>
+__device__ __forceinline__ typename Vec4<R>::T load_frac(const void *rw, int idx)
+{
+    if constexpr (sizeof(R) == 4) return __ldg((const float4 *)rw + idx);
+    else return ldg4((const double4 *)rw + idx);
+}
+
+// Bin kernel of the compact path: one thread per (charge, bead), stencil
+// origin in FP64 with PINY's operation order (as pme_bin_kernel), record
+// (atom, la, lb, lc) + (fa, fb, fc, q), record number filed under its tile.
+template <typename R, int NI>
+__global__ void __launch_bounds__(256) pme_bin_compact_kernel(PmeArgs a, Cell cell, TileArgs t)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)a.nchrg * a.P) return;
+    const int b = (int)(idx % a.P);
+    const int k = (int)(idx / a.P);
+    const int at = a.ichrg[k];
+    int la, lb, lc;
+    double fa, fb, fc;
+    stencil_origin(a, cell, at, b, NI, la, lb, lc, fa, fb, fc);
+    typename Vec4<R>::T fr;
+    fr.x = (R)fa;
+    fr.y = (R)fb;
+    fr.z = (R)fc;
+    fr.w = (R)a.charge[at];
+    ((typename Vec4<R>::T *)a.rw)[idx] = fr;
+    a.rhead[idx] = make_int4(at, la, lb, lc);
+    const int T = t.T;
+    const int tile = ((lc / T) * t.ntb + lb / T) * t.nta + la / T;
+    const int slot = atomicAdd(&t.cnt[b * t.ntile + tile], 1);
+    if (slot < t.cap) t.bin[((size_t)b * t.ntile + tile) * t.cap + slot] = (int)idx;
+    else t.ovf[atomicAdd(&t.cnt[a.P * t.ntile], 1)] = (int)idx;
+}
+
+// Weights one spread lane needs (lanes = 8 a points x 4 b rows): its a
+// points la8 (+8), its b rows lb4 + 4 i, and all c points, the latter
+// evaluated by lanes 0..NI-1 and shuffled.  Every lane of the warp calls it.
+template <typename R, int NI>
+struct SpreadW {
+    static constexpr int NTB = (NI + 3) / 4, NSA = (NI + 7) / 8;
+    R wa[NSA], mb[NTB], mc[NI];
+    __device__ __forceinline__ void eval(const PolyTab<R, NI> &pt, const typename Vec4<R>::T &fr, int lane)
+    {
+        const int la8 = lane & 7, lb4 = lane >> 3;
+#pragma unroll
+        for (int s = 0; s < NSA; s++) wa[s] = la8 + 8 * s < NI ? poly_eval<R, NI>(pt.m[NI - 1 - (la8 + 8 * s)], fr.x) : (R)0;
+#pragma unroll
+        for (int i = 0; i < NTB; i++) mb[i] = lb4 + 4 * i < NI ? poly_eval<R, NI>(pt.m[NI - 1 - (lb4 + 4 * i)], fr.y) : (R)0;
+        const R mcl = lane < NI ? poly_eval<R, NI>(pt.m[NI - 1 - lane], fr.z) : (R)0;
+#pragma unroll
+        for (int tc = 0; tc < NI; tc++) mc[tc] = __shfl_sync(0xffffffffu, mcl, tc);
+    }
+};
+
+// One record spread straight into the grid g of its bead (origin outside
+// the block's tile, or an overflow record); a warp, lanes as SpreadW.
+template <typename R, int NI>
+__device__ __forceinline__ void spread_warp_global(const PmeArgs &a, R *g, int la, int lb, int lc,
+                                                   const SpreadW<R, NI> &w, R q, int lane)
+{
+    const int la8 = lane & 7, lb4 = lane >> 3;
+#pragma unroll
+    for (int s = 0; s < SpreadW<R, NI>::NSA; s++) {
+        if (la8 + 8 * s >= NI) break;
+        const int ga = wrapi(la + la8 + 8 * s, a.Na);
+        const R qa = q * w.wa[s];
+#pragma unroll
+        for (int tc = 0; tc < NI; tc++) {
+            const int gc = wrapi(lc + tc, a.Nc);
+            const R cq = qa * w.mc[tc];
+#pragma unroll
+            for (int i = 0; i < SpreadW<R, NI>::NTB; i++)
+                if (lb4 + 4 * i < NI) atomicAdd(g + ((size_t)gc * a.Nb + wrapi(lb + lb4 + 4 * i, a.Nb)) * a.Na + ga, cq * w.mb[i]);
+        }
+    }
+}
+
+// Spread of the compact path: as spread_tile_kernel (one block per (tile,
+// bead), one warp per record into a shared copy of the tile, the copy added
+// to the grid once), with the weights evaluated in the block and the next
+// record read ahead.
+template <typename R, int NI, int TT>
+__global__ void __launch_bounds__(256) spread_tile_c_kernel(PmeArgs a, TileArgs t)
+{
+    typedef TileGeom<NI, TT> TG;
+    typedef typename Vec4<R>::T R4;
+    constexpr int NTB = SpreadW<R, NI>::NTB;
+    extern __shared__ unsigned char smem_raw[];
+    R *tl = (R *)smem_raw;
+    __shared__ __align__(16) PolyTab<R, NI> pt;
+    for (int i = threadIdx.x; i < TG::NPT; i += blockDim.x) tl[i] = (R)0;
+    pt.fill(false);
+    __syncthreads();
+    const int tile = blockIdx.x, b = blockIdx.y;
+    const int ta0 = (tile % t.nta) * TG::T, tb0 = ((tile / t.nta) % t.ntb) * TG::T, tc0 = (tile / (t.nta * t.ntb)) * TG::T;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int la8 = lane & 7, lb4 = lane >> 3;
+    const int n = min(t.cnt[b * t.ntile + tile], t.cap);
+    const int *list = t.bin + ((size_t)b * t.ntile + tile) * t.cap;
+    R *g = (R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
+    int4 hn = make_int4(0, 0, 0, 0);
+    R4 fn = {};
+    if (warp < n) {
+        const int idx = list[warp];
+        hn = a.rhead[idx];
+        fn = load_frac<R>(a.rw, idx);
+    }
+    for (int e = warp; e < n; e += nwarp) {
+        const int4 h = hn;
+        const R4 fr = fn;
+        if (e + nwarp < n) {
+            const int idx = list[e + nwarp];
+            hn = a.rhead[idx];
+            fn = load_frac<R>(a.rw, idx);
+        }
+        SpreadW<R, NI> w;
+        w.eval(pt, fr, lane);
+        const R q = fr.w;
+        const int oa = h.y - ta0, ob = h.z - tb0, oc = h.w - tc0;
+        if (oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T) {
+            R *base = tl + (oc * TG::E + ob + lb4) * TG::PA + oa + la8;
+#pragma unroll
+            for (int s = 0; s < SpreadW<R, NI>::NSA; s++) {
+                if (la8 + 8 * s >= NI) break;
+                const R qa = q * w.wa[s];
+#pragma unroll
+                for (int tc = 0; tc < NI; tc++) {
+                    const R cq = qa * w.mc[tc];
+#pragma unroll
+                    for (int i = 0; i < NTB; i++)
+                        if (lb4 + 4 * i < NI) atomicAdd(base + (tc * TG::E + 4 * i) * TG::PA + 8 * s, cq * w.mb[i]);
+                }
+            }
+        } else {
+            spread_warp_global<R, NI>(a, g, h.y, h.z, h.w, w, q, lane);
+        }
+    }
+    // overflow records: one warp each, straight into the grid
+    const int nov = t.cnt[a.P * t.ntile];
+    const int gid = blockIdx.y * gridDim.x + blockIdx.x, nblk = gridDim.x * gridDim.y;
+    for (int e = gid * nwarp + warp; e < nov; e += nblk * nwarp) {
+        const int idx = t.ovf[e];
+        const int4 h = a.rhead[idx];
+        const R4 fr = load_frac<R>(a.rw, idx);
+        SpreadW<R, NI> w;
+        w.eval(pt, fr, lane);
+        R *g2 = (R *)a.grid + (size_t)(idx % a.P) * a.Na * a.Nb * a.Nc;
+        spread_warp_global<R, NI>(a, g2, h.y, h.z, h.w, w, fr.w, lane);
+    }
+    __syncthreads();
+    constexpr int NROW = TG::E * TG::E;
+    if (sizeof(R) == 4 && (a.Na & 3) == 0) {
+        constexpr int NQ = TG::PA / 4;
+        constexpr int RPI = 32 / NQ;
+        for (int r0 = warp * RPI; r0 < NROW; r0 += nwarp * RPI) {
+            const int row = r0 + lane / NQ, q4 = lane % NQ;
+            if (lane >= RPI * NQ || row >= NROW) continue;
+            const float4 v = ((const float4 *)tl)[row * NQ + q4];
+            if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
+            const int cz = row / TG::E, by = row - cz * TG::E;
+            const int gc = wrapi(tc0 + cz, a.Nc), gb = wrapi(tb0 + by, a.Nb), ga = wrapi(ta0 + 4 * q4, a.Na);
+            atomicAdd((float4 *)((float *)g + ((size_t)gc * a.Nb + gb) * a.Na + ga), v);
+        }
+    } else {
+        for (int row = warp; row < NROW; row += nwarp) {
+            const int cz = row / TG::E, by = row - cz * TG::E;
+            R *dst = g + ((size_t)wrapi(tc0 + cz, a.Nc) * a.Nb + wrapi(tb0 + by, a.Nb)) * a.Na;
+            for (int ax = lane; ax < TG::E; ax += 32) {
+                const R v = tl[row * TG::PA + ax];
+                if (v != (R)0) atomicAdd(dst + wrapi(ta0 + ax, a.Na), v);
+            }
+        }
+    }
+}
+
+// Gather weights of one record for lane l8 of an 8-lane group: its a
+// points (l8, l8 + 8) with derivatives, and all b and c points, evaluated by
+// lane t % 8 of the group and shuffled.  Every lane of the warp calls it.
+template <typename R, int NI>
+__device__ __forceinline__ void gather_weights(const PolyTab<R, NI> &pt, const typename Vec4<R>::T &fr, int l8,
+                                               LaneW<R, NI, true> &lw)
+{
+    const bool t0 = l8 < NI, t1 = NI > 8 && l8 + 8 < NI;
+    const int p0 = NI - 1 - (t0 ? l8 : 0), p1 = NI - 1 - (t1 ? l8 + 8 : 0);
+    lw.wa0 = t0 ? poly_eval<R, NI>(pt.m[p0], fr.x) : (R)0;
+    lw.da0 = t0 ? poly_eval<R, NI>(pt.dm[p0], fr.x) : (R)0;
+    lw.wa1 = t1 ? poly_eval<R, NI>(pt.m[p1], fr.x) : (R)0;
+    lw.da1 = t1 ? poly_eval<R, NI>(pt.dm[p1], fr.x) : (R)0;
+    R ob[2], odb[2], oc[2], odc[2];
+    ob[0] = t0 ? poly_eval<R, NI>(pt.m[p0], fr.y) : (R)0;
+    odb[0] = t0 ? poly_eval<R, NI>(pt.dm[p0], fr.y) : (R)0;
+    oc[0] = t0 ? poly_eval<R, NI>(pt.m[p0], fr.z) : (R)0;
+    odc[0] = t0 ? poly_eval<R, NI>(pt.dm[p0], fr.z) : (R)0;
+    ob[1] = t1 ? poly_eval<R, NI>(pt.m[p1], fr.y) : (R)0;
+    odb[1] = t1 ? poly_eval<R, NI>(pt.dm[p1], fr.y) : (R)0;
+    oc[1] = t1 ? poly_eval<R, NI>(pt.m[p1], fr.z) : (R)0;
+    odc[1] = t1 ? poly_eval<R, NI>(pt.dm[p1], fr.z) : (R)0;
+#pragma unroll
+    for (int s = 0; s < RecGeom<NI>::NIP; s++) {
+        if (s >= NI) {
+            lw.mb[s] = lw.mc[s] = lw.db[s] = lw.dc[s] = (R)0;
+            continue;
+        }
+        const int h = s >= 8 ? 1 : 0;
+        lw.mb[s] = __shfl_sync(0xffffffffu, ob[h], s & 7, 8);
+        lw.db[s] = __shfl_sync(0xffffffffu, odb[h], s & 7, 8);
+        lw.mc[s] = __shfl_sync(0xffffffffu, oc[h], s & 7, 8);
+        lw.dc[s] = __shfl_sync(0xffffffffu, odc[h], s & 7, 8);
+    }
+}
+
+// Gather of the compact path: as gather_tile_kernel (one block per (tile,
+// bead), the tile's potential copied to shared memory once, 8 lanes per
+// record), with the weights evaluated in the block and the next record
+// read ahead.
+template <typename R, int NI, int TT>
+__global__ void __launch_bounds__(256) gather_tile_c_kernel(PmeArgs a, Cell cell, TileArgs t)
+{
+    typedef TileGeom<NI, TT> TG;
+    typedef typename Vec4<R>::T R4;
+    extern __shared__ unsigned char smem_raw[];
+    R *tl = (R *)smem_raw;
+    __shared__ __align__(16) PolyTab<R, NI> pt;
+    pt.fill(true);
+    const int tile = blockIdx.x, b = blockIdx.y;
+    const int ta0 = (tile % t.nta) * TG::T, tb0 = ((tile / t.nta) % t.ntb) * TG::T, tc0 = (tile / (t.nta * t.ntb)) * TG::T;
+    const R *g = (const R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
+    const int n = min(t.cnt[b * t.ntile + tile], t.cap);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    if (n > 0) {
+        constexpr int NROW = TG::E * TG::E;
+        if (sizeof(R) == 4 && (a.Na & 3) == 0) {
+            constexpr int NQ = TG::PA / 4;
+            constexpr int RPI = 32 / NQ;
+            for (int r0 = warp * RPI; r0 < NROW; r0 += nwarp * RPI) {
+                const int row = r0 + lane / NQ, q4 = lane % NQ;
+                if (lane >= RPI * NQ || row >= NROW) continue;
+                const int cz = row / TG::E, by = row - cz * TG::E;
+                const float *src = (const float *)g +
+                                   ((size_t)wrapi(tc0 + cz, a.Nc) * a.Nb + wrapi(tb0 + by, a.Nb)) * a.Na +
+                                   wrapi(ta0 + 4 * q4, a.Na);
+                ((float4 *)tl)[row * NQ + q4] = __ldg((const float4 *)src);
+            }
+        } else {
+            for (int row = warp; row < NROW; row += nwarp) {
+                const int cz = row / TG::E, by = row - cz * TG::E;
+                const R *src = g + ((size_t)wrapi(tc0 + cz, a.Nc) * a.Nb + wrapi(tb0 + by, a.Nb)) * a.Na;
+                for (int ax = lane; ax < TG::PA; ax += 32)
+                    tl[row * TG::PA + ax] = ax < TG::E ? src[wrapi(ta0 + ax, a.Na)] : (R)0;
+            }
+        }
+    }
+    __syncthreads();
+    const int grp = threadIdx.x >> 3, l8 = threadIdx.x & 7, ngrp = blockDim.x >> 3;
+    const int *list = t.bin + ((size_t)b * t.ntile + tile) * t.cap;
+    const int nr = (n + ngrp - 1) / ngrp;  // same trip count in every group of a warp (shuffles)
+    int4 hn = make_int4(0, 0, 0, 0);
+    R4 fn = {};
+    int in = 0;
+    if (grp < n) {
+        in = list[grp];
+        hn = a.rhead[in];
+        fn = load_frac<R>(a.rw, in);
+    }
+    for (int r = 0; r < nr; r++) {
+        const int e = r * ngrp + grp;
+        const bool act = e < n;
+        const int idx = in;
+        const int4 h = hn;
+        const R4 fr = fn;
+        if (e + ngrp < n) {
+            in = list[e + ngrp];
+            hn = a.rhead[in];
+            fn = load_frac<R>(a.rw, in);
+        }
+        LaneW<R, NI, true> lw;
+        gather_weights<R, NI>(pt, fr, l8, lw);
+        double ea = 0, eb = 0, ec = 0;
+        if (act) {
+            const int oa = h.y - ta0, ob = h.z - tb0, oc = h.w - tc0;
+            if (oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T) {
+                const R *base = tl + (oc * TG::E + ob) * TG::PA + oa;
+                gather_lane<R, NI>([&](int tc, int tb, int ta) { return base[(tc * TG::E + tb) * TG::PA + ta]; }, lw,
+                                   l8, ea, eb, ec);
+            } else {
+                gather_lane<R, NI>(
+                    [&](int tc, int tb, int ta) {
+                        return g[((size_t)wrapi(h.w + tc, a.Nc) * a.Nb + wrapi(h.z + tb, a.Nb)) * a.Na +
+                                 wrapi(h.y + ta, a.Na)];
+                    },
+                    lw, l8, ea, eb, ec);
+            }
+        }
+        gather_store(a, cell, h.x, idx, ea, eb, ec, act ? l8 : 1);
+    }
+    const int nov = t.cnt[a.P * t.ntile];
+    const int gid = blockIdx.y * gridDim.x + blockIdx.x, nblk = gridDim.x * gridDim.y;
+    const int nr2 = (nov + nblk * ngrp - 1) / (nblk * ngrp);
+    for (int r = 0; r < nr2; r++) {
+        const int e = (r * nblk + gid) * ngrp + grp;
+        const bool act = e < nov;
+        int idx = 0;
+        int4 h = make_int4(0, 0, 0, 0);
+        R4 fr = {};
+        if (act) {
+            idx = t.ovf[e];
+            h = a.rhead[idx];
+            fr = load_frac<R>(a.rw, idx);
+        }
+        LaneW<R, NI, true> lw;
+        gather_weights<R, NI>(pt, fr, l8, lw);
+        double ea = 0, eb = 0, ec = 0;
+        if (act) {
+            const R *g2 = (const R *)a.grid + (size_t)(idx % a.P) * a.Na * a.Nb * a.Nc;
+            gather_lane<R, NI>(
+                [&](int tc, int tb, int ta) {
+                    return g2[((size_t)wrapi(h.w + tc, a.Nc) * a.Nb + wrapi(h.z + tb, a.Nb)) * a.Na +
+                              wrapi(h.y + ta, a.Na)];
+                },
+                lw, l8, ea, eb, ec);
+        }
+        gather_store(a, cell, h.x, idx, ea, eb, ec, act ? l8 : 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // In-place FFTs of `nl` lines of length N held in shared memory: element n of
 // line l at sm[l * ls + n * es].  Unnormalised, exp(sign 2 pi i n k / N);
 // tw[2m], tw[2m+1] = cos, sin(2 pi m / N).  Power-of-two lengths up to 256
@@ -1012,18 +1432,24 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     if (err != cudaSuccess) return err;
     const long long nt = (long long)a.nchrg * a.P;
     const int threads = 256;
-    pme_bin_kernel<R, NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell, t);
+    // the parameter adjoint reads the full weight records of the forward pass
+    const bool full = c->pme_full_records;
+    if (full) pme_bin_kernel<R, NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell, t);
+    else pme_bin_compact_kernel<R, NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell, t);
     const size_t st = (size_t)TileGeom<NI, TT>::NPT * sizeof(R), ss_spread = spread_smem<R, NI, TT>();
-    if (ss_spread > 48 * 1024) {
+    if (ss_spread > 48 * 1024 - sizeof(PolyTab<R, NI>)) {
         err = smem_optin((const void *)spread_tile_kernel<R, NI, TT>, (int)ss_spread);
+        if (err == cudaSuccess) err = smem_optin((const void *)spread_tile_c_kernel<R, NI, TT>, (int)ss_spread);
         if (err != cudaSuccess) return err;
     }
-    if (st > 48 * 1024) {
+    if (st > 48 * 1024 - sizeof(PolyTab<R, NI>)) {
         err = smem_optin((const void *)gather_tile_kernel<R, NI, TT>, (int)st);
+        if (err == cudaSuccess) err = smem_optin((const void *)gather_tile_c_kernel<R, NI, TT>, (int)st);
         if (err != cudaSuccess) return err;
     }
     const dim3 tgrid((unsigned)t.ntile, (unsigned)a.P);
-    spread_tile_kernel<R, NI, TT><<<tgrid, 256, ss_spread, c->stream>>>(a, t);
+    if (full) spread_tile_kernel<R, NI, TT><<<tgrid, 256, ss_spread, c->stream>>>(a, t);
+    else spread_tile_c_kernel<R, NI, TT><<<tgrid, 256, ss_spread, c->stream>>>(a, t);
     const R *twbase = (const R *)(f64 ? (const void *)c->d_twiddle64 : (const void *)c->d_twiddle32);
     const R *tw[3] = {twbase, twbase + 2 * 256, twbase + 4 * 256};
     const size_t sp = pme_plane_smem(a.Na, a.Nb, f64), ss = pme_slab_smem(a.Na, a.Nc, f64);
@@ -1038,7 +1464,8 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     default: err = launch_fft_t<R, 0>(c, a, cell, spec, filt, tw, sp, ss, energy); break;
     }
     if (err != cudaSuccess) return err;
-    gather_tile_kernel<R, NI, TT><<<tgrid, 256, st, c->stream>>>(a, cell, t);
+    if (full) gather_tile_kernel<R, NI, TT><<<tgrid, 256, st, c->stream>>>(a, cell, t);
+    else gather_tile_c_kernel<R, NI, TT><<<tgrid, 256, st, c->stream>>>(a, cell, t);
     return cudaGetLastError();
 }
 
