@@ -80,6 +80,101 @@ def peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
+def cpu_info():
+    """Host CPU model and logical core count (for the CPU baselines)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "host_cores": os.cpu_count()}
+
+
+def piny_golden(name):
+    """PINY's own evaluation of a benchmark box, when tests/golden holds it:
+    (fixture, bead positions and mode-1 positions PINY used, in Bohr) --
+    the seeded generator's positions moved by the stored ulp offsets."""
+    from piny_b200 import water
+    path = os.path.join(ROOT, "tests", "golden", name + ".npz")
+    if not os.path.exists(path):
+        return None
+    F = dict(np.load(path))
+    if "pos" in F:  # a fixture that holds the positions themselves (every bead)
+        F["ref_beads"] = np.arange(F["pos"].shape[0])
+        return F, F["pos"], F.get("xmod")
+    gen = water.build_positions(water.named_spec(name)) / water.BOHR
+    pos = (gen.view(np.int64) + F["pos_ulp"].astype(np.int64)).view(np.float64)
+    xmod = None
+    if "xmod_ulp" in F:
+        xmod = (gen.mean(axis=0).view(np.int64) + F["xmod_ulp"].astype(np.int64)).view(np.float64)
+    return F, pos, xmod
+
+
+def kernel_bytes(S, P, precision, npairs, nmolp):
+    """Algorithmic bytes of one launch of each kernel of an evaluation (all
+    P beads): what the kernel must read and write at least, given the data
+    layout (FP64 positions and forces [site][xyz][bead]; a real PME grid of
+    4 (MIXED) or 8 (FP64) bytes per point; half spectrum; per (charge, bead)
+    PME records of 32 / 48 bytes plus a 4-byte bin entry)."""
+    N, G = int(S["natm"]), int(S["ngrid_a"]) * int(S["ngrid_b"]) * int(S["ngrid_c"])
+    nq = int(np.count_nonzero(S["charge"]))
+    rb = 4 if precision == "mixed" else 8
+    rec = 32 if precision == "mixed" else 48
+    nrec = nq * P
+    spec = (int(S["ngrid_a"]) // 2 + 1) * int(S["ngrid_b"]) * int(S["ngrid_c"]) * 2 * rb * P
+    nb, nbe, nec = int(S.get("nbond", 0)), int(S.get("nbend", 0)), int(S.get("necor", 0))
+    return {
+        "transpose_in": 48.0 * N * P,
+        "ghost_pos": 96.0 * int(S.get("nghost", 0)) * P,
+        # positions in, forces out, the shared list once (the scope table's pair figure)
+        "pair": 48.0 * N * P + 4.0 * npairs,
+        "pme_grid_clear (memset)": float(G * P * rb),
+        "pme_bin": nrec * (24.0 + rec + 4.0),
+        "pme_spread": nrec * (rec + 4.0) + G * P * rb,
+        "pme_plane_fwd": float(G * P * rb + spec),
+        "pme_conv_c": 2.0 * spec,
+        "pme_plane_inv": float(spec + G * P * rb),
+        "pme_gather": G * P * rb + nrec * (rec + 4.0 + 24.0),
+        "pme_force_add": 72.0 * nrec,
+        "intra (bond, bend, ecor)": 72.0 * P * (2 * nb + 3 * nbe + 2 * nec),
+        "transpose_out": 48.0 * N * P,
+    }
+
+
+def kernel_profile(box, step, S, P, precision, npairs, nmolp, flush, stream, reps=5):
+    """Serialised per-kernel times of `reps` evaluations (CUDA events after
+    every kernel, pinyb200_set_kernel_timing; L2 flushed before each), the
+    median per kernel with its algorithmic bytes and HBM fraction."""
+    import torch
+    hbm, _ = peaks()
+    box.set_kernel_timing(True)
+    step()
+    torch.cuda.synchronize()
+    runs = []
+    for _ in range(reps):
+        flush.zero_()
+        step()
+        torch.cuda.synchronize()
+        runs.append(box.kernel_times())
+    box.set_kernel_timing(False)
+    kb = kernel_bytes(S, P, precision, npairs, nmolp)
+    out = []
+    for i, (name, _) in enumerate(runs[0]):
+        ms = float(np.median([r[i][1] for r in runs]))
+        b = kb.get(name)
+        gbs = b / (ms * 1e-3) / 1e9 if b and ms > 0 else None
+        out.append({"kernel": name, "ms": ms, "algorithmic_bytes": b, "achieved_GBs": gbs,
+                    "hbm_frac": gbs / hbm if gbs else None})
+    tot = sum(k["ms"] for k in out)
+    for k in out:
+        k["share"] = k["ms"] / tot if tot > 0 else None
+    return out
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
 
@@ -166,6 +261,36 @@ def time_piny_cpu(spec, pos_A, nproc, beads_per_proc, reps):
     return nproc * beads_per_proc / step_s, step_s
 
 
+def piny_bead_seconds(specs, reps=3, workers=None):
+    """Seconds per bead-force evaluation of PINY's CPU path for each box of
+    `specs` (oracle/_ref/piny_ref, 1 bead, median of `reps` after its
+    warm-up), the boxes run as concurrent single-threaded processes, at most
+    `workers` (default: every host core) at a time."""
+    from piny_b200 import water
+    exe = piny_ref_binary()
+    workers = workers or (os.cpu_count() or 1)
+    tmp = tempfile.mkdtemp(prefix="piny_cpu_")
+    out = [None] * len(specs)
+    running = []
+    todo = list(range(len(specs)))
+    # largest boxes first, so the pool drains evenly
+    todo.sort(key=lambda i: -specs[i].nmol)
+    while todo or running:
+        while todo and len(running) < workers:
+            i = todo.pop(0)
+            d = os.path.join(tmp, "b%d" % i)
+            water.write_piny_input(d, specs[i], water.build_positions(specs[i]))
+            running.append((i, subprocess.Popen([exe, "time", d, "water.input", str(reps), "1"],
+                                                stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+        i, p = running.pop(0)
+        o, e = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError("piny_ref failed: " + e[-300:])
+        out[i] = float(np.median([float(l.split()[3]) for l in o.splitlines() if l.startswith("time")]))
+    shutil.rmtree(tmp, ignore_errors=True)
+    return np.array(out)
+
+
 def time_oracle_port(S, pos_bohr, xmod, beads):
     from oracle.oracle import Oracle
     O = Oracle()
@@ -176,15 +301,29 @@ def time_oracle_port(S, pos_bohr, xmod, beads):
     return beads / dt, dt
 
 
-def cpu_baseline(spec, pos_A, pos_bohr, S, xmod):
+def cpu_baseline(spec, pos_A, pos_bohr, S, xmod, reps=5):
+    """PINY's CPU path on one host core: a bounded sample of the box (at most
+    2 of its beads per step), the median of `reps` steps after one warm-up,
+    scaled per bead-force evaluation."""
+    nb = min(2, spec.nbeads)
     if piny_ref_binary():
-        rate, steps = time_piny_cpu(spec, pos_A, nproc=1, beads_per_proc=2, reps=2)
+        rate, steps = time_piny_cpu(spec, pos_A, nproc=1, beads_per_proc=nb, reps=reps)
         return {"value": float(np.median(rate)), "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": "PINY energy_control sub-steps (oracle/_ref/piny_ref), 2 of 32 beads per step, "
-                          "1 host core, median of 2 steps after 1 warm-up"}
+                "sample": "PINY energy_control sub-steps (oracle/_ref/piny_ref) on %d of %d beads per step, "
+                          "1 host core, median of %d steps after 1 warm-up" % (nb, spec.nbeads, reps),
+                "step_s": [float(x) for x in steps], **cpu_info()}
     rate, dt = time_oracle_port(S, pos_bohr, xmod, 1)
     return {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": "oracle restatement, 1 of 32 beads, 1 host core"}
+            "sample": "oracle restatement, 1 of %d beads, 1 host core" % spec.nbeads, **cpu_info()}
+
+
+def box_config(spec, args, natm, grid, npairs=None, list_s=None):
+    """The config object of a single-box line (both arms print the same)."""
+    return {"workload": args.config, "molecules": spec.nmol, "sites": natm, "beads": spec.nbeads,
+            "box_A": spec.L, "pme_grid": grid, "pme_order": spec.order, "cutoff_A": spec.cutoff,
+            "precision": args.precision, "verlet_pairs": npairs, "list_build_s": list_s,
+            "l2": "256 MiB buffer written between timed steps; per-step CUDA events on the launch stream",
+            "parallelism": "replica per GPU" if args.gpus > 1 else "single GPU"}
 
 
 def run_reference(args, ws, rank):
@@ -192,27 +331,87 @@ def run_reference(args, ws, rank):
     if rank != 0:
         return 0
     from piny_b200 import water
+    if piny_ref_binary() is not None and (args.config.startswith("c4_batch") or args.config == "c5_grad"):
+        return run_reference_sampled(args)
+    if args.config not in ("tip4pf_4096_p32", "tip4pf_1024_p16", "tip4pf_1024_p32", "spcfw_256_p1",
+                           "spcfw_256_p32", "tip4pf_256_p4", "spcfw_216_p4"):
+        print(json.dumps({"impl": "reference", "unavailable": "no PINY CPU arm for the %s workload "
+                                                              "(PINY has no device-side MD step)" % args.config}))
+        return 0
     spec = water.named_spec(args.config)
     if piny_ref_binary() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/piny_ref not built (needs the PINY "
                                                                 "sources at build time)"}))
         return 0
+    from piny_b200 import system
     pos_A = water.build_positions(spec)
+    S = system.build_system(spec, pos_A / water.BOHR)
     ncpu = os.cpu_count() or 1
     nproc = max(1, min(ncpu, spec.nbeads))
-    rate, steps = time_piny_cpu(spec, pos_A, nproc=nproc, beads_per_proc=1, reps=max(1, args.steps))
+    warm = max(3, args.warmup)
+    # piny_ref makes one warm-up evaluation itself; the rest are dropped here
+    rate, steps = time_piny_cpu(spec, pos_A, nproc=nproc, beads_per_proc=1, reps=max(1, args.steps) + warm - 1)
+    rate, steps = rate[warm - 1:], steps[warm - 1:]
     value = float(np.mean(rate))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
-        "steps": args.steps, "warmup": 1, "ms_per_step": float(np.mean(steps)) * 1e3,
+        "steps": args.steps, "warmup": warm, "ms_per_step": float(np.mean(steps)) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.config, "molecules": spec.nmol, "beads": spec.nbeads, "pme_grid": spec.grid,
-                   "pme_order": spec.order, "cutoff_A": spec.cutoff},
+        "config": box_config(spec, args, int(S["natm"]), int(S["ngrid_a"])),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "reference",
                          "sample": "%d PINY processes (oracle/_ref/piny_ref) x 1 bead per step, one per host "
-                                   "core, the box's list fixed" % nproc},
+                                   "core, the box's list fixed; a step is %d of the box's %d bead "
+                                   "evaluations" % (nproc, nproc, spec.nbeads), **cpu_info()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    print(json.dumps(line))
+    return 0
+
+
+def run_reference_sampled(args):
+    """--impl reference for the batched and the gradient workloads: PINY's
+    CPU path, one bead of each box per host process, every host core.
+    c4_batch64: per step every bead of the 64 boxes; the step time is the
+    per-bead seconds of each box times its beads, spread over the cores.
+    c5_grad: the gradient by central differences, 2 x 9 + 1 evaluations of
+    the 16-bead box per gradient, spread over the cores."""
+    from piny_b200 import system, water
+    ncpu = os.cpu_count() or 1
+    warm = max(3, args.warmup)
+    if args.config.startswith("c4_batch"):
+        nbox = int(args.config[len("c4_batch"):] or 64)
+        specs = water.c4_specs(nbox=nbox, seed=2024)
+        t = piny_bead_seconds(specs, reps=max(3, min(args.steps, 5)))
+        work = float(np.sum([sp.nbeads * t[i] for i, sp in enumerate(specs)]))
+        nbead = sum(sp.nbeads for sp in specs)
+        step_s = work / ncpu
+        value, unit = nbead / step_s, UNIT
+        metric = "bead-force evals/s (64 uneven TIP4P/F boxes, batched)"
+        sample = ("PINY (oracle/_ref/piny_ref): 1 bead of each of the %d boxes, median of its steps after a "
+                  "warm-up, boxes as concurrent single-threaded processes; a step = every bead of every box, "
+                  "the summed seconds spread over %d cores" % (nbox, ncpu))
+        cfg = {"workload": args.config, "boxes": nbox, "bead_evals_per_step": nbead,
+               "molecules": [sp.nmol for sp in specs], "beads": [sp.nbeads for sp in specs],
+               "pme_grid": [sp.grid for sp in specs], "precision": args.precision}
+    else:
+        spec = water.named_spec("tip4pf_1024_p16")
+        t = piny_bead_seconds([spec], reps=max(3, min(args.steps, 5)))[0]
+        nev = 2 * 9 + 1
+        step_s = nev * spec.nbeads * t / min(ncpu, nev * spec.nbeads)
+        value, unit = 1.0 / step_s, "gradient evals/s"
+        metric = ("parameter-gradient evals/s (9 q-TIP4P/F parameters; energy + force-matching loss; "
+                  "1024 mol x 16 beads)")
+        sample = ("PINY (oracle/_ref/piny_ref) has no gradient: central differences, %d evaluations of the "
+                  "16-bead box per gradient, from PINY's seconds per bead (median after a warm-up), spread "
+                  "over %d cores" % (nev, min(ncpu, nev * spec.nbeads)))
+        cfg = {"workload": "c5_grad", "molecules": spec.nmol, "beads": spec.nbeads, "pme_grid": spec.grid,
+               "parameters": 9}
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": 0, "steps": args.steps,
+            "warmup": warm, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": unit, "cores": ncpu, "kind": "reference", "sample": sample,
+                             **cpu_info()},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
 
@@ -290,6 +489,38 @@ def run_grad(args, ws, rank, local):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
     g_mixed = dE + dF
+    # end to end: positions in from pinned host memory, the gradient back
+    pin = torch.empty(mixed.d_pos.shape, dtype=torch.float64).pin_memory()
+    pin.copy_(mixed.d_pos.cpu())
+    e2e_ms = []
+    for k in range(args.steps + 2):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        mixed.d_pos.copy_(pin, non_blocking=True)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        if k >= 2:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e = float(np.mean(e2e_ms))
+    npairs = box.list_info()["npairs"]
+    alg = 2.0 * sum(kernel_bytes(mixed.S, spec.nbeads, args.precision, npairs, 0).values())
+    hbm, peak_kind = peaks()
+    c5_cpu = None
+    if rank == 0 and not args.no_cpu_baseline and piny_ref_binary():
+        try:
+            tb = float(piny_bead_seconds([spec], reps=5, workers=1)[0])
+            nev = 2 * len(theta) + 1
+            c5_cpu = {"value": 1.0 / (nev * spec.nbeads * tb), "unit": "gradient evals/s", "cores": 1,
+                      "kind": "reference",
+                      "sample": "PINY (oracle/_ref/piny_ref) has no gradient: central differences take %d "
+                                "evaluations of the 16-bead box; PINY's seconds per bead (1 bead, median of 5 "
+                                "after a warm-up, 1 host core) x %d" % (nev, nev * spec.nbeads),
+                      "seconds_per_bead": tb, **cpu_info()}
+        except Exception as exc:  # reported, not fatal
+            c5_cpu = {"value": None, "unit": "gradient evals/s", "cores": 1, "kind": "reference",
+                      "sample": "failed: %s" % exc}
     rel_mixed = float(np.abs(g_mixed - g64).max() / np.abs(g64).max())
     fd = None
     if getattr(args, "fd", False):
@@ -318,8 +549,19 @@ def run_grad(args, ws, rank, local):
                        "l2": "256 MiB buffer written between timed steps; CUDA events on the launch stream"},
             "gradient": {"theta": theta.tolist(), "mixed": g_mixed.tolist(), "fp64": g64.tolist(),
                          "max_rel_mixed_vs_fp64": rel_mixed, "finite_differences_fp64": fd},
-            "roofline": None, "cpu_baseline": None, "e2e": None,
-            "gpu_launches": None, "clocks": clocks,
+            "roofline": {"bound": "hbm", "kernel": "gradient step (forward evaluation + adjoint)",
+                         "achieved": alg / (ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": alg / (ms * 1e-3) / 1e9 / hbm, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg,
+                         "bytes_model": "twice the forward evaluation's per-kernel algorithmic bytes (the adjoint "
+                                        "re-reads positions, list, grid and records the same way)"},
+            "cpu_baseline": c5_cpu,
+            "e2e": {"value": ws * 1e3 / e2e, "unit": "gradient evals/s",
+                    "h2d_bytes_per_step": int(pin.numel() * 8), "d2h_bytes_per_step": int(2 * len(theta) * 8),
+                    "ms_per_step": e2e},
+            # forward evaluation, then u, ghost, pair, ecor, bond, bend adjoint
+            # kernels and the PME adjoint (dipole spread, 3 FFT kernels, gather)
+            "gpu_launches": (box_launches(mixed.S, spec.nbeads) + 12) * args.steps, "clocks": clocks,
         }
         print(json.dumps(line))
     f64.close()
@@ -712,6 +954,17 @@ def run_batch(args, ws, rank, local):
     hbm, peak_kind = peaks()
     achieved = alg / (ms * 1e-3) / 1e9
     nbytes = sum(int(p[0].numel()) * 8 for p in pins)
+    c4_cpu = None
+    if rank == 0 and not args.no_cpu_baseline and piny_ref_binary():
+        try:
+            t = piny_bead_seconds(specs, reps=3)
+            c4_cpu = {"value": float(nbead / np.sum([sp.nbeads * t[i] for i, sp in enumerate(specs)])),
+                      "unit": UNIT, "cores": 1, "kind": "reference",
+                      "sample": "PINY (oracle/_ref/piny_ref): 1 bead of each of the %d boxes, median of 3 after "
+                                "a warm-up (boxes run as concurrent single-threaded processes); a step = every "
+                                "bead of every box on one core" % nbox, **cpu_info()}
+        except Exception as exc:  # reported, not fatal
+            c4_cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": "failed: %s" % exc}
     if rank == 0:
         line = {
             "metric": "bead-force evals/s (64 uneven TIP4P/F boxes, batched)", "value": value, "unit": UNIT,
@@ -729,7 +982,7 @@ def run_batch(args, ws, rank, local):
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg,
                          "bytes_model": "per bead-eval 48 B/site + 4 B x list/P + 6 grid passes"},
-            "cpu_baseline": None,
+            "cpu_baseline": c4_cpu,
             "e2e": {"value": ws * nbead / (e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "ms_per_step": e2e},
             "gpu_launches": nkern * args.steps,
@@ -880,32 +1133,59 @@ def main():
     h2d = pos.nbytes + xmod.nbytes
     d2h = pos.nbytes + C.sizeof(PinyEnergies)
 
-    # roofline of the dominant kernel phase
+    # every kernel serialised (events after each), with its HBM fraction
+    linfo = box.list_info()
+    kernels = kernel_profile(box, lambda: step(box, d_force), S, P, args.precision, npairs,
+                             linfo.get("nmol_pairs", 0), flush, stream)
+    # roofline of the dominant kernel by serialised time; its duration is
+    # the one measured inside the timed steps (pair phase events / PME phase)
     hbm, peak_kind = peaks()
     names = ["total", "pair", "pme", "intra"]
-    dom = 1 if phase[1] >= phase[2] else 2
-    G = S["ngrid_a"] * S["ngrid_b"] * S["ngrid_c"]
-    nq = int(np.count_nonzero(S["charge"]))
-    bg = 8 if args.precision == "mixed" else 16
-    if dom == 1:
-        # positions in + forces out for all beads, the active pair list once
-        alg_bytes = 48.0 * natm * P + 4.0 * box.list_info()["nactive"] + 4.0 * (natm + 1)
-        unit_note = "48 B/site/bead (FP64 positions + forces) + 4 B per active list pair"
+    dom_k = max(kernels, key=lambda k: k["ms"])
+    pme_ms = sum(k["ms"] for k in kernels if k["kernel"].startswith("pme_"))
+    if dom_k["kernel"] == "pair" or dom_k["ms"] >= pme_ms:
+        # the scope table's per bead-eval figure for the pair kernel:
+        # 48 B/site (FP64 positions in, forces out) + 4 B x list pairs / P
+        alg_bytes = 48.0 * natm * P + 4.0 * npairs
+        dom_name, dom_ms = "pair", float(phase[1])
+        unit_note = "48 B/site/bead (FP64 positions + forces) + 4 B per Verlet-list pair per launch"
     else:
-        alg_bytes = P * (6.0 * G * bg + 24.0 * nq * 2)
-        unit_note = "per bead 6 grid passes x %d B/point + charge positions in and forces out" % bg
-    achieved = alg_bytes / (phase[dom] * 1e-3) / 1e9
+        G = S["ngrid_a"] * S["ngrid_b"] * S["ngrid_c"]
+        bg = 8 if args.precision == "mixed" else 16
+        alg_bytes = P * 6.0 * G * bg
+        dom_name, dom_ms = "pme phase", float(phase[2])
+        unit_note = "per bead 6 grid passes x %d B/point" % bg
+    achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get("%s_%s_%s" % (args.config, args.precision, names[dom]))
+            traffic = json.load(open(tf)).get("%s_%s_%s" % (args.config, args.precision, dom_name.split()[0]))
         except Exception:
             traffic = None
-    roof = {"bound": "hbm", "kernel": names[dom] + " phase", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+    roof = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
             "algorithmic_bytes_per_launch": alg_bytes, "bytes_model": unit_note,
+            "duration_ms": dom_ms, "duration_from": "pair-phase CUDA events of the timed steps (PME concurrent)"
+            if dom_name == "pair" else "PME-phase CUDA events of the timed steps",
             "phase_ms": {names[i]: float(phase[i]) for i in range(4)}}
+
+    # against PINY itself: forces of the beads PINY's evaluation of this
+    # box stored (tests/golden), device run on the positions PINY used
+    piny = None
+    gold = piny_golden(args.config)
+    if gold is not None:
+        F, gpos, gxm = gold
+        piny = {"beads": [int(b) for b in F["ref_beads"]], "npairs_piny": int(F["npairs"])}
+        for prec in ("mixed", "fp64"):
+            bx = DeviceBox(S, P, prec)
+            bx.build_list(gpos[0], gxm, F["hmat"], F["cutskin2"])
+            fg, eg = bx.energy_force(gpos, gxm, F["hmat"])
+            ref = F["ref_force_raw"]
+            piny["force_rel_rms_%s" % prec] = float(np.linalg.norm(fg[F["ref_beads"]] - ref) / np.linalg.norm(ref))
+            piny["vintert_rel_%s" % prec] = float(abs(eg["vintert"] - F["ref_vintert"]) / abs(F["ref_vintert"]))
+            piny["npairs_%s" % prec] = int(bx.list_info()["npairs"])
+            bx.close()
     # the bound that applies to the pair kernel: FP32 issue, not HBM
     alu = None
     try:
@@ -934,12 +1214,10 @@ def main():
             "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64acc" if args.precision == "mixed" else "f64",
             "data": "synthetic",
-            "config": {"workload": args.config, "molecules": spec.nmol, "sites": natm, "beads": P,
-                       "box_A": spec.L, "pme_grid": S["ngrid_a"], "pme_order": spec.order, "cutoff_A": spec.cutoff,
-                       "precision": args.precision, "verlet_pairs": int(npairs), "list_build_s": list_s,
-                       "l2": "256 MiB buffer written between timed steps; per-step CUDA events on the launch stream",
-                       "parallelism": "replica per GPU" if ws > 1 else "single GPU"},
+            "config": box_config(spec, args, int(natm), int(S["ngrid_a"]), int(npairs), list_s),
             "roofline": roof,
+            "kernels": kernels,
+            "vs_piny": piny,
             "alu_roofline": alu,
             "cpu_baseline": cpu,
             "e2e": {"value": ws * P / (e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),

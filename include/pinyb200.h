@@ -451,6 +451,16 @@ int pinyb200_grad(pinyb200_ctx *ctx, const double *d_pos, const double *d_xmod,
  * the context, concurrently with 1 and 3, so 1 + 2 + 3 may exceed 0. */
 int pinyb200_last_timing(pinyb200_ctx *ctx, float *ms, int n);
 
+/* Per-kernel timing, for measurement.  With on != 0 every later evaluation
+ * of the context runs its kernels one after another on the context's
+ * stream (PME not overlapped) with a CUDA event after each kernel;
+ * pinyb200_kernel_times returns, for the last evaluation, the kernels in
+ * launch order (names[i], static strings) and their milliseconds ms[i],
+ * at most cap of them, their number in *count.  No counterpart in PINY
+ * (its timer.c brackets whole routines on the host). */
+int pinyb200_set_kernel_timing(pinyb200_ctx *ctx, int on);
+int pinyb200_kernel_times(pinyb200_ctx *ctx, const char **names, float *ms, int cap, int *count);
+
 /* FMA throughput of the current GPU in GFLOP/s (fp64 = 0: FP32, 1: FP64),
  * best of `reps` timed launches of a register-only probe: the ALU peak the
  * benchmark's roofline divides by.  No counterpart in PINY. */

@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -273,6 +274,8 @@ int pinyb200_destroy(pinyb200_ctx *c)
                     c->d_colR, c->d_rtot, c->d_xm0, c->d_cs0, c->d_ecor_res_tab, c->d_cs_in};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    for (cudaEvent_t e : c->kt_ev) cudaEventDestroy(e);
+    if (c->eg_exec) cudaGraphExecDestroy(c->eg_exec);
     if (c->h_acc_pin) cudaFreeHost(c->h_acc_pin);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -695,11 +698,13 @@ int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, boo
 {
     const bool energy = !(flags & PINYB200_NO_ENERGY);
     const size_t nb = (size_t)c->sys.natm * 3 * c->P;
-    if (timing) CK(cudaEventRecord(c->ev[0], c->stream));
+    if (timing) CK(ev_rec(c->ev[0], c->stream));
+    if (c->kt_n == 0) CK(kt_mark(c, nullptr));
     CK(launch_ghost_pos(c));
+    CK(kt_mark(c, "ghost_pos"));
     CK(cudaMemsetAsync(c->d_forceT, 0, nb * sizeof(double), c->stream));
     CK(cudaMemsetAsync(c->d_acc, 0, (size_t)c->P * S_NSLOT * sizeof(double), c->stream));
-    if (timing) CK(cudaEventRecord(c->ev[1], c->stream));
+    if (timing) CK(ev_rec(c->ev[1], c->stream));
     // PME on its own stream, concurrently with the pair and intramolecular
     // kernels: it reads the positions, writes its own force buffer and adds
     // its energies and virial atomically
@@ -707,10 +712,10 @@ int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, boo
     CK(cudaStreamWaitEvent(c->pme_stream, c->ev_fork, 0));
     {
         cudaStream_t main_stream = c->stream;
-        if (c->pme_overlap) c->stream = c->pme_stream;
-        cudaError_t perr = timing ? cudaEventRecord(c->ev_pme[0], c->stream) : cudaSuccess;
+        if (c->pme_overlap && !c->kt_on) c->stream = c->pme_stream;
+        cudaError_t perr = timing ? ev_rec(c->ev_pme[0], c->stream) : cudaSuccess;
         if (perr == cudaSuccess) perr = launch_pme(c, cell, energy);
-        if (perr == cudaSuccess && timing) perr = cudaEventRecord(c->ev_pme[1], c->stream);
+        if (perr == cudaSuccess && timing) perr = ev_rec(c->ev_pme[1], c->stream);
         if (perr == cudaSuccess) perr = cudaEventRecord(c->ev_join, c->stream);
         c->stream = main_stream;
         CK(perr);
@@ -722,6 +727,7 @@ int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, boo
     else if (c->use_mol && c->mol_ok && ortho && c->pair_variant != 1 && !(flags & PINYB200_SITE_PAIRS))
         CK(launch_mol_pair(c, cell, energy));
     else CK(launch_pair(c, cell, energy));
+    CK(kt_mark(c, "pair"));
     if (respa_w) {
         // RESPA outer level: the weighted pair forces from the plain ones
         // (so far the only forces in the buffer) and the switched pairs
@@ -729,21 +735,23 @@ int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, boo
         CK(launch_respa_scale_copy(c, c->r_wter, respa_w));
         if (c->r_int_res_ter) CK(launch_pair_respa(c, cell, 4, respa_w));
     }
-    if (timing) CK(cudaEventRecord(c->ev[2], c->stream));
+    if (timing) CK(ev_rec(c->ev[2], c->stream));
     CK(launch_intra(c, cell, energy));
+    CK(kt_mark(c, "intra (bond, bend, ecor)"));
     if (respa_w) {
         CK(launch_intra_respa(c, true, respa_w));
         CK(launch_ecor_weighted(c, c->r_wter, respa_w, c->r_kres ? 2 : 0));
     }
-    if (timing) CK(cudaEventRecord(c->ev[3], c->stream));
+    if (timing) CK(ev_rec(c->ev[3], c->stream));
     CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     CK(launch_pme_force_add(c));
+    CK(kt_mark(c, "pme_force_add"));
     if (respa_w) CK(launch_pme_force_add_scaled(c, c->r_kres ? c->r_wter_res : c->r_wter, respa_w));
     if (flags & PINYB200_DISTRIB_GHOSTS) {
         CK(launch_ghost_distrib(c));
         if (respa_w) CK(launch_ghost_distrib(c, respa_w));
     }
-    if (timing) CK(cudaEventRecord(c->ev[4], c->stream));
+    if (timing) CK(ev_rec(c->ev[4], c->stream));
     if (energy && h_acc)
         CK(cudaMemcpyAsync(h_acc, c->d_acc, (size_t)c->P * S_NSLOT * sizeof(double), cudaMemcpyDeviceToHost,
                            c->stream));
@@ -807,11 +815,15 @@ __global__ void centroid_kernel(const double *__restrict__ posT, double *__restr
 int pinyb200::enqueue_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const Cell &cell, int flags,
                              double *d_force, bool timing, double *h_acc)
 {
+    c->kt_n = 0;
+    CK(kt_mark(c, nullptr));
     int rc = stage_positions(c, d_pos, d_xmod, cell, flags);
     if (rc) return rc;
+    CK(kt_mark(c, "transpose_in"));
     rc = evaluate_enqueue(c, cell, flags, timing, h_acc);
     if (rc) return rc;
     CK(launch_transpose_out(c, d_force));
+    CK(kt_mark(c, "transpose_out"));
     return PINYB200_OK;
 }
 
@@ -841,6 +853,56 @@ int pinyb200::stage_positions(pinyb200_ctx *c, const double *d_pos, const double
     return PINYB200_OK;
 }
 
+// One evaluation enqueued through the context's cached CUDA graph.  A call
+// whose key (pointers, stream, flags, cell, context generation) equals the
+// previous call's replays one graph launch instead of ~15 kernel launches
+// from the host: the first call with a key runs the work plainly (it sets
+// kernel attributes and builds the influence function outside any
+// capture), the second captures and launches it, later ones launch it.
+// Per-kernel timing runs plainly.
+static int run_eval_graph(pinyb200_ctx *c, const std::vector<double> &key, const std::function<int()> &body)
+{
+    if (c->kt_on || c->no_graph) return body();
+    if (c->eg_exec && key == c->eg_key) {
+        CK(cudaGraphLaunch(c->eg_exec, c->stream));
+        return PINYB200_OK;
+    }
+    if (key != c->eg_seen) {
+        c->eg_seen = key;
+        return body();
+    }
+    if (c->eg_exec) cudaGraphExecDestroy(c->eg_exec);
+    c->eg_exec = nullptr;
+    c->eg_key.clear();
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ec != cudaSuccess) return fail(c, PINYB200_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+    const cudaError_t ei = cudaGraphInstantiate(&c->eg_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        c->eg_exec = nullptr;
+        return fail(c, PINYB200_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    }
+    c->eg_key = key;
+    CK(cudaGraphLaunch(c->eg_exec, c->stream));
+    return PINYB200_OK;
+}
+
+static std::vector<double> eval_key(pinyb200_ctx *c, int entry, const void *a, const void *b, const void *d,
+                                    const double *hmat, int flags)
+{
+    std::vector<double> k = {(double)entry, (double)(uintptr_t)a, (double)(uintptr_t)b, (double)(uintptr_t)d,
+                             (double)(uintptr_t)c->stream, (double)flags, (double)c->gen};
+    for (int i = 0; i < 9; i++) k.push_back(hmat[i]);
+    return k;
+}
+
 extern "C" {
 
 int pinyb200_energy_force_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, const double *hmat,
@@ -859,15 +921,17 @@ int pinyb200_energy_force_device(pinyb200_ctx *c, const double *d_pos, const dou
     } restore{c, own};
     Cell cell = make_cell(hmat);
     const bool energy = !(flags & PINYB200_NO_ENERGY);
-    std::vector<double> acc(energy ? (size_t)c->P * S_NSLOT : 0);
-    int rc = enqueue_device(c, d_pos, d_xmod, cell, flags, d_force, true, energy ? acc.data() : nullptr);
+    if (energy && !c->h_acc_pin) CK(cudaMallocHost(&c->h_acc_pin, (size_t)c->P * S_NSLOT * sizeof(double)));
+    double *acc = energy ? c->h_acc_pin : nullptr;  // pinned: the copy can sit in the graph
+    int rc = run_eval_graph(c, eval_key(c, 1, d_pos, d_xmod, d_force, hmat, flags),
+                            [&]() { return enqueue_device(c, d_pos, d_xmod, cell, flags, d_force, true, acc); });
     if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream));
     CK(cudaEventElapsedTime(&c->last_ms[0], c->ev[0], c->ev[4]));
     CK(cudaEventElapsedTime(&c->last_ms[1], c->ev[1], c->ev[2]));
     CK(cudaEventElapsedTime(&c->last_ms[2], c->ev_pme[0], c->ev_pme[1]));
     CK(cudaEventElapsedTime(&c->last_ms[3], c->ev[2], c->ev[3]));
-    evaluate_finish(c, cell, flags, energy ? acc.data() : nullptr, e);
+    evaluate_finish(c, cell, flags, acc, e);
     if (energy && e && !std::isfinite(e->vintert + e->vintrat))
         return fail(c, PINYB200_ERR_NAN, "non-finite energy: check the positions (forces were written)");
     return PINYB200_OK;
@@ -882,26 +946,30 @@ int pinyb200_energy_force(pinyb200_ctx *c, const double *pos, const double *xmod
     const size_t nb = (size_t)c->sys.natm * 3 * c->P;
     CK(cudaEventRecord(c->ev[6], c->stream));
     CK(cudaMemcpyAsync(c->d_pos_aos, pos, nb * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (c->P > 1 && xmod)
+        CK(cudaMemcpyAsync(c->d_xmod, xmod, (size_t)c->sys.natm * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                           c->stream));
     Cell cell = make_cell(hmat);
-    CK(launch_transpose_in(c, c->d_pos_aos));
-    if (c->P > 1) {
-        if (xmod) {
-            CK(cudaMemcpyAsync(c->d_xmod, xmod, (size_t)c->sys.natm * 3 * sizeof(double), cudaMemcpyHostToDevice,
-                               c->stream));
-        } else {
-            const long long n = (long long)c->sys.natm * 3;
-            centroid_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->d_posT, c->d_xmod, c->sys.natm, c->P);
-            CK(cudaGetLastError());
-        }
-    }
     // everything enqueued, one wait: the forces come back right behind the
-    // evaluation
+    // evaluation; the device part replays the context's graph
     const bool energy = !(flags & PINYB200_NO_ENERGY);
     if (energy && !c->h_acc_pin) CK(cudaMallocHost(&c->h_acc_pin, (size_t)c->P * S_NSLOT * sizeof(double)));
     double *acc = energy ? c->h_acc_pin : nullptr;  // pinned: the copy is queued, not waited for
-    int rc = evaluate_enqueue(c, cell, flags, true, acc);
+    int rc = run_eval_graph(c, eval_key(c, 2, c->d_pos_aos, xmod ? c->d_xmod : nullptr, c->d_force_aos, hmat, flags),
+                            [&]() {
+                                CK(launch_transpose_in(c, c->d_pos_aos));
+                                if (c->P > 1 && !xmod) {
+                                    const long long n = (long long)c->sys.natm * 3;
+                                    centroid_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+                                        c->d_posT, c->d_xmod, c->sys.natm, c->P);
+                                    CK(cudaGetLastError());
+                                }
+                                int r = evaluate_enqueue(c, cell, flags, true, acc);
+                                if (r) return r;
+                                CK(launch_transpose_out(c, c->d_force_aos));
+                                return (int)PINYB200_OK;
+                            });
     if (rc) return rc;
-    CK(launch_transpose_out(c, c->d_force_aos));
     CK(cudaMemcpyAsync(force, c->d_force_aos, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaEventRecord(c->ev[7], c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -1046,6 +1114,29 @@ int pinyb200_list_info(pinyb200_ctx *c, long *npairs, long *nactive, long *capac
     if (nactive) *nactive = (long)c->nactive;
     if (capacity) *capacity = (long)c->list_cap;
     return c->have_list ? PINYB200_OK : fail(c, PINYB200_ERR_STATE, "no list built yet");
+}
+
+int pinyb200_set_kernel_timing(pinyb200_ctx *c, int on)
+{
+    if (!c) return fail(c, PINYB200_ERR_ARG, "set_kernel_timing: NULL");
+    c->kt_on = on != 0;
+    c->gen++;  // a captured graph holds no marks
+    return PINYB200_OK;
+}
+
+int pinyb200_kernel_times(pinyb200_ctx *c, const char **names, float *ms, int cap, int *count)
+{
+    if (!c || !names || !ms || !count) return fail(c, PINYB200_ERR_ARG, "kernel_times: NULL");
+    if (!c->kt_on) return fail(c, PINYB200_ERR_STATE, "kernel_times: per-kernel timing is off");
+    CK(cudaSetDevice(c->device));
+    *count = 0;
+    for (int k = 1; k < c->kt_n && *count < cap; k++) {
+        CK(cudaEventSynchronize(c->kt_ev[k]));
+        CK(cudaEventElapsedTime(&ms[*count], c->kt_ev[k - 1], c->kt_ev[k]));
+        names[*count] = c->kt_name[k];
+        (*count)++;
+    }
+    return PINYB200_OK;
 }
 
 int pinyb200_last_timing(pinyb200_ctx *c, float *ms, int n)

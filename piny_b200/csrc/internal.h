@@ -214,6 +214,16 @@ struct pinyb200_ctx {
     bool filter_ok = false;
     cudaEvent_t ev[8];
     float last_ms[5] = {0, 0, 0, 0, 0};
+    // per-kernel timing (pinyb200_set_kernel_timing): an event after every
+    // kernel of a serialised evaluation, named by the kernel it closes
+    // cached CUDA graph of one evaluation (the single-box entry points)
+    cudaGraphExec_t eg_exec = nullptr;
+    std::vector<double> eg_key, eg_seen;
+    bool no_graph = false;
+    bool kt_on = false;
+    int kt_n = 0;
+    std::vector<cudaEvent_t> kt_ev;
+    std::vector<const char *> kt_name;
     // bumped whenever launch shapes or device buffers may change (list
     // builds, tuning, PME tiles): captured graphs compare it before replay
     unsigned long long gen = 0;
@@ -304,6 +314,34 @@ inline cudaError_t smem_optin(const void *func, int bytes)
     if (e == cudaSuccess) have = bytes;
     return e;
 }
+// Timing event that stays a real event record when the stream is being
+// captured into a graph (an external event node), so the phase times of a
+// graph replay are measured as those of a plain run.
+inline cudaError_t ev_rec(cudaEvent_t e, cudaStream_t s)
+{
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaError_t err = cudaStreamIsCapturing(s, &st);
+    if (err != cudaSuccess) return err;
+    return cudaEventRecordWithFlags(e, s, st == cudaStreamCaptureStatusActive ? cudaEventRecordExternal
+                                                                              : cudaEventRecordDefault);
+}
+
+// Per-kernel timing mark: with kt_on, an event on c->stream closing the
+// kernel `name` (the first mark, name nullptr, opens the evaluation).
+inline cudaError_t kt_mark(pinyb200_ctx *c, const char *name)
+{
+    if (!c->kt_on) return cudaSuccess;
+    if (c->kt_n >= (int)c->kt_ev.size()) {
+        cudaEvent_t e;
+        cudaError_t err = cudaEventCreate(&e);
+        if (err != cudaSuccess) return err;
+        c->kt_ev.push_back(e);
+        c->kt_name.push_back(nullptr);
+    }
+    c->kt_name[c->kt_n] = name;
+    return cudaEventRecord(c->kt_ev[c->kt_n++], c->stream);
+}
+
 // cudaFuncSetAttribute(PreferredSharedMemoryCarveout) once per kernel and
 // device: a kernel that gathers from tables held in L1 asks for a small
 // shared-memory share, leaving the rest of the unified cache to L1.

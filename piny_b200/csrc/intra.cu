@@ -9,6 +9,8 @@
 //           spline of -erf(alpha r)/r plus the finite-k correction
 //   ghosts  get_ghost_pos / distrib_ghost_force
 //           (src/energy/intra_con/ghost_control.c:28-129)
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace pinyb200 {
@@ -29,25 +31,32 @@ __device__ __forceinline__ void block_acc(double *acc, int P, int b, const int *
         if (sh[i] != 0.0) atomicAdd(&acc[(size_t)(i / NV) * S_NSLOT + slot[i % NV]], sh[i]);
 }
 
-__global__ void transpose_in_kernel(const double *__restrict__ aos, double *__restrict__ posT, int natm, int P)
+// out[c][r] = in[r][c] for an rows x cols matrix of doubles, through a
+// 32 x 32 shared tile (padded against bank conflicts): both the global reads
+// and the global writes are 256-byte rows.  Positions in: in = [P][natm*3]
+// (PINY's bead-major order), out = [natm*3][P]; forces out the reverse.
+__global__ void __launch_bounds__(256) transpose_tiled_kernel(const double *__restrict__ in, double *__restrict__ out,
+                                                              int rows, long long cols)
 {
-    // aos[b][i][d] -> posT[i][d][b]
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long n = (long long)natm * 3 * P;
-    if (t >= n) return;
-    const int b = (int)(t % P);
-    const long long id = t / P;  // i*3 + d
-    posT[t] = aos[(size_t)b * natm * 3 + id];
-}
-
-__global__ void transpose_out_kernel(const double *__restrict__ fT, double *__restrict__ aos, int natm, int P)
-{
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long n = (long long)natm * 3 * P;
-    if (t >= n) return;
-    const long long id = t % ((long long)natm * 3);
-    const int b = (int)(t / ((long long)natm * 3));
-    aos[t] = fT[id * P + b];
+    __shared__ double tile[32][33];
+    const long long c0 = (long long)blockIdx.x * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r0 = blockIdx.y * 32; r0 < rows; r0 += gridDim.y * 32) {
+#pragma unroll
+        for (int k = 0; k < 32; k += 8) {
+            const int r = r0 + ty + k;
+            const long long c = c0 + tx;
+            if (r < rows && c < cols) tile[ty + k][tx] = in[(size_t)r * cols + c];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 32; k += 8) {
+            const long long c = c0 + ty + k;
+            const int r = r0 + tx;
+            if (r < rows && c < cols) out[(size_t)c * rows + r] = tile[tx][ty + k];
+        }
+        __syncthreads();
+    }
 }
 
 __global__ void ghost_pos_kernel(double *__restrict__ posT, int P, int nghost, int ncomp,
@@ -384,15 +393,17 @@ static inline unsigned nblk_gs(pinyb200_ctx *c, long long n)
 
 cudaError_t launch_transpose_in(pinyb200_ctx *c, const double *d_aos)
 {
-    const long long n = (long long)c->sys.natm * 3 * c->P;
-    transpose_in_kernel<<<nblk(n, 256), 256, 0, c->stream>>>(d_aos, c->d_posT, c->sys.natm, c->P);
+    const long long M = (long long)c->sys.natm * 3;
+    const dim3 grid((unsigned)((M + 31) / 32), (unsigned)((c->P + 31) / 32));
+    transpose_tiled_kernel<<<grid, 256, 0, c->stream>>>(d_aos, c->d_posT, c->P, M);
     return cudaGetLastError();
 }
 
 cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_aos, const double *fT)
 {
-    const long long n = (long long)c->sys.natm * 3 * c->P;
-    transpose_out_kernel<<<nblk(n, 256), 256, 0, c->stream>>>(fT ? fT : c->d_forceT, d_aos, c->sys.natm, c->P);
+    const long long M = (long long)c->sys.natm * 3;
+    const dim3 grid((unsigned)((c->P + 31) / 32), (unsigned)std::min<long long>((M + 31) / 32, 65535));
+    transpose_tiled_kernel<<<grid, 256, 0, c->stream>>>(fT ? fT : c->d_forceT, d_aos, (int)M, c->P);
     return cudaGetLastError();
 }
 

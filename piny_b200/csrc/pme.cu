@@ -1388,9 +1388,12 @@ static cudaError_t launch_fft_t(pinyb200_ctx *c, const PmeArgs &a, const Cell &c
     }
     plane_fwd_kernel<R, NF><<<a.P * a.Nc, 256, sp, c->stream>>>((const R *)a.grid, spec, a.Na, a.Nb, a.Nc, tw[0],
                                                                 tw[1]);
+    if ((err = kt_mark(c, "pme_plane_fwd")) != cudaSuccess) return err;
     conv_c_kernel<R, NF><<<a.P * a.Nb, 256, ss, c->stream>>>(spec, filt, a.Na, a.Nb, a.Nc, tw[2], cell, c->alp_ewd,
                                                              c->d_acc, energy ? 1 : 0);
+    if ((err = kt_mark(c, "pme_conv_c")) != cudaSuccess) return err;
     plane_inv_kernel<R, NF><<<a.P * a.Nc, 256, sp, c->stream>>>(spec, (R *)a.grid, a.Na, a.Nb, a.Nc, tw[0], tw[1]);
+    if ((err = kt_mark(c, "pme_plane_inv")) != cudaSuccess) return err;
     return cudaGetLastError();
 }
 
@@ -1418,6 +1421,7 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     const bool f64 = sizeof(R) == 8;
     cudaError_t err = cudaMemsetAsync(c->d_grid, 0, sizeof(R) * G * c->P, c->stream);
     if (err != cudaSuccess) return err;
+    if ((err = kt_mark(c, "pme_grid_clear (memset)")) != cudaSuccess) return err;
     TileArgs t;
     t.T = TT;
     t.nta = c->pme_nt[0];
@@ -1436,6 +1440,7 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     const bool full = c->pme_full_records;
     if (full) pme_bin_kernel<R, NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell, t);
     else pme_bin_compact_kernel<R, NI><<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(a, cell, t);
+    if ((err = kt_mark(c, "pme_bin")) != cudaSuccess) return err;
     const size_t st = (size_t)TileGeom<NI, TT>::NPT * sizeof(R), ss_spread = spread_smem<R, NI, TT>();
     if (ss_spread > 48 * 1024 - sizeof(PolyTab<R, NI>)) {
         err = smem_optin((const void *)spread_tile_kernel<R, NI, TT>, (int)ss_spread);
@@ -1450,6 +1455,7 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     const dim3 tgrid((unsigned)t.ntile, (unsigned)a.P);
     if (full) spread_tile_kernel<R, NI, TT><<<tgrid, 256, ss_spread, c->stream>>>(a, t);
     else spread_tile_c_kernel<R, NI, TT><<<tgrid, 256, ss_spread, c->stream>>>(a, t);
+    if ((err = kt_mark(c, "pme_spread")) != cudaSuccess) return err;
     const R *twbase = (const R *)(f64 ? (const void *)c->d_twiddle64 : (const void *)c->d_twiddle32);
     const R *tw[3] = {twbase, twbase + 2 * 256, twbase + 4 * 256};
     const size_t sp = pme_plane_smem(a.Na, a.Nb, f64), ss = pme_slab_smem(a.Na, a.Nc, f64);
@@ -1466,6 +1472,7 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     if (err != cudaSuccess) return err;
     if (full) gather_tile_kernel<R, NI, TT><<<tgrid, 256, st, c->stream>>>(a, cell, t);
     else gather_tile_c_kernel<R, NI, TT><<<tgrid, 256, st, c->stream>>>(a, cell, t);
+    if ((err = kt_mark(c, "pme_gather")) != cudaSuccess) return err;
     return cudaGetLastError();
 }
 

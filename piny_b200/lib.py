@@ -112,7 +112,8 @@ EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb
            "pinyb200_fma_peak", "pinyb200_pimd_transform", "pinyb200_pimd_create", "pinyb200_pimd_destroy",
            "pinyb200_pimd_set_nhc", "pinyb200_pimd_get_nhc", "pinyb200_pimd_forces", "pinyb200_pimd_step",
            "pinyb200_update_list_device", "pinyb200_list_set_spread", "pinyb200_list_status",
-           "pinyb200_set_respa", "pinyb200_respa_force_device", "pinyb200_piny_force_respa")
+           "pinyb200_set_respa", "pinyb200_respa_force_device", "pinyb200_piny_force_respa",
+           "pinyb200_set_kernel_timing", "pinyb200_kernel_times")
 
 STAGING, NORMAL_MODES = 1, 2                      # PINYB200_STAGING / _NORMAL_MODES
 TO_MODES, TO_BEADS, FORCE_TO_MODES = 0, 1, 2      # PINYB200_TO_MODES / _TO_BEADS / _FORCE_TO_MODES
@@ -151,6 +152,9 @@ def load(build_if_missing: bool = True):
     L.pinyb200_piny_force.argtypes = [C.c_void_p] + [C.c_void_p] * 3 + [_pd] * 3 + [_pd] + [C.c_void_p] * 3 + \
         [_pd, C.POINTER(PinyEnergies)]
     L.pinyb200_last_timing.argtypes = [C.c_void_p, C.POINTER(C.c_float), _i]
+    L.pinyb200_set_kernel_timing.argtypes = [C.c_void_p, _i]
+    L.pinyb200_kernel_times.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), _i,
+                                        C.POINTER(C.c_int)]
     L.pinyb200_count_list_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, _pd, C.POINTER(C.c_long),
                                              C.POINTER(C.c_long), C.c_void_p]
     L.pinyb200_check_list_device.argtypes = [C.c_void_p, C.c_void_p, _d, _pi, _pd, _pd, _pd, C.c_void_p]
@@ -457,6 +461,18 @@ class DeviceBox:
                                          None if stream is None else C.c_void_p(stream)), "grad")
         k = getattr(self, "_ntan", 0)
         return dE[:k], dF[:k]
+
+    def set_kernel_timing(self, on=True):
+        """Serialised evaluations with an event after every kernel."""
+        self._check(self.L.pinyb200_set_kernel_timing(self.h, 1 if on else 0), "set_kernel_timing")
+
+    def kernel_times(self):
+        """[(kernel, ms)] of the last evaluation, in launch order."""
+        names = (C.c_char_p * 64)()
+        ms = (C.c_float * 64)()
+        n = C.c_int()
+        self._check(self.L.pinyb200_kernel_times(self.h, names, ms, 64, C.byref(n)), "kernel_times")
+        return [(names[i].decode(), float(ms[i])) for i in range(n.value)]
 
     def last_timing(self):
         ms = (C.c_float * 5)()
