@@ -887,8 +887,69 @@ static int run_io(const char *dir, const char *input, const char *outdir_rel, in
     return 0;
 }
 
+#ifdef PINY_WITH_GPU
+/* piny_ref_gpu gpu_dump <dir> <input> <out.bin> <mixed 0|1>: the same
+ * evaluation as dump with the three force sub-steps replaced by the
+ * libpinyb200 binding (energy_control_gpu.c), run twice -- a first call that
+ * builds the device list, then PINY's own list test and a second evaluation
+ * of the same positions -- and dumped after the second, with the device
+ * list as gpu_pairs. */
+#include "pinyb200.h"
+int gpu_force_init(CLASS *, BONDED *, GENERAL_DATA *, int, pinyb200_ctx **);
+int gpu_energy_control(pinyb200_ctx *, CLASS *, BONDED *, GENERAL_DATA *, int);
+
+static int run_gpu_dump(const char *dir, const char *input, const char *outpath, int mixed)
+{
+    setup(dir, input);
+    pinyb200_ctx *ctx = NULL;
+    int rc = gpu_force_init(&class_, &bonded_, &gd_, mixed, &ctx);
+    if (rc) {
+        fprintf(stderr, "@@@ gpu_force_init: %s\n", pinyb200_last_error(ctx));
+        return 3;
+    }
+    double updates0 = 0.0;
+    for (int call = 0; call < 2; call++) {
+        int ip;
+        for (ip = 1; ip <= class_.clatoms_info.pi_beads_proc; ip++)
+            get_ghost_pos(&class_.clatoms_info, &class_.clatoms_pos[ip], &class_.ghost_atoms);
+        energy_control_initial(&class_, &bonded_, &gd_);
+        if (call == 1) updates0 = gd_.stat_avg.updates;
+        rc = gpu_energy_control(ctx, &class_, &bonded_, &gd_, call == 0);
+        if (rc) {
+            fprintf(stderr, "@@@ gpu_energy_control: %s\n", pinyb200_last_error(ctx));
+            return 3;
+        }
+    }
+    dump_all(outpath);
+    /* device list (i > j, 1-based like verlist_pairs) and the second call's rebuilds */
+    long np = 0, na = 0, cap = 0;
+    pinyb200_list_info(ctx, &np, &na, &cap);
+    int *pi = (int *)malloc(sizeof(int) * (size_t)(np + 1)), *pj = (int *)malloc(sizeof(int) * (size_t)(np + 1));
+    long got = 0;
+    pinyb200_get_list(ctx, pi, pj, np, &got);
+    int *pairs = (int *)malloc(sizeof(int) * (size_t)(2 * got + 2));
+    for (long k = 0; k < got; k++) {
+        pairs[2 * k] = pi[k] + 1;
+        pairs[2 * k + 1] = pj[k] + 1;
+    }
+    g_out = fopen(outpath, "ab");
+    put("gpu_pairs", 'i', pairs, 2 * got);
+    put1d("gpu_rebuilds_second_call", gd_.stat_avg.updates - updates0);
+    fclose(g_out);
+    free(pi);
+    free(pj);
+    free(pairs);
+    pinyb200_destroy(ctx);
+    return 0;
+}
+#endif
+
 int main(int argc, char **argv)
 {
+#ifdef PINY_WITH_GPU
+    if (argc == 6 && strcmp(argv[1], "gpu_dump") == 0)
+        return run_gpu_dump(argv[2], argv[3], resolve_out(argv[4]), atoi(argv[5]));
+#endif
     if (argc == 6 && strcmp(argv[1], "io") == 0) return run_io(argv[2], argv[3], argv[4], atoi(argv[5]));
     if (argc == 6 && strcmp(argv[1], "respa_time") == 0)
         return run_respa_time(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]));

@@ -68,3 +68,24 @@ def headline_inputs(name):
         xmod = (gen.mean(axis=0).view(np.int64) + F["xmod_ulp"].astype(np.int64)).view(np.float64)
     S = system.build_system(spec, pos)
     return F, spec, pos, xmod, S
+
+
+def read_piny_dump(path):
+    """Records of a piny_ref dump file: per record a 32-byte name, a kind
+    byte ('d' double, 'i' int32, 'c' text), padding, an int64 count, data."""
+    import struct
+    out = {}
+    with open(path, "rb") as f:
+        while True:
+            h = f.read(40)
+            if len(h) < 40:
+                break
+            name = h[:32].split(b"\0")[0].decode()
+            kind = chr(h[32])
+            n = struct.unpack("<q", f.read(8))[0]
+            if kind == "c":
+                out[name] = f.read(n).decode()
+                continue
+            dt = np.float64 if kind == "d" else np.int32
+            out[name] = np.frombuffer(f.read(n * np.dtype(dt).itemsize), dtype=dt).copy()
+    return out
