@@ -743,7 +743,14 @@ struct MixArgs {
 #define PINYB200_MIX_BLOCKS 6
 #endif
 
-template <int P, int NS, bool ENERGY>
+// Site-pair table patterns known at compile time: bit si * NS + sj of CM
+// (Coulomb table) and VM (vdW table).  kAnyPair takes them from
+// MixArgs::eflag at run time.
+constexpr unsigned kAnyPair = 0xffffffffu;
+constexpr unsigned kTip4pCoul = 0xEEE0u, kTip4pVdw = 0x1u;  // O H H M: H, M charged; LJ on O-O
+constexpr unsigned kSpcCoul = 0x1FFu, kSpcVdw = 0x1u;       // O H H: all charged; LJ on O-O
+
+template <int P, int NS, bool ENERGY, unsigned CM = kAnyPair, unsigned VM = kAnyPair>
 __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kernel(MixArgs a, Cell cell)
 {
     constexpr int G = P >= 32 ? 32 : P;  // lanes per molecule pair
@@ -848,6 +855,9 @@ __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kerne
 #pragma unroll
                 for (int si = 0; si < NS; si++) {
                     const int sp = si * NS + sj;
+                    const bool coul = CM == kAnyPair ? (a.eflag[sp] & 2) != 0 : ((CM >> sp) & 1u) != 0;
+                    const bool vdw = VM == kAnyPair ? (a.eflag[sp] & 1) != 0 : ((VM >> sp) & 1u) != 0;
+                    if (CM != kAnyPair && !coul && !vdw) continue;  // a pair the masks never hold
                     if (!((mask >> sp) & 1u)) continue;
                     const float rx = dj[sj][0] + ei[si][0];
                     const float ry = dj[sj][1] + ei[si][1];
@@ -861,11 +871,11 @@ __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kerne
                         const float del = t - __fsub_rn(tr, kRound);
                         const float4 *row = tab + (a.toff[sp] + kn);
                         float dv = 0.0f;
-                        if (a.eflag[sp] & 2) {
+                        if (coul) {
                             const float4 cf = ldg_keep(row + T_CDV0C * a.tstride);
                             dv = a.q2[sp] * (cf.x + del * (cf.y + del * (cf.z + del * cf.w)));
                         }
-                        if (a.eflag[sp] & 1) {
+                        if (vdw) {
                             const float4 cf = ldg_keep(row + T_CDV0 * a.tstride);
                             dv += cf.x + del * (cf.y + del * (cf.z + del * cf.w));
                         }
@@ -877,22 +887,26 @@ __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kerne
                         fjy -= fy;
                         fjz -= fz;
                         if (ENERGY) {
-                            if (a.eflag[sp] & 1) {
+                            if (vdw) {
                                 const float4 ce = ldg_keep(row + T_CV0 * a.tstride);
                                 evs += ce.x + del * (ce.y + del * (ce.z + del * ce.w));
                             }
-                            if (a.eflag[sp] & 2) {
+                            if (coul) {
                                 const float4 ce = ldg_keep(row + T_CV0C * a.tstride);
                                 ecs += a.q2[sp] * (ce.x + del * (ce.y + del * (ce.z + del * ce.w)));
                             }
-                            pvs[0] += rx * fx;
-                            pvs[1] += ry * fy;
-                            pvs[2] += rz * fz;
-                            pvs[3] += rx * fy;
-                            pvs[4] += rx * fz;
-                            pvs[5] += ry * fz;
                         }
                     }
+                }
+                // virial: r = dj + e_i, so sum r (x) f = dj (x) sum_i f (= -fj here)
+                // + e_i (x) f_i, the latter once per chunk below
+                if (ENERGY) {
+                    pvs[0] -= dj[sj][0] * fjx;
+                    pvs[1] -= dj[sj][1] * fjy;
+                    pvs[2] -= dj[sj][2] * fjz;
+                    pvs[3] -= dj[sj][0] * fjy;
+                    pvs[4] -= dj[sj][0] * fjz;
+                    pvs[5] -= dj[sj][1] * fjz;
                 }
                 if (fjx != 0.0f || fjy != 0.0f || fjz != 0.0f) {
                     const int j = j0 + sj;
@@ -900,6 +914,18 @@ __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kerne
                     atomicAdd(&a.forceT[(3 * (size_t)j + 1) * P + b], (double)fjy);
                     atomicAdd(&a.forceT[(3 * (size_t)j + 2) * P + b], (double)fjz);
                 }
+            }
+        }
+        if (ENERGY) {
+            // the e_i (x) f_i part of the virial: e_i is fixed over the chunk
+#pragma unroll
+            for (int s = 0; s < NS; s++) {
+                pvs[0] += ei[s][0] * fi[s][0];
+                pvs[1] += ei[s][1] * fi[s][1];
+                pvs[2] += ei[s][2] * fi[s][2];
+                pvs[3] += ei[s][0] * fi[s][1];
+                pvs[4] += ei[s][0] * fi[s][2];
+                pvs[5] += ei[s][1] * fi[s][2];
             }
         }
 #pragma unroll
@@ -1070,6 +1096,19 @@ cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy)
 }
 
 
+template <int P, int NS, unsigned CM, unsigned VM>
+static void launch_mix_pattern(pinyb200_ctx *c, const MixArgs &a, const Cell &cell, bool energy, dim3 grid)
+{
+    const int threads = 128;
+    if (energy) {
+        carveout_pref((const void *)mol_pair_mixed_kernel<P, NS, true, CM, VM>, c->pair_carveout);
+        mol_pair_mixed_kernel<P, NS, true, CM, VM><<<grid, threads, 0, c->stream>>>(a, cell);
+    } else {
+        carveout_pref((const void *)mol_pair_mixed_kernel<P, NS, false, CM, VM>, c->pair_carveout);
+        mol_pair_mixed_kernel<P, NS, false, CM, VM><<<grid, threads, 0, c->stream>>>(a, cell);
+    }
+}
+
 template <int P, int NS>
 static void launch_mix_t(pinyb200_ctx *c, const MixArgs &a, const Cell &cell, bool energy)
 {
@@ -1079,13 +1118,18 @@ static void launch_mix_t(pinyb200_ctx *c, const MixArgs &a, const Cell &cell, bo
     if (blocks > maxb) blocks = maxb;
     if (blocks < 1) blocks = 1;
     dim3 grid((unsigned)blocks, P > 32 ? P / 32 : 1);
-    if (energy) {
-        carveout_pref((const void *)mol_pair_mixed_kernel<P, NS, true>, c->pair_carveout);
-        mol_pair_mixed_kernel<P, NS, true><<<grid, threads, 0, c->stream>>>(a, cell);
-    } else {
-        carveout_pref((const void *)mol_pair_mixed_kernel<P, NS, false>, c->pair_carveout);
-        mol_pair_mixed_kernel<P, NS, false><<<grid, threads, 0, c->stream>>>(a, cell);
+    // the site-pair table pattern of the molecule, from the per-pair flags
+    unsigned cm = 0, vm = 0;
+    for (int k = 0; k < NS * NS; k++) {
+        if (c->mix_eflag[k] & 2) cm |= 1u << k;
+        if (c->mix_eflag[k] & 1) vm |= 1u << k;
     }
+    if (NS == 4 && cm == kTip4pCoul && vm == kTip4pVdw)
+        launch_mix_pattern<P, NS, kTip4pCoul, kTip4pVdw>(c, a, cell, energy, grid);
+    else if (NS == 3 && cm == kSpcCoul && vm == kSpcVdw)
+        launch_mix_pattern<P, NS, kSpcCoul, kSpcVdw>(c, a, cell, energy, grid);
+    else
+        launch_mix_pattern<P, NS, kAnyPair, kAnyPair>(c, a, cell, energy, grid);
 }
 
 template <int NS>
