@@ -231,6 +231,27 @@ static void mixed_setup(pinyb200_ctx *c, const pinyb200_system *s, int n0)
     c->mix_dri = (float)s->dri_spl[u0];
     c->mix_rmd = (float)(s->rmin_spl[u0] * s->dri_spl[u0]);
     c->mix_tmax = (float)(s->nsplin - 5);
+    // force and energy rows of each interval side by side, for the
+    // evaluations with energies: [vdW, Coulomb][u][k][force, energy]
+    {
+        const size_t nu = (size_t)c->sys.nuniq;
+        std::vector<double> cf, ce;
+        std::vector<float> fe((size_t)2 * nu * per * 8, 0.0f);
+        const double *tf[2] = {s->cdv0, s->cdv0_c}, *te[2] = {s->cv0, s->cv0_c};
+        for (int kind = 0; kind < 2; kind++)
+            for (size_t u = 0; u < nu; u++) {
+                if (!tf[kind] || !te[kind]) continue;
+                cubic_coefs(tf[kind] + u * per, s->nsplin, cf);
+                cubic_coefs(te[kind] + u * per, s->nsplin, ce);
+                float *dst = fe.data() + ((size_t)kind * nu + u) * per * 8;
+                for (size_t k = 0; k < per; k++)
+                    for (int e = 0; e < 4; e++) {
+                        dst[8 * k + e] = (float)cf[4 * k + e];
+                        dst[8 * k + 4 + e] = (float)ce[4 * k + e];
+                    }
+            }
+        if (upload((float **)&c->d_tabfe, fe.data(), fe.size()) != cudaSuccess) return;
+    }
     c->mix_ok = (size_t)c->sys.nuniq * per * 4 < (size_t)0x7fffffff;
     // one wave of resident blocks (6 per SM at its register count) serves
     // the grid-strided chunks best at the benchmark sizes
@@ -271,7 +292,7 @@ int pinyb200_destroy(pinyb200_ctx *c)
                     c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf, c->d_x0, c->d_forceP,
                     c->d_pme_head, c->d_pme_w, c->d_nchunk, c->d_ls, c->d_cs, c->d_mchunk, c->d_mmaskf,
                     c->d_reach, c->d_cut_res, c->d_bond_eq_res, c->d_forceW, c->d_forcet_aos, c->d_rowR,
-                    c->d_colR, c->d_rtot, c->d_xm0, c->d_cs0, c->d_ecor_res_tab, c->d_cs_in};
+                    c->d_colR, c->d_rtot, c->d_xm0, c->d_cs0, c->d_ecor_res_tab, c->d_cs_in, c->d_tabfe};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : c->kt_ev) cudaEventDestroy(e);

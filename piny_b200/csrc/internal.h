@@ -167,6 +167,7 @@ struct pinyb200_ctx {
     bool mix_ok = false;
     int mix_toff[16] = {0}, mix_eflag[16] = {0};
     float mix_q2[16] = {0};
+    float4 *d_tabfe = nullptr;  // [2][nuniq][nsplin][2] vdW / Coulomb force and energy rows side by side
     float mix_rc2 = 0, mix_dri = 0, mix_rmd = 0, mix_tmax = 0;
     bool mol_ok = false;       // the current molecule list matches the site list
     int nmol = 0, mol_ns = 0;

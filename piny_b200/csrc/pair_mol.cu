@@ -730,6 +730,7 @@ struct MixArgs {
     const double *cutoff, *rmin, *dri;
     const int *has_vdw;
     const float4 *tab;   // [4][nuniq][nsplin] interval coefficients (TabKind order)
+    const float4 *tabfe; // [2][nuniq][nsplin][2]: vdW then Coulomb; force and energy rows interleaved
     double *forceT;
     double *acc;
     int toff[16];        // per site pair si * NS + sj: u * nsplin + 2, its rows at nint(t) = 0
@@ -869,14 +870,30 @@ __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kerne
                         const float tr = __fadd_rn(t, kRound);
                         const int kn = __float_as_int(tr) - __float_as_int(kRound);
                         const float del = t - __fsub_rn(tr, kRound);
+                        // with energies: the force and energy rows of an interval
+                        // sit side by side (one cache line for both loads)
                         const float4 *row = tab + (a.toff[sp] + kn);
+                        const float4 *rfe = a.tabfe + 2 * (a.toff[sp] + kn);
                         float dv = 0.0f;
+                        float4 ecf = make_float4(0.f, 0.f, 0.f, 0.f), evf = ecf;
                         if (coul) {
-                            const float4 cf = ldg_keep(row + T_CDV0C * a.tstride);
+                            float4 cf;
+                            if (ENERGY) {
+                                cf = ldg_keep(rfe + 2 * a.tstride);
+                                ecf = ldg_keep(rfe + 2 * a.tstride + 1);
+                            } else {
+                                cf = ldg_keep(row + T_CDV0C * a.tstride);
+                            }
                             dv = a.q2[sp] * (cf.x + del * (cf.y + del * (cf.z + del * cf.w)));
                         }
                         if (vdw) {
-                            const float4 cf = ldg_keep(row + T_CDV0 * a.tstride);
+                            float4 cf;
+                            if (ENERGY) {
+                                cf = ldg_keep(rfe);
+                                evf = ldg_keep(rfe + 1);
+                            } else {
+                                cf = ldg_keep(row + T_CDV0 * a.tstride);
+                            }
                             dv += cf.x + del * (cf.y + del * (cf.z + del * cf.w));
                         }
                         const float fx = rx * dv, fy = ry * dv, fz = rz * dv;
@@ -887,14 +904,8 @@ __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kerne
                         fjy -= fy;
                         fjz -= fz;
                         if (ENERGY) {
-                            if (vdw) {
-                                const float4 ce = ldg_keep(row + T_CV0 * a.tstride);
-                                evs += ce.x + del * (ce.y + del * (ce.z + del * ce.w));
-                            }
-                            if (coul) {
-                                const float4 ce = ldg_keep(row + T_CV0C * a.tstride);
-                                ecs += a.q2[sp] * (ce.x + del * (ce.y + del * (ce.z + del * ce.w)));
-                            }
+                            if (vdw) evs += evf.x + del * (evf.y + del * (evf.z + del * evf.w));
+                            if (coul) ecs += a.q2[sp] * (ecf.x + del * (ecf.y + del * (ecf.z + del * ecf.w)));
                         }
                     }
                 }
@@ -1173,6 +1184,7 @@ cudaError_t launch_mol_pair_mixed(pinyb200_ctx *c, const Cell &cell, bool energy
     a.dri = s.dri;
     a.has_vdw = s.has_vdw;
     a.tab = s.tab32;
+    a.tabfe = c->d_tabfe;
     a.forceT = c->d_forceT;
     a.acc = c->d_acc;
     for (int k = 0; k < 16; k++) {
