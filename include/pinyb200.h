@@ -173,6 +173,33 @@ int pinyb200_get_list(pinyb200_ctx *ctx, int *pi, int *pj, long cap,
                       long *npairs);
 
 /*
+ * How the molecule-pair list is enumerated, PINY's two list generators
+ * (verlist_control.c:64-110):
+ *   PINYB200_LIST_LNK   (default) link cells, as lnk_ver_update /
+ *                       lnk_ver_gen_pad: molecules binned by their site-0
+ *                       bead-1 position into cells at least half the
+ *                       molecule reach wide; each home cell's molecules
+ *                       meet the molecules of the 5 x 5 x 5 cells around
+ *                       it.  Used when every cell axis holds >= 5 cells and
+ *                       the 125 cells are at most 40 % of the box, else the
+ *                       sweep runs.
+ *   PINYB200_LIST_NOLST the all-pairs sweep, as nolst_ver_update /
+ *                       nolst_ver_gen.
+ * Both give the same pair set; a row's pairs come in neighbour-cell order
+ * with cells and in index order with the sweep.  The method applies from
+ * the next pinyb200_build_list (which plans the cells for its positions;
+ * device rebuilds keep that plan and sweep when the molecules' reach has
+ * outgrown it).  pinyb200_list_cells returns the plan of the current list:
+ * cells[0..2] the cells along a, b, c (zeros when it swept) and cells[3] 1
+ * when the cells built it.  Systems not made of molecules of <= 4
+ * sites use the site sweep for either method.
+ */
+#define PINYB200_LIST_LNK 0
+#define PINYB200_LIST_NOLST 1
+int pinyb200_set_list_method(pinyb200_ctx *ctx, int method);
+int pinyb200_list_cells(pinyb200_ctx *ctx, int *cells);
+
+/*
  * Rebuild test of the current list for positions on the device, as PINY
  * runs it each step before the force call (nbr_list_control.c:63-110):
  *   *rmax       = max over atoms of |r(bead 1) - r(at the last build)|

@@ -98,6 +98,9 @@ class Oracle:
         L.orc_verlist.restype = C.c_long
         L.orc_verlist.argtypes = [C.POINTER(OrcSystem), _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd,
                                   C.c_long, _pi, _pi]
+        L.orc_verlist_rows.restype = C.c_long
+        L.orc_verlist_rows.argtypes = [C.POINTER(OrcSystem), _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _i, _i,
+                                       C.c_long, _pi, _pi]
         L.orc_energy_force.argtypes = [C.POINTER(OrcSystem), _i, _pd, _pd, _pd, C.c_long, _pi, _pi, _i,
                                        _pd, C.POINTER(OrcEnergies)]
         L.orc_respa_force.argtypes = [C.POINTER(OrcSystem), C.POINTER(OrcRespa), _i, _i, _pd, _pd, _pd,
@@ -256,6 +259,27 @@ class Oracle:
                              z.ctypes.data_as(_pd), *xp, ph, None, pcs, cnt,
                              pi.ctypes.data_as(_pi), pj.ctypes.data_as(_pi))
         del n
+        return pi[:cnt], pj[:cnt]
+
+    def verlist_rows(self, sysd, pos1, xmod, hmat, cutskin2, ilo, ihi):
+        """The pairs (i, j) of verlist with ilo <= i < ihi."""
+        s = self.make_struct(sysd)
+        pos1 = np.ascontiguousarray(pos1, np.float64).reshape(-1, 3)
+        xs = [np.ascontiguousarray(pos1[:, d]) for d in range(3)]
+        xp = [a.ctypes.data_as(_pd) for a in xs]
+        if xmod is not None:
+            xm = np.ascontiguousarray(xmod, np.float64).reshape(-1, 3)
+            ms = [np.ascontiguousarray(xm[:, d]) for d in range(3)]
+            mp = [a.ctypes.data_as(_pd) for a in ms]
+        else:
+            mp = [None, None, None]
+        hmat, ph = self._d(hmat)
+        cs, pcs = self._d(cutskin2)
+        cnt = self.lib.orc_verlist_rows(C.byref(s), *xp, *mp, ph, pcs, int(ilo), int(ihi), 0, None, None)
+        pi = np.zeros(max(cnt, 1), np.int32)
+        pj = np.zeros(max(cnt, 1), np.int32)
+        self.lib.orc_verlist_rows(C.byref(s), *xp, *mp, ph, pcs, int(ilo), int(ihi), cnt,
+                                  pi.ctypes.data_as(_pi), pj.ctypes.data_as(_pi))
         return pi[:cnt], pj[:cnt]
 
     def energy_force(self, sysd, pos, xmod, hmat, pi, pj, distribute_ghosts=False):

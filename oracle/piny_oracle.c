@@ -534,17 +534,19 @@ static inline int pair_type(int ti, int tj, int ntyp)
 /* separation satisfies r^2 < cutskin^2 of its pair type.  Brute force;     */
 /* PINY's link cells only enumerate candidates, the accepted set is this.   */
 /* ------------------------------------------------------------------------ */
-long orc_verlist(const orc_system *s, const double *x, const double *y, const double *z,
-                 const double *xmod, const double *ymod, const double *zmod, const double *h,
-                 const double *hi_unused, const double *cutskin2, long cap, int *pi, int *pj)
+/* Rows i in [ilo, ihi) of the list below. */
+long orc_verlist_rows(const orc_system *s, const double *x, const double *y, const double *z,
+                      const double *xmod, const double *ymod, const double *zmod, const double *h,
+                      const double *cutskin2, int ilo, int ihi, long cap, int *pi, int *pj)
 {
     double hi[9];
-    (void)hi_unused;
     cell_inverse(h, hi);
     int cubic = is_cubic(h);
     long n = 0;
     char *ex = calloc((size_t)s->natm, 1);
-    for (int i = 1; i < s->natm; i++) {
+    if (ilo < 1) ilo = 1;
+    if (ihi > s->natm) ihi = s->natm;
+    for (int i = ilo; i < ihi; i++) {
         for (int e = s->excl_off[i]; e < s->excl_off[i + 1]; e++) ex[s->excl_j[e]] = 1;
         for (int j = 0; j < i; j++) {
             if (ex[j]) continue;
@@ -564,6 +566,14 @@ long orc_verlist(const orc_system *s, const double *x, const double *y, const do
     }
     free(ex);
     return n;
+}
+
+long orc_verlist(const orc_system *s, const double *x, const double *y, const double *z,
+                 const double *xmod, const double *ymod, const double *zmod, const double *h,
+                 const double *hi_unused, const double *cutskin2, long cap, int *pi, int *pj)
+{
+    (void)hi_unused;
+    return orc_verlist_rows(s, x, y, z, xmod, ymod, zmod, h, cutskin2, 1, s->natm, cap, pi, pj);
 }
 
 /* 4-point cubic of npol_vspl_fetch (force_npol.c:339-375); table is 0-based

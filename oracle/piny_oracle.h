@@ -169,6 +169,12 @@ long orc_verlist(const orc_system *sys, const double *x, const double *y,
                  const double *z, const double *xmod, const double *ymod,
                  const double *zmod, const double *hmat, const double *hmati,
                  const double *cutskin2, long cap, int *pi, int *pj);
+/* The rows i in [ilo, ihi) of the same list (checks of large boxes). */
+long orc_verlist_rows(const orc_system *sys, const double *x, const double *y,
+                      const double *z, const double *xmod, const double *ymod,
+                      const double *zmod, const double *hmat,
+                      const double *cutskin2, int ilo, int ihi, long cap,
+                      int *pi, int *pj);
 
 /* Verlet-list rebuild test: check_ver_list (nbr_list_control.c:182-247),
  * get_pimd_spread (pimd_estimators.c:121-220), get_cut_skin

@@ -292,7 +292,9 @@ int pinyb200_destroy(pinyb200_ctx *c)
                     c->d_pme_cnt, c->d_pme_bin, c->d_pme_ovf, c->d_x0, c->d_forceP,
                     c->d_pme_head, c->d_pme_w, c->d_nchunk, c->d_ls, c->d_cs, c->d_mchunk, c->d_mmaskf,
                     c->d_reach, c->d_cut_res, c->d_bond_eq_res, c->d_forceW, c->d_forcet_aos, c->d_rowR,
-                    c->d_colR, c->d_rtot, c->d_xm0, c->d_cs0, c->d_ecor_res_tab, c->d_cs_in, c->d_tabfe};
+                    c->d_colR, c->d_rtot, c->d_xm0, c->d_cs0, c->d_ecor_res_tab, c->d_cs_in, c->d_tabfe,
+                    c->d_mcell, c->d_msf, c->d_ccnt, c->d_coff, c->d_cmol, c->d_cellok, c->d_ctot, c->d_ent, c->d_nent,
+                    c->d_scan_part, c->d_reach_acc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : c->kt_ev) cudaEventDestroy(e);
@@ -563,6 +565,8 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
             CK(upload(&c->d_mstart, mstart.data(), mstart.size()));
             CK(cudaMalloc(&c->d_mcount, (size_t)c->nmol * sizeof(int)));
             CK(cudaMalloc(&c->d_mrow, (size_t)(c->nmol + 1) * sizeof(int)));
+            CK(cudaMalloc(&c->d_msf, (size_t)c->nmol * sizeof(float4)));
+            CK(cudaMalloc(&c->d_nent, sizeof(unsigned long long)));
             const int n0 = mstart[1];
             bool strided = true;
             for (size_t m = 0; m < mstart.size(); m++) strided &= mstart[m] == (int)m * n0;
@@ -572,6 +576,11 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
     }
     CK(cudaMalloc(&c->d_err, sizeof(int)));
     CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    // device-wide scans: tile sums for two arrays of up to max(natm + 1, 64^3) counts
+    c->scan_part_cap = 2LL * scan_tiles(std::max(natm + 1, 1 << 18));
+    CK(cudaMalloc(&c->d_scan_part, (size_t)c->scan_part_cap * sizeof(long long)));
+    CK(cudaMalloc(&c->d_reach_acc, 4 * sizeof(unsigned long long)));
+    CK(cudaMemset(c->d_reach_acc, 0, 4 * sizeof(unsigned long long)));
     *out = c;
     return PINYB200_OK;
 }
@@ -611,6 +620,7 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
     if (c->use_mol) {
         // molecule-pair list first; the site lists are expanded from its masks
         if (!c->d_reach) CK(cudaMalloc(&c->d_reach, sizeof(double)));
+        if (int rc = mol_cells_plan(c, cell, d_p1, d_cs)) return rc;
         CK(cudaMemsetAsync(c->d_tot, 0, 4 * sizeof(long long), c->stream));
         CK(launch_mol_list(c, cell, d_p1, d_xm, d_cs, 0));
         CK(cudaMemcpyAsync(tot, c->d_tot, sizeof(tot), cudaMemcpyDeviceToHost, c->stream));
@@ -619,13 +629,19 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
             if (c->d_mj) cudaFree(c->d_mj);
             if (c->d_mmask) cudaFree(c->d_mmask);
             if (c->d_mmaskf) cudaFree(c->d_mmaskf);
+            if (c->d_ent) cudaFree(c->d_ent);
             c->d_mj = nullptr;
             c->d_mmask = c->d_mmaskf = nullptr;
+            c->d_ent = nullptr;
+            c->ent_cap = 0;
             const long long cap = tot[2] + tot[2] / 4 + 1024;
             CK(cudaMalloc(&c->d_mj, cap * sizeof(int)));
             CK(cudaMalloc(&c->d_mmask, cap * sizeof(unsigned)));
             CK(cudaMalloc(&c->d_mmaskf, cap * sizeof(unsigned)));
-            c->mlist_cap = cap;
+            CK(cudaMalloc(&c->d_ent, cap * sizeof(int4)));
+            c->mlist_cap = c->ent_cap = cap;
+            // the count pass wrote its pairs into the freed buffer: the fill computes
+            CK(cudaMemsetAsync(c->d_nent, 0xff, sizeof(unsigned long long), c->stream));
         }
         CK(launch_mol_list(c, cell, d_p1, d_xm, d_cs, 1));
         CK(launch_site_from_mol(c, 0));
@@ -685,6 +701,29 @@ int pinyb200_build_list(pinyb200_ctx *c, const double *pos1, const double *xmod,
     c->have_list = true;
     if (int rc = list_reset_flags(c)) return rc;
     if (npairs) *npairs = (long)tot[0];
+    return PINYB200_OK;
+}
+
+int pinyb200_set_list_method(pinyb200_ctx *c, int method)
+{
+    if (!c) return fail(c, PINYB200_ERR_ARG, "NULL context");
+    if (method != PINYB200_LIST_LNK && method != PINYB200_LIST_NOLST)
+        return fail(c, PINYB200_ERR_ARG, "set_list_method: unknown method");
+    c->list_method = method;
+    return PINYB200_OK;
+}
+
+int pinyb200_list_cells(pinyb200_ctx *c, int *cells)
+{
+    if (!c || !cells) return fail(c, PINYB200_ERR_ARG, "list_cells: NULL argument");
+    if (!c->have_list) return fail(c, PINYB200_ERR_STATE, "no list built yet");
+    CK(cudaSetDevice(c->device));
+    for (int d = 0; d < 3; d++) cells[d] = c->use_mol ? c->cell_n[d] : 0;
+    cells[3] = 0;
+    if (c->use_mol && c->cell_n[0] > 0) {
+        CK(cudaStreamSynchronize(c->stream));
+        CK(cudaMemcpy(&cells[3], c->d_cellok, sizeof(int), cudaMemcpyDeviceToHost));
+    }
     return PINYB200_OK;
 }
 

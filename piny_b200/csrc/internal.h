@@ -178,6 +178,23 @@ struct pinyb200_ctx {
     unsigned *d_mmask = nullptr;   // active site pairs of each molecule pair
     unsigned *d_mmaskf = nullptr;  // all site pairs (PINY's list) of each molecule pair
     double *d_reach = nullptr;     // list build: reach of the molecule bound
+    float4 *d_msf = nullptr;    // [nmol] wrapped fractional site-0 bead-1 positions (FP32)
+    int4 *d_ent = nullptr;      // [ent_cap] molecule pairs found by the count pass (fill by scatter)
+    long long ent_cap = 0;
+    unsigned long long *d_nent = nullptr;  // [1] pairs the count pass found
+    unsigned long long *d_reach_acc = nullptr;  // [4] reach maxima (bit patterns) and blocks done, kept zero
+    long long *d_scan_part = nullptr;  // [scan_part_cap] tile sums of the device-wide scans
+    long long scan_part_cap = 0;
+    // link cells of the molecule-pair list build, planned at each host build
+    int list_method = 0;        // PINYB200_LIST_LNK or PINYB200_LIST_NOLST
+    int cell_n[3] = {0, 0, 0};  // cells along a, b, c (each >= 5); 0: every build sweeps
+    int cell_cap = 0;           // cells the buffers below hold
+    int *d_mcell = nullptr;     // [nmol] cell of each molecule
+    int *d_ccnt = nullptr;      // [2][cell_cap] molecules per cell, scatter counters
+    int *d_coff = nullptr;      // [cell_cap + 1] first molecule of each cell in d_cmol
+    int *d_cmol = nullptr;      // [2][nmol] molecules in cell order: arrival, then sorted
+    int *d_cellok = nullptr;    // [1] the cells serve the current build
+    long long *d_ctot = nullptr;  // [1] scan total
     long long mlist_cap = 0, nmp = 0;
     int nchunk = 0;
     int *d_chunk = nullptr;    // [chunk_cap][3]
@@ -267,11 +284,15 @@ cudaError_t launch_pme_force_add_scaled(pinyb200_ctx *c, double w, double *targe
 cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
                             const double *d_cutskin2, int pass, const int *gate = nullptr,
                             cudaStream_t st = nullptr);
+int mol_cells_plan(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_cutskin2);
+// Exclusive prefix sums of K (1 or 2) arrays of n counts at count + k n into
+// out_k[0..n] (out_k[n] the total) and tot[k]; uses c->d_scan_part.
+int scan_tiles(int n);
+cudaError_t launch_scan(pinyb200_ctx *c, const int *gate, int n, int K, const int *count, int *out0, int *out1,
+                        long long *tot, cudaStream_t st);
 cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_mol_pair_mixed(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_site_from_mol(pinyb200_ctx *c, int pass, const int *gate = nullptr, cudaStream_t st = nullptr);
-__global__ void __launch_bounds__(1024) scan_kernel(const int *gate, int n, const int *count, int *row, int *rowA,
-                                                     long long *tot);
 cudaError_t launch_pme(pinyb200_ctx *c, const Cell &cell, bool energy);
 cudaError_t launch_pme_force_add(pinyb200_ctx *c);
 
@@ -369,8 +390,6 @@ cudaError_t launch_transpose_out(pinyb200_ctx *c, double *d_force_aos, const dou
 cudaError_t launch_list_count(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
                               const double *d_cutskin2, int *d_count, cudaStream_t st);
 cudaError_t launch_list_check(pinyb200_ctx *c, const double *d_pos, unsigned long long *d_out, cudaStream_t st);
-__global__ void __launch_bounds__(1024) mol_scan_kernel(const int *gate, int n, const int *count, int *row,
-                                                         long long *tot);
 // device list update (update.cu)
 int list_update_prepare(pinyb200_ctx *c);
 int list_update_enqueue(pinyb200_ctx *c, const double *d_pos, const double *d_xm, const Cell &cell, cudaStream_t st);

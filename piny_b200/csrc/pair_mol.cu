@@ -19,7 +19,10 @@
 //     is evaluated from the mode-1 separations the same way.
 //   * FP64: every site-pair separation and image shift in FP64 with PINY's
 //     operation order, as in the site kernel.
+#include <algorithm>
+#include <cmath>
 #include <cstddef>
+#include <string>
 
 #include "common.cuh"
 
@@ -37,157 +40,619 @@ namespace pinyb200 {
 // is excluded (checked when the context is made), so no site pair is lost.
 //
 // A molecule pair is skipped without looking at its sites when a lower
-// bound of the distance between any images of the two site-0 mode-1
-// positions exceeds the reach R = max cutskin + 2 (e + d), e = largest
-// distance of a site from its molecule's site 0 and d = largest distance of
-// a bead-1 position from its mode-1 position (mode-1 positions: xm, or the
-// bead-1 positions for one bead).  Any site pair of a pair so skipped is
-// farther apart than max cutskin on every image.
+// bound of the distance between the images of the two site-0 bead-1
+// positions exceeds the reach R = max cutskin + 2 e, e = largest distance of
+// a bead-1 site from its molecule's site 0.  Every image shift period /
+// period_pimd applies is a lattice vector and no image of a site pair is
+// nearer than the nearest image less 2 e, so a pair so skipped has no site
+// pair inside max cutskin.  The bound, from the wrapped fractional
+// separation t along each cell axis times the lattice-plane spacing w: the
+// exact minimum-image distance sqrt(sum (t w)^2) in an orthorhombic cell
+// (where the axes separate), the largest t w otherwise.  It is evaluated in
+// FP32 from fractional positions rounded to FP32, against R widened by more
+// than that rounding can move it (bound_slack): a filter that only ever lets
+// extra pairs through to the exact FP64 test.
 
-// Lower bound of |dx + h n| over all lattice vectors h n: along each cell
-// axis the wrapped fractional separation times the lattice-plane spacing.
-__device__ __forceinline__ double image_lower_bound(double dx, double dy, double dz, const Cell &c)
+// Plane spacings of the cell, whether it is orthorhombic, and the widened
+// reach the FP32 bound is compared with (squared; set on the device).
+struct CellPlanes {
+    double w[3];
+    int ortho;
+};
+
+// R plus the FP32 rounding allowance of the bound: fractional positions in
+// [0, 1) rounded to FP32 (2^-25), their difference and wrap (2^-24 each),
+// times w, with a factor 20 to spare; 1e-6 Bohr absolute.
+__host__ __device__ inline double bound_slack(const CellPlanes &pl)
 {
-    double lb = 0.0;
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        const double b0 = c.hi[d], b1 = c.hi[3 + d], b2 = c.hi[6 + d];
-        const double sd = dx * b0 + dy * b1 + dz * b2;
-        const double w = fabs(sd - rint(sd)) * rsqrt(b0 * b0 + b1 * b1 + b2 * b2);
-        lb = fmax(lb, w);
-    }
-    return lb;
+    return 4e-6 * fmax(pl.w[0], fmax(pl.w[1], pl.w[2])) + 1e-6;
 }
 
-// The reach R (above) into *reach; one block.
-__global__ void __launch_bounds__(1024) mol_reach_kernel(const int *__restrict__ gate, int nmol,
-                                                          const int *__restrict__ mstart,
-                                                          const double *__restrict__ pos1,
-                                                          const double *__restrict__ xm, int use_xm,
-                                                          const double *__restrict__ cs, int npt,
-                                                          double *__restrict__ reach)
+// Squared bound from the fractional separations (FP32).
+__device__ __forceinline__ float bound2_frac(float t0, float t1, float t2, const CellPlanes &pl)
+{
+    t0 = fabsf(t0 - rintf(t0)) * (float)pl.w[0];
+    t1 = fabsf(t1 - rintf(t1)) * (float)pl.w[1];
+    t2 = fabsf(t2 - rintf(t2)) * (float)pl.w[2];
+    return pl.ortho ? t0 * t0 + t1 * t1 + t2 * t2 : fmaxf(t0 * t0, fmaxf(t1 * t1, t2 * t2));
+}
+
+// The reach R (above) into *reach.  Each block's maxima go into acc[0] and
+// acc[2] by atomicMax on their bit patterns (non-negative doubles order as
+// their bits; fmax has already dropped any NaN); the last block to finish
+// turns them into R and clears acc[0..3] for the next launch.
+__global__ void __launch_bounds__(256) mol_reach_kernel(const int *__restrict__ gate, int nmol,
+                                                         const int *__restrict__ mstart,
+                                                         const double *__restrict__ pos1,
+                                                         const double *__restrict__ cs, int npt,
+                                                         unsigned long long *__restrict__ acc,
+                                                         double *__restrict__ reach)
 {
     if (gate && *gate == 0) return;
-    __shared__ double red[3][32];
-    double ext = 0.0, dev = 0.0, cmax = 0.0;
-    for (int k = threadIdx.x; k < npt; k += blockDim.x) cmax = fmax(cmax, cs[k]);
-    for (int m = threadIdx.x; m < nmol; m += blockDim.x) {
+    __shared__ double red[2][8];
+    __shared__ int last;
+    double ext = 0.0, cmax = 0.0;
+    if (blockIdx.x == 0)
+        for (int k = threadIdx.x; k < npt; k += blockDim.x) cmax = fmax(cmax, cs[k]);
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < nmol; m += gridDim.x * blockDim.x) {
         const int i0 = mstart[m], i1 = mstart[m + 1];
-        const double *x0 = (use_xm ? xm : pos1) + 3 * (size_t)i0;
-        for (int i = i0; i < i1; i++) {
-            const double *xi = (use_xm ? xm : pos1) + 3 * (size_t)i;
+        const double *x0 = pos1 + 3 * (size_t)i0;
+        for (int i = i0 + 1; i < i1; i++) {
+            const double *xi = pos1 + 3 * (size_t)i;
             const double ex = xi[0] - x0[0], ey = xi[1] - x0[1], ez = xi[2] - x0[2];
             ext = fmax(ext, sqrt(ex * ex + ey * ey + ez * ez));
-            if (use_xm) {
-                const double *p = pos1 + 3 * (size_t)i;
-                const double qx = p[0] - xi[0], qy = p[1] - xi[1], qz = p[2] - xi[2];
-                dev = fmax(dev, sqrt(qx * qx + qy * qy + qz * qz));
-            }
         }
     }
     for (int o = 16; o >= 1; o >>= 1) {
         ext = fmax(ext, __shfl_xor_sync(0xffffffffu, ext, o));
-        dev = fmax(dev, __shfl_xor_sync(0xffffffffu, dev, o));
         cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (lane == 0) {
         red[0][w] = ext;
-        red[1][w] = dev;
-        red[2][w] = cmax;
+        red[1][w] = cmax;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int k = 1; k < (int)(blockDim.x >> 5); k++) {
             ext = fmax(ext, red[0][k]);
-            dev = fmax(dev, red[1][k]);
-            cmax = fmax(cmax, red[2][k]);
+            cmax = fmax(cmax, red[1][k]);
         }
-        // rounding of the bound and of the criterion: a generous margin
-        *reach = (sqrt(cmax) + 2.0 * (ext + dev)) * (1.0 + 1e-12) + 1e-9;
+        atomicMax(&acc[0], (unsigned long long)__double_as_longlong(ext));
+        atomicMax(&acc[2], (unsigned long long)__double_as_longlong(cmax));
+        __threadfence();
+        last = atomicAdd(&acc[3], 1ull) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        const double e = __longlong_as_double((long long)atomicExch(&acc[0], 0ull));
+        const double c2 = __longlong_as_double((long long)atomicExch(&acc[2], 0ull));
+        atomicExch(&acc[3], 0ull);
+        // rounding of the distances and of the criterion: a generous margin
+        *reach = (sqrt(c2) + 2.0 * e) * (1.0 + 1e-12) + 1e-9;
     }
 }
 
-template <int FILL, int NS>
-__global__ void __launch_bounds__(256) mol_list_kernel(const int *__restrict__ gate, int nmol,
-                                                       const int *__restrict__ mstart, int ntyp,
-                                                       const double *__restrict__ pos1, const double *__restrict__ xm,
-                                                       int use_xm, Cell cell, const double *__restrict__ cutskin2,
-                                                       const int *__restrict__ atm_typ,
-                                                       const double *__restrict__ charge,
-                                                       const int *__restrict__ inter_map,
-                                                       const int *__restrict__ has_vdw,
-                                                       const double *__restrict__ reach, int *__restrict__ count,
-                                                       const int *__restrict__ row, int *__restrict__ mj_out,
-                                                       unsigned *__restrict__ mask_out, unsigned *__restrict__ maskf_out,
-                                                       long long cap, unsigned long long *__restrict__ nsite)
+// Blocks of mol_reach_kernel.
+static int reach_blocks(const pinyb200_ctx *c) { return std::max(1, std::min((c->nmol + 255) / 256, 2 * c->sm_count)); }
+
+// Wrapped fractional site-0 bead-1 position of every molecule (FP32), and
+// with cells, its cell and the cells' populations (ccnt, zeroed before).
+__global__ void __launch_bounds__(256) mol_frac_kernel(const int *__restrict__ gate, int nmol,
+                                                       const int *__restrict__ mstart, const double *__restrict__ pos1,
+                                                       Cell cell, int na, int nb, int nc, float4 *__restrict__ msf,
+                                                       int *__restrict__ mcell, int *__restrict__ ccnt)
+{
+    if (gate && *gate == 0) return;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nmol) return;
+    const double *x = pos1 + 3 * (size_t)mstart[m];
+    const int n[3] = {na, nb, nc};
+    float f[3];
+    int k[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        double sd = x[0] * cell.hi[d] + x[1] * cell.hi[3 + d] + x[2] * cell.hi[6 + d];
+        sd -= floor(sd);
+        f[d] = (float)sd;
+        int q = (int)(sd * n[d]);
+        if (!(q >= 0 && q < n[d])) q = q >= n[d] ? n[d] - 1 : 0;  // sd == 1 after rounding, or not finite
+        k[d] = q;
+    }
+    msf[m] = make_float4(f[0], f[1], f[2], 0.0f);
+    if (mcell) {
+        const int id = (k[2] * nb + k[1]) * na + k[0];
+        mcell[m] = id;
+        atomicAdd(&ccnt[id], 1);
+    }
+}
+
+// PINY's list criterion for every site pair of one molecule pair (mi with
+// sites i0.., mj with sites j0..): r^2 < cutskin^2 of the pair type on the
+// bead-1 separation and PINY's image (period / period_pimd with the mode-1
+// separation), in FP64 with PINY's operation order (verlist_create.c:
+// 373-503).  maskf gets bit si * NS + sj for every site pair inside, mask
+// for those that also carry a force (a vdW table or a charge product); the
+// molecules are identical, so cutskin^2 and that flag come per (si, sj)
+// from tcs2 / tact.
+//
+// The image.  In a cubic cell PINY's shift along an axis is -NINT of
+// (separation * hi), the separation being the mode-1 one (period_pimd) or
+// the bead-1 one (period).  Rounded subtraction and multiplication by
+// hi > 0 are monotone, and so is NINT, so over all site pairs of the pair
+// that NINT lies between its values at the two ends of the range of the
+// separation, formed from the extreme site coordinates of the two
+// molecules.  When those agree, every site pair has that NINT and it is
+// applied once; otherwise each site pair evaluates its own.  The shifted
+// separations are bit for bit PINY's either way.
+template <int NS, bool XM>
+__device__ __forceinline__ void mol_pair_masks(int i0, int ni, int j0, int nj, const double *__restrict__ pos1,
+                                               const double *__restrict__ xm, const Cell &cell,
+                                               const double *tcs2, const unsigned char *tact, unsigned &mask,
+                                               unsigned &maskf)
+{
+    // mj's sites once into registers (each lane tests its own mj; mi is the
+    // same across the warp, so its loads are broadcasts)
+    double xj[NS][3], mj[NS][3];
+#pragma unroll
+    for (int sj = 0; sj < NS; sj++) {
+        const int j = j0 + (sj < nj ? sj : 0);
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            xj[sj][d] = pos1[3 * j + d];
+            if (XM) mj[sj][d] = xm[3 * j + d];
+        }
+    }
+    // one image for the whole pair (cubic cell), when the range allows
+    bool uni = cell.cubic;
+    double nn[3] = {0.0, 0.0, 0.0};
+    if (uni) {
+        const double *ai = (XM ? xm : pos1) + 3 * (size_t)i0;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            double amin = ai[d], amax = ai[d];
+            for (int si = 1; si < ni; si++) {
+                amin = fmin(amin, ai[3 * si + d]);
+                amax = fmax(amax, ai[3 * si + d]);
+            }
+            double bmin = XM ? mj[0][d] : xj[0][d], bmax = bmin;
+#pragma unroll
+            for (int sj = 1; sj < NS; sj++)
+                if (sj < nj) {
+                    const double b = XM ? mj[sj][d] : xj[sj][d];
+                    bmin = fmin(bmin, b);
+                    bmax = fmax(bmax, b);
+                }
+            const double hid = cell.hi[4 * d];
+            const double lo = nint_rn(__dmul_rn(__dsub_rn(amin, bmax), hid));
+            const double hi = nint_rn(__dmul_rn(__dsub_rn(amax, bmin), hid));
+            uni = uni && lo == hi;
+            nn[d] = lo;
+        }
+    }
+    double sh[3];  // the pair's shift (period_pimd's -NINT * h)
+#pragma unroll
+    for (int d = 0; d < 3; d++) sh[d] = __dmul_rn(-nn[d], cell.h[4 * d]);
+#pragma unroll 1
+    for (int si = 0; si < ni; si++) {
+        const int i = i0 + si;
+        const double xi = pos1[3 * i], yi = pos1[3 * i + 1], zi = pos1[3 * i + 2];
+        double mxi = 0.0, myi = 0.0, mzi = 0.0;
+        if (XM && !uni) {
+            mxi = xm[3 * i];
+            myi = xm[3 * i + 1];
+            mzi = xm[3 * i + 2];
+        }
+#pragma unroll
+        for (int sj = 0; sj < NS; sj++) {
+            if (sj >= nj) break;
+            double dx = __dsub_rn(xi, xj[sj][0]);
+            double dy = __dsub_rn(yi, xj[sj][1]);
+            double dz = __dsub_rn(zi, xj[sj][2]);
+            if (uni) {
+                if (XM) {
+                    dx = __dadd_rn(dx, sh[0]);
+                    dy = __dadd_rn(dy, sh[1]);
+                    dz = __dadd_rn(dz, sh[2]);
+                } else {
+                    dx = __dmul_rn(__dsub_rn(__dmul_rn(dx, cell.hi[0]), nn[0]), cell.h[0]);
+                    dy = __dmul_rn(__dsub_rn(__dmul_rn(dy, cell.hi[4]), nn[1]), cell.h[4]);
+                    dz = __dmul_rn(__dsub_rn(__dmul_rn(dz, cell.hi[8]), nn[2]), cell.h[8]);
+                }
+            } else if (XM) {
+                period_pimd_exact(dx, dy, dz, __dsub_rn(mxi, mj[sj][0]), __dsub_rn(myi, mj[sj][1]),
+                                  __dsub_rn(mzi, mj[sj][2]), cell);
+            } else {
+                period_exact(dx, dy, dz, cell);
+            }
+            const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            const int k = si * NS + sj;
+            if (r2 < tcs2[k]) {
+                maskf |= 1u << k;
+                if (tact[k]) mask |= 1u << k;
+            }
+        }
+    }
+}
+
+// Arguments of the molecule-pair list kernels.  count: per molecule row
+// (pass 0); row, mj, mask, maskf, cap, nsite: the fill (pass 1).  ent
+// (ent_cap entries, nent counted): the pairs the count pass found, written
+// as it goes when they fit, (mi, index in the row, mj, mask | maskf << 16),
+// so that the fill is a scatter; a count pass that found more computes the
+// fill again.
+struct MolListArgs {
+    const int *mstart;
+    int stride;  // sites per molecule when molecule m starts at site m * stride, else 0
+    int ntyp;
+    const double *pos1, *xm;  // bead-1 positions; mode-1 positions or nullptr (one bead)
+    const float4 *msf;        // wrapped fractional site-0 bead-1 positions
+    const double *cutskin2;
+    const int *atm_typ;
+    const double *charge;
+    const int *inter_map, *has_vdw;
+    const double *reach;
+    int *count;
+    const int *row;
+    int *mj;
+    unsigned *mask, *maskf;
+    long long cap;
+    unsigned long long *nsite;
+    int4 *ent;
+    long long ent_cap;
+    unsigned long long *nent;
+};
+
+// Per (si, sj) of the (identical) molecules: cutskin^2 of the pair type
+// and whether the pair carries a force; NS * NS threads of the block.
+template <int NS>
+__device__ __forceinline__ void mol_site_tables(const MolListArgs &a, double *tcs2, unsigned char *tact)
+{
+    const int t = threadIdx.x;
+    if (t < NS * NS) {
+        const int n0 = a.mstart[1] - a.mstart[0];
+        const int si = min(t / NS, n0 - 1), sj = min(t % NS, n0 - 1);
+        const int pt = pair_type(a.atm_typ[si], a.atm_typ[sj], a.ntyp);
+        tcs2[t] = a.cutskin2[pt];
+        tact[t] = (a.has_vdw[a.inter_map[pt]] || a.charge[si] * a.charge[sj] != 0.0) ? 1 : 0;
+    }
+}
+
+// Candidates of one row that passed the bound wait in a per-warp queue (a
+// ring in shared memory) and are tested 32 at a time, one per lane, so the
+// site-pair loop runs on full warps: on a dense row only a few candidates in
+// a warp's 32 pass, and a lane-per-candidate test would keep the whole warp
+// in the site-pair loop for each of them.  The queue keeps the candidates'
+// order, so a row lists its pairs in the order they were enumerated.  The
+// kernels bound four groups of 32 candidates per step (their loads in
+// flight together) and call the test from one place, so that its code,
+// which is most of the kernel, appears once.
+#define PINYB200_QUEUE 256  // ring entries per warp (>= 31 left over + 4 x 32 appended)
+
+struct MolQueue {
+    int *q;    // PINYB200_QUEUE entries
+    int head;  // first waiting entry
+    int nq;    // entries waiting
+};
+
+// Append the lanes with pass set, in lane order.
+__device__ __forceinline__ void mol_queue_append(MolQueue &Q, bool pass, int mj)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned bp = __ballot_sync(0xffffffffu, pass);
+    if (pass) Q.q[(Q.head + Q.nq + __popc(bp & ((1u << lane) - 1u))) & (PINYB200_QUEUE - 1)] = mj;
+    Q.nq += __popc(bp);
+}
+
+// Test every full group of 32 waiting candidates, and with all, the rest.
+template <int FILL, int NS, bool XM>
+__device__ __forceinline__ void mol_queue_drain(MolQueue &Q, bool all, int mi, int i0, int ni, const MolListArgs &a,
+                                                const Cell &cell, const double *tcs2, const unsigned char *tact,
+                                                int &n, long long w0, unsigned long long &sites)
+{
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    while (Q.nq >= 32 || (all && Q.nq > 0)) {
+        const int k = min(Q.nq, 32);
+        unsigned mask = 0, maskf = 0;
+        int mj = 0;
+        if (lane < k) {
+            mj = Q.q[(Q.head + lane) & (PINYB200_QUEUE - 1)];
+            const int j0 = a.stride ? mj * a.stride : a.mstart[mj];
+            const int nj = a.stride ? a.stride : a.mstart[mj + 1] - j0;
+            mol_pair_masks<NS, XM>(i0, ni, j0, nj, a.pos1, a.xm, cell, tcs2, tact, mask, maskf);
+        }
+        Q.head = (Q.head + k) & (PINYB200_QUEUE - 1);
+        Q.nq -= k;
+        const bool keep = maskf != 0;
+        const unsigned bk = __ballot_sync(0xffffffffu, keep);
+        const int below = __popc(bk & ((1u << lane) - 1u));
+        if (FILL) {
+            if (keep) {
+                const long long p = w0 + n + below;
+                if (p < a.cap) {
+                    a.mj[p] = mj;
+                    a.mask[p] = mask;
+                    a.maskf[p] = maskf;
+                }
+            }
+            sites += __popc(mask);
+        } else if (bk) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(a.nent, (unsigned long long)__popc(bk));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (keep && base + __popc(bk) <= (unsigned long long)a.ent_cap)
+                a.ent[base + below] = make_int4(mi, n + below, mj, (int)(mask | (maskf << 16)));
+        }
+        n += __popc(bk);
+    }
+    __syncwarp();
+}
+
+// The fill pass computes only when the count pass's pairs did not fit.
+__device__ __forceinline__ bool fill_from_entries(const MolListArgs &a)
+{
+    return *a.nent <= (unsigned long long)a.ent_cap;
+}
+
+// The sweep: one warp per molecule row mi over every mj < mi, rows taken
+// in pairs (r, nmol - 1 - r) so that every warp sweeps nmol - 1 candidates.
+template <int FILL, int NS, bool XM>
+__global__ void __launch_bounds__(256, 2) mol_list_kernel(const int *__restrict__ gate, int nmol, Cell cell,
+                                                          CellPlanes pl, MolListArgs a,
+                                                          const int *__restrict__ cells)
 {
     if (gate && *gate == 0) return;  // device list update: no rebuild this step
+    if (cells && *cells) return;     // the link-cell kernel builds this list
+    if (FILL && fill_from_entries(a)) return;
+    __shared__ int queue[8][PINYB200_QUEUE];
+    __shared__ double tcs2[NS * NS];
+    __shared__ unsigned char tact[NS * NS];
+    mol_site_tables<NS>(a, tcs2, tact);
+    __syncthreads();
     const int lane = threadIdx.x & 31;
+    MolQueue Q{queue[threadIdx.x >> 5], 0, 0};
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const double R = *reach;
-    const double *x0 = use_xm ? xm : pos1;  // site-0 mode-1 positions for the bound
+    const double Rw = *a.reach + bound_slack(pl);
+    const float R2 = (float)(Rw * Rw);
     unsigned long long sites = 0;
-    for (int mi = warp; mi < nmol; mi += nwarps) {
-        const int i0 = mstart[mi], ni = mstart[mi + 1] - i0;
-        const double bx = x0[3 * (size_t)i0], by = x0[3 * (size_t)i0 + 1], bz = x0[3 * (size_t)i0 + 2];
-        int n = 0;
-        const long long w0 = FILL ? row[mi] : 0;
-        for (int m0 = 0; m0 < mi; m0 += 32) {
-            const int mj = m0 + lane;
-            unsigned mask = 0, maskf = 0;
-            if (mj < mi) {
-                const int j0 = mstart[mj], nj = mstart[mj + 1] - j0;
-                const double lb = image_lower_bound(bx - x0[3 * (size_t)j0], by - x0[3 * (size_t)j0 + 1],
-                                                    bz - x0[3 * (size_t)j0 + 2], cell);
-                if (!(lb > R)) {
-                    for (int si = 0; si < ni; si++) {
-                        const int i = i0 + si;
-                        const double xi = pos1[3 * i], yi = pos1[3 * i + 1], zi = pos1[3 * i + 2];
-                        const int ti = atm_typ[i];
-                        const double qi = charge[i];
-                        for (int sj = 0; sj < nj; sj++) {
-                            const int j = j0 + sj;
-                            double dx = __dsub_rn(xi, pos1[3 * j]);
-                            double dy = __dsub_rn(yi, pos1[3 * j + 1]);
-                            double dz = __dsub_rn(zi, pos1[3 * j + 2]);
-                            if (use_xm)
-                                period_pimd_exact(dx, dy, dz, __dsub_rn(xm[3 * i], xm[3 * j]),
-                                                  __dsub_rn(xm[3 * i + 1], xm[3 * j + 1]),
-                                                  __dsub_rn(xm[3 * i + 2], xm[3 * j + 2]), cell);
-                            else
-                                period_exact(dx, dy, dz, cell);
-                            const double r2 =
-                                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-                            const int pt = pair_type(ti, atm_typ[j], ntyp);
-                            if (r2 < cutskin2[pt]) {
-                                const unsigned bit = 1u << (si * NS + sj);
-                                maskf |= bit;
-                                if (has_vdw[inter_map[pt]] || qi * charge[j] != 0.0) mask |= bit;
-                            }
-                        }
+    for (int rr = warp; 2 * rr < nmol; rr += nwarps) {
+        for (int h = 0; h < 2; h++) {
+            const int mi = h ? nmol - 1 - rr : rr;
+            if (h && mi == rr) break;
+            const int i0 = a.mstart[mi], ni = a.mstart[mi + 1] - i0;
+            const float4 si = a.msf[mi];
+            int n = 0;
+            const long long w0 = FILL ? a.row[mi] : 0;
+            for (int m0 = 0;; m0 += 4 * 32) {
+                const bool last = m0 >= mi;
+                if (!last) {
+                    // four candidates per lane in flight, then their bounds in order
+                    float4 sj[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int mj = m0 + 32 * u + lane;
+                        if (mj < mi) sj[u] = a.msf[mj];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int mj = m0 + 32 * u + lane;
+                        mol_queue_append(Q, mj < mi && !(bound2_frac(si.x - sj[u].x, si.y - sj[u].y,
+                                                                     si.z - sj[u].z, pl) > R2), mj);
                     }
                 }
+                mol_queue_drain<FILL, NS, XM>(Q, last, mi, i0, ni, a, cell, tcs2, tact, n, w0, sites);
+                if (last) break;
             }
-            const bool keep = maskf != 0;
-            const unsigned bk = __ballot_sync(0xffffffffu, keep);
-            if (FILL && keep) {
-                const long long p = w0 + n + __popc(bk & ((1u << lane) - 1u));
-                if (p < cap) {
-                    mj_out[p] = mj;
-                    mask_out[p] = mask;
-                    maskf_out[p] = maskf;
-                }
-            }
-            if (FILL) sites += __popc(mask);
-            n += __popc(bk);
+            if (!FILL && lane == 0) a.count[mi] = n;
         }
-        if (!FILL && lane == 0) count[mi] = n;
     }
     if (FILL) {
         for (int o = 16; o >= 1; o >>= 1) sites += __shfl_xor_sync(0xffffffffu, sites, o);
-        if (lane == 0) atomicAdd(nsite, sites);
+        if (lane == 0) atomicAdd(a.nsite, sites);
+    }
+}
+
+// The fill from the count pass's entries: every pair to its row position.
+__global__ void __launch_bounds__(256) mol_scatter_kernel(const int *__restrict__ gate, MolListArgs a)
+{
+    if (gate && *gate == 0) return;
+    if (!fill_from_entries(a)) return;  // the fill kernels compute
+    const long long ne = (long long)*a.nent;
+    unsigned long long sites = 0;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < ne;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int4 v = a.ent[e];
+        const long long p = (long long)a.row[v.x] + v.y;
+        const unsigned mask = (unsigned)v.w & 0xffffu, maskf = (unsigned)v.w >> 16;
+        if (p < a.cap) {
+            a.mj[p] = v.z;
+            a.mask[p] = mask;
+            a.maskf[p] = maskf;
+        }
+        sites += __popc(mask);
+    }
+    for (int o = 16; o >= 1; o >>= 1) sites += __shfl_xor_sync(0xffffffffu, sites, o);
+    if ((threadIdx.x & 31) == 0 && sites) atomicAdd(a.nsite, sites);
+}
+
+// ---------------------------------------------------------------------------
+// Link cells for the molecule-pair list.
+//
+// PINY builds its Verlet list from a link-cell list by default (update_type
+// lnk_list: make_lnk_lst.c:37, lnk_ver_gen_pad at verlist_control.c:1738).
+// Here the molecules are binned by the wrapped fractional coordinates of
+// their site-0 bead-1 position into n_a x n_b x n_c cells (each n >= 5)
+// whose edges, measured between lattice planes, are at least half the reach
+// R of the bound above.  A pair the bound keeps has, along each axis, a
+// wrapped fractional separation of at most R / plane spacing <= 2 / n, so
+// its cells are at most 2 apart on each axis: the 5 x 5 x 5 cells around a
+// molecule's own hold every candidate.  One block per home cell stages the
+// flattened candidate list of those 125 cells (molecule index and FP32
+// fractional position) in shared memory, a batch at a time; warps take the
+// home molecules, lanes the staged candidates mj < mi, and the pairs that
+// pass the bound go through the warp queue to mol_pair_masks, the criterion
+// of the sweep.  The list holds exactly the sweep's pairs, each row in the
+// order of the neighbour cells and, within a cell, of molecule index (the
+// members of each cell are sorted), so every build of the same positions
+// gives the same list.  The grid is planned at each host build with room for
+// R to grow by 15 %; a device rebuild whose R no longer fits the cells, or
+// whose fullest cell holds more than PINYB200_CELL_HOME molecules, runs the
+// sweep instead (cell_decide_kernel).
+
+#define PINYB200_CELL_BATCH 4096  // candidate molecules staged at a time
+#define PINYB200_CELL_HOME 256    // most molecules of a home cell the kernel keeps row counters for
+
+// Molecules into their cells' ranges (in arrival order; fill: ncell
+// counters, zeroed before).
+__global__ void __launch_bounds__(256) cell_scatter_kernel(const int *__restrict__ gate, int nmol,
+                                                           const int *__restrict__ mcell,
+                                                           const int *__restrict__ coff, int *__restrict__ fill,
+                                                           int *__restrict__ cmol)
+{
+    if (gate && *gate == 0) return;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nmol) return;
+    const int id = mcell[m];
+    cmol[coff[id] + atomicAdd(&fill[id], 1)] = m;
+}
+
+// Each cell's members in index order (one warp per cell, rank by count of
+// smaller indices); cells fuller than the kernel takes are left as they are.
+__global__ void __launch_bounds__(256) cell_sort_kernel(const int *__restrict__ gate, int ncell,
+                                                        const int *__restrict__ coff, const int *__restrict__ in,
+                                                        int *__restrict__ out)
+{
+    if (gate && *gate == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int c = warp; c < ncell; c += nwarps) {
+        const int c0 = coff[c], len = coff[c + 1] - c0;
+        if (len > PINYB200_CELL_HOME) continue;
+        for (int k = lane; k < len; k += 32) {
+            const int m = in[c0 + k];
+            int r = 0;
+            for (int u = 0; u < len; u++) r += in[c0 + u] < m;
+            out[c0 + r] = m;
+        }
+    }
+}
+
+// Whether the cells serve this build: R within the cells' design (R at most
+// twice the narrowest cell edge) and no cell fuller than the kernel takes.
+__global__ void __launch_bounds__(1024) cell_decide_kernel(const int *__restrict__ gate, int ncell,
+                                                           const int *__restrict__ coff,
+                                                           const double *__restrict__ reach, double edge2,
+                                                           int *__restrict__ ok)
+{
+    if (gate && *gate == 0) return;
+    __shared__ int full;
+    if (threadIdx.x == 0) full = 0;
+    __syncthreads();
+    int mx = 0;
+    for (int c = threadIdx.x; c < ncell; c += blockDim.x) mx = max(mx, coff[c + 1] - coff[c]);
+    atomicMax(&full, mx);
+    __syncthreads();
+    if (threadIdx.x == 0) *ok = (*reach * (1.0 + 1e-9) <= edge2 && full <= PINYB200_CELL_HOME) ? 1 : 0;
+}
+
+template <int FILL, int NS, bool XM>
+__global__ void __launch_bounds__(256, 2) mol_list_cell_kernel(const int *__restrict__ gate,
+                                                               const int *__restrict__ ok, int na, int nb, int nc,
+                                                               const int *__restrict__ coff,
+                                                               const int *__restrict__ cmol, CellPlanes pl,
+                                                               Cell cell, MolListArgs a)
+{
+    if (gate && *gate == 0) return;
+    if (!*ok) return;  // the sweep builds this list
+    if (FILL && fill_from_entries(a)) return;
+    extern __shared__ float4 cell_smem[];
+    float4 *sx = cell_smem;  // [BATCH] fractional position, molecule index in .w
+    __shared__ int nbase[125], nstart[126];  // each neighbour cell: start in cmol, start in the flattened list
+    __shared__ int hcnt[PINYB200_CELL_HOME];
+    __shared__ int queue[8][PINYB200_QUEUE];
+    __shared__ double tcs2[NS * NS];
+    __shared__ unsigned char tact[NS * NS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    MolQueue Q{queue[warp], 0, 0};
+    const int home = blockIdx.x;
+    const int ha = home % na, hb = (home / na) % nb, hc = home / (na * nb);
+    const int h0 = coff[home], nhome = coff[home + 1] - h0;
+    if (nhome == 0) return;
+    mol_site_tables<NS>(a, tcs2, tact);
+    if (threadIdx.x < 125) {
+        const int k = threadIdx.x;
+        const int da = k % 5 - 2, db = (k / 5) % 5 - 2, dc = k / 25 - 2;
+        const int cid = ((hc + dc + nc) % nc * nb + (hb + db + nb) % nb) * na + (ha + da + na) % na;
+        nbase[k] = coff[cid];
+        nstart[k + 1] = coff[cid + 1] - coff[cid];
+    }
+    for (int k = threadIdx.x; k < PINYB200_CELL_HOME; k += blockDim.x) hcnt[k] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        nstart[0] = 0;
+        for (int k = 1; k <= 125; k++) nstart[k] += nstart[k - 1];
+    }
+    __syncthreads();
+    const int total = nstart[125];
+    const double Rw = *a.reach + bound_slack(pl);
+    const float R2 = (float)(Rw * Rw);
+    unsigned long long sites = 0;
+    for (int b0 = 0; b0 < total; b0 += PINYB200_CELL_BATCH) {
+        const int nst = min(PINYB200_CELL_BATCH, total - b0);
+        __syncthreads();  // the previous batch is done with the staging buffer
+        for (int e = threadIdx.x; e < nst; e += blockDim.x) {
+            const int f = b0 + e;
+            int lo = 0, hi = 125;  // the neighbour cell k with nstart[k] <= f < nstart[k + 1]
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (nstart[mid] <= f) lo = mid;
+                else hi = mid;
+            }
+            const int mj = cmol[nbase[lo] + f - nstart[lo]];
+            float4 v = a.msf[mj];
+            v.w = __int_as_float(mj);
+            sx[e] = v;
+        }
+        __syncthreads();
+        for (int hk = warp; hk < nhome; hk += nwarp) {
+            const int mi = cmol[h0 + hk];
+            const int i0 = a.mstart[mi], ni = a.mstart[mi + 1] - i0;
+            const float4 si = a.msf[mi];
+            int n = hcnt[hk];
+            const long long w0 = FILL ? a.row[mi] : 0;
+            for (int q0 = 0;; q0 += 4 * 32) {
+                const bool last = q0 >= nst;
+                if (!last) {
+                    float4 sj[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int e = q0 + 32 * u + lane;
+                        sj[u] = e < nst ? sx[e] : make_float4(0.f, 0.f, 0.f, __int_as_float(0x7fffffff));
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int mj = __float_as_int(sj[u].w);  // past the batch: INT_MAX, never < mi
+                        mol_queue_append(Q, mj < mi && !(bound2_frac(si.x - sj[u].x, si.y - sj[u].y,
+                                                                     si.z - sj[u].z, pl) > R2), mj);
+                    }
+                }
+                mol_queue_drain<FILL, NS, XM>(Q, last, mi, i0, ni, a, cell, tcs2, tact, n, w0, sites);
+                if (last) break;
+            }
+            if (lane == 0) hcnt[hk] = n;
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    if (!FILL)
+        for (int hk = threadIdx.x; hk < nhome; hk += blockDim.x) a.count[cmol[h0 + hk]] = hcnt[hk];
+    if (FILL) {
+        for (int o = 16; o >= 1; o >>= 1) sites += __shfl_xor_sync(0xffffffffu, sites, o);
+        if (lane == 0) atomicAdd(a.nsite, sites);
     }
 }
 
@@ -284,36 +749,6 @@ __global__ void __launch_bounds__(256) site_fill_kernel(const int *__restrict__ 
                 wa += __shfl_sync(0xffffffffu, pa, 31);
             }
         }
-    }
-}
-
-__global__ void __launch_bounds__(1024) mol_scan_kernel(const int *__restrict__ gate, int n,
-                                                         const int *__restrict__ count, int *__restrict__ row,
-                                                         long long *__restrict__ tot)
-{
-    if (gate && *gate == 0) return;
-    __shared__ long long part[1024];
-    const int t = threadIdx.x;
-    const int chunk = (n + blockDim.x - 1) / blockDim.x;
-    const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
-    long long s0 = 0;
-    for (int i = lo; i < hi; i++) s0 += count[i];
-    part[t] = s0;
-    __syncthreads();
-    for (int o = 1; o < blockDim.x; o <<= 1) {
-        long long a0 = t >= o ? part[t - o] : 0;
-        __syncthreads();
-        part[t] += a0;
-        __syncthreads();
-    }
-    long long b0 = part[t] - s0;
-    for (int i = lo; i < hi; i++) {
-        row[i] = (int)b0;
-        b0 += count[i];
-    }
-    if (t == blockDim.x - 1) {
-        row[n] = (int)part[t];
-        *tot = part[t];
     }
 }
 
@@ -969,39 +1404,170 @@ __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kerne
 // ---------------------------------------------------------------------------
 // launchers
 
-// pass 0: reach, counts, row offsets and the molecule-pair total (tot[2]);
-// pass 1: the fill, adding the active site pairs into tot[3].
+static CellPlanes cell_planes(const Cell &cell)
+{
+    CellPlanes pl;
+    for (int d = 0; d < 3; d++) {
+        const double b0 = cell.hi[d], b1 = cell.hi[3 + d], b2 = cell.hi[6 + d];
+        pl.w[d] = 1.0 / std::sqrt(b0 * b0 + b1 * b1 + b2 * b2);
+    }
+    pl.ortho = cell.h[1] == 0.0 && cell.h[2] == 0.0 && cell.h[3] == 0.0 && cell.h[5] == 0.0 && cell.h[6] == 0.0 &&
+               cell.h[7] == 0.0;
+    return pl;
+}
+
+// pass 0: reach, fractional positions (and cells), counts with the pairs
+// into the entry buffer when they fit, row offsets and the molecule-pair
+// total (tot[2]); pass 1: the fill (a scatter of the entries, or computed
+// again when they did not fit), adding the active site pairs into tot[3].
 cudaError_t launch_mol_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
                             const double *d_cutskin2, int pass, const int *gate, cudaStream_t st)
 {
     if (!st) st = c->stream;
     const DeviceSystem &s = c->sys;
     const int threads = 256;
-    int blocks = (c->nmol * 32 + threads - 1) / threads;
+    int blocks = (((c->nmol + 1) / 2) * 32 + threads - 1) / threads;  // a warp per pair of rows
     const int maxb = c->sm_count * 8;
     if (blocks > maxb) blocks = maxb;
     if (blocks < 1) blocks = 1;
-    const int use_xm = d_xm != nullptr;
-    if (pass == 0)
-        mol_reach_kernel<<<1, 1024, 0, st>>>(gate, c->nmol, c->d_mstart, d_pos1, d_xm, use_xm, d_cutskin2,
-                                             s.npair_typ, c->d_reach);
-#define MOL_LIST(NSV)                                                                                             \
-    if (pass == 0) {                                                                                              \
-        mol_list_kernel<0, NSV><<<blocks, threads, 0, st>>>(                                                      \
-            gate, c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, use_xm, cell, d_cutskin2, s.atm_typ, s.charge,      \
-            s.inter_map, s.has_vdw, c->d_reach, c->d_mcount, nullptr, nullptr, nullptr, nullptr, 0, nullptr);    \
-        mol_scan_kernel<<<1, 1024, 0, st>>>(gate, c->nmol, c->d_mcount, c->d_mrow, c->d_tot + 2);                 \
-    } else {                                                                                                      \
-        mol_list_kernel<1, NSV><<<blocks, threads, 0, st>>>(                                                      \
-            gate, c->nmol, c->d_mstart, s.ntyp, d_pos1, d_xm, use_xm, cell, d_cutskin2, s.atm_typ, s.charge,      \
-            s.inter_map, s.has_vdw, c->d_reach, c->d_mcount, c->d_mrow, c->d_mj, c->d_mmask, c->d_mmaskf,         \
-            c->mlist_cap, (unsigned long long *)(c->d_tot + 3));                                                  \
+    const bool use_xm = d_xm != nullptr;
+    MolListArgs a{};
+    a.mstart = c->d_mstart;
+    a.stride = c->mol_stride;
+    a.ntyp = s.ntyp;
+    a.pos1 = d_pos1;
+    a.xm = d_xm;
+    a.msf = c->d_msf;
+    a.cutskin2 = d_cutskin2;
+    a.atm_typ = s.atm_typ;
+    a.charge = s.charge;
+    a.inter_map = s.inter_map;
+    a.has_vdw = s.has_vdw;
+    a.reach = c->d_reach;
+    a.count = c->d_mcount;
+    a.ent = c->d_ent;
+    a.ent_cap = c->d_ent ? c->ent_cap : 0;
+    a.nent = c->d_nent;
+    if (pass == 1) {
+        a.row = c->d_mrow;
+        a.mj = c->d_mj;
+        a.mask = c->d_mmask;
+        a.maskf = c->d_mmaskf;
+        a.cap = c->mlist_cap;
+        a.nsite = (unsigned long long *)(c->d_tot + 3);
     }
-    if (c->mol_ns == 3) { MOL_LIST(3) }
-    else if (c->mol_ns == 4) { MOL_LIST(4) }
-    else return cudaErrorInvalidValue;
+    const int ncell = c->cell_n[0] * c->cell_n[1] * c->cell_n[2];
+    const bool cells = ncell > 0;
+    const int *cellok = cells ? c->d_cellok : nullptr;
+    const CellPlanes pl = cell_planes(cell);
+    cudaError_t e;
+    if (pass == 0) {
+        const int mb = (c->nmol + 255) / 256;
+        if ((e = cudaMemsetAsync(c->d_nent, 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
+        if (cells && (e = cudaMemsetAsync(c->d_ccnt, 0, 2 * (size_t)c->cell_cap * sizeof(int), st)) != cudaSuccess)
+            return e;
+        mol_reach_kernel<<<reach_blocks(c), 256, 0, st>>>(gate, c->nmol, c->d_mstart, d_pos1, d_cutskin2,
+                                                          s.npair_typ, c->d_reach_acc, c->d_reach);
+        mol_frac_kernel<<<mb, 256, 0, st>>>(gate, c->nmol, c->d_mstart, d_pos1, cell, c->cell_n[0], c->cell_n[1],
+                                            c->cell_n[2], c->d_msf, cells ? c->d_mcell : nullptr, c->d_ccnt);
+        if (cells) {
+            // cell membership (sorted), the cells' offsets, and whether they serve this build
+            double edge2 = 1e300;
+            for (int d = 0; d < 3; d++) edge2 = std::min(edge2, 2.0 * pl.w[d] / c->cell_n[d]);
+            if ((e = launch_scan(c, gate, ncell, 1, c->d_ccnt, c->d_coff, nullptr, c->d_ctot, st)) != cudaSuccess)
+                return e;
+            cell_scatter_kernel<<<mb, 256, 0, st>>>(gate, c->nmol, c->d_mcell, c->d_coff, c->d_ccnt + c->cell_cap,
+                                                    c->d_cmol);
+            cell_sort_kernel<<<(ncell + 7) / 8, 256, 0, st>>>(gate, ncell, c->d_coff, c->d_cmol,
+                                                              c->d_cmol + c->nmol);
+            cell_decide_kernel<<<1, 1024, 0, st>>>(gate, ncell, c->d_coff, c->d_reach, edge2, c->d_cellok);
+        }
+    }
+    const int cell_smem = PINYB200_CELL_BATCH * (int)sizeof(float4);
+#define MOL_LIST(NSV, FILLV, XMV)                                                                                 \
+    {                                                                                                             \
+        if (cells) {                                                                                              \
+            if ((e = smem_optin((const void *)mol_list_cell_kernel<FILLV, NSV, XMV>, cell_smem)) != cudaSuccess)  \
+                return e;                                                                                         \
+            mol_list_cell_kernel<FILLV, NSV, XMV><<<ncell, 256, cell_smem, st>>>(                                 \
+                gate, cellok, c->cell_n[0], c->cell_n[1], c->cell_n[2], c->d_coff, c->d_cmol + c->nmol, pl, cell,  \
+                a);                                                                                               \
+        }                                                                                                         \
+        mol_list_kernel<FILLV, NSV, XMV><<<blocks, threads, 0, st>>>(gate, c->nmol, cell, pl, a, cellok);       \
+    }
+#define MOL_LIST_XM(NSV, FILLV)                                                                                   \
+    {                                                                                                             \
+        if (use_xm) MOL_LIST(NSV, FILLV, true) else MOL_LIST(NSV, FILLV, false)                                   \
+    }
+    if (c->mol_ns == 3) {
+        if (pass == 0) MOL_LIST_XM(3, 0) else MOL_LIST_XM(3, 1)
+    } else if (c->mol_ns == 4) {
+        if (pass == 0) MOL_LIST_XM(4, 0) else MOL_LIST_XM(4, 1)
+    } else {
+        return cudaErrorInvalidValue;
+    }
+#undef MOL_LIST_XM
 #undef MOL_LIST
-    return cudaGetLastError();
+    if (pass == 1) mol_scatter_kernel<<<c->sm_count * 4, 256, 0, st>>>(gate, a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (pass == 0) return launch_scan(c, gate, c->nmol, 1, c->d_mcount, c->d_mrow, nullptr, c->d_tot + 2, st);
+    return cudaSuccess;
+}
+
+// Plan the link cells for the positions of a host build (reach R measured
+// on the device): n_d = floor(plane spacing / (1.15 R / 2)), at most 64,
+// used when every n_d >= 5 and the 125 cells around a molecule are at most
+// 40 % of the box (below that the sweep's simpler enumeration is as fast);
+// otherwise every build sweeps.  Buffers grow as needed and are kept, so
+// device rebuilds with the same plan allocate nothing.
+int mol_cells_plan(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_cutskin2)
+{
+    cudaError_t e;
+    mol_reach_kernel<<<reach_blocks(c), 256, 0, c->stream>>>(nullptr, c->nmol, c->d_mstart, d_pos1, d_cutskin2,
+                                                             c->sys.npair_typ, c->d_reach_acc, c->d_reach);
+    double R = 0.0;
+    if ((e = cudaMemcpyAsync(&R, c->d_reach, sizeof(double), cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+        return record_error(c, PINYB200_ERR_CUDA, std::string("list cells: ") + cudaGetErrorString(e));
+    int n[3];
+    bool on = c->list_method == PINYB200_LIST_LNK && std::isfinite(R) && R > 0.0;
+    for (int d = 0; d < 3 && on; d++) {
+        const double b0 = cell.hi[d], b1 = cell.hi[3 + d], b2 = cell.hi[6 + d];
+        const double w = 1.0 / std::sqrt(b0 * b0 + b1 * b1 + b2 * b2);
+        const double k = std::floor(w / (1.15 * R / 2.0));
+        n[d] = k > 64.0 ? 64 : (int)k;
+        on = n[d] >= 5;
+    }
+    const long long ncell = on ? (long long)n[0] * n[1] * n[2] : 0;
+    if (!on || ncell * 2 < 625) {  // 125 / ncell > 0.4
+        c->cell_n[0] = c->cell_n[1] = c->cell_n[2] = 0;
+        return PINYB200_OK;
+    }
+    auto alloc = [&](void **p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    };
+    e = cudaSuccess;
+    if (!c->d_mcell) {
+        alloc((void **)&c->d_mcell, (size_t)c->nmol * sizeof(int));
+        alloc((void **)&c->d_cmol, 2 * (size_t)c->nmol * sizeof(int));
+        alloc((void **)&c->d_cellok, sizeof(int));
+        alloc((void **)&c->d_ctot, sizeof(long long));
+    }
+    if (ncell > c->cell_cap) {
+        if (c->d_ccnt) cudaFree(c->d_ccnt);
+        if (c->d_coff) cudaFree(c->d_coff);
+        c->d_ccnt = c->d_coff = nullptr;
+        c->cell_cap = 0;
+        alloc((void **)&c->d_ccnt, 2 * (size_t)ncell * sizeof(int));
+        alloc((void **)&c->d_coff, ((size_t)ncell + 1) * sizeof(int));
+        if (e == cudaSuccess) c->cell_cap = (int)ncell;
+    }
+    if (e != cudaSuccess) {
+        c->cell_n[0] = c->cell_n[1] = c->cell_n[2] = 0;
+        return record_error(c, PINYB200_ERR_CUDA, std::string("list cells: ") + cudaGetErrorString(e));
+    }
+    for (int d = 0; d < 3; d++) c->cell_n[d] = n[d];
+    return PINYB200_OK;
 }
 
 // Site lists from the molecule list.  pass 0: counts, row offsets, totals
@@ -1019,7 +1585,6 @@ cudaError_t launch_site_from_mol(pinyb200_ctx *c, int pass, const int *gate, cud
     if (pass == 0) {                                                                                               \
         site_count_kernel<NSV><<<blocks, threads, 0, st>>>(gate, c->nmol, natm, c->d_mstart, c->d_mrow, c->d_mmaskf, \
                                                            c->d_mmask, c->mlist_cap, c->d_count);                 \
-        scan_kernel<<<1, 1024, 0, st>>>(gate, natm, c->d_count, c->d_row, c->d_rowA, c->d_tot);                   \
     } else {                                                                                                       \
         site_fill_kernel<NSV><<<blocks, threads, 0, st>>>(gate, c->nmol, c->d_mstart, c->d_mrow, c->d_mj,          \
                                                           c->d_mmaskf, c->d_mmask, c->mlist_cap, c->d_row,        \
@@ -1029,7 +1594,10 @@ cudaError_t launch_site_from_mol(pinyb200_ctx *c, int pass, const int *gate, cud
     else if (c->mol_ns == 4) { SITE_LIST(4) }
     else return cudaErrorInvalidValue;
 #undef SITE_LIST
-    return cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (pass == 0) return launch_scan(c, gate, natm, 2, c->d_count, c->d_row, c->d_rowA, c->d_tot, st);
+    return cudaSuccess;
 }
 
 template <typename R, int P, int NS>

@@ -85,7 +85,6 @@ __global__ void __launch_bounds__(256) respa_list_kernel(const int *__restrict__
         }
         if (!FILL && lane == 0) {
             count[i] = n;
-            count[natm + i] = n;  // the scan fills two row arrays: both are rowR
         }
     }
 }
@@ -134,11 +133,12 @@ int respa_list_enqueue(pinyb200_ctx *c, const Cell &cell, const int *gate, cudaS
     respa_list_kernel<0><<<blocks, threads, 0, st>>>(gate, s.natm, s.ntyp, c->d_x0, c->d_xm0, use_xm, cell, c->d_cs0,
                                                      s.cutoff, c->d_cut_res, s.atm_typ, c->d_rowA, c->d_colA,
                                                      c->d_count, nullptr, nullptr, 0);
-    scan_kernel<<<1, 1024, 0, st>>>(gate, s.natm, c->d_count, c->d_rowR, c->d_rowR, c->d_rtot);
+    cudaError_t e = launch_scan(c, gate, s.natm, 1, c->d_count, c->d_rowR, nullptr, c->d_rtot, st);
+    if (e != cudaSuccess) return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
     respa_list_kernel<1><<<blocks, threads, 0, st>>>(gate, s.natm, s.ntyp, c->d_x0, c->d_xm0, use_xm, cell, c->d_cs0,
                                                      s.cutoff, c->d_cut_res, s.atm_typ, c->d_rowA, c->d_colA,
                                                      nullptr, c->d_rowR, c->d_colR, c->res_cap);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess) return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
     return PINYB200_OK;
 }

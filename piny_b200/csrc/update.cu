@@ -169,7 +169,9 @@ int list_update_enqueue(pinyb200_ctx *c, const double *d_pos, const double *d_xm
         const int ch = PINYB200_MOL_CHUNK * jpi;
         const int blocks = (c->nmol + 255) / 256;
         ls_chunk_count_kernel<<<blocks, 256, 0, st>>>(gate, c->nmol, c->d_mrow, ch, c->d_mchunk);
-        mol_scan_kernel<<<1, 1024, 0, st>>>(gate, c->nmol, c->d_mchunk, c->d_mchunk + c->nmol, chunk_tot);
+        if ((e = launch_scan(c, gate, c->nmol, 1, c->d_mchunk, c->d_mchunk + c->nmol, nullptr, chunk_tot, st)) !=
+            cudaSuccess)
+            return record_error(c, PINYB200_ERR_CUDA, cudaGetErrorString(e));
         ls_chunk_fill_kernel<<<blocks, 256, 0, st>>>(gate, c->nmol, c->d_mrow, ch, c->d_mchunk,
                                                      c->d_mchunk + c->nmol, c->d_chunk, c->chunk_cap);
     } else if ((e = launch_build_list(c, cell, d_pos, xm, c->d_cs, 0, gate, st)) != cudaSuccess ||

@@ -87,44 +87,6 @@ __global__ void __launch_bounds__(256) list_kernel(const int *__restrict__ gate,
     }
 }
 
-// Exclusive scan of two count arrays (full, active) into row pointers; one
-// block, each thread sums a contiguous chunk.
-__global__ void __launch_bounds__(1024) scan_kernel(const int *__restrict__ gate, int n, const int *__restrict__ count,
-                                                     int *__restrict__ row, int *__restrict__ rowA,
-                                                     long long *__restrict__ tot)
-{
-    if (gate && *gate == 0) return;
-    __shared__ long long part[2][1024];
-    const int t = threadIdx.x;
-    const int chunk = (n + blockDim.x - 1) / blockDim.x;
-    const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
-    long long s0 = 0, s1 = 0;
-    for (int i = lo; i < hi; i++) { s0 += count[i]; s1 += count[n + i]; }
-    part[0][t] = s0;
-    part[1][t] = s1;
-    __syncthreads();
-    for (int o = 1; o < blockDim.x; o <<= 1) {
-        long long a0 = t >= o ? part[0][t - o] : 0, a1 = t >= o ? part[1][t - o] : 0;
-        __syncthreads();
-        part[0][t] += a0;
-        part[1][t] += a1;
-        __syncthreads();
-    }
-    long long b0 = part[0][t] - s0, b1 = part[1][t] - s1;
-    for (int i = lo; i < hi; i++) {
-        row[i] = (int)b0;
-        rowA[i] = (int)b1;
-        b0 += count[i];
-        b1 += count[n + i];
-    }
-    if (t == blockDim.x - 1) {
-        row[n] = (int)part[0][t];
-        rowA[n] = (int)part[1][t];
-        tot[0] = part[0][t];
-        tot[1] = part[1][t];
-    }
-}
-
 cudaError_t launch_build_list(pinyb200_ctx *c, const Cell &cell, const double *d_pos1, const double *d_xm,
                               const double *d_cutskin2, int pass, const int *gate, cudaStream_t st)
 {
@@ -139,7 +101,9 @@ cudaError_t launch_build_list(pinyb200_ctx *c, const Cell &cell, const double *d
                                                           d_cutskin2, s.atm_typ, s.charge, s.inter_map, s.has_vdw,
                                                           s.excl_off, s.excl_j, c->d_count, nullptr, nullptr,
                                                           nullptr, nullptr, 0);
-        scan_kernel<<<1, 1024, 0, st>>>(gate, s.natm, c->d_count, c->d_row, c->d_rowA, c->d_tot);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        return launch_scan(c, gate, s.natm, 2, c->d_count, c->d_row, c->d_rowA, c->d_tot, st);
     } else {
         list_kernel<1><<<blocks, threads, 0, st>>>(gate, s.natm, s.ntyp, d_pos1, d_xm, d_xm != nullptr, cell,
                                                           d_cutskin2, s.atm_typ, s.charge, s.inter_map, s.has_vdw,

@@ -113,8 +113,10 @@ EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb
            "pinyb200_pimd_set_nhc", "pinyb200_pimd_get_nhc", "pinyb200_pimd_forces", "pinyb200_pimd_step",
            "pinyb200_update_list_device", "pinyb200_list_set_spread", "pinyb200_list_status",
            "pinyb200_set_respa", "pinyb200_respa_force_device", "pinyb200_piny_force_respa",
-           "pinyb200_set_kernel_timing", "pinyb200_kernel_times")
+           "pinyb200_set_kernel_timing", "pinyb200_kernel_times", "pinyb200_set_list_method",
+           "pinyb200_list_cells")
 
+LIST_LNK, LIST_NOLST = 0, 1                       # PINYB200_LIST_LNK / _NOLST
 STAGING, NORMAL_MODES = 1, 2                      # PINYB200_STAGING / _NORMAL_MODES
 TO_MODES, TO_BEADS, FORCE_TO_MODES = 0, 1, 2      # PINYB200_TO_MODES / _TO_BEADS / _FORCE_TO_MODES
 
@@ -145,6 +147,8 @@ def load(build_if_missing: bool = True):
     L.pinyb200_destroy.argtypes = [C.c_void_p]
     L.pinyb200_build_list.argtypes = [C.c_void_p, _pd, _pd, _pd, _pd, C.POINTER(C.c_long)]
     L.pinyb200_get_list.argtypes = [C.c_void_p, _pi, _pi, C.c_long, C.POINTER(C.c_long)]
+    L.pinyb200_set_list_method.argtypes = [C.c_void_p, _i]
+    L.pinyb200_list_cells.argtypes = [C.c_void_p, _pi]
     L.pinyb200_list_info.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long), C.POINTER(C.c_long)]
     L.pinyb200_energy_force.argtypes = [C.c_void_p, _pd, _pd, _pd, _i, _pd, C.POINTER(PinyEnergies)]
     L.pinyb200_energy_force_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _pd, _i, C.c_void_p,
@@ -342,6 +346,16 @@ class DeviceBox:
         self._check(self.L.pinyb200_get_list(self.h, pi.ctypes.data_as(_pi), pj.ctypes.data_as(_pi), n.value,
                                              C.byref(n)), "get_list")
         return pi[:n.value], pj[:n.value]
+
+    def set_list_method(self, method):
+        """LIST_LNK (link cells when the box allows, the default) or LIST_NOLST (all-pairs sweep)."""
+        self._check(self.L.pinyb200_set_list_method(self.h, int(method)), "set_list_method")
+
+    def list_cells(self):
+        """Cells along a, b, c of the current list's plan (zeros: swept) and whether the cells built it."""
+        cells = np.zeros(4, np.int32)
+        self._check(self.L.pinyb200_list_cells(self.h, cells.ctypes.data_as(_pi)), "list_cells")
+        return tuple(int(v) for v in cells[:3]), bool(cells[3])
 
     def list_info(self):
         n, a, c = C.c_long(), C.c_long(), C.c_long()
