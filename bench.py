@@ -47,7 +47,8 @@ def parse_args():
                          "c5_grad: parameter gradients of 1024 TIP4P/F x 16 beads; "
                          "pimd_nvt: PINY's NVT ring-polymer MD step of 4096 TIP4P/F x 32 beads; "
                          "respa: the force calls of one PINY RESPA step (respa_steps_lrf 2, respa_steps_intra 2) "
-                         "of 4096 TIP4P/F x 32 beads; pimd_nvt_respa: the NVT PIMD step with those RESPA loops")
+                         "of 4096 TIP4P/F x 32 beads; pimd_nvt_respa: the NVT PIMD step with those RESPA loops; "
+                         "list_<N>: Verlet-list builds of N TIP4P/F molecules x 4 beads, link cells and sweep")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
@@ -421,6 +422,95 @@ def run_reference_sampled(args):
                              **cpu_info()},
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+    return 0
+
+
+def list_timing(S, P, ns, pos, xmod, precision, dev, reps=5, methods=None):
+    """Verlet-list builds of one box: the host call pinyb200_build_list
+    (wall time, median of reps after one) and device rebuilds
+    (pinyb200_update_list_device, CUDA events on the stream, median) with
+    the molecules moved rigidly between calls so that each one rebuilds,
+    per list method (link cells / sweep)."""
+    import torch
+
+    from piny_b200 import lib
+    from piny_b200.lib import DeviceBox
+    rng = np.random.default_rng(3)
+    natm = int(S["natm"])
+    # rigid molecule moves: one random vector per molecule of ns consecutive sites
+    mol_of = np.arange(natm) // ns
+    shift = rng.normal(scale=0.4, size=(natm // ns, 3))[mol_of]
+    p2 = pos + shift[None]
+    d0 = torch.from_numpy(pos).to(dev)
+    d2 = torch.from_numpy(p2).to(dev)
+    x0 = torch.from_numpy(np.ascontiguousarray(pos.mean(axis=0))).to(dev)
+    x2 = torch.from_numpy(np.ascontiguousarray(p2.mean(axis=0))).to(dev)
+    # the rebuild is enqueued without a host wait: time it on a stream of its own
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.synchronize()
+    out = {}
+    for method, name in ((lib.LIST_LNK, "lnk"), (lib.LIST_NOLST, "nolst")):
+        if methods and name not in methods:
+            continue
+        box = DeviceBox(S, P, precision)
+        box.set_list_method(method)
+        host = []
+        for k in range(reps + 1):
+            t0 = time.perf_counter()
+            npairs = box.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+            host.append(time.perf_counter() - t0)
+        cells, _ = box.list_cells()
+        sp0 = box.check_list_device(d0.data_ptr(), 0.0)[2]
+        box.list_set_spread(sp0)
+        dev_ms, used = [], []
+        for k in range(2 * reps + 1):
+            d, x = (d2, x2) if k % 2 == 0 else (d0, x0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            box.update_list_device(d.data_ptr(), x.data_ptr(), S["hmat"], stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            if k:
+                dev_ms.append(e0.elapsed_time(e1))
+                used.append(box.list_cells()[1])
+        st = box.list_status(stream=stream.cuda_stream)
+        out[name] = {"host_build_ms": 1e3 * float(np.median(host[1:])), "device_rebuild_ms": float(np.median(dev_ms)),
+                     "device_rebuilds": int(st["rebuilds"]), "cells": list(cells),
+                     "cells_used_on_device": bool(all(used)), "npairs": int(npairs)}
+        box.close()
+    return out
+
+
+def run_list(args, ws, rank, local):
+    """--config list_<N>: list builds of N TIP4P/F molecules x 4 beads;
+    list_<named box>: of that box (e.g. list_tip4pf_4096_p32)."""
+    import torch
+
+    from piny_b200 import system, water
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    what = args.config[len("list_"):]
+    if what.isdigit():
+        nmol = int(what)
+        spec = water.BoxSpec(water.TIP4P_F, nmol, water.density_box_edge(nmol), 4, 298.0, 7, grid=32, order=6)
+    else:
+        spec = water.named_spec(what)
+        nmol = spec.nmol
+    pos = water.build_positions(spec) / water.BOHR
+    S = system.build_system(spec, pos)
+    res = list_timing(S, spec.nbeads, spec.model.nsite, pos, pos.mean(axis=0), args.precision, dev,
+                      reps=max(3, args.steps))
+    if rank == 0:
+        best = min(v["device_rebuild_ms"] for v in res.values())
+        print(json.dumps({"metric": "Verlet-list device rebuilds/s (%s %d mol x %d beads)" %
+                                    (spec.model.name, nmol, spec.nbeads),
+                          "value": 1e3 / best, "unit": "rebuilds/s", "n_gpus": 1, "steps": max(3, args.steps),
+                          "warmup": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": "list build, %d %s molecules, %d beads, box %.1f A, "
+                                                 "rigid molecule moves of 0.4 Bohr rms per component" %
+                                                 (nmol, spec.model.name, spec.nbeads, spec.L)},
+                          "methods": res}))
     return 0
 
 
@@ -1021,6 +1111,8 @@ def main():
         return run_pimd(args, ws, rank, local)
     if args.config == "respa":
         return run_respa(args, ws, rank, local)
+    if args.config.startswith("list_"):
+        return run_list(args, ws, rank, local)
 
     import torch
 
@@ -1209,6 +1301,12 @@ def main():
     except Exception as exc:  # reported, not fatal
         alu = {"error": str(exc)}
 
+    # Verlet-list builds of this box (host call and device rebuild)
+    try:
+        lists = list_timing(S, P, spec.model.nsite, pos, xmod, args.precision, dev, reps=3)
+    except Exception as exc:  # reported, not fatal
+        lists = {"error": str(exc)}
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -1227,6 +1325,7 @@ def main():
             "kernels": kernels,
             "vs_piny": piny,
             "alu_roofline": alu,
+            "list_build": lists,
             "cpu_baseline": cpu,
             "e2e": {"value": ws * P / (e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e},
