@@ -152,7 +152,7 @@ int pinyb200_autotune(pinyb200_ctx *c, const double *d_pos, const double *d_xmod
     std::vector<int> variants = {1};
     if (c->use_mol && c->mol_ok) variants.insert(variants.begin(), 0);
     if (c->use_mol && c->mol_ok && c->mix_ok) variants.push_back(2);
-    const int bps[5] = {4, 6, 8, 16, 32};
+    const int bps[5] = {4, 5, 8, 16, 32};
     int best[4];
     get_choice(c, best);
     float tbest = 1e30f;

@@ -253,9 +253,9 @@ static void mixed_setup(pinyb200_ctx *c, const pinyb200_system *s, int n0)
         if (upload((float **)&c->d_tabfe, fe.data(), fe.size()) != cudaSuccess) return;
     }
     c->mix_ok = (size_t)c->sys.nuniq * per * 4 < (size_t)0x7fffffff;
-    // one wave of resident blocks (6 per SM at its register count) serves
+    // one wave of resident blocks (5 per SM at its register count) serves
     // the grid-strided chunks best at the benchmark sizes
-    if (c->mix_ok) c->pair_blocks_per_sm = 6;
+    if (c->mix_ok) c->pair_blocks_per_sm = 5;
 }
 
 extern "C" {

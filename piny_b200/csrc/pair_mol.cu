@@ -1153,6 +1153,15 @@ __device__ __forceinline__ float4 ldg_keep(const float4 *p)
     return v;
 }
 
+// The force and energy rows of one interval (32 bytes, 32-byte aligned) in
+// one 256-bit load: one L1 request per lane instead of two.
+__device__ __forceinline__ void ldg_keep_pair(const float4 *p, float4 &f, float4 &e)
+{
+    asm("ld.global.nc.L1::evict_last.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(f.x), "=f"(f.y), "=f"(f.z), "=f"(f.w), "=f"(e.x), "=f"(e.y), "=f"(e.z), "=f"(e.w)
+        : "l"(p));
+}
+
 struct MixArgs {
     const int *nchunk, *chunk, *bad, *mj;
     const unsigned *mask;
@@ -1175,8 +1184,11 @@ struct MixArgs {
     float rc2, dri_f, rmd, tmax;  // cutoff^2, 1/dr, rmin/dr, last interval
 };
 
+// Resident blocks per SM of the MIXED molecule-pair kernel: 5 x 128
+// threads leave it 96 registers and no spills (at 6, 85 registers spilled
+// ~180 bytes per thread into L1, the cache its table gathers depend on).
 #ifndef PINYB200_MIX_BLOCKS
-#define PINYB200_MIX_BLOCKS 6
+#define PINYB200_MIX_BLOCKS 5
 #endif
 
 // Site-pair table patterns known at compile time: bit si * NS + sj of CM
@@ -1314,8 +1326,7 @@ __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kerne
                         if (coul) {
                             float4 cf;
                             if (ENERGY) {
-                                cf = ldg_keep(rfe + 2 * a.tstride);
-                                ecf = ldg_keep(rfe + 2 * a.tstride + 1);
+                                ldg_keep_pair(rfe + 2 * a.tstride, cf, ecf);
                             } else {
                                 cf = ldg_keep(row + T_CDV0C * a.tstride);
                             }
@@ -1324,8 +1335,7 @@ __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kerne
                         if (vdw) {
                             float4 cf;
                             if (ENERGY) {
-                                cf = ldg_keep(rfe);
-                                evf = ldg_keep(rfe + 1);
+                                ldg_keep_pair(rfe, cf, evf);
                             } else {
                                 cf = ldg_keep(row + T_CDV0 * a.tstride);
                             }
