@@ -322,8 +322,20 @@ int pinyb200_piny_force(pinyb200_ctx *ctx, double *const *x,
  *                  wght_ter_res (ecorr.c:97-106) and at the outer level as
  *                  ecor_both, wght_ter F + (wght_ter_res - wght_ter) F_res
  *                  (ecorr.c:349-351, :497-505)
- *   pme_res_on     part_mesh.pme_res_on: a separate RESPA PME grid; not
- *                  supported (PINYB200_ERR_UNSUPPORTED)
+ *   pme_res_on     part_mesh.pme_res_on (ewald_respa_pme_opt on): the
+ *                  RESPA reciprocal set on its own PME mesh
+ *                  (energy_control_inter_recip.c:215-271, irespa = 1 in
+ *                  ewald3d_pme.c:204-216): at inner inter levels PME on
+ *                  that mesh x wght_ter_res; at the outer level PME on
+ *                  the full mesh x wght_ter plus PME on the RESPA mesh x
+ *                  (wght_ter_res - wght_ter), both added unweighted to the
+ *                  virial forces (ewald3d_pme.c:563-585), the energy and
+ *                  pvten_tot from the full mesh only
+ *   ngrid_res, n_interp_res
+ *                  part_mesh.ngrid_a_res/_b_res/_c_res, n_interp_res
+ *   kastr_res, kbstr_res, kcstr_res
+ *                  ewald.kastr_res... (nktot_res each): the RESPA k sphere
+ *   bweight_res    part_mesh.bweight_tot_res (nktot_res)
  *   ecor_cdv0_res  ecor.cdv0_res (ecor_nsplin entries) when nktot_res > 0
  * pinyb200_respa_force_device evaluates one level, `level` being the OR of
  * the PINYB200_* flag bits below that PINY has set: one of
@@ -358,6 +370,10 @@ typedef struct pinyb200_respa {
     int nktot_res;
     int pme_res_on;
     const double *ecor_cdv0_res;
+    int ngrid_res[3];
+    int n_interp_res;
+    const int *kastr_res, *kbstr_res, *kcstr_res;
+    const double *bweight_res;
 } pinyb200_respa;
 int pinyb200_set_respa(pinyb200_ctx *ctx, const pinyb200_respa *r);
 int pinyb200_respa_force_device(pinyb200_ctx *ctx, const double *d_pos,

@@ -56,6 +56,8 @@ class OrcRespa(C.Structure):
         ("int_res_ter", _i), ("int_res_inter", _i), ("ires_bond", _i),
         ("cutoff_res", _pd), ("rheal_res", _d), ("bond_eq_res", _pd),
         ("nktot_res", _i), ("ecor_cdv0_res", _pd),
+        ("pme_res_on", _i), ("ngrid_res", _i * 3), ("n_interp_res", _i),
+        ("kastr_res", _pi), ("kbstr_res", _pi), ("kcstr_res", _pi), ("bweight_res", _pd),
     ]
 
 
@@ -306,20 +308,30 @@ class Oracle:
         """orc_respa_force: PINY's weighted forces at one RESPA level and, at
         a full inter level, the virial forces (else None).  ``respa`` holds
         wght_ter, wght_ter_res, wght_tra_res, int_res_ter, int_res_inter,
-        ires_bond, cutoff_res [npair_typ], rheal_res, bond_eq_res."""
+        ires_bond, cutoff_res [npair_typ], rheal_res, bond_eq_res and, for
+        the reciprocal RESPA set, nktot_res, ecor_cdv0_res and (PINY's
+        separate RESPA PME mesh) pme_res_on, ngrid_res, n_interp_res,
+        kastr_res, kbstr_res, kcstr_res, bweight_res."""
         s = self.make_struct(sysd)
         r = OrcRespa()
         keep = []
         for name, ctype in OrcRespa._fields_:
             v = respa.get(name)
             if v is None:
-                v = np.zeros(1) if ctype is _pd else 0
+                v = np.zeros(1) if ctype in (_pd, _pi) else (None if ctype is _i * 3 else 0)
             if ctype is _pd:
                 a, p = self._d(v)
                 keep.append(a)
                 setattr(r, name, p)
+            elif ctype is _pi:
+                a, p = self._i(v)
+                keep.append(a)
+                setattr(r, name, p)
+            elif ctype is _i * 3:
+                if v is not None:
+                    r.ngrid_res[:] = [int(x) for x in v]
             else:
-                setattr(r, name, v)
+                setattr(r, name, int(v) if ctype is _i else v)
         pos = np.ascontiguousarray(pos, np.float64)
         P = pos.shape[0]
         force = np.zeros_like(pos)

@@ -1152,10 +1152,45 @@ void orc_respa_force(const orc_system *s, const orc_respa *r, int level, int P,
          * forces x wght_now, ecorr.c:100 wfor); with it (one grid) PME at
          * every inner inter step x wght_ter_res, ecor from the RESPA table
          * x wght_ter_res (ecorr.c:103-106) or, at full steps, ecor_both
-         * (ecorr.c:349-351, :497-505) */
+         * (ecorr.c:349-351, :497-505).  With the separate RESPA mesh
+         * (:215-271): PME on that mesh (the RESPA k sphere, irespa = 1,
+         * ewald3d_pme.c:204-216) x wght_ter_res at inner inter steps; at full
+         * steps x (wght_ter_res - wght_ter) and the full-mesh PME x wght_ter,
+         * both unweighted into the virial forces (ewald3d_pme.c:563-585) */
         const int kres = r->nktot_res > 0;
-        if (kres && res_inter) {
+        if (kres && res_inter && r->pme_res_on) {
             if (s->nktot > 0) {
+                orc_system sr = *s;
+                sr.ngrid_a = r->ngrid_res[0];
+                sr.ngrid_b = r->ngrid_res[1];
+                sr.ngrid_c = r->ngrid_res[2];
+                sr.n_interp = r->n_interp_res;
+                sr.nktot = r->nktot_res;
+                sr.kastr = r->kastr_res;
+                sr.kbstr = r->kbstr_res;
+                sr.kcstr = r->kcstr_res;
+                sr.bweight = r->bweight_res;
+                double pvr[10] = {0};
+                memset(tmp, 0, sizeof(double) * 3 * natm);
+                pme_bead(&sr, pos, h, hi, vol, tmp, pvr);
+                const double wr = full_inter ? w_res - w_full : w_res;
+                for (long a = 0; a < 3 * natm; a++) {
+                    if (ft) ft[a] += tmp[a];
+                    f[a] += tmp[a] * wr;
+                }
+                if (full_inter) {
+                    double pvf[10] = {0};
+                    memset(tmp, 0, sizeof(double) * 3 * natm);
+                    pme_bead(s, pos, h, hi, vol, tmp, pvf);
+                    for (long a = 0; a < 3 * natm; a++) {
+                        ft[a] += tmp[a];
+                        f[a] += tmp[a] * w_full;
+                    }
+                }
+            }
+        }
+        if (kres && res_inter) {
+            if (s->nktot > 0 && !r->pme_res_on) {
                 double pvr[10] = {0};
                 memset(tmp, 0, sizeof(double) * 3 * natm);
                 pme_bead(s, pos, h, hi, vol, tmp, pvr);

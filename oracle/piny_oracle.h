@@ -128,8 +128,15 @@ typedef struct orc_respa {
     const double *cutoff_res;   /* [npair_typ] interact.cutoff_res (Bohr)   */
     double rheal_res;           /* interact.rheal_res (Bohr)                */
     const double *bond_eq_res;  /* [nbond_typ] bond.eq_pow_res              */
-    int nktot_res;              /* ewald.nktot_res (one PME grid)           */
+    int nktot_res;              /* ewald.nktot_res                          */
     const double *ecor_cdv0_res; /* [ecor_nsplin] ecor.cdv0_res             */
+    /* PINY's separate RESPA PME mesh (part_mesh.pme_res_on): mesh, order,
+     * RESPA k sphere and its B-spline weights (bweight_tot_res)           */
+    int pme_res_on;
+    int ngrid_res[3];
+    int n_interp_res;
+    const int *kastr_res, *kbstr_res, *kcstr_res;
+    const double *bweight_res;
 } orc_respa;
 #define ORC_FULL_INTER 1
 #define ORC_RES_INTER 2

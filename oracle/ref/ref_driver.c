@@ -772,6 +772,18 @@ static int run_respa(const char *dir, const char *input, const char *outpath)
     if (bonded_.bond.npow > 0) putd("bond_eq_res", bonded_.bond.eq_pow_res, bonded_.bond.ntyp_pow);
     put1i("nktot_res", gd_.ewald.nktot_res);
     put1i("pme_res_on", class_.part_mesh.pme_res_on);
+    if (class_.part_mesh.pme_res_on && gd_.ewald.nktot_res > 0) {
+        /* the separate RESPA PME grid: its mesh, order, k sphere and weights */
+        const PART_MESH *pm = &class_.part_mesh;
+        const int g3[3] = {pm->ngrid_a_res, pm->ngrid_b_res, pm->ngrid_c_res};
+        put("ngrid_res", 'i', g3, 3);
+        put1i("n_interp_res", pm->n_interp_res);
+        put1i("kmax_pme_res", pm->kmax_pme_res);
+        puti("kastr_res", gd_.ewald.kastr_res, gd_.ewald.nktot_res);
+        puti("kbstr_res", gd_.ewald.kbstr_res, gd_.ewald.nktot_res);
+        puti("kcstr_res", gd_.ewald.kcstr_res, gd_.ewald.nktot_res);
+        putd("bweight_tot_res", pm->bweight_tot_res, gd_.ewald.nktot_res);
+    }
     if (bonded_.ecor.num > 0 && bonded_.ecor.nktot_res > 0) {
         putd("ecor_cdv0_res", bonded_.ecor.cdv0_res, bonded_.ecor.nsplin);
         put1d("ecor_ecut_res", bonded_.ecor.ecut_res);

@@ -195,6 +195,132 @@ static int pme_tiles_setup(pinyb200_ctx *c, int T)
     return PINYB200_OK;
 }
 
+// PME mesh of one reciprocal set into the context's PME fields (sys.ngrid,
+// k list, B-spline weights, k mask; grid, spectrum, filter, tiles, records,
+// twiddles): the evaluation's mesh at creation, PINY's RESPA mesh into a
+// PmeSet by way of pme_swap.
+static int pme_alloc(pinyb200_ctx *c, int nbeads, const int *ngrid, int n_interp, int nktot, const int *kastr,
+                     const int *kbstr, const int *kcstr, const double *bweight)
+{
+    DeviceSystem &d = c->sys;
+    d.nktot = nktot;
+    d.ngrid[0] = ngrid[0];
+    d.ngrid[1] = ngrid[1];
+    d.ngrid[2] = ngrid[2];
+    d.n_interp = n_interp;
+    if (nktot > 0) {
+        std::vector<int> kv((size_t)3 * nktot);
+        for (int i = 0; i < nktot; i++) {
+            kv[3 * i] = kastr[i];
+            kv[3 * i + 1] = kbstr[i];
+            kv[3 * i + 2] = kcstr[i];
+        }
+        CK(upload(&d.kvec, kv.data(), kv.size()));
+        CK(upload(&d.bweight, bweight, nktot));
+        const int Na = ngrid[0], Nb = ngrid[1], Nc = ngrid[2];
+        const size_t G = (size_t)Na * Nb * Nc;
+        std::vector<int> mask(G, -1);
+        for (int i = 0; i < nktot; i++) {
+            int a = ((kastr[i] % Na) + Na) % Na, b = ((kbstr[i] % Nb) + Nb) % Nb, cc = ((kcstr[i] % Nc) + Nc) % Nc;
+            mask[((size_t)cc * Nb + b) * Na + a] = i;
+            int am = (Na - a) % Na, bm = (Nb - b) % Nb, cm = (Nc - cc) % Nc;
+            mask[((size_t)cm * Nb + bm) * Na + am] = i;
+        }
+        CK(upload(&d.kmask, mask.data(), G));
+        CK(cudaMalloc(&c->d_filter, G * (sizeof(double) + sizeof(float))));
+        const bool f64 = c->precision == PINYB200_FP64;
+        if (pme_plane_smem(Na, Nb, f64) > 220 * 1024 || pme_slab_smem(Na, Nc, f64) > 220 * 1024)
+            return fail(c, PINYB200_ERR_UNSUPPORTED, "PME grid plane too large for shared memory");
+        const size_t rsz = f64 ? sizeof(double) : sizeof(float);
+        const size_t csz = f64 ? sizeof(double2) : sizeof(float2);
+        CK(cudaMalloc(&c->d_grid, rsz * G * nbeads));
+        CK(cudaMalloc(&c->d_spec, csz * (size_t)Nc * Nb * (Na / 2 + 1) * nbeads));
+        // charge bins per grid tile and bead: 16^3 tiles, or 8^3 on small
+        // meshes so that spread and gather still get enough blocks
+        {
+            const int rc2 = pme_tiles_setup(c, std::min(Na, std::min(Nb, Nc)) >= 32 ? 16 : 8);
+            if (rc2) return rc2;
+        }
+        CK(cudaMalloc(&c->d_pme_ovf, (size_t)std::max(1, d.nchrg) * nbeads * sizeof(int)));
+        // per (charge, bead) records: stencil origin and the six weight rows
+        const int nip = n_interp <= 4 ? 4 : (n_interp <= 8 ? 8 : 12);
+        const size_t nrec = (size_t)std::max(1, d.nchrg) * nbeads;
+        CK(cudaMalloc(&c->d_pme_head, nrec * 4 * sizeof(int)));
+        CK(cudaMalloc(&c->d_forceP, nrec * 3 * sizeof(double)));
+        CK(cudaMalloc(&c->d_pme_w, nrec * 6 * nip * rsz));
+        // twiddles exp(2 pi i m / N) per axis, 256 entries each
+        std::vector<double> tw(2 * 256 * 3, 0.0);
+        std::vector<float> tw32(tw.size());
+        const int N3[3] = {Na, Nb, Nc};
+        for (int ax = 0; ax < 3; ax++)
+            for (int m = 0; m < N3[ax]; m++) {
+                tw[2 * (256 * ax + m)] = cos(2.0 * M_PI * m / N3[ax]);
+                tw[2 * (256 * ax + m) + 1] = sin(2.0 * M_PI * m / N3[ax]);
+            }
+        for (size_t i = 0; i < tw.size(); i++) tw32[i] = (float)tw[i];
+        CK(upload(&c->d_twiddle64, tw.data(), tw.size()));
+        CK(upload(&c->d_twiddle32, tw32.data(), tw32.size()));
+    }
+    c->filter_ok = false;
+    return PINYB200_OK;
+}
+
+void pinyb200::pme_swap(pinyb200_ctx *c, PmeSet &p)
+{
+    using std::swap;
+    DeviceSystem &d = c->sys;
+    for (int k = 0; k < 3; k++) {
+        swap(d.ngrid[k], p.ngrid[k]);
+        swap(c->pme_nt[k], p.pme_nt[k]);
+    }
+    swap(d.n_interp, p.n_interp);
+    swap(d.nktot, p.nktot);
+    swap(d.kvec, p.kvec);
+    swap(d.kmask, p.kmask);
+    swap(d.bweight, p.bweight);
+    swap(c->d_grid, p.d_grid);
+    swap(c->d_spec, p.d_spec);
+    swap(c->d_filter, p.d_filter);
+    swap(c->d_forceP, p.d_forceP);
+    swap(c->pme_tile, p.pme_tile);
+    swap(c->pme_ntile, p.pme_ntile);
+    swap(c->pme_cap, p.pme_cap);
+    swap(c->d_pme_cnt, p.d_pme_cnt);
+    swap(c->d_pme_bin, p.d_pme_bin);
+    swap(c->d_pme_ovf, p.d_pme_ovf);
+    swap(c->d_pme_head, p.d_pme_head);
+    swap(c->d_pme_w, p.d_pme_w);
+    swap(c->d_twiddle64, p.d_twiddle64);
+    swap(c->d_twiddle32, p.d_twiddle32);
+    swap(c->filter_ok, p.filter_ok);
+    for (int k = 0; k < 9; k++) swap(c->filter_h[k], p.filter_h[k]);
+}
+
+// PINY's separate RESPA PME mesh into c->pme_res (replacing any earlier one).
+int pinyb200::pme_res_setup(pinyb200_ctx *c, const int *ngrid, int n_interp, int nktot, const int *kastr,
+                            const int *kbstr, const int *kcstr, const double *bweight)
+{
+    pme_res_free(c);
+    PmeSet fresh;
+    pme_swap(c, fresh);  // the context's PME fields are empty now
+    int rc = pme_alloc(c, c->P, ngrid, n_interp, nktot, kastr, kbstr, kcstr, bweight);
+    pme_swap(c, fresh);  // the new mesh into `fresh`, the evaluation's back
+    c->pme_res = fresh;
+    c->pme_res.on = rc == PINYB200_OK;
+    if (rc) pme_res_free(c);
+    return rc;
+}
+
+void pinyb200::pme_res_free(pinyb200_ctx *c)
+{
+    PmeSet &p = c->pme_res;
+    void *ptrs[] = {p.kvec, p.kmask, p.bweight, p.d_grid, p.d_spec, p.d_filter, p.d_forceP, p.d_pme_cnt, p.d_pme_bin,
+                    p.d_pme_ovf, p.d_pme_head, p.d_pme_w, p.d_twiddle64, p.d_twiddle32};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    p = PmeSet();
+}
+
 // Per-site-pair parameters of the MIXED molecule-pair kernel
 // (mol_pair_mixed_kernel): for site pair (si, sj) of the uniform molecule
 // with pair type p and table u = inter_map[p], its row offset u * nsplin + 2,
@@ -285,6 +411,7 @@ int pinyb200_destroy(pinyb200_ctx *c)
 {
     if (!c) return PINYB200_OK;
     cudaSetDevice(c->device);
+    pme_res_free(c);
     free_sys(c->sys);
     void *ptrs[] = {c->d_row, c->d_col, c->d_rowA, c->d_colA, c->d_count, c->d_tot, c->d_posT, c->d_forceT,
                     c->d_xmod, c->d_pos_aos, c->d_force_aos, c->d_acc, c->d_grid, c->d_spec, c->d_filter, c->d_twiddle64,
@@ -392,67 +519,14 @@ int pinyb200_create(const pinyb200_system *s, int nbeads, int precision, pinyb20
     }
     c->alp_ewd = s->alp_ewd;
     c->self_erf = s->self_erf;
-    d.nktot = s->nktot;
-    d.ngrid[0] = s->ngrid_a;
-    d.ngrid[1] = s->ngrid_b;
-    d.ngrid[2] = s->ngrid_c;
-    d.n_interp = s->n_interp;
-    if (s->nktot > 0) {
-        std::vector<int> kv((size_t)3 * s->nktot);
-        for (int i = 0; i < s->nktot; i++) {
-            kv[3 * i] = s->kastr[i];
-            kv[3 * i + 1] = s->kbstr[i];
-            kv[3 * i + 2] = s->kcstr[i];
-        }
-        CK(upload(&d.kvec, kv.data(), kv.size()));
-        CK(upload(&d.bweight, s->bweight, s->nktot));
-        const int Na = s->ngrid_a, Nb = s->ngrid_b, Nc = s->ngrid_c;
-        const size_t G = (size_t)Na * Nb * Nc;
-        std::vector<int> mask(G, -1);
-        for (int i = 0; i < s->nktot; i++) {
-            int a = ((s->kastr[i] % Na) + Na) % Na, b = ((s->kbstr[i] % Nb) + Nb) % Nb,
-                cc = ((s->kcstr[i] % Nc) + Nc) % Nc;
-            mask[((size_t)cc * Nb + b) * Na + a] = i;
-            int am = (Na - a) % Na, bm = (Nb - b) % Nb, cm = (Nc - cc) % Nc;
-            mask[((size_t)cm * Nb + bm) * Na + am] = i;
-        }
-        CK(upload(&d.kmask, mask.data(), G));
-        CK(cudaMalloc(&c->d_filter, G * (sizeof(double) + sizeof(float))));
-        const bool f64 = precision == PINYB200_FP64;
-        if (pme_plane_smem(Na, Nb, f64) > 220 * 1024 || pme_slab_smem(Na, Nc, f64) > 220 * 1024) {
-            int rc2 = fail(nullptr, PINYB200_ERR_UNSUPPORTED, "PME grid plane too large for shared memory");
+    {
+        const int ng[3] = {s->ngrid_a, s->ngrid_b, s->ngrid_c};
+        if (int rc = pme_alloc(c, nbeads, ng, s->n_interp, s->nktot, s->kastr, s->kbstr, s->kcstr, s->bweight)) {
+            if (rc != PINYB200_ERR_UNSUPPORTED) return rc;
+            const std::string msg = c->err;
             pinyb200_destroy(c);
-            return rc2;
+            return fail(nullptr, rc, msg);
         }
-        const size_t rsz = f64 ? sizeof(double) : sizeof(float);
-        const size_t csz = f64 ? sizeof(double2) : sizeof(float2);
-        CK(cudaMalloc(&c->d_grid, rsz * G * nbeads));
-        CK(cudaMalloc(&c->d_spec, csz * (size_t)Nc * Nb * (Na / 2 + 1) * nbeads));
-        // charge bins per grid tile and bead: 16^3 tiles, or 8^3 on small
-        // meshes so that spread and gather still get enough blocks
-        {
-            const int rc2 = pme_tiles_setup(c, std::min(Na, std::min(Nb, Nc)) >= 32 ? 16 : 8);
-            if (rc2) return rc2;
-        }
-        CK(cudaMalloc(&c->d_pme_ovf, (size_t)std::max(1, d.nchrg) * nbeads * sizeof(int)));
-        // per (charge, bead) records: stencil origin and the six weight rows
-        const int nip = s->n_interp <= 4 ? 4 : (s->n_interp <= 8 ? 8 : 12);
-        const size_t nrec = (size_t)std::max(1, d.nchrg) * nbeads;
-        CK(cudaMalloc(&c->d_pme_head, nrec * 4 * sizeof(int)));
-        CK(cudaMalloc(&c->d_forceP, nrec * 3 * sizeof(double)));
-        CK(cudaMalloc(&c->d_pme_w, nrec * 6 * nip * rsz));
-        // twiddles exp(2 pi i m / N) per axis, 256 entries each
-        std::vector<double> tw(2 * 256 * 3, 0.0);
-        std::vector<float> tw32(tw.size());
-        const int N3[3] = {Na, Nb, Nc};
-        for (int ax = 0; ax < 3; ax++)
-            for (int m = 0; m < N3[ax]; m++) {
-                tw[2 * (256 * ax + m)] = cos(2.0 * M_PI * m / N3[ax]);
-                tw[2 * (256 * ax + m) + 1] = sin(2.0 * M_PI * m / N3[ax]);
-            }
-        for (size_t i = 0; i < tw.size(); i++) tw32[i] = (float)tw[i];
-        CK(upload(&c->d_twiddle64, tw.data(), tw.size()));
-        CK(upload(&c->d_twiddle32, tw32.data(), tw32.size()));
     }
     d.necor = s->necor;
     if (s->necor > 0) {
@@ -806,7 +880,21 @@ int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, boo
     CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     CK(launch_pme_force_add(c));
     CK(kt_mark(c, "pme_force_add"));
-    if (respa_w) CK(launch_pme_force_add_scaled(c, c->r_kres ? c->r_wter_res : c->r_wter, respa_w));
+    if (respa_w) {
+        const bool mesh_res = c->r_kres && c->pme_res.on;
+        CK(launch_pme_force_add_scaled(c, c->r_kres && !mesh_res ? c->r_wter_res : c->r_wter, respa_w));
+        if (mesh_res) {
+            // PINY's RESPA mesh at the outer step (energy_control_inter_recip.c:
+            // 233-244): x (wght_ter_res - wght_ter) into the weighted forces and,
+            // unweighted, into the virial forces; its energy is discarded
+            pme_swap(c, c->pme_res);
+            cudaError_t e = launch_pme(c, cell, false);
+            if (e == cudaSuccess) e = launch_pme_force_add_scaled(c, c->r_wter_res - c->r_wter, respa_w);
+            if (e == cudaSuccess) e = launch_pme_force_add(c);
+            pme_swap(c, c->pme_res);
+            CK(e);
+        }
+    }
     if (flags & PINYB200_DISTRIB_GHOSTS) {
         CK(launch_ghost_distrib(c));
         if (respa_w) CK(launch_ghost_distrib(c, respa_w));

@@ -130,6 +130,26 @@ cudaError_t launch_grad_terms(pinyb200_ctx *c, const Cell &cell, const GradArgs 
 
 }  // namespace pinyb200
 
+// State of one PME mesh.  The evaluation's mesh lives in the context's own
+// fields (sys.ngrid..., d_grid...); PINY's separate RESPA mesh (pme_res_on)
+// is held here and swapped into those fields while its kernels are
+// enqueued (pme_swap), so every PME launcher serves both.
+struct PmeSet {
+    bool on = false;
+    int ngrid[3] = {0, 0, 0}, n_interp = 0, nktot = 0;
+    int *kvec = nullptr, *kmask = nullptr;
+    double *bweight = nullptr;
+    void *d_grid = nullptr, *d_spec = nullptr, *d_filter = nullptr;
+    double *d_forceP = nullptr;
+    int pme_tile = 16, pme_nt[3] = {0, 0, 0}, pme_ntile = 0, pme_cap = 0;
+    int *d_pme_cnt = nullptr, *d_pme_bin = nullptr, *d_pme_ovf = nullptr;
+    void *d_pme_head = nullptr, *d_pme_w = nullptr;
+    double *d_twiddle64 = nullptr;
+    float *d_twiddle32 = nullptr;
+    bool filter_ok = false;
+    double filter_h[9] = {0};
+};
+
 struct pinyb200_ctx {
     int device = 0;
     int precision = PINYB200_FP64;
@@ -251,6 +271,7 @@ struct pinyb200_ctx {
     double r_wter = 1, r_wter_res = 1, r_wtra_res = 1, r_rheal = 1;
     int r_int_res_ter = 0, r_int_res_inter = 0, r_ires_bond = 0;
     int r_kres = 0;                   // reciprocal-space RESPA on one grid (nktot_res > 0)
+    PmeSet pme_res;                   // PINY's separate RESPA PME mesh (pme_res_on), when on
     double *d_ecor_res_tab = nullptr; // [ecor_nsplin][4] cubic coefficients of ecor.cdv0_res
     double *d_cut_res = nullptr;      // [npair_typ] inner cutoffs (Bohr)
     double *d_bond_eq_res = nullptr;  // [nbond_typ] RESPA bond equilibria
@@ -318,6 +339,10 @@ int enqueue_device(pinyb200_ctx *c, const double *d_pos, const double *d_xmod, c
                    double *d_force, bool timing, double *h_acc);
 Cell cell_from_hmat(const double *hmat);
 int pme_tiles_resize(pinyb200_ctx *c, int T);
+void pme_swap(pinyb200_ctx *c, PmeSet &p);
+int pme_res_setup(pinyb200_ctx *c, const int *ngrid, int n_interp, int nktot, const int *kastr, const int *kbstr,
+                  const int *kcstr, const double *bweight);
+void pme_res_free(pinyb200_ctx *c);
 void table_coefs(const double *t, int nsplin, std::vector<double> &out);
 
 // cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per kernel, device

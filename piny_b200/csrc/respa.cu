@@ -207,10 +207,15 @@ int pinyb200::respa_level_enqueue(pinyb200_ctx *c, const Cell &cell, int level, 
     RK(cudaMemsetAsync(c->d_forceW, 0, nb * sizeof(double), c->stream));
     if (inter) RK(launch_pair_respa(c, cell, 1, c->d_forceW));
     if (inter && c->r_kres) {
-        // reciprocal-space RESPA with one grid: the reciprocal sum and the
-        // exclusion correction (RESPA table) belong to this level
-        RK(launch_pme(c, cell, false));
-        RK(launch_pme_force_add_scaled(c, c->r_wter_res, c->d_forceW));
+        // reciprocal-space RESPA: the reciprocal sum (on the one mesh, or
+        // on PINY's separate RESPA mesh) and the exclusion correction
+        // (RESPA table) belong to this level
+        const bool mesh_res = c->pme_res.on;
+        if (mesh_res) pme_swap(c, c->pme_res);
+        cudaError_t e = launch_pme(c, cell, false);
+        if (e == cudaSuccess) e = launch_pme_force_add_scaled(c, c->r_wter_res, c->d_forceW);
+        if (mesh_res) pme_swap(c, c->pme_res);
+        RK(e);
         RK(launch_ecor_weighted(c, c->r_wter_res, c->d_forceW, 1));
     }
     RK(launch_intra_respa(c, inter, c->d_forceW));
@@ -244,9 +249,22 @@ int pinyb200_set_respa(pinyb200_ctx *c, const pinyb200_respa *r)
         c->respa_on = false;
         return PINYB200_OK;
     }
-    if (r->nktot_res > 0 && r->pme_res_on)
-        return record_error(c, PINYB200_ERR_UNSUPPORTED,
-                            "set_respa: a separate RESPA PME grid (ewald_respa_pme_opt on) is not supported");
+    const bool mesh_res = r->nktot_res > 0 && r->pme_res_on;
+    if (mesh_res) {
+        if (!r->kastr_res || !r->kbstr_res || !r->kcstr_res || !r->bweight_res)
+            return record_error(c, PINYB200_ERR_ARG, "set_respa: RESPA PME mesh k vectors / weights missing");
+        for (int d = 0; d < 3; d++)
+            if (r->ngrid_res[d] < r->n_interp_res || r->ngrid_res[d] > 256)
+                return record_error(c, PINYB200_ERR_ARG, "set_respa: RESPA PME mesh size out of range");
+        if (r->n_interp_res < 4 || r->n_interp_res > 10)
+            return record_error(c, PINYB200_ERR_UNSUPPORTED, "set_respa: RESPA PME order outside 4..10");
+        for (int i = 0; i < r->nktot_res; i++) {
+            const int k[3] = {r->kastr_res[i], r->kbstr_res[i], r->kcstr_res[i]};
+            for (int d = 0; d < 3; d++)
+                if (2 * abs(k[d]) >= r->ngrid_res[d])
+                    return record_error(c, PINYB200_ERR_ARG, "set_respa: RESPA k vector beyond its PME mesh");
+        }
+    }
     if (r->nktot_res > 0 && c->sys.necor > 0 && !r->ecor_cdv0_res)
         return record_error(c, PINYB200_ERR_ARG, "set_respa: ecor_cdv0_res missing (nktot_res > 0)");
     if (!r->cutoff_res || (c->sys.nbond && !r->bond_eq_res))
@@ -267,6 +285,13 @@ int pinyb200_set_respa(pinyb200_ctx *c, const pinyb200_respa *r)
     }
     if (!c->d_forceW) RK(cudaMalloc(&c->d_forceW, (size_t)c->sys.natm * 3 * c->P * sizeof(double)));
     c->r_kres = r->nktot_res > 0 ? 1 : 0;
+    if (mesh_res && c->sys.nchrg > 0) {
+        if (int rc = pme_res_setup(c, r->ngrid_res, r->n_interp_res, r->nktot_res, r->kastr_res, r->kbstr_res,
+                                   r->kcstr_res, r->bweight_res))
+            return rc;
+    } else {
+        pme_res_free(c);
+    }
     if (c->r_kres && c->sys.necor > 0) {
         std::vector<double> coef;
         table_coefs(r->ecor_cdv0_res, c->sys.ecor_nsplin, coef);

@@ -91,7 +91,8 @@ class PinyRespa(C.Structure):
     _fields_ = [("wght_ter", _d), ("wght_ter_res", _d), ("wght_tra_res", _d),
                 ("int_res_ter", _i), ("int_res_inter", _i), ("ires_bond", _i),
                 ("cutoff_res", _pd), ("rheal_res", _d), ("bond_eq_res", _pd), ("nktot_res", _i),
-                ("pme_res_on", _i), ("ecor_cdv0_res", _pd)]
+                ("pme_res_on", _i), ("ecor_cdv0_res", _pd), ("ngrid_res", _i * 3), ("n_interp_res", _i),
+                ("kastr_res", _pi), ("kbstr_res", _pi), ("kcstr_res", _pi), ("bweight_res", _pd)]
 
 
 class PinyTangent(C.Structure):
@@ -403,6 +404,18 @@ class DeviceBox:
                       int(respa["int_res_ter"]), int(respa["int_res_inter"]), int(respa["ires_bond"]), _dp(cut),
                       float(respa["rheal_res"]), _dp(eqr), int(respa.get("nktot_res", 0)),
                       int(respa.get("pme_res_on", 0)), None if ecr is None else _dp(ecr))
+        keep = []
+        if int(respa.get("pme_res_on", 0)) and "ngrid_res" in respa:
+            # PINY's separate RESPA PME mesh: its size, order, k sphere and weights
+            r.ngrid_res[:] = [int(v) for v in respa["ngrid_res"]]
+            r.n_interp_res = int(respa["n_interp_res"])
+            for name in ("kastr_res", "kbstr_res", "kcstr_res"):
+                a = np.ascontiguousarray(respa[name], np.int32)
+                keep.append(a)
+                setattr(r, name, a.ctypes.data_as(_pi))
+            bw = np.ascontiguousarray(respa["bweight_res"], np.float64)
+            keep.append(bw)
+            r.bweight_res = _dp(bw)
         self._check(self.L.pinyb200_set_respa(self.h, C.byref(r)), "set_respa")
 
     def respa_force_device(self, d_pos: int, d_xmod, hmat, level: int, d_force: int, d_forcet=None, stream=None,

@@ -30,7 +30,7 @@ def respa_weights(nres_ter: int, nres_tor: int, nres_tra: int, nres_pimd: int, p
 
 
 def respa_setup(nres_ter: int, nres_tor: int, nres_tra: int, nres_pimd: int, pimd_on: bool, int_res_ter: bool,
-                cutoff_res, rheal_res: float, bond_eq_res, nktot_res: int = 0, ecor_cdv0_res=None):
+                cutoff_res, rheal_res: float, bond_eq_res, nktot_res: int = 0, ecor_cdv0_res=None, mesh_res=None):
     """Everything pinyb200_set_respa takes: the weights, PINY's switches
     int_res_ter (``respa_steps_lrf`` given), int_res_inter (nres_ter > 1,
     energy_control_initial.c:223-229) and the bond RESPA flag of
@@ -39,7 +39,9 @@ def respa_setup(nres_ter: int, nres_tor: int, nres_tra: int, nres_pimd: int, pim
     equilibrium lengths per bond type (Bohr) and, for the reciprocal-space
     RESPA set on the one PME grid (``ewald_respa_kmax`` = ``ewald_kmax``),
     its k-vector count and the exclusion correction's RESPA force table
-    (``system.ecor_res_table``)."""
+    (``system.ecor_res_table``).  ``mesh_res`` -- PINY's separate RESPA PME
+    mesh (``ewald_respa_pme_opt on``) as ``system.pme_res_mesh`` returns it:
+    ngrid_res, n_interp_res, kastr_res/kbstr_res/kcstr_res, bweight_res."""
     w_ter, w_ter_res, w_tra_res = respa_weights(nres_ter, nres_tor, nres_tra, nres_pimd, pimd_on)
     out = {"wght_ter": w_ter, "wght_ter_res": w_ter_res, "wght_tra_res": w_tra_res,
            "int_res_ter": int(bool(int_res_ter)), "int_res_inter": int(nres_ter > 1),
@@ -49,6 +51,9 @@ def respa_setup(nres_ter: int, nres_tor: int, nres_tra: int, nres_pimd: int, pim
            "pme_res_on": 0}
     if ecor_cdv0_res is not None:
         out["ecor_cdv0_res"] = np.ascontiguousarray(ecor_cdv0_res, np.float64)
+    if mesh_res is not None:
+        out["pme_res_on"] = 1
+        out.update(mesh_res)
     return out
 
 

@@ -304,6 +304,27 @@ def ecor_res_table(nsplin, rmax, alp, ecut, ecut_res):
     return cdv0 - dchi(math.sqrt(2.0 * ecut)) + dchi(math.sqrt(2.0 * ecut_res))
 
 
+def pme_res_mesh(hmat, kmax_res, kmax_pme_res, n_interp_res):
+    """PINY's separate RESPA PME mesh (ewald_respa_pme_opt on,
+    control_set_cp_ewald.c:451-504): the RESPA k sphere of ewald_respa_kmax
+    (calc_cutoff, countkvec3d / setkvec3d), the mesh of set_pme_grid for
+    ewald_respa_kmax_pme, and set_pme_wght's B-spline weights of order
+    ewald_respa_interp_pme on that mesh.  ``hmat`` 9 column-major (Bohr).
+    Returns the fields of pinyb200_respa's RESPA mesh."""
+    hm = np.asarray(hmat, np.float64)
+    hi, vol = gethinv(hm)
+    ecut = ewald_ecut(int(kmax_res), vol)
+    kmaxv = kmaxv_of(ecut, hi)
+    ka, kb, kc = kvectors(ecut, kmaxv, hi)
+    ng = pme_grid(ecut, vol, hi, kmaxv, int(kmax_pme_res))
+    n = int(n_interp_res)
+    wa, wb, wc = (bspline_weight_1d(n, g) for g in ng)
+    bw = wa[np.where(ka < 0, ka + ng[0], ka)] * wb[np.where(kb < 0, kb + ng[1], kb)] \
+        * wc[np.where(kc < 0, kc + ng[2], kc)]
+    return {"ngrid_res": np.array(ng, np.int32), "n_interp_res": n, "kastr_res": ka, "kbstr_res": kb,
+            "kcstr_res": kc, "bweight_res": bw}
+
+
 def bend_harm_coefs(fk, theta0):
     """bend_coef "harm" (intra_coefs.c:240-276) and derivatives (:355-371)."""
     cn1, cn2, cn3, cn4 = 49.0 / 72.0, 3.0 / 4.0, 3.0 / 40.0, 1.0 / 180.0

@@ -25,7 +25,9 @@ switch the split on.
 Run in a container that has the PINY tree:  python tests/golden/make_golden.py
 (``--pimd-only`` regenerates just the transform, MD-bookkeeping, I/O and
 RESPA fixtures; ``--headline-only`` just the benchmark configurations
-evaluated in full: spcfw_256_p32, tip4pf_4096_p32, tip4pf_1024_p16)
+evaluated in full: spcfw_256_p32, tip4pf_4096_p32, tip4pf_1024_p16;
+``--respa-grid-only`` just the RESPA fixture with PINY's separate RESPA PME
+grid)
 The GPU tests only read the .npz files.
 """
 from __future__ import annotations
@@ -361,18 +363,19 @@ RESPA_CASES = [
      {"lrf": 2, "intra": 2, "pimd": 1, "rheal": 0.8, "eq_res": 0.02, "kmax_res": 6}),
 ]
 
-# PINY's separate RESPA PME grid (ewald_respa_pme_opt on, kmax_res < kmax):
-# only its set-up products are kept (the exclusion correction's RESPA table)
+# PINY's separate RESPA PME grid (ewald_respa_pme_opt on, kmax_res < kmax,
+# kmax_pme_res 4, order 4): the forces of every level and the grid's set-up
+# products (mesh, k sphere, B-spline weights, exclusion-correction table)
 RESPA_GRID_CASE = ("respa_pmegrid_tip4pf_64_p4",
                    water.BoxSpec(water.TIP4P_F, 64, 12.416, 4, 298.0, 108, cutoff=6.0, grid=16, order=8, kmax=6),
                    {"lrf": 2, "intra": 1, "pimd": 1, "rheal": 0.8, "eq_res": 0.0, "kmax_res": 3, "pme_res": (4, 4)})
 
 
-def respa_fixture(tmp):
+def respa_fixture(tmp, cases=None):
     """PINY's forces at each RESPA level (``piny_ref respa``): the flags
     int_NVT_pimd sets at the outer step, an inner inter step, an intra step
     and the innermost step, on seeded boxes with RESPA inputs."""
-    for name, spec, rk in RESPA_CASES + [RESPA_GRID_CASE]:
+    for name, spec, rk in (cases if cases is not None else RESPA_CASES + [RESPA_GRID_CASE]):
         pos = water.build_positions(spec)
         d = os.path.join(tmp, "respa_inp")
         shutil.rmtree(d, ignore_errors=True)
@@ -394,6 +397,13 @@ def respa_fixture(tmp):
         if "ecor_cdv0_res" in D:
             fx["ecor_cdv0_res"] = D["ecor_cdv0_res"]
             fx["ecor_ecut_res"] = float(D["ecor_ecut_res"][0])
+        if "ngrid_res" in D:
+            fx["kmax_res"] = int(rk["kmax_res"])
+            fx["ngrid_res"] = D["ngrid_res"]
+            fx["n_interp_res"] = int(D["n_interp_res"][0])
+            fx["kmax_pme_res"] = int(D["kmax_pme_res"][0])
+            for k in ("kastr_res", "kbstr_res", "kcstr_res", "bweight_tot_res"):
+                fx[k] = D[k]
         for lv in range(4):
             fx["L%d_flags" % lv] = D["L%d_flags" % lv]
             fx["ref_L%d_force_raw" % lv] = D["L%d_force_raw" % lv].reshape(P, n, 3)
@@ -408,10 +418,6 @@ def respa_fixture(tmp):
         fx["spec_order"] = spec.order
         fx["spec_nsplin"] = spec.nsplin
         fx["spec_temperature"] = spec.temperature
-        if name == RESPA_GRID_CASE[0]:
-            keep = ("ecor_nsplin", "ecor_rmax", "alp_ewd", "ecor_ecut", "ecor_ecut_res", "ecor_cdv0",
-                    "ecor_cdv0_res", "nktot", "nktot_res", "pme_res_on", "natm", "nbeads")
-            fx = {k: fx[k] for k in keep}
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **{k: np.asarray(v) for k, v in fx.items()})
         print(name, os.path.getsize(path), "bytes")
@@ -480,6 +486,11 @@ def headline_fixture(name, tmp):
 
 
 def main():
+    if "--respa-grid-only" in sys.argv[1:]:
+        tmp = tempfile.mkdtemp(prefix="piny_golden_")
+        respa_fixture(tmp, [RESPA_GRID_CASE])
+        shutil.rmtree(tmp, ignore_errors=True)
+        return
     if "--headline-only" in sys.argv[1:]:
         tmp = tempfile.mkdtemp(prefix="piny_golden_")
         for name in HEADLINE_NAMES:

@@ -32,16 +32,22 @@ def rel_rms(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
 
 
-RESPA_NAMES = ["respa_tip4pf_64_p4", "respa_spcfw_64_p1", "respa_kspace_tip4pf_64_p4"]
+RESPA_NAMES = ["respa_tip4pf_64_p4", "respa_spcfw_64_p1", "respa_kspace_tip4pf_64_p4", "respa_pmegrid_tip4pf_64_p4"]
 
 
 def respa_from_fixture(F):
     """pinyb200_set_respa's inputs for a RESPA fixture, formed from its step
     counts the way PINY forms them."""
+    from piny_b200 import system
     from piny_b200.respa import respa_setup
+    mesh = None
+    if int(F.get("pme_res_on", 0)):
+        # PINY's separate RESPA PME mesh, set up here as PINY does
+        mesh = system.pme_res_mesh(F["hmat"], int(F["kmax_res"]), int(F["kmax_pme_res"]), int(F["n_interp_res"]))
     return respa_setup(int(F["nres_ter"]), int(F["nres_tor"]), int(F["nres_tra"]), int(F["nres_pimd"]),
                        int(F["nbeads"]) > 1, bool(F["int_res_ter"]), F["cutoff_res"], float(F["rheal_res"]),
-                       F["bond_eq_res"], nktot_res=int(F["nktot_res"]), ecor_cdv0_res=F.get("ecor_cdv0_res"))
+                       F["bond_eq_res"], nktot_res=int(F["nktot_res"]), ecor_cdv0_res=F.get("ecor_cdv0_res"),
+                       mesh_res=mesh)
 
 
 def fixture_level(F, lv):

@@ -114,8 +114,15 @@ def test_respa_arguments():
     bad = dict(rs, cutoff_res=np.asarray(F["cutoff"]) + 1.0)
     with pytest.raises(PinyError, match="ERR_ARG"):
         box.set_respa(bad)
+    with pytest.raises(PinyError, match="ERR_ARG"):
+        box.set_respa(dict(rs, nktot_res=12, pme_res_on=1))  # the RESPA mesh's k sphere is needed
+    G = load_fixture("respa_pmegrid_tip4pf_64_p4")
+    mesh = respa_from_fixture(G)
     with pytest.raises(PinyError, match="ERR_UNSUPPORTED"):
-        box.set_respa(dict(rs, nktot_res=12, pme_res_on=1))
+        box.set_respa(dict(rs, nktot_res=mesh["nktot_res"], pme_res_on=1, ngrid_res=mesh["ngrid_res"],
+                           n_interp_res=12, kastr_res=mesh["kastr_res"], kbstr_res=mesh["kbstr_res"],
+                           kcstr_res=mesh["kcstr_res"], bweight_res=mesh["bweight_res"],
+                           ecor_cdv0_res=G["ecor_cdv0_res"]))
     with pytest.raises(PinyError, match="ERR_ARG"):
         box.set_respa(dict(rs, nktot_res=12))  # the RESPA exclusion table is needed
     box.set_respa(rs)

@@ -29,13 +29,15 @@ def test_respa_oracle_matches_piny(name, oracle):
         if lv == 0 and "ref_L0_forcet_raw" in F:
             assert rel_rms(ft, F["ref_L0_forcet_raw"]) < 1e-13
     # the full level with every weight 1 is the plain evaluation, and so are
-    # PINY's virial forces of the full level
+    # PINY's virial forces of the full level -- except with the separate
+    # RESPA PME mesh, whose forces PINY adds to the virial forces too at the
+    # full step (ewald3d_pme.c:563-585 runs for both meshes)
     plain, _ = oracle.energy_force(F, F["pos"], xmod, F["hmat"], pi, pj)
     one = dict(r, wght_ter=1.0, wght_ter_res=1.0, wght_tra_res=1.0)
     f, ft = oracle.respa_force(F, one, R.FULL_INTER | R.FULL_INTRA | R.RES_INTRA, F["pos"], xmod, F["hmat"], pi, pj)
     assert rel_rms(f, plain) < 1e-13
     assert rel_rms(ft, plain) < 1e-13
-    if "ref_L0_forcet_raw" in F:
+    if "ref_L0_forcet_raw" in F and not int(F.get("pme_res_on", 0)):
         assert rel_rms(plain, F["ref_L0_forcet_raw"]) < 1e-13
 
 
@@ -54,6 +56,18 @@ def test_ecor_res_table_matches_piny(name):
     assert np.abs(t - ref).max() <= 1e-10 * np.abs(ref).max()
     if name == "respa_pmegrid_tip4pf_64_p4":
         assert np.abs(ref - F["ecor_cdv0"]).max() > 1e-6 * np.abs(ref).max()
+
+
+def test_respa_pme_mesh_matches_piny():
+    """PINY's separate RESPA PME mesh (ewald_respa_pme_opt on): the host
+    set-up's mesh, RESPA k sphere and B-spline weights against PINY's."""
+    from piny_b200 import system
+    F = load_fixture("respa_pmegrid_tip4pf_64_p4")
+    m = system.pme_res_mesh(F["hmat"], int(F["kmax_res"]), int(F["kmax_pme_res"]), int(F["n_interp_res"]))
+    assert list(m["ngrid_res"]) == list(F["ngrid_res"])
+    for k in ("kastr_res", "kbstr_res", "kcstr_res"):
+        assert np.array_equal(m[k], F[k]), k
+    assert np.abs(m["bweight_res"] - F["bweight_tot_res"]).max() <= 1e-14 * np.abs(F["bweight_tot_res"]).max()
 
 
 def test_respa_loop_levels():
