@@ -111,8 +111,31 @@ __device__ __forceinline__ void stencil_origin(const PmeArgs &a, const Cell &cel
 }
 
 // Charges binned by the grid tile that holds their stencil origin, per bead.
+// Largest value of the order-n cardinal B-spline (PINY's m[] over the
+// fractional offset, ewald3d_pme.c:301-338), sampled finely: a bound for the
+// fixed-point spread.
+static double bspline_peak(int n)
+{
+    double best = 0.0;
+    for (int k = 0; k <= 1024; k++) {
+        const double f = k / 1024.0;
+        double m[16] = {0}, u[16];
+        for (int j = 1; j <= n; j++) u[j] = f + (double)(j - 1);
+        m[1] = 1.0 - std::fabs(u[1] - 1.0);
+        m[2] = 1.0 - std::fabs(u[2] - 1.0);
+        for (int nn = 3; nn <= n; nn++) {
+            const double rn1 = 1.0 / (double)(nn - 1);
+            for (int j = nn; j >= 2; j--) m[j] = (u[j] * m[j] + ((double)nn - u[j]) * m[j - 1]) * rn1;
+            m[1] = u[1] * m[1] * rn1;
+        }
+        for (int j = 1; j <= n; j++) best = std::max(best, m[j]);
+    }
+    return best * (1.0 + 1e-6);
+}
+
 struct TileArgs {
     int T;  // tile edge (grid points)
+    float qfix, qfix_inv;  // FP32 spread: fixed-point scale 2^S of the shared tile, and 2^-S
     int nta, ntb, ntc, ntile, cap;
     int *cnt;  // [P][ntile], then the overflow count
     int *bin;  // [P][ntile][cap] record numbers k*P + b
@@ -775,7 +798,7 @@ __global__ void __launch_bounds__(256) spread_tile_c_kernel(PmeArgs a, TileArgs 
         const R q = fr.w;
         const int oa = h.y - ta0, ob = h.z - tb0, oc = h.w - tc0;
         if (oa >= 0 && oa < TG::T && ob >= 0 && ob < TG::T && oc >= 0 && oc < TG::T) {
-            R *base = tl + (oc * TG::E + ob + lb4) * TG::PA + oa + la8;
+            const int off0 = (oc * TG::E + ob + lb4) * TG::PA + oa + la8;
 #pragma unroll
             for (int s = 0; s < SpreadW<R, NI>::NSA; s++) {
                 if (la8 + 8 * s >= NI) break;
@@ -784,8 +807,20 @@ __global__ void __launch_bounds__(256) spread_tile_c_kernel(PmeArgs a, TileArgs 
                 for (int tc = 0; tc < NI; tc++) {
                     const R cq = qa * w.mc[tc];
 #pragma unroll
-                    for (int i = 0; i < NTB; i++)
-                        if (lb4 + 4 * i < NI) atomicAdd(base + (tc * TG::E + 4 * i) * TG::PA + 8 * s, cq * w.mb[i]);
+                    for (int i = 0; i < NTB; i++) {
+                        if (lb4 + 4 * i >= NI) continue;
+                        const int o = off0 + (tc * TG::E + 4 * i) * TG::PA + 8 * s;
+                        if constexpr (sizeof(R) == 4) {
+                            // fixed point: v 2^S + 1.5 2^23 is exact to the nearest
+                            // integer for |v 2^S| < 2^22, whose bits less those of
+                            // 1.5 2^23 are that integer; integer shared atomics run
+                            // at twice the rate of FP32 ones
+                            const float y = fmaf(cq * w.mb[i], t.qfix, 12582912.0f);
+                            atomicAdd((int *)tl + o, __float_as_int(y) - 0x4B400000);
+                        } else {
+                            atomicAdd(tl + o, cq * w.mb[i]);
+                        }
+                    }
                 }
             }
         } else {
@@ -812,8 +847,10 @@ __global__ void __launch_bounds__(256) spread_tile_c_kernel(PmeArgs a, TileArgs 
         for (int r0 = warp * RPI; r0 < NROW; r0 += nwarp * RPI) {
             const int row = r0 + lane / NQ, q4 = lane % NQ;
             if (lane >= RPI * NQ || row >= NROW) continue;
-            const float4 v = ((const float4 *)tl)[row * NQ + q4];
-            if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
+            const int4 iv = ((const int4 *)tl)[row * NQ + q4];
+            if ((iv.x | iv.y | iv.z | iv.w) == 0) continue;
+            const float4 v = make_float4((float)iv.x * t.qfix_inv, (float)iv.y * t.qfix_inv,
+                                         (float)iv.z * t.qfix_inv, (float)iv.w * t.qfix_inv);
             const int cz = row / TG::E, by = row - cz * TG::E;
             const int gc = wrapi(tc0 + cz, a.Nc), gb = wrapi(tb0 + by, a.Nb), ga = wrapi(ta0 + 4 * q4, a.Na);
             atomicAdd((float4 *)((float *)g + ((size_t)gc * a.Nb + gb) * a.Na + ga), v);
@@ -823,7 +860,9 @@ __global__ void __launch_bounds__(256) spread_tile_c_kernel(PmeArgs a, TileArgs 
             const int cz = row / TG::E, by = row - cz * TG::E;
             R *dst = g + ((size_t)wrapi(tc0 + cz, a.Nc) * a.Nb + wrapi(tb0 + by, a.Nb)) * a.Na;
             for (int ax = lane; ax < TG::E; ax += 32) {
-                const R v = tl[row * TG::PA + ax];
+                R v;
+                if constexpr (sizeof(R) == 4) v = (R)((float)((const int *)tl)[row * TG::PA + ax] * t.qfix_inv);
+                else v = tl[row * TG::PA + ax];
                 if (v != (R)0) atomicAdd(dst + wrapi(ta0 + ax, a.Na), v);
             }
         }
@@ -1424,6 +1463,19 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     if ((err = kt_mark(c, "pme_grid_clear (memset)")) != cudaSuccess) return err;
     TileArgs t;
     t.T = TT;
+    // fixed-point scale of the FP32 spread tile: every contribution q M_a M_b
+    // M_c (bounded by max |q| times the B-spline's peak cubed) below 2^22
+    // after scaling, the range the rounding trick is exact in; at most 2^24
+    // (a resolution of 6e-8 against contributions of up to ~0.15)
+    {
+        double qmax = 0.0;
+        for (double q : c->h_charge) qmax = std::max(qmax, std::fabs(q));
+        const double bmax = bspline_peak(NI);
+        int S = 24;
+        while (S > 8 && std::ldexp(qmax * bmax * bmax * bmax, S) >= 0.99 * std::ldexp(1.0, 22)) S--;
+        t.qfix = (float)std::ldexp(1.0, S);
+        t.qfix_inv = (float)std::ldexp(1.0, -S);
+    }
     t.nta = c->pme_nt[0];
     t.ntb = c->pme_nt[1];
     t.ntc = c->pme_nt[2];
