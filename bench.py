@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-energy", action="store_true", help="forces only (PINYB200_NO_ENERGY), for profiling")
     ap.add_argument("--fd", action="store_true", help="c5_grad: also check against central differences")
+    ap.add_argument("--batch-branches", action="store_true",
+                    help="c4_batch: one graph branch per box instead of the multi-box kernels")
     ap.add_argument("--tuning", default="", help="pin a launch shape: tile,pair_kernel,blocks_per_sm,overlap")
     return ap.parse_args()
 
@@ -961,7 +963,9 @@ def respa_cpu_baseline(spec, pos_A, rk, levels):
 
 
 def run_batch(args, ws, rank, local):
-    """64 uneven TIP4P/F boxes, all beads, one CUDA graph launch per step."""
+    """64 uneven TIP4P/F boxes, all beads, one CUDA graph launch per step:
+    the multi-box kernels (one persistent launch per phase and shape group)
+    unless --batch-branches asks for one graph branch per box."""
     import torch
 
     from piny_b200 import system, water
@@ -973,7 +977,6 @@ def run_batch(args, ws, rank, local):
     specs = water.c4_specs(nbox=nbox, seed=2024 + 1000 * rank)
     boxes, keep, d_pos, d_xm, d_f, hm, pins = [], [], [], [], [], [], []
     alg = 0.0
-    nkern = 0
     t0 = time.perf_counter()
     for sp in specs:
         pos = water.build_positions(sp) / water.BOHR
@@ -992,7 +995,6 @@ def run_batch(args, ws, rank, local):
         d_f.append(f.data_ptr())
         hm.append(S["hmat"])
         alg += sp.nbeads * alg_bytes_per_bead_eval(S, sp.nbeads, npairs, args.precision)
-        nkern += box_launches(S, sp.nbeads)
     setup_s = time.perf_counter() - t0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -1003,9 +1005,11 @@ def run_batch(args, ws, rank, local):
     batch = DeviceBatch(boxes)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    br = args.batch_branches
     for _ in range(max(3, args.warmup)):
-        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream)
+        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream, branches=br)
     torch.cuda.synchronize()
+    fused, graph_launches = batch.last_mode()
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
@@ -1018,7 +1022,7 @@ def run_batch(args, ws, rank, local):
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream)
+        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream, branches=br)
         ev1.record(stream)
         ev1.synchronize()
         step_ms.append(ev0.elapsed_time(ev1))
@@ -1041,7 +1045,7 @@ def run_batch(args, ws, rank, local):
         ev0.record(stream)
         for i in range(nbox):
             keep[3 * i].copy_(pins[i][0], non_blocking=True)
-        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream)
+        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream, branches=br)
         for i in range(nbox):
             pins[i][1].copy_(keep[3 * i + 2], non_blocking=True)
         ev1.record(stream)
@@ -1074,8 +1078,10 @@ def run_batch(args, ws, rank, local):
                        "pme_grid": [sp.grid for sp in specs], "precision": args.precision,
                        "tuning": choices, "setup_s": setup_s, "autotune_s": tune_s,
                        "l2": "256 MiB buffer written between timed steps; CUDA events on the launch stream",
-                       "launch": "one CUDA graph launch per step (boxes as parallel branches, "
-                                 "%d kernel nodes)" % nkern},
+                       "launch": ("one CUDA graph launch per step: multi-box kernels, one persistent launch "
+                                  "per phase and shape group (%d kernel nodes for %d boxes)" % (graph_launches, nbox))
+                       if fused else ("one CUDA graph launch per step (boxes as parallel branches, "
+                                      "%d kernel nodes)" % graph_launches)},
             "roofline": {"bound": "hbm", "kernel": "whole batch step", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg,
@@ -1083,7 +1089,7 @@ def run_batch(args, ws, rank, local):
             "cpu_baseline": c4_cpu,
             "e2e": {"value": ws * nbead / (e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "ms_per_step": e2e},
-            "gpu_launches": nkern * args.steps,
+            "gpu_launches": graph_launches * args.steps,
             "clocks": clocks,
         }
         print(json.dumps(line))

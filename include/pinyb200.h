@@ -45,7 +45,9 @@ enum {
     PINYB200_NO_ENERGY = 2,      /* skip energy/virial reductions                   */
     PINYB200_SITE_PAIRS = 4,     /* walk the site list instead of molecule pairs    */
     PINYB200_TUNE_AGAIN = 8,     /* pinyb200_autotune: ignore remembered results    */
-    PINYB200_UPDATE_LIST = 16    /* device list test and rebuild before the forces  */
+    PINYB200_UPDATE_LIST = 16,   /* device list test and rebuild before the forces  */
+    PINYB200_BATCH_BRANCHES = 32 /* batch call: one graph branch per box instead of */
+                                 /* the multi-box kernels                           */
 };
 
 /*
@@ -427,13 +429,21 @@ int pinyb200_set_tuning(pinyb200_ctx *ctx, const int *choice);
  * pinyb200_batch_energy_force_device evaluates every box, as
  * pinyb200_energy_force_device would one by one, from per-box device arrays
  * (d_xmod may be NULL, or hold NULL entries) and host cells, and writes
- * e[i] for box i (e may be NULL).  All boxes run as parallel branches of one
- * CUDA graph launched once per call; the graph is captured on the first call
- * and again whenever a device pointer, a cell or the flags change, after one
- * plain run of every box.  The call returns when the work is done.  PINY's
- * Python driver reaches several replicas through one energy_control call
- * per CLASS (python/piny/piny.pyx:426-436); this entry point has no
- * counterpart there.
+ * e[i] for box i (e may be NULL).  The work of one call is one CUDA graph
+ * launch, captured on the first call and again whenever a device pointer, a
+ * cell or the flags change, after one plain run of every box.  When every
+ * box is MIXED with the molecule-pair kernel (q-TIP4P/F or q-SPC/Fw site
+ * pattern), an orthorhombic cell and the compact PME path, and flags hold
+ * neither PINYB200_UPDATE_LIST, PINYB200_SITE_PAIRS nor
+ * PINYB200_BATCH_BRANCHES, the graph holds multi-box kernels: each phase
+ * (staging, PME bin / spread / three FFT passes / gather, pair forces,
+ * intramolecular terms, finishing) is one persistent launch per group of
+ * boxes sharing its compile-time shape, walking every (box, bead, tile or
+ * chunk) block of the group, with PME on a second branch beside the pair
+ * and intramolecular launches.  Otherwise every box is a parallel branch of
+ * its own kernels.  The call returns when the work is done.  PINY's Python
+ * driver reaches several replicas through one energy_control call per CLASS
+ * (python/piny/piny.pyx:426-436); this entry point has no counterpart there.
  */
 typedef struct pinyb200_batch pinyb200_batch;
 int pinyb200_batch_create(pinyb200_ctx *const *ctx, int nbox,
@@ -447,6 +457,9 @@ int pinyb200_batch_energy_force_device(pinyb200_batch *batch,
                                        pinyb200_energies *e, void *stream);
 /* Device time of the last batch call (CUDA events around the graph launch). */
 int pinyb200_batch_last_ms(pinyb200_batch *batch, float *ms);
+/* How the last captured batch graph runs: *fused 1 for the multi-box
+ * kernels, 0 for one branch per box; *launches its kernel launches. */
+int pinyb200_batch_last_mode(pinyb200_batch *batch, int *fused, int *launches);
 const char *pinyb200_batch_last_error(pinyb200_batch *batch);
 
 /*

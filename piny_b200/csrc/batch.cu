@@ -2,12 +2,17 @@
 //
 // A batch holds the contexts of independent boxes (different sizes, bead
 // counts and meshes).  One call enqueues every box's whole evaluation --
-// positions in, list-based pair forces, PME on its own stream, intramolecular
-// terms, forces out, energy sums to pinned host memory -- with the boxes as
-// parallel branches forked from and joined to one stream.  The first call
-// (and any call whose device pointers, cells or flags differ from the
-// previous one) captures that work into a CUDA graph; every call launches
-// the graph once and then does the host bookkeeping of each box.
+// positions in, list-based pair forces, PME, intramolecular terms, forces
+// out, energy sums to pinned host memory -- in one of two forms:
+//   multi-box kernels: each phase is one persistent launch per group of
+//     boxes that share its compile-time shape (boxtab.cuh), PME on a second
+//     branch beside the pair and intramolecular launches -- a few dozen
+//     launches for any number of boxes;
+//   branches: every box's own kernels as a parallel branch forked from and
+//     joined to one stream (for boxes the multi-box kernels do not cover).
+// The first call (and any call whose device pointers, cells or flags differ
+// from the previous one) captures that work into a CUDA graph; every call
+// launches the graph once and then does the host bookkeeping of each box.
 //
 // The autotuner times, on the caller's own inputs, the launch shapes a
 // context can run with -- PME tile edge (8 or 16 grid points), pair kernel
@@ -80,6 +85,11 @@ struct pinyb200_batch {
     int key_flags = -1;
     float last_ms = 0;
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    // the multi-box form: PME branch and its fork/join events
+    cudaStream_t pme_stream = nullptr;
+    cudaEvent_t pfork = nullptr, pjoin = nullptr;
+    int fused = 0;     // form of the captured graph
+    int launches = 0;  // kernel nodes of the captured graph
     std::string err;
 };
 
@@ -97,6 +107,87 @@ int bfail(pinyb200_batch *bt, int code, const std::string &msg)
         if (e_ != cudaSuccess)                                                                      \
             return bfail(bt, PINYB200_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
     } while (0)
+
+// Whether the multi-box kernels cover every box of the call: MIXED
+// molecule-pair kernel with a known site pattern, orthorhombic cells,
+// compact PME records, flags they serve.
+bool fused_ok(const pinyb200_batch *bt, const double *const *hmat, int flags)
+{
+    if (flags & (PINYB200_UPDATE_LIST | PINYB200_SITE_PAIRS | PINYB200_BATCH_BRANCHES)) return false;
+    for (size_t i = 0; i < bt->box.size(); i++) {
+        const pinyb200_ctx *c = bt->box[i];
+        const double *h = hmat[i];
+        const bool ortho = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0;
+        if (c->precision != PINYB200_MIXED || !c->use_mol || !c->mol_ok || !c->mix_ok || mix_pattern(c) == 0 ||
+            !ortho || c->pme_full_records || c->sm_count != bt->box[0]->sm_count)
+            return false;
+    }
+    return true;
+}
+
+// Every box's evaluation as multi-box kernels on bt->stream: the work of
+// enqueue_device for each box, phase by phase.
+int fused_enqueue(pinyb200_batch *bt, const double *const *d_pos, const double *const *d_xmod,
+                  const double *const *hmat, int flags, double *const *d_force)
+{
+    const int nbox = (int)bt->box.size();
+    const int sm = bt->box[0]->sm_count;
+    const bool energy = !(flags & PINYB200_NO_ENERGY);
+    cudaStream_t st = bt->stream;
+    std::vector<Cell> cells;
+    std::vector<const double *> pos;
+    std::vector<double *> force;
+    std::vector<std::pair<void *, size_t>> zero;
+    std::vector<CopySeg> xm, acc;
+    for (int i = 0; i < nbox; i++) {
+        pinyb200_ctx *c = bt->box[i];
+        cells.push_back(cell_from_hmat(hmat[i]));
+        pos.push_back(d_pos[i]);
+        force.push_back(d_force[i]);
+        const size_t nb = (size_t)c->sys.natm * 3 * c->P;
+        zero.emplace_back(c->d_forceT, nb * sizeof(double));
+        zero.emplace_back(c->d_acc, (size_t)c->P * S_NSLOT * sizeof(double));
+        if (c->P > 1) {
+            const double *src = d_xmod ? d_xmod[i] : nullptr;
+            if (src != c->d_xmod) xm.push_back(CopySeg{src, c->d_posT, c->d_xmod, (long long)c->sys.natm * 3, c->P});
+        }
+        if (energy)
+            acc.push_back(CopySeg{c->d_acc, nullptr, bt->h_acc + bt->acc_off[i], (long long)c->P * S_NSLOT, 1});
+    }
+    cudaError_t e = launch_zero_batch(zero, sm, st);
+    if (e == cudaSuccess) e = launch_transpose_in_batch(bt->box, pos, sm, st);
+    if (e == cudaSuccess && !xm.empty()) e = launch_copy_batch(xm, sm, st);
+    if (e == cudaSuccess) e = launch_ghost_batch(bt->box, false, sm, st);
+    // PME beside the pair and intramolecular kernels
+    if (e == cudaSuccess) e = cudaEventRecord(bt->pfork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(bt->pme_stream, bt->pfork, 0);
+    if (e == cudaSuccess) e = launch_pme_batch(bt->box, cells, energy, sm, bt->pme_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(bt->pjoin, bt->pme_stream);
+    if (e == cudaSuccess) e = launch_mol_pair_mixed_batch(bt->box, cells, energy, sm, st);
+    if (e == cudaSuccess) e = launch_intra_batch(bt->box, energy, sm, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, bt->pjoin, 0);
+    if (e == cudaSuccess) e = launch_pme_force_add_batch(bt->box, sm, st);
+    if (e == cudaSuccess && (flags & PINYB200_DISTRIB_GHOSTS)) e = launch_ghost_batch(bt->box, true, sm, st);
+    if (e == cudaSuccess) e = launch_transpose_out_batch(bt->box, force, sm, st);
+    // per-bead sums straight into the pinned host buffer
+    if (e == cudaSuccess && energy) e = launch_copy_batch(acc, sm, st);
+    if (e != cudaSuccess) return bfail(bt, PINYB200_ERR_CUDA, std::string("batch kernels: ") + cudaGetErrorString(e));
+    return PINYB200_OK;
+}
+
+int count_kernel_nodes(cudaGraph_t g)
+{
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+    int k = 0;
+    for (size_t i = 0; i < n; i++) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+    }
+    return k;
+}
 
 void drop_graph(pinyb200_batch *bt)
 {
@@ -211,6 +302,9 @@ int pinyb200_batch_create(pinyb200_ctx *const *ctx, int nbox, pinyb200_batch **o
     };
     if (cudaSetDevice(bt->device) != cudaSuccess) return cleanup(bfail(nullptr, PINYB200_ERR_CUDA, "batch: device"));
     if (cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&bt->pme_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&bt->pfork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&bt->pjoin, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&bt->fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreate(&bt->ev[0]) != cudaSuccess || cudaEventCreate(&bt->ev[1]) != cudaSuccess)
         return cleanup(bfail(nullptr, PINYB200_ERR_CUDA, "batch: stream/event creation failed"));
@@ -236,6 +330,9 @@ int pinyb200_batch_destroy(pinyb200_batch *bt)
     for (cudaEvent_t e : bt->join)
         if (e) cudaEventDestroy(e);
     if (bt->fork) cudaEventDestroy(bt->fork);
+    if (bt->pfork) cudaEventDestroy(bt->pfork);
+    if (bt->pjoin) cudaEventDestroy(bt->pjoin);
+    if (bt->pme_stream) cudaStreamDestroy(bt->pme_stream);
     for (int i = 0; i < 2; i++)
         if (bt->ev[i]) cudaEventDestroy(bt->ev[i]);
     if (bt->stream) cudaStreamDestroy(bt->stream);
@@ -277,10 +374,19 @@ int pinyb200_batch_energy_force_device(pinyb200_batch *bt, const double *const *
             if (rc) return bfail(bt, rc, std::string("batch warm-up: ") + pinyb200_last_error(c));
             BCK(cudaStreamSynchronize(c->stream));
         }
+        const bool fused = fused_ok(bt, hmat, flags);
+        if (fused) {
+            // one plain run of the multi-box kernels: kernel attributes and
+            // occupancy queries happen outside the capture
+            int rc = fused_enqueue(bt, d_pos, d_xmod, hmat, flags, d_force);
+            if (rc) return rc;
+            BCK(cudaStreamSynchronize(bt->stream));
+        }
         BCK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeRelaxed));
         int rc = PINYB200_OK;
-        cudaError_t ce = cudaEventRecord(bt->fork, bt->stream);
-        for (int i = 0; i < nbox && ce == cudaSuccess && rc == PINYB200_OK; i++) {
+        cudaError_t ce = fused ? cudaSuccess : cudaEventRecord(bt->fork, bt->stream);
+        if (fused) rc = fused_enqueue(bt, d_pos, d_xmod, hmat, flags, d_force);
+        for (int i = 0; i < nbox && !fused && ce == cudaSuccess && rc == PINYB200_OK; i++) {
             pinyb200_ctx *c = bt->box[i];
             ce = cudaStreamWaitEvent(c->stream, bt->fork, 0);
             if (ce != cudaSuccess) break;
@@ -295,7 +401,7 @@ int pinyb200_batch_energy_force_device(pinyb200_batch *bt, const double *const *
         const cudaError_t ee = cudaStreamEndCapture(bt->stream, &g);
         if (rc) {
             if (g) cudaGraphDestroy(g);
-            return bfail(bt, rc, "batch capture: enqueue failed");
+            return fused ? rc : bfail(bt, rc, "batch capture: enqueue failed");
         }
         if (ce != cudaSuccess || ee != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
@@ -303,6 +409,8 @@ int pinyb200_batch_energy_force_device(pinyb200_batch *bt, const double *const *
                          std::string("batch capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee));
         }
         bt->graph = g;
+        bt->fused = fused ? 1 : 0;
+        bt->launches = count_kernel_nodes(g);
         BCK(cudaGraphInstantiate(&bt->exec, bt->graph, 0));
         bt->key_ptr = kp;
         bt->key_h = kh;
@@ -326,6 +434,14 @@ int pinyb200_batch_last_ms(pinyb200_batch *bt, float *ms)
 {
     if (!bt || !ms) return bfail(bt, PINYB200_ERR_ARG, "batch_last_ms: NULL");
     *ms = bt->last_ms;
+    return PINYB200_OK;
+}
+
+int pinyb200_batch_last_mode(pinyb200_batch *bt, int *fused, int *launches)
+{
+    if (!bt) return bfail(bt, PINYB200_ERR_ARG, "batch_last_mode: NULL");
+    if (fused) *fused = bt->fused;
+    if (launches) *launches = bt->launches;
     return PINYB200_OK;
 }
 

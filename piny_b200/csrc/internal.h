@@ -425,3 +425,32 @@ size_t pme_plane_smem(int Na, int Nb, bool fp64);
 size_t pme_slab_smem(int Na, int Nc, bool fp64);
 
 }  // namespace pinyb200
+
+namespace pinyb200 {
+// Batched launches over many boxes: one persistent kernel per group of
+// boxes that share a kernel's compile-time shape (boxtab.cuh).
+int mix_pattern(const pinyb200_ctx *c);
+cudaError_t launch_mol_pair_mixed_batch(const std::vector<pinyb200_ctx *> &box, const std::vector<Cell> &cells,
+                                        bool energy, int sm_count, cudaStream_t st);
+cudaError_t launch_pme_batch(const std::vector<pinyb200_ctx *> &box, const std::vector<Cell> &cells, bool energy,
+                             int sm_count, cudaStream_t st);
+cudaError_t launch_pme_force_add_batch(const std::vector<pinyb200_ctx *> &box, int sm_count, cudaStream_t st);
+// zero byte ranges (pointer, bytes; 4-byte multiples) in one launch
+cudaError_t launch_zero_batch(const std::vector<std::pair<void *, size_t>> &seg, int sm_count, cudaStream_t st);
+// copies of n doubles src -> dst (device or pinned host memory); src null:
+// dst = the bead centroid of posT [n][P]
+struct CopySeg {
+    const double *src;
+    const double *posT;
+    double *dst;
+    long long n;
+    int P;
+};
+cudaError_t launch_copy_batch(const std::vector<CopySeg> &seg, int sm_count, cudaStream_t st);
+cudaError_t launch_transpose_in_batch(const std::vector<pinyb200_ctx *> &box, const std::vector<const double *> &d_pos,
+                                      int sm_count, cudaStream_t st);
+cudaError_t launch_transpose_out_batch(const std::vector<pinyb200_ctx *> &box, const std::vector<double *> &d_force,
+                                       int sm_count, cudaStream_t st);
+cudaError_t launch_ghost_batch(const std::vector<pinyb200_ctx *> &box, bool distrib, int sm_count, cudaStream_t st);
+cudaError_t launch_intra_batch(const std::vector<pinyb200_ctx *> &box, bool energy, int sm_count, cudaStream_t st);
+}  // namespace pinyb200

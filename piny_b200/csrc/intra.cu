@@ -11,6 +11,9 @@
 //           (src/energy/intra_con/ghost_control.c:28-129)
 #include <algorithm>
 
+#include <vector>
+
+#include "boxtab.cuh"
 #include "common.cuh"
 
 namespace pinyb200 {
@@ -35,13 +38,13 @@ __device__ __forceinline__ void block_acc(double *acc, int P, int b, const int *
 // 32 x 32 shared tile (padded against bank conflicts): both the global reads
 // and the global writes are 256-byte rows.  Positions in: in = [P][natm*3]
 // (PINY's bead-major order), out = [natm*3][P]; forces out the reverse.
-__global__ void __launch_bounds__(256) transpose_tiled_kernel(const double *__restrict__ in, double *__restrict__ out,
-                                                              int rows, long long cols)
+__device__ __forceinline__ void transpose_tiled_body(const double *__restrict__ in, double *__restrict__ out, int rows,
+                                                     long long cols, const VBlk vb)
 {
     __shared__ double tile[32][33];
-    const long long c0 = (long long)blockIdx.x * 32;
+    const long long c0 = (long long)vb.x * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int r0 = blockIdx.y * 32; r0 < rows; r0 += gridDim.y * 32) {
+    for (int r0 = vb.y * 32; r0 < rows; r0 += vb.gy * 32) {
 #pragma unroll
         for (int k = 0; k < 32; k += 8) {
             const int r = r0 + ty + k;
@@ -59,11 +62,17 @@ __global__ void __launch_bounds__(256) transpose_tiled_kernel(const double *__re
     }
 }
 
-__global__ void ghost_pos_kernel(double *__restrict__ posT, int P, int nghost, int ncomp,
-                                 const int *__restrict__ gatom, const int *__restrict__ gcomp,
-                                 const double *__restrict__ gcoef)
+__global__ void __launch_bounds__(256) transpose_tiled_kernel(const double *__restrict__ in, double *__restrict__ out,
+                                                              int rows, long long cols)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    transpose_tiled_body(in, out, rows, cols, hw_blk());
+}
+
+__device__ __forceinline__ void ghost_pos_body(double *__restrict__ posT, int P, int nghost, int ncomp,
+                                 const int *__restrict__ gatom, const int *__restrict__ gcomp,
+                                 const double *__restrict__ gcoef, const VBlk vb)
+{
+    const long long t = (long long)vb.x * blockDim.x + threadIdx.x;
     if (t >= (long long)nghost * P) return;
     const int b = (int)(t % P);
     const int g = (int)(t / P);
@@ -80,11 +89,18 @@ __global__ void ghost_pos_kernel(double *__restrict__ posT, int P, int nghost, i
     }
 }
 
-__global__ void ghost_distrib_kernel(double *__restrict__ fT, int P, int nghost, int ncomp,
-                                     const int *__restrict__ gatom, const int *__restrict__ gcomp,
-                                     const double *__restrict__ gcoef)
+__global__ void ghost_pos_kernel(double *__restrict__ posT, int P, int nghost, int ncomp,
+                                 const int *__restrict__ gatom, const int *__restrict__ gcomp,
+                                 const double *__restrict__ gcoef)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    ghost_pos_body(posT, P, nghost, ncomp, gatom, gcomp, gcoef, hw_blk());
+}
+
+__device__ __forceinline__ void ghost_distrib_body(double *__restrict__ fT, int P, int nghost, int ncomp,
+                                     const int *__restrict__ gatom, const int *__restrict__ gcomp,
+                                     const double *__restrict__ gcoef, const VBlk vb)
+{
+    const long long t = (long long)vb.x * blockDim.x + threadIdx.x;
     if (t >= (long long)nghost * P) return;
     const int b = (int)(t % P);
     const int g = (int)(t / P);
@@ -99,6 +115,13 @@ __global__ void ghost_distrib_kernel(double *__restrict__ fT, int P, int nghost,
         }
         fT[(3 * (size_t)gl + d) * P + b] = 0.0;
     }
+}
+
+__global__ void ghost_distrib_kernel(double *__restrict__ fT, int P, int nghost, int ncomp,
+                                     const int *__restrict__ gatom, const int *__restrict__ gcomp,
+                                     const double *__restrict__ gcoef)
+{
+    ghost_distrib_body(fT, P, nghost, ncomp, gatom, gcomp, gcoef, hw_blk());
 }
 
 struct IntraArgs {
@@ -124,13 +147,13 @@ __device__ __forceinline__ void load_x(const double *posT, int P, int at, int b,
     z = posT[(3 * (size_t)at + 2) * P + b];
 }
 
-__global__ void __launch_bounds__(256) bond_kernel(IntraArgs a, int nbond, const int *__restrict__ bj,
+__device__ __forceinline__ void bond_body(const IntraArgs &a, int nbond, const int *__restrict__ bj,
                                                    const double *__restrict__ eq, const double *__restrict__ cc,
-                                                   const double *__restrict__ dc)
+                                                   const double *__restrict__ dc, const VBlk vb)
 {
     __shared__ double sh[64 * 7];
-    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long stride = (long long)gridDim.x * blockDim.x;  // a multiple of P
+    const long long t0 = (long long)vb.x * blockDim.x + threadIdx.x;
+    const long long stride = (long long)vb.gx * blockDim.x;  // a multiple of P
     const int b = (int)(t0 % a.P);
     double v = 0, p[6] = {0, 0, 0, 0, 0, 0};
     for (long long t = t0; t < (long long)nbond * a.P; t += stride) {
@@ -156,6 +179,13 @@ __global__ void __launch_bounds__(256) bond_kernel(IntraArgs a, int nbond, const
         const double vals[7] = {v, p[0], p[1], p[2], p[3], p[4], p[5]};
         block_acc<7>(a.acc, a.P, b, slot, vals, sh);
     }
+}
+
+__global__ void __launch_bounds__(256) bond_kernel(const __grid_constant__ IntraArgs a, int nbond, const int *__restrict__ bj,
+                                                   const double *__restrict__ eq, const double *__restrict__ cc,
+                                                   const double *__restrict__ dc)
+{
+    bond_body(a, nbond, bj, eq, cc, dc, hw_blk());
 }
 
 // One bend of one bead (bend.c:186-330): forces on the outer atoms f1, f3
@@ -206,13 +236,13 @@ __device__ __forceinline__ void bend_term(const double *posT, int P, int a1, int
     t.dx23 = dx23; t.dy23 = dy23; t.dz23 = dz23;
 }
 
-__global__ void __launch_bounds__(256) bend_kernel(IntraArgs a, int nbend, const int *__restrict__ bj,
+__device__ __forceinline__ void bend_body(const IntraArgs &a, int nbend, const int *__restrict__ bj,
                                                    const double *__restrict__ bc, const double *__restrict__ bs,
-                                                   const double *__restrict__ bdc, const double *__restrict__ bds)
+                                                   const double *__restrict__ bdc, const double *__restrict__ bds, const VBlk vb)
 {
     __shared__ double sh[64 * 7];
-    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long stride = (long long)gridDim.x * blockDim.x;  // a multiple of P
+    const long long t0 = (long long)vb.x * blockDim.x + threadIdx.x;
+    const long long stride = (long long)vb.gx * blockDim.x;  // a multiple of P
     const int b = (int)(t0 % a.P);
     double v = 0, p[6] = {0, 0, 0, 0, 0, 0};
     for (long long t = t0; t < (long long)nbend * a.P; t += stride) {
@@ -238,13 +268,20 @@ __global__ void __launch_bounds__(256) bend_kernel(IntraArgs a, int nbend, const
     }
 }
 
-__global__ void __launch_bounds__(256) ecor_kernel(IntraArgs a, int necor, const int *__restrict__ j1s,
+__global__ void __launch_bounds__(256) bend_kernel(const __grid_constant__ IntraArgs a, int nbend, const int *__restrict__ bj,
+                                                   const double *__restrict__ bc, const double *__restrict__ bs,
+                                                   const double *__restrict__ bdc, const double *__restrict__ bds)
+{
+    bend_body(a, nbend, bj, bc, bs, bdc, bds, hw_blk());
+}
+
+__device__ __forceinline__ void ecor_body(const IntraArgs &a, int necor, const int *__restrict__ j1s,
                                                    const int *__restrict__ j2s, int nsplin, double rmin, double dr,
-                                                   double dri, const double4 *__restrict__ tab)
+                                                   double dri, const double4 *__restrict__ tab, const VBlk vb)
 {
     __shared__ double sh[64 * 7];
-    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long stride = (long long)gridDim.x * blockDim.x;  // a multiple of P
+    const long long t0 = (long long)vb.x * blockDim.x + threadIdx.x;
+    const long long stride = (long long)vb.gx * blockDim.x;  // a multiple of P
     const int b = (int)(t0 % a.P);
     double v = 0, p[6] = {0, 0, 0, 0, 0, 0};
     for (long long t = t0; t < (long long)necor * a.P; t += stride) {
@@ -273,6 +310,13 @@ __global__ void __launch_bounds__(256) ecor_kernel(IntraArgs a, int necor, const
         const double vals[7] = {v, p[0], p[1], p[2], p[3], p[4], p[5]};
         block_acc<7>(a.acc, a.P, b, slot, vals, sh);
     }
+}
+
+__global__ void __launch_bounds__(256) ecor_kernel(const __grid_constant__ IntraArgs a, int necor, const int *__restrict__ j1s,
+                                                   const int *__restrict__ j2s, int nsplin, double rmin, double dr,
+                                                   double dri, const double4 *__restrict__ tab)
+{
+    ecor_body(a, necor, j1s, j2s, nsplin, rmin, dr, dri, tab, hw_blk());
 }
 
 // ---- RESPA: weighted intramolecular forces, no energies -------------------
@@ -474,6 +518,222 @@ cudaError_t launch_ecor_weighted(pinyb200_ctx *c, double w, double *target, int 
         c->P, c->d_posT, target, s.charge, s.necor, s.ecor_j1, s.ecor_j2, s.ecor_nsplin, s.ecor_rmin, s.ecor_dr,
         s.ecor_dri, s.ecor_tab, (const double4 *)c->d_ecor_res_tab, table, w, c->r_wter_res);
     return cudaGetLastError();
+}
+
+
+// ---------------------------------------------------------------------------
+// Many boxes per launch (the batched evaluation): staging, intramolecular
+// terms and the finishing steps of every box in a few persistent launches.
+
+struct ZeroBox {
+    unsigned *p;
+    long long n;  // 4-byte words
+};
+
+// 1024 words per block, 16-byte stores where the range allows
+__device__ __forceinline__ void zero_body(unsigned *p, long long n, const VBlk vb)
+{
+    const long long w = ((long long)vb.x * blockDim.x + threadIdx.x) * 4;
+    if (w >= n) return;
+    if (w + 4 <= n && (((uintptr_t)(p + w)) & 15) == 0) {
+        *(uint4 *)(p + w) = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+        for (long long k = w; k < n && k < w + 4; k++) p[k] = 0u;
+    }
+}
+
+__global__ void __launch_bounds__(256) zero_batch_kernel(const __grid_constant__ BoxTab<ZeroBox> t)
+{
+    PINYB200_BOX_LOOP(t, i, vb, (zero_body(t.arg[i].p, t.arg[i].n, vb)));
+}
+
+__global__ void __launch_bounds__(256) copy_batch_kernel(const __grid_constant__ BoxTab<CopySeg> t)
+{
+    PINYB200_BOX_LOOP(t, i, vb, {
+        const CopySeg &c = t.arg[i];
+        const long long k = (long long)vb.x * blockDim.x + threadIdx.x;
+        if (k < c.n) {
+            if (c.src) {
+                c.dst[k] = c.src[k];
+            } else {
+                double v = 0.0;
+                for (int b = 0; b < c.P; b++) v += c.posT[k * c.P + b];
+                c.dst[k] = v / (double)c.P;
+            }
+        }
+    });
+}
+
+struct TrBox {
+    const double *in;
+    double *out;
+    int rows;
+    long long cols;
+};
+
+__global__ void __launch_bounds__(256) transpose_batch_kernel(const __grid_constant__ BoxTab<TrBox> t)
+{
+    PINYB200_BOX_LOOP(t, i, vb, (transpose_tiled_body(t.arg[i].in, t.arg[i].out, t.arg[i].rows, t.arg[i].cols, vb)));
+}
+
+struct GhostBox {
+    double *x;  // positions (placement) or forces (distribution)
+    int P, nghost, ncomp;
+    const int *gatom, *gcomp;
+    const double *gcoef;
+};
+
+template <bool DISTRIB>
+__global__ void __launch_bounds__(256) ghost_batch_kernel(const __grid_constant__ BoxTab<GhostBox> t)
+{
+    PINYB200_BOX_LOOP(t, i, vb, {
+        const GhostBox &g = t.arg[i];
+        if (DISTRIB) ghost_distrib_body(g.x, g.P, g.nghost, g.ncomp, g.gatom, g.gcomp, g.gcoef, vb);
+        else ghost_pos_body(g.x, g.P, g.nghost, g.ncomp, g.gatom, g.gcomp, g.gcoef, vb);
+    });
+}
+
+// One intramolecular term of one box: kind 0 bonds, 1 bends, 2 excluded-pair
+// correction; the three kinds of every box share one launch (a typed work list).
+struct IntraBox {
+    IntraArgs a;
+    int kind, n;
+    const int *j1, *j2;
+    const double *c0, *c1, *c2, *c3;
+    int nsplin;
+    double rmin, dr, dri;
+    const double4 *tab;
+};
+
+__global__ void __launch_bounds__(256) intra_batch_kernel(const __grid_constant__ BoxTab<IntraBox> t)
+{
+    PINYB200_BOX_LOOP(t, i, vb, {
+        const IntraBox &x = t.arg[i];
+        if (x.kind == 0) bond_body(x.a, x.n, x.j1, x.c0, x.c1, x.c2, vb);
+        else if (x.kind == 1) bend_body(x.a, x.n, x.j1, x.c0, x.c1, x.c2, x.c3, vb);
+        else ecor_body(x.a, x.n, x.j1, x.j2, x.nsplin, x.rmin, x.dr, x.dri, x.tab, vb);
+    });
+}
+
+cudaError_t launch_zero_batch(const std::vector<std::pair<void *, size_t>> &seg, int sm_count, cudaStream_t st)
+{
+    BoxTabBuilder<ZeroBox> tb;
+    for (const auto &z : seg) {
+        const long long n = (long long)(z.second / 4);
+        tb.add(ZeroBox{(unsigned *)z.first, n}, (int)((n + 1023) / 1024), 1, (double)n);
+    }
+    return launch_tables(tb, (const void *)zero_batch_kernel, 256, 0, sm_count,
+                         [&](const BoxTab<ZeroBox> &t, int g) { zero_batch_kernel<<<g, 256, 0, st>>>(t); });
+}
+
+cudaError_t launch_copy_batch(const std::vector<CopySeg> &seg, int sm_count, cudaStream_t st)
+{
+    BoxTabBuilder<CopySeg> tb;
+    for (const CopySeg &c : seg) tb.add(c, (int)((c.n + 255) / 256), 1, (double)c.n * (c.src ? 1 : c.P));
+    return launch_tables(tb, (const void *)copy_batch_kernel, 256, 0, sm_count,
+                         [&](const BoxTab<CopySeg> &t, int g) { copy_batch_kernel<<<g, 256, 0, st>>>(t); });
+}
+
+// Positions of every box into its [atom][xyz][bead] layout (from d_pos[i],
+// PINY's [bead][atom][xyz]).
+cudaError_t launch_transpose_in_batch(const std::vector<pinyb200_ctx *> &box, const std::vector<const double *> &d_pos,
+                                      int sm_count, cudaStream_t st)
+{
+    BoxTabBuilder<TrBox> tb;
+    for (size_t i = 0; i < box.size(); i++) {
+        pinyb200_ctx *c = box[i];
+        const long long M = (long long)c->sys.natm * 3;
+        tb.add(TrBox{d_pos[i], c->d_posT, c->P, M}, (int)((M + 31) / 32), (c->P + 31) / 32, (double)M * c->P);
+    }
+    return launch_tables(tb, (const void *)transpose_batch_kernel, 256, 0, sm_count,
+                         [&](const BoxTab<TrBox> &t, int g) { transpose_batch_kernel<<<g, 256, 0, st>>>(t); });
+}
+
+// Site forces of every box out to d_force[i] in PINY's order.
+cudaError_t launch_transpose_out_batch(const std::vector<pinyb200_ctx *> &box, const std::vector<double *> &d_force,
+                                       int sm_count, cudaStream_t st)
+{
+    BoxTabBuilder<TrBox> tb;
+    for (size_t i = 0; i < box.size(); i++) {
+        pinyb200_ctx *c = box[i];
+        const long long M = (long long)c->sys.natm * 3;
+        tb.add(TrBox{c->d_forceT, d_force[i], (int)M, c->P}, (c->P + 31) / 32,
+               (int)std::min<long long>((M + 31) / 32, 65535), (double)M * c->P);
+    }
+    return launch_tables(tb, (const void *)transpose_batch_kernel, 256, 0, sm_count,
+                         [&](const BoxTab<TrBox> &t, int g) { transpose_batch_kernel<<<g, 256, 0, st>>>(t); });
+}
+
+cudaError_t launch_ghost_batch(const std::vector<pinyb200_ctx *> &box, bool distrib, int sm_count, cudaStream_t st)
+{
+    BoxTabBuilder<GhostBox> tb;
+    for (pinyb200_ctx *c : box) {
+        const DeviceSystem &s = c->sys;
+        if (s.nghost == 0) continue;
+        const long long n = (long long)s.nghost * c->P;
+        tb.add(GhostBox{distrib ? c->d_forceT : c->d_posT, c->P, s.nghost, s.ghost_ncomp, s.ghost_atom, s.ghost_comp,
+                        s.ghost_coef},
+               (int)((n + 255) / 256), 1, (double)n);
+    }
+    if (distrib)
+        return launch_tables(tb, (const void *)ghost_batch_kernel<true>, 256, 0, sm_count,
+                             [&](const BoxTab<GhostBox> &t, int g) { ghost_batch_kernel<true><<<g, 256, 0, st>>>(t); });
+    return launch_tables(tb, (const void *)ghost_batch_kernel<false>, 256, 0, sm_count,
+                         [&](const BoxTab<GhostBox> &t, int g) { ghost_batch_kernel<false><<<g, 256, 0, st>>>(t); });
+}
+
+// Bonds, bends and excluded-pair corrections of every box in one launch.
+cudaError_t launch_intra_batch(const std::vector<pinyb200_ctx *> &box, bool energy, int sm_count, cudaStream_t st)
+{
+    BoxTabBuilder<IntraBox> tb;
+    for (pinyb200_ctx *c : box) {
+        const DeviceSystem &s = c->sys;
+        IntraBox x;
+        memset(&x, 0, sizeof(x));
+        x.a.natm = s.natm;
+        x.a.P = c->P;
+        x.a.posT = c->d_posT;
+        x.a.forceT = c->d_forceT;
+        x.a.acc = c->d_acc;
+        x.a.charge = s.charge;
+        x.a.energy = energy ? 1 : 0;
+        if (s.nbond) {
+            IntraBox b = x;
+            b.kind = 0;
+            b.n = s.nbond;
+            b.j1 = s.bond_j;
+            b.c0 = s.bond_eq;
+            b.c1 = s.bond_c;
+            b.c2 = s.bond_dc;
+            tb.add(b, (int)nblk_gs(c, (long long)s.nbond * c->P), 1, (double)s.nbond * c->P);
+        }
+        if (s.nbend) {
+            IntraBox b = x;
+            b.kind = 1;
+            b.n = s.nbend;
+            b.j1 = s.bend_j;
+            b.c0 = s.bend_c;
+            b.c1 = s.bend_s;
+            b.c2 = s.bend_dc;
+            b.c3 = s.bend_ds;
+            tb.add(b, (int)nblk_gs(c, (long long)s.nbend * c->P), 1, 2.0 * s.nbend * c->P);
+        }
+        if (s.necor) {
+            IntraBox b = x;
+            b.kind = 2;
+            b.n = s.necor;
+            b.j1 = s.ecor_j1;
+            b.j2 = s.ecor_j2;
+            b.nsplin = s.ecor_nsplin;
+            b.rmin = s.ecor_rmin;
+            b.dr = s.ecor_dr;
+            b.dri = s.ecor_dri;
+            b.tab = s.ecor_tab;
+            tb.add(b, (int)nblk_gs(c, (long long)s.necor * c->P), 1, (double)s.necor * c->P);
+        }
+    }
+    return launch_tables(tb, (const void *)intra_batch_kernel, 256, 0, sm_count,
+                         [&](const BoxTab<IntraBox> &t, int g) { intra_batch_kernel<<<g, 256, 0, st>>>(t); });
 }
 
 }  // namespace pinyb200

@@ -20,10 +20,13 @@
 //   * FP64: every site-pair separation and image shift in FP64 with PINY's
 //     operation order, as in the site kernel.
 #include <algorithm>
+#include <map>
+#include <vector>
 #include <cmath>
 #include <cstddef>
 #include <string>
 
+#include "boxtab.cuh"
 #include "common.cuh"
 
 namespace pinyb200 {
@@ -1198,8 +1201,8 @@ constexpr unsigned kAnyPair = 0xffffffffu;
 constexpr unsigned kTip4pCoul = 0xEEE0u, kTip4pVdw = 0x1u;  // O H H M: H, M charged; LJ on O-O
 constexpr unsigned kSpcCoul = 0x1FFu, kSpcVdw = 0x1u;       // O H H: all charged; LJ on O-O
 
-template <int P, int NS, bool ENERGY, unsigned CM = kAnyPair, unsigned VM = kAnyPair>
-__global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kernel(MixArgs a, Cell cell)
+template <int P, int NS, bool ENERGY, unsigned CM, unsigned VM>
+__device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell &cell, const VBlk vb)
 {
     constexpr int G = P >= 32 ? 32 : P;  // lanes per molecule pair
     constexpr int JPI = 32 / G;          // molecule pairs per warp step
@@ -1225,15 +1228,15 @@ __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kerne
         for (int c = 0; c < 8; c++) sacc[c][threadIdx.x] = 0.0;
     __syncthreads();
     if (a.bad && (a.bad[0] | a.bad[1])) {
-        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) a.acc[S_VVDW] = __longlong_as_double(0x7ff8000000000000LL);
+        if (vb.x == 0 && vb.y == 0 && threadIdx.x == 0) a.acc[S_VVDW] = __longlong_as_double(0x7ff8000000000000LL);
         return;
     }
     const float4 *__restrict__ tab = a.tab;
     const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int warp = (vb.x * (int)blockDim.x + (int)threadIdx.x) >> 5;
+    const int nwarps = (vb.gx * (int)blockDim.x) >> 5;
     const int sub = lane / G;
-    const int b = (lane % G) + 32 * blockIdx.y;  // bead
+    const int b = (lane % G) + 32 * vb.y;  // bead
     const double *__restrict__ posT = a.posT;
     const float rc2 = a.rc2, dri = a.dri_f, rmd = a.rmd, tmax = a.tmax;
     constexpr float kRound = 12582912.0f;  // 1.5 * 2^23: x + kRound - kRound = nearest integer of x
@@ -1409,6 +1412,33 @@ __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS) mol_pair_mixed_kerne
             if (G == 32 || sub == 0) atomicAdd(&a.acc[(size_t)b * S_NSLOT + slot[c]], t);
         }
     }
+}
+
+
+template <int P, int NS, bool ENERGY, unsigned CM = kAnyPair, unsigned VM = kAnyPair>
+__global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS)
+    mol_pair_mixed_kernel(const __grid_constant__ MixArgs a, const __grid_constant__ Cell cell)
+{
+    mol_pair_mixed_body<P, NS, ENERGY, CM, VM>(a, cell, hw_blk());
+}
+
+// Many boxes of one bead count and site pattern in one persistent launch.
+struct MixBox {
+    MixArgs a;
+    Cell cell;
+};
+
+// Resident blocks per SM of the batched MIXED kernel: the argument table
+// is indexed at run time, which costs registers (4 x 128 threads leave 128,
+// no spills; at 5 it spills 100-200 bytes).
+#ifndef PINYB200_MIX_BATCH_BLOCKS
+#define PINYB200_MIX_BATCH_BLOCKS 4
+#endif
+template <int P, int NS, bool ENERGY, unsigned CM = kAnyPair, unsigned VM = kAnyPair>
+__global__ void __launch_bounds__(128, PINYB200_MIX_BATCH_BLOCKS)
+    mol_pair_mixed_batch_kernel(const __grid_constant__ BoxTab<MixBox> t)
+{
+    PINYB200_BOX_LOOP(t, i, vb, (mol_pair_mixed_body<P, NS, ENERGY, CM, VM>(t.arg[i].a, t.arg[i].cell, vb)));
 }
 
 // ---------------------------------------------------------------------------
@@ -1737,8 +1767,8 @@ static cudaError_t launch_mix_ns(pinyb200_ctx *c, const MixArgs &a, const Cell &
     return cudaGetLastError();
 }
 
-// The MIXED kernel with combined per-site-pair tables (pinyb200_ctx::mix_ok).
-cudaError_t launch_mol_pair_mixed(pinyb200_ctx *c, const Cell &cell, bool energy)
+// Arguments of the MIXED molecule-pair kernel for one context.
+static MixArgs mix_args(pinyb200_ctx *c)
 {
     const DeviceSystem &s = c->sys;
     MixArgs a;
@@ -1775,8 +1805,95 @@ cudaError_t launch_mol_pair_mixed(pinyb200_ctx *c, const Cell &cell, bool energy
     a.dri_f = c->mix_dri;
     a.rmd = c->mix_rmd;
     a.tmax = c->mix_tmax;
+    return a;
+}
+
+// The MIXED kernel with combined per-site-pair tables (pinyb200_ctx::mix_ok).
+cudaError_t launch_mol_pair_mixed(pinyb200_ctx *c, const Cell &cell, bool energy)
+{
+    const MixArgs a = mix_args(c);
     if (c->mol_ns == 3) return launch_mix_ns<3>(c, a, cell, energy);
     return launch_mix_ns<4>(c, a, cell, energy);
+}
+
+// Site-pair table pattern of a context: 1 q-TIP4P/F-like (4 sites), 2
+// q-SPC/Fw-like (3 sites), 0 another pattern.
+int mix_pattern(const pinyb200_ctx *c)
+{
+    unsigned cm = 0, vm = 0;
+    const int NS = c->mol_ns;
+    for (int k = 0; k < NS * NS; k++) {
+        if (c->mix_eflag[k] & 2) cm |= 1u << k;
+        if (c->mix_eflag[k] & 1) vm |= 1u << k;
+    }
+    if (NS == 4 && cm == kTip4pCoul && vm == kTip4pVdw) return 1;
+    if (NS == 3 && cm == kSpcCoul && vm == kSpcVdw) return 2;
+    return 0;
+}
+
+template <int P, int NS, unsigned CM, unsigned VM>
+static cudaError_t launch_mix_batch_t(const std::vector<pinyb200_ctx *> &box, const std::vector<Cell> &cells,
+                                      bool energy, int sm_count, cudaStream_t st)
+{
+    BoxTabBuilder<MixBox> tb;
+    for (size_t i = 0; i < box.size(); i++) {
+        pinyb200_ctx *c = box[i];
+        // blocks of the box's own grid-stride loop over its chunks: about
+        // two chunks per warp
+        const long long vb = std::max<long long>(1, (c->chunk_cap + 7) / 8);
+        tb.add(MixBox{mix_args(c), cells[i]}, (int)std::min<long long>(vb, 1 << 20), P > 32 ? P / 32 : 1,
+               (double)c->chunk_cap * P);
+    }
+    const void *fn = energy ? (const void *)mol_pair_mixed_batch_kernel<P, NS, true, CM, VM>
+                            : (const void *)mol_pair_mixed_batch_kernel<P, NS, false, CM, VM>;
+    cudaError_t err = carveout_pref(fn, box.empty() ? 25 : box[0]->pair_carveout);
+    if (err != cudaSuccess) return err;
+    return launch_tables(tb, fn, 128, 0, sm_count, [&](const BoxTab<MixBox> &t, int g) {
+        if (energy) mol_pair_mixed_batch_kernel<P, NS, true, CM, VM><<<g, 128, 0, st>>>(t);
+        else mol_pair_mixed_batch_kernel<P, NS, false, CM, VM><<<g, 128, 0, st>>>(t);
+    });
+}
+
+template <int NS, unsigned CM, unsigned VM>
+static cudaError_t launch_mix_batch_p(int P, const std::vector<pinyb200_ctx *> &box, const std::vector<Cell> &cells,
+                                      bool energy, int sm_count, cudaStream_t st)
+{
+    switch (P) {
+    case 1: return launch_mix_batch_t<1, NS, CM, VM>(box, cells, energy, sm_count, st);
+    case 2: return launch_mix_batch_t<2, NS, CM, VM>(box, cells, energy, sm_count, st);
+    case 4: return launch_mix_batch_t<4, NS, CM, VM>(box, cells, energy, sm_count, st);
+    case 8: return launch_mix_batch_t<8, NS, CM, VM>(box, cells, energy, sm_count, st);
+    case 16: return launch_mix_batch_t<16, NS, CM, VM>(box, cells, energy, sm_count, st);
+    case 32: return launch_mix_batch_t<32, NS, CM, VM>(box, cells, energy, sm_count, st);
+    case 64: return launch_mix_batch_t<64, NS, CM, VM>(box, cells, energy, sm_count, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// MIXED molecule-pair forces of many boxes: one persistent launch per
+// (bead count, site pattern) group.  Every box must have mix_pattern() != 0.
+cudaError_t launch_mol_pair_mixed_batch(const std::vector<pinyb200_ctx *> &box, const std::vector<Cell> &cells,
+                                        bool energy, int sm_count, cudaStream_t st)
+{
+    std::map<std::pair<int, int>, std::pair<std::vector<pinyb200_ctx *>, std::vector<Cell>>> groups;
+    for (size_t i = 0; i < box.size(); i++) {
+        auto &g = groups[std::make_pair(box[i]->P, mix_pattern(box[i]))];
+        g.first.push_back(box[i]);
+        g.second.push_back(cells[i]);
+    }
+    for (auto &kv : groups) {
+        const int P = kv.first.first, pat = kv.first.second;
+        cudaError_t err;
+        if (pat == 1)
+            err = launch_mix_batch_p<4, kTip4pCoul, kTip4pVdw>(P, kv.second.first, kv.second.second, energy, sm_count,
+                                                                st);
+        else if (pat == 2)
+            err = launch_mix_batch_p<3, kSpcCoul, kSpcVdw>(P, kv.second.first, kv.second.second, energy, sm_count, st);
+        else
+            err = cudaErrorInvalidValue;
+        if (err != cudaSuccess) return err;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace pinyb200

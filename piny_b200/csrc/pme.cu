@@ -27,6 +27,11 @@
 //               inverse FFT along a, real potential out
 //   gather      per (tile, bead): forces from a shared copy of the tile's
 //               potential
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "boxtab.cuh"
 #include "common.cuh"
 
 namespace pinyb200 {
@@ -455,15 +460,21 @@ __device__ __forceinline__ void gather_store(const PmeArgs &a, const Cell &cell,
 }
 
 // Adds the PME forces [nchrg][3][P] to the site forces [natm][3][P].
-__global__ void __launch_bounds__(256) pme_force_add_kernel(int nchrg, int P, const int *__restrict__ ichrg,
-                                                            const double *__restrict__ fP, double *__restrict__ fT)
+__device__ __forceinline__ void pme_force_add_body(int nchrg, int P, const int *__restrict__ ichrg,
+                                                   const double *__restrict__ fP, double *__restrict__ fT, const VBlk vb)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long t = (long long)vb.x * blockDim.x + threadIdx.x;
     if (t >= (long long)nchrg * 3 * P) return;
     const long long kd = t / P;
     const int b = (int)(t - kd * P);
     const int k = (int)(kd / 3), d = (int)(kd - 3LL * k);
     fT[(3 * (size_t)ichrg[k] + d) * P + b] += fP[t];
+}
+
+__global__ void __launch_bounds__(256) pme_force_add_kernel(int nchrg, int P, const int *__restrict__ ichrg,
+                                                            const double *__restrict__ fP, double *__restrict__ fT)
+{
+    pme_force_add_body(nchrg, P, ichrg, fP, fT, hw_blk());
 }
 
 // RESPA outer level: PME forces x wght_ter into another buffer
@@ -688,9 +699,10 @@ __device__ __forceinline__ typename Vec4<R>::T load_frac(const void *rw, int idx
 // origin in FP64 with PINY's operation order (as pme_bin_kernel), record
 // (atom, la, lb, lc) + (fa, fb, fc, q), record number filed under its tile.
 template <typename R, int NI>
-__global__ void __launch_bounds__(256) pme_bin_compact_kernel(PmeArgs a, Cell cell, TileArgs t)
+__device__ __forceinline__ void pme_bin_compact_body(const PmeArgs &a, const Cell &cell, const TileArgs &t,
+                                                     const VBlk vb)
 {
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long idx = (long long)vb.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)a.nchrg * a.P) return;
     const int b = (int)(idx % a.P);
     const int k = (int)(idx / a.P);
@@ -710,6 +722,14 @@ __global__ void __launch_bounds__(256) pme_bin_compact_kernel(PmeArgs a, Cell ce
     const int slot = atomicAdd(&t.cnt[b * t.ntile + tile], 1);
     if (slot < t.cap) t.bin[((size_t)b * t.ntile + tile) * t.cap + slot] = (int)idx;
     else t.ovf[atomicAdd(&t.cnt[a.P * t.ntile], 1)] = (int)idx;
+}
+
+template <typename R, int NI>
+__global__ void __launch_bounds__(256) pme_bin_compact_kernel(const __grid_constant__ PmeArgs a,
+                                                              const __grid_constant__ Cell cell,
+                                                              const __grid_constant__ TileArgs t)
+{
+    pme_bin_compact_body<R, NI>(a, cell, t, hw_blk());
 }
 
 // Weights one spread lane needs (lanes = 8 a points x 4 b rows): its a
@@ -760,7 +780,7 @@ __device__ __forceinline__ void spread_warp_global(const PmeArgs &a, R *g, int l
 // to the grid once), with the weights evaluated in the block and the next
 // record read ahead.
 template <typename R, int NI, int TT>
-__global__ void __launch_bounds__(256) spread_tile_c_kernel(PmeArgs a, TileArgs t)
+__device__ __forceinline__ void spread_tile_c_body(const PmeArgs &a, const TileArgs &t, const VBlk vb)
 {
     typedef TileGeom<NI, TT> TG;
     typedef typename Vec4<R>::T R4;
@@ -771,7 +791,7 @@ __global__ void __launch_bounds__(256) spread_tile_c_kernel(PmeArgs a, TileArgs 
     for (int i = threadIdx.x; i < TG::NPT; i += blockDim.x) tl[i] = (R)0;
     pt.fill(false);
     __syncthreads();
-    const int tile = blockIdx.x, b = blockIdx.y;
+    const int tile = vb.x, b = vb.y;
     const int ta0 = (tile % t.nta) * TG::T, tb0 = ((tile / t.nta) % t.ntb) * TG::T, tc0 = (tile / (t.nta * t.ntb)) * TG::T;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int la8 = lane & 7, lb4 = lane >> 3;
@@ -829,7 +849,7 @@ __global__ void __launch_bounds__(256) spread_tile_c_kernel(PmeArgs a, TileArgs 
     }
     // overflow records: one warp each, straight into the grid
     const int nov = t.cnt[a.P * t.ntile];
-    const int gid = blockIdx.y * gridDim.x + blockIdx.x, nblk = gridDim.x * gridDim.y;
+    const int gid = vb.y * vb.gx + vb.x, nblk = vb.gx * vb.gy;
     for (int e = gid * nwarp + warp; e < nov; e += nblk * nwarp) {
         const int idx = t.ovf[e];
         const int4 h = a.rhead[idx];
@@ -867,6 +887,13 @@ __global__ void __launch_bounds__(256) spread_tile_c_kernel(PmeArgs a, TileArgs 
             }
         }
     }
+}
+
+template <typename R, int NI, int TT>
+__global__ void __launch_bounds__(256) spread_tile_c_kernel(const __grid_constant__ PmeArgs a,
+                                                            const __grid_constant__ TileArgs t)
+{
+    spread_tile_c_body<R, NI, TT>(a, t, hw_blk());
 }
 
 // Gather weights of one record for lane l8 of an 8-lane group: its a
@@ -910,7 +937,7 @@ __device__ __forceinline__ void gather_weights(const PolyTab<R, NI> &pt, const t
 // record), with the weights evaluated in the block and the next record
 // read ahead.
 template <typename R, int NI, int TT>
-__global__ void __launch_bounds__(256) gather_tile_c_kernel(PmeArgs a, Cell cell, TileArgs t)
+__device__ __forceinline__ void gather_tile_c_body(const PmeArgs &a, const Cell &cell, const TileArgs &t, const VBlk vb)
 {
     typedef TileGeom<NI, TT> TG;
     typedef typename Vec4<R>::T R4;
@@ -918,7 +945,7 @@ __global__ void __launch_bounds__(256) gather_tile_c_kernel(PmeArgs a, Cell cell
     R *tl = (R *)smem_raw;
     __shared__ __align__(16) PolyTab<R, NI> pt;
     pt.fill(true);
-    const int tile = blockIdx.x, b = blockIdx.y;
+    const int tile = vb.x, b = vb.y;
     const int ta0 = (tile % t.nta) * TG::T, tb0 = ((tile / t.nta) % t.ntb) * TG::T, tc0 = (tile / (t.nta * t.ntb)) * TG::T;
     const R *g = (const R *)a.grid + (size_t)b * a.Na * a.Nb * a.Nc;
     const int n = min(t.cnt[b * t.ntile + tile], t.cap);
@@ -990,7 +1017,7 @@ __global__ void __launch_bounds__(256) gather_tile_c_kernel(PmeArgs a, Cell cell
         gather_store(a, cell, h.x, idx, ea, eb, ec, act ? l8 : 1);
     }
     const int nov = t.cnt[a.P * t.ntile];
-    const int gid = blockIdx.y * gridDim.x + blockIdx.x, nblk = gridDim.x * gridDim.y;
+    const int gid = vb.y * vb.gx + vb.x, nblk = vb.gx * vb.gy;
     const int nr2 = (nov + nblk * ngrp - 1) / (nblk * ngrp);
     for (int r = 0; r < nr2; r++) {
         const int e = (r * nblk + gid) * ngrp + grp;
@@ -1017,6 +1044,14 @@ __global__ void __launch_bounds__(256) gather_tile_c_kernel(PmeArgs a, Cell cell
         }
         gather_store(a, cell, h.x, idx, ea, eb, ec, act ? l8 : 1);
     }
+}
+
+template <typename R, int NI, int TT>
+__global__ void __launch_bounds__(256) gather_tile_c_kernel(const __grid_constant__ PmeArgs a,
+                                                            const __grid_constant__ Cell cell,
+                                                            const __grid_constant__ TileArgs t)
+{
+    gather_tile_c_body<R, NI, TT>(a, cell, t, hw_blk());
 }
 
 // ---------------------------------------------------------------------------
@@ -1203,6 +1238,12 @@ __device__ __forceinline__ void line_fft(typename Cplx<R>::T *sm, int N, int nl,
     }
 }
 
+// Resident blocks per SM the plane and slab kernels of compile-time length
+// are compiled for (their registers: 256 threads x 128 / this).
+#ifndef PINYB200_FFT_BLOCKS
+#define PINYB200_FFT_BLOCKS 2
+#endif
+
 template <typename R>
 __device__ __forceinline__ void load_twiddles(R *dst, const R *src, int N)
 {
@@ -1212,9 +1253,9 @@ __device__ __forceinline__ void load_twiddles(R *dst, const R *src, int N)
 // Forward transform of one (bead, c) plane along a then b; half spectrum
 // (a <= Na/2) out.  Shared: plane [Nb][Na+1] complex, twiddles.
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) plane_fwd_kernel(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
-                                                        int Na, int Nb, int Nc, const R *__restrict__ twa,
-                                                        const R *__restrict__ twb)
+__device__ __forceinline__ void plane_fwd_body(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec, int Na,
+                                               int Nb, int Nc, const R *__restrict__ twa, const R *__restrict__ twb,
+                                               const VBlk vb)
 {
     if (NF > 0) Na = Nb = NF;  // cubic power-of-two grid known at compile time
     (void)Nc;
@@ -1225,7 +1266,7 @@ __global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) plane_fwd_kernel(const R 
     R *ta = (R *)(pl + (size_t)Nb * ls);
     R *tb = ta + 2 * Na;
     const int Nh = Na / 2 + 1;
-    const size_t plane = blockIdx.x;  // bead * Nc + c
+    const size_t plane = vb.x;  // bead * Nc + c
     load_twiddles(ta, twa, Na);
     load_twiddles(tb, twb, Nb);
     const R *src = q + plane * Na * Nb;
@@ -1242,13 +1283,21 @@ __global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) plane_fwd_kernel(const R 
     for (int idx = threadIdx.x; idx < Nb * Nh; idx += blockDim.x) dst[idx] = pl[(idx / Nh) * ls + idx % Nh];
 }
 
+template <typename R, int NF>
+__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1) plane_fwd_kernel(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
+                                                        int Na, int Nb, int Nc, const R *__restrict__ twa,
+                                                        const R *__restrict__ twb)
+{
+    plane_fwd_body<R, NF>(q, spec, Na, Nb, Nc, twa, twb, hw_blk());
+}
+
 // Inverse of plane_fwd: half spectrum in, along b, Hermitian completion of
 // each row (U(Na-a) = conj U(a) once b and c are back in real space), along
 // a, real part out.
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) plane_inv_kernel(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phi,
-                                                        int Na, int Nb, int Nc, const R *__restrict__ twa,
-                                                        const R *__restrict__ twb)
+__device__ __forceinline__ void plane_inv_body(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phi, int Na,
+                                               int Nb, int Nc, const R *__restrict__ twa, const R *__restrict__ twb,
+                                               const VBlk vb)
 {
     if (NF > 0) Na = Nb = NF;  // cubic power-of-two grid known at compile time
     (void)Nc;
@@ -1259,7 +1308,7 @@ __global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) plane_inv_kernel(const ty
     R *ta = (R *)(pl + (size_t)Nb * ls);
     R *tb = ta + 2 * Na;
     const int Nh = Na / 2 + 1;
-    const size_t plane = blockIdx.x;
+    const size_t plane = vb.x;
     load_twiddles(ta, twa, Na);
     load_twiddles(tb, twb, Nb);
     const C2 *src = spec + plane * (size_t)Nb * Nh;
@@ -1280,14 +1329,22 @@ __global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) plane_inv_kernel(const ty
     for (int idx = threadIdx.x; idx < Na * Nb; idx += blockDim.x) dst[idx] = pl[(idx / Na) * ls + idx % Na].x;
 }
 
+template <typename R, int NF>
+__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1) plane_inv_kernel(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phi,
+                                                        int Na, int Nb, int Nc, const R *__restrict__ twa,
+                                                        const R *__restrict__ twb)
+{
+    plane_inv_body<R, NF>(spec, phi, Na, Nb, Nc, twa, twb, hw_blk());
+}
+
 // One (bead, b) slab of the half spectrum: FFT along c, energy and virial
 // of the k-sphere terms (ewald3d_pme.c:366-425), multiplication by the
 // influence function, inverse FFT along c.  Half-spectrum points with
 // 0 < a < Na/2 stand for two full-grid points; E = 1/2 sum_full w |S|^2.
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) conv_c_kernel(typename Cplx<R>::T *__restrict__ spec, const R *__restrict__ filt,
-                                                     int Na, int Nb, int Nc, const R *__restrict__ twc, Cell cell,
-                                                     double alp, double *__restrict__ acc, int energy)
+__device__ __forceinline__ void conv_c_body(typename Cplx<R>::T *__restrict__ spec, const R *__restrict__ filt, int Na,
+                                            int Nb, int Nc, const R *__restrict__ twc, const Cell &cell, double alp,
+                                            double *__restrict__ acc, int energy, const VBlk vb)
 {
     if (NF > 0) Na = Nb = Nc = NF;  // cubic power-of-two grid known at compile time
     typedef typename Cplx<R>::T C2;
@@ -1297,7 +1354,7 @@ __global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) conv_c_kernel(typename Cp
     const int ls = Nh + 1;  // padded line stride: element c of column a at sl[c * ls + a]
     R *tc = (R *)(sl + (size_t)Nc * ls);
     __shared__ double red[7][8];
-    const int bead = blockIdx.x / Nb, b = blockIdx.x % Nb;
+    const int bead = vb.x / Nb, b = vb.x % Nb;
     load_twiddles(tc, twc, Nc);
     C2 *base = spec + ((size_t)bead * Nc * Nb + b) * Nh;
     const size_t cstride = (size_t)Nb * Nh;
@@ -1368,6 +1425,15 @@ __global__ void __launch_bounds__(256, NF > 0 ? 2 : 1) conv_c_kernel(typename Cp
     }
 }
 
+template <typename R, int NF>
+__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1) conv_c_kernel(typename Cplx<R>::T *__restrict__ spec, const R *__restrict__ filt,
+                                                     int Na, int Nb, int Nc, const R *__restrict__ twc,
+                                                     const __grid_constant__ Cell cell, double alp,
+                                                     double *__restrict__ acc, int energy)
+{
+    conv_c_body<R, NF>(spec, filt, Na, Nb, Nc, twc, cell, alp, acc, energy, hw_blk());
+}
+
 // ---------------------------------------------------------------------------
 // Influence function on the full grid: preg * bweight for grid points whose
 // k (or -k) is on PINY's list, zero elsewhere.
@@ -1436,10 +1502,9 @@ static cudaError_t launch_fft_t(pinyb200_ctx *c, const PmeArgs &a, const Cell &c
     return cudaGetLastError();
 }
 
-template <typename R, int NI, int TT>
-static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
+// Kernel arguments of a context's PME mesh.
+static PmeArgs pme_args_of(pinyb200_ctx *c)
 {
-    typedef typename Cplx<R>::T C2;
     const DeviceSystem &s = c->sys;
     PmeArgs a;
     a.natm = s.natm;
@@ -1456,11 +1521,13 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     a.forceP = c->d_forceP;
     a.rhead = (int4 *)c->d_pme_head;
     a.rw = c->d_pme_w;
-    const size_t G = (size_t)a.Na * a.Nb * a.Nc;
-    const bool f64 = sizeof(R) == 8;
-    cudaError_t err = cudaMemsetAsync(c->d_grid, 0, sizeof(R) * G * c->P, c->stream);
-    if (err != cudaSuccess) return err;
-    if ((err = kt_mark(c, "pme_grid_clear (memset)")) != cudaSuccess) return err;
+    return a;
+}
+
+// Tile binning arguments of a context's PME mesh for spline order NI and
+// tile edge TT.
+static TileArgs tile_args_of(pinyb200_ctx *c, int NI, int TT)
+{
     TileArgs t;
     t.T = TT;
     // fixed-point scale of the FP32 spread tile: every contribution q M_a M_b
@@ -1484,6 +1551,20 @@ static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
     t.cnt = c->d_pme_cnt;
     t.bin = c->d_pme_bin;
     t.ovf = c->d_pme_ovf;
+    return t;
+}
+
+template <typename R, int NI, int TT>
+static cudaError_t launch_pme_t(pinyb200_ctx *c, const Cell &cell, bool energy)
+{
+    typedef typename Cplx<R>::T C2;
+    const PmeArgs a = pme_args_of(c);
+    const size_t G = (size_t)a.Na * a.Nb * a.Nc;
+    const bool f64 = sizeof(R) == 8;
+    cudaError_t err = cudaMemsetAsync(c->d_grid, 0, sizeof(R) * G * c->P, c->stream);
+    if (err != cudaSuccess) return err;
+    if ((err = kt_mark(c, "pme_grid_clear (memset)")) != cudaSuccess) return err;
+    const TileArgs t = tile_args_of(c, NI, TT);
     err = cudaMemsetAsync(t.cnt, 0, ((size_t)a.P * t.ntile + 1) * sizeof(int), c->stream);
     if (err != cudaSuccess) return err;
     const long long nt = (long long)a.nchrg * a.P;
@@ -1582,6 +1663,257 @@ cudaError_t launch_pme(pinyb200_ctx *c, const Cell &cell, bool energy)
     }
     if (c->precision == PINYB200_FP64) return launch_pme_r<double>(c, cell, energy);
     return launch_pme_r<float>(c, cell, energy);
+}
+
+// ---------------------------------------------------------------------------
+// Many boxes per launch (the batched evaluation): every forward PME kernel of
+// the compact FP32 path over a table of boxes, one persistent launch per
+// group of boxes that share the kernel's compile-time shape.
+
+struct PmeBox {
+    PmeArgs a;
+    TileArgs t;
+    Cell cell;
+};
+
+struct FftBox {
+    const void *q;      // real grid (forward input, inverse output)
+    void *spec;         // half spectrum
+    const void *filt;   // influence function (FP32)
+    const void *tw[3];  // twiddles per axis
+    int Na, Nb, Nc;
+    Cell cell;
+    double alp;
+    double *acc;
+    int energy;
+};
+
+struct AddBox {
+    int nchrg, P;
+    const int *ichrg;
+    const double *fP;
+    double *fT;
+};
+
+template <typename R, int NI>
+__global__ void __launch_bounds__(256) pme_bin_batch_kernel(const __grid_constant__ BoxTab<PmeBox> t)
+{
+    PINYB200_BOX_LOOP(t, i, vb, (pme_bin_compact_body<R, NI>(t.arg[i].a, t.arg[i].cell, t.arg[i].t, vb)));
+}
+
+template <typename R, int NI, int TT>
+__global__ void __launch_bounds__(256) spread_batch_kernel(const __grid_constant__ BoxTab<PmeBox> t)
+{
+    PINYB200_BOX_LOOP(t, i, vb, (spread_tile_c_body<R, NI, TT>(t.arg[i].a, t.arg[i].t, vb)));
+}
+
+template <typename R, int NI, int TT>
+__global__ void __launch_bounds__(256) gather_batch_kernel(const __grid_constant__ BoxTab<PmeBox> t)
+{
+    PINYB200_BOX_LOOP(t, i, vb, (gather_tile_c_body<R, NI, TT>(t.arg[i].a, t.arg[i].cell, t.arg[i].t, vb)));
+}
+
+template <typename R, int NF>
+__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1)
+    plane_fwd_batch_kernel(const __grid_constant__ BoxTab<FftBox> t)
+{
+    typedef typename Cplx<R>::T C2;
+    PINYB200_BOX_LOOP(t, i, vb,
+                      (plane_fwd_body<R, NF>((const R *)t.arg[i].q, (C2 *)t.arg[i].spec, t.arg[i].Na, t.arg[i].Nb,
+                                             t.arg[i].Nc, (const R *)t.arg[i].tw[0], (const R *)t.arg[i].tw[1], vb)));
+}
+
+template <typename R, int NF>
+__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1)
+    conv_c_batch_kernel(const __grid_constant__ BoxTab<FftBox> t)
+{
+    typedef typename Cplx<R>::T C2;
+    PINYB200_BOX_LOOP(t, i, vb,
+                      (conv_c_body<R, NF>((C2 *)t.arg[i].spec, (const R *)t.arg[i].filt, t.arg[i].Na, t.arg[i].Nb,
+                                          t.arg[i].Nc, (const R *)t.arg[i].tw[2], t.arg[i].cell, t.arg[i].alp,
+                                          t.arg[i].acc, t.arg[i].energy, vb)));
+}
+
+template <typename R, int NF>
+__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1)
+    plane_inv_batch_kernel(const __grid_constant__ BoxTab<FftBox> t)
+{
+    typedef typename Cplx<R>::T C2;
+    PINYB200_BOX_LOOP(t, i, vb,
+                      (plane_inv_body<R, NF>((const C2 *)t.arg[i].spec, (R *)t.arg[i].q, t.arg[i].Na, t.arg[i].Nb,
+                                             t.arg[i].Nc, (const R *)t.arg[i].tw[0], (const R *)t.arg[i].tw[1], vb)));
+}
+
+__global__ void __launch_bounds__(256) pme_force_add_batch_kernel(const __grid_constant__ BoxTab<AddBox> t)
+{
+    PINYB200_BOX_LOOP(t, i, vb,
+                      (pme_force_add_body(t.arg[i].nchrg, t.arg[i].P, t.arg[i].ichrg, t.arg[i].fP, t.arg[i].fT, vb)));
+}
+
+// stage 0 bin, 1 spread, 2 gather for the boxes of one (order, tile edge) group
+template <int NI, int TT>
+static cudaError_t pme_batch_tiles(const std::vector<PmeBox> &bx, const std::vector<int> &P, int sm_count,
+                                   cudaStream_t st, int stage)
+{
+    typedef float R;
+    BoxTabBuilder<PmeBox> tb;
+    for (size_t i = 0; i < bx.size(); i++) {
+        const double work = (double)bx[i].a.nchrg * P[i];
+        if (stage == 0) tb.add(bx[i], (int)(((long long)bx[i].a.nchrg * P[i] + 255) / 256), 1, work);
+        else tb.add(bx[i], bx[i].t.ntile, P[i], work);
+    }
+    if (stage == 0)
+        return launch_tables(tb, (const void *)pme_bin_batch_kernel<R, NI>, 256, 0, sm_count,
+                             [&](const BoxTab<PmeBox> &t, int g) { pme_bin_batch_kernel<R, NI><<<g, 256, 0, st>>>(t); });
+    if (stage == 1) {
+        const size_t ss = spread_smem<R, NI, TT>();
+        return launch_tables(tb, (const void *)spread_batch_kernel<R, NI, TT>, 256, ss, sm_count,
+                             [&](const BoxTab<PmeBox> &t, int g) { spread_batch_kernel<R, NI, TT><<<g, 256, ss, st>>>(t); });
+    }
+    const size_t sg = (size_t)TileGeom<NI, TT>::NPT * sizeof(R);
+    return launch_tables(tb, (const void *)gather_batch_kernel<R, NI, TT>, 256, sg, sm_count,
+                         [&](const BoxTab<PmeBox> &t, int g) { gather_batch_kernel<R, NI, TT><<<g, 256, sg, st>>>(t); });
+}
+
+template <int TT>
+static cudaError_t pme_batch_tiles_n(int NI, const std::vector<PmeBox> &bx, const std::vector<int> &P, int sm_count,
+                                     cudaStream_t st, int stage)
+{
+    switch (NI) {
+    case 4: return pme_batch_tiles<4, TT>(bx, P, sm_count, st, stage);
+    case 5: return pme_batch_tiles<5, TT>(bx, P, sm_count, st, stage);
+    case 6: return pme_batch_tiles<6, TT>(bx, P, sm_count, st, stage);
+    case 7: return pme_batch_tiles<7, TT>(bx, P, sm_count, st, stage);
+    case 8: return pme_batch_tiles<8, TT>(bx, P, sm_count, st, stage);
+    case 10: return pme_batch_tiles<10, TT>(bx, P, sm_count, st, stage);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// stage 0 forward plane FFT, 1 c-axis FFT with the convolution, 2 inverse
+// plane FFT for the boxes of one mesh
+template <int NF>
+static cudaError_t pme_batch_fft(const std::vector<FftBox> &bx, const std::vector<int> &P, int sm_count,
+                                 cudaStream_t st, int stage)
+{
+    typedef float R;
+    size_t sp = 0, ss = 0;
+    BoxTabBuilder<FftBox> tb;
+    for (size_t i = 0; i < bx.size(); i++) {
+        sp = std::max(sp, pme_plane_smem(bx[i].Na, bx[i].Nb, false));
+        ss = std::max(ss, pme_slab_smem(bx[i].Na, bx[i].Nc, false));
+        const double work = (double)bx[i].Na * bx[i].Nb * bx[i].Nc * P[i];
+        tb.add(bx[i], P[i] * (stage == 1 ? bx[i].Nb : bx[i].Nc), 1, work);
+    }
+    if (stage == 0)
+        return launch_tables(tb, (const void *)plane_fwd_batch_kernel<R, NF>, 256, sp, sm_count,
+                             [&](const BoxTab<FftBox> &t, int g) { plane_fwd_batch_kernel<R, NF><<<g, 256, sp, st>>>(t); });
+    if (stage == 1)
+        return launch_tables(tb, (const void *)conv_c_batch_kernel<R, NF>, 256, ss, sm_count,
+                             [&](const BoxTab<FftBox> &t, int g) { conv_c_batch_kernel<R, NF><<<g, 256, ss, st>>>(t); });
+    return launch_tables(tb, (const void *)plane_inv_batch_kernel<R, NF>, 256, sp, sm_count,
+                         [&](const BoxTab<FftBox> &t, int g) { plane_inv_batch_kernel<R, NF><<<g, 256, sp, st>>>(t); });
+}
+
+static cudaError_t pme_batch_tiles_group(const std::pair<int, int> &key, const std::vector<PmeBox> &bx,
+                                         const std::vector<int> &P, int sm_count, cudaStream_t st, int stage)
+{
+    return key.second == 8 ? pme_batch_tiles_n<8>(key.first, bx, P, sm_count, st, stage)
+                           : pme_batch_tiles_n<16>(key.first, bx, P, sm_count, st, stage);
+}
+
+// Forward PME of many MIXED contexts on stream st, as launch_pme does for
+// one: grids and bin counters cleared, charges binned, spread, transformed,
+// convolved (energies and virials into each context's per-bead sums when
+// `energy`), transformed back and gathered into each context's PME forces.
+// The contexts' meshes use the compact records (pme_full_records off).
+cudaError_t launch_pme_batch(const std::vector<pinyb200_ctx *> &box, const std::vector<Cell> &cells, bool energy,
+                             int sm_count, cudaStream_t st)
+{
+    // groups: tiles by (order, tile edge), FFTs by mesh
+    std::map<std::pair<int, int>, std::pair<std::vector<PmeBox>, std::vector<int>>> tiles;
+    std::map<std::tuple<int, int, int>, std::pair<std::vector<FftBox>, std::vector<int>>> ffts;
+    std::vector<std::pair<void *, size_t>> zero;
+    for (size_t i = 0; i < box.size(); i++) {
+        pinyb200_ctx *c = box[i];
+        if (c->sys.nchrg == 0 || c->sys.nktot == 0) continue;
+        if (c->precision != PINYB200_MIXED || c->pme_full_records) return cudaErrorInvalidValue;
+        const Cell &cell = cells[i];
+        const size_t G = (size_t)c->sys.ngrid[0] * c->sys.ngrid[1] * c->sys.ngrid[2];
+        bool same = c->filter_ok;
+        for (int k = 0; k < 9 && same; k++) same = c->filter_h[k] == cell.h[k];
+        if (!same) {
+            // the influence function of this cell (normally built by the plain run before capture)
+            filter_kernel<<<(unsigned)((G + 255) / 256), 256, 0, st>>>(
+                c->sys.ngrid[0], c->sys.ngrid[1], c->sys.ngrid[2], c->sys.kmask, c->sys.kvec, c->sys.bweight, cell,
+                c->alp_ewd, (double *)c->d_filter, (float *)((double *)c->d_filter + G));
+            for (int k = 0; k < 9; k++) c->filter_h[k] = cell.h[k];
+            c->filter_ok = true;
+        }
+        PmeBox pb;
+        pb.a = pme_args_of(c);
+        pb.t = tile_args_of(c, c->sys.n_interp, c->pme_tile);
+        pb.cell = cell;
+        auto &tg = tiles[std::make_pair(c->sys.n_interp, c->pme_tile)];
+        tg.first.push_back(pb);
+        tg.second.push_back(c->P);
+        FftBox fb;
+        fb.q = c->d_grid;
+        fb.spec = c->d_spec;
+        fb.filt = (const void *)((const double *)c->d_filter + G);
+        fb.tw[0] = c->d_twiddle32;
+        fb.tw[1] = c->d_twiddle32 + 2 * 256;
+        fb.tw[2] = c->d_twiddle32 + 4 * 256;
+        fb.Na = c->sys.ngrid[0];
+        fb.Nb = c->sys.ngrid[1];
+        fb.Nc = c->sys.ngrid[2];
+        fb.cell = cell;
+        fb.alp = c->alp_ewd;
+        fb.acc = c->d_acc;
+        fb.energy = energy ? 1 : 0;
+        auto &fg = ffts[std::make_tuple(fb.Na, fb.Nb, fb.Nc)];
+        fg.first.push_back(fb);
+        fg.second.push_back(c->P);
+        zero.emplace_back(c->d_grid, sizeof(float) * G * c->P);
+        zero.emplace_back(c->d_pme_cnt, ((size_t)c->P * c->pme_ntile + 1) * sizeof(int));
+    }
+    cudaError_t err = launch_zero_batch(zero, sm_count, st);
+    for (int stage = 0; stage < 2 && err == cudaSuccess; stage++)
+        for (auto &kv : tiles) {
+            err = pme_batch_tiles_group(kv.first, kv.second.first, kv.second.second, sm_count, st, stage);
+            if (err != cudaSuccess) break;
+        }
+    for (int stage = 0; stage < 3 && err == cudaSuccess; stage++)
+        for (auto &kv : ffts) {
+            const int Na = std::get<0>(kv.first), Nb = std::get<1>(kv.first), Nc = std::get<2>(kv.first);
+            switch (Na == Nb && Na == Nc ? Na : 0) {
+            case 16: err = pme_batch_fft<16>(kv.second.first, kv.second.second, sm_count, st, stage); break;
+            case 32: err = pme_batch_fft<32>(kv.second.first, kv.second.second, sm_count, st, stage); break;
+            case 64: err = pme_batch_fft<64>(kv.second.first, kv.second.second, sm_count, st, stage); break;
+            case 128: err = pme_batch_fft<128>(kv.second.first, kv.second.second, sm_count, st, stage); break;
+            default: err = pme_batch_fft<0>(kv.second.first, kv.second.second, sm_count, st, stage); break;
+            }
+            if (err != cudaSuccess) break;
+        }
+    for (auto &kv : tiles) {
+        if (err != cudaSuccess) break;
+        err = pme_batch_tiles_group(kv.first, kv.second.first, kv.second.second, sm_count, st, 2);
+    }
+    return err;
+}
+
+// PME forces of many contexts added to their site forces.
+cudaError_t launch_pme_force_add_batch(const std::vector<pinyb200_ctx *> &box, int sm_count, cudaStream_t st)
+{
+    BoxTabBuilder<AddBox> tb;
+    for (pinyb200_ctx *c : box) {
+        if (c->sys.nchrg == 0 || c->sys.nktot == 0) continue;
+        const long long n = (long long)c->sys.nchrg * 3 * c->P;
+        tb.add(AddBox{c->sys.nchrg, c->P, c->sys.ichrg, c->d_forceP, c->d_forceT}, (int)((n + 255) / 256), 1,
+               (double)n);
+    }
+    return launch_tables(tb, (const void *)pme_force_add_batch_kernel, 256, 0, sm_count,
+                         [&](const BoxTab<AddBox> &t, int g) { pme_force_add_batch_kernel<<<g, 256, 0, st>>>(t); });
 }
 
 }  // namespace pinyb200

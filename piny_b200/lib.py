@@ -25,6 +25,7 @@ NO_ENERGY = 2
 SITE_PAIRS = 4
 TUNE_AGAIN = 8
 UPDATE_LIST = 16       # PINYB200_UPDATE_LIST
+BATCH_BRANCHES = 32    # PINYB200_BATCH_BRANCHES
 
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NO_DEVICE", 4: "ERR_LIST_OVERFLOW", 5: "ERR_CUTOFF",
           6: "ERR_TIMEOUT", 7: "ERR_NAN", 8: "ERR_UNSUPPORTED", 9: "ERR_STATE"}
@@ -109,7 +110,7 @@ EXPORTS = ("pinyb200_version", "pinyb200_device_info", "pinyb200_create", "pinyb
            "pinyb200_last_error", "pinyb200_count_list_device", "pinyb200_check_list_device",
            "pinyb200_autotune", "pinyb200_get_tuning", "pinyb200_set_tuning", "pinyb200_batch_create",
            "pinyb200_batch_destroy", "pinyb200_batch_energy_force_device", "pinyb200_batch_last_ms",
-           "pinyb200_batch_last_error", "pinyb200_grad_prepare", "pinyb200_grad",
+           "pinyb200_batch_last_error", "pinyb200_batch_last_mode", "pinyb200_grad_prepare", "pinyb200_grad",
            "pinyb200_fma_peak", "pinyb200_pimd_transform", "pinyb200_pimd_create", "pinyb200_pimd_destroy",
            "pinyb200_pimd_set_nhc", "pinyb200_pimd_get_nhc", "pinyb200_pimd_forces", "pinyb200_pimd_step",
            "pinyb200_update_list_device", "pinyb200_list_set_spread", "pinyb200_list_status",
@@ -172,6 +173,7 @@ def load(build_if_missing: bool = True):
                                                      C.POINTER(_pd), _i, C.POINTER(C.c_void_p),
                                                      C.POINTER(PinyEnergies), C.c_void_p]
     L.pinyb200_batch_last_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
+    L.pinyb200_batch_last_mode.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.pinyb200_batch_last_error.restype = C.c_char_p
     L.pinyb200_batch_last_error.argtypes = [C.c_void_p]
     L.pinyb200_grad_prepare.argtypes = [C.c_void_p, _i, C.POINTER(PinyTangent)]
@@ -522,7 +524,10 @@ class DeviceBatch:
                                                               self.L.pinyb200_last_error(None).decode()))
         self.h = h
 
-    def energy_force_device(self, d_pos, d_xmod, hmats, d_force, stream=None, energy=True, update_list=False):
+    def energy_force_device(self, d_pos, d_xmod, hmats, d_force, stream=None, energy=True, update_list=False,
+                            branches=False, distribute_ghosts=False):
+        """Every box in one graph launch: the multi-box kernels where they
+        cover the boxes, else (or with branches=True) one graph branch per box."""
         n = len(self.boxes)
         P = (C.c_void_p * n)(*[int(p) for p in d_pos])
         X = (C.c_void_p * n)(*[None if x is None else int(x) for x in d_xmod]) if d_xmod is not None else None
@@ -530,7 +535,8 @@ class DeviceBatch:
         hm = [np.ascontiguousarray(h, np.float64) for h in hmats]
         H = (_pd * n)(*[_dp(h) for h in hm])
         E = (PinyEnergies * n)()
-        flags = (0 if energy else NO_ENERGY) | (UPDATE_LIST if update_list else 0)
+        flags = (0 if energy else NO_ENERGY) | (UPDATE_LIST if update_list else 0) | \
+            (BATCH_BRANCHES if branches else 0) | (DISTRIB_GHOSTS if distribute_ghosts else 0)
         rc = self.L.pinyb200_batch_energy_force_device(self.h, P, X, H, flags, F, E,
                                                        None if stream is None else C.c_void_p(stream))
         if rc != 0:
@@ -542,6 +548,12 @@ class DeviceBatch:
         ms = C.c_float()
         self.L.pinyb200_batch_last_ms(self.h, C.byref(ms))
         return ms.value
+
+    def last_mode(self):
+        """(fused, kernel launches) of the graph the last call ran."""
+        f, k = C.c_int(), C.c_int()
+        self.L.pinyb200_batch_last_mode(self.h, C.byref(f), C.byref(k))
+        return bool(f.value), int(k.value)
 
     def close(self):
         if getattr(self, "h", None):

@@ -208,3 +208,60 @@ def test_mixed_pair_kernels_agree_with_fp64():
             scale = abs(e0["vvdw"]) + abs(e0["vcoul"]) + abs(e0["vrecip"]) + abs(e0["vself"])
             assert abs(e["vintert"] - e0["vintert"]) <= 1e-6 * scale
             b.close()
+
+
+@pytest.mark.parametrize("flags", [{}, {"energy": False}, {"distribute_ghosts": True}])
+def test_batch_kernels_match_branches(flags):
+    """The multi-box kernels (one persistent launch per phase and shape
+    group) and one graph branch per box give the same MIXED forces (1e-5
+    relative RMS of each box, and against the FP64 one-box path) and
+    energies; the multi-box graph holds a few dozen launches, not one set per
+    box.  Boxes of 1-64 beads on 16^3 and 32^3 meshes, so that several bead
+    groups, tile edges and FFT lengths share a call."""
+    import torch
+
+    from piny_b200.lib import DeviceBatch, DeviceBox
+    boxes = _boxes(nbox=12, seed=33)
+    ctxs, d_pos, d_xm, hm, keep = [], [], [], [], []
+    for sp, pos, S in boxes:
+        b = DeviceBox(S, sp.nbeads, "mixed")
+        xmod = pos.mean(axis=0) if sp.nbeads > 1 else None
+        b.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+        d = torch.from_numpy(pos).to("cuda:0")
+        dx = torch.from_numpy(xmod).to("cuda:0") if xmod is not None else None
+        keep += [d, dx]
+        ctxs.append(b)
+        d_pos.append(d.data_ptr())
+        d_xm.append(None if dx is None else dx.data_ptr())
+        hm.append(S["hmat"])
+    f_fused = [torch.zeros_like(keep[2 * i]) for i in range(len(boxes))]
+    f_branch = [torch.zeros_like(keep[2 * i]) for i in range(len(boxes))]
+    batch = DeviceBatch(ctxs)
+    energy = flags.get("energy", True)
+    ghosts = flags.get("distribute_ghosts", False)
+    for call in range(2):
+        ef = batch.energy_force_device(d_pos, d_xm, hm, [f.data_ptr() for f in f_fused], energy=energy,
+                                       distribute_ghosts=ghosts)
+        fused, nk = batch.last_mode()
+        assert fused and 0 < nk <= 48, (fused, nk)
+        eb = batch.energy_force_device(d_pos, d_xm, hm, [f.data_ptr() for f in f_branch], energy=energy,
+                                       distribute_ghosts=ghosts, branches=True)
+        fused_b, nkb = batch.last_mode()
+        assert not fused_b and nkb > 4 * len(boxes)
+        torch.cuda.synchronize()
+        for i, (sp, pos, S) in enumerate(boxes):
+            a, b = f_fused[i].cpu().numpy(), f_branch[i].cpu().numpy()
+            assert rel_rms(a, b) < 1e-5, (call, i)
+            if energy:
+                scale = abs(eb[i]["vvdw"]) + abs(eb[i]["vcoul"]) + abs(eb[i]["vrecip"]) + abs(eb[i]["vself"])
+                assert abs(ef[i]["vintert"] - eb[i]["vintert"]) <= 1e-6 * scale, i
+                assert abs(ef[i]["vintrat"] - eb[i]["vintrat"]) <= 1e-9 * max(1.0, abs(eb[i]["vintrat"])), i
+                assert np.allclose(ef[i]["pvten"], eb[i]["pvten"], rtol=1e-5, atol=1e-6 * scale)
+    if not ghosts:
+        for i, (sp, pos, S) in enumerate(boxes[:3]):
+            b0, f0, _ = _single(S, pos, sp.nbeads, "fp64")
+            b0.close()
+            assert rel_rms(f_fused[i].cpu().numpy(), f0) < 1e-5, i
+    batch.close()
+    for b in ctxs:
+        b.close()
