@@ -439,9 +439,9 @@ int pinyb200_set_tuning(pinyb200_ctx *ctx, const int *choice);
  * (staging, PME bin / spread / three FFT passes / gather, pair forces,
  * intramolecular terms, finishing) is one persistent launch per group of
  * boxes sharing its compile-time shape, walking every (box, bead, tile or
- * chunk) block of the group, with PME on a second branch beside the pair
- * and intramolecular launches.  Otherwise every box is a parallel branch of
- * its own kernels.  The call returns when the work is done.  PINY's Python
+ * chunk) block of the group; the groups' PME chains, pair launches and the
+ * intramolecular launch are parallel branches of the graph.  Otherwise
+ * every box is a parallel branch of its own kernels.  The call returns when the work is done.  PINY's Python
  * driver reaches several replicas through one energy_control call per CLASS
  * (python/piny/piny.pyx:426-436); this entry point has no counterpart there.
  */

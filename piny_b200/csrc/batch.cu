@@ -5,9 +5,10 @@
 // positions in, list-based pair forces, PME, intramolecular terms, forces
 // out, energy sums to pinned host memory -- in one of two forms:
 //   multi-box kernels: each phase is one persistent launch per group of
-//     boxes that share its compile-time shape (boxtab.cuh), PME on a second
-//     branch beside the pair and intramolecular launches -- a few dozen
-//     launches for any number of boxes;
+//     boxes that share its compile-time shape (boxtab.cuh); the groups'
+//     PME chains, pair launches and the intramolecular launch are parallel
+//     graph branches between the staging and the finishing launches -- a
+//     few dozen launches for any number of boxes;
 //   branches: every box's own kernels as a parallel branch forked from and
 //     joined to one stream (for boxes the multi-box kernels do not cover).
 // The first call (and any call whose device pointers, cells or flags differ
@@ -19,6 +20,7 @@
 // (molecule-pair or site-list), pair grid size (blocks per SM) and PME
 // overlap with the pair kernel -- keeps the fastest, and remembers it per
 // system shape for the rest of the process.
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <string>
@@ -85,9 +87,11 @@ struct pinyb200_batch {
     int key_flags = -1;
     float last_ms = 0;
     cudaEvent_t ev[2] = {nullptr, nullptr};
-    // the multi-box form: PME branch and its fork/join events
-    cudaStream_t pme_stream = nullptr;
-    cudaEvent_t pfork = nullptr, pjoin = nullptr;
+    // the multi-box form: one graph branch per shape group (streams reused
+    // round-robin past the pool), a join event per branch
+    std::vector<cudaStream_t> gstream;
+    std::vector<cudaEvent_t> gjoin;
+    cudaEvent_t pfork = nullptr;
     int fused = 0;     // form of the captured graph
     int launches = 0;  // kernel nodes of the captured graph
     std::string err;
@@ -158,14 +162,61 @@ int fused_enqueue(pinyb200_batch *bt, const double *const *d_pos, const double *
     if (e == cudaSuccess) e = launch_transpose_in_batch(bt->box, pos, sm, st);
     if (e == cudaSuccess && !xm.empty()) e = launch_copy_batch(xm, sm, st);
     if (e == cudaSuccess) e = launch_ghost_batch(bt->box, false, sm, st);
-    // PME beside the pair and intramolecular kernels
+    // The force terms as parallel branches: one per PME shape group (order,
+    // tile edge, mesh: its whole chain of launches), one per pair-kernel
+    // group (bead count, site pattern), one for the intramolecular terms;
+    // heaviest first.  Independent groups overlap, so no launch's tail
+    // leaves the GPU idle while other groups still have work.
+    struct Branch {
+        int kind;  // 0 PME, 1 pair, 2 intramolecular
+        std::vector<pinyb200_ctx *> box;
+        std::vector<Cell> cell;
+        double work;
+    };
+    std::map<std::tuple<int, int, int, int, int, int>, Branch> groups;
+    for (int i = 0; i < nbox; i++) {
+        pinyb200_ctx *c = bt->box[i];
+        const double G = (double)c->sys.ngrid[0] * c->sys.ngrid[1] * c->sys.ngrid[2];
+        if (c->sys.nchrg > 0 && c->sys.nktot > 0) {
+            Branch &b = groups[std::make_tuple(0, c->sys.n_interp, c->pme_tile, c->sys.ngrid[0], c->sys.ngrid[1],
+                                               c->sys.ngrid[2])];
+            b.kind = 0;
+            b.box.push_back(c);
+            b.cell.push_back(cells[i]);
+            b.work += (G + 40.0 * c->sys.nchrg) * c->P;
+        }
+        Branch &q = groups[std::make_tuple(1, c->P, mix_pattern(c), 0, 0, 0)];
+        q.kind = 1;
+        q.box.push_back(c);
+        q.cell.push_back(cells[i]);
+        q.work += 300.0 * c->chunk_cap * c->P;
+    }
+    std::vector<Branch> br;
+    for (auto &kv : groups) br.push_back(kv.second);
+    br.push_back(Branch{2, bt->box, cells, 0.0});
+    std::stable_sort(br.begin(), br.end(), [](const Branch &x, const Branch &y) { return x.work > y.work; });
+    const size_t npool = 12;
+    while (e == cudaSuccess && bt->gstream.size() < std::min(npool, br.size())) {
+        cudaStream_t s = nullptr;
+        e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        if (e == cudaSuccess) bt->gstream.push_back(s);
+    }
+    while (e == cudaSuccess && bt->gjoin.size() < br.size()) {
+        cudaEvent_t ev = nullptr;
+        e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) bt->gjoin.push_back(ev);
+    }
     if (e == cudaSuccess) e = cudaEventRecord(bt->pfork, st);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(bt->pme_stream, bt->pfork, 0);
-    if (e == cudaSuccess) e = launch_pme_batch(bt->box, cells, energy, sm, bt->pme_stream);
-    if (e == cudaSuccess) e = cudaEventRecord(bt->pjoin, bt->pme_stream);
-    if (e == cudaSuccess) e = launch_mol_pair_mixed_batch(bt->box, cells, energy, sm, st);
-    if (e == cudaSuccess) e = launch_intra_batch(bt->box, energy, sm, st);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, bt->pjoin, 0);
+    for (size_t k = 0; k < br.size() && e == cudaSuccess; k++) {
+        cudaStream_t s = bt->gstream[k % bt->gstream.size()];
+        e = cudaStreamWaitEvent(s, bt->pfork, 0);
+        if (e != cudaSuccess) break;
+        if (br[k].kind == 0) e = launch_pme_batch(br[k].box, br[k].cell, energy, sm, s);
+        else if (br[k].kind == 1) e = launch_mol_pair_mixed_batch(br[k].box, br[k].cell, energy, sm, s);
+        else e = launch_intra_batch(br[k].box, energy, sm, s);
+        if (e == cudaSuccess) e = cudaEventRecord(bt->gjoin[k], s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, bt->gjoin[k], 0);
+    }
     if (e == cudaSuccess) e = launch_pme_force_add_batch(bt->box, sm, st);
     if (e == cudaSuccess && (flags & PINYB200_DISTRIB_GHOSTS)) e = launch_ghost_batch(bt->box, true, sm, st);
     if (e == cudaSuccess) e = launch_transpose_out_batch(bt->box, force, sm, st);
@@ -302,9 +353,7 @@ int pinyb200_batch_create(pinyb200_ctx *const *ctx, int nbox, pinyb200_batch **o
     };
     if (cudaSetDevice(bt->device) != cudaSuccess) return cleanup(bfail(nullptr, PINYB200_ERR_CUDA, "batch: device"));
     if (cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&bt->pme_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&bt->pfork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&bt->pjoin, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&bt->fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreate(&bt->ev[0]) != cudaSuccess || cudaEventCreate(&bt->ev[1]) != cudaSuccess)
         return cleanup(bfail(nullptr, PINYB200_ERR_CUDA, "batch: stream/event creation failed"));
@@ -331,8 +380,8 @@ int pinyb200_batch_destroy(pinyb200_batch *bt)
         if (e) cudaEventDestroy(e);
     if (bt->fork) cudaEventDestroy(bt->fork);
     if (bt->pfork) cudaEventDestroy(bt->pfork);
-    if (bt->pjoin) cudaEventDestroy(bt->pjoin);
-    if (bt->pme_stream) cudaStreamDestroy(bt->pme_stream);
+    for (cudaEvent_t e : bt->gjoin) cudaEventDestroy(e);
+    for (cudaStream_t s : bt->gstream) cudaStreamDestroy(s);
     for (int i = 0; i < 2; i++)
         if (bt->ev[i]) cudaEventDestroy(bt->ev[i]);
     if (bt->stream) cudaStreamDestroy(bt->stream);

@@ -1238,11 +1238,14 @@ __device__ __forceinline__ void line_fft(typename Cplx<R>::T *sm, int N, int nl,
     }
 }
 
-// Resident blocks per SM the plane and slab kernels of compile-time length
-// are compiled for (their registers: 256 threads x 128 / this).
+// Resident blocks per SM the FP32 plane and slab kernels of compile-time
+// length are compiled for (their registers: 65536 / (256 x this)); the
+// FP64 ones and the multi-box ones (whose run-time argument table costs
+// registers) hold 2.
 #ifndef PINYB200_FFT_BLOCKS
 #define PINYB200_FFT_BLOCKS 2
 #endif
+#define PINYB200_FFT_LB(R, NF) (NF > 0 ? (sizeof(R) == 4 ? PINYB200_FFT_BLOCKS : 2) : 1)
 
 template <typename R>
 __device__ __forceinline__ void load_twiddles(R *dst, const R *src, int N)
@@ -1284,7 +1287,7 @@ __device__ __forceinline__ void plane_fwd_body(const R *__restrict__ q, typename
 }
 
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1) plane_fwd_kernel(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
+__global__ void __launch_bounds__(256, PINYB200_FFT_LB(R, NF)) plane_fwd_kernel(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
                                                         int Na, int Nb, int Nc, const R *__restrict__ twa,
                                                         const R *__restrict__ twb)
 {
@@ -1330,7 +1333,7 @@ __device__ __forceinline__ void plane_inv_body(const typename Cplx<R>::T *__rest
 }
 
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1) plane_inv_kernel(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phi,
+__global__ void __launch_bounds__(256, PINYB200_FFT_LB(R, NF)) plane_inv_kernel(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phi,
                                                         int Na, int Nb, int Nc, const R *__restrict__ twa,
                                                         const R *__restrict__ twb)
 {
@@ -1426,7 +1429,7 @@ __device__ __forceinline__ void conv_c_body(typename Cplx<R>::T *__restrict__ sp
 }
 
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1) conv_c_kernel(typename Cplx<R>::T *__restrict__ spec, const R *__restrict__ filt,
+__global__ void __launch_bounds__(256, PINYB200_FFT_LB(R, NF)) conv_c_kernel(typename Cplx<R>::T *__restrict__ spec, const R *__restrict__ filt,
                                                      int Na, int Nb, int Nc, const R *__restrict__ twc,
                                                      const __grid_constant__ Cell cell, double alp,
                                                      double *__restrict__ acc, int energy)
@@ -1714,7 +1717,7 @@ __global__ void __launch_bounds__(256) gather_batch_kernel(const __grid_constant
 }
 
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1)
+__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1)
     plane_fwd_batch_kernel(const __grid_constant__ BoxTab<FftBox> t)
 {
     typedef typename Cplx<R>::T C2;
@@ -1724,7 +1727,7 @@ __global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1)
 }
 
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1)
+__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1)
     conv_c_batch_kernel(const __grid_constant__ BoxTab<FftBox> t)
 {
     typedef typename Cplx<R>::T C2;
@@ -1735,7 +1738,7 @@ __global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1)
 }
 
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_FFT_BLOCKS : 1)
+__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1)
     plane_inv_batch_kernel(const __grid_constant__ BoxTab<FftBox> t)
 {
     typedef typename Cplx<R>::T C2;
