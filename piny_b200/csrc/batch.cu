@@ -162,6 +162,7 @@ int fused_enqueue(pinyb200_batch *bt, const double *const *d_pos, const double *
     if (e == cudaSuccess) e = launch_transpose_in_batch(bt->box, pos, sm, st);
     if (e == cudaSuccess && !xm.empty()) e = launch_copy_batch(xm, sm, st);
     if (e == cudaSuccess) e = launch_ghost_batch(bt->box, false, sm, st);
+    if (e == cudaSuccess) e = launch_mol_extent_batch(bt->box, sm, st);
     // The force terms as parallel branches: one per PME shape group (order,
     // tile edge, mesh: its whole chain of launches), one per pair-kernel
     // group (bead count, site pattern), one for the intramolecular terms;

@@ -838,6 +838,9 @@ int pinyb200::evaluate_enqueue(pinyb200_ctx *c, const Cell &cell, int flags, boo
     CK(kt_mark(c, "ghost_pos"));
     CK(cudaMemsetAsync(c->d_forceT, 0, nb * sizeof(double), c->stream));
     CK(cudaMemsetAsync(c->d_acc, 0, (size_t)c->P * S_NSLOT * sizeof(double), c->stream));
+    // the molecule extent bound the pair kernels' image test uses
+    CK(launch_mol_extent(c));
+    CK(kt_mark(c, "mol_extent"));
     if (timing) CK(ev_rec(c->ev[1], c->stream));
     // PME on its own stream, concurrently with the pair and intramolecular
     // kernels: it reads the positions, writes its own force buffer and adds

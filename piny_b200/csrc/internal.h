@@ -23,6 +23,7 @@ enum Slot {
     S_VBOND,
     S_VBEND,
     S_PXX, S_PYY, S_PZZ, S_PXY, S_PXZ, S_PYZ,  // bead pressure tensor
+    S_EXT = 15,   // bead 0 only: molecule extent bound of the evaluation (bits of a double >= 0)
     S_NSLOT = 16
 };
 
@@ -430,6 +431,8 @@ namespace pinyb200 {
 // Batched launches over many boxes: one persistent kernel per group of
 // boxes that share a kernel's compile-time shape (boxtab.cuh).
 int mix_pattern(const pinyb200_ctx *c);
+cudaError_t launch_mol_extent(pinyb200_ctx *c);
+cudaError_t launch_mol_extent_batch(const std::vector<pinyb200_ctx *> &box, int sm_count, cudaStream_t st);
 cudaError_t launch_mol_pair_mixed_batch(const std::vector<pinyb200_ctx *> &box, const std::vector<Cell> &cells,
                                         bool energy, int sm_count, cudaStream_t st);
 cudaError_t launch_pme_batch(const std::vector<pinyb200_ctx *> &box, const std::vector<Cell> &cells, bool energy,

@@ -767,6 +767,7 @@ struct MolArgs {
     const int *mstart;
     int ntyp, npt, nuniq, nsplin;
     const double *posT, *xmod;  // xmod: [natm][3] (bead positions when P == 1)
+    const unsigned long long *ext;  // extent bound of the evaluation (mol_extent_kernel), or nullptr
     int pimd;
     const int *atm_typ;
     const double *charge;
@@ -795,11 +796,45 @@ struct PairConst {
 // diagonal of an orthorhombic cell (period_pimd, period.c:163-176).
 __device__ __forceinline__ double shift_exact(double dm, double hi) { return -nint_rn(__dmul_rn(dm, hi)); }
 
-// Sites of a molecule sit within this distance (Bohr) of its site 0 in the
-// mode-1 coordinates; a site pair can take a different image than the
-// site-0 pair only when the site-0 separation is within twice this of half
-// a box, and only then is its own shift evaluated.
+// A site pair of a molecule pair can take a different image than the
+// site-0 pair only when the site-0 separation (mode-1 coordinates) is
+// within twice the molecular extent of half a box along some axis, and only
+// then is its own shift evaluated.  The extent is measured on the device
+// every evaluation (mol_extent_kernel: the largest |x_s - x_s0| over sites,
+// molecules and axes); this fixed bound (Bohr) serves kernels given none.
 #define PINYB200_MOL_EXTENT 5.0
+
+// Twice the extent bound of this evaluation, with a margin for the
+// rounding of the separations the image tests compare.
+__device__ __forceinline__ double ext2_of(const unsigned long long *ext)
+{
+    if (!ext) return 2.0 * PINYB200_MOL_EXTENT;
+    const double e = fmax(__longlong_as_double((long long)__ldcg(ext)), 0.0);
+    return 2.0 * (e * (1.0 + 1e-6) + 1e-9);
+}
+
+// The extent of every molecule: max |x_s - x_s0| over its sites s and the
+// three axes of the mode-1 positions xm [natm][3], as an atomic maximum of
+// the bit pattern (non-negative doubles order as integers).
+__device__ __forceinline__ void mol_extent_body(const int *__restrict__ mstart, int nmol, const double *__restrict__ xm,
+                                                unsigned long long *out, const VBlk vb)
+{
+    double e = 0.0;
+    for (int m = vb.x * (int)blockDim.x + (int)threadIdx.x; m < nmol; m += vb.gx * (int)blockDim.x) {
+        const int s0 = mstart[m], s1 = mstart[m + 1];
+        for (int s = s0 + 1; s < s1; s++)
+            for (int d = 0; d < 3; d++) e = fmax(e, fabs(xm[3 * (size_t)s + d] - xm[3 * (size_t)s0 + d]));
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+    if ((threadIdx.x & 31) == 0 && e > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(e));
+}
+
+__global__ void __launch_bounds__(256) mol_extent_kernel(const int *__restrict__ mstart, int nmol,
+                                                         const double *__restrict__ xm, unsigned long long *out)
+{
+    mol_extent_body(mstart, nmol, xm, out, hw_blk());
+}
 
 // Resident blocks of 128 threads per SM the register allocation aims at.
 #ifndef PINYB200_MOL_BLOCKS32
@@ -964,6 +999,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
     const int nsm2 = a.nsplin - 2;
     const double *__restrict__ posT = a.posT;
 
+    const double ext2 = ext2_of(a.ext);  // image test margin of this evaluation
     const int nch = *a.nchunk;
     for (int ch = warp; ch < nch; ch += nwarps) {
         const int mi = a.chunk[3 * ch], beg = a.chunk[3 * ch + 1], end = a.chunk[3 * ch + 2];
@@ -1014,7 +1050,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? PINYB200_MOL_BLOCKS32 : 
                     const double hid = cell.hi[4 * d];
                     const double t = __dmul_rn(dm[d], hid);
                     sh0[d] = -nint_rn(t);
-                    near |= fabs(t + sh0[d]) > 0.5 - 2.0 * PINYB200_MOL_EXTENT * hid;
+                    near |= fabs(t + sh0[d]) > 0.5 - ext2 * hid;
                 }
             }
             if (near) {
@@ -1171,6 +1207,7 @@ struct MixArgs {
     const int *mstart;
     int ntyp, nuniq, nsplin, stride;
     const double *posT, *xmod;
+    const unsigned long long *ext;  // extent bound of the evaluation (mol_extent_kernel), or nullptr
     const int *atm_typ;
     const double *charge;
     const int *inter_map;
@@ -1241,6 +1278,7 @@ __device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell
     const float rc2 = a.rc2, dri = a.dri_f, rmd = a.rmd, tmax = a.tmax;
     constexpr float kRound = 12582912.0f;  // 1.5 * 2^23: x + kRound - kRound = nearest integer of x
 
+    const double ext2 = ext2_of(a.ext);  // image test margin of this evaluation
     const int nch = *a.nchunk;
     for (int ch = warp; ch < nch; ch += nwarps) {
         const int mi = a.chunk[3 * ch], beg = a.chunk[3 * ch + 1], end = a.chunk[3 * ch + 2];
@@ -1269,7 +1307,7 @@ __device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell
                 const double hid = cell.hi[4 * d];
                 const double t = __dmul_rn(__dsub_rn(a.xmod[3 * (size_t)i0 + d], __ldcg(a.xmod + 3 * (size_t)j0 + d)), hid);
                 sh0[d] = -nint_rn(t);
-                near |= fabs(t + sh0[d]) > 0.5 - 2.0 * PINYB200_MOL_EXTENT * hid;
+                near |= fabs(t + sh0[d]) > 0.5 - ext2 * hid;
             }
             if (near) {
                 mol_pair_near<float, P, NS, true, ENERGY>(posT, a.xmod, a.forceT, &pc, a.tab,
@@ -1693,6 +1731,7 @@ cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy)
     a.posT = c->d_posT;
     a.pimd = c->P > 1;
     a.xmod = c->P > 1 ? c->d_xmod : c->d_posT;  // P == 1: [natm][3][1] is [natm][3]
+    a.ext = (const unsigned long long *)(c->d_acc + S_EXT);
     a.atm_typ = s.atm_typ;
     a.charge = s.charge;
     a.inter_map = s.inter_map;
@@ -1784,6 +1823,7 @@ static MixArgs mix_args(pinyb200_ctx *c)
     a.stride = c->mol_stride;
     a.posT = c->d_posT;
     a.xmod = c->P > 1 ? c->d_xmod : c->d_posT;
+    a.ext = (const unsigned long long *)(c->d_acc + S_EXT);
     a.atm_typ = s.atm_typ;
     a.charge = s.charge;
     a.inter_map = s.inter_map;
@@ -1814,6 +1854,42 @@ cudaError_t launch_mol_pair_mixed(pinyb200_ctx *c, const Cell &cell, bool energy
     const MixArgs a = mix_args(c);
     if (c->mol_ns == 3) return launch_mix_ns<3>(c, a, cell, energy);
     return launch_mix_ns<4>(c, a, cell, energy);
+}
+
+// The molecule extent bound of this evaluation into the context's per-bead
+// sums (slot S_EXT of bead 0, cleared with them), from the mode-1 positions.
+cudaError_t launch_mol_extent(pinyb200_ctx *c)
+{
+    if (!c->use_mol || c->nmol == 0) return cudaSuccess;
+    const double *xm = c->P > 1 ? c->d_xmod : c->d_posT;
+    const int blocks = std::max(1, std::min((c->nmol + 255) / 256, c->sm_count * 4));
+    mol_extent_kernel<<<blocks, 256, 0, c->stream>>>(c->d_mstart, c->nmol, xm,
+                                                      (unsigned long long *)(c->d_acc + S_EXT));
+    return cudaGetLastError();
+}
+
+struct ExtBox {
+    const int *mstart;
+    int nmol;
+    const double *xm;
+    unsigned long long *out;
+};
+
+__global__ void __launch_bounds__(256) mol_extent_batch_kernel(const __grid_constant__ BoxTab<ExtBox> t)
+{
+    PINYB200_BOX_LOOP(t, i, vb, (mol_extent_body(t.arg[i].mstart, t.arg[i].nmol, t.arg[i].xm, t.arg[i].out, vb)));
+}
+
+cudaError_t launch_mol_extent_batch(const std::vector<pinyb200_ctx *> &box, int sm_count, cudaStream_t st)
+{
+    BoxTabBuilder<ExtBox> tb;
+    for (pinyb200_ctx *c : box) {
+        if (!c->use_mol || c->nmol == 0) continue;
+        tb.add(ExtBox{c->d_mstart, c->nmol, c->P > 1 ? c->d_xmod : c->d_posT, (unsigned long long *)(c->d_acc + S_EXT)},
+               (c->nmol + 255) / 256, 1, (double)c->nmol);
+    }
+    return launch_tables(tb, (const void *)mol_extent_batch_kernel, 256, 0, sm_count,
+                         [&](const BoxTab<ExtBox> &t, int g) { mol_extent_batch_kernel<<<g, 256, 0, st>>>(t); });
 }
 
 // Site-pair table pattern of a context: 1 q-TIP4P/F-like (4 sites), 2

@@ -1243,7 +1243,7 @@ __device__ __forceinline__ void line_fft(typename Cplx<R>::T *sm, int N, int nl,
 // FP64 ones and the multi-box ones (whose run-time argument table costs
 // registers) hold 2.
 #ifndef PINYB200_FFT_BLOCKS
-#define PINYB200_FFT_BLOCKS 2
+#define PINYB200_FFT_BLOCKS 4
 #endif
 #define PINYB200_FFT_LB(R, NF) (NF > 0 ? (sizeof(R) == 4 ? PINYB200_FFT_BLOCKS : 2) : 1)
 
