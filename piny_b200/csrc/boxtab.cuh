@@ -104,14 +104,22 @@ struct BoxTabBuilder {
     }
 };
 
-// Resident CTAs of a persistent launch: the blocks of the launch, at most
-// the SMs times the blocks of this kernel one SM holds.
+// Waves of resident CTAs a batched launch holds (0: one CTA per block of
+// the launch, which lets the block scheduler interleave launches of
+// parallel graph branches).
+#ifndef PINYB200_BATCH_WAVES
+#define PINYB200_BATCH_WAVES 1
+#endif
+
+// CTAs of a persistent launch: the blocks of the launch, at most the SMs
+// times the blocks of this kernel one SM holds (times the waves).
 inline int persistent_grid(const void *func, int threads, size_t smem, int sm_count, int blocks)
 {
+    if (PINYB200_BATCH_WAVES <= 0) return std::max(1, blocks);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;
-    const long long cap = (long long)per_sm * sm_count;
+    const long long cap = (long long)per_sm * sm_count * PINYB200_BATCH_WAVES;
     return (int)std::max<long long>(1, std::min<long long>(blocks, cap));
 }
 
