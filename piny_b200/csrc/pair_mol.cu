@@ -21,6 +21,7 @@
 //     operation order, as in the site kernel.
 #include <algorithm>
 #include <map>
+#include <tuple>
 #include <vector>
 #include <cmath>
 #include <cstddef>
@@ -1205,7 +1206,6 @@ struct MixArgs {
     const int *nchunk, *chunk, *bad, *mj;
     const unsigned *mask;
     const int *mstart;
-    int ntyp, nuniq, nsplin, stride;
     const double *posT, *xmod;
     const unsigned long long *ext;  // extent bound of the evaluation (mol_extent_kernel), or nullptr
     const int *atm_typ;
@@ -1217,6 +1217,13 @@ struct MixArgs {
     const float4 *tabfe; // [2][nuniq][nsplin][2]: vdW then Coulomb; force and energy rows interleaved
     double *forceT;
     double *acc;
+};
+
+// The water model's site-pair constants of the MIXED kernel: the same for
+// every box of one model, so a multi-box launch takes them once, outside
+// its per-box table.
+struct MixSite {
+    int ntyp, nuniq, nsplin, stride;
     int toff[16];        // per site pair si * NS + sj: u * nsplin + 2, its rows at nint(t) = 0
     float q2[16];        // charge product of the site pair
     int eflag[16];       // tables the site pair uses: 1 vdW, 2 Coulomb
@@ -1239,7 +1246,8 @@ constexpr unsigned kTip4pCoul = 0xEEE0u, kTip4pVdw = 0x1u;  // O H H M: H, M cha
 constexpr unsigned kSpcCoul = 0x1FFu, kSpcVdw = 0x1u;       // O H H: all charged; LJ on O-O
 
 template <int P, int NS, bool ENERGY, unsigned CM, unsigned VM>
-__device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell &cell, const VBlk vb)
+__device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const MixSite &m, const Cell &cell,
+                                                    const VBlk vb)
 {
     constexpr int G = P >= 32 ? 32 : P;  // lanes per molecule pair
     constexpr int JPI = 32 / G;          // molecule pairs per warp step
@@ -1249,7 +1257,7 @@ __device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell
         const int si = threadIdx.x / NS, sj = threadIdx.x % NS;
         const int nm0 = a.mstart[1];
         const int ia = si < nm0 ? si : 0, ja = sj < nm0 ? sj : 0;
-        const int p = pair_type(a.atm_typ[ia], a.atm_typ[ja], a.ntyp);
+        const int p = pair_type(a.atm_typ[ia], a.atm_typ[ja], m.ntyp);
         const int u = a.inter_map[p];
         const double q2 = a.charge[ia] * a.charge[ja];
         float4 c;
@@ -1259,7 +1267,7 @@ __device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell
         c.w = (float)q2;
         pc.c[threadIdx.x] = c;
         pc.q2[threadIdx.x] = (float)q2;
-        pc.o[threadIdx.x] = make_int2(u * a.nsplin, a.has_vdw[u]);
+        pc.o[threadIdx.x] = make_int2(u * m.nsplin, a.has_vdw[u]);
     }
     if (ENERGY)
         for (int c = 0; c < 8; c++) sacc[c][threadIdx.x] = 0.0;
@@ -1275,14 +1283,14 @@ __device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell
     const int sub = lane / G;
     const int b = (lane % G) + 32 * vb.y;  // bead
     const double *__restrict__ posT = a.posT;
-    const float rc2 = a.rc2, dri = a.dri_f, rmd = a.rmd, tmax = a.tmax;
+    const float rc2 = m.rc2, dri = m.dri_f, rmd = m.rmd, tmax = m.tmax;
     constexpr float kRound = 12582912.0f;  // 1.5 * 2^23: x + kRound - kRound = nearest integer of x
 
     const double ext2 = ext2_of(a.ext);  // image test margin of this evaluation
     const int nch = *a.nchunk;
     for (int ch = warp; ch < nch; ch += nwarps) {
         const int mi = a.chunk[3 * ch], beg = a.chunk[3 * ch + 1], end = a.chunk[3 * ch + 2];
-        const int i0 = mi * a.stride, ni = a.stride;
+        const int i0 = mi * m.stride, ni = m.stride;
         float ei[NS][3], fi[NS][3];
 #pragma unroll
         for (int s = 0; s < NS; s++) {
@@ -1297,7 +1305,7 @@ __device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell
         for (int k = beg + sub; k < end; k += JPI) {
             const int mj = __ldcg(a.mj + k);
             const unsigned mask = __ldcg(a.mask + k);
-            const int j0 = mj * a.stride;
+            const int j0 = mj * m.stride;
             // site-0 image from the mode-1 separation (FP64) and whether site
             // pairs may take other images
             double sh0[3];
@@ -1311,7 +1319,7 @@ __device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell
             }
             if (near) {
                 mol_pair_near<float, P, NS, true, ENERGY>(posT, a.xmod, a.forceT, &pc, a.tab,
-                                                           (size_t)a.nuniq * a.nsplin, a.nsplin - 2, i0, j0, mask, b,
+                                                           (size_t)m.nuniq * m.nsplin, m.nsplin - 2, i0, j0, mask, b,
                                                            cell.h[0], cell.h[4], cell.h[8], cell.hi[0], cell.hi[4],
                                                            cell.hi[8], &sacc[0][threadIdx.x]);
                 continue;
@@ -1344,8 +1352,8 @@ __device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell
 #pragma unroll
                 for (int si = 0; si < NS; si++) {
                     const int sp = si * NS + sj;
-                    const bool coul = CM == kAnyPair ? (a.eflag[sp] & 2) != 0 : ((CM >> sp) & 1u) != 0;
-                    const bool vdw = VM == kAnyPair ? (a.eflag[sp] & 1) != 0 : ((VM >> sp) & 1u) != 0;
+                    const bool coul = CM == kAnyPair ? (m.eflag[sp] & 2) != 0 : ((CM >> sp) & 1u) != 0;
+                    const bool vdw = VM == kAnyPair ? (m.eflag[sp] & 1) != 0 : ((VM >> sp) & 1u) != 0;
                     if (CM != kAnyPair && !coul && !vdw) continue;  // a pair the masks never hold
                     if (!((mask >> sp) & 1u)) continue;
                     const float rx = dj[sj][0] + ei[si][0];
@@ -1360,25 +1368,25 @@ __device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell
                         const float del = t - __fsub_rn(tr, kRound);
                         // with energies: the force and energy rows of an interval
                         // sit side by side (one cache line for both loads)
-                        const float4 *row = tab + (a.toff[sp] + kn);
-                        const float4 *rfe = a.tabfe + 2 * (a.toff[sp] + kn);
+                        const float4 *row = tab + (m.toff[sp] + kn);
+                        const float4 *rfe = a.tabfe + 2 * (m.toff[sp] + kn);
                         float dv = 0.0f;
                         float4 ecf = make_float4(0.f, 0.f, 0.f, 0.f), evf = ecf;
                         if (coul) {
                             float4 cf;
                             if (ENERGY) {
-                                ldg_keep_pair(rfe + 2 * a.tstride, cf, ecf);
+                                ldg_keep_pair(rfe + 2 * m.tstride, cf, ecf);
                             } else {
-                                cf = ldg_keep(row + T_CDV0C * a.tstride);
+                                cf = ldg_keep(row + T_CDV0C * m.tstride);
                             }
-                            dv = a.q2[sp] * (cf.x + del * (cf.y + del * (cf.z + del * cf.w)));
+                            dv = m.q2[sp] * (cf.x + del * (cf.y + del * (cf.z + del * cf.w)));
                         }
                         if (vdw) {
                             float4 cf;
                             if (ENERGY) {
                                 ldg_keep_pair(rfe, cf, evf);
                             } else {
-                                cf = ldg_keep(row + T_CDV0 * a.tstride);
+                                cf = ldg_keep(row + T_CDV0 * m.tstride);
                             }
                             dv += cf.x + del * (cf.y + del * (cf.z + del * cf.w));
                         }
@@ -1391,7 +1399,7 @@ __device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell
                         fjz -= fz;
                         if (ENERGY) {
                             if (vdw) evs += evf.x + del * (evf.y + del * (evf.z + del * evf.w));
-                            if (coul) ecs += a.q2[sp] * (ecf.x + del * (ecf.y + del * (ecf.z + del * ecf.w)));
+                            if (coul) ecs += m.q2[sp] * (ecf.x + del * (ecf.y + del * (ecf.z + del * ecf.w)));
                         }
                     }
                 }
@@ -1455,9 +1463,10 @@ __device__ __forceinline__ void mol_pair_mixed_body(const MixArgs &a, const Cell
 
 template <int P, int NS, bool ENERGY, unsigned CM = kAnyPair, unsigned VM = kAnyPair>
 __global__ void __launch_bounds__(128, PINYB200_MIX_BLOCKS)
-    mol_pair_mixed_kernel(const __grid_constant__ MixArgs a, const __grid_constant__ Cell cell)
+    mol_pair_mixed_kernel(const __grid_constant__ MixArgs a, const __grid_constant__ MixSite m,
+                          const __grid_constant__ Cell cell)
 {
-    mol_pair_mixed_body<P, NS, ENERGY, CM, VM>(a, cell, hw_blk());
+    mol_pair_mixed_body<P, NS, ENERGY, CM, VM>(a, m, cell, hw_blk());
 }
 
 // Many boxes of one bead count and site pattern in one persistent launch.
@@ -1474,9 +1483,9 @@ struct MixBox {
 #endif
 template <int P, int NS, bool ENERGY, unsigned CM = kAnyPair, unsigned VM = kAnyPair>
 __global__ void __launch_bounds__(128, PINYB200_MIX_BATCH_BLOCKS)
-    mol_pair_mixed_batch_kernel(const __grid_constant__ BoxTab<MixBox> t)
+    mol_pair_mixed_batch_kernel(const __grid_constant__ BoxTab<MixBox> t, const __grid_constant__ MixSite m)
 {
-    PINYB200_BOX_LOOP(t, i, vb, (mol_pair_mixed_body<P, NS, ENERGY, CM, VM>(t.arg[i].a, t.arg[i].cell, vb)));
+    PINYB200_BOX_LOOP(t, i, vb, (mol_pair_mixed_body<P, NS, ENERGY, CM, VM>(t.arg[i].a, m, t.arg[i].cell, vb)));
 }
 
 // ---------------------------------------------------------------------------
@@ -1755,20 +1764,21 @@ cudaError_t launch_mol_pair(pinyb200_ctx *c, const Cell &cell, bool energy)
 
 
 template <int P, int NS, unsigned CM, unsigned VM>
-static void launch_mix_pattern(pinyb200_ctx *c, const MixArgs &a, const Cell &cell, bool energy, dim3 grid)
+static void launch_mix_pattern(pinyb200_ctx *c, const MixArgs &a, const MixSite &m, const Cell &cell, bool energy,
+                               dim3 grid)
 {
     const int threads = 128;
     if (energy) {
         carveout_pref((const void *)mol_pair_mixed_kernel<P, NS, true, CM, VM>, c->pair_carveout);
-        mol_pair_mixed_kernel<P, NS, true, CM, VM><<<grid, threads, 0, c->stream>>>(a, cell);
+        mol_pair_mixed_kernel<P, NS, true, CM, VM><<<grid, threads, 0, c->stream>>>(a, m, cell);
     } else {
         carveout_pref((const void *)mol_pair_mixed_kernel<P, NS, false, CM, VM>, c->pair_carveout);
-        mol_pair_mixed_kernel<P, NS, false, CM, VM><<<grid, threads, 0, c->stream>>>(a, cell);
+        mol_pair_mixed_kernel<P, NS, false, CM, VM><<<grid, threads, 0, c->stream>>>(a, m, cell);
     }
 }
 
 template <int P, int NS>
-static void launch_mix_t(pinyb200_ctx *c, const MixArgs &a, const Cell &cell, bool energy)
+static void launch_mix_t(pinyb200_ctx *c, const MixArgs &a, const MixSite &m, const Cell &cell, bool energy)
 {
     const int threads = 128;
     long long blocks = ((long long)c->chunk_cap * 32 + threads - 1) / threads;
@@ -1783,24 +1793,24 @@ static void launch_mix_t(pinyb200_ctx *c, const MixArgs &a, const Cell &cell, bo
         if (c->mix_eflag[k] & 1) vm |= 1u << k;
     }
     if (NS == 4 && cm == kTip4pCoul && vm == kTip4pVdw)
-        launch_mix_pattern<P, NS, kTip4pCoul, kTip4pVdw>(c, a, cell, energy, grid);
+        launch_mix_pattern<P, NS, kTip4pCoul, kTip4pVdw>(c, a, m, cell, energy, grid);
     else if (NS == 3 && cm == kSpcCoul && vm == kSpcVdw)
-        launch_mix_pattern<P, NS, kSpcCoul, kSpcVdw>(c, a, cell, energy, grid);
+        launch_mix_pattern<P, NS, kSpcCoul, kSpcVdw>(c, a, m, cell, energy, grid);
     else
-        launch_mix_pattern<P, NS, kAnyPair, kAnyPair>(c, a, cell, energy, grid);
+        launch_mix_pattern<P, NS, kAnyPair, kAnyPair>(c, a, m, cell, energy, grid);
 }
 
 template <int NS>
-static cudaError_t launch_mix_ns(pinyb200_ctx *c, const MixArgs &a, const Cell &cell, bool energy)
+static cudaError_t launch_mix_ns(pinyb200_ctx *c, const MixArgs &a, const MixSite &m, const Cell &cell, bool energy)
 {
     switch (c->P) {
-    case 1: launch_mix_t<1, NS>(c, a, cell, energy); break;
-    case 2: launch_mix_t<2, NS>(c, a, cell, energy); break;
-    case 4: launch_mix_t<4, NS>(c, a, cell, energy); break;
-    case 8: launch_mix_t<8, NS>(c, a, cell, energy); break;
-    case 16: launch_mix_t<16, NS>(c, a, cell, energy); break;
-    case 32: launch_mix_t<32, NS>(c, a, cell, energy); break;
-    case 64: launch_mix_t<64, NS>(c, a, cell, energy); break;
+    case 1: launch_mix_t<1, NS>(c, a, m, cell, energy); break;
+    case 2: launch_mix_t<2, NS>(c, a, m, cell, energy); break;
+    case 4: launch_mix_t<4, NS>(c, a, m, cell, energy); break;
+    case 8: launch_mix_t<8, NS>(c, a, m, cell, energy); break;
+    case 16: launch_mix_t<16, NS>(c, a, m, cell, energy); break;
+    case 32: launch_mix_t<32, NS>(c, a, m, cell, energy); break;
+    case 64: launch_mix_t<64, NS>(c, a, m, cell, energy); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -1817,10 +1827,6 @@ static MixArgs mix_args(pinyb200_ctx *c)
     a.mj = c->d_mj;
     a.mask = c->d_mmask;
     a.mstart = c->d_mstart;
-    a.ntyp = s.ntyp;
-    a.nuniq = s.nuniq;
-    a.nsplin = s.nsplin;
-    a.stride = c->mol_stride;
     a.posT = c->d_posT;
     a.xmod = c->P > 1 ? c->d_xmod : c->d_posT;
     a.ext = (const unsigned long long *)(c->d_acc + S_EXT);
@@ -1835,25 +1841,39 @@ static MixArgs mix_args(pinyb200_ctx *c)
     a.tabfe = c->d_tabfe;
     a.forceT = c->d_forceT;
     a.acc = c->d_acc;
-    for (int k = 0; k < 16; k++) {
-        a.toff[k] = c->mix_toff[k];
-        a.q2[k] = c->mix_q2[k];
-        a.eflag[k] = c->mix_eflag[k];
-    }
-    a.tstride = s.nuniq * s.nsplin;
-    a.rc2 = c->mix_rc2;
-    a.dri_f = c->mix_dri;
-    a.rmd = c->mix_rmd;
-    a.tmax = c->mix_tmax;
     return a;
+}
+
+// Site-pair constants of the MIXED molecule-pair kernel for one context.
+static MixSite mix_site(const pinyb200_ctx *c)
+{
+    const DeviceSystem &s = c->sys;
+    MixSite m;
+    memset(&m, 0, sizeof(m));
+    m.ntyp = s.ntyp;
+    m.nuniq = s.nuniq;
+    m.nsplin = s.nsplin;
+    m.stride = c->mol_stride;
+    for (int k = 0; k < 16; k++) {
+        m.toff[k] = c->mix_toff[k];
+        m.q2[k] = c->mix_q2[k];
+        m.eflag[k] = c->mix_eflag[k];
+    }
+    m.tstride = s.nuniq * s.nsplin;
+    m.rc2 = c->mix_rc2;
+    m.dri_f = c->mix_dri;
+    m.rmd = c->mix_rmd;
+    m.tmax = c->mix_tmax;
+    return m;
 }
 
 // The MIXED kernel with combined per-site-pair tables (pinyb200_ctx::mix_ok).
 cudaError_t launch_mol_pair_mixed(pinyb200_ctx *c, const Cell &cell, bool energy)
 {
     const MixArgs a = mix_args(c);
-    if (c->mol_ns == 3) return launch_mix_ns<3>(c, a, cell, energy);
-    return launch_mix_ns<4>(c, a, cell, energy);
+    const MixSite m = mix_site(c);
+    if (c->mol_ns == 3) return launch_mix_ns<3>(c, a, m, cell, energy);
+    return launch_mix_ns<4>(c, a, m, cell, energy);
 }
 
 // The molecule extent bound of this evaluation into the context's per-bead
@@ -1912,6 +1932,7 @@ static cudaError_t launch_mix_batch_t(const std::vector<pinyb200_ctx *> &box, co
                                       bool energy, int sm_count, cudaStream_t st)
 {
     BoxTabBuilder<MixBox> tb;
+    const MixSite m = mix_site(box[0]);  // one model per group (launch_mol_pair_mixed_batch)
     for (size_t i = 0; i < box.size(); i++) {
         pinyb200_ctx *c = box[i];
         // blocks of the box's own grid-stride loop over its chunks: about
@@ -1925,8 +1946,8 @@ static cudaError_t launch_mix_batch_t(const std::vector<pinyb200_ctx *> &box, co
     cudaError_t err = carveout_pref(fn, box.empty() ? 25 : box[0]->pair_carveout);
     if (err != cudaSuccess) return err;
     return launch_tables(tb, fn, 128, 0, sm_count, [&](const BoxTab<MixBox> &t, int g) {
-        if (energy) mol_pair_mixed_batch_kernel<P, NS, true, CM, VM><<<g, 128, 0, st>>>(t);
-        else mol_pair_mixed_batch_kernel<P, NS, false, CM, VM><<<g, 128, 0, st>>>(t);
+        if (energy) mol_pair_mixed_batch_kernel<P, NS, true, CM, VM><<<g, 128, 0, st>>>(t, m);
+        else mol_pair_mixed_batch_kernel<P, NS, false, CM, VM><<<g, 128, 0, st>>>(t, m);
     });
 }
 
@@ -1951,14 +1972,16 @@ static cudaError_t launch_mix_batch_p(int P, const std::vector<pinyb200_ctx *> &
 cudaError_t launch_mol_pair_mixed_batch(const std::vector<pinyb200_ctx *> &box, const std::vector<Cell> &cells,
                                         bool energy, int sm_count, cudaStream_t st)
 {
-    std::map<std::pair<int, int>, std::pair<std::vector<pinyb200_ctx *>, std::vector<Cell>>> groups;
+    // groups of one bead count, site pattern and set of site-pair constants
+    std::map<std::tuple<int, int, std::string>, std::pair<std::vector<pinyb200_ctx *>, std::vector<Cell>>> groups;
     for (size_t i = 0; i < box.size(); i++) {
-        auto &g = groups[std::make_pair(box[i]->P, mix_pattern(box[i]))];
+        const MixSite ms = mix_site(box[i]);
+        auto &g = groups[std::make_tuple(box[i]->P, mix_pattern(box[i]), std::string((const char *)&ms, sizeof(ms)))];
         g.first.push_back(box[i]);
         g.second.push_back(cells[i]);
     }
     for (auto &kv : groups) {
-        const int P = kv.first.first, pat = kv.first.second;
+        const int P = std::get<0>(kv.first), pat = std::get<1>(kv.first);
         cudaError_t err;
         if (pat == 1)
             err = launch_mix_batch_p<4, kTip4pCoul, kTip4pVdw>(P, kv.second.first, kv.second.second, energy, sm_count,
