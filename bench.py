@@ -55,7 +55,9 @@ def parse_args():
     ap.add_argument("--no-energy", action="store_true", help="forces only (PINYB200_NO_ENERGY), for profiling")
     ap.add_argument("--fd", action="store_true", help="c5_grad: also check against central differences")
     ap.add_argument("--batch-branches", action="store_true",
-                    help="c4_batch: one graph branch per box instead of the multi-box kernels")
+                    help="c4_batch: one graph branch per box (no timing of the two forms)")
+    ap.add_argument("--batch-kernels", action="store_true",
+                    help="c4_batch: the multi-box kernels (no timing of the two forms)")
     ap.add_argument("--tuning", default="", help="pin a launch shape: tile,pair_kernel,blocks_per_sm,overlap")
     return ap.parse_args()
 
@@ -964,8 +966,9 @@ def respa_cpu_baseline(spec, pos_A, rk, levels):
 
 def run_batch(args, ws, rank, local):
     """64 uneven TIP4P/F boxes, all beads, one CUDA graph launch per step:
-    the multi-box kernels (one persistent launch per phase and shape group)
-    unless --batch-branches asks for one graph branch per box."""
+    the faster (timed at capture) of the multi-box kernels (one persistent
+    launch per phase and shape group) and one graph branch per box, unless
+    --batch-kernels or --batch-branches pins one."""
     import torch
 
     from piny_b200 import system, water
@@ -1005,9 +1008,9 @@ def run_batch(args, ws, rank, local):
     batch = DeviceBatch(boxes)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    br = args.batch_branches
+    br, bk = args.batch_branches, args.batch_kernels
     for _ in range(max(3, args.warmup)):
-        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream, branches=br)
+        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream, branches=br, kernels=bk)
     torch.cuda.synchronize()
     fused, graph_launches = batch.last_mode()
     sampler = ClockSampler(local)
@@ -1022,7 +1025,7 @@ def run_batch(args, ws, rank, local):
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream, branches=br)
+        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream, branches=br, kernels=bk)
         ev1.record(stream)
         ev1.synchronize()
         step_ms.append(ev0.elapsed_time(ev1))
@@ -1045,7 +1048,7 @@ def run_batch(args, ws, rank, local):
         ev0.record(stream)
         for i in range(nbox):
             keep[3 * i].copy_(pins[i][0], non_blocking=True)
-        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream, branches=br)
+        batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream, branches=br, kernels=bk)
         for i in range(nbox):
             pins[i][1].copy_(keep[3 * i + 2], non_blocking=True)
         ev1.record(stream)
@@ -1053,6 +1056,20 @@ def run_batch(args, ws, rank, local):
         if k >= 2:
             e2e_ms.append(ev0.elapsed_time(ev1))
     e2e = float(np.mean(e2e_ms))
+    # each form pinned, for the record (the timed steps above ran the kept one)
+    forms_ms = {}
+    for name, fb, fk in (("multi_box_kernels", False, True), ("branches", True, False)):
+        ts = []
+        for k in range(6):
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            batch.energy_force_device(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream, branches=fb, kernels=fk)
+            ev1.record(stream)
+            ev1.synchronize()
+            if k >= 1:
+                ts.append(ev0.elapsed_time(ev1))
+        forms_ms[name] = {"ms": float(np.median(ts)), "launches": batch.last_mode()[1]}
     hbm, peak_kind = peaks()
     achieved = alg / (ms * 1e-3) / 1e9
     nbytes = sum(int(p[0].numel()) * 8 for p in pins)
@@ -1081,7 +1098,8 @@ def run_batch(args, ws, rank, local):
                        "launch": ("one CUDA graph launch per step: multi-box kernels, one persistent launch "
                                   "per phase and shape group (%d kernel nodes for %d boxes)" % (graph_launches, nbox))
                        if fused else ("one CUDA graph launch per step (boxes as parallel branches, "
-                                      "%d kernel nodes)" % graph_launches)},
+                                      "%d kernel nodes)" % graph_launches),
+                       "forms_ms": forms_ms},
             "roofline": {"bound": "hbm", "kernel": "whole batch step", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg,

@@ -46,8 +46,8 @@ enum {
     PINYB200_SITE_PAIRS = 4,     /* walk the site list instead of molecule pairs    */
     PINYB200_TUNE_AGAIN = 8,     /* pinyb200_autotune: ignore remembered results    */
     PINYB200_UPDATE_LIST = 16,   /* device list test and rebuild before the forces  */
-    PINYB200_BATCH_BRANCHES = 32 /* batch call: one graph branch per box instead of */
-                                 /* the multi-box kernels                           */
+    PINYB200_BATCH_BRANCHES = 32, /* batch call: one graph branch per box           */
+    PINYB200_BATCH_KERNELS = 64   /* batch call: the multi-box kernels, untimed     */
 };
 
 /*
@@ -441,7 +441,10 @@ int pinyb200_set_tuning(pinyb200_ctx *ctx, const int *choice);
  * boxes sharing its compile-time shape, walking every (box, bead, tile or
  * chunk) block of the group; the groups' PME chains, pair launches and the
  * intramolecular launch are parallel branches of the graph.  Otherwise
- * every box is a parallel branch of its own kernels.  The call returns when the work is done.  PINY's Python
+ * every box is a parallel branch of its own kernels.  Where the multi-box
+ * kernels cover the boxes, the capture times both forms on the call's
+ * inputs and keeps the faster, unless flags ask for one form
+ * (PINYB200_BATCH_KERNELS or PINYB200_BATCH_BRANCHES).  The call returns when the work is done.  PINY's Python
  * driver reaches several replicas through one energy_control call per CLASS
  * (python/piny/piny.pyx:426-436); this entry point has no counterpart there.
  */

@@ -249,6 +249,57 @@ void drop_graph(pinyb200_batch *bt)
     bt->graph = nullptr;
 }
 
+// Capture one form of the batch call into a graph: the multi-box kernels
+// (after one plain run of them, so that kernel attributes and occupancy
+// queries happen outside the capture) or one branch per box.
+int capture_form(pinyb200_batch *bt, bool fused, const double *const *d_pos, const double *const *d_xmod,
+                 const double *const *hmat, int flags, double *const *d_force, cudaGraph_t *out,
+                 cudaGraphExec_t *exec)
+{
+    const int nbox = (int)bt->box.size();
+    *out = nullptr;
+    *exec = nullptr;
+    if (fused) {
+        int rc = fused_enqueue(bt, d_pos, d_xmod, hmat, flags, d_force);
+        if (rc) return rc;
+        BCK(cudaStreamSynchronize(bt->stream));
+    }
+    BCK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeRelaxed));
+    int rc = PINYB200_OK;
+    cudaError_t ce = fused ? cudaSuccess : cudaEventRecord(bt->fork, bt->stream);
+    if (fused) rc = fused_enqueue(bt, d_pos, d_xmod, hmat, flags, d_force);
+    for (int i = 0; i < nbox && !fused && ce == cudaSuccess && rc == PINYB200_OK; i++) {
+        pinyb200_ctx *c = bt->box[i];
+        ce = cudaStreamWaitEvent(c->stream, bt->fork, 0);
+        if (ce != cudaSuccess) break;
+        const Cell cell = cell_from_hmat(hmat[i]);
+        rc = enqueue_device(c, d_pos[i], d_xmod ? d_xmod[i] : nullptr, cell, flags, d_force[i], false,
+                            bt->h_acc + bt->acc_off[i]);
+        if (rc) break;
+        ce = cudaEventRecord(bt->join[i], c->stream);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(bt->stream, bt->join[i], 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(bt->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return fused ? rc : bfail(bt, rc, "batch capture: enqueue failed");
+    }
+    if (ce != cudaSuccess || ee != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return bfail(bt, PINYB200_ERR_CUDA,
+                     std::string("batch capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+    }
+    const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
+    if (ei != cudaSuccess) {
+        cudaGraphDestroy(g);
+        *exec = nullptr;
+        return bfail(bt, PINYB200_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ei));
+    }
+    *out = g;
+    return PINYB200_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -424,44 +475,45 @@ int pinyb200_batch_energy_force_device(pinyb200_batch *bt, const double *const *
             if (rc) return bfail(bt, rc, std::string("batch warm-up: ") + pinyb200_last_error(c));
             BCK(cudaStreamSynchronize(c->stream));
         }
-        const bool fused = fused_ok(bt, hmat, flags);
-        if (fused) {
-            // one plain run of the multi-box kernels: kernel attributes and
-            // occupancy queries happen outside the capture
-            int rc = fused_enqueue(bt, d_pos, d_xmod, hmat, flags, d_force);
-            if (rc) return rc;
-            BCK(cudaStreamSynchronize(bt->stream));
+        // the forms to capture: the multi-box kernels where they cover the
+        // boxes, the branches otherwise; both, when neither is asked for,
+        // and the faster one is kept (timed on these inputs)
+        const bool can_fuse = fused_ok(bt, hmat, flags);
+        std::vector<int> forms;
+        if (!can_fuse) forms = {0};
+        else if (flags & PINYB200_BATCH_KERNELS) forms = {1};
+        else forms = {1, 0};
+        float tbest = 1e30f;
+        for (int form : forms) {
+            cudaGraph_t g = nullptr;
+            cudaGraphExec_t x = nullptr;
+            int rc = capture_form(bt, form == 1, d_pos, d_xmod, hmat, flags, d_force, &g, &x);
+            if (rc) {
+                drop_graph(bt);
+                return rc;
+            }
+            float t = 0.0f;
+            if (forms.size() > 1) {
+                for (int r = 0; r < 2; r++) {
+                    BCK(cudaEventRecord(bt->ev[0], bt->stream));
+                    BCK(cudaGraphLaunch(x, bt->stream));
+                    BCK(cudaEventRecord(bt->ev[1], bt->stream));
+                    BCK(cudaStreamSynchronize(bt->stream));
+                    BCK(cudaEventElapsedTime(&t, bt->ev[0], bt->ev[1]));
+                }
+            }
+            if (t < tbest) {
+                drop_graph(bt);
+                tbest = t;
+                bt->graph = g;
+                bt->exec = x;
+                bt->fused = form;
+                bt->launches = count_kernel_nodes(g);
+            } else {
+                cudaGraphExecDestroy(x);
+                cudaGraphDestroy(g);
+            }
         }
-        BCK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeRelaxed));
-        int rc = PINYB200_OK;
-        cudaError_t ce = fused ? cudaSuccess : cudaEventRecord(bt->fork, bt->stream);
-        if (fused) rc = fused_enqueue(bt, d_pos, d_xmod, hmat, flags, d_force);
-        for (int i = 0; i < nbox && !fused && ce == cudaSuccess && rc == PINYB200_OK; i++) {
-            pinyb200_ctx *c = bt->box[i];
-            ce = cudaStreamWaitEvent(c->stream, bt->fork, 0);
-            if (ce != cudaSuccess) break;
-            const Cell cell = cell_from_hmat(hmat[i]);
-            rc = enqueue_device(c, d_pos[i], d_xmod ? d_xmod[i] : nullptr, cell, flags, d_force[i], false,
-                                bt->h_acc + bt->acc_off[i]);
-            if (rc) break;
-            ce = cudaEventRecord(bt->join[i], c->stream);
-            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(bt->stream, bt->join[i], 0);
-        }
-        cudaGraph_t g = nullptr;
-        const cudaError_t ee = cudaStreamEndCapture(bt->stream, &g);
-        if (rc) {
-            if (g) cudaGraphDestroy(g);
-            return fused ? rc : bfail(bt, rc, "batch capture: enqueue failed");
-        }
-        if (ce != cudaSuccess || ee != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            return bfail(bt, PINYB200_ERR_CUDA,
-                         std::string("batch capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee));
-        }
-        bt->graph = g;
-        bt->fused = fused ? 1 : 0;
-        bt->launches = count_kernel_nodes(g);
-        BCK(cudaGraphInstantiate(&bt->exec, bt->graph, 0));
         bt->key_ptr = kp;
         bt->key_h = kh;
         bt->key_flags = flags;

@@ -26,6 +26,7 @@ SITE_PAIRS = 4
 TUNE_AGAIN = 8
 UPDATE_LIST = 16       # PINYB200_UPDATE_LIST
 BATCH_BRANCHES = 32    # PINYB200_BATCH_BRANCHES
+BATCH_KERNELS = 64     # PINYB200_BATCH_KERNELS
 
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NO_DEVICE", 4: "ERR_LIST_OVERFLOW", 5: "ERR_CUTOFF",
           6: "ERR_TIMEOUT", 7: "ERR_NAN", 8: "ERR_UNSUPPORTED", 9: "ERR_STATE"}
@@ -525,9 +526,10 @@ class DeviceBatch:
         self.h = h
 
     def energy_force_device(self, d_pos, d_xmod, hmats, d_force, stream=None, energy=True, update_list=False,
-                            branches=False, distribute_ghosts=False):
-        """Every box in one graph launch: the multi-box kernels where they
-        cover the boxes, else (or with branches=True) one graph branch per box."""
+                            branches=False, kernels=False, distribute_ghosts=False):
+        """Every box in one graph launch: the faster of the multi-box kernels
+        and one graph branch per box (timed at capture) where the kernels
+        cover the boxes, else branches; kernels=True / branches=True pick one."""
         n = len(self.boxes)
         P = (C.c_void_p * n)(*[int(p) for p in d_pos])
         X = (C.c_void_p * n)(*[None if x is None else int(x) for x in d_xmod]) if d_xmod is not None else None
@@ -536,7 +538,8 @@ class DeviceBatch:
         H = (_pd * n)(*[_dp(h) for h in hm])
         E = (PinyEnergies * n)()
         flags = (0 if energy else NO_ENERGY) | (UPDATE_LIST if update_list else 0) | \
-            (BATCH_BRANCHES if branches else 0) | (DISTRIB_GHOSTS if distribute_ghosts else 0)
+            (BATCH_BRANCHES if branches else 0) | (BATCH_KERNELS if kernels else 0) | \
+            (DISTRIB_GHOSTS if distribute_ghosts else 0)
         rc = self.L.pinyb200_batch_energy_force_device(self.h, P, X, H, flags, F, E,
                                                        None if stream is None else C.c_void_p(stream))
         if rc != 0:

@@ -87,6 +87,42 @@ def test_batch_matches_single_boxes(prec):
         r[0].close()
 
 
+def test_batch_keeps_the_faster_form():
+    """Without a form asked for, a batch the multi-box kernels cover is
+    captured in both forms and the faster kept: either form is valid, the
+    mode query names it, and the forces equal the one-box path."""
+    import torch
+
+    from piny_b200.lib import DeviceBatch, DeviceBox
+    boxes = _boxes(nbox=6, seed=33)
+    ctxs, d_pos, d_xm, d_f, hm, keep = [], [], [], [], [], []
+    for sp, pos, S in boxes:
+        b = DeviceBox(S, sp.nbeads, "mixed")
+        xmod = pos.mean(axis=0) if sp.nbeads > 1 else None
+        b.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+        d = torch.from_numpy(pos).to("cuda:0")
+        dx = torch.from_numpy(xmod).to("cuda:0") if xmod is not None else None
+        f = torch.zeros_like(d)
+        keep += [d, dx, f]
+        ctxs.append(b)
+        d_pos.append(d.data_ptr())
+        d_xm.append(None if dx is None else dx.data_ptr())
+        d_f.append(f.data_ptr())
+        hm.append(S["hmat"])
+    batch = DeviceBatch(ctxs)
+    batch.energy_force_device(d_pos, d_xm, hm, d_f)
+    fused, nk = batch.last_mode()
+    assert nk > 0 and (nk <= 48 if fused else nk > 4 * len(boxes))
+    torch.cuda.synchronize()
+    for i, (sp, pos, S) in enumerate(boxes):
+        b0, f0, _ = _single(S, pos, sp.nbeads, "fp64")
+        b0.close()
+        assert rel_rms(keep[3 * i + 2].cpu().numpy(), f0) < 1e-5, i
+    batch.close()
+    for b in ctxs:
+        b.close()
+
+
 def test_every_launch_shape_gives_the_same_forces():
     boxes = _boxes(nbox=2, seed=5)
     for sp, pos, S in boxes:
@@ -241,7 +277,7 @@ def test_batch_kernels_match_branches(flags):
     ghosts = flags.get("distribute_ghosts", False)
     for call in range(2):
         ef = batch.energy_force_device(d_pos, d_xm, hm, [f.data_ptr() for f in f_fused], energy=energy,
-                                       distribute_ghosts=ghosts)
+                                       distribute_ghosts=ghosts, kernels=True)
         fused, nk = batch.last_mode()
         assert fused and 0 < nk <= 48, (fused, nk)
         eb = batch.energy_force_device(d_pos, d_xm, hm, [f.data_ptr() for f in f_branch], energy=energy,
