@@ -1936,8 +1936,10 @@ static cudaError_t launch_mix_batch_t(const std::vector<pinyb200_ctx *> &box, co
     for (size_t i = 0; i < box.size(); i++) {
         pinyb200_ctx *c = box[i];
         // blocks of the box's own grid-stride loop over its chunks: about
-        // two chunks per warp
-        const long long vb = std::max<long long>(1, (c->chunk_cap + 7) / 8);
+        // sixteen chunks per warp, so that a block's set-up (site-pair
+        // constants) and energy flush (FP64 atomics per bead and slot) are
+        // spread over enough molecule pairs
+        const long long vb = std::max<long long>(1, (c->chunk_cap + 63) / 64);
         tb.add(MixBox{mix_args(c), cells[i]}, (int)std::min<long long>(vb, 1 << 20), P > 32 ? P / 32 : 1,
                (double)c->chunk_cap * P);
     }
