@@ -1003,12 +1003,11 @@ def run_batch(args, ws, rank, local):
     setup_s = time.perf_counter() - t0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    choices = []
-    for i, b in enumerate(boxes):
-        choices.append(b.autotune(d_pos[i], d_xm[i], hm[i], reps=2)[0])
-    tune_s = time.perf_counter() - t0
     batch = DeviceBatch(boxes)
     stream = torch.cuda.current_stream(dev)
+    tune_ms, tune_keep = batch.tune(d_pos, d_xm, hm, d_f, stream=stream.cuda_stream)
+    choices = [b.tuning() for b in boxes]
+    tune_s = time.perf_counter() - t0
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     br, bk = args.batch_branches, args.batch_kernels
     for _ in range(max(3, args.warmup)):
@@ -1104,7 +1103,8 @@ def run_batch(args, ws, rank, local):
             "config": {"workload": args.config, "boxes": nbox, "bead_evals_per_step": nbead,
                        "molecules": [sp.nmol for sp in specs], "beads": [sp.nbeads for sp in specs],
                        "pme_grid": [sp.grid for sp in specs], "precision": args.precision,
-                       "tuning": choices, "setup_s": setup_s, "autotune_s": tune_s,
+                       "tuning": choices, "tuning_set": {"kept": tune_keep, "batch_ms": tune_ms},
+                       "setup_s": setup_s, "autotune_s": tune_s,
                        "l2": "256 MiB buffer written between timed steps; CUDA events on the launch stream",
                        "launch": ("one CUDA graph launch per step: multi-box kernels, one persistent launch "
                                   "per phase and shape group (%d kernel nodes for %d boxes)" % (graph_launches, nbox))

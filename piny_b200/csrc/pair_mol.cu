@@ -1933,14 +1933,25 @@ static cudaError_t launch_mix_batch_t(const std::vector<pinyb200_ctx *> &box, co
 {
     BoxTabBuilder<MixBox> tb;
     const MixSite m = mix_site(box[0]);  // one model per group (launch_mol_pair_mixed_batch)
+    // Blocks of each box's own grid-stride loop over its chunks: about 16
+    // chunks' worth of 32-bead work per warp (a warp takes 32 / P molecule
+    // pairs at a time below 32 beads), so that a block's set-up (site-pair
+    // constants) and energy flush (FP64 atomics per bead and slot) are
+    // spread over enough molecule pairs; more, down to 2 chunks per warp,
+    // while the group has fewer than two blocks per resident CTA.
+    const int G = P >= 32 ? 32 : P;
+    std::vector<long long> vb(box.size());
+    long long tot = 0;
+    for (size_t i = 0; i < box.size(); i++) {
+        vb[i] = std::max<long long>(1, (box[i]->chunk_cap * G + 4LL * 16 * 32 - 1) / (4LL * 16 * 32));
+        tot += vb[i] * (P > 32 ? P / 32 : 1);
+    }
+    const long long want = 2LL * sm_count * PINYB200_MIX_BATCH_BLOCKS;
+    const long long scale = tot < want ? (want + tot - 1) / tot : 1;
     for (size_t i = 0; i < box.size(); i++) {
         pinyb200_ctx *c = box[i];
-        // blocks of the box's own grid-stride loop over its chunks: about
-        // sixteen chunks per warp, so that a block's set-up (site-pair
-        // constants) and energy flush (FP64 atomics per bead and slot) are
-        // spread over enough molecule pairs
-        const long long vb = std::max<long long>(1, (c->chunk_cap + 63) / 64);
-        tb.add(MixBox{mix_args(c), cells[i]}, (int)std::min<long long>(vb, 1 << 20), P > 32 ? P / 32 : 1,
+        const long long v = std::min(vb[i] * scale, std::max<long long>(1, (c->chunk_cap + 7) / 8));
+        tb.add(MixBox{mix_args(c), cells[i]}, (int)std::min<long long>(v, 1 << 20), P > 32 ? P / 32 : 1,
                (double)c->chunk_cap * P);
     }
     const void *fn = energy ? (const void *)mol_pair_mixed_batch_kernel<P, NS, true, CM, VM>

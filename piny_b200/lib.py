@@ -552,6 +552,30 @@ class DeviceBatch:
         self.L.pinyb200_batch_last_ms(self.h, C.byref(ms))
         return ms.value
 
+    def tune(self, d_pos, d_xmod, hmats, d_force, stream=None, reps=3):
+        """Launch shapes for the batch as a whole: each box's own autotuned
+        shape (pinyb200_autotune, timed on the box alone) and the default
+        shapes are each timed as a batch call (the capture keeps the faster
+        graph form for each); the faster set is kept.  Returns
+        {set name: ms} and the kept set's name."""
+        base = [b.tuning() for b in self.boxes]
+        own = [b.autotune(d_pos[i], None if d_xmod is None else d_xmod[i], hmats[i], reps=2)[0]
+               for i, b in enumerate(self.boxes)]
+        times = {}
+        for name, choice in (("per_box", own), ("defaults", base)):
+            for b, ch in zip(self.boxes, choice):
+                b.set_tuning(ch)
+            ts = []
+            for k in range(reps + 1):
+                self.energy_force_device(d_pos, d_xmod, hmats, d_force, stream=stream)
+                if k:
+                    ts.append(self.last_ms())
+            times[name] = float(np.median(ts))
+        keep = min(times, key=times.get)
+        for b, ch in zip(self.boxes, own if keep == "per_box" else base):
+            b.set_tuning(ch)
+        return times, keep
+
     def last_mode(self):
         """(fused, kernel launches) of the graph the last call ran."""
         f, k = C.c_int(), C.c_int()
