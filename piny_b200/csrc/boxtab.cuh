@@ -59,11 +59,11 @@ __device__ __forceinline__ VBlk tab_blk(const BoxTab<A> &t, int i, int w)
 
 // The persistent loop of a batched kernel over table t: binds box index i
 // and VBlk vb for the body, then a block-wide barrier.
-#define PINYB200_BOX_LOOP(t, i, vb, BODY)                                        \
+#define PINYB200_BOX_LOOP(t, i, vb, ...)                                         \
     for (int w_ = (int)blockIdx.x; w_ < (t).off[(t).n]; w_ += (int)gridDim.x) { \
         const int i = tab_box((t).off, (t).n, w_);                               \
         const VBlk vb = tab_blk((t), i, w_);                                     \
-        BODY;                                                                    \
+        __VA_ARGS__;                                                             \
         __syncthreads();                                                         \
     }
 
