@@ -47,7 +47,8 @@ enum {
     PINYB200_TUNE_AGAIN = 8,     /* pinyb200_autotune: ignore remembered results    */
     PINYB200_UPDATE_LIST = 16,   /* device list test and rebuild before the forces  */
     PINYB200_BATCH_BRANCHES = 32, /* batch call: one graph branch per box           */
-    PINYB200_BATCH_KERNELS = 64   /* batch call: the multi-box kernels, untimed     */
+    PINYB200_BATCH_KERNELS = 64   /* batch call: the multi-box kernels where they   */
+                                  /* cover the boxes (branches otherwise), untimed  */
 };
 
 /*
