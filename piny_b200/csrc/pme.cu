@@ -1253,7 +1253,11 @@ __device__ __forceinline__ void line_fft(typename Cplx<R>::T *sm, int N, int nl,
 #ifndef PINYB200_FFT_BLOCKS
 #define PINYB200_FFT_BLOCKS 4
 #endif
+#ifndef PINYB200_PLANE_BLOCKS
+#define PINYB200_PLANE_BLOCKS PINYB200_FFT_BLOCKS  // the plane passes alone (their shared plane allows 6)
+#endif
 #define PINYB200_FFT_LB(R, NF) (NF > 0 ? (sizeof(R) == 4 ? PINYB200_FFT_BLOCKS : 2) : 1)
+#define PINYB200_PLANE_LB(R, NF) (NF > 0 ? (sizeof(R) == 4 ? PINYB200_PLANE_BLOCKS : 2) : 1)
 
 template <typename R>
 __device__ __forceinline__ void load_twiddles(R *dst, const R *src, int N)
@@ -1295,7 +1299,7 @@ __device__ __forceinline__ void plane_fwd_body(const R *__restrict__ q, typename
 }
 
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, PINYB200_FFT_LB(R, NF)) plane_fwd_kernel(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
+__global__ void __launch_bounds__(256, PINYB200_PLANE_LB(R, NF)) plane_fwd_kernel(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
                                                         int Na, int Nb, int Nc, const R *__restrict__ twa,
                                                         const R *__restrict__ twb)
 {
@@ -1341,7 +1345,7 @@ __device__ __forceinline__ void plane_inv_body(const typename Cplx<R>::T *__rest
 }
 
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, PINYB200_FFT_LB(R, NF)) plane_inv_kernel(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phi,
+__global__ void __launch_bounds__(256, PINYB200_PLANE_LB(R, NF)) plane_inv_kernel(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phi,
                                                         int Na, int Nb, int Nc, const R *__restrict__ twa,
                                                         const R *__restrict__ twb)
 {
