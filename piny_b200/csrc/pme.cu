@@ -1049,12 +1049,12 @@ __device__ __forceinline__ void gather_tile_c_body(const PmeArgs &a, const Cell 
 // Resident blocks per SM the FP32 gather (order <= 8) is compiled for: its
 // shared tile of 16-point edges allows 4; at 4 the 64-register cap spills
 // 60 bytes and the C3 evaluation is still 2.8 % faster than at 3 (80
-// registers).
+// registers).  The others hold 2 (128 registers).
 #ifndef PINYB200_GATHER_BLOCKS
 #define PINYB200_GATHER_BLOCKS 4
 #endif
 template <typename R, int NI, int TT>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 && NI <= 8 ? PINYB200_GATHER_BLOCKS : 1)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 && NI <= 8 ? PINYB200_GATHER_BLOCKS : 2)
     gather_tile_c_kernel(const __grid_constant__ PmeArgs a,
                                                             const __grid_constant__ Cell cell,
                                                             const __grid_constant__ TileArgs t)
