@@ -301,3 +301,40 @@ def test_batch_kernels_match_branches(flags):
     batch.close()
     for b in ctxs:
         b.close()
+
+
+def test_batch_tune_keeps_a_shape_set_that_gives_the_same_forces():
+    """DeviceBatch.tune times the batch with every box's own autotuned
+    launch shape and with the defaults, keeps the faster set, and the
+    forces stay those of the one-box FP64 path (MIXED tolerance)."""
+    import torch
+
+    from piny_b200.lib import DeviceBatch, DeviceBox
+    boxes = _boxes(nbox=5, seed=21)
+    ctxs, d_pos, d_xm, d_f, hm, keep = [], [], [], [], [], []
+    for sp, pos, S in boxes:
+        b = DeviceBox(S, sp.nbeads, "mixed")
+        xmod = pos.mean(axis=0) if sp.nbeads > 1 else None
+        b.build_list(pos[0], xmod, S["hmat"], S["cutskin2"])
+        d = torch.from_numpy(pos).to("cuda:0")
+        dx = torch.from_numpy(xmod).to("cuda:0") if xmod is not None else None
+        f = torch.zeros_like(d)
+        keep += [d, dx, f]
+        ctxs.append(b)
+        d_pos.append(d.data_ptr())
+        d_xm.append(None if dx is None else dx.data_ptr())
+        d_f.append(f.data_ptr())
+        hm.append(S["hmat"])
+    batch = DeviceBatch(ctxs)
+    times, kept = batch.tune(d_pos, d_xm, hm, d_f, reps=2)
+    assert set(times) == {"per_box", "defaults"} and kept in times and all(t > 0 for t in times.values())
+    assert times[kept] == min(times.values())
+    batch.energy_force_device(d_pos, d_xm, hm, d_f)
+    torch.cuda.synchronize()
+    for i, (sp, pos, S) in enumerate(boxes):
+        b0, f0, _ = _single(S, pos, sp.nbeads, "fp64")
+        b0.close()
+        assert rel_rms(keep[3 * i + 2].cpu().numpy(), f0) < 1e-5, i
+    batch.close()
+    for b in ctxs:
+        b.close()

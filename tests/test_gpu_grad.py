@@ -184,3 +184,41 @@ def test_ghost_parameter_without_tabulated_coulomb(oracle):
     assert abs(dF[k] - gL) <= 1e-7 * abs(gL)
     assert abs(dE[k] - gE) <= 1e-7 * abs(gE)
     box.close()
+
+
+def test_c5_size_adjoint_matches_device_differences():
+    """The gradient configuration itself (1024 q-TIP4P/F, 16 beads, 32^3
+    mesh, order 8): the FP64 adjoint against central differences (h = 1e-5
+    relative) of the FP64 device energy and force-matching loss, at the
+    tolerances above; the MIXED adjoint against the FP64 one."""
+    from piny_b200 import params, water
+    from piny_b200.params import PARAMS, PinyForceField
+    spec = water.named_spec("tip4pf_1024_p16")
+    pos_A = water.build_positions(spec)
+    theta = params.theta_of(spec.model)
+    rng = np.random.default_rng(2024)
+    theta_t = theta * (1.0 + rng.uniform(-0.02, 0.02, size=theta.shape))
+    field = PinyForceField(spec, pos_A, "fp64")
+    _, f_target = field.energy_forces(theta_t)
+    gE_fd, gL_fd = np.zeros(len(theta)), np.zeros(len(theta))
+    for k in range(len(theta)):
+        h = 1e-5 * abs(theta[k])
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += h
+        tm[k] -= h
+        Ep, Fp = field.energy_forces(tp)
+        Em, Fm = field.energy_forces(tm)
+        gE_fd[k] = (Ep - Em) / (2 * h)
+        gL_fd[k] = (((Fp - f_target) ** 2).sum() - ((Fm - f_target) ** 2).sum()) / (2 * h)
+    field.close()
+    _, _, gE, gL = _adjoint(spec, pos_A, theta, f_target, "fp64")
+    sE, sL = np.abs(gE_fd).max(), np.abs(gL_fd).max()
+    for k in range(len(theta)):
+        assert abs(gE[k] - gE_fd[k]) <= 2e-5 * sE, ("dE", k, gE[k], gE_fd[k])
+        assert abs(gL[k] - gL_fd[k]) <= 2e-5 * sL, ("dL", k, gL[k], gL_fd[k])
+        if PARAMS[k] != "gamma":
+            assert abs(gE[k] - gE_fd[k]) <= 2e-6 * abs(gE_fd[k]), ("dE", PARAMS[k], gE[k], gE_fd[k])
+            assert abs(gL[k] - gL_fd[k]) <= 2e-6 * abs(gL_fd[k]), ("dL", PARAMS[k], gL[k], gL_fd[k])
+    _, _, gE32, gL32 = _adjoint(spec, pos_A, theta, f_target, "mixed")
+    assert np.abs(gE32 - gE).max() <= 1e-3 * np.abs(gE).max()
+    assert np.abs(gL32 - gL).max() <= 1e-3 * np.abs(gL).max()
