@@ -1691,6 +1691,15 @@ struct PmeBox {
     Cell cell;
 };
 
+// Resident blocks per SM of the multi-box plane FFT passes and gather (their
+// run-time argument tables cost registers over the one-box kernels').
+#ifndef PINYB200_PLANE_BATCH_BLOCKS
+#define PINYB200_PLANE_BATCH_BLOCKS 2
+#endif
+#ifndef PINYB200_GATHER_BATCH_BLOCKS
+#define PINYB200_GATHER_BATCH_BLOCKS 1
+#endif
+
 struct FftBox {
     const void *q;      // real grid (forward input, inverse output)
     void *spec;         // half spectrum
@@ -1723,13 +1732,14 @@ __global__ void __launch_bounds__(256) spread_batch_kernel(const __grid_constant
 }
 
 template <typename R, int NI, int TT>
-__global__ void __launch_bounds__(256) gather_batch_kernel(const __grid_constant__ BoxTab<PmeBox> t)
+__global__ void __launch_bounds__(256, NI <= 8 ? PINYB200_GATHER_BATCH_BLOCKS : 1)
+    gather_batch_kernel(const __grid_constant__ BoxTab<PmeBox> t)
 {
     PINYB200_BOX_LOOP(t, i, vb, (gather_tile_c_body<R, NI, TT>(t.arg[i].a, t.arg[i].cell, t.arg[i].t, vb)));
 }
 
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1)
+__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_PLANE_BATCH_BLOCKS : 1)
     plane_fwd_batch_kernel(const __grid_constant__ BoxTab<FftBox> t)
 {
     typedef typename Cplx<R>::T C2;
@@ -1750,7 +1760,7 @@ __global__ void __launch_bounds__(256, NF > 0 ? 2 : 1)
 }
 
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1)
+__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_PLANE_BATCH_BLOCKS : 1)
     plane_inv_batch_kernel(const __grid_constant__ BoxTab<FftBox> t)
 {
     typedef typename Cplx<R>::T C2;
