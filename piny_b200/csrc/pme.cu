@@ -1692,12 +1692,14 @@ struct PmeBox {
 };
 
 // Resident blocks per SM of the multi-box plane FFT passes and gather (their
-// run-time argument tables cost registers over the one-box kernels').
+// run-time argument tables cost registers over the one-box kernels'): 3 and
+// 4 (80 and 64 registers, 16-36 bytes of spills) take the 64-box C4 step
+// from 5.56 to 5.36 ms against 2 and 1.
 #ifndef PINYB200_PLANE_BATCH_BLOCKS
-#define PINYB200_PLANE_BATCH_BLOCKS 2
+#define PINYB200_PLANE_BATCH_BLOCKS 3
 #endif
 #ifndef PINYB200_GATHER_BATCH_BLOCKS
-#define PINYB200_GATHER_BATCH_BLOCKS 1
+#define PINYB200_GATHER_BATCH_BLOCKS 4
 #endif
 
 struct FftBox {
