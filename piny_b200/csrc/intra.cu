@@ -469,15 +469,9 @@ cudaError_t launch_ghost_distrib(pinyb200_ctx *c, double *fT)
     return cudaGetLastError();
 }
 
-// Bonds, bends and excluded-pair corrections as one typed launch (the
-// multi-box kernel over this one box) or as three launches.
-#ifndef PINYB200_INTRA_ONE_LAUNCH
-#define PINYB200_INTRA_ONE_LAUNCH 0
-#endif
 cudaError_t launch_intra(pinyb200_ctx *c, const Cell &cell, bool energy)
 {
     (void)cell;
-    if (PINYB200_INTRA_ONE_LAUNCH) return launch_intra_batch(std::vector<pinyb200_ctx *>(1, c), energy, c->sm_count, c->stream);
     const DeviceSystem &s = c->sys;
     IntraArgs a;
     a.natm = s.natm;
