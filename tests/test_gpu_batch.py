@@ -171,7 +171,8 @@ def test_c4_set_matches_oracle_box_by_box(prec, oracle):
     every box's pair set equals the oracle's bit for bit and the forces of
     its first and last bead match the oracle's within 1e-12 (FP64) / 1e-5
     (MIXED) relative RMS; energies of boxes with at most 8 beads (the oracle
-    evaluates all their beads) within 1e-11 relative / 1e-6 of the terms."""
+    evaluates all their beads) within 1e-11 relative / 1e-6 of the terms.
+    MIXED runs the multi-box kernels, FP64 one graph branch per box."""
     import torch
 
     from helpers import pair_hash
@@ -205,7 +206,9 @@ def test_c4_set_matches_oracle_box_by_box(prec, oracle):
     tol = {"fp64": 1e-12, "mixed": 1e-5}[prec]
     etol = {"fp64": 1e-11, "mixed": 1e-6}[prec]
     for call in range(2):  # capture, then replay of the graph
-        es = batch.energy_force_device(d_pos, d_xm, hm, d_f)
+        # MIXED: the multi-box kernels (the form the capture keeps for this set)
+        es = batch.energy_force_device(d_pos, d_xm, hm, d_f, kernels=(prec == "mixed"))
+        assert batch.last_mode()[0] == (prec == "mixed")
         torch.cuda.synchronize()
         for i, (sp, pos, S, xmod, pi, pj, b) in enumerate(boxes):
             P = sp.nbeads
