@@ -1172,13 +1172,18 @@ def main():
     t0 = time.perf_counter()
     npairs = box.build_list(pos[0], xmod, hmat, S["cutskin2"])
     list_s = time.perf_counter() - t0
-    if args.tuning:
-        box.set_tuning([int(v) for v in args.tuning.split(",")])
-
     stream = torch.cuda.current_stream(dev)
     d_pos = torch.from_numpy(pos).to(dev)
     d_xmod = torch.from_numpy(xmod).to(dev)
     d_force = torch.empty_like(d_pos)
+    # launch shapes: pinned by --tuning, else the project's autotuner on these inputs
+    tuning = {}
+    if args.tuning:
+        box.set_tuning([int(v) for v in args.tuning.split(",")])
+        tuning[args.precision] = box.tuning()
+    else:
+        tuning[args.precision] = box.autotune(d_pos.data_ptr(), d_xmod.data_ptr(), hmat, reps=3,
+                                              energy=not args.no_energy)[0]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def step(b, force):
@@ -1224,6 +1229,9 @@ def main():
     if not args.no_fp64:
         box64 = DeviceBox(S, P, "fp64")
         box64.build_list(pos[0], xmod, hmat, S["cutskin2"])
+        if not args.tuning:
+            tuning["fp64"] = box64.autotune(d_pos.data_ptr(), d_xmod.data_ptr(), hmat, reps=3,
+                                            energy=not args.no_energy)[0]
         f64 = torch.empty_like(d_pos)
         for _ in range(2):
             step(box64, f64)
@@ -1356,6 +1364,8 @@ def main():
             "vs_baseline": None, "dtype": "f32+f64acc" if args.precision == "mixed" else "f64",
             "data": "synthetic",
             "config": box_config(spec, args, int(natm), int(S["ngrid_a"]), int(npairs), list_s),
+            "tuning": {k: {"pme_tile": v[0], "pair_kernel": v[1], "pair_blocks_per_sm": v[2], "pme_overlap": v[3]}
+                       for k, v in tuning.items()},
             "roofline": roof,
             "kernels": kernels,
             "vs_piny": piny,
