@@ -554,15 +554,20 @@ class DeviceBatch:
 
     def tune(self, d_pos, d_xmod, hmats, d_force, stream=None, reps=3):
         """Launch shapes for the batch as a whole: each box's own autotuned
-        shape (pinyb200_autotune, timed on the box alone) and the default
-        shapes are each timed as a batch call (the capture keeps the faster
-        graph form for each); the faster set is kept.  Returns
-        {set name: ms} and the kept set's name."""
+        shape (pinyb200_autotune, timed on the box alone), the default
+        shapes, and the defaults with each box's own PME tile edge are each
+        timed as a batch call (the capture keeps the faster graph form for
+        each); the fastest set is kept.  Returns {set name: ms} and the kept
+        set's name."""
         base = [b.tuning() for b in self.boxes]
         own = [b.autotune(d_pos[i], None if d_xmod is None else d_xmod[i], hmats[i], reps=2)[0]
                for i, b in enumerate(self.boxes)]
         times = {}
-        for name, choice in (("per_box", own), ("defaults", base)):
+        # the defaults with each box's own PME tile edge: the tile choice
+        # alone, without the per-box pair-kernel choices
+        tiles = [[o[0]] + list(d[1:]) for o, d in zip(own, base)]
+        sets = {"per_box": own, "defaults": base, "defaults_own_tiles": tiles}
+        for name, choice in sets.items():
             for b, ch in zip(self.boxes, choice):
                 b.set_tuning(ch)
             ts = []
@@ -572,7 +577,7 @@ class DeviceBatch:
                     ts.append(self.last_ms())
             times[name] = float(np.median(ts))
         keep = min(times, key=times.get)
-        for b, ch in zip(self.boxes, own if keep == "per_box" else base):
+        for b, ch in zip(self.boxes, sets[keep]):
             b.set_tuning(ch)
         return times, keep
 
