@@ -1750,8 +1750,13 @@ __global__ void __launch_bounds__(256, NF > 0 ? PINYB200_PLANE_BATCH_BLOCKS : 1)
                                              t.arg[i].Nc, (const R *)t.arg[i].tw[0], (const R *)t.arg[i].tw[1], vb)));
 }
 
+// (the multi-box slab pass: at 3, 80 registers spill 236 bytes and the C4
+// step takes 5.50 against 5.37 ms)
+#ifndef PINYB200_CONV_BATCH_BLOCKS
+#define PINYB200_CONV_BATCH_BLOCKS 2
+#endif
 template <typename R, int NF>
-__global__ void __launch_bounds__(256, NF > 0 ? 2 : 1)
+__global__ void __launch_bounds__(256, NF > 0 ? PINYB200_CONV_BATCH_BLOCKS : 1)
     conv_c_batch_kernel(const __grid_constant__ BoxTab<FftBox> t)
 {
     typedef typename Cplx<R>::T C2;
